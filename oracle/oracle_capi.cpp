@@ -1,0 +1,157 @@
+// oracle_capi.cpp -- TEST INFRASTRUCTURE ONLY: C entry points of the CPU
+// oracle (whir_oracle.hpp) for the Python tests (ctypes).  Never linked into,
+// or called by, the product library.
+#include "whir_oracle.hpp"
+
+#include <cstring>
+#include <exception>
+#include <new>
+
+using namespace oracle;
+
+namespace {
+Params make_params(u64 rho, u64 k, u64 sec, u64 powb, int unique) {
+    Params p;
+    p.starting_log_inv_rate = rho;
+    p.initial_folding_factor = k;
+    p.folding_factor = k;
+    p.security_level = sec;
+    p.pow_bits = powb;
+    p.unique_decoding = unique != 0;
+    p.batch_size = 1;
+    return p;
+}
+std::vector<E3> read_e3(const u64* w, size_t n) {
+    std::vector<E3> v(n);
+    for (size_t i = 0; i < n; ++i) for (int c = 0; c < 3; ++c) v[i].c[c] = w[3 * i + c];
+    return v;
+}
+}  // namespace
+
+extern "C" {
+
+void oracle_blake3(const u8* d, size_t n, u8* out) { Hash h = blake3(d, n); std::memcpy(out, h.data(), 32); }
+void oracle_sha3_256(const u8* d, size_t n, u8* out) { sha3_256(d, n, out); }
+void oracle_sha3_512(const u8* d, size_t n, u8* out) { sha3_512(d, n, out); }
+void oracle_shake128(const u8* d, size_t n, u8* out, size_t m) { shake128(d, n, out, m); }
+void oracle_keccak_f1600(u64* s) { keccak_f1600(s); }
+
+u64 oracle_fmul(u64 a, u64 b) { return fmul(a, b); }
+u64 oracle_root_of_unity(u64 n) { return root_of_unity(n); }
+void oracle_e3_mul(const u64* a, const u64* b, u64* out) {
+    E3 x, y;
+    for (int i = 0; i < 3; ++i) { x.c[i] = a[i]; y.c[i] = b[i]; }
+    E3 r = x * y;
+    for (int i = 0; i < 3; ++i) out[i] = r.c[i];
+}
+
+void oracle_ntt(u64* data, size_t n) {
+    std::vector<u64> v(data, data + n);
+    ntt_inplace(v);
+    std::memcpy(data, v.data(), n * 8);
+}
+// RS encode of one base vector into a row-major N x depth matrix.
+void oracle_rs_encode_base(const u64* v, size_t len, u64 N, u64 depth, u64* out) {
+    std::vector<u64> in(v, v + len);
+    auto m = rs_encode_base(in, N, depth);
+    std::memcpy(out, m.data(), m.size() * 8);
+}
+// RS encode of one Ext3 vector (AoS, 3 words per element) into AoS rows.
+void oracle_rs_encode_e3(const u64* v, size_t len, u64 N, u64 depth, u64* out) {
+    auto m = rs_encode_e3(read_e3(v, len), N, depth);
+    std::memcpy(out, m.data(), m.size() * 24);
+}
+// Merkle root (and optionally the node array) of `n` 32-byte leaves.
+void oracle_merkle_root(const u8* leaves, size_t n, u8* root_out, u8* nodes_out) {
+    std::vector<Hash> lv(n);
+    for (size_t i = 0; i < n; ++i) std::memcpy(lv[i].data(), leaves + 32 * i, 32);
+    auto nodes = merkle_build(lv);
+    std::memcpy(root_out, nodes.back().data(), 32);
+    if (nodes_out) for (size_t i = 0; i < nodes.size(); ++i) std::memcpy(nodes_out + 32 * i, nodes[i].data(), 32);
+}
+// Merkle opening hints; returns the number of 32-byte hints written.
+size_t oracle_merkle_open(const u8* leaves, size_t n, const u64* idx, size_t nidx, u8* out, size_t cap) {
+    std::vector<Hash> lv(n);
+    for (size_t i = 0; i < n; ++i) std::memcpy(lv[i].data(), leaves + 32 * i, 32);
+    auto nodes = merkle_build(lv);
+    auto hints = merkle_open(nodes, layers_for(n), std::vector<u64>(idx, idx + nidx));
+    for (size_t i = 0; i < hints.size() && i < cap; ++i) std::memcpy(out + 32 * i, hints[i].data(), 32);
+    return hints.size();
+}
+u64 oracle_find_nonce(const u8* ch, u64 threshold) { return find_nonce(ch, threshold); }
+
+// Opaque transcript for the per-primitive pins (base/Ext3 challenges).
+void* oracle_tx_new(void) { return new (std::nothrow) Transcript(); }
+void oracle_tx_free(void* t) { delete static_cast<Transcript*>(t); }
+void oracle_tx_absorb(void* t, const u8* d, size_t n) { static_cast<Transcript*>(t)->absorb(d, n); }
+void oracle_tx_message(void* t, const u8* d, size_t n) { static_cast<Transcript*>(t)->message_bytes(d, n); }
+void oracle_tx_squeeze(void* t, u8* out, size_t n) { static_cast<Transcript*>(t)->squeeze(out, n); }
+u64 oracle_tx_challenge_base(void* t) { return static_cast<Transcript*>(t)->challenge_base(); }
+void oracle_tx_challenge_e3(void* t, u64* out) {
+    E3 e = static_cast<Transcript*>(t)->challenge_e3();
+    for (int i = 0; i < 3; ++i) out[i] = e.c[i];
+}
+size_t oracle_tx_narg(void* t, u8* out, size_t cap) {
+    auto& v = static_cast<Transcript*>(t)->narg;
+    if (out) std::memcpy(out, v.data(), std::min(cap, v.size()));
+    return v.size();
+}
+
+void oracle_cli_domain_separator(u64 rho, u64 k, u64 sec, u64 powb, int unique, u8* out96) {
+    DomainSep ds = cli_domain_separator(make_params(rho, k, sec, powb, unique));
+    std::memcpy(out96, ds.protocol_id, 64);
+    std::memcpy(out96 + 64, ds.session_id, 32);
+}
+
+// Schedule of Config::from_params as a flat u64 array:
+//   [n_rounds, init_N, init_q, init_ood, init_sc_pow, skip_pow,
+//    per round: vec, N, q, ood, pow, sc_pow,  final_size, final_rounds, final_pow, final_sc_pow]
+size_t oracle_whir_config(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique, u64* out, size_t cap) {
+    try {
+        WhirCfg c = whir_from_params(1ull << n, make_params(rho, k, sec, powb, unique));
+        std::vector<u64> v{c.rounds.size(), c.initial.codeword_length, c.initial.in_domain, c.initial.out_domain,
+                           c.initial_sumcheck.pow_threshold, c.initial_skip_pow};
+        for (auto& r : c.rounds) {
+            v.insert(v.end(), {r.irs.vector_size, r.irs.codeword_length, r.irs.in_domain, r.irs.out_domain,
+                               r.pow_threshold, r.sumcheck.pow_threshold});
+        }
+        v.insert(v.end(), {c.final_sumcheck.initial_size, c.final_sumcheck.num_rounds, c.final_pow,
+                           c.final_sumcheck.pow_threshold});
+        for (size_t i = 0; i < v.size() && i < cap; ++i) out[i] = v[i];
+        return v.size();
+    } catch (const std::exception&) {
+        return 0;
+    }
+}
+
+// MLE of a base vector (2^n entries) at an Ext3 point (n coordinates).
+void oracle_mle_eval_base(const u64* v, u64 n, const u64* point, u64* out) {
+    std::vector<u64> vec(v, v + (1ull << n));
+    E3 r = mle_eval_base(vec, read_e3(point, n));
+    for (int i = 0; i < 3; ++i) out[i] = r.c[i];
+}
+
+// Whole commit + prove with the CLI domain separator and MLE-point forms.
+// Returns 0 on success; narg/hints lengths are written to lens[0], lens[1]
+// (the buffers receive min(cap, len) bytes).
+int oracle_whir_prove(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique, const u64* coeffs,
+                      const u64* points, size_t npoints, const u64* evals, u8* narg, size_t narg_cap,
+                      u8* hints, size_t hints_cap, u64* lens) {
+    try {
+        Params p = make_params(rho, k, sec, powb, unique);
+        std::vector<u64> v(coeffs, coeffs + (1ull << n));
+        Statement st;
+        for (size_t i = 0; i < npoints; ++i) st.mle_points.push_back(read_e3(points + 3 * n * i, n));
+        st.evaluations = read_e3(evals, npoints);
+        ProofOut o = prove(p, v, st, cli_domain_separator(p));
+        lens[0] = o.narg.size();
+        lens[1] = o.hints.size();
+        std::memcpy(narg, o.narg.data(), std::min(narg_cap, o.narg.size()));
+        std::memcpy(hints, o.hints.data(), std::min(hints_cap, o.hints.size()));
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,182 @@
+"""Test infrastructure: run the reference C++ prover (oracle/_ref/ref_driver)
+and the CPU restatement (oracle/liboracle.so) on the same inputs.
+
+Only the tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline and
+reference arms use this module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import struct
+import subprocess
+import tempfile
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+
+
+@dataclass
+class RefProof:
+    narg: bytes
+    hints: bytes
+    evaluations: np.ndarray  # (num_points, 3) uint64
+    commit_ms: float
+    prove_ms: float
+    verify_ok: float  # 1.0 accepted, 0.0 rejected, -1.0 not run
+
+
+def write_input(path, n, k, rho, sec, pow_bits, points, coeffs):
+    """Input file of ref_driver.cpp (format documented there)."""
+    points = np.ascontiguousarray(points, dtype=np.uint64).reshape(-1, n, 3)
+    coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+    assert coeffs.size == 1 << n
+    with open(path, "wb") as f:
+        f.write(struct.pack("<II", 0x49524857, 1))
+        f.write(struct.pack("<6Q", n, k, rho, sec, pow_bits, points.shape[0]))
+        f.write(points.tobytes())
+        f.write(coeffs.tobytes())
+
+
+def read_output(path, num_points) -> RefProof:
+    with open(path, "rb") as f:
+        b = f.read()
+    pos = 0
+    (ln,) = struct.unpack_from("<Q", b, pos); pos += 8
+    narg = b[pos:pos + ln]; pos += ln
+    (lh,) = struct.unpack_from("<Q", b, pos); pos += 8
+    hints = b[pos:pos + lh]; pos += lh
+    ev = np.frombuffer(b, dtype=np.uint64, count=3 * num_points, offset=pos).reshape(num_points, 3).copy()
+    pos += 24 * num_points
+    cms, pms, vok = struct.unpack_from("<3d", b, pos)
+    return RefProof(narg, hints, ev, cms, pms, vok)
+
+
+def ref_available() -> bool:
+    return os.access(REF_DRIVER, os.X_OK)
+
+
+def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1, threads=None,
+                  timeout=3600) -> RefProof:
+    """Runs the unmodified reference prover (compiled in place by oracle/Makefile)."""
+    if not ref_available():
+        raise FileNotFoundError(f"{REF_DRIVER} not built (make -C oracle ref)")
+    env = dict(os.environ)
+    if threads is not None:
+        env["OMP_NUM_THREADS"] = str(threads)
+    npts = np.asarray(points).reshape(-1, n, 3).shape[0]
+    with tempfile.TemporaryDirectory() as td:
+        inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        write_input(inp, n, k, rho, sec, pow_bits, points, coeffs)
+        cmd = [REF_DRIVER, inp, out] + (["--verify"] if verify else []) + (["--reps", str(reps)] if reps > 1 else [])
+        subprocess.run(cmd, check=True, env=env, timeout=timeout, stdout=subprocess.DEVNULL)
+        return read_output(out, npts)
+
+
+class Oracle:
+    """ctypes view of oracle/liboracle.so (the CPU restatement)."""
+
+    def __init__(self, path: str = ORACLE_SO):
+        self.lib = L = ctypes.CDLL(path)
+        u64, sz, p = ctypes.c_uint64, ctypes.c_size_t, ctypes.c_void_p
+        L.oracle_blake3.argtypes = [p, sz, p]
+        L.oracle_sha3_256.argtypes = [p, sz, p]
+        L.oracle_sha3_512.argtypes = [p, sz, p]
+        L.oracle_shake128.argtypes = [p, sz, p, sz]
+        L.oracle_fmul.argtypes = [u64, u64]; L.oracle_fmul.restype = u64
+        L.oracle_root_of_unity.argtypes = [u64]; L.oracle_root_of_unity.restype = u64
+        L.oracle_e3_mul.argtypes = [p, p, p]
+        L.oracle_ntt.argtypes = [p, sz]
+        L.oracle_rs_encode_base.argtypes = [p, sz, u64, u64, p]
+        L.oracle_rs_encode_e3.argtypes = [p, sz, u64, u64, p]
+        L.oracle_merkle_root.argtypes = [p, sz, p, p]
+        L.oracle_merkle_open.argtypes = [p, sz, p, sz, p, sz]; L.oracle_merkle_open.restype = sz
+        L.oracle_find_nonce.argtypes = [p, u64]; L.oracle_find_nonce.restype = u64
+        L.oracle_tx_new.restype = p
+        L.oracle_tx_free.argtypes = [p]
+        L.oracle_tx_absorb.argtypes = [p, p, sz]
+        L.oracle_tx_message.argtypes = [p, p, sz]
+        L.oracle_tx_squeeze.argtypes = [p, p, sz]
+        L.oracle_tx_challenge_base.argtypes = [p]; L.oracle_tx_challenge_base.restype = u64
+        L.oracle_tx_challenge_e3.argtypes = [p, p]
+        L.oracle_tx_narg.argtypes = [p, p, sz]; L.oracle_tx_narg.restype = sz
+        L.oracle_cli_domain_separator.argtypes = [u64, u64, u64, u64, ctypes.c_int, p]
+        L.oracle_whir_config.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, p, sz]
+        L.oracle_whir_config.restype = sz
+        L.oracle_mle_eval_base.argtypes = [p, u64, p, p]
+        L.oracle_whir_prove.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, p, p, sz, p, p, sz, p, sz, p]
+        L.oracle_whir_prove.restype = ctypes.c_int
+
+    # -- primitives -------------------------------------------------------
+    def blake3(self, data: bytes) -> bytes:
+        out = ctypes.create_string_buffer(32)
+        self.lib.oracle_blake3(data, len(data), out)
+        return out.raw
+
+    def ntt(self, v) -> np.ndarray:
+        a = np.ascontiguousarray(v, dtype=np.uint64).copy()
+        self.lib.oracle_ntt(a.ctypes.data, a.size)
+        return a
+
+    def rs_encode_base(self, v, N, depth) -> np.ndarray:
+        v = np.ascontiguousarray(v, dtype=np.uint64)
+        out = np.empty((N, depth), dtype=np.uint64)
+        self.lib.oracle_rs_encode_base(v.ctypes.data, v.size, N, depth, out.ctypes.data)
+        return out
+
+    def rs_encode_e3(self, v, N, depth) -> np.ndarray:
+        v = np.ascontiguousarray(v, dtype=np.uint64).reshape(-1, 3)
+        out = np.empty((N, depth, 3), dtype=np.uint64)
+        self.lib.oracle_rs_encode_e3(v.ctypes.data, v.shape[0], N, depth, out.ctypes.data)
+        return out
+
+    def merkle_root(self, leaves: bytes) -> bytes:
+        out = ctypes.create_string_buffer(32)
+        self.lib.oracle_merkle_root(leaves, len(leaves) // 32, out, None)
+        return out.raw
+
+    def merkle_open(self, leaves: bytes, idx) -> list:
+        idx = np.ascontiguousarray(idx, dtype=np.uint64)
+        cap = 64 * max(1, idx.size)
+        out = ctypes.create_string_buffer(32 * cap)
+        cnt = self.lib.oracle_merkle_open(leaves, len(leaves) // 32, idx.ctypes.data, idx.size, out, cap)
+        return [out.raw[32 * i:32 * i + 32] for i in range(cnt)]
+
+    def find_nonce(self, challenge: bytes, threshold: int) -> int:
+        return self.lib.oracle_find_nonce(challenge, threshold)
+
+    def domain_separator(self, rho, k, sec, pow_bits, unique=False) -> bytes:
+        out = ctypes.create_string_buffer(96)
+        self.lib.oracle_cli_domain_separator(rho, k, sec, pow_bits, int(unique), out)
+        return out.raw
+
+    def whir_config(self, n, rho, k, sec, pow_bits, unique=False) -> list:
+        out = (ctypes.c_uint64 * 512)()
+        cnt = self.lib.oracle_whir_config(n, rho, k, sec, pow_bits, int(unique), out, 512)
+        return list(out[:cnt])
+
+    def mle_eval_base(self, coeffs, point) -> np.ndarray:
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+        point = np.ascontiguousarray(point, dtype=np.uint64)
+        n = point.size // 3
+        out = np.zeros(3, dtype=np.uint64)
+        self.lib.oracle_mle_eval_base(coeffs.ctypes.data, n, point.ctypes.data, out.ctypes.data)
+        return out
+
+    def prove(self, n, k, rho, sec, pow_bits, points, coeffs, evaluations):
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+        points = np.ascontiguousarray(points, dtype=np.uint64).reshape(-1, n, 3)
+        evals = np.ascontiguousarray(evaluations, dtype=np.uint64).reshape(-1, 3)
+        cap = 64 << 20
+        narg = ctypes.create_string_buffer(cap)
+        hints = ctypes.create_string_buffer(cap)
+        lens = (ctypes.c_uint64 * 2)()
+        rc = self.lib.oracle_whir_prove(n, rho, k, sec, pow_bits, 0, coeffs.ctypes.data, points.ctypes.data,
+                                        points.shape[0], evals.ctypes.data, narg, cap, hints, cap, lens)
+        if rc != 0:
+            raise RuntimeError("oracle prove failed")
+        return narg.raw[:lens[0]], hints.raw[:lens[1]]
