@@ -1,0 +1,136 @@
+/* whirgpu.h -- C ABI of the B200-native WHIR prover (whirplonk_b200/libwhirgpu.so).
+ *
+ * Drop-in boundary for the reference C++ prover of hxd77/WhirPlonk
+ * (cpp/include/whir/protocols/whir/whir.hpp, whir_prover.hpp): the same
+ * ProtocolParameters, the same SHAKE128 Fiat-Shamir transcript and the same
+ * proof byte layout ({narg_string, hints}), for
+ *   M = Basefield<GoldilocksExt3> (Goldilocks vectors, Ext3 challenges),
+ *   hash = BLAKE3, one committed vector, MultilinearExtension statements.
+ * Everything below is plain C: opaque handles, pointers, sizes and status
+ * codes; no C++ types or exceptions cross this boundary.
+ *
+ * Threading: a context is used by one host thread at a time (the reference's
+ * NttEngine singletons and GpuPool are single-threaded too,
+ * cpp/include/whir/algebra/ntt/cooley_tukey_goldilocks.hpp:6-9).
+ */
+#ifndef WHIRGPU_H
+#define WHIRGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    WHIRGPU_OK = 0,
+    WHIRGPU_E_INVALID = 1,     /* bad argument or parameters the reference asserts on */
+    WHIRGPU_E_UNSUPPORTED = 2, /* valid for the reference but not on this path (e.g. SHA2 hash) */
+    WHIRGPU_E_OOM = 3,         /* device or pinned memory exhausted, or above the HBM budget */
+    WHIRGPU_E_CUDA = 4,        /* CUDA runtime error (text in whirgpu_last_error) */
+    WHIRGPU_E_DEVICE = 5,      /* a kernel reported an error word (overflow, PoW exhausted) */
+    WHIRGPU_E_TIMEOUT = 6      /* a bounded device wait expired */
+} whirgpu_status;
+
+/* Byte-for-byte the fields of whir::ProtocolParameters
+ * (cpp/include/whir/parameters.hpp:25-34), in the same order. */
+typedef struct {
+    uint8_t unique_decoding;
+    uint64_t starting_log_inv_rate;
+    uint64_t initial_folding_factor;
+    uint64_t folding_factor;
+    uint64_t security_level;
+    uint64_t pow_bits;
+    uint64_t batch_size;
+    uint8_t hash_id[32]; /* EngineId; only BLAKE3 (03e01749...5b4c) is on this path */
+} whirgpu_params;
+
+typedef struct whirgpu_ctx whirgpu_ctx;
+typedef struct whirgpu_transcript whirgpu_transcript;
+typedef struct whirgpu_witness whirgpu_witness;
+
+/* Coefficient pointers may be host or device memory. */
+#define WHIRGPU_INPUT_HOST 0
+#define WHIRGPU_INPUT_DEVICE 1
+
+/* ---- context ---------------------------------------------------------------
+ * One CUDA device, one stream, a workspace cache bounded by hbm_budget bytes
+ * (0 = no bound).  Replaces the reference's GpuPool singleton
+ * (cpp/cuda/cuda_integration.hpp:142-282). */
+whirgpu_status whirgpu_ctx_create(int device, uint64_t hbm_budget, whirgpu_ctx** out);
+void whirgpu_ctx_destroy(whirgpu_ctx* ctx);
+const char* whirgpu_last_error(const whirgpu_ctx* ctx);
+/* cudaStream_t of the context, for callers that time or order work around it. */
+void* whirgpu_stream(whirgpu_ctx* ctx);
+
+/* ---- parameters ------------------------------------------------------------
+ * Round schedule of Config::from_params (whir.hpp:118-224) as a flat array:
+ *   [n_rounds, init_N, init_q, init_ood, init_sumcheck_pow_thr, skip_pow_thr,
+ *    per round: vector_size, N, q, ood, pow_thr, sumcheck_pow_thr,
+ *    final_size, final_rounds, final_pow_thr, final_sumcheck_pow_thr]
+ * Returns the number of words (0 on invalid parameters). */
+size_t whirgpu_schedule(const whirgpu_params* params, uint64_t num_variables, uint64_t* out, size_t cap);
+
+/* Domain separator of the reference CLI (cpp/main.cpp:174-215):
+ * out[0..64) = SHA3-512(CBOR(params)), out[64..96) = SHA3-256(CBOR(session)). */
+whirgpu_status whirgpu_cli_domain_separator(const whirgpu_params* params, uint8_t out[96]);
+
+/* ---- transcript (ProverState, transcript.hpp:595-662) ------------------------ */
+whirgpu_status whirgpu_transcript_create(whirgpu_ctx* ctx, const uint8_t protocol_id[64], const uint8_t session_id[32],
+                                         const uint8_t* instance, size_t instance_len, whirgpu_transcript** out);
+void whirgpu_transcript_destroy(whirgpu_transcript* tx);
+/* Proof bytes after whirgpu_prove: pointers stay valid until the transcript is destroyed. */
+whirgpu_status whirgpu_proof_get(const whirgpu_transcript* tx, const uint8_t** narg, size_t* narg_len,
+                                 const uint8_t** hints, size_t* hints_len);
+
+/* ---- commit (Config::commit, whir.hpp:303-309) ---------------------------------
+ * Encodes, hashes and commits one vector of 2^num_variables canonical
+ * Goldilocks words; the codeword matrix and Merkle tree stay in HBM in the
+ * witness.  Work is queued on the context stream; the call returns without
+ * waiting for it. */
+whirgpu_status whirgpu_commit(whirgpu_ctx* ctx, const whirgpu_params* params, const uint64_t* coeffs,
+                              uint64_t num_variables, int coeffs_location, whirgpu_transcript* tx,
+                              whirgpu_witness** out);
+void whirgpu_witness_destroy(whirgpu_witness* w);
+
+/* ---- prove (Config::prove, whir_prover.hpp:56-407) ---------------------------
+ * Statement: num_points MultilinearExtension forms; points are
+ * num_points * num_variables Ext3 coordinates (3 words each, c0 c1 c2),
+ * evaluations are num_points Ext3 values (the claimed MLE values).
+ * On return the proof is complete and readable with whirgpu_proof_get.
+ * evaluation_point (optional) receives num_variables Ext3 values (the
+ * FinalClaim evaluation point), rlc (optional) num_points Ext3 values. */
+whirgpu_status whirgpu_prove(whirgpu_ctx* ctx, whirgpu_witness* witness, const uint64_t* points, size_t num_points,
+                             const uint64_t* evaluations, whirgpu_transcript* tx, uint64_t* evaluation_point,
+                             uint64_t* rlc);
+
+/* ---- helpers ------------------------------------------------------------------- */
+/* Multilinear extension of 2^num_variables base coefficients at an Ext3 point
+ * (MultilinearExtension::evaluate, linear_form.hpp:119-126), on the device. */
+whirgpu_status whirgpu_mle_evaluate(whirgpu_ctx* ctx, const uint64_t* coeffs, uint64_t num_variables,
+                                    int coeffs_location, const uint64_t* point, uint64_t out[3]);
+/* Seeded uniform Goldilocks words: ChaCha20 block function (RFC 8439),
+ * key = seed as 8 LE bytes then 24 zero bytes, nonce 0, counter from 0;
+ * each 64-bit LE keystream word below p is taken, others are skipped. */
+void whirgpu_sample_goldilocks(uint64_t seed, uint64_t* out, size_t count);
+/* Raw ChaCha20 block (for known-answer tests). */
+void whirgpu_chacha20_block(const uint8_t key[32], uint32_t counter, const uint8_t nonce[12], uint8_t out[64]);
+/* Page-locked host memory for fast host<->device copies. */
+void* whirgpu_host_alloc(size_t bytes);
+void whirgpu_host_free(void* p);
+
+/* ---- timing of the hot kernels (for roofline reporting) --------------------------
+ * When enabled, every kernel family is bracketed by CUDA events on the context
+ * stream; whirgpu_kernel_stats returns, per family, launches and total ms
+ * accumulated since the last reset.  Families: 0 NTT/LDE, 1 leaf hash,
+ * 2 Merkle, 3 OOD, 4 sumcheck, 5 covector, 6 PoW, 7 opening, 8 transcript. */
+#define WHIRGPU_NUM_FAMILIES 9
+whirgpu_status whirgpu_set_timing(whirgpu_ctx* ctx, int enabled);
+whirgpu_status whirgpu_kernel_stats(whirgpu_ctx* ctx, uint64_t launches[WHIRGPU_NUM_FAMILIES],
+                                    double ms[WHIRGPU_NUM_FAMILIES], int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WHIRGPU_H */

@@ -1,0 +1,22 @@
+"""B200-native WHIR prover (commit + prove over Goldilocks, Ext3 sumcheck,
+BLAKE3 Merkle commitments) behind the reference C++ prover API.
+
+The prover itself is libwhirgpu.so (hand-written sm_100a CUDA kernels behind
+the C ABI in include/whirgpu.h); this package is its Python mirror.
+"""
+from .whir import (  # noqa: F401
+    ENGINE_ID_BLAKE3,
+    ENGINE_ID_SHA2,
+    P,
+    Config,
+    Context,
+    DomainSeparator,
+    FinalClaim,
+    MultilinearExtension,
+    ProtocolParameters,
+    ProverState,
+    cli_domain_separator,
+    default_context,
+    prove_once,
+    sample_goldilocks,
+)

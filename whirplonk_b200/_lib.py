@@ -1,0 +1,103 @@
+"""ctypes binding of libwhirgpu.so (the C ABI in include/whirgpu.h).
+
+The library is built in tree (``whirplonk_b200/libwhirgpu.so``) by
+``__graft_entry__.build()``.  There is no CPU fallback: importing a prover
+entry point without the library raises immediately.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libwhirgpu.so")
+
+OK, E_INVALID, E_UNSUPPORTED, E_OOM, E_CUDA, E_DEVICE, E_TIMEOUT = range(7)
+STATUS_NAMES = {0: "OK", 1: "E_INVALID", 2: "E_UNSUPPORTED", 3: "E_OOM", 4: "E_CUDA", 5: "E_DEVICE", 6: "E_TIMEOUT"}
+NUM_FAMILIES = 9
+FAMILY_NAMES = ["ntt", "leaf_hash", "merkle", "ood", "sumcheck", "covector", "pow", "opening", "transcript"]
+
+# Every symbol include/whirgpu.h declares.
+EXPORTED = [
+    "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_schedule",
+    "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
+    "whirgpu_commit", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_mle_evaluate",
+    "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
+    "whirgpu_set_timing", "whirgpu_kernel_stats",
+]
+
+
+class WhirParams(ctypes.Structure):
+    """Mirror of whirgpu_params / whir::ProtocolParameters (same field order)."""
+
+    _fields_ = [
+        ("unique_decoding", ctypes.c_uint8),
+        ("starting_log_inv_rate", ctypes.c_uint64),
+        ("initial_folding_factor", ctypes.c_uint64),
+        ("folding_factor", ctypes.c_uint64),
+        ("security_level", ctypes.c_uint64),
+        ("pow_bits", ctypes.c_uint64),
+        ("batch_size", ctypes.c_uint64),
+        ("hash_id", ctypes.c_uint8 * 32),
+    ]
+
+
+class WhirGpuError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads libwhirgpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() (make -C whirplonk_b200/csrc)")
+    L = ctypes.CDLL(LIB_PATH)
+    p, sz, u64, i32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_int
+    vp = ctypes.POINTER(ctypes.c_void_p)
+    L.whirgpu_ctx_create.argtypes = [i32, u64, vp]
+    L.whirgpu_ctx_destroy.argtypes = [p]
+    L.whirgpu_last_error.argtypes = [p]
+    L.whirgpu_last_error.restype = ctypes.c_char_p
+    L.whirgpu_stream.argtypes = [p]
+    L.whirgpu_stream.restype = p
+    L.whirgpu_schedule.argtypes = [ctypes.POINTER(WhirParams), u64, p, sz]
+    L.whirgpu_schedule.restype = sz
+    L.whirgpu_cli_domain_separator.argtypes = [ctypes.POINTER(WhirParams), p]
+    L.whirgpu_transcript_create.argtypes = [p, p, p, p, sz, vp]
+    L.whirgpu_transcript_destroy.argtypes = [p]
+    L.whirgpu_proof_get.argtypes = [p, vp, ctypes.POINTER(sz), vp, ctypes.POINTER(sz)]
+    L.whirgpu_commit.argtypes = [p, ctypes.POINTER(WhirParams), p, u64, i32, p, vp]
+    L.whirgpu_witness_destroy.argtypes = [p]
+    L.whirgpu_prove.argtypes = [p, p, p, sz, p, p, p, p]
+    L.whirgpu_mle_evaluate.argtypes = [p, p, u64, i32, p, p]
+    L.whirgpu_sample_goldilocks.argtypes = [u64, p, sz]
+    L.whirgpu_sample_goldilocks.restype = None
+    L.whirgpu_chacha20_block.argtypes = [p, ctypes.c_uint32, p, p]
+    L.whirgpu_chacha20_block.restype = None
+    L.whirgpu_host_alloc.argtypes = [sz]
+    L.whirgpu_host_alloc.restype = p
+    L.whirgpu_host_free.argtypes = [p]
+    L.whirgpu_set_timing.argtypes = [p, i32]
+    L.whirgpu_kernel_stats.argtypes = [p, p, p, i32]
+    for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
+                 "whirgpu_proof_get", "whirgpu_commit", "whirgpu_prove", "whirgpu_mle_evaluate",
+                 "whirgpu_set_timing", "whirgpu_kernel_stats"):
+        getattr(L, name).restype = i32
+    _lib = L
+    return L
+
+
+def check(status: int, ctx=None):
+    if status != OK:
+        msg = ""
+        if ctx:
+            raw = load().whirgpu_last_error(ctx)
+            msg = raw.decode() if raw else ""
+        raise WhirGpuError(status, msg)

@@ -1,0 +1,575 @@
+// capi.cu -- implementation of the C ABI declared in include/whirgpu.h.
+//
+// Owns the CUDA context state (device, stream, twiddle tables, workspace
+// cache bounded by an HBM budget, pinned staging for proof read-back) and maps
+// every failure to a status code plus a message (no exceptions cross the ABI).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/whirgpu.h"
+#include "launch.h"
+#include "prover.h"
+#include "state.cuh"
+
+using namespace wg;
+
+namespace {
+
+constexpr uint8_t BLAKE3_ENGINE_ID[32] = {0x03, 0xe0, 0x17, 0x49, 0xeb, 0xcc, 0x04, 0x77, 0x92, 0x42, 0x54,
+                                          0xeb, 0x48, 0x20, 0x66, 0xb8, 0x64, 0xa8, 0xdd, 0x4d, 0x77, 0x25,
+                                          0x24, 0x64, 0xca, 0x6f, 0x5b, 0x6f, 0x5c, 0xc0, 0x5b, 0x4c};
+
+// ---------------------------------------------------------------------------
+// Host Keccak / SHA3 (FIPS 202) for the domain-separator helper; constants
+// from the compile-time derivations shared with the device transcript.
+// ---------------------------------------------------------------------------
+void keccak_f1600_host(uint64_t a[25]) {
+    for (int round = 0; round < 24; ++round) {
+        uint64_t c[5], b[25];
+        for (int x = 0; x < 5; ++x) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
+        for (int x = 0; x < 5; ++x) {
+            const uint64_t r = c[(x + 1) % 5];
+            const uint64_t d = c[(x + 4) % 5] ^ ((r << 1) | (r >> 63));
+            for (int y = 0; y < 5; ++y) a[x + 5 * y] ^= d;
+        }
+        for (int x = 0; x < 5; ++x)
+            for (int y = 0; y < 5; ++y) {
+                const int s = keccak_rho(x, y);
+                const uint64_t v = a[x + 5 * y];
+                b[y + 5 * ((2 * x + 3 * y) % 5)] = s ? ((v << s) | (v >> (64 - s))) : v;
+            }
+        for (int y = 0; y < 5; ++y)
+            for (int x = 0; x < 5; ++x) a[x + 5 * y] = b[x + 5 * y] ^ (~b[(x + 1) % 5 + 5 * y] & b[(x + 2) % 5 + 5 * y]);
+        a[0] ^= keccak_rc(round);
+    }
+}
+void sha3_host(const uint8_t* d, size_t n, size_t rate, uint8_t* out, size_t outlen) {
+    uint64_t s[25] = {};
+    size_t pos = 0;
+    auto xb = [&](size_t p, uint8_t v) { s[p / 8] ^= (uint64_t)v << (8 * (p % 8)); };
+    for (size_t i = 0; i < n; ++i) {
+        xb(pos++, d[i]);
+        if (pos == rate) { keccak_f1600_host(s); pos = 0; }
+    }
+    xb(pos, 0x06);
+    xb(rate - 1, 0x80);
+    keccak_f1600_host(s);
+    for (size_t i = 0; i < outlen; ++i) out[i] = (uint8_t)(s[i / 8] >> (8 * (i % 8)));
+}
+
+void cbor_head(std::vector<uint8_t>& o, uint8_t major, uint64_t v) {
+    const uint8_t m = (uint8_t)(major << 5);
+    if (v < 24) o.push_back(m | (uint8_t)v);
+    else if (v <= 0xFF) { o.push_back(m | 24); o.push_back((uint8_t)v); }
+    else if (v <= 0xFFFF) { o.push_back(m | 25); for (int s = 8; s >= 0; s -= 8) o.push_back((uint8_t)(v >> s)); }
+    else if (v <= 0xFFFFFFFFull) { o.push_back(m | 26); for (int s = 24; s >= 0; s -= 8) o.push_back((uint8_t)(v >> s)); }
+    else { o.push_back(m | 27); for (int s = 56; s >= 0; s -= 8) o.push_back((uint8_t)(v >> s)); }
+}
+void cbor_text(std::vector<uint8_t>& o, const char* s) {
+    const size_t n = std::strlen(s);
+    cbor_head(o, 3, n);
+    o.insert(o.end(), s, s + n);
+}
+
+// ---------------------------------------------------------------------------
+// ChaCha20 block function (RFC 8439 section 2.3).
+// ---------------------------------------------------------------------------
+inline uint32_t rotl32(uint32_t v, int s) { return (v << s) | (v >> (32 - s)); }
+#define WG_QR(a, b, c, d)                   \
+    a += b; d ^= a; d = rotl32(d, 16);      \
+    c += d; b ^= c; b = rotl32(b, 12);      \
+    a += b; d ^= a; d = rotl32(d, 8);       \
+    c += d; b ^= c; b = rotl32(b, 7);
+void chacha20_words(const uint32_t key[8], uint32_t counter, const uint32_t nonce[3], uint32_t out[16]) {
+    uint32_t s[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u, key[0], key[1], key[2], key[3],
+                      key[4], key[5], key[6], key[7], counter, nonce[0], nonce[1], nonce[2]};
+    uint32_t x[16];
+    for (int i = 0; i < 16; ++i) x[i] = s[i];
+    for (int i = 0; i < 10; ++i) {
+        WG_QR(x[0], x[4], x[8], x[12]);
+        WG_QR(x[1], x[5], x[9], x[13]);
+        WG_QR(x[2], x[6], x[10], x[14]);
+        WG_QR(x[3], x[7], x[11], x[15]);
+        WG_QR(x[0], x[5], x[10], x[15]);
+        WG_QR(x[1], x[6], x[11], x[12]);
+        WG_QR(x[2], x[7], x[8], x[13]);
+        WG_QR(x[3], x[4], x[9], x[14]);
+    }
+    for (int i = 0; i < 16; ++i) out[i] = x[i] + s[i];
+}
+
+ProtocolParams to_params(const whirgpu_params* p) {
+    ProtocolParams q;
+    q.unique_decoding = p->unique_decoding != 0;
+    q.starting_log_inv_rate = p->starting_log_inv_rate;
+    q.initial_folding_factor = p->initial_folding_factor;
+    q.folding_factor = p->folding_factor;
+    q.security_level = p->security_level;
+    q.pow_bits = p->pow_bits;
+    q.batch_size = p->batch_size;
+    return q;
+}
+
+struct EventTimer : Timer {
+    struct Pair { int fam; cudaEvent_t a, b; };
+    std::vector<Pair> pending;
+    std::vector<cudaEvent_t> pool;
+    uint64_t launches[FAM_COUNT] = {};
+    double ms[FAM_COUNT] = {};
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int fam, cudaStream_t st) override {
+        Pair p{fam, get(), nullptr};
+        cudaEventRecord(p.a, st);
+        pending.push_back(p);
+    }
+    void end(int fam, cudaStream_t st) override {
+        for (auto it = pending.rbegin(); it != pending.rend(); ++it)
+            if (it->fam == fam && it->b == nullptr) {
+                it->b = get();
+                cudaEventRecord(it->b, st);
+                return;
+            }
+    }
+    void harvest() {  // after a stream synchronisation
+        for (auto& p : pending) {
+            if (!p.b) continue;
+            float t = 0;
+            cudaEventElapsedTime(&t, p.a, p.b);
+            ms[p.fam] += t;
+            launches[p.fam] += 1;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    ~EventTimer() override {
+        for (auto& p : pending) { cudaEventDestroy(p.a); if (p.b) cudaEventDestroy(p.b); }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+}  // namespace
+
+struct Workspace {
+    ProofPlan plan;
+    char* dev = nullptr;
+    bool busy = false;
+};
+
+struct whirgpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    uint64_t allocated = 0;
+    DeviceTables tw;
+    std::string err;
+    std::map<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t>, std::vector<Workspace*>> cache;
+    uint8_t* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    char* mle_scratch = nullptr;
+    size_t mle_scratch_bytes = 0;
+    std::unique_ptr<EventTimer> timer;
+    uint64_t stat_launches[FAM_COUNT] = {};
+    double stat_ms[FAM_COUNT] = {};
+};
+
+struct whirgpu_transcript {
+    whirgpu_ctx* ctx = nullptr;
+    std::vector<uint8_t> ds;  // protocol_id || session_id || instance
+    std::vector<uint8_t> narg, hints;
+    bool complete = false;
+};
+
+struct whirgpu_witness {
+    whirgpu_ctx* ctx = nullptr;
+    Workspace* ws = nullptr;
+    whirgpu_transcript* tx = nullptr;
+};
+
+namespace {
+
+whirgpu_status fail(whirgpu_ctx* c, whirgpu_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+whirgpu_status cuda_fail(whirgpu_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, e == cudaErrorMemoryAllocation ? WHIRGPU_E_OOM : WHIRGPU_E_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define WG_CUDA(c, x, what)                               \
+    do {                                                  \
+        cudaError_t _e = (x);                             \
+        if (_e != cudaSuccess) return cuda_fail(c, _e, what); \
+    } while (0)
+
+whirgpu_status ensure_pinned(whirgpu_ctx* c, size_t bytes) {
+    if (c->pinned_bytes >= bytes) return WHIRGPU_OK;
+    if (c->pinned) cudaFreeHost(c->pinned);
+    c->pinned = nullptr;
+    c->pinned_bytes = 0;
+    WG_CUDA(c, cudaMallocHost(&c->pinned, bytes), "cudaMallocHost");
+    c->pinned_bytes = bytes;
+    return WHIRGPU_OK;
+}
+
+whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out) {
+    ProofPlan plan;
+    try {
+        plan = make_plan((uint32_t)n, to_params(params), MAX_FORMS, std::max<size_t>(ds_len, 96));
+    } catch (const std::exception& e) {
+        return fail(c, WHIRGPU_E_INVALID, e.what());
+    }
+    auto key = std::make_tuple(n, params->starting_log_inv_rate, params->initial_folding_factor, params->folding_factor,
+                               params->security_level, params->pow_bits,
+                               (uint64_t)params->unique_decoding | ((uint64_t)std::max<size_t>(ds_len, 96) << 1));
+    auto& vec = c->cache[key];
+    for (Workspace* w : vec)
+        if (!w->busy) { w->busy = true; *out = w; return WHIRGPU_OK; }
+    if (c->budget && c->allocated + plan.total_bytes > c->budget)
+        return fail(c, WHIRGPU_E_OOM, "workspace above the HBM budget");
+    Workspace* w = new Workspace();
+    w->plan = plan;
+    cudaError_t e = cudaMalloc(&w->dev, plan.total_bytes);
+    if (e != cudaSuccess) { delete w; return cuda_fail(c, e, "cudaMalloc workspace"); }
+    // Counters and tickets start at zero and reset themselves after use.
+    e = cudaMemsetAsync(w->dev + plan.off_sc_scratch, 0, plan.off_tx - plan.off_sc_scratch, c->stream);
+    if (e != cudaSuccess) { cudaFree(w->dev); delete w; return cuda_fail(c, e, "cudaMemset"); }
+    c->allocated += plan.total_bytes;
+    w->busy = true;
+    vec.push_back(w);
+    *out = w;
+    return WHIRGPU_OK;
+}
+
+bool is_blake3(const whirgpu_params* p) { return std::memcmp(p->hash_id, BLAKE3_ENGINE_ID, 32) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+whirgpu_status whirgpu_ctx_create(int device, uint64_t hbm_budget, whirgpu_ctx** out) {
+    if (!out) return WHIRGPU_E_INVALID;
+    *out = nullptr;
+    auto c = std::make_unique<whirgpu_ctx>();
+    c->device = device;
+    c->budget = hbm_budget;
+    WG_CUDA(nullptr, cudaSetDevice(device), "cudaSetDevice");
+    WG_CUDA(nullptr, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (lde_prepare() != 0) return WHIRGPU_E_CUDA;
+    std::vector<uint64_t> st(1u << (TW_STAGE_LOG - 1)), hi(1u << TW_HALF), lo(1u << TW_HALF);
+    host_twiddles(st.data(), hi.data(), lo.data());
+    WG_CUDA(nullptr, cudaMalloc(&c->tw.tw_stage, st.size() * 8), "cudaMalloc twiddles");
+    WG_CUDA(nullptr, cudaMalloc(&c->tw.tw_hi, hi.size() * 8), "cudaMalloc twiddles");
+    WG_CUDA(nullptr, cudaMalloc(&c->tw.tw_lo, lo.size() * 8), "cudaMalloc twiddles");
+    WG_CUDA(nullptr, cudaMemcpy(c->tw.tw_stage, st.data(), st.size() * 8, cudaMemcpyHostToDevice), "upload");
+    WG_CUDA(nullptr, cudaMemcpy(c->tw.tw_hi, hi.data(), hi.size() * 8, cudaMemcpyHostToDevice), "upload");
+    WG_CUDA(nullptr, cudaMemcpy(c->tw.tw_lo, lo.data(), lo.size() * 8, cudaMemcpyHostToDevice), "upload");
+    *out = c.release();
+    return WHIRGPU_OK;
+}
+
+void whirgpu_ctx_destroy(whirgpu_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->cache)
+        for (Workspace* w : kv.second) { cudaFree(w->dev); delete w; }
+    cudaFree(c->tw.tw_stage);
+    cudaFree(c->tw.tw_hi);
+    cudaFree(c->tw.tw_lo);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->mle_scratch) cudaFree(c->mle_scratch);
+    c->timer.reset();
+    cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* whirgpu_last_error(const whirgpu_ctx* c) { return c ? c->err.c_str() : "no context"; }
+void* whirgpu_stream(whirgpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+size_t whirgpu_schedule(const whirgpu_params* params, uint64_t n, uint64_t* out, size_t cap) {
+    if (!params) return 0;
+    try {
+        WhirSchedule s = make_schedule(n, to_params(params));
+        std::vector<uint64_t> v{s.rounds.size(), s.initial.codeword_length, s.initial.in_domain, s.initial.out_domain,
+                                s.initial_sumcheck.pow_threshold, s.initial_skip_pow};
+        for (const auto& r : s.rounds)
+            v.insert(v.end(), {r.irs.vector_size, r.irs.codeword_length, r.irs.in_domain, r.irs.out_domain,
+                               r.pow_threshold, r.sumcheck.pow_threshold});
+        v.insert(v.end(), {s.final_sumcheck.initial_size, s.final_sumcheck.num_rounds, s.final_pow,
+                           s.final_sumcheck.pow_threshold});
+        for (size_t i = 0; i < v.size() && i < cap; ++i) out[i] = v[i];
+        return v.size();
+    } catch (const std::exception&) {
+        return 0;
+    }
+}
+
+whirgpu_status whirgpu_cli_domain_separator(const whirgpu_params* p, uint8_t out[96]) {
+    if (!p || !out) return WHIRGPU_E_INVALID;
+    std::vector<uint8_t> c;
+    cbor_head(c, 5, 8);
+    cbor_text(c, "unique_decoding");
+    c.push_back(p->unique_decoding ? 0xF5 : 0xF4);
+    cbor_text(c, "starting_log_inv_rate"); cbor_head(c, 0, p->starting_log_inv_rate);
+    cbor_text(c, "initial_folding_factor"); cbor_head(c, 0, p->initial_folding_factor);
+    cbor_text(c, "folding_factor"); cbor_head(c, 0, p->folding_factor);
+    cbor_text(c, "security_level"); cbor_head(c, 0, p->security_level);
+    cbor_text(c, "pow_bits"); cbor_head(c, 0, p->pow_bits);
+    cbor_text(c, "batch_size"); cbor_head(c, 0, p->batch_size);
+    cbor_text(c, "hash_id"); cbor_head(c, 4, 32);
+    for (int i = 0; i < 32; ++i) cbor_head(c, 0, p->hash_id[i]);
+    sha3_host(c.data(), c.size(), 72, out, 64);
+    std::vector<uint8_t> s;
+    cbor_text(s, "Example at src/bin/main.rs:133");
+    sha3_host(s.data(), s.size(), 136, out + 64, 32);
+    return WHIRGPU_OK;
+}
+
+whirgpu_status whirgpu_transcript_create(whirgpu_ctx* ctx, const uint8_t protocol_id[64], const uint8_t session_id[32],
+                                         const uint8_t* instance, size_t instance_len, whirgpu_transcript** out) {
+    if (!ctx || !protocol_id || !session_id || !out || (instance_len && !instance)) return WHIRGPU_E_INVALID;
+    auto t = new whirgpu_transcript();
+    t->ctx = ctx;
+    t->ds.insert(t->ds.end(), protocol_id, protocol_id + 64);
+    t->ds.insert(t->ds.end(), session_id, session_id + 32);
+    if (instance_len) t->ds.insert(t->ds.end(), instance, instance + instance_len);
+    *out = t;
+    return WHIRGPU_OK;
+}
+
+void whirgpu_transcript_destroy(whirgpu_transcript* t) { delete t; }
+
+whirgpu_status whirgpu_proof_get(const whirgpu_transcript* t, const uint8_t** narg, size_t* narg_len,
+                                 const uint8_t** hints, size_t* hints_len) {
+    if (!t || !t->complete) return WHIRGPU_E_INVALID;
+    if (narg) *narg = t->narg.data();
+    if (narg_len) *narg_len = t->narg.size();
+    if (hints) *hints = t->hints.data();
+    if (hints_len) *hints_len = t->hints.size();
+    return WHIRGPU_OK;
+}
+
+whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs,
+                              uint64_t n, int where, whirgpu_transcript* tx, whirgpu_witness** out) {
+    if (!c || !params || !coeffs || !tx || !out || tx->ctx != c) return fail(c, WHIRGPU_E_INVALID, "null argument");
+    *out = nullptr;
+    if (!is_blake3(params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 engine is on this path");
+    if (n >= 40) return fail(c, WHIRGPU_E_INVALID, "num_variables too large");
+    Workspace* ws = nullptr;
+    whirgpu_status s = acquire_workspace(c, n, params, tx->ds.size(), &ws);
+    if (s != WHIRGPU_OK) return s;
+    const ProofPlan& p = ws->plan;
+    cudaError_t e = cudaMemcpyAsync(ws->dev + p.off_coeffs, coeffs, (8ull << n),
+                                    where == WHIRGPU_INPUT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ws->dev + p.off_ds, tx->ds.data(), tx->ds.size(), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) { ws->busy = false; return cuda_fail(c, e, "input copy"); }
+    if (enqueue_commit(p, ws->dev, (uint32_t)tx->ds.size(), c->tw, c->stream, c->timer.get()) != 0) {
+        ws->busy = false;
+        return fail(c, WHIRGPU_E_INVALID, "commit launch failed");
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) { ws->busy = false; return cuda_fail(c, e, "commit kernels"); }
+    auto w = new whirgpu_witness();
+    w->ctx = c;
+    w->ws = ws;
+    w->tx = tx;
+    tx->complete = false;
+    *out = w;
+    return WHIRGPU_OK;
+}
+
+void whirgpu_witness_destroy(whirgpu_witness* w) {
+    if (!w) return;
+    if (w->ws) {
+        cudaStreamSynchronize(w->ctx->stream);
+        w->ws->busy = false;
+    }
+    delete w;
+}
+
+whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t* points, size_t num_points,
+                             const uint64_t* evaluations, whirgpu_transcript* tx, uint64_t* evaluation_point,
+                             uint64_t* rlc) {
+    if (!c || !w || !tx || w->ctx != c || w->tx != tx) return fail(c, WHIRGPU_E_INVALID, "bad handles");
+    if (num_points > (size_t)MAX_FORMS || (num_points && (!points || !evaluations)))
+        return fail(c, WHIRGPU_E_INVALID, "bad statement");
+    ProofPlan p = w->ws->plan;
+    p.n_forms = (int)num_points;
+    if (num_points + p.sch.initial.out_domain == 0)
+        return fail(c, WHIRGPU_E_UNSUPPORTED, "statement-free proofs are not on this path");
+    char* ws = w->ws->dev;
+    ProofScalars* sc = plan_scalars(p, ws);
+    cudaError_t e = cudaSuccess;
+    if (num_points) {
+        e = cudaMemcpyAsync(ws + p.off_points, points, num_points * p.n * 24, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&sc->forms_eval[0], evaluations, num_points * 24, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "statement upload");
+    }
+    if (enqueue_prove(p, ws, c->tw, c->stream, c->timer.get()) != 0) return fail(c, WHIRGPU_E_INVALID, "prove launch failed");
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "prove kernels");
+    // Read-back: transcript state, narg (exact size), hints (bounded), challenges.
+    const size_t need = sizeof(TxState) + p.narg_len + p.hints_cap + 64 * 24 + MAX_FORMS * 24 + 64;
+    whirgpu_status s = ensure_pinned(c, need);
+    if (s != WHIRGPU_OK) return s;
+    uint8_t* h = c->pinned;
+    TxState* htx = reinterpret_cast<TxState*>(h);
+    uint8_t* hnarg = h + sizeof(TxState);
+    uint8_t* hhints = hnarg + p.narg_len;
+    uint8_t* hr = hhints + p.hints_cap;
+    uint8_t* hrlc = hr + 64 * 24;
+    WG_CUDA(c, cudaMemcpyAsync(htx, plan_tx(p, ws), sizeof(TxState), cudaMemcpyDeviceToHost, c->stream), "read-back");
+    WG_CUDA(c, cudaMemcpyAsync(hnarg, ws + p.off_narg, p.narg_len, cudaMemcpyDeviceToHost, c->stream), "read-back");
+    WG_CUDA(c, cudaMemcpyAsync(hhints, ws + p.off_hints, p.hints_cap, cudaMemcpyDeviceToHost, c->stream), "read-back");
+    WG_CUDA(c, cudaMemcpyAsync(hr, &sc->sc_r[0], p.total_sumcheck_rounds * 24, cudaMemcpyDeviceToHost, c->stream),
+            "read-back");
+    WG_CUDA(c, cudaMemcpyAsync(hrlc, &sc->crlc[0], std::max<size_t>(num_points, 1) * 24, cudaMemcpyDeviceToHost, c->stream),
+            "read-back");
+    WG_CUDA(c, cudaStreamSynchronize(c->stream), "prove");
+    if (c->timer) {
+        c->timer->harvest();
+    }
+    if (htx->err) {
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "device error word 0x%x", htx->err);
+        return fail(c, WHIRGPU_E_DEVICE, buf);
+    }
+    if (htx->narg_len != p.narg_len || htx->hints_len > p.hints_cap)
+        return fail(c, WHIRGPU_E_DEVICE, "proof stream length mismatch");
+    tx->narg.assign(hnarg, hnarg + p.narg_len);
+    tx->hints.assign(hhints, hhints + htx->hints_len);
+    tx->complete = true;
+    if (evaluation_point) std::memcpy(evaluation_point, hr, p.total_sumcheck_rounds * 24);
+    if (rlc && num_points) std::memcpy(rlc, hrlc, num_points * 24);
+    return WHIRGPU_OK;
+}
+
+whirgpu_status whirgpu_mle_evaluate(whirgpu_ctx* c, const uint64_t* coeffs, uint64_t n, int where,
+                                    const uint64_t* point, uint64_t out[3]) {
+    if (!c || !coeffs || !point || !out || n >= 40) return fail(c, WHIRGPU_E_INVALID, "bad argument");
+    const size_t scratch = mle_eval_scratch_bytes((uint32_t)n);
+    const size_t point_region = (n * 24 + 24 + 255) / 256 * 256;  // point (n Ext3) + result (1 Ext3)
+    const size_t need = scratch + point_region + (where == WHIRGPU_INPUT_DEVICE ? 0 : (8ull << n));
+    if (c->mle_scratch_bytes < need) {
+        if (c->mle_scratch) cudaFree(c->mle_scratch);
+        c->mle_scratch = nullptr;
+        c->mle_scratch_bytes = 0;
+        WG_CUDA(c, cudaMalloc(&c->mle_scratch, need), "cudaMalloc");
+        c->mle_scratch_bytes = need;
+        WG_CUDA(c, cudaMemsetAsync(c->mle_scratch, 0, need, c->stream), "cudaMemset");
+    }
+    char* base = c->mle_scratch;
+    uint64_t* dpoint = reinterpret_cast<uint64_t*>(base + scratch);
+    uint64_t* dout = dpoint + n * 3;
+    const uint64_t* dcoeffs = coeffs;
+    if (where != WHIRGPU_INPUT_DEVICE) {
+        uint64_t* dc = reinterpret_cast<uint64_t*>(base + scratch + point_region);
+        WG_CUDA(c, cudaMemcpyAsync(dc, coeffs, 8ull << n, cudaMemcpyHostToDevice, c->stream), "upload");
+        dcoeffs = dc;
+    }
+    WG_CUDA(c, cudaMemcpyAsync(dpoint, point, n * 24, cudaMemcpyHostToDevice, c->stream), "upload");
+    launch_mle_eval(dcoeffs, (uint32_t)n, dpoint, base, dout, c->stream);
+    WG_CUDA(c, cudaMemcpyAsync(out, dout, 24, cudaMemcpyDeviceToHost, c->stream), "read-back");
+    WG_CUDA(c, cudaStreamSynchronize(c->stream), "mle");
+    return WHIRGPU_OK;
+}
+
+void whirgpu_chacha20_block(const uint8_t key[32], uint32_t counter, const uint8_t nonce[12], uint8_t out[64]) {
+    uint32_t k[8], nn[3], o[16];
+    for (int i = 0; i < 8; ++i) std::memcpy(&k[i], key + 4 * i, 4);
+    for (int i = 0; i < 3; ++i) std::memcpy(&nn[i], nonce + 4 * i, 4);
+    chacha20_words(k, counter, nn, o);
+    std::memcpy(out, o, 64);
+}
+
+void whirgpu_sample_goldilocks(uint64_t seed, uint64_t* out, size_t count) {
+    uint32_t key[8] = {(uint32_t)seed, (uint32_t)(seed >> 32), 0, 0, 0, 0, 0, 0};
+    const uint32_t nonce[3] = {0, 0, 0};
+    uint32_t counter = 0;
+    size_t got = 0;
+    uint32_t blk[16];
+    while (got < count) {
+        chacha20_words(key, counter++, nonce, blk);
+        for (int w = 0; w < 8 && got < count; ++w) {
+            const uint64_t v = (uint64_t)blk[2 * w] | ((uint64_t)blk[2 * w + 1] << 32);
+            if (v < GL_P) out[got++] = v;
+        }
+        if (counter == 0) key[2] += 1;  // past 2^38 bytes: continue in the next key slot
+    }
+}
+
+void* whirgpu_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+    return p;
+}
+void whirgpu_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
+whirgpu_status whirgpu_set_timing(whirgpu_ctx* c, int enabled) {
+    if (!c) return WHIRGPU_E_INVALID;
+    if (enabled && !c->timer) c->timer.reset(new EventTimer());
+    if (!enabled && c->timer) {
+        cudaStreamSynchronize(c->stream);
+        c->timer->harvest();
+        for (int f = 0; f < FAM_COUNT; ++f) { c->stat_launches[f] += c->timer->launches[f]; c->stat_ms[f] += c->timer->ms[f]; }
+        c->timer.reset();
+    }
+    return WHIRGPU_OK;
+}
+
+whirgpu_status whirgpu_kernel_stats(whirgpu_ctx* c, uint64_t launches[WHIRGPU_NUM_FAMILIES],
+                                    double ms[WHIRGPU_NUM_FAMILIES], int reset) {
+    if (!c) return WHIRGPU_E_INVALID;
+    if (c->timer) {
+        cudaStreamSynchronize(c->stream);
+        c->timer->harvest();
+    }
+    for (int f = 0; f < FAM_COUNT; ++f) {
+        uint64_t l = c->stat_launches[f] + (c->timer ? c->timer->launches[f] : 0);
+        double m = c->stat_ms[f] + (c->timer ? c->timer->ms[f] : 0.0);
+        if (launches) launches[f] = l;
+        if (ms) ms[f] = m;
+    }
+    if (reset) {
+        for (int f = 0; f < FAM_COUNT; ++f) { c->stat_launches[f] = 0; c->stat_ms[f] = 0; }
+        if (c->timer) for (int f = 0; f < FAM_COUNT; ++f) { c->timer->launches[f] = 0; c->timer->ms[f] = 0; }
+    }
+    return WHIRGPU_OK;
+}
+
+}  // extern "C"
+
+namespace wg {
+void host_twiddles(u64* stage, u64* hi, u64* lo) {
+    const u64 w11 = gl_pow_host(7, (GL_P - 1) >> TW_STAGE_LOG);
+    u64 acc = 1;
+    for (u32 u = 0; u < (1u << (TW_STAGE_LOG - 1)); ++u) { stage[u] = acc; acc = gl_mul_host(acc, w11); }
+    const u64 w = gl_pow_host(7, (GL_P - 1) >> TW_LOG);
+    acc = 1;
+    for (u32 u = 0; u < (1u << TW_HALF); ++u) { lo[u] = acc; acc = gl_mul_host(acc, w); }
+    const u64 wh = acc;  // w^(2^TW_HALF)
+    acc = 1;
+    for (u32 u = 0; u < (1u << TW_HALF); ++u) { hi[u] = acc; acc = gl_mul_host(acc, wh); }
+}
+}  // namespace wg

@@ -1,0 +1,218 @@
+// k_hash.cu -- matrix commitment: BLAKE3 leaf hashing of codeword rows, Merkle
+// levels, and the out-of-domain evaluation that closes irs_commit::commit.
+//
+// Leaves (cpp/include/whir/protocols/matrix_commit.hpp:169-195): leaf i is the
+// BLAKE3 hash of row i's canonical little-endian bytes -- `depth` elements of
+// 8 B (base) or 24 B (Ext3, c0 c1 c2).  Rows are gathered from the codeword
+// planes written by the encoder, so each warp reads 8-byte words of 32
+// consecutive rows per plane: fully coalesced.
+//
+// Merkle tree (merkle_tree.hpp:104-147): parent = BLAKE3(left || right),
+// node array [leaves | level 1 | ... | root].  A CTA hashes a 512-leaf subtree
+// (9 levels) in shared memory, so a 2^22-leaf tree takes three launches.
+#include "launch.h"
+#include "blake3.cuh"
+#include "state.cuh"
+
+namespace wg {
+
+__device__ __forceinline__ void store_node(u32* nodes, u64 idx, const unsigned cv[8]) {
+    uint4* p = reinterpret_cast<uint4*>(nodes + idx * 8);
+    p[0] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+    p[1] = make_uint4(cv[4], cv[5], cv[6], cv[7]);
+}
+__device__ __forceinline__ void load_node(const u32* nodes, u64 idx, unsigned* m) {
+    const uint4* p = reinterpret_cast<const uint4*>(nodes + idx * 8);
+    uint4 a = p[0], b = p[1];
+    m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w;
+    m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+}
+
+// Row i = words w = 0 .. depth*ncomp-1 with w -> (element w / ncomp, component w % ncomp),
+// read from plane (component * depth + element).
+template <int NCOMP>
+__global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes) {
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const u32 nwords = depth * NCOMP;           // 64-bit words per row
+    const u32 bytes = nwords * 8;
+    const u32 nblocks = (bytes + 63) / 64;
+    unsigned cv[8];
+    b3_init(cv);
+    for (u32 t = 0; t < nblocks; ++t) {
+        unsigned m[16];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const u32 w = t * 8 + q;
+            u64 v = 0;
+            if (w < nwords) {
+                const u32 el = w / NCOMP, c = w - el * NCOMP;
+                v = planes[((u64)c * depth + el) * N + i];
+            }
+            m[2 * q] = (unsigned)v;
+            m[2 * q + 1] = (unsigned)(v >> 32);
+        }
+        const u32 len = (t + 1 == nblocks) ? bytes - 64 * t : 64;
+        const unsigned flags = (t == 0 ? B3_CHUNK_START : 0u) | (t + 1 == nblocks ? (B3_CHUNK_END | B3_ROOT) : 0u);
+        b3_compress(cv, m, flags, len);
+    }
+    store_node(nodes, i, cv);
+}
+
+int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st) {
+    if (depth * ncomp * 8 > 1024) return -1;  // multi-chunk BLAKE3 rows are not on this path
+    const unsigned grid = (unsigned)((N + 255) / 256);
+    if (ncomp == 1) k_leaves<1><<<grid, 256, 0, st>>>(planes, N, depth, nodes);
+    else if (ncomp == 3) k_leaves<3><<<grid, 256, 0, st>>>(planes, N, depth, nodes);
+    else return -1;
+    return 0;
+}
+
+__host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
+    // [leaves (2^logN) | 2^(logN-1) | ... ]: offset of level l = 2^(logN+1) - 2^(logN+1-l)
+    return (2ull << logN) - (2ull << (logN - l));
+}
+
+// One CTA hashes a subtree of height `levels` whose children sit at level
+// `level_in`; every produced level is written to global memory.
+__global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_in, u32 levels, TxState* tx,
+                                                ProofScalars* sc, int commit_idx, int n_ood, int finish) {
+    __shared__ unsigned buf[2][256 * 8];
+    if (levels > 0) {
+        const u32 nparents = 1u << (levels - 1);
+        const u64 in_off = level_offset(logN, level_in);
+        const u64 out_off = level_offset(logN, level_in + 1);
+        for (u32 t = threadIdx.x; t < nparents; t += blockDim.x) {
+            unsigned m[16];
+            const u64 child = ((u64)blockIdx.x << levels) + 2 * t;
+            load_node(nodes, in_off + child, m);
+            load_node(nodes, in_off + child + 1, m + 8);
+            unsigned cv[8];
+            b3_hash64(m, cv);
+            store_node(nodes, out_off + ((u64)blockIdx.x << (levels - 1)) + t, cv);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) buf[0][t * 8 + k] = cv[k];
+        }
+        __syncthreads();
+        int cur = 0;
+        for (u32 lv = 1; lv < levels; ++lv) {
+            const u32 np = nparents >> lv;
+            const u64 off = level_offset(logN, level_in + 1 + lv);
+            for (u32 t = threadIdx.x; t < np; t += blockDim.x) {
+                unsigned m[16];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) m[k] = buf[cur][t * 16 + k];
+                unsigned cv[8];
+                b3_hash64(m, cv);
+                store_node(nodes, off + ((u64)blockIdx.x << (levels - 1 - lv)) + t, cv);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) buf[cur ^ 1][t * 8 + k] = cv[k];
+            }
+            __syncthreads();
+            cur ^= 1;
+        }
+    }
+    if (finish && threadIdx.x == 0) {
+        __threadfence();
+        const u64 root = level_offset(logN, logN);
+        u64 w[4];
+        for (int k = 0; k < 4; ++k) w[k] = (u64)nodes[root * 8 + 2 * k] | ((u64)nodes[root * 8 + 2 * k + 1] << 32);
+        tx_message_words(tx, w, 4);
+        for (int j = 0; j < n_ood; ++j) sc->ood_pts[commit_idx][j] = tx_challenge_e3(tx);
+    }
+}
+
+int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, cudaStream_t st) {
+    u32 level = 0;
+    if (logN == 0) {
+        k_merkle<<<1, 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1);
+        return 0;
+    }
+    while (level < logN) {
+        const u32 levels = (logN - level) < 9 ? (logN - level) : 9;
+        const u32 ctas = 1u << (logN - level - levels);
+        const int finish = (level + levels == logN) ? 1 : 0;
+        k_merkle<<<ctas, 256, 0, st>>>(nodes, logN, level, levels, tx, sc, commit_idx, n_ood, finish);
+        level += levels;
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Out-of-domain evaluation: value_j = sum_i v_i z_j^i
+// (irs_commit.hpp:472-554 -> utilities.hpp:196-246).  Thread g of T handles
+// i = g + T e with running power z^g (z^T)^e; exact field sums, so the
+// association order is free.  The last CTA (ticket) finishes the sums and sends
+// the values as prover messages.
+// ---------------------------------------------------------------------------
+constexpr int OOD_GRID = 592, OOD_THREADS = 256;
+
+__device__ __forceinline__ E3 block_sum_e3(E3 v, E3* red) {
+    v = e3_warp_sum(v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    E3 r = e3_zero();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = e3_add(r, red[k]);
+    __syncthreads();
+    return r;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(OOD_THREADS) k_ood(const u64* v0, const u64* v1, const u64* v2, int ext3, u64 size,
+                                                     TxState* tx, ProofScalars* sc, int commit_idx, int n_ood,
+                                                     E3* partials, unsigned* counter) {
+    __shared__ E3 red[32];
+    __shared__ bool is_last;
+    const u64 T = (u64)gridDim.x * blockDim.x;
+    const u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int j = 0; j < n_ood; ++j) {
+        const E3 z = sc->ood_pts[commit_idx][j];
+        E3 p = e3_pow(z, g);
+        const E3 zT = e3_pow(z, T);
+        E3 acc = e3_zero();
+        for (u64 i = g; i < size; i += T) {
+            if (ext3) acc = e3_add(acc, e3_mul(E3{v0[i], v1[i], v2[i]}, p));
+            else acc = e3_add(acc, e3_mul_base(p, v0[i]));
+            p = e3_mul(p, zT);
+        }
+        E3 bs = block_sum_e3(acc, red);
+        if (threadIdx.x == 0) partials[blockIdx.x * MAX_OOD + j] = bs;
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned ticket = atomicAdd(counter, 1u);
+        is_last = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    for (int j = 0; j < n_ood; ++j) {
+        E3 acc = e3_zero();
+        for (u32 b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+            const E3* pp = &partials[b * MAX_OOD + j];
+            acc = e3_add(acc, E3{__ldcg(&pp->c0), __ldcg(&pp->c1), __ldcg(&pp->c2)});
+        }
+        E3 total = block_sum_e3(acc, red);
+        if (threadIdx.x == 0) {
+            sc->ood_vals[commit_idx][j] = total;
+            tx_message_e3(tx, total);
+        }
+    }
+    if (threadIdx.x == 0) *counter = 0;
+}
+
+size_t ood_scratch_bytes() { return (size_t)OOD_GRID * MAX_OOD * sizeof(E3) + 256; }
+
+int launch_ood(const u64* v0, const u64* v1, const u64* v2, bool ext3, u64 size, TxState* tx, ProofScalars* sc,
+               int commit_idx, int n_ood, void* scratch, cudaStream_t st) {
+    if (n_ood <= 0) return 0;
+    if (n_ood > MAX_OOD) return -1;
+    u64 want = (size + OOD_THREADS * 8 - 1) / (OOD_THREADS * 8);
+    unsigned grid = (unsigned)(want < 1 ? 1 : (want > OOD_GRID ? OOD_GRID : want));
+    E3* partials = reinterpret_cast<E3*>(scratch);
+    unsigned* counter = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(scratch) + (size_t)OOD_GRID * MAX_OOD * sizeof(E3));
+    k_ood<<<grid, OOD_THREADS, 0, st>>>(v0, v1, v2, ext3 ? 1 : 0, size, tx, sc, commit_idx, n_ood, partials, counter);
+    return 0;
+}
+
+}  // namespace wg

@@ -1,0 +1,409 @@
+// k_sumcheck.cu -- extension-field sumcheck and the covector it runs against.
+//
+// Sumcheck round (cpp/include/whir/algebra/sumcheck.hpp:43-116,
+// protocols/sumcheck_protocol.hpp:99-135): on vectors a, b of size s,
+//   c0 = sum_{i<s/2} a_i b_i,  c2 = sum_{i<s/2} (a_{i+s/2}-a_i)(b_{i+s/2}-b_i),
+// prover messages c0, c2, optional PoW, challenge r, then the fold
+//   a_i <- a_i + r (a_{i+s/2} - a_i)  (same for b), sum <- (c2 r + c1) r + c0.
+// Here the fold of round t is fused into the kernel of round t+1 (one HBM pass
+// per round), partial sums are warp-reduced, and the last CTA to finish
+// (atomic ticket) does the transcript step on one thread.
+//
+// Covector (whir_prover.hpp:150-197, linear_form.hpp:186-206,
+// multilinear.hpp:121-133): cov[i] = sum_f crlc_f eq(p_f, i) + sum_j crlc_j z_j^i,
+// later cov[i] += sum_j stir_rlc_j z_j^i per round (utilities.hpp:261-307).
+#include "launch.h"
+#include "state.cuh"
+
+namespace wg {
+
+constexpr int SC_THREADS = 256, SC_GRID = 148 * 4;
+
+__device__ __forceinline__ E3 block_sum(E3 v, E3* red) {
+    v = e3_warp_sum(v);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    E3 r = e3_zero();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) r = e3_add(r, red[k]);
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ E3 ld3(u64* const p[3], u64 i) { return E3{p[0][i], p[1][i], p[2][i]}; }
+__device__ __forceinline__ void st3(u64* const p[3], u64 i, E3 v) { p[0][i] = v.c0; p[1][i] = v.c1; p[2][i] = v.c2; }
+
+struct ScKernelArgs {
+    const u64* a_base;
+    u64* a_in[3];
+    u64* a_out[3];
+    u64* b[3];
+    u64 size;
+    int fold, fold_r, r_slot;
+    u64 pow_threshold;
+    TxState* tx;
+    ProofScalars* sc;
+    E3* partials;
+    unsigned* counter;
+};
+
+// Loads a_i of the round vector, folding on the fly when requested.
+__device__ __forceinline__ E3 load_a(const ScKernelArgs& a, u64 i, const E3& r) {
+    if (!a.fold) return a.a_base ? e3_base(a.a_base[i]) : ld3(a.a_in, i);
+    if (a.a_base) {
+        const u64 x0 = a.a_base[i], x1 = a.a_base[i + a.size];
+        return e3_add(e3_base(x0), e3_mul_base(r, gl_sub(x1, x0)));
+    }
+    const E3 x0 = ld3(a.a_in, i), x1 = ld3(a.a_in, i + a.size);
+    return e3_add(x0, e3_mul(r, e3_sub(x1, x0)));
+}
+__device__ __forceinline__ E3 load_b(const ScKernelArgs& a, u64 i, const E3& r) {
+    if (!a.fold) return ld3(a.b, i);
+    const E3 y0 = ld3(a.b, i), y1 = ld3(a.b, i + a.size);
+    return e3_add(y0, e3_mul(r, e3_sub(y1, y0)));
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_sumcheck_round(ScKernelArgs a) {
+    __shared__ E3 red[32];
+    __shared__ bool is_last;
+    const E3 r = a.fold ? a.sc->sc_r[a.fold_r] : e3_zero();
+    const u64 half = a.size >> 1;
+    E3 c0 = e3_zero(), c2 = e3_zero();
+    const u64 T = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += T) {
+        const E3 al = load_a(a, i, r), ah = load_a(a, i + half, r);
+        const E3 bl = load_b(a, i, r), bh = load_b(a, i + half, r);
+        if (a.fold) {
+            st3(a.a_out, i, al); st3(a.a_out, i + half, ah);
+            st3(a.b, i, bl); st3(a.b, i + half, bh);
+        }
+        c0 = e3_add(c0, e3_mul(al, bl));
+        c2 = e3_add(c2, e3_mul(e3_sub(ah, al), e3_sub(bh, bl)));
+    }
+    const E3 s0 = block_sum(c0, red);
+    const E3 s2 = block_sum(c2, red);
+    if (threadIdx.x == 0) {
+        a.partials[2 * blockIdx.x] = s0;
+        a.partials[2 * blockIdx.x + 1] = s2;
+        __threadfence();
+        is_last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    E3 t0 = e3_zero(), t2 = e3_zero();
+    for (u32 k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+        const E3* p0 = &a.partials[2 * k];
+        const E3* p2 = &a.partials[2 * k + 1];
+        t0 = e3_add(t0, E3{__ldcg(&p0->c0), __ldcg(&p0->c1), __ldcg(&p0->c2)});
+        t2 = e3_add(t2, E3{__ldcg(&p2->c0), __ldcg(&p2->c1), __ldcg(&p2->c2)});
+    }
+    const E3 C0 = block_sum(t0, red);
+    const E3 C2 = block_sum(t2, red);
+    if (threadIdx.x == 0) {
+        *a.counter = 0;
+        ProofScalars* sc = a.sc;
+        TxState* tx = a.tx;
+        sc->c0 = C0;
+        sc->c2 = C2;
+        tx_message_e3(tx, C0);
+        tx_message_e3(tx, C2);
+        if (a.pow_threshold != ~0ull) {
+            // PoW follows in-stream (k_pow_grind / k_sc_after_pow).
+            tx_squeeze(tx, sc->pow_ch, 32);
+            sc->pow_best = ~0ull;
+        } else {
+            const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
+            const E3 rn = tx_challenge_e3(tx);
+            sc->sc_r[a.r_slot] = rn;
+            sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+        }
+    }
+}
+
+// After a round PoW: send the nonce, squeeze r, update the sum.
+__global__ void k_sc_after_pow(TxState* tx, ProofScalars* sc, int r_slot) {
+    if (threadIdx.x != 0) return;
+    const u64 n = sc->pow_best;
+    if (n == ~0ull) tx->err |= TX_ERR_POW_EXHAUSTED;
+    tx_message_u64(tx, n);
+    const E3 C0 = sc->c0, C2 = sc->c2;
+    const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
+    const E3 rn = tx_challenge_e3(tx);
+    sc->sc_r[r_slot] = rn;
+    sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+}
+
+static ScKernelArgs make_sc(const SumcheckArgs& s) {
+    ScKernelArgs a{};
+    a.a_base = s.a_base;
+    for (int c = 0; c < 3; ++c) { a.a_in[c] = s.a_in[c]; a.a_out[c] = s.a_out[c]; a.b[c] = s.b[c]; }
+    a.size = s.size;
+    a.fold = s.fold;
+    a.fold_r = s.fold_r;
+    a.r_slot = s.r_slot;
+    a.pow_threshold = s.pow_threshold;
+    a.tx = s.tx;
+    a.sc = s.sc;
+    a.partials = reinterpret_cast<E3*>(s.scratch);
+    a.counter = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(s.scratch) + (size_t)SC_GRID * 2 * sizeof(E3));
+    return a;
+}
+
+size_t sumcheck_scratch_bytes() { return (size_t)SC_GRID * 2 * sizeof(E3) + 256; }
+
+int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st);  // k_tx.cu
+
+int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
+    if (s.size < 2) return -1;
+    ScKernelArgs a = make_sc(s);
+    const u64 half = s.size >> 1;
+    u64 want = (half + SC_THREADS - 1) / SC_THREADS;
+    const unsigned grid = (unsigned)(want > SC_GRID ? SC_GRID : (want < 1 ? 1 : want));
+    k_sumcheck_round<<<grid, SC_THREADS, 0, st>>>(a);
+    if (s.pow_threshold != ~0ull) {
+        launch_pow_grind_only(s.sc, s.pow_threshold, st);
+        k_sc_after_pow<<<1, 32, 0, st>>>(s.tx, s.sc, s.r_slot);
+    }
+    return 0;
+}
+
+__global__ void __launch_bounds__(SC_THREADS) k_fold(ScKernelArgs a) {
+    const E3 r = a.sc->sc_r[a.fold_r];
+    const u64 T = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.size; i += T) {
+        st3(a.a_out, i, load_a(a, i, r));
+        st3(a.b, i, load_b(a, i, r));
+    }
+}
+
+int launch_fold(const SumcheckArgs& s, cudaStream_t st) {
+    ScKernelArgs a = make_sc(s);
+    a.fold = 1;
+    u64 want = (s.size + SC_THREADS - 1) / SC_THREADS;
+    const unsigned grid = (unsigned)(want > SC_GRID ? SC_GRID : (want < 1 ? 1 : want));
+    k_fold<<<grid, SC_THREADS, 0, st>>>(a);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Initial covector.  i = hi * 2^LO + lo; per form f the factors
+// eq_hi_f[hi] (scaled by crlc_f) and eq_lo_f[lo] are tabulated, per OOD point
+// z_j the powers crlc_{F+j} z_j^(hi 2^LO) and z_j^lo; then
+//   cov[i] = sum_f eq_hi_f[hi] eq_lo_f[lo] + sum_j zhi_j[hi] zlo_j[lo].
+// ---------------------------------------------------------------------------
+constexpr u32 COV_LO = 10;
+
+__global__ void k_cov_tables(const u64* points, u32 logS, int n_forms, int n_ood, ProofScalars* sc, E3* tab) {
+    const u32 lo_bits = logS < COV_LO ? logS : COV_LO, hi_bits = logS - lo_bits;
+    const u32 nlo = 1u << lo_bits, nhi = 1u << hi_bits;
+    const u32 per = nlo + nhi;
+    const u32 nterms = (u32)(n_forms + n_ood);
+    const u64 total = (u64)per * nterms;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
+        const u32 term = (u32)(e / per), k = (u32)(e % per);
+        E3 v;
+        if ((int)term < n_forms) {
+            const u64* pt = points + (u64)term * logS * 3;
+            // coordinate c <-> bit (logS - 1 - c) of i; hi bits are coordinates 0..hi_bits-1
+            v = e3_one();
+            if (k < nlo) {
+                for (u32 c = hi_bits; c < logS; ++c) {
+                    const E3 x{pt[3 * c], pt[3 * c + 1], pt[3 * c + 2]};
+                    const bool bit = (k >> (logS - 1 - c)) & 1;
+                    v = e3_mul(v, bit ? x : e3_sub(e3_one(), x));
+                }
+            } else {
+                const u32 h = k - nlo;
+                for (u32 c = 0; c < hi_bits; ++c) {
+                    const E3 x{pt[3 * c], pt[3 * c + 1], pt[3 * c + 2]};
+                    const bool bit = (h >> (hi_bits - 1 - c)) & 1;
+                    v = e3_mul(v, bit ? x : e3_sub(e3_one(), x));
+                }
+                // linear_forms[0] is accumulated with scalar ONE (whir_prover.hpp:161)
+                v = e3_mul(v, term == 0 ? e3_one() : sc->crlc[term]);
+            }
+        } else {
+            const int j = (int)term - n_forms;
+            const E3 z = sc->ood_pts[0][j];
+            if (k < nlo) v = e3_pow(z, k);
+            else v = e3_mul(sc->crlc[n_forms + j], e3_pow(z, (u64)(k - nlo) << lo_bits));
+        }
+        tab[e] = v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_cov_init(CovInitArgs a, const E3* tab) {
+    const u32 lo_bits = a.logS < COV_LO ? a.logS : COV_LO, hi_bits = a.logS - lo_bits;
+    const u32 nlo = 1u << lo_bits, nhi = 1u << hi_bits;
+    const u32 per = nlo + nhi;
+    const int nterms = a.n_forms + a.n_ood;
+    const u64 S = 1ull << a.logS;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < S; i += (u64)gridDim.x * blockDim.x) {
+        const u32 hi = (u32)(i >> lo_bits), lo = (u32)(i & (nlo - 1));
+        E3 acc = e3_zero();
+        for (int t = 0; t < nterms; ++t) acc = e3_add(acc, e3_mul(tab[(u64)t * per + nlo + hi], tab[(u64)t * per + lo]));
+        a.cov[0][i] = acc.c0;
+        a.cov[1][i] = acc.c1;
+        a.cov[2][i] = acc.c2;
+    }
+    (void)nhi;
+}
+
+size_t cov_init_scratch_bytes(u32 logS, int n_forms, int n_ood) {
+    const u32 lo_bits = logS < COV_LO ? logS : COV_LO, hi_bits = logS - lo_bits;
+    return ((size_t)(1u << lo_bits) + (1u << hi_bits)) * (size_t)(n_forms + n_ood) * sizeof(E3) + 256;
+}
+
+int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
+    if (a.n_forms > MAX_FORMS || a.n_ood > MAX_OOD) return -1;
+    E3* tab = reinterpret_cast<E3*>(a.scratch);
+    const int nterms = a.n_forms + a.n_ood;
+    const u64 S = 1ull << a.logS;
+    if (nterms == 0) {
+        for (int c = 0; c < 3; ++c) cudaMemsetAsync(a.cov[c], 0, S * 8, st);
+        return 0;
+    }
+    k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.sc, tab);
+    u64 want = (S + 255) / 256;
+    k_cov_init<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// STIR covector update: cov[i] += sum_j rlc_j z_j^i for the round's OOD points
+// (Ext3) and in-domain points (base field, lifted).  Thread-contiguous chunks
+// of CA_E elements: start power from two tables (z^(hi 2^LO), z^lo), then one
+// multiplication per step.
+// ---------------------------------------------------------------------------
+constexpr u32 CA_E = 8, CA_LO = 10;
+
+__global__ void k_cov_acc_tables(const ProofScalars* sc, int n_points, u32 hi_count, E3* tab) {
+    const u32 per = (1u << CA_LO) + hi_count;
+    const u64 total = (u64)per * n_points;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
+        const u32 j = (u32)(e / per), k = (u32)(e % per);
+        const E3 z = sc->stir_pts[j];
+        tab[e] = k < (1u << CA_LO) ? e3_pow(z, k) : e3_pow(z, (u64)(k - (1u << CA_LO)) << CA_LO);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* tab, u32 hi_count) {
+    const u32 per = (1u << CA_LO) + hi_count;
+    const int npts = a.n_ext + a.n_base;
+    const u64 nchunks = (a.size + CA_E - 1) / CA_E;
+    for (u64 ch = (u64)blockIdx.x * blockDim.x + threadIdx.x; ch < nchunks; ch += (u64)gridDim.x * blockDim.x) {
+        const u64 i0 = ch * CA_E;
+        const u32 cnt = (u32)((a.size - i0) < CA_E ? (a.size - i0) : CA_E);
+        E3 acc[CA_E];
+#pragma unroll
+        for (u32 e = 0; e < CA_E; ++e) acc[e] = e3_zero();
+        const u32 hi = (u32)(i0 >> CA_LO), lo = (u32)(i0 & ((1u << CA_LO) - 1));
+        for (int j = 0; j < npts; ++j) {
+            const E3 s = a.sc->stir_rlc[j];
+            const E3* tj = tab + (u64)j * per;
+            if (j < a.n_ext) {
+                const E3 z = a.sc->stir_pts[j];
+                E3 p = e3_mul(s, e3_mul(tj[(1u << CA_LO) + hi], tj[lo]));
+#pragma unroll
+                for (u32 e = 0; e < CA_E; ++e) {
+                    acc[e] = e3_add(acc[e], p);
+                    p = e3_mul(p, z);
+                }
+            } else {
+                const u64 z = a.sc->stir_pts[j].c0;
+                u64 w = gl_mul(tj[(1u << CA_LO) + hi].c0, tj[lo].c0);
+#pragma unroll
+                for (u32 e = 0; e < CA_E; ++e) {
+                    acc[e] = e3_add(acc[e], e3_mul_base(s, w));
+                    w = gl_mul(w, z);
+                }
+            }
+        }
+#pragma unroll
+        for (u32 e = 0; e < CA_E; ++e) {
+            if (e < cnt) {
+                const u64 i = i0 + e;
+                a.cov[0][i] = gl_add(a.cov[0][i], acc[e].c0);
+                a.cov[1][i] = gl_add(a.cov[1][i], acc[e].c1);
+                a.cov[2][i] = gl_add(a.cov[2][i], acc[e].c2);
+            }
+        }
+    }
+}
+
+static u32 ca_hi_count(u64 size) { return (u32)((size + (1ull << CA_LO) - 1) >> CA_LO) + 1; }
+
+size_t cov_acc_scratch_bytes(u64 size, int n_points) {
+    return ((size_t)(1u << CA_LO) + ca_hi_count(size)) * (size_t)n_points * sizeof(E3) + 256;
+}
+
+int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
+    const int npts = a.n_ext + a.n_base;
+    if (npts == 0 || a.size == 0) return 0;
+    const u32 hc = ca_hi_count(a.size);
+    E3* tab = reinterpret_cast<E3*>(a.scratch);
+    k_cov_acc_tables<<<148, 256, 0, st>>>(a.sc, npts, hc, tab);
+    const u64 nchunks = (a.size + CA_E - 1) / CA_E;
+    u64 want = (nchunks + 255) / 256;
+    k_cov_accumulate<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab, hc);
+    return 0;
+}
+
+}  // namespace wg
+
+namespace wg {
+
+// MLE evaluation sum_i v_i eq(p, i): eq factors from k_cov_tables (one form,
+// scalar one), then a CTA-reduced dot product with a last-CTA finish.
+__global__ void __launch_bounds__(256) k_mle_dot(const u64* v, u32 logS, const E3* tab, E3* partials,
+                                                 unsigned* counter, u64* out) {
+    __shared__ E3 red[32];
+    __shared__ bool is_last;
+    const u32 lo_bits = logS < COV_LO ? logS : COV_LO;
+    const u32 nlo = 1u << lo_bits;
+    const u64 S = 1ull << logS;
+    E3 acc = e3_zero();
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < S; i += (u64)gridDim.x * blockDim.x) {
+        const u32 hi = (u32)(i >> lo_bits), lo = (u32)(i & (nlo - 1));
+        acc = e3_add(acc, e3_mul_base(e3_mul(tab[nlo + hi], tab[lo]), v[i]));
+    }
+    const E3 s = block_sum(acc, red);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = s;
+        __threadfence();
+        is_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    E3 t = e3_zero();
+    for (u32 k = threadIdx.x; k < gridDim.x; k += blockDim.x)
+        t = e3_add(t, E3{__ldcg(&partials[k].c0), __ldcg(&partials[k].c1), __ldcg(&partials[k].c2)});
+    const E3 tot = block_sum(t, red);
+    if (threadIdx.x == 0) {
+        out[0] = tot.c0;
+        out[1] = tot.c1;
+        out[2] = tot.c2;
+        *counter = 0;
+    }
+}
+
+size_t mle_eval_scratch_bytes(u32 logS) { return 256 + 592 * sizeof(E3) + cov_init_scratch_bytes(logS, 1, 0); }
+
+int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch, u64* out, cudaStream_t st) {
+    // [ticket counter | per-CTA partials | eq tables]: the counter keeps a
+    // fixed offset whatever logS, and is cleared before every launch.
+    char* base = reinterpret_cast<char*>(scratch);
+    unsigned* counter = reinterpret_cast<unsigned*>(base);
+    E3* partials = reinterpret_cast<E3*>(base + 256);
+    E3* tab = reinterpret_cast<E3*>(base + 256 + 592 * sizeof(E3));
+    cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
+    k_cov_tables<<<148, 256, 0, st>>>(point, logS, 1, 0, nullptr, tab);
+    const u64 S = 1ull << logS;
+    u64 want = (S + 255) / 256;
+    const unsigned grid = (unsigned)(want > 592 ? 592 : want);
+    k_mle_dot<<<grid, 256, 0, st>>>(coeffs, logS, tab, partials, counter, out);
+    return 0;
+}
+
+}  // namespace wg

@@ -1,0 +1,353 @@
+// k_tx.cu -- the sequential Fiat-Shamir steps of the prover, executed on the
+// device: transcript start, constraint/STIR combination challenges, proof of
+// work grinding, in-domain openings (indices, row hints, Merkle paths) and
+// the final-vector message.  Protocol order and byte layout follow
+// cpp/include/whir/protocols/whir/whir_prover.hpp:56-407.
+#include "launch.h"
+#include "blake3.cuh"
+#include "state.cuh"
+
+namespace wg {
+
+// ---------------------------------------------------------------------------
+// Transcript start: ProverState::from_ds (transcript.hpp:605-610) absorbs
+// protocol_id || session_id || instance bytes.
+// ---------------------------------------------------------------------------
+__global__ void k_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
+                          unsigned char* hints, u64 hints_cap, ProofScalars* sc) {
+    if (threadIdx.x != 0) return;
+    for (int i = 0; i < 25; ++i) { tx->hasher[i] = 0; tx->reader[i] = 0; }
+    tx->hpos = tx->rpos = tx->has_reader = tx->err = 0;
+    tx->narg_len = tx->hints_len = 0;
+    tx->narg_cap = narg_cap;
+    tx->hints_cap = hints_cap;
+    tx->narg = narg;
+    tx->hints = hints;
+    tx_absorb(tx, ds, ds_len);
+    for (int i = 0; i < 64; ++i) sc->counters[i] = 0;
+}
+
+int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
+                   unsigned char* hints, u64 hints_cap, ProofScalars* sc, cudaStream_t st) {
+    k_tx_init<<<1, 32, 0, st>>>(tx, ds, ds_len, narg, narg_cap, hints, hints_cap, sc);
+    return 0;
+}
+
+// geometric_challenge (geometric_challenge.hpp:39-44): [] / [1] / squeeze x -> [1, x, x^2, ...].
+__device__ void geometric_challenge(TxState* tx, E3* out, int count) {
+    if (count <= 0) return;
+    out[0] = e3_one();
+    if (count == 1) return;
+    const E3 x = tx_challenge_e3(tx);
+    for (int i = 1; i < count; ++i) out[i] = e3_mul(out[i - 1], x);
+}
+
+// Constraint RLC and "the sum" (whir_prover.hpp:150-197) for one vector:
+// sum = sum_f crlc_f eval_f + sum_j crlc_{F+j} ood_val_j.
+__global__ void k_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood) {
+    if (threadIdx.x != 0) return;
+    const int count = n_forms + n_ood;
+    geometric_challenge(tx, sc->crlc, count);
+    E3 sum = e3_zero();
+    for (int f = 0; f < n_forms; ++f) sum = e3_add(sum, e3_mul(sc->crlc[f], sc->forms_eval[f]));
+    for (int j = 0; j < n_ood; ++j) sum = e3_add(sum, e3_mul(sc->crlc[n_forms + j], sc->ood_vals[0][j]));
+    sc->sum = sum;
+}
+
+int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood, cudaStream_t st) {
+    if (n_forms > MAX_FORMS || n_ood > MAX_OOD) return -1;
+    k_constraint_rlc<<<1, 32, 0, st>>>(tx, sc, n_forms, n_ood);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Proof of work (proof_of_work.hpp:95-193, 236-257): the smallest nonce n >= 0
+// with LE_u64(BLAKE3(challenge || n_le || 0^24)[0..8]) <= threshold.
+// Every thread walks n = g, g + T, g + 2T, ... and stops once n exceeds the
+// best nonce found so far, so every nonce below the final minimum has been
+// tested: the result is the reference's minimum, independent of scheduling.
+// ---------------------------------------------------------------------------
+// Search bound: 2^36 nonces (~1.5 s of grinding).  A 20-bit threshold fails to
+// hit within it with probability e^(-2^16); exhaustion sets TX_ERR_POW_EXHAUSTED.
+constexpr u64 POW_NONCE_LIMIT = 1ull << 36;
+
+__global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
+    if (threadIdx.x != 0) return;
+    tx_squeeze(tx, sc->pow_ch, 32);
+    sc->pow_best = ~0ull;
+}
+
+__global__ void __launch_bounds__(256) k_pow_grind(ProofScalars* sc, u64 threshold) {
+    __shared__ unsigned ch[8];
+    if (threadIdx.x < 8) {
+        const unsigned char* c = sc->pow_ch + 4 * threadIdx.x;
+        ch[threadIdx.x] = (unsigned)c[0] | ((unsigned)c[1] << 8) | ((unsigned)c[2] << 16) | ((unsigned)c[3] << 24);
+    }
+    __syncthreads();
+    unsigned m[16];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) m[k] = ch[k];
+#pragma unroll
+    for (int k = 10; k < 16; ++k) m[k] = 0;
+    const u64 T = (u64)gridDim.x * blockDim.x;
+    volatile u64* best = &sc->pow_best;
+    for (u64 n = (u64)blockIdx.x * blockDim.x + threadIdx.x; n < POW_NONCE_LIMIT; n += T) {
+        const u64 cur = *best;
+        if (n > cur) break;
+        m[8] = (unsigned)n;
+        m[9] = (unsigned)(n >> 32);
+        unsigned h[8];
+        b3_hash64(m, h);
+        const u64 v = (u64)h[0] | ((u64)h[1] << 32);
+        if (v <= threshold) {
+            atomicMin(reinterpret_cast<unsigned long long*>(&sc->pow_best), n);
+            break;
+        }
+    }
+}
+
+__global__ void k_pow_finish(TxState* tx, ProofScalars* sc, int slot) {
+    if (threadIdx.x != 0) return;
+    const u64 n = sc->pow_best;
+    if (n == ~0ull) tx->err |= TX_ERR_POW_EXHAUSTED;
+    if (slot >= 0 && slot < MAX_COMMITS + 4) sc->pow_nonces[slot] = n;
+    tx_message_u64(tx, n);
+}
+
+int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st) {
+    k_pow_grind<<<148 * 8, 256, 0, st>>>(sc, threshold);
+    return 0;
+}
+
+int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, cudaStream_t st) {
+    if (threshold == ~0ull) return 0;  // zero difficulty: nothing sent (proof_of_work.hpp:241)
+    k_pow_challenge<<<1, 32, 0, st>>>(tx, sc);
+    k_pow_grind<<<148 * 8, 256, 0, st>>>(sc, threshold);
+    k_pow_finish<<<1, 32, 0, st>>>(tx, sc, slot);
+    return 0;
+}
+
+// Final vector: prover_message of every coefficient (whir_prover.hpp:360-362).
+__global__ void k_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size) {
+    if (threadIdx.x != 0) return;
+    for (u64 i = 0; i < size; ++i) tx_message_e3(tx, E3{c0[i], c1[i], c2[i]});
+}
+
+int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size, cudaStream_t st) {
+    k_send_vector<<<1, 32, 0, st>>>(tx, c0, c1, c2, size);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Opening (irs_commit.hpp:600-713, challenge_indices.hpp:56-119,
+// merkle_tree.hpp:165-211), one CTA of 1024 threads:
+//   1. squeeze q * ceil(log2(N)/8) bytes, index = big-endian bytes mod N;
+//   2. hint: u64 (q * depth), then the q rows in index order (duplicates kept);
+//   3. (STIR) point gen^idx and value <row, eq_weights(last folding randomness)>;
+//   4. Merkle hints: sorted, deduplicated indices climbed level by level, a
+//      node's sibling is emitted unless the sibling is itself in the set.
+// ---------------------------------------------------------------------------
+constexpr int OPEN_THREADS = 1024;
+
+// Exclusive prefix count of `flag` over the CTA; *total receives the sum.
+__device__ u32 block_scan(bool flag, u32* warp_tot, u32* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, flag);
+    const u32 pre = __popc(bal & ((1u << lane) - 1));
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    if (warp == 0) {
+        u32 v = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+        u32 incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            u32 t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        warp_tot[lane] = incl - v;  // exclusive
+        if (lane == 31) *total = incl;
+    }
+    __syncthreads();
+    const u32 r = warp_tot[warp] + pre;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
+    __shared__ u64 idx_s[MAX_QUERIES];
+    __shared__ u64 cur[MAX_QUERIES];
+    __shared__ u32 warp_tot[32];
+    __shared__ u32 total;
+    __shared__ E3 eqw[MAX_DEPTH];
+    __shared__ u64 hint_base;
+    TxState* tx = a.tx;
+    ProofScalars* sc = a.sc;
+    const u32 t = threadIdx.x;
+    const u32 q = a.q;
+
+    // 1. indices
+    if (t == 0) {
+        if (a.N == 1) {
+            for (u32 i = 0; i < q; ++i) idx_s[i] = 0;
+        } else {
+            const u32 nbytes = (a.logN + 7) / 8;
+            for (u32 i = 0; i < q; ++i) {
+                unsigned char b[8];
+                tx_squeeze(tx, b, nbytes);
+                u64 acc = 0;
+                for (u32 k = 0; k < nbytes; ++k) acc = (acc << 8) | b[k];
+                idx_s[i] = acc & (a.N - 1);  // N is a power of two
+            }
+        }
+        hint_base = tx->hints_len;
+        // 3a. eq weights of the last `fold` folding challenges (multilinear_point.hpp:40-62)
+        if (a.stir) {
+            const u32 d = 1u << a.fold;
+            for (u32 i = 0; i < d; ++i) {
+                E3 acc = e3_one();
+                for (u32 k = 0; k < a.fold; ++k) {
+                    const E3 r = sc->sc_r[a.r_offset + k];
+                    const bool bit = (i >> (a.fold - 1 - k)) & 1;
+                    acc = e3_mul(acc, bit ? r : e3_sub(e3_one(), r));
+                }
+                eqw[i] = acc;
+            }
+        }
+    }
+    __syncthreads();
+    for (u32 i = t; i < q; i += blockDim.x) sc->indices[i] = idx_s[i];
+
+    // 2. row hint
+    const u64 esz = 8ull * a.ncomp;
+    const u64 row_bytes = esz * a.depth;
+    const u64 total_hint = 8 + row_bytes * q + 0;
+    const bool fits = hint_base + total_hint <= tx->hints_cap;
+    unsigned char* hb = tx->hints + hint_base;
+    if (fits) {
+        if (t == 0) {
+            const u64 len = (u64)q * a.depth;
+            for (int k = 0; k < 8; ++k) hb[k] = (unsigned char)(len >> (8 * k));
+        }
+        const u64 nwords = (u64)q * a.depth * a.ncomp;
+        for (u64 w = t; w < nwords; w += blockDim.x) {
+            const u64 qi = w / ((u64)a.depth * a.ncomp);
+            const u64 rem = w - qi * a.depth * a.ncomp;
+            const u32 el = (u32)(rem / a.ncomp), c = (u32)(rem % a.ncomp);
+            const u64 v = a.planes[((u64)c * a.depth + el) * a.N + idx_s[qi]];
+            unsigned char* dst = hb + 8 + qi * row_bytes + (u64)el * esz + 8ull * c;
+            for (int k = 0; k < 8; ++k) dst[k] = (unsigned char)(v >> (8 * k));
+        }
+    }
+
+    // 3b. STIR point and value of each opened row
+    if (a.stir) {
+        for (u32 i = t; i < q; i += blockDim.x) {
+            const u64 id = idx_s[i];
+            E3 val = e3_zero();
+            for (u32 el = 0; el < a.depth; ++el) {
+                E3 x;
+                if (a.ncomp == 1) x = e3_base(a.planes[(u64)el * a.N + id]);
+                else x = E3{a.planes[(u64)el * a.N + id], a.planes[((u64)a.depth + el) * a.N + id],
+                            a.planes[((u64)2 * a.depth + el) * a.N + id]};
+                val = e3_add(val, e3_mul(x, eqw[el]));
+            }
+            sc->stir_pts[a.ood_offset + i] = e3_base(gl_pow(a.gen, id));
+            sc->stir_vals[a.ood_offset + i] = val;
+        }
+    }
+
+    // 4. Merkle hints.  Sort + dedup: a first occurrence v goes to slot
+    //    #{j : idx_j < v}; distinct values get distinct, order-preserving
+    //    slots, which are then compacted with a CTA scan.
+    __shared__ unsigned char occ[MAX_QUERIES];
+    for (u32 s2 = t; s2 < (u32)MAX_QUERIES; s2 += blockDim.x) occ[s2] = 0;
+    __syncthreads();
+    if (t < q) {
+        const u64 v = idx_s[t];
+        u32 lt = 0;
+        bool dup = false;
+        for (u32 j = 0; j < q; ++j) {
+            const u64 o = idx_s[j];
+            lt += (o < v) ? 1u : 0u;
+            dup |= (o == v && j < t);
+        }
+        if (!dup) { cur[lt] = v; occ[lt] = 1; }
+    }
+    __syncthreads();
+    const bool present = t < q && occ[t];
+    const u64 pv = present ? cur[t] : 0;
+    const u32 pos = block_scan(present, warp_tot, &total);
+    const u32 tot_distinct = total;
+    if (present) cur[pos] = pv;
+    __syncthreads();
+
+    u64 node_hint_off = hint_base + total_hint;
+    u32 u = tot_distinct;
+    u64 level_off = 0, level_len = a.N;
+    // (the reference leaf layer is 2^ceil(log2 N) = N for power-of-two N)
+    for (u32 lvl = 0; lvl < a.logN; ++lvl) {
+        const bool act = t < u;
+        u64 v = act ? cur[t] : 0;
+        bool sib_present = false;
+        if (act) {
+            if ((v & 1) == 0) sib_present = (t + 1 < u) && cur[t + 1] == v + 1;
+            else sib_present = (t > 0) && cur[t - 1] == v - 1;
+        }
+        const bool emit = act && !sib_present;
+        const u32 epos = block_scan(emit, warp_tot, &total);
+        const u32 nemit = total;
+        if (emit && fits && node_hint_off + 32ull * (epos + 1) <= tx->hints_cap) {
+            const uint4* src = reinterpret_cast<const uint4*>(a.nodes + (level_off + (v ^ 1)) * 8);
+            const uint4 h0 = src[0], h1 = src[1];
+            unsigned char* dst = tx->hints + node_hint_off + 32ull * epos;
+            const unsigned w8[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+            for (int k = 0; k < 32; ++k) dst[k] = (unsigned char)(w8[k >> 2] >> (8 * (k & 3)));
+        }
+        node_hint_off += 32ull * nemit;
+        // next level: parents, deduplicated (sorted input -> equal parents are adjacent)
+        const u64 par = v >> 1;
+        const bool keep = act && (t == 0 || (cur[t - 1] >> 1) != par);
+        __syncthreads();
+        const u32 kpos = block_scan(keep, warp_tot, &total);
+        const u32 nu = total;
+        if (keep) cur[kpos] = par;
+        __syncthreads();
+        u = nu;
+        level_off += level_len;
+        level_len >>= 1;
+    }
+    if (t == 0) {
+        if (!fits || node_hint_off > tx->hints_cap) tx->err |= TX_ERR_HINT_OVERFLOW;
+        else tx->hints_len = node_hint_off;
+    }
+}
+
+int launch_open(const OpenArgs& a, cudaStream_t st) {
+    if (a.q > (u32)MAX_QUERIES || a.depth > (u32)MAX_DEPTH) return -1;
+    k_open<<<1, OPEN_THREADS, 0, st>>>(a);
+    return 0;
+}
+
+// STIR combination: the new commitment's OOD points/values first, then the
+// in-domain ones written by k_open; RLC = geometric_challenge(O + q);
+// sum += <rlc, values>.
+__global__ void k_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int q) {
+    if (threadIdx.x != 0) return;
+    for (int j = 0; j < n_ood; ++j) {
+        sc->stir_pts[j] = sc->ood_pts[commit_idx][j];
+        sc->stir_vals[j] = sc->ood_vals[commit_idx][j];
+    }
+    const int count = n_ood + q;
+    geometric_challenge(tx, sc->stir_rlc, count);
+    E3 acc = sc->sum;
+    for (int j = 0; j < count; ++j) acc = e3_add(acc, e3_mul(sc->stir_rlc[j], sc->stir_vals[j]));
+    sc->sum = acc;
+}
+
+int launch_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int q, cudaStream_t st) {
+    if (n_ood > MAX_OOD || q > MAX_QUERIES) return -1;
+    k_stir_rlc<<<1, 32, 0, st>>>(tx, sc, commit_idx, n_ood, q);
+    return 0;
+}
+
+}  // namespace wg

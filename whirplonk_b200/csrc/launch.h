@@ -1,0 +1,162 @@
+// launch.h -- host-side declarations of the kernel launchers (implemented in
+// the k_*.cu files) used by the prover schedule in prover.cu.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime_api.h>
+
+namespace wg {
+
+typedef uint64_t u64;
+typedef unsigned int u32;
+struct TxState;
+struct ProofScalars;
+
+// Twiddle tables: w_{2^TW_LOG}^E = tw_hi[E >> TW_HALF] * tw_lo[E & (2^TW_HALF - 1)],
+// and stage twiddles tw_stage[u] = w_{2^TW_STAGE_LOG}^u, u < 2^(TW_STAGE_LOG-1).
+constexpr u32 TW_LOG = 26, TW_HALF = 13, TW_STAGE_LOG = 11;
+
+// ---- Reed-Solomon encoder -------------------------------------------------
+struct LdePlan {
+    u32 logN, npass;
+    u32 logR[3];
+};
+struct NttPassArgs {
+    const u64* src[3];
+    u64 m;
+    u64* tmp;
+    u64* out;
+    u32 depth, logN, logR, logS, logW, npass, pass, logR0, logR1;
+    const u64* tw_stage;
+    const u64* tw_hi;
+    const u64* tw_lo;
+};
+struct LdeArgs {
+    const u64* src[3];  // component planes of the message vector (block b at src[c] + b*m)
+    u64 m;              // message length per block
+    u32 depth;          // interleaving depth (blocks per component)
+    u32 planes;         // depth * components
+    u32 logN;           // codeword length
+    u64* tmp;           // scratch, planes * N words
+    u64* out;           // codeword planes, planes * N words
+    const u64* tw_stage;
+    const u64* tw_hi;
+    const u64* tw_lo;
+};
+LdePlan plan_lde(u32 logN);
+int launch_lde(const LdeArgs& a, cudaStream_t st);
+int lde_prepare();
+
+// ---- Merkle commitment ------------------------------------------------------
+// Leaf i = BLAKE3 of row i (LE bytes of `depth` elements of `ncomp` words),
+// written to nodes[i].  Rows are gathered from the codeword planes.
+int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st);
+// Builds all Merkle levels above the leaves of a 2^logN-leaf tree in `nodes`
+// ([leaves | level 1 | ... | root], 8 words per node).  The CTA that computes
+// the root also performs the transcript step of irs_commit::commit
+// (irs_commit.hpp:433-478): prover_message(root), then squeezes `n_ood`
+// Ext3 out-of-domain points into sc->ood_pts[commit_idx].
+int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, cudaStream_t st);
+
+// ---- Out-of-domain evaluation ----------------------------------------------
+// value_j = sum_i v_i z_j^i for z_j = sc->ood_pts[commit_idx][j]; the last CTA
+// sends every value as a prover message (in point order) and stores them in
+// sc->ood_vals[commit_idx].
+int launch_ood(const u64* v0, const u64* v1, const u64* v2, bool ext3, u64 size, TxState* tx, ProofScalars* sc,
+               int commit_idx, int n_ood, void* scratch, cudaStream_t st);
+size_t ood_scratch_bytes();
+
+// ---- Transcript / protocol steps (single-thread kernels) ---------------------
+int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
+                   unsigned char* hints, u64 hints_cap, ProofScalars* sc, cudaStream_t st);
+// Constraint RLC + initial sum (whir_prover.hpp:150-197).
+int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood, cudaStream_t st);
+// PoW: squeeze the 32-byte challenge, grind the minimum nonce, send it.
+int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, cudaStream_t st);
+// Sends every coefficient of the final folded vector (whir_prover.hpp:360-362).
+int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size, cudaStream_t st);
+
+// ---- Opening ------------------------------------------------------------------
+struct OpenArgs {
+    TxState* tx;
+    ProofScalars* sc;
+    const u64* planes;  // codeword planes of the opened commitment
+    const u32* nodes;   // its Merkle nodes
+    u64 N;              // codeword length
+    u32 logN;
+    u32 depth, ncomp;   // row = depth elements of ncomp words
+    u32 q;              // in-domain samples
+    u64 gen;            // w_N (evaluation-domain generator)
+    int stir;           // also fill sc->stir_pts/stir_vals[ood_offset + i]
+    int ood_offset;
+    int r_offset;       // sc->sc_r[r_offset .. r_offset + fold) are the folding randomness
+    u32 fold;           // number of folding variables (depth = 2^fold)
+};
+int launch_open(const OpenArgs& a, cudaStream_t st);
+// STIR combination (whir_prover.hpp:283-336): copy the new commitment's OOD
+// points/values into the STIR arrays, squeeze the geometric RLC, update the sum.
+int launch_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int q, cudaStream_t st);
+
+// ---- Covector / sumcheck ---------------------------------------------------------
+// cov[i] = sum_f crlc_f eq(p_f, i) + sum_j crlc_{F+j} z_j^i over 2^logS entries.
+struct CovInitArgs {
+    u64* cov[3];
+    u32 logS;
+    const u64* points;  // n_forms * logS * 3 words (Ext3 coordinates)
+    int n_forms, n_ood;
+    ProofScalars* sc;
+    void* scratch;
+};
+int launch_cov_init(const CovInitArgs& a, cudaStream_t st);
+size_t cov_init_scratch_bytes(u32 logS, int n_forms, int n_ood);
+// cov[i] += sum_j stir_rlc_j stir_pts_j^i (Ext3 OOD points first, then base points).
+struct CovAccArgs {
+    u64* cov[3];
+    u64 size;
+    int n_ext, n_base;
+    ProofScalars* sc;
+    void* scratch;
+};
+int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st);
+size_t cov_acc_scratch_bytes(u64 size, int n_points);
+
+struct SumcheckArgs {
+    const u64* a_base;  // non-null: the (unfolded) vector is in the base field
+    u64* a_in[3];
+    u64* a_out[3];
+    u64* b[3];
+    u64 size;           // vector size of this round (after the optional fold)
+    int fold;           // fold from 2*size with sc->sc_r[fold_r] first
+    int fold_r;
+    int r_slot;         // this round's challenge goes to sc->sc_r[r_slot]
+    u64 pow_threshold;
+    TxState* tx;
+    ProofScalars* sc;
+    void* scratch;
+};
+// One sumcheck round (sumcheck_protocol.hpp:99-135) with the previous round's
+// fold fused in.  PoW (if any) and the challenge squeeze happen in-stream.
+int launch_sumcheck_round(const SumcheckArgs& a, cudaStream_t st);
+// Fold only: a_out[i] = a_in[i] + r (a_in[i+size] - a_in[i]), same for b.
+int launch_fold(const SumcheckArgs& a, cudaStream_t st);
+size_t sumcheck_scratch_bytes();
+
+// ---- Twiddle tables ----------------------------------------------------------------
+void host_twiddles(u64* stage /*1024*/, u64* hi /*8192*/, u64* lo /*8192*/);
+
+}  // namespace wg
+
+namespace wg {
+// Multilinear extension of base coefficients at one Ext3 point; the result
+// (3 words) is written to `out` in device memory.
+int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch, u64* out, cudaStream_t st);
+size_t mle_eval_scratch_bytes(u32 logS);
+
+// Kernel-family timing hooks used by the schedule (null timer = off).
+enum Family { FAM_NTT = 0, FAM_LEAF, FAM_MERKLE, FAM_OOD, FAM_SUMCHECK, FAM_COV, FAM_POW, FAM_OPEN, FAM_TX, FAM_COUNT };
+struct Timer {
+    virtual ~Timer() {}
+    virtual void begin(int fam, cudaStream_t st) = 0;
+    virtual void end(int fam, cudaStream_t st) = 0;
+};
+}  // namespace wg

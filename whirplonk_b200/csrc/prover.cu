@@ -1,0 +1,320 @@
+// prover.cu -- workspace layout and kernel schedule of commit + prove.
+//
+// The order of steps is the reference's (cpp/include/whir/protocols/whir/
+// whir.hpp:303-309 and whir_prover.hpp:56-407) specialised to one committed
+// vector over Goldilocks with Ext3 challenges:
+//   commit:  RS encode -> leaves -> Merkle root (message) -> OOD points/values
+//   prove:   constraint RLC, covector, initial sumcheck,
+//            per round: commit folded vector, PoW, open previous commitment,
+//                       STIR RLC + covector update, sumcheck;
+//            final vector, final PoW, final opening, final sumcheck.
+#include <algorithm>
+#include <stdexcept>
+
+#include "launch.h"
+#include "prover.h"
+#include "state.cuh"
+
+namespace wg {
+
+namespace {
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+struct Bump {
+    size_t cur = 0;
+    size_t take(size_t bytes) {
+        size_t o = cur;
+        cur = align_up(cur + bytes, 256);
+        return o;
+    }
+};
+uint32_t ilog2(uint64_t v) {
+    uint32_t k = 0;
+    while ((1ull << k) < v) ++k;
+    return k;
+}
+}  // namespace
+
+ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_t ds_len) {
+    ProofPlan p;
+    p.sch = make_schedule(n, params);
+    p.params = params;
+    p.n = n;
+    p.n_forms = n_forms;
+    if (n_forms < 0 || n_forms > MAX_FORMS) throw std::invalid_argument("too many statement forms");
+    const WhirSchedule& s = p.sch;
+    auto check_irs = [](const IrsSchedule& c, uint32_t ncomp) {
+        const uint64_t N = c.codeword_length;
+        if (N == 0 || (N & (N - 1))) throw std::invalid_argument("codeword length must be a power of two");
+        if (ilog2(N) > TW_LOG) throw std::invalid_argument("codeword length above 2^26");
+        if (c.depth > (uint64_t)MAX_DEPTH) throw std::invalid_argument("folding factor too large");
+        if (c.depth * ncomp * 8 > 1024) throw std::invalid_argument("rows above one BLAKE3 chunk");
+        if (c.in_domain > (uint64_t)MAX_QUERIES) throw std::invalid_argument("too many in-domain samples");
+        if (c.out_domain > (uint64_t)MAX_OOD) throw std::invalid_argument("too many out-of-domain samples");
+        if (N % c.message_length() != 0) throw std::invalid_argument("codeword length not a multiple of message length");
+    };
+    check_irs(s.initial, 1);
+    for (const auto& r : s.rounds) check_irs(r.irs, 3);
+    if ((size_t)n > (size_t)MAX_SC_ROUNDS) throw std::invalid_argument("too many variables");
+    if (s.rounds.size() + 1 > (size_t)MAX_COMMITS) throw std::invalid_argument("too many rounds");
+
+    Bump b;
+    const uint64_t size = 1ull << n;
+    p.off_coeffs = b.take(size * 8);
+    p.a_plane_words = std::max<uint64_t>(size / 2, 1);
+    p.off_a = b.take(3 * p.a_plane_words * 8);
+    p.cov_plane_words = size;
+    p.off_cov = b.take(3 * size * 8);
+    size_t tmp_words = 0;
+    auto add_commit = [&](const IrsSchedule& c, uint32_t ncomp) {
+        CommitBuffers cb;
+        cb.N = c.codeword_length;
+        cb.logN = ilog2(cb.N);
+        cb.depth = (uint32_t)c.depth;
+        cb.ncomp = ncomp;
+        const size_t words = (size_t)cb.N * cb.depth * ncomp;
+        cb.planes = b.take(words * 8);
+        cb.nodes = b.take((2 * cb.N - 1) * 32);
+        tmp_words = std::max(tmp_words, words);
+        p.commits.push_back(cb);
+    };
+    add_commit(s.initial, 1);
+    for (const auto& r : s.rounds) add_commit(r.irs, 3);
+    p.off_tmp = b.take(tmp_words * 8);
+    p.off_sc_scratch = b.take(sumcheck_scratch_bytes());
+    p.off_ood_scratch = b.take(ood_scratch_bytes());
+    size_t cov_scratch = cov_init_scratch_bytes(n, n_forms, (int)s.initial.out_domain);
+    for (size_t r = 0; r < s.rounds.size(); ++r) {
+        const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;
+        const int npts = (int)(s.rounds[r].irs.out_domain + prev.in_domain);
+        cov_scratch = std::max(cov_scratch, cov_acc_scratch_bytes(s.rounds[r].irs.vector_size, npts));
+    }
+    p.off_cov_scratch = b.take(cov_scratch);
+    p.off_tx = b.take(sizeof(TxState));
+    p.off_scalars = b.take(sizeof(ProofScalars));
+
+    // Proof stream sizes.
+    size_t narg = 0, hints = 0;
+    auto commit_narg = [](const IrsSchedule& c) { return 32 + 24 * c.out_domain; };
+    auto pow_narg = [](uint64_t thr) { return thr == ~0ull ? 0 : 8; };
+    auto sumcheck_narg = [&](const SumcheckSchedule& sc) { return sc.num_rounds * (48 + pow_narg(sc.pow_threshold)); };
+    auto open_hints = [](const IrsSchedule& c, uint32_t ncomp) {
+        const uint64_t logN = ilog2(c.codeword_length);
+        const uint64_t merkle = std::min<uint64_t>(c.in_domain * logN, c.codeword_length);
+        return 8 + c.in_domain * c.depth * 8 * ncomp + 32 * merkle;
+    };
+    narg += commit_narg(s.initial);
+    const bool has_constraints = n_forms + s.initial.out_domain > 0;
+    if (has_constraints) narg += sumcheck_narg(s.initial_sumcheck);
+    else narg += pow_narg(s.initial_skip_pow);
+    size_t sc_rounds = s.initial_sumcheck.num_rounds;
+    for (size_t r = 0; r < s.rounds.size(); ++r) {
+        narg += commit_narg(s.rounds[r].irs) + pow_narg(s.rounds[r].pow_threshold) + sumcheck_narg(s.rounds[r].sumcheck);
+        hints += r == 0 ? open_hints(s.initial, 1) : open_hints(s.rounds[r - 1].irs, 3);
+        sc_rounds += s.rounds[r].sumcheck.num_rounds;
+    }
+    narg += 24 * s.final_sumcheck.initial_size + pow_narg(s.final_pow) + sumcheck_narg(s.final_sumcheck);
+    hints += s.rounds.empty() ? open_hints(s.initial, 1) : open_hints(s.rounds.back().irs, 3);
+    sc_rounds += s.final_sumcheck.num_rounds;
+    p.narg_len = narg;
+    p.hints_cap = hints;
+    p.total_sumcheck_rounds = sc_rounds;
+    p.off_narg = b.take(narg + 64);
+    p.off_hints = b.take(hints + 64);
+    p.ds_cap = std::max<size_t>(ds_len, 96);
+    p.off_ds = b.take(p.ds_cap);
+    p.off_points = b.take((size_t)std::max(n_forms, 1) * n * 24 + 64);
+    p.total_bytes = b.cur;
+    return p;
+}
+
+TxState* plan_tx(const ProofPlan& p, char* ws) { return reinterpret_cast<TxState*>(ws + p.off_tx); }
+ProofScalars* plan_scalars(const ProofPlan& p, char* ws) { return reinterpret_cast<ProofScalars*>(ws + p.off_scalars); }
+
+namespace {
+
+struct Ctx {
+    const ProofPlan& p;
+    char* ws;
+    const DeviceTables& tw;
+    cudaStream_t st;
+    Timer* timer;
+    TxState* tx() const { return plan_tx(p, ws); }
+    ProofScalars* sc() const { return plan_scalars(p, ws); }
+    uint64_t* w(size_t off) const { return reinterpret_cast<uint64_t*>(ws + off); }
+    uint64_t* a(int c) const { return w(p.off_a) + (size_t)c * p.a_plane_words; }
+    uint64_t* cov(int c) const { return w(p.off_cov) + (size_t)c * p.cov_plane_words; }
+};
+
+#define WG_TRY(x)                 \
+    do {                          \
+        int _rc = (x);            \
+        if (_rc != 0) return _rc; \
+    } while (0)
+
+// Launch `x` bracketed by the family timer when timing is on.
+#define WG_TIMED(c, fam, x)                                \
+    do {                                                   \
+        if ((c).timer) (c).timer->begin((fam), (c).st);    \
+        int _rc = (x);                                     \
+        if ((c).timer) (c).timer->end((fam), (c).st);      \
+        if (_rc != 0) return _rc;                          \
+    } while (0)
+
+// RS encode + leaves + Merkle + OOD of commitment `ci` whose message is the
+// vector (src planes, vsize words each).
+int commit_vector(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t ncomp, uint64_t vsize, int n_ood) {
+    const CommitBuffers& cb = c.p.commits[ci];
+    LdeArgs L{};
+    for (int k = 0; k < 3; ++k) L.src[k] = src[k] ? src[k] : src[0];
+    L.m = vsize / cb.depth;
+    L.depth = cb.depth;
+    L.planes = cb.depth * ncomp;
+    L.logN = cb.logN;
+    L.tmp = c.w(c.p.off_tmp);
+    L.out = c.w(cb.planes);
+    L.tw_stage = c.tw.tw_stage;
+    L.tw_hi = c.tw.tw_hi;
+    L.tw_lo = c.tw.tw_lo;
+    WG_TIMED(c, FAM_NTT, launch_lde(L, c.st));
+    uint32_t* nodes = reinterpret_cast<uint32_t*>(c.ws + cb.nodes);
+    WG_TIMED(c, FAM_LEAF, launch_leaves(c.w(cb.planes), cb.N, cb.depth, ncomp, nodes, c.st));
+    WG_TIMED(c, FAM_MERKLE, launch_merkle(nodes, cb.logN, c.tx(), c.sc(), ci, n_ood, c.st));
+    WG_TIMED(c, FAM_OOD, launch_ood(src[0], src[1], src[2], ncomp == 3, vsize, c.tx(), c.sc(), ci, n_ood,
+                                    c.ws + c.p.off_ood_scratch, c.st));
+    return 0;
+}
+
+// `rounds` sumcheck rounds on (a, cov) of size `size`.  `base_first`: the
+// vector is still the base-field coefficient array (first sumcheck only).
+// Leaves a, cov folded to size >> rounds when `fold_after` is set.
+int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_first, int& r_slot, bool fold_after) {
+    for (uint64_t t = 0; t < s.num_rounds; ++t) {
+        SumcheckArgs a{};
+        const bool from_base = base_first && t <= 1;
+        a.a_base = from_base ? c.w(c.p.off_coeffs) : nullptr;
+        for (int k = 0; k < 3; ++k) { a.a_in[k] = c.a(k); a.a_out[k] = c.a(k); a.b[k] = c.cov(k); }
+        a.size = size >> t;
+        a.fold = t > 0;
+        a.fold_r = r_slot - 1;
+        a.r_slot = r_slot;
+        a.pow_threshold = s.pow_threshold;
+        a.tx = c.tx();
+        a.sc = c.sc();
+        a.scratch = c.ws + c.p.off_sc_scratch;
+        if (base_first && t == 0) a.a_base = c.w(c.p.off_coeffs);
+        WG_TIMED(c, FAM_SUMCHECK, launch_sumcheck_round(a, c.st));
+        ++r_slot;
+    }
+    if (fold_after && s.num_rounds > 0) {
+        SumcheckArgs a{};
+        const bool from_base = base_first && s.num_rounds == 1;
+        a.a_base = from_base ? c.w(c.p.off_coeffs) : nullptr;
+        for (int k = 0; k < 3; ++k) { a.a_in[k] = c.a(k); a.a_out[k] = c.a(k); a.b[k] = c.cov(k); }
+        a.size = size >> s.num_rounds;
+        a.fold_r = r_slot - 1;
+        a.sc = c.sc();
+        WG_TIMED(c, FAM_SUMCHECK, launch_fold(a, c.st));
+    }
+    return 0;
+}
+
+}  // namespace
+
+int enqueue_commit(const ProofPlan& p, char* ws, uint32_t ds_len, const DeviceTables& tw, cudaStream_t st,
+                   Timer* timer) {
+    Ctx c{p, ws, tw, st, timer};
+    WG_TIMED(c, FAM_TX, launch_tx_init(c.tx(), reinterpret_cast<const unsigned char*>(ws + p.off_ds), ds_len,
+                          reinterpret_cast<unsigned char*>(ws + p.off_narg), p.narg_len + 64,
+                          reinterpret_cast<unsigned char*>(ws + p.off_hints), p.hints_cap + 64, c.sc(), st));
+    const uint64_t* src[3] = {c.w(p.off_coeffs), nullptr, nullptr};
+    return commit_vector(c, 0, src, 1, 1ull << p.n, (int)p.sch.initial.out_domain);
+}
+
+int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStream_t st, Timer* timer) {
+    Ctx c{p, ws, tw, st, timer};
+    const WhirSchedule& s = p.sch;
+    const int ood0 = (int)s.initial.out_domain;
+    WG_TIMED(c, FAM_TX, launch_constraint_rlc(c.tx(), c.sc(), p.n_forms, ood0, st));
+    const bool has_constraints = p.n_forms + ood0 > 0;
+    int r_slot = 0;
+    const uint64_t size0 = 1ull << p.n;
+    if (has_constraints) {
+        CovInitArgs ci{};
+        for (int k = 0; k < 3; ++k) ci.cov[k] = c.cov(k);
+        ci.logS = p.n;
+        ci.points = c.w(p.off_points);
+        ci.n_forms = p.n_forms;
+        ci.n_ood = ood0;
+        ci.sc = c.sc();
+        ci.scratch = ws + p.off_cov_scratch;
+        WG_TIMED(c, FAM_COV, launch_cov_init(ci, st));
+        WG_TRY(sumcheck(c, s.initial_sumcheck, size0, true, r_slot, true));
+    } else {
+        return -2;  // statement-free proofs (unique decoding, no forms) are not on this path
+    }
+
+    uint64_t vsize = size0 >> s.initial_sumcheck.num_rounds;
+    for (size_t r = 0; r < s.rounds.size(); ++r) {
+        const RoundSchedule& rc = s.rounds[r];
+        const int ci = (int)r + 1;
+        const uint64_t* src[3] = {c.a(0), c.a(1), c.a(2)};
+        WG_TRY(commit_vector(c, ci, src, 3, vsize, (int)rc.irs.out_domain));
+        WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), rc.pow_threshold, ci, st));
+        // open the previous commitment
+        const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;
+        const CommitBuffers& pb = p.commits[ci - 1];
+        OpenArgs oa{};
+        oa.tx = c.tx();
+        oa.sc = c.sc();
+        oa.planes = c.w(pb.planes);
+        oa.nodes = reinterpret_cast<const uint32_t*>(ws + pb.nodes);
+        oa.N = pb.N;
+        oa.logN = pb.logN;
+        oa.depth = pb.depth;
+        oa.ncomp = pb.ncomp;
+        oa.q = (uint32_t)prev.in_domain;
+        oa.gen = gl_pow_host(7, (GL_P - 1) / pb.N);  // w_N = 7^((p-1)/N)
+        oa.stir = 1;
+        oa.ood_offset = (int)rc.irs.out_domain;
+        const uint32_t prev_fold = (uint32_t)(r == 0 ? s.initial_sumcheck.num_rounds : s.rounds[r - 1].sumcheck.num_rounds);
+        oa.fold = prev_fold;
+        oa.r_offset = r_slot - (int)prev_fold;
+        WG_TIMED(c, FAM_OPEN, launch_open(oa, st));
+        WG_TIMED(c, FAM_TX, launch_stir_rlc(c.tx(), c.sc(), ci, (int)rc.irs.out_domain, (int)prev.in_domain, st));
+        CovAccArgs ca{};
+        for (int k = 0; k < 3; ++k) ca.cov[k] = c.cov(k);
+        ca.size = vsize;
+        ca.n_ext = (int)rc.irs.out_domain;
+        ca.n_base = (int)prev.in_domain;
+        ca.sc = c.sc();
+        ca.scratch = ws + p.off_cov_scratch;
+        WG_TIMED(c, FAM_COV, launch_cov_accumulate(ca, st));
+        WG_TRY(sumcheck(c, rc.sumcheck, vsize, false, r_slot, true));
+        vsize >>= rc.sumcheck.num_rounds;
+    }
+
+    // final vector, PoW, opening, sumcheck
+    WG_TIMED(c, FAM_TX, launch_send_vector(c.tx(), c.a(0), c.a(1), c.a(2), vsize, st));
+    WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), s.final_pow, (int)s.rounds.size() + 1, st));
+    {
+        const IrsSchedule& last = s.rounds.empty() ? s.initial : s.rounds.back().irs;
+        const CommitBuffers& lb = p.commits.back();
+        OpenArgs oa{};
+        oa.tx = c.tx();
+        oa.sc = c.sc();
+        oa.planes = c.w(lb.planes);
+        oa.nodes = reinterpret_cast<const uint32_t*>(ws + lb.nodes);
+        oa.N = lb.N;
+        oa.logN = lb.logN;
+        oa.depth = lb.depth;
+        oa.ncomp = lb.ncomp;
+        oa.q = (uint32_t)last.in_domain;
+        oa.gen = 1;
+        oa.stir = 0;
+        WG_TIMED(c, FAM_OPEN, launch_open(oa, st));
+    }
+    if (s.final_sumcheck.num_rounds > 0) WG_TRY(sumcheck(c, s.final_sumcheck, vsize, false, r_slot, false));
+    return 0;
+}
+
+}  // namespace wg

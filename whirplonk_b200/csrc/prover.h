@@ -1,0 +1,67 @@
+// prover.h -- the device-resident WHIR prover schedule.
+//
+// A ProofPlan is a pure function of (num_variables, ProtocolParameters,
+// number of statement forms): every buffer offset and every kernel launch of
+// commit + prove is fixed by it.  All data-dependent values (challenges,
+// indices, nonces, hint lengths) stay on the device, so a plan is enqueued
+// without a single host synchronisation and can be captured into a CUDA graph.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime_api.h>
+
+#include "params.h"
+
+namespace wg {
+
+struct TxState;
+struct ProofScalars;
+
+struct CommitBuffers {
+    uint64_t N = 0;
+    uint32_t logN = 0, depth = 0, ncomp = 0;
+    size_t planes = 0, nodes = 0;  // byte offsets in the workspace
+};
+
+struct ProofPlan {
+    WhirSchedule sch;
+    ProtocolParams params;
+    uint32_t n = 0;          // num_variables
+    int n_forms = 0;
+    // byte offsets in the workspace
+    size_t off_coeffs = 0, off_a = 0, off_cov = 0, off_tmp = 0;
+    size_t off_sc_scratch = 0, off_ood_scratch = 0, off_cov_scratch = 0;
+    size_t off_tx = 0, off_scalars = 0, off_narg = 0, off_hints = 0, off_ds = 0, off_points = 0;
+    std::vector<CommitBuffers> commits;  // [initial, round 0, round 1, ...]
+    size_t a_plane_words = 0, cov_plane_words = 0;
+    size_t narg_len = 0;       // exact narg length (every message has a fixed size)
+    size_t hints_cap = 0;      // upper bound of the hint stream
+    size_t ds_cap = 0;
+    size_t total_bytes = 0;
+    size_t total_sumcheck_rounds = 0;
+};
+
+// Throws std::invalid_argument on unsupported parameters.
+ProofPlan make_plan(uint32_t num_variables, const ProtocolParams& p, int n_forms, size_t ds_len);
+
+struct DeviceTables {
+    uint64_t* tw_stage = nullptr;
+    uint64_t* tw_hi = nullptr;
+    uint64_t* tw_lo = nullptr;
+};
+
+// Enqueue the whole commit (Config::commit) on `st`.  The workspace must hold
+// the coefficients at off_coeffs and the domain-separator bytes at off_ds.
+struct Timer;
+int enqueue_commit(const ProofPlan& p, char* ws, uint32_t ds_len, const DeviceTables& tw, cudaStream_t st,
+                   Timer* timer = nullptr);
+// Enqueue Config::prove for MLE-point statements (points at off_points,
+// claimed evaluations already in ProofScalars::forms_eval).
+int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStream_t st, Timer* timer = nullptr);
+
+TxState* plan_tx(const ProofPlan& p, char* ws);
+ProofScalars* plan_scalars(const ProofPlan& p, char* ws);
+
+}  // namespace wg

@@ -1,0 +1,39 @@
+// state.cuh -- per-proof device state shared by all kernels of one proof.
+//
+// Everything the reference prover keeps in host variables between transcript
+// interactions (whir_prover.hpp:56-407: the running sum, folding randomness,
+// OOD points/values, constraint and STIR combination coefficients, opened
+// indices, PoW nonces) lives here in HBM, so the whole commit+prove is one
+// stream of kernels with no host round trip.
+#pragma once
+#include "gl.cuh"
+#include "transcript.cuh"
+
+namespace wg {
+
+constexpr int MAX_OOD = 8;          // out-of-domain samples per commitment
+constexpr int MAX_FORMS = 8;        // statement linear forms
+constexpr int MAX_QUERIES = 1024;   // in-domain samples per opening
+constexpr int MAX_SC_ROUNDS = 64;   // total sumcheck rounds (= num_variables)
+constexpr int MAX_COMMITS = 24;     // initial + round commitments
+constexpr int MAX_DEPTH = 64;       // interleaving depth 2^k
+
+struct ProofScalars {
+    E3 sum;                                  // claimed <vector, covector>
+    E3 c0, c2;                               // current sumcheck round polynomial
+    E3 sc_r[MAX_SC_ROUNDS];                  // folding randomness, in order (= evaluation point)
+    E3 ood_pts[MAX_COMMITS][MAX_OOD];
+    E3 ood_vals[MAX_COMMITS][MAX_OOD];
+    E3 crlc[MAX_FORMS + MAX_OOD];            // constraint RLC coefficients
+    E3 forms_eval[MAX_FORMS];                // claimed evaluations (input)
+    E3 stir_rlc[MAX_QUERIES + MAX_OOD];      // STIR combination coefficients of the current round
+    E3 stir_pts[MAX_QUERIES + MAX_OOD];      // OOD points then in-domain points (base, lifted)
+    E3 stir_vals[MAX_QUERIES + MAX_OOD];
+    u64 indices[MAX_QUERIES];                // opened rows of the current opening
+    u64 pow_best;                            // minimum valid nonce (atomicMin target)
+    u64 pow_nonces[MAX_COMMITS + 4];         // recorded nonces (diagnostics)
+    unsigned char pow_ch[32];
+    unsigned counters[64];                   // self-resetting last-block tickets
+};
+
+}  // namespace wg
