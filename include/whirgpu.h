@@ -105,6 +105,9 @@ whirgpu_status whirgpu_prove(whirgpu_ctx* ctx, whirgpu_witness* witness, const u
                              const uint64_t* evaluations, whirgpu_transcript* tx, uint64_t* evaluation_point,
                              uint64_t* rlc);
 
+/* Bytes the last commit + prove pair moved host->device and device->host. */
+void whirgpu_last_io_bytes(const whirgpu_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
+
 /* ---- helpers ------------------------------------------------------------------- */
 /* Multilinear extension of 2^num_variables base coefficients at an Ext3 point
  * (MultilinearExtension::evaluate, linear_form.hpp:119-126), on the device. */
@@ -127,6 +130,8 @@ void whirgpu_host_free(void* p);
  * 2 Merkle, 3 OOD, 4 sumcheck, 5 covector, 6 PoW, 7 opening, 8 transcript. */
 #define WHIRGPU_NUM_FAMILIES 9
 whirgpu_status whirgpu_set_timing(whirgpu_ctx* ctx, int enabled);
+/* Number of kernels this library has launched in the process so far. */
+uint64_t whirgpu_launch_count(void);
 whirgpu_status whirgpu_kernel_stats(whirgpu_ctx* ctx, uint64_t launches[WHIRGPU_NUM_FAMILIES],
                                     double ms[WHIRGPU_NUM_FAMILIES], int reset);
 

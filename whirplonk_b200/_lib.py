@@ -23,7 +23,7 @@ EXPORTED = [
     "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
     "whirgpu_commit", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_mle_evaluate",
     "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
-    "whirgpu_set_timing", "whirgpu_kernel_stats",
+    "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
 ]
 
 
@@ -86,6 +86,10 @@ def load() -> ctypes.CDLL:
     L.whirgpu_host_free.argtypes = [p]
     L.whirgpu_set_timing.argtypes = [p, i32]
     L.whirgpu_kernel_stats.argtypes = [p, p, p, i32]
+    L.whirgpu_launch_count.argtypes = []
+    L.whirgpu_launch_count.restype = u64
+    L.whirgpu_last_io_bytes.argtypes = [p, ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.whirgpu_last_io_bytes.restype = None
     for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
                  "whirgpu_proof_get", "whirgpu_commit", "whirgpu_prove", "whirgpu_mle_evaluate",
                  "whirgpu_set_timing", "whirgpu_kernel_stats"):

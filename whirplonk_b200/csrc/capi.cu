@@ -5,6 +5,7 @@
 // every failure to a status code plus a message (no exceptions cross the ABI).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -186,6 +187,7 @@ struct whirgpu_ctx {
     std::unique_ptr<EventTimer> timer;
     uint64_t stat_launches[FAM_COUNT] = {};
     double stat_ms[FAM_COUNT] = {};
+    uint64_t io_h2d = 0, io_d2h = 0;
 };
 
 struct whirgpu_transcript {
@@ -381,6 +383,8 @@ whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, cons
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(ws->dev + p.off_ds, tx->ds.data(), tx->ds.size(), cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) { ws->busy = false; return cuda_fail(c, e, "input copy"); }
+    c->io_h2d = (where == WHIRGPU_INPUT_DEVICE ? 0 : (8ull << n)) + tx->ds.size();
+    c->io_d2h = 0;
     if (enqueue_commit(p, ws->dev, (uint32_t)tx->ds.size(), c->tw, c->stream, c->timer.get()) != 0) {
         ws->busy = false;
         return fail(c, WHIRGPU_E_INVALID, "commit launch failed");
@@ -423,6 +427,7 @@ whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t*
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(&sc->forms_eval[0], evaluations, num_points * 24, cudaMemcpyHostToDevice, c->stream);
         if (e != cudaSuccess) return cuda_fail(c, e, "statement upload");
+        c->io_h2d += num_points * p.n * 24 + num_points * 24;
     }
     if (enqueue_prove(p, ws, c->tw, c->stream, c->timer.get()) != 0) return fail(c, WHIRGPU_E_INVALID, "prove launch failed");
     e = cudaGetLastError();
@@ -445,6 +450,8 @@ whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t*
     WG_CUDA(c, cudaMemcpyAsync(hrlc, &sc->crlc[0], std::max<size_t>(num_points, 1) * 24, cudaMemcpyDeviceToHost, c->stream),
             "read-back");
     WG_CUDA(c, cudaStreamSynchronize(c->stream), "prove");
+    c->io_d2h += sizeof(TxState) + p.narg_len + p.hints_cap + p.total_sumcheck_rounds * 24 +
+                 std::max<size_t>(num_points, 1) * 24;
     if (c->timer) {
         c->timer->harvest();
     }
@@ -558,9 +565,20 @@ whirgpu_status whirgpu_kernel_stats(whirgpu_ctx* c, uint64_t launches[WHIRGPU_NU
     return WHIRGPU_OK;
 }
 
+uint64_t whirgpu_launch_count(void) { return launch_count(); }
+
+void whirgpu_last_io_bytes(const whirgpu_ctx* c, uint64_t* h2d, uint64_t* d2h) {
+    if (h2d) *h2d = c ? c->io_h2d : 0;
+    if (d2h) *d2h = c ? c->io_d2h : 0;
+}
+
 }  // extern "C"
 
 namespace wg {
+static std::atomic<u64> g_launches{0};
+void count_launches(u64 k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+u64 launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 void host_twiddles(u64* stage, u64* hi, u64* lo) {
     const u64 w11 = gl_pow_host(7, (GL_P - 1) >> TW_STAGE_LOG);
     u64 acc = 1;

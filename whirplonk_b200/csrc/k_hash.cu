@@ -65,6 +65,7 @@ int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cu
     if (ncomp == 1) k_leaves<1><<<grid, 256, 0, st>>>(planes, N, depth, nodes);
     else if (ncomp == 3) k_leaves<3><<<grid, 256, 0, st>>>(planes, N, depth, nodes);
     else return -1;
+    count_launches(1);
     return 0;
 }
 
@@ -126,6 +127,7 @@ int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commi
     u32 level = 0;
     if (logN == 0) {
         k_merkle<<<1, 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1);
+        count_launches(1);
         return 0;
     }
     while (level < logN) {
@@ -133,6 +135,7 @@ int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commi
         const u32 ctas = 1u << (logN - level - levels);
         const int finish = (level + levels == logN) ? 1 : 0;
         k_merkle<<<ctas, 256, 0, st>>>(nodes, logN, level, levels, tx, sc, commit_idx, n_ood, finish);
+        count_launches(1);
         level += levels;
     }
     return 0;
@@ -212,6 +215,7 @@ int launch_ood(const u64* v0, const u64* v1, const u64* v2, bool ext3, u64 size,
     E3* partials = reinterpret_cast<E3*>(scratch);
     unsigned* counter = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(scratch) + (size_t)OOD_GRID * MAX_OOD * sizeof(E3));
     k_ood<<<grid, OOD_THREADS, 0, st>>>(v0, v1, v2, ext3 ? 1 : 0, size, tx, sc, commit_idx, n_ood, partials, counter);
+    count_launches(1);
     return 0;
 }
 

@@ -197,6 +197,7 @@ int launch_lde(const LdeArgs& L, cudaStream_t st) {
         }
         size_t smem = lde_smem_bytes(a.logR, a.logW);
         k_ntt_pass<<<grid, 256, smem, st>>>(a);
+        count_launches(1);
     }
     return 0;
 }

@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(SC_THREADS) k_sumcheck_round(ScKernelArgs a) {
         tx_message_e3(tx, C0);
         tx_message_e3(tx, C2);
         if (a.pow_threshold != ~0ull) {
-            // PoW follows in-stream (k_pow_grind / k_sc_after_pow).
+            // PoW follows in-stream (ordered windows, then k_sc_after_pow).
             tx_squeeze(tx, sc->pow_ch, 32);
             sc->pow_best = ~0ull;
         } else {
@@ -161,9 +161,11 @@ int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
     u64 want = (half + SC_THREADS - 1) / SC_THREADS;
     const unsigned grid = (unsigned)(want > SC_GRID ? SC_GRID : (want < 1 ? 1 : want));
     k_sumcheck_round<<<grid, SC_THREADS, 0, st>>>(a);
+    count_launches(1);
     if (s.pow_threshold != ~0ull) {
         launch_pow_grind_only(s.sc, s.pow_threshold, st);
         k_sc_after_pow<<<1, 32, 0, st>>>(s.tx, s.sc, s.r_slot);
+        count_launches(1);
     }
     return 0;
 }
@@ -183,6 +185,7 @@ int launch_fold(const SumcheckArgs& s, cudaStream_t st) {
     u64 want = (s.size + SC_THREADS - 1) / SC_THREADS;
     const unsigned grid = (unsigned)(want > SC_GRID ? SC_GRID : (want < 1 ? 1 : want));
     k_fold<<<grid, SC_THREADS, 0, st>>>(a);
+    count_launches(1);
     return 0;
 }
 
@@ -265,8 +268,10 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
         return 0;
     }
     k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.sc, tab);
+    count_launches(1);
     u64 want = (S + 255) / 256;
     k_cov_init<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab);
+    count_launches(1);
     return 0;
 }
 
@@ -344,9 +349,11 @@ int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
     const u32 hc = ca_hi_count(a.size);
     E3* tab = reinterpret_cast<E3*>(a.scratch);
     k_cov_acc_tables<<<148, 256, 0, st>>>(a.sc, npts, hc, tab);
+    count_launches(1);
     const u64 nchunks = (a.size + CA_E - 1) / CA_E;
     u64 want = (nchunks + 255) / 256;
     k_cov_accumulate<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab, hc);
+    count_launches(1);
     return 0;
 }
 
@@ -399,10 +406,12 @@ int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch
     E3* tab = reinterpret_cast<E3*>(base + 256 + 592 * sizeof(E3));
     cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
     k_cov_tables<<<148, 256, 0, st>>>(point, logS, 1, 0, nullptr, tab);
+    count_launches(1);
     const u64 S = 1ull << logS;
     u64 want = (S + 255) / 256;
     const unsigned grid = (unsigned)(want > 592 ? 592 : want);
     k_mle_dot<<<grid, 256, 0, st>>>(coeffs, logS, tab, partials, counter, out);
+    count_launches(1);
     return 0;
 }
 

@@ -30,6 +30,7 @@ __global__ void k_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsi
 int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
                    unsigned char* hints, u64 hints_cap, ProofScalars* sc, cudaStream_t st) {
     k_tx_init<<<1, 32, 0, st>>>(tx, ds, ds_len, narg, narg_cap, hints, hints_cap, sc);
+    count_launches(1);
     return 0;
 }
 
@@ -57,19 +58,26 @@ __global__ void k_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int
 int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood, cudaStream_t st) {
     if (n_forms > MAX_FORMS || n_ood > MAX_OOD) return -1;
     k_constraint_rlc<<<1, 32, 0, st>>>(tx, sc, n_forms, n_ood);
+    count_launches(1);
     return 0;
 }
 
 // ---------------------------------------------------------------------------
 // Proof of work (proof_of_work.hpp:95-193, 236-257): the smallest nonce n >= 0
 // with LE_u64(BLAKE3(challenge || n_le || 0^24)[0..8]) <= threshold.
-// Every thread walks n = g, g + T, g + 2T, ... and stops once n exceeds the
-// best nonce found so far, so every nonce below the final minimum has been
-// tested: the result is the reference's minimum, independent of scheduling.
+//
+// The nonce space is scanned in ordered windows [base, base + count), one
+// kernel launch per window.  A window is scanned completely (a thread only
+// skips nonces above an already published hit), so the smallest hit of the
+// first window that has one is the global minimum -- the reference's answer,
+// whatever the warp scheduling.  Later windows see the published result at
+// launch and return at once.  Window sizes grow geometrically from the
+// expected search length 2^64 / threshold until 64x that length has been
+// covered (miss probability e^-64), capped at POW_NONCE_LIMIT; running out
+// sets TX_ERR_POW_EXHAUSTED.
 // ---------------------------------------------------------------------------
-// Search bound: 2^36 nonces (~1.5 s of grinding).  A 20-bit threshold fails to
-// hit within it with probability e^(-2^16); exhaustion sets TX_ERR_POW_EXHAUSTED.
 constexpr u64 POW_NONCE_LIMIT = 1ull << 36;
+constexpr unsigned POW_GRID = 148 * 6, POW_THREADS = 256;
 
 __global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
     if (threadIdx.x != 0) return;
@@ -77,7 +85,9 @@ __global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
     sc->pow_best = ~0ull;
 }
 
-__global__ void __launch_bounds__(256) k_pow_grind(ProofScalars* sc, u64 threshold) {
+__global__ void __launch_bounds__(POW_THREADS) k_pow_window(ProofScalars* sc, u64 threshold, u64 base, u64 count) {
+    const u64* best = &sc->pow_best;
+    if (__ldcg(best) != ~0ull) return;  // an earlier window already holds the minimum
     __shared__ unsigned ch[8];
     if (threadIdx.x < 8) {
         const unsigned char* c = sc->pow_ch + 4 * threadIdx.x;
@@ -90,20 +100,37 @@ __global__ void __launch_bounds__(256) k_pow_grind(ProofScalars* sc, u64 thresho
 #pragma unroll
     for (int k = 10; k < 16; ++k) m[k] = 0;
     const u64 T = (u64)gridDim.x * blockDim.x;
-    volatile u64* best = &sc->pow_best;
-    for (u64 n = (u64)blockIdx.x * blockDim.x + threadIdx.x; n < POW_NONCE_LIMIT; n += T) {
-        const u64 cur = *best;
-        if (n > cur) break;
+    for (u64 off = (u64)blockIdx.x * blockDim.x + threadIdx.x; off < count; off += T) {
+        const u64 n = base + off;
+        if (n > __ldcg(best)) break;  // only nonces above a published hit are skipped
         m[8] = (unsigned)n;
         m[9] = (unsigned)(n >> 32);
         unsigned h[8];
         b3_hash64(m, h);
         const u64 v = (u64)h[0] | ((u64)h[1] << 32);
         if (v <= threshold) {
-            atomicMin(reinterpret_cast<unsigned long long*>(&sc->pow_best), n);
+            atomicMin(reinterpret_cast<unsigned long long*>(&sc->pow_best), (unsigned long long)n);
             break;
         }
     }
+}
+
+// Launches the ordered windows for one PoW search (challenge already squeezed).
+int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st) {
+    const double expect = threshold == 0 ? 1.8446744073709552e19 : 18446744073709551616.0 / (double)threshold;
+    u64 cover = expect * 64.0 >= (double)POW_NONCE_LIMIT ? POW_NONCE_LIMIT : (u64)(expect * 64.0) + 1;
+    u64 win = expect < (double)(1u << 18) ? (1ull << 18) : (u64)expect;
+    const u64 max_win = 1ull << 27;
+    if (win > max_win) win = max_win;
+    u64 base = 0;
+    while (base < cover) {
+        const u64 cnt = win < cover - base ? win : cover - base;
+        k_pow_window<<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, base, cnt);
+        count_launches(1);
+        base += cnt;
+        if (win < max_win) win <<= 1;
+    }
+    return 0;
 }
 
 __global__ void k_pow_finish(TxState* tx, ProofScalars* sc, int slot) {
@@ -114,16 +141,13 @@ __global__ void k_pow_finish(TxState* tx, ProofScalars* sc, int slot) {
     tx_message_u64(tx, n);
 }
 
-int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st) {
-    k_pow_grind<<<148 * 8, 256, 0, st>>>(sc, threshold);
-    return 0;
-}
-
 int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, cudaStream_t st) {
     if (threshold == ~0ull) return 0;  // zero difficulty: nothing sent (proof_of_work.hpp:241)
     k_pow_challenge<<<1, 32, 0, st>>>(tx, sc);
-    k_pow_grind<<<148 * 8, 256, 0, st>>>(sc, threshold);
+    count_launches(1);
+    launch_pow_grind_only(sc, threshold, st);
     k_pow_finish<<<1, 32, 0, st>>>(tx, sc, slot);
+    count_launches(1);
     return 0;
 }
 
@@ -135,6 +159,7 @@ __global__ void k_send_vector(TxState* tx, const u64* c0, const u64* c1, const u
 
 int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size, cudaStream_t st) {
     k_send_vector<<<1, 32, 0, st>>>(tx, c0, c1, c2, size);
+    count_launches(1);
     return 0;
 }
 
@@ -325,6 +350,7 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
 int launch_open(const OpenArgs& a, cudaStream_t st) {
     if (a.q > (u32)MAX_QUERIES || a.depth > (u32)MAX_DEPTH) return -1;
     k_open<<<1, OPEN_THREADS, 0, st>>>(a);
+    count_launches(1);
     return 0;
 }
 
@@ -347,6 +373,7 @@ __global__ void k_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_
 int launch_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int q, cudaStream_t st) {
     if (n_ood > MAX_OOD || q > MAX_QUERIES) return -1;
     k_stir_rlc<<<1, 32, 0, st>>>(tx, sc, commit_idx, n_ood, q);
+    count_launches(1);
     return 0;
 }
 

@@ -152,6 +152,10 @@ namespace wg {
 int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch, u64* out, cudaStream_t st);
 size_t mle_eval_scratch_bytes(u32 logS);
 
+// Process-wide count of kernel launches issued by the launchers.
+void count_launches(u64 k);
+u64 launch_count();
+
 // Kernel-family timing hooks used by the schedule (null timer = off).
 enum Family { FAM_NTT = 0, FAM_LEAF, FAM_MERKLE, FAM_OOD, FAM_SUMCHECK, FAM_COV, FAM_POW, FAM_OPEN, FAM_TX, FAM_COUNT };
 struct Timer {

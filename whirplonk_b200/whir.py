@@ -112,6 +112,15 @@ class Context:
         _lib.check(self._L.whirgpu_kernel_stats(self.handle, launches, ms, int(reset)), self.handle)
         return {name: (int(launches[i]), float(ms[i])) for i, name in enumerate(_lib.FAMILY_NAMES)}
 
+    def last_io_bytes(self):
+        h2d, d2h = ctypes.c_uint64(), ctypes.c_uint64()
+        self._L.whirgpu_last_io_bytes(self.handle, ctypes.byref(h2d), ctypes.byref(d2h))
+        return int(h2d.value), int(d2h.value)
+
+    @staticmethod
+    def launch_count() -> int:
+        return int(_lib.load().whirgpu_launch_count())
+
     def mle_evaluate(self, coeffs, point, on_device_ptr: Optional[int] = None):
         """MultilinearExtension::evaluate of base coefficients at an Ext3 point."""
         point = np.ascontiguousarray(point, dtype=np.uint64).reshape(-1)
