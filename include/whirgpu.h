@@ -30,7 +30,8 @@ typedef enum {
     WHIRGPU_E_OOM = 3,         /* device or pinned memory exhausted, or above the HBM budget */
     WHIRGPU_E_CUDA = 4,        /* CUDA runtime error (text in whirgpu_last_error) */
     WHIRGPU_E_DEVICE = 5,      /* a kernel reported an error word (overflow, PoW exhausted) */
-    WHIRGPU_E_TIMEOUT = 6      /* a bounded device wait expired */
+    WHIRGPU_E_TIMEOUT = 6,     /* a bounded device wait expired */
+    WHIRGPU_E_TOO_LARGE = 7    /* size above the fixed capacity of an allocation-free entry point */
 } whirgpu_status;
 
 /* Byte-for-byte the fields of whir::ProtocolParameters
@@ -113,6 +114,24 @@ void whirgpu_last_io_bytes(const whirgpu_ctx* ctx, uint64_t* h2d, uint64_t* d2h)
  * (MultilinearExtension::evaluate, linear_form.hpp:119-126), on the device. */
 whirgpu_status whirgpu_mle_evaluate(whirgpu_ctx* ctx, const uint64_t* coeffs, uint64_t num_variables,
                                     int coeffs_location, const uint64_t* point, uint64_t out[3]);
+/* Allocation-free variant of whirgpu_mle_evaluate.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc where they need the
+ * value (host callbacks and driver hooks, callers whose device memory comes
+ * from their own pool or arena, latency-critical loops): it allocates nothing
+ * and needs no context.  Inputs and output are device buffers the caller owns:
+ * d_coeffs (2^num_variables words), d_point (num_variables Ext3 coordinates,
+ * 3 words each), d_out (3 words); the work is queued on `stream`
+ * (a cudaStream_t, NULL = legacy stream) of the current device and the call
+ * returns without waiting.  Working memory is a fixed file-scope device array
+ * of under 0.5 MiB, held on every GPU that loads the library until the process
+ * exits; num_variables above WHIRGPU_NOALLOC_MLE_MAX_VARS is rejected with
+ * WHIRGPU_E_TOO_LARGE.  The first call on each device looks the array up
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All
+ * calls on a device share the array: calls whose kernels overlap on the GPU
+ * race and give wrong results, so order them on one stream. */
+#define WHIRGPU_NOALLOC_MLE_MAX_VARS 24
+whirgpu_status whirgpu_mle_evaluate_noalloc(const uint64_t* d_coeffs, uint64_t num_variables, const uint64_t* d_point,
+                                            uint64_t* d_out, void* stream);
 /* Seeded uniform Goldilocks words: ChaCha20 block function (RFC 8439),
  * key = seed as 8 LE bytes then 24 zero bytes, nonce 0, counter from 0;
  * each 64-bit LE keystream word below p is taken, others are skipped. */

@@ -12,8 +12,10 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libwhirgpu.so")
 
-OK, E_INVALID, E_UNSUPPORTED, E_OOM, E_CUDA, E_DEVICE, E_TIMEOUT = range(7)
-STATUS_NAMES = {0: "OK", 1: "E_INVALID", 2: "E_UNSUPPORTED", 3: "E_OOM", 4: "E_CUDA", 5: "E_DEVICE", 6: "E_TIMEOUT"}
+OK, E_INVALID, E_UNSUPPORTED, E_OOM, E_CUDA, E_DEVICE, E_TIMEOUT, E_TOO_LARGE = range(8)
+STATUS_NAMES = {0: "OK", 1: "E_INVALID", 2: "E_UNSUPPORTED", 3: "E_OOM", 4: "E_CUDA", 5: "E_DEVICE", 6: "E_TIMEOUT",
+                7: "E_TOO_LARGE"}
+NOALLOC_MLE_MAX_VARS = 24
 NUM_FAMILIES = 9
 FAMILY_NAMES = ["ntt", "leaf_hash", "merkle", "ood", "sumcheck", "covector", "pow", "opening", "transcript"]
 
@@ -21,7 +23,7 @@ FAMILY_NAMES = ["ntt", "leaf_hash", "merkle", "ood", "sumcheck", "covector", "po
 EXPORTED = [
     "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_schedule",
     "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
-    "whirgpu_commit", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_mle_evaluate",
+    "whirgpu_commit", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
     "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
     "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
 ]
@@ -77,6 +79,7 @@ def load() -> ctypes.CDLL:
     L.whirgpu_witness_destroy.argtypes = [p]
     L.whirgpu_prove.argtypes = [p, p, p, sz, p, p, p, p]
     L.whirgpu_mle_evaluate.argtypes = [p, p, u64, i32, p, p]
+    L.whirgpu_mle_evaluate_noalloc.argtypes = [p, u64, p, p, p]
     L.whirgpu_sample_goldilocks.argtypes = [u64, p, sz]
     L.whirgpu_sample_goldilocks.restype = None
     L.whirgpu_chacha20_block.argtypes = [p, ctypes.c_uint32, p, p]
@@ -92,6 +95,7 @@ def load() -> ctypes.CDLL:
     L.whirgpu_last_io_bytes.restype = None
     for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
                  "whirgpu_proof_get", "whirgpu_commit", "whirgpu_prove", "whirgpu_mle_evaluate",
+                 "whirgpu_mle_evaluate_noalloc",
                  "whirgpu_set_timing", "whirgpu_kernel_stats"):
         getattr(L, name).restype = i32
     _lib = L
