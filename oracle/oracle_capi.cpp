@@ -37,6 +37,14 @@ void oracle_shake128(const u8* d, size_t n, u8* out, size_t m) { shake128(d, n, 
 void oracle_keccak_f1600(u64* s) { keccak_f1600(s); }
 
 u64 oracle_fmul(u64 a, u64 b) { return fmul(a, b); }
+u64 oracle_fadd(u64 a, u64 b) { return fadd(a, b); }
+u64 oracle_fsub(u64 a, u64 b) { return fsub(a, b); }
+u64 oracle_fpow(u64 a, u64 e) { return fpow(a, e); }
+size_t oracle_indices(const u8* ent, u64 N, u64 count, int dedup, u64* out) {
+    auto v = indices_from_entropy(ent, N, count, dedup != 0);
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i];
+    return v.size();
+}
 u64 oracle_root_of_unity(u64 n) { return root_of_unity(n); }
 void oracle_e3_mul(const u64* a, const u64* b, u64* out) {
     E3 x, y;

@@ -77,6 +77,44 @@ def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1
         return read_output(out, npts)
 
 
+class OracleTranscript:
+    """The oracle's SHAKE128 prover transcript (absorb / message / squeeze)."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        self.h = lib.oracle_tx_new()
+
+    def __del__(self):
+        if self.h:
+            self.lib.oracle_tx_free(self.h)
+            self.h = None
+
+    def absorb(self, data: bytes):
+        self.lib.oracle_tx_absorb(self.h, data, len(data))
+
+    def message(self, data: bytes):
+        self.lib.oracle_tx_message(self.h, data, len(data))
+
+    def squeeze(self, n: int) -> bytes:
+        b = ctypes.create_string_buffer(n)
+        self.lib.oracle_tx_squeeze(self.h, b, n)
+        return b.raw
+
+    def challenge_base(self) -> int:
+        return int(self.lib.oracle_tx_challenge_base(self.h))
+
+    def challenge_e3(self) -> list:
+        o = (ctypes.c_uint64 * 3)()
+        self.lib.oracle_tx_challenge_e3(self.h, o)
+        return list(o)
+
+    def narg(self) -> bytes:
+        n = self.lib.oracle_tx_narg(self.h, None, 0)
+        b = ctypes.create_string_buffer(max(n, 1))
+        self.lib.oracle_tx_narg(self.h, b, n)
+        return b.raw[:n]
+
+
 class Oracle:
     """ctypes view of oracle/liboracle.so (the CPU restatement)."""
 
@@ -88,6 +126,11 @@ class Oracle:
         L.oracle_sha3_512.argtypes = [p, sz, p]
         L.oracle_shake128.argtypes = [p, sz, p, sz]
         L.oracle_fmul.argtypes = [u64, u64]; L.oracle_fmul.restype = u64
+        for nm in ("oracle_fadd", "oracle_fsub", "oracle_fpow"):
+            getattr(L, nm).argtypes = [u64, u64]
+            getattr(L, nm).restype = u64
+        L.oracle_indices.argtypes = [p, u64, u64, ctypes.c_int, p]
+        L.oracle_indices.restype = sz
         L.oracle_root_of_unity.argtypes = [u64]; L.oracle_root_of_unity.restype = u64
         L.oracle_e3_mul.argtypes = [p, p, p]
         L.oracle_ntt.argtypes = [p, sz]
@@ -116,6 +159,21 @@ class Oracle:
         out = ctypes.create_string_buffer(32)
         self.lib.oracle_blake3(data, len(data), out)
         return out.raw
+
+    def indices(self, entropy: bytes, N: int, count: int, dedup: bool) -> list:
+        out = (ctypes.c_uint64 * max(count, 1))()
+        k = self.lib.oracle_indices(bytes(entropy), N, count, int(dedup), out)
+        return list(out[:k])
+
+    def e3_mul(self, a, b) -> list:
+        x = (ctypes.c_uint64 * 3)(*a)
+        y = (ctypes.c_uint64 * 3)(*b)
+        o = (ctypes.c_uint64 * 3)()
+        self.lib.oracle_e3_mul(x, y, o)
+        return list(o)
+
+    def tx(self):
+        return OracleTranscript(self.lib)
 
     def ntt(self, v) -> np.ndarray:
         a = np.ascontiguousarray(v, dtype=np.uint64).copy()

@@ -752,20 +752,33 @@ inline Witness commit_e3(Transcript& t, const IrsCfg& c, const std::vector<E3>& 
     }
     return w;
 }
-// challenge_indices.hpp:56-119 (no dedup), byte-wise squeezes, big-endian.
-inline std::vector<u64> challenge_indices(Transcript& t, u64 N, u64 count) {
+// indices_from_entropy (challenge_indices.hpp:56-98): ceil(log2 N / 8) bytes
+// per index, big-endian, mod N; optional sort + dedup.
+inline std::vector<u64> indices_from_entropy(const u8* ent, u64 N, u64 count, bool dedup) {
     if (count == 0) return {};
-    if (N == 1) return std::vector<u64>(count, 0);
+    if (N == 1) return dedup ? std::vector<u64>{0} : std::vector<u64>(count, 0);
     u64 nbytes = (layers_for(N) + 7) / 8;
-    std::vector<u8> ent(count * nbytes);
-    t.squeeze(ent.data(), ent.size());
     std::vector<u64> out;
     for (u64 i = 0; i < count; ++i) {
         u64 acc = 0;
         for (u64 b = 0; b < nbytes; ++b) acc = (acc << 8) | ent[i * nbytes + b];
         out.push_back(acc % N);
     }
+    if (dedup) {
+        std::sort(out.begin(), out.end());
+        out.erase(std::unique(out.begin(), out.end()), out.end());
+    }
     return out;
+}
+// challenge_indices (challenge_indices.hpp:100-119), no dedup on the WHIR path;
+// the bytes come from byte-wise squeezes, which read the XOF sequentially.
+inline std::vector<u64> challenge_indices(Transcript& t, u64 N, u64 count) {
+    if (count == 0) return {};
+    if (N == 1) return std::vector<u64>(count, 0);
+    u64 nbytes = (layers_for(N) + 7) / 8;
+    std::vector<u8> ent(count * nbytes);
+    t.squeeze(ent.data(), ent.size());
+    return indices_from_entropy(ent.data(), N, count, false);
 }
 struct Opening { std::vector<E3> points; std::vector<E3> rows; };  // rows lifted to Ext3
 inline Opening open_witness(Transcript& t, const IrsCfg& c, const Witness& w) {

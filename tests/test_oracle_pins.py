@@ -1,0 +1,141 @@
+"""Pins of the CPU oracle (oracle/liboracle.so) -- no GPU needed.
+
+The oracle is trusted as the parity checker only because it reproduces
+(a) every known-answer vector of the reference's own golden dumps that lies on
+    the WHIR path (tests/golden/reference_goldens.json, extracted from
+    cpp/dump_output/* by tests/golden/make_fixtures.py), and
+(b) whole proofs of the unmodified reference prover on seeded inputs
+    (tests/golden/reference_proofs.json), and, when oracle/_ref is built,
+    fresh proofs of the reference prover run live.
+"""
+import hashlib
+import json
+import os
+import struct
+
+import numpy as np
+import pytest
+
+from oracle.refio import ref_available, run_reference
+from whirplonk_b200 import sample_goldilocks
+
+P = 0xFFFFFFFF00000001
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = json.load(open(os.path.join(HERE, "golden", "reference_goldens.json")))
+PROOFS = json.load(open(os.path.join(HERE, "golden", "reference_proofs.json")))["cases"]
+
+
+def test_fields_base(oracle):
+    L = oracle.lib
+    for case in GOLD["fields"]["base"]:
+        a, b = case["inputs"]
+        ops = case["ops"]
+        assert L.oracle_fadd(a, b) == ops["add"][0]
+        assert L.oracle_fsub(a, b) == ops["sub"][0]
+        assert L.oracle_fsub(0, a) == ops["neg"][0]
+        assert L.oracle_fmul(a, b) == ops["mul"][0]
+        assert L.oracle_fmul(a, a) == ops["sq"][0]
+        assert L.oracle_fpow(a, 10) == ops["pow10"][0]
+        assert L.oracle_fmul(L.oracle_fpow(a, P - 2), a) == 1
+        assert L.oracle_fpow(a, P - 2) == ops["inv"][0]
+
+
+def test_fields_ext3(oracle):
+    for case in GOLD["fields"]["ext3"]:
+        x, y = case["inputs"][:3], case["inputs"][3:]
+        assert oracle.e3_mul(x, y) == case["ops"]["mul"]
+        assert oracle.e3_mul(x, x) == case["ops"]["sq"]
+        assert [(u + v) % P for u, v in zip(x, y)] == case["ops"]["add"]
+
+
+def test_blake3_known_answers(oracle):
+    for case in GOLD["blake3"]:
+        for msg, dig in zip(case["messages"], case["digests"]):
+            assert oracle.blake3(bytes.fromhex(msg)).hex() == dig
+    # empty message (BLAKE3 spec / blake3_engine.hpp:102-107)
+    assert oracle.blake3(b"").hex() == "af1349b9f5f9a1a6a0404dea36dcc9499bcb25c9adc112b7cc9a93cae41f3262"
+
+
+def test_merkle_known_answers(oracle):
+    for case in GOLD["merkle"]:
+        leaves = bytes.fromhex(case["leaves"])
+        assert oracle.merkle_root(leaves).hex() == case["root"]
+        assert [h.hex() for h in oracle.merkle_open(leaves, case["indices"])] == case["hints"]
+
+
+def test_matrix_commit_leaves(oracle):
+    for case in GOLD["matrix_commit"]:
+        for row, leaf in zip(case["rows"], case["leaves"]):
+            assert oracle.blake3(bytes.fromhex(row)).hex() == leaf
+
+
+def test_challenge_indices(oracle):
+    for case in GOLD["indices"]:
+        got = oracle.indices(bytes(case["entropy"]), case["num_leaves"], case["count"], case["dedup"])
+        assert got == case["indices"]
+
+
+def test_pow_known_answer(oracle):
+    g = GOLD["pow"]
+    ch = bytes.fromhex(g["challenge"])
+    assert oracle.find_nonce(ch, g["threshold"]) == g["nonce"]
+    msg = ch + struct.pack("<Q", g["nonce"]) + bytes(24)
+    assert oracle.blake3(msg).hex() == g["hash"]
+
+
+def test_sumcheck_transcript_base_field(oracle):
+    """The reference's base-field sumcheck dump: SHAKE128 duplex, 40-byte challenge
+    decoding, c0/c2 messages and folds (cpp/tests/dump_sumcheck.cpp)."""
+    g = GOLD["sumcheck"]
+    t = oracle.tx()
+    t.absorb(bytes.fromhex(g["protocol_id"]))
+    t.absorb(bytes.fromhex(g["session_id"]))
+    a, b, s = list(g["a"]), list(g["b"]), g["sum"]
+    for rnd in g["rounds"]:
+        h = len(a) // 2
+        c0 = sum(a[i] * b[i] for i in range(h)) % P
+        c2 = sum((a[h + i] - a[i]) * (b[h + i] - b[i]) for i in range(h)) % P
+        assert (c0, c2) == (rnd["c0"], rnd["c2"])
+        t.message(struct.pack("<Q", c0))
+        t.message(struct.pack("<Q", c2))
+        r = t.challenge_base()
+        assert r == rnd["r"]
+        a = [(a[i] + r * (a[h + i] - a[i])) % P for i in range(h)]
+        b = [(b[i] + r * (b[h + i] - b[i])) % P for i in range(h)]
+        c1 = (s - 2 * c0 - c2) % P
+        s = ((c2 * r + c1) * r + c0) % P
+        assert s == rnd["sum"]
+    assert t.narg().hex() == g["narg"]
+
+
+def _case_inputs(case):
+    n = case["n"]
+    coeffs = sample_goldilocks(case["seed"], 1 << n)
+    points = sample_goldilocks(case["seed"] + 5000, case["n_points"] * n * 3).reshape(case["n_points"], n, 3)
+    return coeffs, points
+
+
+@pytest.mark.parametrize("case", PROOFS, ids=lambda c: f"n{c['n']}k{c['k']}r{c['rho']}s{c['security']}p{c['pow_bits']}")
+def test_oracle_proofs_match_reference_fixtures(oracle, case):
+    coeffs, points = _case_inputs(case)
+    evals = np.array(case["evaluations"], dtype=np.uint64)
+    for i in range(case["n_points"]):
+        assert [int(x) for x in oracle.mle_eval_base(coeffs, points[i])] == case["evaluations"][i]
+    narg, hints = oracle.prove(case["n"], case["k"], case["rho"], case["security"], case["pow_bits"], points, coeffs,
+                               evals)
+    assert (len(narg), len(hints)) == (case["narg_len"], case["hints_len"])
+    assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
+    if "narg" in case:
+        assert narg.hex() == case["narg"] and hints.hex() == case["hints"]
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("n,k,rho,sec,pb,seed", [(6, 2, 1, 90, 12, 901), (11, 4, 2, 100, 20, 902), (15, 3, 1, 100, 18, 903)])
+def test_oracle_matches_live_reference(oracle, n, k, rho, sec, pb, seed):
+    coeffs = sample_goldilocks(seed, 1 << n)
+    points = sample_goldilocks(seed + 1, n * 3).reshape(1, n, 3)
+    ref = run_reference(n, k, rho, sec, pb, points, coeffs, verify=True)
+    assert ref.verify_ok == 1.0
+    narg, hints = oracle.prove(n, k, rho, sec, pb, points, coeffs, ref.evaluations)
+    assert narg == ref.narg and hints == ref.hints
