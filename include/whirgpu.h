@@ -132,6 +132,10 @@ whirgpu_status whirgpu_mle_evaluate(whirgpu_ctx* ctx, const uint64_t* coeffs, ui
 #define WHIRGPU_NOALLOC_MLE_MAX_VARS 24
 whirgpu_status whirgpu_mle_evaluate_noalloc(const uint64_t* d_coeffs, uint64_t num_variables, const uint64_t* d_point,
                                             uint64_t* d_out, void* stream);
+/* Diagnostics: runs the device field arithmetic on n host operand pairs
+ * (op 0: a+b, 1: a-b, 2: a*b in Goldilocks; 3: a*b in Ext3, three words per
+ * element) and copies the results back.  Operands must be canonical. */
+whirgpu_status whirgpu_debug_field_ops(const uint64_t* a, const uint64_t* b, uint64_t* out, uint64_t n, int op);
 /* Seeded uniform Goldilocks words: ChaCha20 block function (RFC 8439),
  * key = seed as 8 LE bytes then 24 zero bytes, nonce 0, counter from 0;
  * each 64-bit LE keystream word below p is taken, others are skipped. */

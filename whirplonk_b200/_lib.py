@@ -24,7 +24,7 @@ EXPORTED = [
     "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_schedule",
     "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
     "whirgpu_commit", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
-    "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
+    "whirgpu_debug_field_ops", "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
     "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
 ]
 
@@ -80,6 +80,7 @@ def load() -> ctypes.CDLL:
     L.whirgpu_prove.argtypes = [p, p, p, sz, p, p, p, p]
     L.whirgpu_mle_evaluate.argtypes = [p, p, u64, i32, p, p]
     L.whirgpu_mle_evaluate_noalloc.argtypes = [p, u64, p, p, p]
+    L.whirgpu_debug_field_ops.argtypes = [p, p, p, u64, i32]
     L.whirgpu_sample_goldilocks.argtypes = [u64, p, sz]
     L.whirgpu_sample_goldilocks.restype = None
     L.whirgpu_chacha20_block.argtypes = [p, ctypes.c_uint32, p, p]
@@ -95,7 +96,7 @@ def load() -> ctypes.CDLL:
     L.whirgpu_last_io_bytes.restype = None
     for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
                  "whirgpu_proof_get", "whirgpu_commit", "whirgpu_prove", "whirgpu_mle_evaluate",
-                 "whirgpu_mle_evaluate_noalloc",
+                 "whirgpu_mle_evaluate_noalloc", "whirgpu_debug_field_ops",
                  "whirgpu_set_timing", "whirgpu_kernel_stats"):
         getattr(L, name).restype = i32
     _lib = L

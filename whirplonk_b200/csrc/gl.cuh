@@ -19,13 +19,14 @@ typedef unsigned int u32;
 constexpr u64 GL_P = 0xFFFFFFFF00000001ull;
 constexpr u64 GL_EPS = 0xFFFFFFFFull;  // 2^64 mod p
 
-__host__ __device__ __forceinline__ u64 gl_add(u64 a, u64 b) {
+// Host forms (also the device fallback for the reference formulas).
+__host__ __device__ __forceinline__ u64 gl_add_ref(u64 a, u64 b) {
     u64 s = a + b;
     if (s < a) s += GL_EPS;  // cannot overflow again: s + EPS < p when a, b < p
     if (s >= GL_P) s -= GL_P;
     return s;
 }
-__host__ __device__ __forceinline__ u64 gl_sub(u64 a, u64 b) {
+__host__ __device__ __forceinline__ u64 gl_sub_ref(u64 a, u64 b) {
     u64 d = a - b;
     if (a < b) d += GL_P;  // wraps back into [0, p)
     return d;
@@ -42,7 +43,92 @@ __host__ __device__ __forceinline__ u64 gl_reduce(u64 lo, u64 hi) {
     if (s >= GL_P) s -= GL_P;
     return s;
 }
-__device__ __forceinline__ u64 gl_mul(u64 a, u64 b) { return gl_reduce(a * b, __umul64hi(a, b)); }
+
+// Device forms on 32-bit carry chains.  A borrow or carry out of the top limb is
+// worth 2^64 == EPS (mod p).  After a subtract chain `subc.u32 m, 0, 0` turns
+// the borrow into the mask m = 0 or 0xFFFFFFFF = EPS; after an add chain the
+// carry is read with `addc` and negated.  The mask is then added or subtracted.
+
+// a + b for canonical a, b: d = a - (p - b); a borrow means a + b < p, and the
+// wrapped difference is then corrected by -EPS (== +p - 2^64).
+__device__ __forceinline__ u64 gl_add(u64 a, u64 b) {
+    unsigned d0, d1;
+    asm("{\n\t.reg .u32 n0, n1, m;\n\t"
+        "sub.cc.u32 n0, 1, %4;\n\t"          // n = p - b  (p = 0xFFFFFFFF:00000001)
+        "subc.u32 n1, 0xFFFFFFFF, %5;\n\t"
+        "sub.cc.u32 %0, %2, n0;\n\t"         // d = a - n
+        "subc.cc.u32 %1, %3, n1;\n\t"
+        "subc.u32 m, 0, 0;\n\t"              // m = borrow ? EPS : 0
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(d0), "=&r"(d1)
+        : "r"((unsigned)a), "r"((unsigned)(a >> 32)), "r"((unsigned)b), "r"((unsigned)(b >> 32)));
+    return ((u64)d1 << 32) | d0;
+}
+// a - b for canonical a, b; on borrow subtract EPS (== add p - 2^64).
+__device__ __forceinline__ u64 gl_sub(u64 a, u64 b) {
+    unsigned d0, d1;
+    asm("{\n\t.reg .u32 m;\n\t"
+        "sub.cc.u32 %0, %2, %4;\n\t"
+        "subc.cc.u32 %1, %3, %5;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(d0), "=&r"(d1)
+        : "r"((unsigned)a), "r"((unsigned)(a >> 32)), "r"((unsigned)b), "r"((unsigned)(b >> 32)));
+    return ((u64)d1 << 32) | d0;
+}
+// (hi 2^64 + lo) mod p, canonical, for any 64-bit lo, hi:
+//   x == lo - hh + hl * (2^32 - 1)   with hi = hh 2^32 + hl.
+__device__ __forceinline__ u64 gl_reduce_dev(u64 lo, u64 hi) {
+    unsigned r0, r1;
+    asm("{\n\t.reg .u32 r2, r3, m;\n\t"
+        "mov.b64 {%0, %1}, %2;\n\t"
+        "mov.b64 {r2, r3}, %3;\n\t"
+        // t = lo - hh ; on borrow subtract EPS
+        "sub.cc.u32 %0, %0, r3;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 %0, %0, m;\n\t"
+        "subc.u32 %1, %1, 0;\n\t"
+        // u = hl * 2^32 - hl  ->  (r3 : m)
+        "sub.cc.u32 m, 0, r2;\n\t"
+        "subc.u32 r3, r2, 0;\n\t"
+        // s = t + u ; on carry add EPS.  The carry of an add chain is read with
+        // addc (subc's borrow-in is only defined after a subtract chain).
+        "add.cc.u32 %0, %0, m;\n\t"
+        "addc.cc.u32 %1, %1, r3;\n\t"
+        "addc.u32 m, 0, 0;\n\t"
+        "sub.u32 m, 0, m;\n\t"
+        "add.cc.u32 %0, %0, m;\n\t"
+        "addc.u32 %1, %1, 0;\n\t"
+        // canonical: s >= p  <=>  s + EPS carries out; then keep s + EPS (mod 2^64)
+        "add.cc.u32 r2, %0, 0xFFFFFFFF;\n\t"
+        "addc.cc.u32 r3, %1, 0;\n\t"
+        "addc.u32 m, 0, 0;\n\t"
+        "sub.u32 m, 0, m;\n\t"
+        "add.cc.u32 %0, %0, m;\n\t"
+        "addc.u32 %1, %1, 0;\n\t}"
+        : "=&r"(r0), "=&r"(r1)
+        : "l"(lo), "l"(hi));
+    return ((u64)r1 << 32) | r0;
+}
+// (a * b) mod p, canonical output for any 64-bit a, b.
+__device__ __forceinline__ u64 gl_mul(u64 a, u64 b) {
+    unsigned r0, r1, r2, r3;
+    asm("mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "addc.u32 %3, %3, 0;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"((unsigned)a), "r"((unsigned)(a >> 32)), "r"((unsigned)b), "r"((unsigned)(b >> 32)));
+    return gl_reduce_dev(((u64)r1 << 32) | r0, ((u64)r3 << 32) | r2);
+}
 __host__ __forceinline__ u64 gl_mul_host(u64 a, u64 b) {
     unsigned __int128 x = (unsigned __int128)a * b;
     return gl_reduce((u64)x, (u64)(x >> 64));
@@ -72,18 +158,57 @@ struct E3 {
 __host__ __device__ __forceinline__ E3 e3_zero() { return E3{0, 0, 0}; }
 __host__ __device__ __forceinline__ E3 e3_one() { return E3{1, 0, 0}; }
 __host__ __device__ __forceinline__ E3 e3_base(u64 a) { return E3{a, 0, 0}; }
-__host__ __device__ __forceinline__ E3 e3_add(E3 a, E3 b) { return E3{gl_add(a.c0, b.c0), gl_add(a.c1, b.c1), gl_add(a.c2, b.c2)}; }
-__host__ __device__ __forceinline__ E3 e3_sub(E3 a, E3 b) { return E3{gl_sub(a.c0, b.c0), gl_sub(a.c1, b.c1), gl_sub(a.c2, b.c2)}; }
+__device__ __forceinline__ E3 e3_add(E3 a, E3 b) { return E3{gl_add(a.c0, b.c0), gl_add(a.c1, b.c1), gl_add(a.c2, b.c2)}; }
+__device__ __forceinline__ E3 e3_sub(E3 a, E3 b) { return E3{gl_sub(a.c0, b.c0), gl_sub(a.c1, b.c1), gl_sub(a.c2, b.c2)}; }
 __host__ __device__ __forceinline__ bool e3_eq(E3 a, E3 b) { return a.c0 == b.c0 && a.c1 == b.c1 && a.c2 == b.c2; }
+// 192-bit accumulator for sums of 64x64 products (delayed reduction).
+struct Acc192 {
+    u64 w0, w1, w2;
+};
+__device__ __forceinline__ void acc_mul(Acc192& x, u64 a, u64 b) {
+    asm("{\n\t.reg .u64 l, h;\n\t"
+        "mul.lo.u64 l, %3, %4;\n\t"
+        "mul.hi.u64 h, %3, %4;\n\t"
+        "add.cc.u64 %0, %0, l;\n\t"
+        "addc.cc.u64 %1, %1, h;\n\t"
+        "addc.u64 %2, %2, 0;\n\t}"
+        : "+l"(x.w0), "+l"(x.w1), "+l"(x.w2)
+        : "l"(a), "l"(b));
+}
+__device__ __forceinline__ Acc192 acc_product(u64 a, u64 b) {
+    Acc192 x;
+    asm("mul.lo.u64 %0, %2, %3;\n\t"
+        "mul.hi.u64 %1, %2, %3;"
+        : "=l"(x.w0), "=l"(x.w1)
+        : "l"(a), "l"(b));
+    x.w2 = 0;
+    return x;
+}
+__device__ __forceinline__ void acc_double(Acc192& x) {
+    x.w2 = (x.w2 << 1) | (x.w1 >> 63);
+    x.w1 = (x.w1 << 1) | (x.w0 >> 63);
+    x.w0 <<= 1;
+}
+// x mod p for x = w0 + w1 2^64 + w2 2^128 with w2 < 2^32:
+// 2^64 == EPS and 2^128 == -2^32 (mod p); w2 2^32 < p is already canonical.
+__device__ __forceinline__ u64 acc_reduce(const Acc192& x) {
+    return gl_sub(gl_reduce_dev(x.w0, x.w1), x.w2 << 32);
+}
+
 __device__ __forceinline__ E3 e3_mul(E3 a, E3 b) {
     // X^3 = 2:  c0 = a0b0 + 2(a1b2 + a2b1), c1 = a0b1 + a1b0 + 2 a2b2, c2 = a0b2 + a1b1 + a2b0
-    u64 t12 = gl_add(gl_mul(a.c1, b.c2), gl_mul(a.c2, b.c1));
-    u64 t22 = gl_mul(a.c2, b.c2);
-    E3 r;
-    r.c0 = gl_add(gl_mul(a.c0, b.c0), gl_add(t12, t12));
-    r.c1 = gl_add(gl_add(gl_mul(a.c0, b.c1), gl_mul(a.c1, b.c0)), gl_add(t22, t22));
-    r.c2 = gl_add(gl_add(gl_mul(a.c0, b.c2), gl_mul(a.c1, b.c1)), gl_mul(a.c2, b.c0));
-    return r;
+    Acc192 s0 = acc_product(a.c1, b.c2);
+    acc_mul(s0, a.c2, b.c1);
+    acc_double(s0);
+    acc_mul(s0, a.c0, b.c0);
+    Acc192 s1 = acc_product(a.c2, b.c2);
+    acc_double(s1);
+    acc_mul(s1, a.c0, b.c1);
+    acc_mul(s1, a.c1, b.c0);
+    Acc192 s2 = acc_product(a.c0, b.c2);
+    acc_mul(s2, a.c1, b.c1);
+    acc_mul(s2, a.c2, b.c0);
+    return E3{acc_reduce(s0), acc_reduce(s1), acc_reduce(s2)};
 }
 __device__ __forceinline__ E3 e3_mul_base(E3 a, u64 b) { return E3{gl_mul(a.c0, b), gl_mul(a.c1, b), gl_mul(a.c2, b)}; }
 __device__ __forceinline__ E3 e3_pow(E3 b, u64 e) {

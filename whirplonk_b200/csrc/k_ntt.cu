@@ -15,6 +15,8 @@
 // *compact* message (the zero padding is never materialised, so an expansion-e
 // LDE reads m = N/e words per plane), the last pass writes the codeword planes
 // M[plane][i] that the leaf hasher and the opener read.
+#include <algorithm>
+
 #include "launch.h"
 #include "gl.cuh"
 
@@ -22,22 +24,67 @@ namespace wg {
 
 __device__ __forceinline__ u32 bitrev(u32 j, u32 bits) { return bits ? (__brev(j) >> (32 - bits)) : 0; }
 
+// Shared-memory word of column element e: one pad word every 32 words keeps
+// strided group accesses off a single bank.
+__device__ __forceinline__ u32 pidx(u32 e) { return e + (e >> 5); }
+__host__ __device__ __forceinline__ u32 col_stride(u32 logR) { return (1u << logR) + ((1u << logR) >> 5); }
+
+// Stages s0+1 .. s0+RR of a radix-2 DIT on W bit-reversed columns of 2^L
+// words, done as independent radix-2^RR groups in registers: a group is the
+// 2^RR elements base + j 2^s0 (j < 2^RR) of one column, and the butterflies of
+// stage s pair j with j + 2^(t-1) (t = s - s0) under the twiddle
+// w_{2^s}^(lo + (j mod 2^(t-1)) 2^s0), lo = base mod 2^s0.
+template <int RR>
+__device__ __forceinline__ void dit_group_pass(u64* sm, u32 W, u32 L, u32 s0, const u64* tws) {
+    constexpr int G = 1 << RR;
+    const u32 gpc_log = L - RR;  // groups per column (log2)
+    const u32 total = W << gpc_log;
+    const u32 cs = col_stride(L);
+    for (u32 g = threadIdx.x; g < total; g += blockDim.x) {
+        const u32 w = g >> gpc_log;
+        const u32 gb = g & ((1u << gpc_log) - 1);
+        const u32 lo = gb & ((1u << s0) - 1);
+        const u32 base = lo + ((gb >> s0) << (s0 + RR));
+        u64* col = sm + w * cs;
+        u64 x[G];
+#pragma unroll
+        for (int j = 0; j < G; ++j) x[j] = col[pidx(base + ((u32)j << s0))];
+#pragma unroll
+        for (int t = 1; t <= RR; ++t) {
+            const int half = 1 << (t - 1);
+            const u32 sh = L - (s0 + t);
+#pragma unroll
+            for (int j = 0; j < G; ++j) {
+                if (j & half) continue;
+                const u64 tw = tws[(lo + ((u32)(j & (half - 1)) << s0)) << sh];
+                const u64 u = x[j], v = gl_mul(x[j + half], tw);
+                x[j] = gl_add(u, v);
+                x[j + half] = gl_sub(u, v);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < G; ++j) col[pidx(base + ((u32)j << s0))] = x[j];
+    }
+}
+
 // w_{2^logM}^e via the two-level table of w_{2^TW_LOG} powers.
 __device__ __forceinline__ u64 twiddle(u64 e, u32 logM, const u64* hi, const u64* lo) {
     u64 E = (e & ((1ull << logM) - 1)) << (TW_LOG - logM);
     return gl_mul(hi[E >> TW_HALF], lo[E & ((1ull << TW_HALF) - 1)]);
 }
 
-__global__ void __launch_bounds__(256) k_ntt_pass(NttPassArgs a) {
+__global__ void __launch_bounds__(256, 2) k_ntt_pass(NttPassArgs a) {
     extern __shared__ u64 sm[];
     const u32 logR = a.logR, R = 1u << logR, W = 1u << a.logW, halfR = R >> 1;
     const u32 tileN = W << logR;
-    u64* tws = sm + tileN;
+    const u32 cs = col_stride(logR);
+    u64* tws = sm + W * cs;
     const u32 plane = blockIdx.y;
     const u64 N = 1ull << a.logN;
     const bool first = a.pass == 0, last = a.pass + 1 == a.npass;
     const u32 comp = plane / a.depth, blk = plane % a.depth;
-    const u64* src = first ? a.src[comp] + (u64)blk * a.m : nullptr;
+    const u64* src0 = comp == 0 ? a.src[0] : (comp == 1 ? a.src[1] : a.src[2]);  // no dynamic param indexing
+    const u64* src = first ? src0 + (u64)blk * a.m : nullptr;
     u64* tmp = a.tmp + (u64)plane * N;
 
     for (u32 u = threadIdx.x; u < halfR; u += blockDim.x) tws[u] = a.tw_stage[u << (TW_STAGE_LOG - logR)];
@@ -59,9 +106,16 @@ __global__ void __launch_bounds__(256) k_ntt_pass(NttPassArgs a) {
         i0base = (u64)(blockIdx.x % groups) << a.logW;
     }
 
-    // Load (bit-reversed within each column).
+    // Load (bit-reversed within each column).  Only the first R >> logE rows of
+    // a column can be nonzero (zero padding of the message); in bit-reversed
+    // order they land on multiples of E, and the first logE DIT stages would
+    // merely copy each of them over its block of E words -- done here as a
+    // broadcast, the butterflies then start at stage logE.
+    const u32 logE = a.logE, E = 1u << logE;
+    const u32 mrows_log = logR - logE;
     if (!last) {
-        for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
+        const u32 n = W << mrows_log;
+        for (u32 e = threadIdx.x; e < n; e += blockDim.x) {
             const u32 w = e & (W - 1), j = e >> a.logW;
             u64 v;
             if (first) {
@@ -70,11 +124,12 @@ __global__ void __launch_bounds__(256) k_ntt_pass(NttPassArgs a) {
             } else {
                 v = tmp[(P * R + j) * S + col0 + w];
             }
-            sm[(w << logR) + bitrev(j, logR)] = v;
+            sm[w * cs + pidx(bitrev(j, logR))] = v;
         }
     } else {
-        for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
-            const u32 w = e >> logR, j = e & (R - 1);
+        const u32 n = W << mrows_log;
+        for (u32 e = threadIdx.x; e < n; e += blockDim.x) {
+            const u32 w = e >> mrows_log, j = e & ((1u << mrows_log) - 1);
             u64 v;
             if (first) {
                 v = j < a.m ? src[j] : 0;
@@ -83,24 +138,27 @@ __global__ void __launch_bounds__(256) k_ntt_pass(NttPassArgs a) {
                 const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + i1;
                 v = tmp[(row << logR) + j];
             }
-            sm[(w << logR) + bitrev(j, logR)] = v;
+            sm[w * cs + pidx(bitrev(j, logR))] = v;
         }
     }
     __syncthreads();
-
-    // Radix-2 decimation-in-time stages, natural-order output.
-    for (u32 s = 1; s <= logR; ++s) {
-        const u32 half = 1u << (s - 1);
-        for (u32 b = threadIdx.x; b < (tileN >> 1); b += blockDim.x) {
-            const u32 w = b >> (logR - 1), bb = b & (halfR - 1);
-            const u32 k = bb & (half - 1), g = bb >> (s - 1);
-            const u32 x0 = (g << s) + k, x1 = x0 + half;
-            u64* col = sm + (w << logR);
-            const u64 t = tws[k << (logR - s)];
-            const u64 u = col[x0], v = gl_mul(col[x1], t);
-            col[x0] = gl_add(u, v);
-            col[x1] = gl_sub(u, v);
+    if (logE) {
+        for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
+            const u32 w = e >> logR, p = e & (R - 1);
+            if (p & (E - 1)) sm[w * cs + pidx(p)] = sm[w * cs + pidx(p & ~(E - 1))];
         }
+        __syncthreads();
+    }
+
+    // Decimation-in-time stages in register groups of up to 16, natural-order output.
+    for (u32 s0 = logE; s0 < logR;) {
+        const u32 left = logR - s0;
+        const u32 rr = left >= 8 ? 4 : (left > 4 ? (left + 1) / 2 : left);
+        if (rr == 4) dit_group_pass<4>(sm, W, logR, s0, tws);
+        else if (rr == 3) dit_group_pass<3>(sm, W, logR, s0, tws);
+        else if (rr == 2) dit_group_pass<2>(sm, W, logR, s0, tws);
+        else dit_group_pass<1>(sm, W, logR, s0, tws);
+        s0 += rr;
         __syncthreads();
     }
 
@@ -110,7 +168,7 @@ __global__ void __launch_bounds__(256) k_ntt_pass(NttPassArgs a) {
         for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
             const u32 w = e & (W - 1), i = e >> a.logW;
             const u64 col = col0 + w;
-            u64 v = sm[(w << logR) + i];
+            u64 v = sm[w * cs + pidx(i)];
             v = gl_mul(v, twiddle(col * i, logNs, a.tw_hi, a.tw_lo));
             tmp[(P * R + i) * S + col] = v;
         }
@@ -120,7 +178,7 @@ __global__ void __launch_bounds__(256) k_ntt_pass(NttPassArgs a) {
         const u64 obase = a.npass == 3 ? i0base + ((u64)i1 << a.logR0) : i0base;
         for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
             const u32 w = e & (W - 1), i = e >> a.logW;
-            out[obase + w + outer * i] = sm[(w << logR) + i];
+            out[obase + w + outer * i] = sm[w * cs + pidx(i)];
         }
     }
 }
@@ -157,7 +215,9 @@ LdePlan plan_lde(u32 logN) {
     return p;
 }
 
-size_t lde_smem_bytes(u32 logR, u32 logW) { return ((size_t)(1u << logW) << logR) * 8 + ((size_t)1 << logR) / 2 * 8 + 16; }
+size_t lde_smem_bytes(u32 logR, u32 logW) {
+    return ((size_t)(1u << logW) * col_stride(logR)) * 8 + ((size_t)1 << logR) / 2 * 8 + 16;
+}
 
 int launch_lde(const LdeArgs& L, cudaStream_t st) {
     const LdePlan pl = plan_lde(L.logN);
@@ -194,6 +254,18 @@ int launch_lde(const LdeArgs& L, cudaStream_t st) {
             u64 groups = (1ull << pl.logR[0]) >> a.logW;
             if (pl.npass == 3) groups <<= pl.logR[1];
             grid = dim3((unsigned)groups, L.planes);
+        }
+        // Nonzero rows of this pass: the input index is (..., j_s, rest) with
+        // rest < S_s; the data can be nonzero only where the index is below
+        // min(m, S_{s-1}) (pass 0: below m).
+        {
+            const u64 bound = s == 0 ? L.m : std::min<u64>(L.m, 1ull << (logrest + a.logR));
+            const u64 S_s = 1ull << a.logS;
+            u64 rows = (bound + S_s - 1) / S_s;
+            if (rows < 1) rows = 1;
+            u32 lr = 0;
+            while ((1ull << lr) < rows) ++lr;
+            a.logE = a.logR > lr ? a.logR - lr : 0;
         }
         size_t smem = lde_smem_bytes(a.logR, a.logW);
         k_ntt_pass<<<grid, 256, smem, st>>>(a);

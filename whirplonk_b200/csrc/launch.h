@@ -26,7 +26,7 @@ struct NttPassArgs {
     u64 m;
     u64* tmp;
     u64* out;
-    u32 depth, logN, logR, logS, logW, npass, pass, logR0, logR1;
+    u32 depth, logN, logR, logS, logW, npass, pass, logR0, logR1, logE;
     const u64* tw_stage;
     const u64* tw_hi;
     const u64* tw_lo;
