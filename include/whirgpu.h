@@ -73,6 +73,10 @@ void* whirgpu_stream(whirgpu_ctx* ctx);
  * Returns the number of words (0 on invalid parameters). */
 size_t whirgpu_schedule(const whirgpu_params* params, uint64_t num_variables, uint64_t* out, size_t cap);
 
+/* Device workspace bytes one proof of this shape occupies (0 when invalid):
+ * what HBM-budget admission counts. */
+uint64_t whirgpu_workspace_bytes(const whirgpu_params* params, uint64_t num_variables);
+
 /* Domain separator of the reference CLI (cpp/main.cpp:174-215):
  * out[0..64) = SHA3-512(CBOR(params)), out[64..96) = SHA3-256(CBOR(session)). */
 whirgpu_status whirgpu_cli_domain_separator(const whirgpu_params* params, uint8_t out[96]);
@@ -108,6 +112,59 @@ whirgpu_status whirgpu_prove(whirgpu_ctx* ctx, whirgpu_witness* witness, const u
 
 /* Bytes the last commit + prove pair moved host->device and device->host. */
 void whirgpu_last_io_bytes(const whirgpu_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
+
+/* ---- many proofs at once --------------------------------------------------------
+ * A request is one complete commit + prove (with its own domain separator).
+ * Proofs are independent: the bytes of each are the same alone or in a batch. */
+typedef struct {
+    uint64_t num_variables;
+    whirgpu_params params;
+    const uint64_t* coeffs;      /* 2^num_variables canonical words */
+    int coeffs_location;         /* WHIRGPU_INPUT_HOST / WHIRGPU_INPUT_DEVICE */
+    const uint64_t* points;      /* num_points * num_variables Ext3 coordinates */
+    const uint64_t* evaluations; /* num_points Ext3 values */
+    uint64_t num_points;
+    uint8_t protocol_id[64];
+    uint8_t session_id[32];
+} whirgpu_request;
+
+typedef struct whirgpu_batch whirgpu_batch;
+/* mode 0: the whole batch captured into one CUDA graph (one branch per proof,
+ *         launched with a single cudaGraphLaunch per run);
+ * mode 1: the same schedule issued stream by stream without a graph;
+ * mode 2: plain -- one proof at a time, each waited for before the next.
+ * Inputs are read again at every run (host inputs through pinned staging). */
+whirgpu_status whirgpu_batch_create(whirgpu_ctx* ctx, const whirgpu_request* reqs, size_t count, int mode,
+                                    whirgpu_batch** out);
+whirgpu_status whirgpu_batch_run(whirgpu_batch* b);
+whirgpu_status whirgpu_batch_proof(const whirgpu_batch* b, size_t i, const uint8_t** narg, size_t* narg_len,
+                                   const uint8_t** hints, size_t* hints_len);
+void whirgpu_batch_destroy(whirgpu_batch* b);
+
+/* Serving: a worker thread admits submitted requests (copied at submit) as
+ * HBM budget and one of max_inflight streams free up -- continuous batching:
+ * requests arriving while others run join them on the device.  Each
+ * workspace keeps a captured CUDA graph of its proof program.  While a server
+ * runs it owns the context.  poll waits up to timeout_ms (WHIRGPU_E_TIMEOUT
+ * if not done); result pointers stay valid until whirgpu_server_release. */
+typedef struct whirgpu_server whirgpu_server;
+typedef struct {
+    whirgpu_status status;
+    const uint8_t* narg;
+    size_t narg_len;
+    const uint8_t* hints;
+    size_t hints_len;
+    double queue_ms; /* submit -> admission */
+    double total_ms; /* submit -> proof complete */
+} whirgpu_result;
+whirgpu_status whirgpu_server_create(whirgpu_ctx* ctx, uint64_t hbm_budget, uint32_t max_inflight,
+                                     whirgpu_server** out);
+whirgpu_status whirgpu_server_submit(whirgpu_server* s, const whirgpu_request* req, uint64_t* ticket);
+whirgpu_status whirgpu_server_poll(whirgpu_server* s, uint64_t ticket, uint32_t timeout_ms, whirgpu_result* out);
+void whirgpu_server_release(whirgpu_server* s, uint64_t ticket);
+void whirgpu_server_stats(whirgpu_server* s, uint64_t* admitted, uint64_t* peak_inflight, uint64_t* peak_bytes,
+                          uint64_t* queued);
+void whirgpu_server_destroy(whirgpu_server* s);
 
 /* ---- helpers ------------------------------------------------------------------- */
 /* Multilinear extension of 2^num_variables base coefficients at an Ext3 point

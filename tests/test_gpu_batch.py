@@ -1,0 +1,104 @@
+"""Batches and the serving loop: every proof made in a mix is byte-identical to
+the same proof made alone (and to the oracle), whatever the mode, the
+interleaving and the admission order; HBM-budget admission holds."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from whirplonk_b200 import Context, ProtocolParameters, prove_once, sample_goldilocks
+from whirplonk_b200.batch import Batch, ProofRequest, Server
+
+pytestmark = pytest.mark.gpu
+
+
+def make_requests(ctx, specs, seed0=3000):
+    reqs = []
+    for i, (n, rho) in enumerate(specs):
+        params = ProtocolParameters.cli(log_inv_rate=rho)
+        coeffs = sample_goldilocks(seed0 + i, 1 << n)
+        pts = sample_goldilocks(seed0 + 500 + i, n * 3).reshape(1, n, 3)
+        ev = np.array(ctx.mle_evaluate(coeffs, pts), dtype=np.uint64).reshape(1, 3)
+        reqs.append(ProofRequest(n, params, coeffs, pts, ev))
+    return reqs
+
+
+def alone(ctx, r):
+    narg, hints, _ = prove_once(r.num_variables, r.params, r.coeffs, r.points, r.evaluations, ctx=ctx)
+    return narg, hints
+
+
+SPECS = [(12, 1), (8, 3), (14, 2), (10, 1), (12, 3), (9, 2), (13, 1), (12, 1), (11, 2), (15, 3)]
+
+
+@pytest.mark.parametrize("mode", [Batch.GRAPH, Batch.STREAMS, Batch.PLAIN])
+def test_batch_matches_alone(gpu_ctx, mode):
+    reqs = make_requests(gpu_ctx, SPECS)
+    expected = [alone(gpu_ctx, r) for r in reqs]
+    with Batch(gpu_ctx, reqs, mode) as b:
+        for _ in range(2):  # the same batch program runs again on fresh copies of the inputs
+            b.run()
+            for i, e in enumerate(expected):
+                assert b.proof(i) == e, f"request {i} {SPECS[i]} differs in mode {mode}"
+
+
+def test_batch_matches_oracle(gpu_ctx, oracle):
+    reqs = make_requests(gpu_ctx, [(10, 2), (11, 1)], seed0=4000)
+    with Batch(gpu_ctx, reqs, Batch.GRAPH) as b:
+        b.run()
+        for i, r in enumerate(reqs):
+            rho = r.params.starting_log_inv_rate
+            onarg, ohints = oracle.prove(r.num_variables, 4, rho, 100, 20, r.points, r.coeffs, r.evaluations)
+            assert b.proof(i) == (onarg, ohints)
+
+
+def test_server_mix_matches_alone():
+    ctx = Context(0)
+    try:
+        reqs = make_requests(ctx, SPECS * 2, seed0=5000)
+        expected = [alone(ctx, r) for r in reqs]
+        srv = Server(ctx, hbm_budget=0, max_inflight=6)
+        tickets = []
+        for r in reqs:  # requests keep arriving while earlier ones run
+            tickets.append(srv.submit(r))
+            time.sleep(0.0005)
+        for i, t in enumerate(tickets):
+            res = srv.poll(t, timeout_ms=60_000)
+            assert res is not None and res.status == 0
+            assert (res.narg, res.hints) == expected[i], f"served request {i} differs"
+            assert res.total_ms >= res.queue_ms >= 0
+        st = srv.stats()
+        assert st["admitted"] == len(reqs) and st["peak_inflight"] > 1
+        srv.close()
+    finally:
+        ctx.close()
+
+
+def test_server_hbm_budget_admission():
+    from whirplonk_b200 import _lib
+    from whirplonk_b200.whir import Config
+
+    ctx = Context(0)
+    try:
+        reqs = make_requests(ctx, [(14, 2)] * 4 + [(10, 1)] * 4, seed0=6000)
+        expected = [alone(ctx, r) for r in reqs]
+        big = Config.from_params(1 << 14, reqs[0].params).workspace_bytes()
+        small = Config.from_params(1 << 10, reqs[-1].params).workspace_bytes()
+        assert big > small > 0
+        srv = Server(ctx, hbm_budget=big - 1, max_inflight=8)
+        with pytest.raises(_lib.WhirGpuError):
+            srv.submit(reqs[0])  # a request that can never fit is refused at submit
+        srv.close()
+        budget = big + 2 * small  # one large proof and two small ones at a time
+        srv = Server(ctx, hbm_budget=budget, max_inflight=8)
+        tickets = [srv.submit(r) for r in reqs]
+        for i, t in enumerate(tickets):
+            res = srv.poll(t, timeout_ms=60_000)
+            assert res.status == 0 and (res.narg, res.hints) == expected[i]
+        st = srv.stats()
+        assert st["admitted"] == len(reqs)
+        assert 0 < st["peak_bytes"] <= budget
+        srv.close()
+    finally:
+        ctx.close()

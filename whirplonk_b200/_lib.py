@@ -22,10 +22,14 @@ FAMILY_NAMES = ["ntt", "leaf_hash", "merkle", "ood", "sumcheck", "covector", "po
 # Every symbol include/whirgpu.h declares.
 EXPORTED = [
     "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_schedule",
+    "whirgpu_workspace_bytes",
     "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
     "whirgpu_commit", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
     "whirgpu_debug_field_ops", "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
     "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
+    "whirgpu_batch_create", "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_batch_destroy",
+    "whirgpu_server_create", "whirgpu_server_submit", "whirgpu_server_poll", "whirgpu_server_release",
+    "whirgpu_server_stats", "whirgpu_server_destroy",
 ]
 
 
@@ -41,6 +45,36 @@ class WhirParams(ctypes.Structure):
         ("pow_bits", ctypes.c_uint64),
         ("batch_size", ctypes.c_uint64),
         ("hash_id", ctypes.c_uint8 * 32),
+    ]
+
+
+class Request(ctypes.Structure):
+    """Mirror of whirgpu_request."""
+
+    _fields_ = [
+        ("num_variables", ctypes.c_uint64),
+        ("params", WhirParams),
+        ("coeffs", ctypes.c_void_p),
+        ("coeffs_location", ctypes.c_int),
+        ("points", ctypes.c_void_p),
+        ("evaluations", ctypes.c_void_p),
+        ("num_points", ctypes.c_uint64),
+        ("protocol_id", ctypes.c_uint8 * 64),
+        ("session_id", ctypes.c_uint8 * 32),
+    ]
+
+
+class Result(ctypes.Structure):
+    """Mirror of whirgpu_result."""
+
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("narg", ctypes.c_void_p),
+        ("narg_len", ctypes.c_size_t),
+        ("hints", ctypes.c_void_p),
+        ("hints_len", ctypes.c_size_t),
+        ("queue_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
     ]
 
 
@@ -71,6 +105,8 @@ def load() -> ctypes.CDLL:
     L.whirgpu_stream.restype = p
     L.whirgpu_schedule.argtypes = [ctypes.POINTER(WhirParams), u64, p, sz]
     L.whirgpu_schedule.restype = sz
+    L.whirgpu_workspace_bytes.argtypes = [ctypes.POINTER(WhirParams), u64]
+    L.whirgpu_workspace_bytes.restype = u64
     L.whirgpu_cli_domain_separator.argtypes = [ctypes.POINTER(WhirParams), p]
     L.whirgpu_transcript_create.argtypes = [p, p, p, p, sz, vp]
     L.whirgpu_transcript_destroy.argtypes = [p]
@@ -94,9 +130,26 @@ def load() -> ctypes.CDLL:
     L.whirgpu_launch_count.restype = u64
     L.whirgpu_last_io_bytes.argtypes = [p, ctypes.POINTER(u64), ctypes.POINTER(u64)]
     L.whirgpu_last_io_bytes.restype = None
+    L.whirgpu_batch_create.argtypes = [p, ctypes.POINTER(Request), sz, i32, vp]
+    L.whirgpu_batch_run.argtypes = [p]
+    L.whirgpu_batch_proof.argtypes = [p, sz, vp, ctypes.POINTER(sz), vp, ctypes.POINTER(sz)]
+    L.whirgpu_batch_destroy.argtypes = [p]
+    L.whirgpu_batch_destroy.restype = None
+    L.whirgpu_server_create.argtypes = [p, u64, ctypes.c_uint32, vp]
+    L.whirgpu_server_submit.argtypes = [p, ctypes.POINTER(Request), ctypes.POINTER(u64)]
+    L.whirgpu_server_poll.argtypes = [p, u64, ctypes.c_uint32, ctypes.POINTER(Result)]
+    L.whirgpu_server_release.argtypes = [p, u64]
+    L.whirgpu_server_release.restype = None
+    L.whirgpu_server_stats.argtypes = [p, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64),
+                                       ctypes.POINTER(u64)]
+    L.whirgpu_server_stats.restype = None
+    L.whirgpu_server_destroy.argtypes = [p]
+    L.whirgpu_server_destroy.restype = None
     for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
                  "whirgpu_proof_get", "whirgpu_commit", "whirgpu_prove", "whirgpu_mle_evaluate",
-                 "whirgpu_mle_evaluate_noalloc", "whirgpu_debug_field_ops",
+                 "whirgpu_mle_evaluate_noalloc", "whirgpu_debug_field_ops", "whirgpu_batch_create",
+                 "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_server_create", "whirgpu_server_submit",
+                 "whirgpu_server_poll",
                  "whirgpu_set_timing", "whirgpu_kernel_stats"):
         getattr(L, name).restype = i32
     _lib = L

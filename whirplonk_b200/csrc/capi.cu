@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/whirgpu.h"
+#include "ctx.h"
 #include "launch.h"
 #include "prover.h"
 #include "state.cuh"
@@ -25,10 +26,6 @@
 using namespace wg;
 
 namespace {
-
-constexpr uint8_t BLAKE3_ENGINE_ID[32] = {0x03, 0xe0, 0x17, 0x49, 0xeb, 0xcc, 0x04, 0x77, 0x92, 0x42, 0x54,
-                                          0xeb, 0x48, 0x20, 0x66, 0xb8, 0x64, 0xa8, 0xdd, 0x4d, 0x77, 0x25,
-                                          0x24, 0x64, 0xca, 0x6f, 0x5b, 0x6f, 0x5c, 0xc0, 0x5b, 0x4c};
 
 // ---------------------------------------------------------------------------
 // Host Keccak / SHA3 (FIPS 202) for the domain-separator helper; constants
@@ -109,101 +106,9 @@ void chacha20_words(const uint32_t key[8], uint32_t counter, const uint32_t nonc
     for (int i = 0; i < 16; ++i) out[i] = x[i] + s[i];
 }
 
-ProtocolParams to_params(const whirgpu_params* p) {
-    ProtocolParams q;
-    q.unique_decoding = p->unique_decoding != 0;
-    q.starting_log_inv_rate = p->starting_log_inv_rate;
-    q.initial_folding_factor = p->initial_folding_factor;
-    q.folding_factor = p->folding_factor;
-    q.security_level = p->security_level;
-    q.pow_bits = p->pow_bits;
-    q.batch_size = p->batch_size;
-    return q;
-}
-
-struct EventTimer : Timer {
-    struct Pair { int fam; cudaEvent_t a, b; };
-    std::vector<Pair> pending;
-    std::vector<cudaEvent_t> pool;
-    uint64_t launches[FAM_COUNT] = {};
-    double ms[FAM_COUNT] = {};
-    cudaEvent_t get() {
-        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        return e;
-    }
-    void begin(int fam, cudaStream_t st) override {
-        Pair p{fam, get(), nullptr};
-        cudaEventRecord(p.a, st);
-        pending.push_back(p);
-    }
-    void end(int fam, cudaStream_t st) override {
-        for (auto it = pending.rbegin(); it != pending.rend(); ++it)
-            if (it->fam == fam && it->b == nullptr) {
-                it->b = get();
-                cudaEventRecord(it->b, st);
-                return;
-            }
-    }
-    void harvest() {  // after a stream synchronisation
-        for (auto& p : pending) {
-            if (!p.b) continue;
-            float t = 0;
-            cudaEventElapsedTime(&t, p.a, p.b);
-            ms[p.fam] += t;
-            launches[p.fam] += 1;
-            pool.push_back(p.a);
-            pool.push_back(p.b);
-        }
-        pending.clear();
-    }
-    ~EventTimer() override {
-        for (auto& p : pending) { cudaEventDestroy(p.a); if (p.b) cudaEventDestroy(p.b); }
-        for (auto e : pool) cudaEventDestroy(e);
-    }
-};
-
 }  // namespace
 
-struct Workspace {
-    ProofPlan plan;
-    char* dev = nullptr;
-    bool busy = false;
-};
-
-struct whirgpu_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    uint64_t budget = 0;
-    uint64_t allocated = 0;
-    DeviceTables tw;
-    std::string err;
-    std::map<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t>, std::vector<Workspace*>> cache;
-    uint8_t* pinned = nullptr;
-    size_t pinned_bytes = 0;
-    char* mle_scratch = nullptr;
-    size_t mle_scratch_bytes = 0;
-    std::unique_ptr<EventTimer> timer;
-    uint64_t stat_launches[FAM_COUNT] = {};
-    double stat_ms[FAM_COUNT] = {};
-    uint64_t io_h2d = 0, io_d2h = 0;
-};
-
-struct whirgpu_transcript {
-    whirgpu_ctx* ctx = nullptr;
-    std::vector<uint8_t> ds;  // protocol_id || session_id || instance
-    std::vector<uint8_t> narg, hints;
-    bool complete = false;
-};
-
-struct whirgpu_witness {
-    whirgpu_ctx* ctx = nullptr;
-    Workspace* ws = nullptr;
-    whirgpu_transcript* tx = nullptr;
-};
-
-namespace {
+namespace wg {
 
 whirgpu_status fail(whirgpu_ctx* c, whirgpu_status s, const std::string& msg) {
     if (c) c->err = msg;
@@ -260,7 +165,31 @@ whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_param
 
 bool is_blake3(const whirgpu_params* p) { return std::memcmp(p->hash_id, BLAKE3_ENGINE_ID, 32) == 0; }
 
-}  // namespace
+void release_workspace(Workspace* w) {
+    if (w) w->busy = false;
+}
+
+size_t workspace_bytes(uint64_t n, const whirgpu_params* params) {
+    try {
+        return make_plan((uint32_t)n, to_params(params), MAX_FORMS, 96).total_bytes;
+    } catch (const std::exception&) {
+        return 0;
+    }
+}
+
+ProtocolParams to_params(const whirgpu_params* p) {
+    ProtocolParams q;
+    q.unique_decoding = p->unique_decoding != 0;
+    q.starting_log_inv_rate = p->starting_log_inv_rate;
+    q.initial_folding_factor = p->initial_folding_factor;
+    q.folding_factor = p->folding_factor;
+    q.security_level = p->security_level;
+    q.pow_bits = p->pow_bits;
+    q.batch_size = p->batch_size;
+    return q;
+}
+
+}  // namespace wg
 
 extern "C" {
 
@@ -320,6 +249,10 @@ size_t whirgpu_schedule(const whirgpu_params* params, uint64_t n, uint64_t* out,
     } catch (const std::exception&) {
         return 0;
     }
+}
+
+uint64_t whirgpu_workspace_bytes(const whirgpu_params* params, uint64_t n) {
+    return params ? workspace_bytes(n, params) : 0;
 }
 
 whirgpu_status whirgpu_cli_domain_separator(const whirgpu_params* p, uint8_t out[96]) {

@@ -1,0 +1,120 @@
+// ctx.h -- internal state behind the C ABI handles, shared by capi.cu
+// (single proofs) and batch.cu (batches and the serving loop).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/whirgpu.h"
+#include "launch.h"
+#include "prover.h"
+
+namespace wg {
+
+constexpr uint8_t BLAKE3_ENGINE_ID[32] = {0x03, 0xe0, 0x17, 0x49, 0xeb, 0xcc, 0x04, 0x77, 0x92, 0x42, 0x54,
+                                          0xeb, 0x48, 0x20, 0x66, 0xb8, 0x64, 0xa8, 0xdd, 0x4d, 0x77, 0x25,
+                                          0x24, 0x64, 0xca, 0x6f, 0x5b, 0x6f, 0x5c, 0xc0, 0x5b, 0x4c};
+
+struct EventTimer : Timer {
+    struct Pair { int fam; cudaEvent_t a, b; };
+    std::vector<Pair> pending;
+    std::vector<cudaEvent_t> pool;
+    uint64_t launches[FAM_COUNT] = {};
+    double ms[FAM_COUNT] = {};
+    cudaEvent_t get() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void begin(int fam, cudaStream_t st) override {
+        Pair p{fam, get(), nullptr};
+        cudaEventRecord(p.a, st);
+        pending.push_back(p);
+    }
+    void end(int fam, cudaStream_t st) override {
+        for (auto it = pending.rbegin(); it != pending.rend(); ++it)
+            if (it->fam == fam && it->b == nullptr) {
+                it->b = get();
+                cudaEventRecord(it->b, st);
+                return;
+            }
+    }
+    void harvest() {  // after a stream synchronisation
+        for (auto& p : pending) {
+            if (!p.b) continue;
+            float t = 0;
+            cudaEventElapsedTime(&t, p.a, p.b);
+            ms[p.fam] += t;
+            launches[p.fam] += 1;
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    ~EventTimer() override {
+        for (auto& p : pending) { cudaEventDestroy(p.a); if (p.b) cudaEventDestroy(p.b); }
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+
+
+struct Workspace {
+    ProofPlan plan;
+    char* dev = nullptr;
+    bool busy = false;
+};
+
+}  // namespace wg
+
+struct whirgpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    uint64_t allocated = 0;
+    wg::DeviceTables tw;
+    std::string err;
+    std::map<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t>, std::vector<wg::Workspace*>>
+        cache;
+    uint8_t* pinned = nullptr;
+    size_t pinned_bytes = 0;
+    char* mle_scratch = nullptr;
+    size_t mle_scratch_bytes = 0;
+    std::unique_ptr<wg::EventTimer> timer;
+    uint64_t stat_launches[wg::FAM_COUNT] = {};
+    double stat_ms[wg::FAM_COUNT] = {};
+    uint64_t io_h2d = 0, io_d2h = 0;
+};
+
+struct whirgpu_transcript {
+    whirgpu_ctx* ctx = nullptr;
+    std::vector<uint8_t> ds;  // protocol_id || session_id || instance
+    std::vector<uint8_t> narg, hints;
+    bool complete = false;
+};
+
+struct whirgpu_witness {
+    whirgpu_ctx* ctx = nullptr;
+    wg::Workspace* ws = nullptr;
+    whirgpu_transcript* tx = nullptr;
+};
+
+namespace wg {
+ProtocolParams to_params(const whirgpu_params* p);
+whirgpu_status fail(whirgpu_ctx* c, whirgpu_status s, const std::string& msg);
+whirgpu_status cuda_fail(whirgpu_ctx* c, cudaError_t e, const char* what);
+whirgpu_status ensure_pinned(whirgpu_ctx* c, size_t bytes);
+// A free workspace for (n, params, ds_len), allocated on first use and kept in
+// the context cache; marked busy until release_workspace.
+whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out);
+void release_workspace(Workspace* w);
+bool is_blake3(const whirgpu_params* p);
+// Plan size of one proof (bytes of device workspace), or 0 when invalid.
+size_t workspace_bytes(uint64_t n, const whirgpu_params* params);
+}  // namespace wg

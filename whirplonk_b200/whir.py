@@ -233,6 +233,11 @@ class Config:
             raise ValueError("invalid protocol parameters")
         return cls(size, params, list(out[:cnt]))
 
+    def workspace_bytes(self) -> int:
+        """Device memory one proof of this shape occupies (HBM-budget unit)."""
+        c = self.params.to_c()
+        return int(_lib.load().whirgpu_workspace_bytes(ctypes.byref(c), self.num_variables))
+
     @property
     def num_variables(self) -> int:
         return self.size.bit_length() - 1
