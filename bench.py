@@ -1,19 +1,30 @@
 #!/usr/bin/env python3
 """Benchmark of the B200 WHIR prover (one JSON line on rank 0).
 
-Workload (default): the plain WHIR commit + prove of config 3 -- one
-multilinear polynomial of 2^24 Goldilocks coefficients (seeded ChaCha20,
-uniform in [0, p)), folding factor 4, starting rate 1/4, 100-bit security,
-20 PoW bits, BLAKE3, one MLE statement at a seeded random Ext3 point, the
-reference CLI domain separator.  One step = one complete proof.
+Workloads (all: folding factor 4, 100-bit security, 20 PoW bits, BLAKE3,
+Goldilocks with Ext3 challenges, one MLE statement at a seeded Ext3 point, the
+reference CLI domain separator, coefficients uniform in [0, p) from a seeded
+ChaCha20 keystream):
 
-  value  : proofs/s with the coefficients already resident in HBM
-  e2e    : proofs/s through the public API with the coefficients in pinned
-           host memory (H2D copy and proof read-back inside every step)
-  p50/p99: per-proof latency of the device-resident steps
-The working set of a step (~3.4 GB) is far above the 126 MB L2, so no flush is
-needed between steps.  Multi-GPU: independent replicas (one proof stream per
-rank, no collective on the data path), weak scaling.
+  whir_served_mixed_n12_24 (default): a seeded stream of prove requests with
+      num_variables uniform on [12, 24] (the size log-uniform on 2^12..2^24,
+      rounded) and log_inv_rate uniform on {1, 2, 3}, served by the
+      continuous-batching server (HBM-budget admission, captured per-proof
+      programs, overlapping proofs).  A step = 32 requests.
+        value : served proofs/s at saturation, coefficients resident in HBM
+        e2e   : the same through the public API from pinned host buffers
+        p50/p99 : latency (submit -> result) under Poisson arrivals at 80% of
+                  the saturated rate, beside the plain path's under the same
+                  arrivals; plain = one proof at a time through the public
+                  single-proof API on the same requests
+  whir_batch64_n14_22: 64 proofs, num_variables uniform on {14..22},
+      log_inv_rate on {1, 2, 3}, in one captured CUDA graph.  A step = one run
+      of the batch.
+  whir_prove_n24_rate4 / _n22_rate4 / _n18_rate2: one plain proof per step.
+
+Every batched or served proof is checked byte-for-byte against the plain
+path's proof of the same request.  Multi-GPU: independent replicas (each rank
+its own stream of requests, no collective on the data path), weak scaling.
 
 --impl reference times the reference C++ CPU prover (oracle/_ref/ref_driver,
 built from the reference sources) on the same workload with all host threads.
@@ -23,6 +34,7 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -36,14 +48,20 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 METRIC = "proofs/s & p50/p99 latency, mixed 2^12–2^24 batched vs plain GPU; 2^24 prove ms"
+FOLD, SEC, POW = 4, 100, 20
 WORKLOADS = {
-    # name: (num_variables, folding, log_inv_rate, security, pow_bits)
-    "whir_prove_n24_rate4": (24, 4, 2, 100, 20),
-    "whir_prove_n22_rate4": (22, 4, 2, 100, 20),
-    "whir_prove_n18_rate2": (18, 4, 1, 100, 20),
+    "whir_served_mixed_n12_24": {"kind": "served", "n": (12, 24), "dist": "log-uniform", "rho": (1, 2, 3),
+                                 "per_step": 32, "seed": 11},
+    "whir_batch64_n14_22": {"kind": "batch", "n": (14, 22), "dist": "uniform", "rho": (1, 2, 3), "count": 64,
+                            "seed": 7},
+    "whir_prove_n24_rate4": {"kind": "single", "n": 24, "rho": 2},
+    "whir_prove_n22_rate4": {"kind": "single", "n": 22, "rho": 2},
+    "whir_prove_n18_rate2": {"kind": "single", "n": 18, "rho": 1},
 }
-DEFAULT_WORKLOAD = "whir_prove_n24_rate4"
+DEFAULT_WORKLOAD = "whir_served_mixed_n12_24"
 FALLBACK_HBM_GBS = 6650.0
+DATA = "synthetic (seeded ChaCha20 coefficients, seeded Ext3 points)"
+DTYPE = "u64 (Goldilocks; Ext3 challenges)"
 
 
 def env_int(name, default):
@@ -159,8 +177,25 @@ def read_traffic(family):
 
 
 # ---------------------------------------------------------------------------
-# reference CPU prover
+# workload: requests and their inputs
 # ---------------------------------------------------------------------------
+def draw_requests(w, count, seed):
+    """(num_variables, log_inv_rate) pairs drawn from the seeded ChaCha20 stream."""
+    from whirplonk_b200 import sample_goldilocks
+
+    words = sample_goldilocks(seed, 2 * count)
+    lo, hi = w["n"]
+    out = []
+    for i in range(count):
+        a, b = int(words[2 * i]), int(words[2 * i + 1])
+        if w["dist"] == "uniform":
+            n = lo + a % (hi - lo + 1)
+        else:  # size log-uniform on [2^lo, 2^hi]: n uniform on [lo, hi], rounded
+            n = int(math.floor(lo + (hi - lo) * ((a >> 11) / float(1 << 53)) + 0.5))
+        out.append((n, w["rho"][b % len(w["rho"])]))
+    return out
+
+
 def make_inputs(n, seed):
     from whirplonk_b200 import sample_goldilocks
 
@@ -169,44 +204,122 @@ def make_inputs(n, seed):
     return coeffs, point
 
 
-def time_reference(n, k, rho, sec, pb, coeffs, point, reps):
-    from oracle.refio import ref_available, run_reference
+def params_for(rho):
+    from whirplonk_b200 import ProtocolParameters
 
-    if not ref_available():
-        return None
-    threads = os.cpu_count() or 1
-    times = []
-    for _ in range(reps):
-        r = run_reference(n, k, rho, sec, pb, point, coeffs, threads=threads)
-        times.append((r.commit_ms + r.prove_ms) / 1000.0)
-    return times, threads
+    return ProtocolParameters.cli(security_level=SEC, pow_bits=POW, folding_factor=FOLD, log_inv_rate=rho)
+
+
+class Inputs:
+    """One coefficient vector per num_variables (host, pinned host and device
+    copies) and one statement per (num_variables, rate)."""
+
+    def __init__(self, ctx, shapes, rank, device):
+        import torch
+
+        self.ctx = ctx
+        self.host, self.pinned, self.dev, self.pts, self.evs = {}, {}, {}, {}, {}
+        self._pinned_ptrs = []
+        for n in sorted({n for n, _ in shapes}):
+            coeffs, _ = make_inputs(n, 1000 * (rank + 1) + n)
+            self.host[n] = coeffs
+            self.dev[n] = torch.from_numpy(coeffs.view(np.int64)).to(device)
+            ptr = ctx._L.whirgpu_host_alloc(coeffs.nbytes)
+            if not ptr:
+                raise MemoryError("pinned allocation failed")
+            self._pinned_ptrs.append(ptr)
+            view = np.ctypeslib.as_array((ctypes.c_uint64 * coeffs.size).from_address(ptr))
+            view[:] = coeffs
+            self.pinned[n] = view
+        for n, rho in sorted(set(shapes)):
+            _, point = make_inputs(n, 5000 * (rank + 1) + 31 * n + rho)
+            self.pts[(n, rho)] = point
+            self.evs[(n, rho)] = np.array(ctx.mle_evaluate(self.host[n], point), dtype=np.uint64).reshape(1, 3)
+        torch.cuda.synchronize()
+
+    def request(self, n, rho, where):
+        from whirplonk_b200.batch import ProofRequest
+
+        if where == "device":
+            return ProofRequest(n, params_for(rho), self.dev[n].data_ptr(), self.pts[(n, rho)], self.evs[(n, rho)],
+                                on_device=True)
+        return ProofRequest(n, params_for(rho), self.pinned[n], self.pts[(n, rho)], self.evs[(n, rho)])
+
+    def coeff_bytes(self, n):
+        return 8 << n
+
+    def close(self):
+        for p in self._pinned_ptrs:
+            self.ctx._L.whirgpu_host_free(p)
+        self._pinned_ptrs = []
+        self.dev.clear()
+
+
+# ---------------------------------------------------------------------------
+# reference CPU prover
+# ---------------------------------------------------------------------------
+def reference_proof_seconds(n, rho, coeffs, point, threads):
+    from oracle.refio import run_reference
+
+    r = run_reference(n, FOLD, rho, SEC, POW, point, coeffs, threads=threads)
+    return (r.commit_ms + r.prove_ms) / 1000.0
+
+
+def workload_shapes(w, count_steps):
+    if w["kind"] == "single":
+        return [(w["n"], w["rho"])] * count_steps
+    if w["kind"] == "batch":
+        return draw_requests(w, w["count"], w["seed"])
+    return draw_requests(w, w["per_step"] * count_steps, w["seed"])
+
+
+def config_of(name, w, world):
+    cfg = {"workload": name, "folding_factor": FOLD, "security_level": SEC, "pow_bits": POW, "hash": "BLAKE3",
+           "field": "Goldilocks3", "statement": "1 MLE evaluation at a seeded Ext3 point"}
+    if w["kind"] == "single":
+        cfg.update(num_variables=w["n"], log_inv_rate=w["rho"])
+    else:
+        cfg.update(num_variables=f"{w['dist']} on [{w['n'][0]}, {w['n'][1]}]", log_inv_rate=list(w["rho"]),
+                   seed=w["seed"])
+        cfg.update(requests_per_step=w["per_step"] if w["kind"] == "served" else w["count"])
+    cfg["parallelism"] = f"replicas x{world}" if world > 1 else "1 GPU"
+    cfg["l2"] = "working set of a step (GBs of codewords and trees) far above the 126 MB L2; no flush"
+    return cfg
 
 
 def run_reference_arm(args, rank, world):
+    from oracle.refio import ref_available
+
     if rank != 0:
         return 0
-    n, k, rho, sec, pb = WORKLOADS[args.workload]
-    coeffs, point = make_inputs(n, 1)
-    warm = min(args.warmup, 1)
-    res = time_reference(n, k, rho, sec, pb, coeffs, point, warm + args.steps)
-    if res is None:
+    w = WORKLOADS[args.workload]
+    if not ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built"}))
         return 0
-    times, threads = res
+    threads = os.cpu_count() or 1
+    warm = min(args.warmup, 1)
+    # one reference proof per step: the step-th request of the workload's stream
+    shapes = workload_shapes(w, warm + args.steps)
+    inputs = {}
+    times = []
+    for i in range(warm + args.steps):
+        n, rho = shapes[i % len(shapes)]
+        if n not in inputs:
+            inputs[n] = make_inputs(n, 1000 + n)[0]
+        _, point = make_inputs(n, 5000 + 31 * n + rho)
+        times.append(reference_proof_seconds(n, rho, inputs[n], point, threads))
     timed = times[warm:]
     total = sum(timed)
     value = len(timed) / total
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world,
-        "steps": args.steps, "warmup": warm, "ms_per_step": 1000.0 * total / len(timed),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)",
-        "data": "synthetic (seeded ChaCha20 coefficients, seeded Ext3 point)",
-        "config": {"workload": args.workload, "num_variables": n, "folding_factor": k, "log_inv_rate": rho,
-                   "security_level": sec, "pow_bits": pb, "hash": "BLAKE3", "field": "Goldilocks3",
-                   "parallelism": "host OpenMP (reference C++ prover)"},
+        "steps": args.steps, "warmup": warm, "ms_per_step": 1000.0 * total / len(timed), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": DATA,
+        "config": config_of(args.workload, w, world) | {"parallelism": "host OpenMP (reference C++ prover)"},
         "p50_ms": 1000.0 * statistics.median(timed), "p99_ms": 1000.0 * max(timed),
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "reference",
-                         "sample": f"{len(timed)} full proofs of the workload (commit+prove, prover clock)"},
+                         "sample": f"{len(timed)} proofs, one per step: the first requests of the workload's "
+                                   "seeded stream (commit+prove, prover clock)"},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -216,155 +329,386 @@ def run_reference_arm(args, rank, world):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
-def run_gpu_arm(args, rank, world, local_rank):
-    import torch
+class Harness:
+    def __init__(self, rank, world, local_rank):
+        import torch
 
-    from whirplonk_b200 import Context, ProtocolParameters, prove_once
-    from whirplonk_b200.whir import Config
+        self.torch = torch
+        self.dist = None
+        if world > 1:
+            import datetime
 
-    dist = None
-    if world > 1:
-        import datetime
+            import torch.distributed as dist
 
-        import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+        torch.cuda.set_device(local_rank)
+        self.device = f"cuda:{local_rank}"
+        self.rank, self.world, self.local_rank = rank, world, local_rank
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    torch.cuda.set_device(local_rank)
-    n, k, rho, sec, pb = WORKLOADS[args.workload]
-    params = ProtocolParameters.cli(security_level=sec, pow_bits=pb, folding_factor=k, log_inv_rate=rho)
-    ctx = Context(local_rank)
-    coeffs, point = make_inputs(n, 1 + rank)
-    ev = np.array(ctx.mle_evaluate(coeffs, point), dtype=np.uint64).reshape(1, 3)
+    def barrier(self):
+        self.torch.cuda.synchronize()
+        if self.dist is not None:
+            self.dist.barrier()
+        self.torch.cuda.synchronize()
 
-    # device-resident copy of the coefficients (plumbing: torch owns the buffer)
-    dcoeffs = torch.from_numpy(coeffs.view(np.int64)).to(f"cuda:{local_rank}")
-    torch.cuda.synchronize()
-    dptr = dcoeffs.data_ptr()
-    # pinned host copy for the end-to-end path
-    L = ctx._L
-    hbuf = L.whirgpu_host_alloc(coeffs.nbytes)
-    if not hbuf:
-        raise MemoryError("pinned allocation failed")
-    hview = np.ctypeslib.as_array((ctypes.c_uint64 * coeffs.size).from_address(hbuf))
-    hview[:] = coeffs
-
-    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local_rank}")
-
-    def step_device():
-        return prove_once(n, params, None, point, ev, ctx=ctx, on_device_ptr=dptr)
-
-    def step_e2e():
-        return prove_once(n, params, hview, point, ev, ctx=ctx)
-
-    ref_proof = step_device()
-    for _ in range(max(args.warmup, 3) - 1):
-        step_device()
-    for _ in range(2):
-        step_e2e()
-    assert step_e2e()[0] == ref_proof[0], "host and device inputs gave different proofs"
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
+    def max_over_ranks(self, x):
+        if self.dist is None:
             return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- timed region 1: device-resident inputs --------------------------------
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    time.sleep(0.3)
+    def sum_over_ranks(self, x):
+        if self.dist is None:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def timed(self, stream, fn):
+        """Device time (ms) of fn() between two events on `stream`, with the
+        device synchronised on both sides (work on other streams included)."""
+        torch = self.torch
+        self.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        out = fn()
+        torch.cuda.synchronize()
+        b.record(stream)
+        b.synchronize()
+        self.barrier()
+        return self.max_over_ranks(a.elapsed_time(b)), out
+
+    def close(self):
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def plain_prove(ctx, inputs, n, rho, where="device"):
+    from whirplonk_b200 import prove_once
+
+    if where == "device":
+        narg, hints, _ = prove_once(n, params_for(rho), None, inputs.pts[(n, rho)], inputs.evs[(n, rho)], ctx=ctx,
+                                    on_device_ptr=inputs.dev[n].data_ptr())
+    else:
+        narg, hints, _ = prove_once(n, params_for(rho), inputs.pinned[n], inputs.pts[(n, rho)],
+                                    inputs.evs[(n, rho)], ctx=ctx)
+    return narg, hints
+
+
+def family_roofline(ctx, inputs, shapes):
+    """Per-family device time over one plain pass of `shapes` (events on the
+    launching stream) against the algorithmic bytes of the same proofs."""
+    from whirplonk_b200.whir import Config
+
     ctx.set_timing(True)
     ctx.kernel_stats(reset=True)
-    launches0 = ctx.launch_count()
-    barrier()
-    ev_start = torch.cuda.Event(enable_timing=True)
-    ev_end = torch.cuda.Event(enable_timing=True)
-    step_events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                   for _ in range(args.steps)]
-    ev_start.record(stream)
-    for i in range(args.steps):
-        step_events[i][0].record(stream)
-        out = step_device()
-        step_events[i][1].record(stream)
-    ev_end.record(stream)
-    barrier()
-    launches = ctx.launch_count() - launches0
+    alg = {}
+    for n, rho in shapes:
+        plain_prove(ctx, inputs, n, rho)
+        sched = Config.from_params(1 << n, params_for(rho)).schedule
+        for f, v in algorithmic_bytes(sched, n, FOLD).items():
+            alg[f] = alg.get(f, 0) + v
     fam = ctx.kernel_stats(reset=True)
     ctx.set_timing(False)
-    elapsed_ms = max_over_ranks(ev_start.elapsed_time(ev_end))
-    lat = sorted(a.elapsed_time(b) for a, b in step_events)
-    assert out[0] == ref_proof[0]
-
-    # ---- timed region 2: end to end through the public API, host inputs ---------
-    barrier()
-    e_start = torch.cuda.Event(enable_timing=True)
-    e_end = torch.cuda.Event(enable_timing=True)
-    e_start.record(stream)
-    for _ in range(args.steps):
-        out = step_e2e()
-    e_end.record(stream)
-    barrier()
-    h2d, d2h = ctx.last_io_bytes()
-    e2e_ms = max_over_ranks(e_start.elapsed_time(e_end))
-    clk = clocks.stop()
-    assert out[0] == ref_proof[0]
-
-    total_proofs = args.steps * world
-    value = total_proofs / (elapsed_ms / 1000.0)
-    e2e_value = total_proofs / (e2e_ms / 1000.0)
-
-    # roofline of the dominant family (algorithmic bytes / measured family time)
-    sched = Config.from_params(1 << n, params).schedule
-    alg = algorithmic_bytes(sched, n, k)
-    fam_ms = {f: v[1] / args.steps for f, v in fam.items()}
+    fam_ms = {f: v[1] for f, v in fam.items()}
     dominant = max(alg.keys(), key=lambda f: fam_ms.get(f, 0.0))
     peak, peak_kind = read_peaks()
     achieved = alg[dominant] / (fam_ms[dominant] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": read_traffic(dominant), "kernel": dominant, "peak_source": peak_kind,
-                "algorithmic_bytes_per_proof": alg[dominant], "ms_per_proof": fam_ms[dominant]}
+    per = len(shapes)
+    return ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+             "traffic": read_traffic(dominant), "kernel": dominant, "peak_source": peak_kind,
+             "algorithmic_bytes_per_proof": alg[dominant] / per, "ms_per_proof": fam_ms[dominant] / per},
+            {f: round(v / per, 4) for f, v in fam_ms.items()})
 
+
+def cpu_sample(shapes, inputs, budget_s=12.0):
+    """The reference prover on the first requests of the stream until ~budget_s of CPU time."""
+    from oracle.refio import ref_available
+
+    if not ref_available():
+        return None
+    threads = os.cpu_count() or 1
+    total, count = 0.0, 0
+    for n, rho in shapes:
+        total += reference_proof_seconds(n, rho, inputs.host[n], inputs.pts[(n, rho)], threads)
+        count += 1
+        if total >= budget_s:
+            break
+    return {"value": count / total, "unit": "proofs/s", "cores": threads, "kind": "reference",
+            "sample": f"the first {count} requests of the workload's stream, proved by the reference C++ prover "
+                      f"(oracle/_ref) one after another, {total:.1f} s"}
+
+
+def pct(xs, q):
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, int(q * len(xs)))] if xs else None
+
+
+def run_single(args, H, ctx, w):
+    torch = H.torch
+    n, rho = w["n"], w["rho"]
+    inputs = Inputs(ctx, [(n, rho)], H.rank, H.device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=H.device)
+    ref_proof = plain_prove(ctx, inputs, n, rho)
+    for _ in range(max(args.warmup, 3) - 1):
+        plain_prove(ctx, inputs, n, rho)
+    for _ in range(2):
+        assert plain_prove(ctx, inputs, n, rho, "host") == ref_proof, "host and device inputs differ"
+
+    clocks = ClockSampler(H.local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = ctx.launch_count()
+    lat = []
+
+    def device_steps():
+        out = None
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = plain_prove(ctx, inputs, n, rho)
+            b.record(stream)
+            lat.append((a, b))
+        return out
+
+    elapsed, out = H.timed(stream, device_steps)
+    launches = ctx.launch_count() - launches0
+    assert out == ref_proof
+    lat = sorted(a.elapsed_time(b) for a, b in lat)
+
+    def host_steps():
+        o = None
+        for _ in range(args.steps):
+            o = plain_prove(ctx, inputs, n, rho, "host")
+        return o
+
+    e2e_ms, out = H.timed(stream, host_steps)
+    h2d, d2h = ctx.last_io_bytes()
+    clk = clocks.stop()
+    assert out == ref_proof
+    roof, fams = family_roofline(ctx, inputs, [(n, rho)] * args.steps)
+    total = args.steps * H.world
     line = {
-        "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
-        "warmup": max(args.warmup, 3), "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks; Ext3 challenges)",
-        "data": "synthetic (seeded ChaCha20 coefficients, seeded Ext3 point)",
-        "config": {"workload": args.workload, "num_variables": n, "folding_factor": k, "log_inv_rate": rho,
-                   "security_level": sec, "pow_bits": pb, "hash": "BLAKE3", "field": "Goldilocks3",
-                   "parallelism": f"replicas x{world}", "l2": "working set ~3.4 GB per step > 126 MB L2 (no flush)"},
-        "prove_ms": elapsed_ms / args.steps, "p50_ms": lat[len(lat) // 2],
-        "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-        "e2e": {"value": e2e_value, "unit": "proofs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": launches,
-        "roofline": roofline,
-        "families_ms_per_proof": {f: round(v, 4) for f, v in fam_ms.items()},
-        "clocks": clk,
+        "value": total / (elapsed / 1000.0), "ms_per_step": elapsed / args.steps,
+        "prove_ms": elapsed / args.steps, "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+        "e2e": {"value": total / (e2e_ms / 1000.0), "unit": "proofs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches, "roofline": roof, "families_ms_per_proof": fams, "clocks": clk,
     }
-    if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        res = time_reference(n, k, rho, sec, pb, coeffs, point, 1)
-        if res is not None:
-            times, threads = res
-            line["cpu_baseline"] = {"value": 1.0 / times[0], "unit": "proofs/s", "cores": threads,
-                                    "kind": "reference",
-                                    "sample": "1 full proof of the workload by the reference C++ prover "
-                                              "(oracle/_ref, commit+prove clock)"}
-        else:
-            line["cpu_baseline"] = None
-    L.whirgpu_host_free(hbuf)
-    del dcoeffs
+    if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample([(n, rho)], inputs, budget_s=0.0)
+    inputs.close()
+    return line
+
+
+def run_batch(args, H, ctx, w):
+    from whirplonk_b200.batch import Batch
+
+    torch = H.torch
+    shapes = workload_shapes(w, 1)
+    inputs = Inputs(ctx, shapes, H.rank, H.device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=H.device)
+    # plain path: one proof at a time, device-resident inputs
+    expected = [plain_prove(ctx, inputs, n, rho) for n, rho in shapes]
+    plain_ms, _ = H.timed(stream, lambda: [plain_prove(ctx, inputs, n, rho) for n, rho in shapes])
+    dev_batch = Batch(ctx, [inputs.request(n, rho, "device") for n, rho in shapes], Batch.GRAPH)
+    host_batch = Batch(ctx, [inputs.request(n, rho, "host") for n, rho in shapes], Batch.GRAPH)
+    for _ in range(max(args.warmup, 3)):
+        dev_batch.run()
+    host_batch.run()
+    for i in range(len(shapes)):
+        assert dev_batch.proof(i) == expected[i] and host_batch.proof(i) == expected[i], f"batched proof {i} differs"
+
+    clocks = ClockSampler(H.local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = ctx.launch_count()
+    lat = []
+
+    def steps(b):
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            b.run()
+            lat.append(1000.0 * (time.perf_counter() - t0))
+
+    elapsed, _ = H.timed(stream, lambda: steps(dev_batch))
+    launches = ctx.launch_count() - launches0
+    lat_dev = list(lat)
+    lat.clear()
+
+    def host_steps():
+        steps(host_batch)
+        return [host_batch.proof(i) for i in range(len(shapes))]
+
+    e2e_ms, proofs = H.timed(stream, host_steps)
+    clk = clocks.stop()
+    assert proofs == expected
+    for i in range(len(shapes)):
+        assert dev_batch.proof(i) == expected[i]
+    h2d = sum(inputs.coeff_bytes(n) + 96 + n * 24 + 24 for n, _ in shapes)
+    d2h = sum(len(a) + len(b) for a, b in expected)
+    dev_batch.close()
+    host_batch.close()
+    roof, fams = family_roofline(ctx, inputs, shapes)
+    count = len(shapes)
+    total = count * args.steps * H.world
+    plain_rate = H.sum_over_ranks(count / (plain_ms / 1000.0))
+    line = {
+        "value": total / (elapsed / 1000.0), "ms_per_step": elapsed / args.steps,
+        "p50_ms": pct(lat_dev, 0.5), "p99_ms": pct(lat_dev, 0.99), "latency_note": "per batch run (64 proofs)",
+        "plain_proofs_per_s": plain_rate, "batched_vs_plain": (total / (elapsed / 1000.0)) / plain_rate,
+        "identical_to_plain": True,
+        "e2e": {"value": total / (e2e_ms / 1000.0), "unit": "proofs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches, "roofline": roof, "families_ms_per_proof_plain": fams, "clocks": clk,
+    }
+    if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(shapes, inputs)
+    inputs.close()
+    return line
+
+
+def serve(srv, reqs, arrivals=None):
+    """Submits `reqs` (all at once, or at the given offsets in seconds) and
+    returns the served results in request order."""
+    tickets = []
+    t0 = time.perf_counter()
+    for i, r in enumerate(reqs):
+        if arrivals is not None:
+            wait = t0 + arrivals[i] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+        tickets.append(srv.submit(r))
+    return [srv.poll(t, timeout_ms=300_000) for t in tickets]
+
+
+def run_served(args, H, ctx, w):
+    from whirplonk_b200.batch import Server
+
+    torch = H.torch
+    shapes = workload_shapes(w, args.steps)
+    inputs = Inputs(ctx, shapes, H.rank, H.device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=H.device)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(0.6 * free)
+    max_inflight = 32
+
+    # plain path: one proof at a time through the single-proof API (warm first)
+    for n, rho in sorted(set(shapes)):
+        plain_prove(ctx, inputs, n, rho)
+    plain_lat = []
+
+    def plain_all():
+        out = []
+        for n, rho in shapes:
+            t0 = time.perf_counter()
+            out.append(plain_prove(ctx, inputs, n, rho))
+            plain_lat.append(1000.0 * (time.perf_counter() - t0))
+        return out
+
+    plain_ms, expected = H.timed(stream, plain_all)
+
+    srv = Server(ctx, hbm_budget=budget, max_inflight=max_inflight)
+    dev_reqs = [inputs.request(n, rho, "device") for n, rho in shapes]
+    host_reqs = [inputs.request(n, rho, "host") for n, rho in shapes]
+    for _ in range(max(args.warmup, 3) - 1):  # captures the per-workspace programs
+        serve(srv, dev_reqs)
+    res = serve(srv, host_reqs)
+    for i, r in enumerate(res):
+        assert r.status == 0 and (r.narg, r.hints) == expected[i], f"served request {i} differs from plain"
+
+    clocks = ClockSampler(H.local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = ctx.launch_count()
+    elapsed, res = H.timed(stream, lambda: serve(srv, dev_reqs))
+    launches = ctx.launch_count() - launches0
+    assert all(r.status == 0 and (r.narg, r.hints) == expected[i] for i, r in enumerate(res))
+    e2e_ms, res = H.timed(stream, lambda: serve(srv, host_reqs))
+    clk = clocks.stop()
+    assert all(r.status == 0 and (r.narg, r.hints) == expected[i] for i, r in enumerate(res))
+
+    count = len(shapes)
+    served_rate = count / (elapsed / 1000.0)
+    plain_rate = count / (plain_ms / 1000.0)
+    # latency under seeded Poisson arrivals
+    rng = np.random.Generator(np.random.PCG64(w["seed"] + H.rank))
+    sweep = []
+    for frac in (0.5, 0.8):
+        lam = frac * served_rate
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, count))
+        arrivals -= arrivals[0]
+        res = serve(srv, dev_reqs, arrivals)
+        assert all(r.status == 0 and (r.narg, r.hints) == expected[i] for i, r in enumerate(res))
+        tot = [r.total_ms for r in res]
+        sweep.append({"offered_proofs_per_s": lam, "p50_ms": pct(tot, 0.5), "p99_ms": pct(tot, 0.99),
+                      "mean_queue_ms": statistics.mean(r.queue_ms for r in res)})
+    # the plain path under the same arrivals as the 80% point: one proof at a time, FIFO
+    plain_tot = []
+    t0 = time.perf_counter()
+    for i, (n, rho) in enumerate(shapes):
+        wait = t0 + arrivals[i] - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        plain_prove(ctx, inputs, n, rho)
+        plain_tot.append(1000.0 * (time.perf_counter() - (t0 + arrivals[i])))
+    st = srv.stats()
+    srv.close()
+
+    # the plain path's 2^24 prove time (config 3 shape: n=24, rate 1/4)
+    if (24, 2) not in inputs.pts:
+        _, point = make_inputs(24, 5000 * (H.rank + 1) + 31 * 24 + 2)
+        if 24 not in inputs.host:
+            inputs.host[24], _ = make_inputs(24, 1000 * (H.rank + 1) + 24)
+            inputs.dev[24] = torch.from_numpy(inputs.host[24].view(np.int64)).to(H.device)
+        inputs.pts[(24, 2)] = point
+        inputs.evs[(24, 2)] = np.array(ctx.mle_evaluate(inputs.host[24], point), dtype=np.uint64).reshape(1, 3)
+    plain_prove(ctx, inputs, 24, 2)
+    n24_ms, _ = H.timed(stream, lambda: [plain_prove(ctx, inputs, 24, 2) for _ in range(5)])
+
+    roof, fams = family_roofline(ctx, inputs, shapes[: w["per_step"]])
+    h2d = sum(inputs.coeff_bytes(n) + 96 + n * 24 + 24 for n, _ in shapes) / args.steps
+    d2h = sum(len(a) + len(b) for a, b in expected) / args.steps
+    total_value = H.sum_over_ranks(served_rate)
+    line = {
+        "value": total_value, "ms_per_step": elapsed / args.steps,
+        "p50_ms": sweep[1]["p50_ms"], "p99_ms": sweep[1]["p99_ms"],
+        "latency_note": "submit -> result under seeded Poisson arrivals at 80% of the saturated served rate",
+        "plain_proofs_per_s": H.sum_over_ranks(plain_rate), "served_vs_plain": served_rate / plain_rate,
+        "plain_p50_ms_same_arrivals": pct(plain_tot, 0.5), "plain_p99_ms_same_arrivals": pct(plain_tot, 0.99),
+        "plain_p50_ms_alone": pct(plain_lat, 0.5), "plain_p99_ms_alone": pct(plain_lat, 0.99),
+        "latency_sweep": sweep, "identical_to_plain": True, "prove_ms_n24_rate4": n24_ms / 5,
+        "server": {"hbm_budget_bytes": budget, "max_inflight": max_inflight, "peak_inflight": st["peak_inflight"],
+                   "peak_bytes": st["peak_bytes"]},
+        "e2e": {"value": H.sum_over_ranks(count / (e2e_ms / 1000.0)), "unit": "proofs/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": launches, "roofline": roof, "families_ms_per_proof_plain": fams, "clocks": clk,
+    }
+    if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(shapes, inputs)
+    inputs.close()
+    return line
+
+
+def run_gpu_arm(args, rank, world, local_rank):
+    from whirplonk_b200 import Context
+
+    H = Harness(rank, world, local_rank)
+    w = WORKLOADS[args.workload]
+    ctx = Context(local_rank)
+    body = {"single": run_single, "batch": run_batch, "served": run_served}[w["kind"]](args, H, ctx, w)
+    line = {"metric": METRIC, "value": body.pop("value"), "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": body.pop("ms_per_step"), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": DATA,
+            "config": config_of(args.workload, w, world)}
+    line.update(body)
     ctx.close()
     if rank == 0:
         print(json.dumps(line))
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    H.close()
     return 0
 
 

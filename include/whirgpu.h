@@ -141,7 +141,9 @@ whirgpu_status whirgpu_batch_proof(const whirgpu_batch* b, size_t i, const uint8
                                    const uint8_t** hints, size_t* hints_len);
 void whirgpu_batch_destroy(whirgpu_batch* b);
 
-/* Serving: a worker thread admits submitted requests (copied at submit) as
+/* Serving: a worker thread admits submitted requests (their host buffers are
+ * borrowed until poll has returned the result, and copied once into pinned
+ * staging at admission) as
  * HBM budget and one of max_inflight streams free up -- continuous batching:
  * requests arriving while others run join them on the device.  Each
  * workspace keeps a captured CUDA graph of its proof program.  While a server

@@ -53,12 +53,17 @@ def test_batch_matches_oracle(gpu_ctx, oracle):
             assert b.proof(i) == (onarg, ohints)
 
 
+MANY = [(8 + (i * 7) % 8, 1 + i % 3) for i in range(48)]
+
+
 def test_server_mix_matches_alone():
+    """Heavy overlap (16 proofs in flight, CTAs of concurrent kernels starting
+    late) must not change a byte: PoW minimum nonces, openings, all of it."""
     ctx = Context(0)
     try:
-        reqs = make_requests(ctx, SPECS * 2, seed0=5000)
+        reqs = make_requests(ctx, SPECS * 2 + MANY, seed0=5000)
         expected = [alone(ctx, r) for r in reqs]
-        srv = Server(ctx, hbm_budget=0, max_inflight=6)
+        srv = Server(ctx, hbm_budget=0, max_inflight=16)
         tickets = []
         for r in reqs:  # requests keep arriving while earlier ones run
             tickets.append(srv.submit(r))
@@ -100,5 +105,39 @@ def test_server_hbm_budget_admission():
         assert st["admitted"] == len(reqs)
         assert 0 < st["peak_bytes"] <= budget
         srv.close()
+    finally:
+        ctx.close()
+
+
+def test_server_device_inputs_and_eviction():
+    """Device-resident coefficients are served like host ones, and a budget
+    too small to cache every shape's workspace evicts idle ones (and their
+    captured programs) without changing any proof."""
+    import torch
+
+    ctx = Context(0)
+    try:
+        specs = [(13, 1), (11, 2), (12, 3), (10, 1), (13, 1), (11, 2), (12, 3), (10, 1)]
+        reqs = make_requests(ctx, specs, seed0=7000)
+        expected = [alone(ctx, r) for r in reqs]
+        dev = [torch.from_numpy(np.asarray(r.coeffs).view(np.int64)).cuda() for r in reqs]
+        torch.cuda.synchronize()
+        dreqs = [ProofRequest(r.num_variables, r.params, d.data_ptr(), r.points, r.evaluations, on_device=True)
+                 for r, d in zip(reqs, dev)]
+        from whirplonk_b200.whir import Config
+
+        sizes = [Config.from_params(1 << n, reqs[i].params).workspace_bytes() for i, (n, _) in enumerate(specs)]
+        budget = max(sizes) + min(sizes)  # at most two shapes resident at once
+        ctx2 = Context(0)  # empty workspace cache: every shape change must evict
+        srv = Server(ctx2, hbm_budget=budget, max_inflight=4)
+        for rounds in range(2):
+            tickets = [srv.submit(r) for r in (dreqs if rounds == 0 else reqs)]
+            for i, t in enumerate(tickets):
+                res = srv.poll(t, timeout_ms=60_000)
+                assert res.status == 0 and (res.narg, res.hints) == expected[i], f"request {i} round {rounds}"
+        st = srv.stats()
+        assert st["peak_bytes"] <= budget
+        srv.close()
+        ctx2.close()
     finally:
         ctx.close()

@@ -116,10 +116,14 @@ class Server:
         h = ctypes.c_void_p()
         _lib.check(self._L.whirgpu_server_create(ctx.handle, hbm_budget, max_inflight, ctypes.byref(h)), ctx.handle)
         self.handle = h.value
+        self._live = {}
 
     def submit(self, req: ProofRequest) -> int:
+        """Queues a request; its arrays are borrowed until poll() returns it."""
         t = ctypes.c_uint64()
-        _lib.check(self._L.whirgpu_server_submit(self.handle, ctypes.byref(req.to_c()), ctypes.byref(t)))
+        creq = req.to_c()
+        _lib.check(self._L.whirgpu_server_submit(self.handle, ctypes.byref(creq), ctypes.byref(t)))
+        self._live[t.value] = req
         return t.value
 
     def poll(self, ticket: int, timeout_ms: int = 60_000) -> Optional[ServedProof]:
@@ -131,6 +135,7 @@ class Server:
         out = ServedProof(r.status, ctypes.string_at(r.narg, r.narg_len) if r.narg_len else b"",
                           ctypes.string_at(r.hints, r.hints_len) if r.hints_len else b"", r.queue_ms, r.total_ms)
         self._L.whirgpu_server_release(self.handle, ticket)
+        self._live.pop(ticket, None)
         return out
 
     def stats(self):

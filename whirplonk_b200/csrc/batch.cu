@@ -27,90 +27,115 @@ using namespace wg;
 
 namespace {
 
-// One proof slot: a workspace plus pinned staging for its inputs and outputs.
+// One proof slot: a workspace plus pinned staging for its small inputs and its
+// outputs.  The coefficients are copied straight from the caller's buffer when
+// it is device or pinned host memory, else through `stage`.
 struct Slot {
     Workspace* ws = nullptr;
     ProofPlan plan;           // copy with n_forms set for the request
-    size_t ds_len = 0;
-    uint8_t* hin = nullptr;   // pinned: [coeffs | ds | points | evals]
+    uint8_t* hin = nullptr;   // pinned: [ds 96 | points | evals]
     size_t hin_bytes = 0;
     uint8_t* hout = nullptr;  // pinned: [TxState | narg | hints]
     size_t hout_bytes = 0;
-    const uint64_t* dev_coeffs = nullptr;  // caller's device pointer (device inputs)
-    cudaGraphExec_t graph = nullptr;       // captured single-proof program (serving)
+    uint8_t* stage = nullptr;          // pinned coefficient staging (pageable callers only)
+    const void* coeff_src = nullptr;   // what the coefficient copy reads
+    cudaGraphExec_t graph = nullptr;   // captured single-proof program (serving)
+    uint64_t graph_kernels = 0;        // kernel nodes in `graph`
 };
 
 size_t coeff_bytes(const ProofPlan& p) { return 8ull << p.n; }
+size_t points_off() { return 96; }
+size_t evals_off(const ProofPlan& p) { return 96 + (size_t)MAX_FORMS * p.n * 24; }
 
-whirgpu_status slot_init(whirgpu_ctx* c, const whirgpu_request& r, Slot& s) {
+bool is_pinned_host(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+whirgpu_status check_request(whirgpu_ctx* c, const whirgpu_request& r) {
     if (!is_blake3(&r.params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 engine is on this path");
     if (r.num_variables >= 40 || r.num_points > (uint64_t)MAX_FORMS) return fail(c, WHIRGPU_E_INVALID, "bad request");
     if (r.num_points && (!r.points || !r.evaluations)) return fail(c, WHIRGPU_E_INVALID, "bad statement");
     if (!r.coeffs) return fail(c, WHIRGPU_E_INVALID, "null coefficients");
-    s.ds_len = 96;
-    whirgpu_status st = acquire_workspace(c, r.num_variables, &r.params, s.ds_len, &s.ws);
-    if (st != WHIRGPU_OK) return st;
-    s.plan = s.ws->plan;
+    return WHIRGPU_OK;
+}
+
+// Binds a slot to workspace `ws` (already acquired) and allocates its staging.
+whirgpu_status slot_bind(whirgpu_ctx* c, const whirgpu_request& r, Workspace* ws, Slot& s) {
+    s.ws = ws;
+    s.plan = ws->plan;
     s.plan.n_forms = (int)r.num_points;
-    if (r.num_points + s.plan.sch.initial.out_domain == 0) {
-        release_workspace(s.ws);
-        s.ws = nullptr;
+    if (r.num_points + s.plan.sch.initial.out_domain == 0)
         return fail(c, WHIRGPU_E_UNSUPPORTED, "statement-free proofs are not on this path");
-    }
-    const size_t n = s.plan.n;
-    s.hin_bytes = coeff_bytes(s.plan) + 96 + MAX_FORMS * n * 24 + MAX_FORMS * 24;
+    s.hin_bytes = evals_off(s.plan) + MAX_FORMS * 24;
     s.hout_bytes = sizeof(TxState) + s.plan.narg_len + s.plan.hints_cap;
     if (cudaMallocHost(&s.hin, s.hin_bytes) != cudaSuccess || cudaMallocHost(&s.hout, s.hout_bytes) != cudaSuccess) {
-        release_workspace(s.ws);
-        s.ws = nullptr;
+        cudaGetLastError();
         return fail(c, WHIRGPU_E_OOM, "pinned staging");
     }
     return WHIRGPU_OK;
 }
 
-void slot_free(Slot& s) {
+// Frees the slot's host staging and graph (not its workspace).
+void slot_free_host(Slot& s) {
     if (s.graph) cudaGraphExecDestroy(s.graph);
     if (s.hin) cudaFreeHost(s.hin);
     if (s.hout) cudaFreeHost(s.hout);
-    release_workspace(s.ws);
-    s = Slot();
+    if (s.stage) cudaFreeHost(s.stage);
+    s.graph = nullptr;
+    s.hin = s.hout = s.stage = nullptr;
 }
 
-// Copies the request into the slot's pinned input staging (host side).
-void slot_stage(Slot& s, const whirgpu_request& r) {
-    const size_t cb = coeff_bytes(s.plan);
+// Copies the request's small inputs into the pinned staging and picks the
+// source of the coefficient copy (host side).
+whirgpu_status slot_stage(whirgpu_ctx* c, Slot& s, const whirgpu_request& r) {
     const size_t n = s.plan.n;
-    if (r.coeffs_location == WHIRGPU_INPUT_DEVICE) s.dev_coeffs = r.coeffs;
-    else {
-        s.dev_coeffs = nullptr;
-        std::memcpy(s.hin, r.coeffs, cb);
+    if (r.coeffs_location == WHIRGPU_INPUT_DEVICE || is_pinned_host(r.coeffs)) {
+        s.coeff_src = r.coeffs;
+    } else {
+        if (!s.stage && cudaMallocHost(&s.stage, coeff_bytes(s.plan)) != cudaSuccess) {
+            cudaGetLastError();
+            s.stage = nullptr;
+            return fail(c, WHIRGPU_E_OOM, "pinned coefficient staging");
+        }
+        std::memcpy(s.stage, r.coeffs, coeff_bytes(s.plan));
+        s.coeff_src = s.stage;
     }
-    std::memcpy(s.hin + cb, r.protocol_id, 64);
-    std::memcpy(s.hin + cb + 64, r.session_id, 32);
+    std::memcpy(s.hin, r.protocol_id, 64);
+    std::memcpy(s.hin + 64, r.session_id, 32);
     if (r.num_points) {
-        std::memcpy(s.hin + cb + 96, r.points, r.num_points * n * 24);
-        std::memcpy(s.hin + cb + 96 + MAX_FORMS * n * 24, r.evaluations, r.num_points * 24);
+        std::memcpy(s.hin + points_off(), r.points, r.num_points * n * 24);
+        std::memcpy(s.hin + evals_off(s.plan), r.evaluations, r.num_points * 24);
     }
+    return WHIRGPU_OK;
 }
 
-// Enqueues input copies, commit, prove and the proof read-back of one slot.
-int slot_enqueue(whirgpu_ctx* c, Slot& s, cudaStream_t st) {
+int copy_coeffs(const Slot& s, cudaStream_t st) {
+    return cudaMemcpyAsync(s.ws->dev + s.plan.off_coeffs, s.coeff_src, coeff_bytes(s.plan), cudaMemcpyDefault, st) ==
+                   cudaSuccess
+               ? 0
+               : -1;
+}
+
+// Enqueues (optionally) the coefficient copy, the small input copies, commit,
+// prove and the proof read-back of one slot.
+int slot_enqueue(whirgpu_ctx* c, Slot& s, cudaStream_t st, bool with_coeffs) {
     const ProofPlan& p = s.plan;
     char* ws = s.ws->dev;
-    const size_t cb = coeff_bytes(p);
     const size_t n = p.n;
-    cudaError_t e;
-    if (s.dev_coeffs) e = cudaMemcpyAsync(ws + p.off_coeffs, s.dev_coeffs, cb, cudaMemcpyDeviceToDevice, st);
-    else e = cudaMemcpyAsync(ws + p.off_coeffs, s.hin, cb, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return -1;
-    if (cudaMemcpyAsync(ws + p.off_ds, s.hin + cb, 96, cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
+    if (with_coeffs && copy_coeffs(s, st) != 0) return -1;
+    if (cudaMemcpyAsync(ws + p.off_ds, s.hin, 96, cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
     ProofScalars* sc = plan_scalars(p, ws);
     if (p.n_forms) {
-        if (cudaMemcpyAsync(ws + p.off_points, s.hin + cb + 96, p.n_forms * n * 24, cudaMemcpyHostToDevice, st) !=
+        if (cudaMemcpyAsync(ws + p.off_points, s.hin + points_off(), p.n_forms * n * 24, cudaMemcpyHostToDevice, st) !=
             cudaSuccess)
             return -1;
-        if (cudaMemcpyAsync(&sc->forms_eval[0], s.hin + cb + 96 + MAX_FORMS * n * 24, p.n_forms * 24,
-                            cudaMemcpyHostToDevice, st) != cudaSuccess)
+        if (cudaMemcpyAsync(&sc->forms_eval[0], s.hin + evals_off(p), p.n_forms * 24, cudaMemcpyHostToDevice, st) !=
+            cudaSuccess)
             return -1;
     }
     if (enqueue_commit(p, ws, 96, c->tw, st, nullptr) != 0) return -2;
@@ -152,6 +177,7 @@ struct whirgpu_batch {
     cudaEvent_t fork = nullptr;
     cudaStream_t main = nullptr;
     cudaGraphExec_t exec = nullptr;
+    uint64_t graph_kernels = 0;
     std::vector<std::vector<uint8_t>> narg, hints;
     std::vector<whirgpu_status> status;
 };
@@ -164,7 +190,7 @@ whirgpu_status batch_enqueue_all(whirgpu_batch* b) {
     for (size_t i = 0; i < b->slots.size(); ++i) {
         cudaStream_t st = b->streams[i % b->streams.size()];
         cudaStreamWaitEvent(st, b->fork, 0);
-        if (slot_enqueue(c, b->slots[i], st) != 0) return fail(c, WHIRGPU_E_CUDA, "batch enqueue");
+        if (slot_enqueue(c, b->slots[i], st, true) != 0) return fail(c, WHIRGPU_E_CUDA, "batch enqueue");
     }
     for (size_t k = 0; k < b->streams.size(); ++k) {
         cudaEventRecord(b->joins[k], b->streams[k]);
@@ -186,12 +212,21 @@ whirgpu_status whirgpu_batch_create(whirgpu_ctx* c, const whirgpu_request* reqs,
     b->mode = mode;
     b->reqs.assign(reqs, reqs + count);
     b->slots.resize(count);
-    for (size_t i = 0; i < count; ++i) {
-        whirgpu_status st = slot_init(c, reqs[i], b->slots[i]);
-        if (st != WHIRGPU_OK) {
-            for (auto& s : b->slots) slot_free(s);
-            return st;
+    auto unwind = [&](whirgpu_status st) {
+        for (auto& sl : b->slots) {
+            slot_free_host(sl);
+            release_workspace(c, sl.ws);
         }
+        return st;
+    };
+    for (size_t i = 0; i < count; ++i) {
+        whirgpu_status st = check_request(c, reqs[i]);
+        Workspace* ws = nullptr;
+        if (st == WHIRGPU_OK) st = acquire_workspace(c, reqs[i].num_variables, &reqs[i].params, 96, &ws);
+        if (st == WHIRGPU_OK) st = slot_bind(c, reqs[i], ws, b->slots[i]);
+        else b->slots[i].ws = nullptr;
+        if (st == WHIRGPU_OK) st = slot_stage(c, b->slots[i], reqs[i]);
+        if (st != WHIRGPU_OK) return unwind(st);
     }
     const size_t nstreams = mode == 2 ? 1 : std::min<size_t>(count, 64);
     b->streams.resize(nstreams);
@@ -205,19 +240,26 @@ whirgpu_status whirgpu_batch_create(whirgpu_ctx* c, const whirgpu_request* reqs,
     b->narg.resize(count);
     b->hints.resize(count);
     b->status.assign(count, WHIRGPU_E_INVALID);
-    for (size_t i = 0; i < count; ++i) slot_stage(b->slots[i], reqs[i]);
     if (mode == 0) {
         // One graph: a fork event, one branch per proof, a join.
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return cuda_fail(c, cudaGetLastError(), "begin capture");
+        set_capturing(true);
         whirgpu_status st = batch_enqueue_all(b.get());
+        set_capturing(false);
         cudaError_t ce = cudaStreamEndCapture(b->main, &g);
-        if (st != WHIRGPU_OK) return st;
-        if (ce != cudaSuccess) return cuda_fail(c, ce, "end capture");
-        ce = cudaGraphInstantiate(&b->exec, g, 0);
-        cudaGraphDestroy(g);
-        if (ce != cudaSuccess) return cuda_fail(c, ce, "graph instantiate");
+        if (st == WHIRGPU_OK && ce != cudaSuccess) st = cuda_fail(c, ce, "end capture");
+        if (st == WHIRGPU_OK) {
+            b->graph_kernels = graph_kernel_nodes(g);
+            ce = cudaGraphInstantiate(&b->exec, g, 0);
+            if (ce != cudaSuccess) st = cuda_fail(c, ce, "graph instantiate");
+        }
+        if (g) cudaGraphDestroy(g);
+        if (st != WHIRGPU_OK) {
+            whirgpu_batch_destroy(b.release());
+            return st;
+        }
     }
     *out = b.release();
     return WHIRGPU_OK;
@@ -226,8 +268,15 @@ whirgpu_status whirgpu_batch_create(whirgpu_ctx* c, const whirgpu_request* reqs,
 whirgpu_status whirgpu_batch_run(whirgpu_batch* b) {
     if (!b) return WHIRGPU_E_INVALID;
     whirgpu_ctx* c = b->ctx;
-    for (size_t i = 0; i < b->slots.size(); ++i) slot_stage(b->slots[i], b->reqs[i]);
+    for (size_t i = 0; i < b->slots.size(); ++i) {
+        const void* before = b->slots[i].coeff_src;
+        whirgpu_status st = slot_stage(c, b->slots[i], b->reqs[i]);
+        if (st != WHIRGPU_OK) return st;
+        if (b->mode == 0 && b->slots[i].coeff_src != before)
+            return fail(c, WHIRGPU_E_INVALID, "coefficient memory changed kind since the batch was captured");
+    }
     if (b->mode == 0) {
+        count_launches(b->graph_kernels);
         cudaError_t e = cudaGraphLaunch(b->exec, b->main);
         if (e != cudaSuccess) return cuda_fail(c, e, "graph launch");
         e = cudaStreamSynchronize(b->main);
@@ -240,7 +289,7 @@ whirgpu_status whirgpu_batch_run(whirgpu_batch* b) {
     } else {
         // plain: one proof at a time, each waited for before the next starts
         for (size_t i = 0; i < b->slots.size(); ++i) {
-            if (slot_enqueue(c, b->slots[i], b->streams[0]) != 0) return fail(c, WHIRGPU_E_CUDA, "enqueue");
+            if (slot_enqueue(c, b->slots[i], b->streams[0], true) != 0) return fail(c, WHIRGPU_E_CUDA, "enqueue");
             cudaError_t e = cudaStreamSynchronize(b->streams[0]);
             if (e != cudaSuccess) return cuda_fail(c, e, "proof");
         }
@@ -266,10 +315,13 @@ whirgpu_status whirgpu_batch_proof(const whirgpu_batch* b, size_t i, const uint8
 
 void whirgpu_batch_destroy(whirgpu_batch* b) {
     if (!b) return;
-    cudaStreamSynchronize(b->main);
+    if (b->main) cudaStreamSynchronize(b->main);
     for (auto st : b->streams) cudaStreamSynchronize(st);
     if (b->exec) cudaGraphExecDestroy(b->exec);
-    for (auto& s : b->slots) slot_free(s);
+    for (auto& s : b->slots) {
+        slot_free_host(s);
+        release_workspace(b->ctx, s.ws);
+    }
     for (auto st : b->streams) cudaStreamDestroy(st);
     for (auto e : b->joins) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
@@ -289,7 +341,6 @@ using Clock = std::chrono::steady_clock;
 struct Ticket {
     uint64_t id = 0;
     whirgpu_request req{};
-    std::vector<uint64_t> coeffs, points, evals;  // owned copies of the inputs
     size_t bytes = 0;                             // workspace bytes it needs
     Clock::time_point t_submit, t_start, t_done;
     Slot* slot = nullptr;
@@ -326,36 +377,61 @@ struct whirgpu_server {
 namespace {
 
 // The cached program for a request: acquires a free workspace of the right
-// shape and, on first use of that workspace, captures its commit + prove.
+// shape and, on first use of that workspace, captures its commit + prove
+// (everything but the coefficient copy, which reads the caller's buffer and is
+// issued before each launch).  The program is dropped with its workspace when
+// the context evicts it.
 whirgpu_status program_for(whirgpu_server* s, const whirgpu_request& r, cudaStream_t cs, Slot** out) {
-    Slot tmp;
-    whirgpu_status st = slot_init(s->ctx, r, tmp);  // acquires a workspace + fresh staging
+    whirgpu_ctx* c = s->ctx;
+    whirgpu_status st = check_request(c, r);
     if (st != WHIRGPU_OK) return st;
-    auto key = std::make_pair(tmp.ws, (int)r.num_points);
+    Workspace* ws = nullptr;
+    st = acquire_workspace(c, r.num_variables, &r.params, 96, &ws, s->budget);
+    if (st != WHIRGPU_OK) return st;
+    auto key = std::make_pair(ws, (int)r.num_points);
     auto it = s->programs.find(key);
     if (it != s->programs.end()) {
-        cudaFreeHost(tmp.hin);
-        cudaFreeHost(tmp.hout);
         *out = it->second.get();
         return WHIRGPU_OK;
     }
-    auto slot = std::make_unique<Slot>(tmp);
-    slot_stage(*slot, r);
+    auto slot = std::make_unique<Slot>();
+    st = slot_bind(c, r, ws, *slot);
+    if (st == WHIRGPU_OK) st = slot_stage(c, *slot, r);
+    if (st != WHIRGPU_OK) {
+        slot_free_host(*slot);
+        release_workspace(c, ws);
+        return st;
+    }
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-        slot_free(*slot);
-        return fail(s->ctx, WHIRGPU_E_CUDA, "begin capture");
+        slot_free_host(*slot);
+        release_workspace(c, ws);
+        return fail(c, WHIRGPU_E_CUDA, "begin capture");
     }
-    const int rc = slot_enqueue(s->ctx, *slot, cs);
+    set_capturing(true);
+    const int rc = slot_enqueue(c, *slot, cs, false);
+    set_capturing(false);
     cudaError_t e = cudaStreamEndCapture(cs, &g);
-    if (rc == 0 && e == cudaSuccess) e = cudaGraphInstantiate(&slot->graph, g, 0);
+    if (rc == 0 && e == cudaSuccess) {
+        slot->graph_kernels = graph_kernel_nodes(g);
+        e = cudaGraphInstantiate(&slot->graph, g, 0);
+    }
     if (g) cudaGraphDestroy(g);
     if (rc != 0 || e != cudaSuccess) {
-        slot_free(*slot);
-        return fail(s->ctx, WHIRGPU_E_CUDA, "capture of the proof program");
+        cudaGetLastError();
+        slot_free_host(*slot);
+        release_workspace(c, ws);
+        return fail(c, WHIRGPU_E_CUDA, "capture of the proof program");
     }
     *out = slot.get();
     s->programs[key] = std::move(slot);
+    ws->on_free[s] = [s, ws] {
+        for (auto pit = s->programs.begin(); pit != s->programs.end();) {
+            if (pit->first.first != ws) { ++pit; continue; }
+            slot_free_host(*pit->second);
+            pit = s->programs.erase(pit);
+        }
+    };
     return WHIRGPU_OK;
 }
 
@@ -373,13 +449,18 @@ void admit(whirgpu_server* s) {
         Slot* slot = nullptr;
         whirgpu_status st = program_for(s, t.req, s->streams[k], &slot);
         if (st == WHIRGPU_OK) {
-            slot_stage(*slot, t.req);
-            cudaError_t e = cudaGraphLaunch(slot->graph, s->streams[k]);
-            if (e == cudaSuccess) e = cudaEventRecord(t.done_ev, s->streams[k]);
-            if (e != cudaSuccess) {
-                release_workspace(slot->ws);
-                st = WHIRGPU_E_CUDA;
+            st = slot_stage(s->ctx, *slot, t.req);
+            cudaError_t e = cudaSuccess;
+            if (st == WHIRGPU_OK) {
+                e = copy_coeffs(*slot, s->streams[k]) == 0 ? cudaSuccess : cudaErrorInvalidValue;
+                if (e == cudaSuccess) {
+                    count_launches(slot->graph_kernels);
+                    e = cudaGraphLaunch(slot->graph, s->streams[k]);
+                }
+                if (e == cudaSuccess) e = cudaEventRecord(t.done_ev, s->streams[k]);
+                if (e != cudaSuccess) st = cuda_fail(s->ctx, e, "proof launch");
             }
+            if (st != WHIRGPU_OK) release_workspace(s->ctx, slot->ws);
         }
         if (st != WHIRGPU_OK) {
             t.status = st;
@@ -412,7 +493,7 @@ void reap(whirgpu_server* s) {
         t.t_done = Clock::now();
         s->stream_busy[t.stream] = 0;
         s->in_use -= t.bytes;
-        release_workspace(t.slot->ws);  // back to the pool with its captured program
+        release_workspace(s->ctx, t.slot->ws);  // back to the pool with its captured program
         t.slot = nullptr;
         s->inflight.erase(s->inflight.begin() + i);
         s->cv_done.notify_all();
@@ -452,22 +533,15 @@ whirgpu_status whirgpu_server_create(whirgpu_ctx* c, uint64_t hbm_budget, uint32
 
 whirgpu_status whirgpu_server_submit(whirgpu_server* s, const whirgpu_request* r, uint64_t* ticket) {
     if (!s || !r || !ticket || !r->coeffs) return WHIRGPU_E_INVALID;
-    if (r->coeffs_location == WHIRGPU_INPUT_DEVICE) return WHIRGPU_E_UNSUPPORTED;  // served inputs are copied
     if (r->num_points > (uint64_t)MAX_FORMS || (r->num_points && (!r->points || !r->evaluations)))
         return WHIRGPU_E_INVALID;
     const size_t bytes = workspace_bytes(r->num_variables, &r->params);
     if (bytes == 0) return WHIRGPU_E_INVALID;
     if (s->budget && bytes > s->budget) return WHIRGPU_E_OOM;  // could never be admitted
+    // The request's buffers are borrowed until poll returns the result: the
+    // only copy is into the workspace's pinned staging at admission.
     auto t = std::make_unique<Ticket>();
     t->req = *r;
-    t->coeffs.assign(r->coeffs, r->coeffs + (1ull << r->num_variables));
-    t->req.coeffs = t->coeffs.data();
-    if (r->num_points) {
-        t->points.assign(r->points, r->points + r->num_points * r->num_variables * 3);
-        t->evals.assign(r->evaluations, r->evaluations + r->num_points * 3);
-    }
-    t->req.points = t->points.data();
-    t->req.evaluations = t->evals.data();
     t->bytes = bytes;
     t->t_submit = Clock::now();
     cudaEventCreateWithFlags(&t->done_ev, cudaEventDisableTiming);
@@ -541,7 +615,14 @@ void whirgpu_server_destroy(whirgpu_server* s) {
     if (s->worker.joinable()) s->worker.join();
     for (auto& kv : s->tickets)
         if (kv.second->done_ev) cudaEventDestroy(kv.second->done_ev);
-    for (auto& kv : s->programs) slot_free(*kv.second);
+    {
+        std::lock_guard<std::recursive_mutex> lk(s->ctx->cache_mu);
+        for (auto& kv : s->programs) {
+            kv.first.first->on_free.erase(s);
+            slot_free_host(*kv.second);
+        }
+        s->programs.clear();
+    }
     for (auto st : s->streams) cudaStreamDestroy(st);
     delete s;
 }

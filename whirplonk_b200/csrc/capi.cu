@@ -134,7 +134,35 @@ whirgpu_status ensure_pinned(whirgpu_ctx* c, size_t bytes) {
     return WHIRGPU_OK;
 }
 
-whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out) {
+namespace {
+
+void free_workspace(whirgpu_ctx* c, Workspace* w) {
+    for (auto& kv : w->on_free) kv.second();
+    cudaFree(w->dev);
+    c->allocated -= w->plan.total_bytes;
+    delete w;
+}
+
+// Frees idle workspaces, least recently used first, until `need` more bytes
+// fit under `limit` (all idle ones when limit is 0).  Returns whether they fit.
+bool evict_idle(whirgpu_ctx* c, uint64_t need, uint64_t limit) {
+    for (;;) {
+        if (limit && c->allocated + need <= limit) return true;
+        Workspace* victim = nullptr;
+        std::vector<Workspace*>* owner = nullptr;
+        for (auto& kv : c->cache)
+            for (Workspace* w : kv.second)
+                if (!w->busy && (!victim || w->last_used < victim->last_used)) { victim = w; owner = &kv.second; }
+        if (!victim) return limit == 0;
+        owner->erase(std::find(owner->begin(), owner->end(), victim));
+        free_workspace(c, victim);
+    }
+}
+
+}  // namespace
+
+whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out,
+                                 uint64_t cap) {
     ProofPlan plan;
     try {
         plan = make_plan((uint32_t)n, to_params(params), MAX_FORMS, std::max<size_t>(ds_len, 96));
@@ -144,29 +172,44 @@ whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_param
     auto key = std::make_tuple(n, params->starting_log_inv_rate, params->initial_folding_factor, params->folding_factor,
                                params->security_level, params->pow_bits,
                                (uint64_t)params->unique_decoding | ((uint64_t)std::max<size_t>(ds_len, 96) << 1));
-    auto& vec = c->cache[key];
-    for (Workspace* w : vec)
-        if (!w->busy) { w->busy = true; *out = w; return WHIRGPU_OK; }
-    if (c->budget && c->allocated + plan.total_bytes > c->budget)
-        return fail(c, WHIRGPU_E_OOM, "workspace above the HBM budget");
+    std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+    for (Workspace* w : c->cache[key])
+        if (!w->busy) {
+            w->busy = true;
+            w->last_used = ++c->use_clock;
+            *out = w;
+            return WHIRGPU_OK;
+        }
+    uint64_t limit = c->budget;
+    if (cap && (!limit || cap < limit)) limit = cap;
+    if (limit && !evict_idle(c, plan.total_bytes, limit)) return fail(c, WHIRGPU_E_OOM, "workspace above the HBM budget");
     Workspace* w = new Workspace();
     w->plan = plan;
     cudaError_t e = cudaMalloc(&w->dev, plan.total_bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        evict_idle(c, plan.total_bytes, 0);
+        e = cudaMalloc(&w->dev, plan.total_bytes);
+    }
     if (e != cudaSuccess) { delete w; return cuda_fail(c, e, "cudaMalloc workspace"); }
     // Counters and tickets start at zero and reset themselves after use.
     e = cudaMemsetAsync(w->dev + plan.off_sc_scratch, 0, plan.off_tx - plan.off_sc_scratch, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { cudaFree(w->dev); delete w; return cuda_fail(c, e, "cudaMemset"); }
     c->allocated += plan.total_bytes;
     w->busy = true;
-    vec.push_back(w);
+    w->last_used = ++c->use_clock;
+    c->cache[key].push_back(w);
     *out = w;
     return WHIRGPU_OK;
 }
 
 bool is_blake3(const whirgpu_params* p) { return std::memcmp(p->hash_id, BLAKE3_ENGINE_ID, 32) == 0; }
 
-void release_workspace(Workspace* w) {
-    if (w) w->busy = false;
+void release_workspace(whirgpu_ctx* c, Workspace* w) {
+    if (!w) return;
+    std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+    w->busy = false;
 }
 
 size_t workspace_bytes(uint64_t n, const whirgpu_params* params) {
@@ -219,7 +262,7 @@ void whirgpu_ctx_destroy(whirgpu_ctx* c) {
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
     for (auto& kv : c->cache)
-        for (Workspace* w : kv.second) { cudaFree(w->dev); delete w; }
+        for (Workspace* w : kv.second) free_workspace(c, w);
     cudaFree(c->tw.tw_stage);
     cudaFree(c->tw.tw_hi);
     cudaFree(c->tw.tw_lo);
@@ -315,15 +358,15 @@ whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, cons
                                     c->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(ws->dev + p.off_ds, tx->ds.data(), tx->ds.size(), cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) { ws->busy = false; return cuda_fail(c, e, "input copy"); }
+    if (e != cudaSuccess) { release_workspace(c, ws); return cuda_fail(c, e, "input copy"); }
     c->io_h2d = (where == WHIRGPU_INPUT_DEVICE ? 0 : (8ull << n)) + tx->ds.size();
     c->io_d2h = 0;
     if (enqueue_commit(p, ws->dev, (uint32_t)tx->ds.size(), c->tw, c->stream, c->timer.get()) != 0) {
-        ws->busy = false;
+        release_workspace(c, ws);
         return fail(c, WHIRGPU_E_INVALID, "commit launch failed");
     }
     e = cudaGetLastError();
-    if (e != cudaSuccess) { ws->busy = false; return cuda_fail(c, e, "commit kernels"); }
+    if (e != cudaSuccess) { release_workspace(c, ws); return cuda_fail(c, e, "commit kernels"); }
     auto w = new whirgpu_witness();
     w->ctx = c;
     w->ws = ws;
@@ -337,7 +380,7 @@ void whirgpu_witness_destroy(whirgpu_witness* w) {
     if (!w) return;
     if (w->ws) {
         cudaStreamSynchronize(w->ctx->stream);
-        w->ws->busy = false;
+        release_workspace(w->ctx, w->ws);
     }
     delete w;
 }
@@ -509,7 +552,23 @@ void whirgpu_last_io_bytes(const whirgpu_ctx* c, uint64_t* h2d, uint64_t* d2h) {
 
 namespace wg {
 static std::atomic<u64> g_launches{0};
-void count_launches(u64 k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+static thread_local bool g_capturing = false;
+void count_launches(u64 k) {
+    if (!g_capturing) g_launches.fetch_add(k, std::memory_order_relaxed);
+}
+void set_capturing(bool on) { g_capturing = on; }
+uint64_t graph_kernel_nodes(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    uint64_t k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+    }
+    return k;
+}
 u64 launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void host_twiddles(u64* stage, u64* hi, u64* lo) {

@@ -5,7 +5,9 @@
 
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <string>
 #include <tuple>
@@ -69,6 +71,8 @@ struct Workspace {
     ProofPlan plan;
     char* dev = nullptr;
     bool busy = false;
+    uint64_t last_used = 0;                    // LRU stamp for eviction of idle workspaces
+    std::map<const void*, std::function<void()>> on_free;  // per owner: drops state tied to `dev` (captured graphs)
 };
 
 }  // namespace wg
@@ -90,6 +94,8 @@ struct whirgpu_ctx {
     uint64_t stat_launches[wg::FAM_COUNT] = {};
     double stat_ms[wg::FAM_COUNT] = {};
     uint64_t io_h2d = 0, io_d2h = 0;
+    std::recursive_mutex cache_mu;  // workspace cache (the serving thread shares the context)
+    uint64_t use_clock = 0;
 };
 
 struct whirgpu_transcript {
@@ -111,9 +117,17 @@ whirgpu_status fail(whirgpu_ctx* c, whirgpu_status s, const std::string& msg);
 whirgpu_status cuda_fail(whirgpu_ctx* c, cudaError_t e, const char* what);
 whirgpu_status ensure_pinned(whirgpu_ctx* c, size_t bytes);
 // A free workspace for (n, params, ds_len), allocated on first use and kept in
-// the context cache; marked busy until release_workspace.
-whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out);
-void release_workspace(Workspace* w);
+// the context cache; marked busy until release_workspace.  Allocation keeps the
+// context's bytes within min(ctx budget, cap) (0 = no limit) by freeing idle
+// workspaces, least recently used first; a failed cudaMalloc frees every idle
+// workspace and tries once more.
+whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out,
+                                 uint64_t cap = 0);
+void release_workspace(whirgpu_ctx* c, Workspace* w);
+// While set, kernel launches of this thread are stream-captured, not run: the
+// launch counter skips them and graph launches add their kernel-node counts.
+void set_capturing(bool on);
+uint64_t graph_kernel_nodes(cudaGraph_t g);
 bool is_blake3(const whirgpu_params* p);
 // Plan size of one proof (bytes of device workspace), or 0 when invalid.
 size_t workspace_bytes(uint64_t n, const whirgpu_params* params);

@@ -87,7 +87,10 @@ __global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
 
 __global__ void __launch_bounds__(POW_THREADS) k_pow_window(ProofScalars* sc, u64 threshold, u64 base, u64 count) {
     const u64* best = &sc->pow_best;
-    if (__ldcg(best) != ~0ull) return;  // an earlier window already holds the minimum
+    // A hit below `base` came from an earlier window and is the minimum.  A hit
+    // of this window (>= base) must not stop a CTA that starts late: its
+    // nonces may lie below that hit, so it scans up to the published hit.
+    if (__ldcg(best) < base) return;
     __shared__ unsigned ch[8];
     if (threadIdx.x < 8) {
         const unsigned char* c = sc->pow_ch + 4 * threadIdx.x;
