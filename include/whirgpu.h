@@ -168,6 +168,58 @@ void whirgpu_server_stats(whirgpu_server* s, uint64_t* admitted, uint64_t* peak_
                           uint64_t* queued);
 void whirgpu_server_destroy(whirgpu_server* s);
 
+/* ---- kernel level: Reed-Solomon encoding and matrix commitment ----------------- */
+/* RS-encode `count` vectors of 2^log_len canonical base-field words each, as
+ * irs_commit::commit encodes one vector (irs_commit.hpp:402-411 -> mod_ntt.hpp:49-130):
+ * interleaving depth 2^log_depth, block b = words [b m, (b+1) m) with
+ * m = 2^(log_len - log_depth), codeword X_b[i] = sum_j v[b m + j] w_N^(i j) for
+ * i < N = 2^log_expansion m, w_N = 7^((p-1)/N).  Device pointers only: the
+ * vectors back to back; d_tmp and d_planes hold count * 2^log_depth * N words
+ * each; plane (vector k, block b) = d_planes + (k 2^log_depth + b) N.
+ * Enqueued on the context stream (whirgpu_stream); returns without waiting. */
+whirgpu_status whirgpu_rs_encode(whirgpu_ctx* ctx, const uint64_t* d_vectors, size_t count, uint32_t log_len,
+                                 uint32_t log_expansion, uint32_t log_depth, uint64_t* d_tmp, uint64_t* d_planes);
+/* RS-encode and Merkle-commit `count` vectors (host or device memory, see
+ * WHIRGPU_INPUT_*): per vector the root of irs_commit::commit's matrix
+ * commitment (rows of 2^log_depth elements, leaf = BLAKE3 of the row's LE bytes,
+ * matrix_commit.hpp:169-195; tree merkle_tree.hpp:104-147), written to
+ * roots[32 k ..].  Synchronous.  Replaces the commitment half of
+ * Config::commit (irs_commit.hpp:433-470) for many vectors at once, without the
+ * transcript. */
+whirgpu_status whirgpu_rs_commit_batch(whirgpu_ctx* ctx, const uint64_t* vectors, int location, size_t count,
+                                       uint32_t log_len, uint32_t log_expansion, uint32_t log_depth, uint8_t* roots);
+
+/* ---- NTT pass plans (autotuned) ------------------------------------------------- */
+/* The LDE of a 2^log_n codeword from a 2^(log_n - log_expansion) message runs in
+ * npass passes of radix 2^log_radix[s] (sum = log_n, each <= 11); pass s stages
+ * 2^log_cols[s] columns per CTA (255 = built-in choice).  No counterpart in the
+ * reference (its NTT engine picks fixed radices, cooley_tukey.hpp:200-259). */
+typedef struct {
+    uint32_t log_n, log_expansion, npass;
+    uint32_t log_radix[3];
+    uint32_t log_cols[3];
+} whirgpu_ntt_plan;
+/* Times every valid plan for the shape on `planes` synthetic planes (median of
+ * `reps` runs each), checks each plan's codeword against the built-in plan's,
+ * installs the fastest agreeing plan for (log_n, log_expansion) and returns it.
+ * Returns WHIRGPU_E_DEVICE (after installing) if any plan disagreed. */
+whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* ctx, uint32_t log_n, uint32_t log_expansion, uint32_t planes,
+                                    uint32_t reps, whirgpu_ntt_plan* best, double* best_us, uint32_t* tried);
+/* Installs a plan (npass = 0 removes the shape's plan); process-wide. */
+whirgpu_status whirgpu_ntt_set_plan(const whirgpu_ntt_plan* plan);
+/* The plan the encoder uses for a shape (installed, else built-in). */
+whirgpu_status whirgpu_ntt_get_plan(uint32_t log_n, uint32_t log_expansion, whirgpu_ntt_plan* out);
+void whirgpu_ntt_clear_plans(void);
+/* Installed plans (returns the count; writes at most cap). */
+size_t whirgpu_ntt_list_plans(whirgpu_ntt_plan* out, size_t cap);
+/* JSON plan files: {"plans": [{"log_n": .., "log_expansion": .., "npass": ..,
+ * "log_radix": [..], "log_cols": [..]}, ..]}. */
+whirgpu_status whirgpu_ntt_load_plans(const char* path, size_t* loaded);
+whirgpu_status whirgpu_ntt_save_plans(const char* path);
+/* Installs, once per process, the plans in $WHIRGPU_NTT_PLANS or else in
+ * ntt_plans.json beside the library (called by whirgpu_ctx_create). */
+void whirgpu_ntt_load_default_plans(void);
+
 /* ---- helpers ------------------------------------------------------------------- */
 /* Multilinear extension of 2^num_variables base coefficients at an Ext3 point
  * (MultilinearExtension::evaluate, linear_form.hpp:119-126), on the device. */

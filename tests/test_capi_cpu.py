@@ -83,3 +83,36 @@ def test_sampler_is_seeded_uniform_and_canonical():
     # crude uniformity: top bits spread
     top = (a >> np.uint64(60)).astype(np.int64)
     assert np.bincount(top, minlength=16).min() > (1 << 14) / 16 * 0.8
+
+
+def test_ntt_plan_table_roundtrip(tmp_path):
+    """Plan install / validation / save / load are host-only."""
+    import ctypes
+
+    from whirplonk_b200 import _lib
+
+    L = _lib.load()
+    L.whirgpu_ntt_clear_plans()
+    good = _lib.NttPlan(20, 3, 2, (9, 11, 0), (4, 2, 255))
+    assert L.whirgpu_ntt_set_plan(ctypes.byref(good)) == _lib.OK
+    for bad in [_lib.NttPlan(20, 3, 2, (8, 11, 0), (255, 255, 255)),   # radices do not sum to log_n
+                _lib.NttPlan(24, 1, 2, (12, 12, 0), (255, 255, 255)),  # radix above 2^11
+                _lib.NttPlan(22, 1, 1, (22, 0, 0), (255, 255, 255)),   # one pass above 2^11
+                _lib.NttPlan(20, 3, 2, (9, 11, 0), (7, 0, 255))]:      # too many columns
+        assert L.whirgpu_ntt_set_plan(ctypes.byref(bad)) == _lib.E_INVALID
+    out = _lib.NttPlan()
+    assert L.whirgpu_ntt_get_plan(20, 3, ctypes.byref(out)) == _lib.OK
+    assert out.as_dict() == good.as_dict()
+    assert L.whirgpu_ntt_get_plan(20, 2, ctypes.byref(out)) == _lib.OK  # untuned: built-in split
+    assert out.npass == 2 and list(out.log_radix)[:2] == [10, 10]
+    path = str(tmp_path / "plans.json")
+    assert L.whirgpu_ntt_save_plans(path.encode()) == _lib.OK
+    L.whirgpu_ntt_clear_plans()
+    assert L.whirgpu_ntt_list_plans(None, 0) == 0
+    n = ctypes.c_size_t()
+    assert L.whirgpu_ntt_load_plans(path.encode(), ctypes.byref(n)) == _lib.OK and n.value == 1
+    assert L.whirgpu_ntt_get_plan(20, 3, ctypes.byref(out)) == _lib.OK and out.as_dict() == good.as_dict()
+    import json
+
+    assert json.load(open(path))["plans"][0]["log_radix"] == [9, 11, 0]
+    L.whirgpu_ntt_clear_plans()

@@ -30,6 +30,9 @@ EXPORTED = [
     "whirgpu_batch_create", "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_batch_destroy",
     "whirgpu_server_create", "whirgpu_server_submit", "whirgpu_server_poll", "whirgpu_server_release",
     "whirgpu_server_stats", "whirgpu_server_destroy",
+    "whirgpu_rs_encode", "whirgpu_rs_commit_batch",
+    "whirgpu_ntt_autotune", "whirgpu_ntt_set_plan", "whirgpu_ntt_get_plan", "whirgpu_ntt_clear_plans",
+    "whirgpu_ntt_list_plans", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans", "whirgpu_ntt_load_default_plans",
 ]
 
 
@@ -76,6 +79,22 @@ class Result(ctypes.Structure):
         ("queue_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
     ]
+
+
+class NttPlan(ctypes.Structure):
+    """Mirror of whirgpu_ntt_plan."""
+
+    _fields_ = [
+        ("log_n", ctypes.c_uint32),
+        ("log_expansion", ctypes.c_uint32),
+        ("npass", ctypes.c_uint32),
+        ("log_radix", ctypes.c_uint32 * 3),
+        ("log_cols", ctypes.c_uint32 * 3),
+    ]
+
+    def as_dict(self):
+        return {"log_n": self.log_n, "log_expansion": self.log_expansion, "npass": self.npass,
+                "log_radix": list(self.log_radix), "log_cols": list(self.log_cols)}
 
 
 class WhirGpuError(RuntimeError):
@@ -145,6 +164,24 @@ def load() -> ctypes.CDLL:
     L.whirgpu_server_stats.restype = None
     L.whirgpu_server_destroy.argtypes = [p]
     L.whirgpu_server_destroy.restype = None
+    u32 = ctypes.c_uint32
+    L.whirgpu_rs_encode.argtypes = [p, p, sz, u32, u32, u32, p, p]
+    L.whirgpu_rs_commit_batch.argtypes = [p, p, i32, sz, u32, u32, u32, p]
+    L.whirgpu_ntt_autotune.argtypes = [p, u32, u32, u32, u32, ctypes.POINTER(NttPlan),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(u32)]
+    L.whirgpu_ntt_set_plan.argtypes = [ctypes.POINTER(NttPlan)]
+    L.whirgpu_ntt_get_plan.argtypes = [u32, u32, ctypes.POINTER(NttPlan)]
+    L.whirgpu_ntt_clear_plans.argtypes = []
+    L.whirgpu_ntt_clear_plans.restype = None
+    L.whirgpu_ntt_list_plans.argtypes = [ctypes.POINTER(NttPlan), sz]
+    L.whirgpu_ntt_list_plans.restype = sz
+    L.whirgpu_ntt_load_plans.argtypes = [ctypes.c_char_p, ctypes.POINTER(sz)]
+    L.whirgpu_ntt_save_plans.argtypes = [ctypes.c_char_p]
+    L.whirgpu_ntt_load_default_plans.argtypes = []
+    L.whirgpu_ntt_load_default_plans.restype = None
+    for name in ("whirgpu_rs_encode", "whirgpu_rs_commit_batch", "whirgpu_ntt_autotune", "whirgpu_ntt_set_plan",
+                 "whirgpu_ntt_get_plan", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans"):
+        getattr(L, name).restype = i32
     for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
                  "whirgpu_proof_get", "whirgpu_commit", "whirgpu_prove", "whirgpu_mle_evaluate",
                  "whirgpu_mle_evaluate_noalloc", "whirgpu_debug_field_ops", "whirgpu_batch_create",

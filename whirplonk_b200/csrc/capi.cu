@@ -245,6 +245,7 @@ whirgpu_status whirgpu_ctx_create(int device, uint64_t hbm_budget, whirgpu_ctx**
     WG_CUDA(nullptr, cudaSetDevice(device), "cudaSetDevice");
     WG_CUDA(nullptr, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     if (lde_prepare() != 0) return WHIRGPU_E_CUDA;
+    whirgpu_ntt_load_default_plans();
     std::vector<uint64_t> st(1u << (TW_STAGE_LOG - 1)), hi(1u << TW_HALF), lo(1u << TW_HALF);
     host_twiddles(st.data(), hi.data(), lo.data());
     WG_CUDA(nullptr, cudaMalloc(&c->tw.tw_stage, st.size() * 8), "cudaMalloc twiddles");
@@ -268,6 +269,7 @@ void whirgpu_ctx_destroy(whirgpu_ctx* c) {
     cudaFree(c->tw.tw_lo);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->mle_scratch) cudaFree(c->mle_scratch);
+    if (c->kscratch) cudaFree(c->kscratch);
     c->timer.reset();
     cudaStreamDestroy(c->stream);
     delete c;

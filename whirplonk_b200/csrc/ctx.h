@@ -90,6 +90,8 @@ struct whirgpu_ctx {
     size_t pinned_bytes = 0;
     char* mle_scratch = nullptr;
     size_t mle_scratch_bytes = 0;
+    char* kscratch = nullptr;  // kernel-level calls (RS encode/commit, autotuner)
+    size_t kscratch_bytes = 0;
     std::unique_ptr<wg::EventTimer> timer;
     uint64_t stat_launches[wg::FAM_COUNT] = {};
     double stat_ms[wg::FAM_COUNT] = {};

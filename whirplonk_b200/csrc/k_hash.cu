@@ -30,10 +30,15 @@ __device__ __forceinline__ void load_node(const u32* nodes, u64 idx, unsigned* m
 
 // Row i = words w = 0 .. depth*ncomp-1 with w -> (element w / ncomp, component w % ncomp),
 // read from plane (component * depth + element).
+// blockIdx.y selects one of several independent matrices (planes and node
+// arrays `plane_stride` / `node_stride` words apart).
 template <int NCOMP>
-__global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes) {
+__global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes,
+                                                u64 plane_stride, u64 node_stride) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
+    planes += blockIdx.y * plane_stride;
+    nodes += blockIdx.y * node_stride;
     const u32 nwords = depth * NCOMP;           // 64-bit words per row
     const u32 bytes = nwords * 8;
     const u32 nblocks = (bytes + 63) / 64;
@@ -59,14 +64,20 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
     store_node(nodes, i, cv);
 }
 
-int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st) {
+int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
+                       u64 node_stride, cudaStream_t st) {
     if (depth * ncomp * 8 > 1024) return -1;  // multi-chunk BLAKE3 rows are not on this path
-    const unsigned grid = (unsigned)((N + 255) / 256);
-    if (ncomp == 1) k_leaves<1><<<grid, 256, 0, st>>>(planes, N, depth, nodes);
-    else if (ncomp == 3) k_leaves<3><<<grid, 256, 0, st>>>(planes, N, depth, nodes);
+    if (count == 0 || count > 65535) return -1;
+    const dim3 grid((unsigned)((N + 255) / 256), count);
+    if (ncomp == 1) k_leaves<1><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+    else if (ncomp == 3) k_leaves<3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
     else return -1;
     count_launches(1);
     return 0;
+}
+
+int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st) {
+    return launch_leaves_batch(planes, N, depth, ncomp, nodes, 1, 0, 0, st);
 }
 
 __host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
@@ -77,8 +88,10 @@ __host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
 // One CTA hashes a subtree of height `levels` whose children sit at level
 // `level_in`; every produced level is written to global memory.
 __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_in, u32 levels, TxState* tx,
-                                                ProofScalars* sc, int commit_idx, int n_ood, int finish) {
+                                                ProofScalars* sc, int commit_idx, int n_ood, int finish,
+                                                u64 node_stride) {
     __shared__ unsigned buf[2][256 * 8];
+    nodes += blockIdx.y * node_stride;
     if (levels > 0) {
         const u32 nparents = 1u << (levels - 1);
         const u64 in_off = level_offset(logN, level_in);
@@ -113,7 +126,7 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
             cur ^= 1;
         }
     }
-    if (finish && threadIdx.x == 0) {
+    if (finish && tx && threadIdx.x == 0) {
         __threadfence();
         const u64 root = level_offset(logN, logN);
         u64 w[4];
@@ -123,22 +136,37 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
     }
 }
 
-int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, cudaStream_t st) {
+// `count` trees `node_stride` words apart; the transcript step (tx non-null)
+// is for a single tree only.
+static int merkle_levels(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, u32 count,
+                         u64 node_stride, cudaStream_t st) {
+    if (count == 0 || count > 65535 || (tx && count != 1)) return -1;
     u32 level = 0;
     if (logN == 0) {
-        k_merkle<<<1, 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1);
-        count_launches(1);
+        if (tx) {
+            k_merkle<<<dim3(1, count), 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1, node_stride);
+            count_launches(1);
+        }
         return 0;
     }
     while (level < logN) {
         const u32 levels = (logN - level) < 9 ? (logN - level) : 9;
         const u32 ctas = 1u << (logN - level - levels);
         const int finish = (level + levels == logN) ? 1 : 0;
-        k_merkle<<<ctas, 256, 0, st>>>(nodes, logN, level, levels, tx, sc, commit_idx, n_ood, finish);
+        k_merkle<<<dim3(ctas, count), 256, 0, st>>>(nodes, logN, level, levels, tx, sc, commit_idx, n_ood, finish,
+                                                    node_stride);
         count_launches(1);
         level += levels;
     }
     return 0;
+}
+
+int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, cudaStream_t st) {
+    return merkle_levels(nodes, logN, tx, sc, commit_idx, n_ood, 1, 0, st);
+}
+
+int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaStream_t st) {
+    return merkle_levels(nodes, logN, nullptr, nullptr, 0, 0, count, node_stride, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -16,6 +16,8 @@
 // LDE reads m = N/e words per plane), the last pass writes the codeword planes
 // M[plane][i] that the leaf hasher and the opener read.
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 #include "launch.h"
 #include "gl.cuh"
@@ -195,9 +197,10 @@ static u32 pick_w(u32 logR, u64 limit_log) {
     return lw;
 }
 
-LdePlan plan_lde(u32 logN) {
+LdePlan default_plan_lde(u32 logN) {
     LdePlan p{};
     p.logN = logN;
+    p.logW[0] = p.logW[1] = p.logW[2] = LDE_W_AUTO;
     if (logN <= 11) {
         p.npass = 1;
         p.logR[0] = logN;
@@ -218,10 +221,71 @@ LdePlan plan_lde(u32 logN) {
 size_t lde_smem_bytes(u32 logR, u32 logW) {
     return ((size_t)(1u << logW) * col_stride(logR)) * 8 + ((size_t)1 << logR) / 2 * 8 + 16;
 }
+constexpr size_t LDE_SMEM_MAX = 100 * 1024;
 
-int launch_lde(const LdeArgs& L, cudaStream_t st) {
-    const LdePlan pl = plan_lde(L.logN);
-    if (L.logN > TW_LOG || L.planes == 0) return -1;
+// Columns per CTA of pass s: the plan's choice, or tile <= 8192 words with at
+// most 16 columns; never more than the dimension being grouped.
+static u32 pass_logW(const LdePlan& pl, u32 s, u32 logS) {
+    if (pl.npass == 1) return 0;
+    const u32 limit = s + 1 < pl.npass ? logS : pl.logR[0];
+    const u32 w = pl.logW[s] == LDE_W_AUTO ? pick_w(pl.logR[s], limit) : pl.logW[s];
+    return w > limit ? limit : w;
+}
+
+bool lde_plan_valid(const LdePlan& p) {
+    if (p.npass < 1 || p.npass > 3 || p.logN > TW_LOG) return false;
+    u32 sum = 0;
+    for (u32 s = 0; s < p.npass; ++s) {
+        if (p.logR[s] < 1 || p.logR[s] > TW_STAGE_LOG) return false;
+        sum += p.logR[s];
+    }
+    if (sum != p.logN) return false;
+    u32 rest = p.logN;
+    for (u32 s = 0; s < p.npass; ++s) {
+        rest -= p.logR[s];
+        if (p.logW[s] != LDE_W_AUTO && p.logW[s] > 6) return false;
+        if (lde_smem_bytes(p.logR[s], pass_logW(p, s, rest)) > LDE_SMEM_MAX) return false;
+    }
+    return true;
+}
+
+static std::mutex g_plan_mu;
+static std::map<u32, LdePlan> g_plans;  // key logN << 8 | logX
+
+void lde_install_plan(u32 logX, const LdePlan& p) {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    const u32 key = p.logN << 8 | logX;
+    if (p.npass == 0) g_plans.erase(key);
+    else g_plans[key] = p;
+}
+void lde_clear_plans() {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    g_plans.clear();
+}
+size_t lde_installed_plans(u32* keys, LdePlan* plans, size_t cap) {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    size_t i = 0;
+    for (const auto& kv : g_plans) {
+        if (i < cap) {
+            if (keys) keys[i] = kv.first;
+            if (plans) plans[i] = kv.second;
+        }
+        ++i;
+    }
+    return i;
+}
+
+LdePlan plan_lde(u32 logN, u32 logX) {
+    {
+        std::lock_guard<std::mutex> lk(g_plan_mu);
+        auto it = g_plans.find(logN << 8 | logX);
+        if (it != g_plans.end()) return it->second;
+    }
+    return default_plan_lde(logN);
+}
+
+int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
+    if (L.logN > TW_LOG || L.planes == 0 || pl.logN != L.logN || !lde_plan_valid(pl)) return -1;
     NttPassArgs a{};
     for (int c = 0; c < 3; ++c) a.src[c] = L.src[c];
     a.m = L.m;
@@ -241,16 +305,14 @@ int launch_lde(const LdeArgs& L, cudaStream_t st) {
         a.logR = pl.logR[s];
         logrest -= a.logR;
         a.logS = logrest;
+        a.logW = pass_logW(pl, s, a.logS);
         dim3 grid;
         if (s + 1 < pl.npass) {
-            a.logW = pick_w(a.logR, a.logS);
             u64 prefixes = s == 0 ? 1 : (1ull << pl.logR[0]);
             grid = dim3((unsigned)(prefixes << (a.logS - a.logW)), L.planes);
         } else if (pl.npass == 1) {
-            a.logW = 0;
             grid = dim3(1, L.planes);
         } else {
-            a.logW = pick_w(a.logR, pl.logR[0]);
             u64 groups = (1ull << pl.logR[0]) >> a.logW;
             if (pl.npass == 3) groups <<= pl.logR[1];
             grid = dim3((unsigned)groups, L.planes);
@@ -274,8 +336,15 @@ int launch_lde(const LdeArgs& L, cudaStream_t st) {
     return 0;
 }
 
+int launch_lde(const LdeArgs& L, cudaStream_t st) {
+    u32 lm = 0;
+    while ((1ull << lm) < L.m) ++lm;
+    const u32 logX = L.logN > lm ? L.logN - lm : 0;
+    return launch_lde_plan(L, plan_lde(L.logN, logX), st);
+}
+
 int lde_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    cudaError_t e = cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LDE_SMEM_MAX);
     return e == cudaSuccess ? 0 : -1;
 }
 

@@ -17,9 +17,13 @@ struct ProofScalars;
 constexpr u32 TW_LOG = 26, TW_HALF = 13, TW_STAGE_LOG = 11;
 
 // ---- Reed-Solomon encoder -------------------------------------------------
+// A pass plan: npass passes of radix 2^logR[s] (sum = logN, each <= 2^11),
+// pass s staging 2^logW[s] columns per CTA (LDE_W_AUTO: the built-in choice).
+constexpr u32 LDE_W_AUTO = 0xFF;
 struct LdePlan {
     u32 logN, npass;
     u32 logR[3];
+    u32 logW[3];
 };
 struct NttPassArgs {
     const u64* src[3];
@@ -43,7 +47,17 @@ struct LdeArgs {
     const u64* tw_hi;
     const u64* tw_lo;
 };
-LdePlan plan_lde(u32 logN);
+// The plan launch_lde uses for a 2^logN codeword of a 2^logN / 2^logX message:
+// an installed (autotuned) plan for (logN, logX) if there is one, else the
+// built-in split.
+LdePlan plan_lde(u32 logN, u32 logX);
+LdePlan default_plan_lde(u32 logN);
+bool lde_plan_valid(const LdePlan& p);
+void lde_install_plan(u32 logX, const LdePlan& p);  // p.npass == 0 removes
+void lde_clear_plans();
+size_t lde_installed_plans(u32* keys, LdePlan* plans, size_t cap);  // keys: logN << 8 | logX
+// Launches one LDE with an explicit plan (autotuner).
+int launch_lde_plan(const LdeArgs& a, const LdePlan& pl, cudaStream_t st);
 int launch_lde(const LdeArgs& a, cudaStream_t st);
 int lde_prepare();
 
@@ -51,12 +65,18 @@ int lde_prepare();
 // Leaf i = BLAKE3 of row i (LE bytes of `depth` elements of `ncomp` words),
 // written to nodes[i].  Rows are gathered from the codeword planes.
 int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st);
+// `count` independent matrices: planes and node arrays `plane_stride` /
+// `node_stride` words apart.
+int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
+                        u64 node_stride, cudaStream_t st);
 // Builds all Merkle levels above the leaves of a 2^logN-leaf tree in `nodes`
 // ([leaves | level 1 | ... | root], 8 words per node).  The CTA that computes
 // the root also performs the transcript step of irs_commit::commit
 // (irs_commit.hpp:433-478): prover_message(root), then squeezes `n_ood`
 // Ext3 out-of-domain points into sc->ood_pts[commit_idx].
 int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, cudaStream_t st);
+// Tree levels only (no transcript) of `count` trees `node_stride` words apart.
+int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaStream_t st);
 
 // ---- Out-of-domain evaluation ----------------------------------------------
 // value_j = sum_i v_i z_j^i for z_j = sc->ood_pts[commit_idx][j]; the last CTA
