@@ -192,12 +192,15 @@ whirgpu_status whirgpu_rs_commit_batch(whirgpu_ctx* ctx, const uint64_t* vectors
 /* ---- NTT pass plans (autotuned) ------------------------------------------------- */
 /* The LDE of a 2^log_n codeword from a 2^(log_n - log_expansion) message runs in
  * npass passes of radix 2^log_radix[s] (sum = log_n, each <= 11); pass s stages
- * 2^log_cols[s] columns per CTA (255 = built-in choice).  No counterpart in the
- * reference (its NTT engine picks fixed radices, cooley_tukey.hpp:200-259). */
+ * 2^log_cols[s] columns per CTA (255 = built-in choice); the kernel variant's
+ * registers are sized for min_blocks CTAs per SM (2..4, 0 = built-in).  No
+ * counterpart in the reference (its NTT engine picks fixed radices,
+ * cooley_tukey.hpp:200-259). */
 typedef struct {
     uint32_t log_n, log_expansion, npass;
     uint32_t log_radix[3];
     uint32_t log_cols[3];
+    uint32_t min_blocks;
 } whirgpu_ntt_plan;
 /* Times every valid plan for the shape on `planes` synthetic planes (median of
  * `reps` runs each), checks each plan's codeword against the built-in plan's,

@@ -90,11 +90,12 @@ class NttPlan(ctypes.Structure):
         ("npass", ctypes.c_uint32),
         ("log_radix", ctypes.c_uint32 * 3),
         ("log_cols", ctypes.c_uint32 * 3),
+        ("min_blocks", ctypes.c_uint32),
     ]
 
     def as_dict(self):
         return {"log_n": self.log_n, "log_expansion": self.log_expansion, "npass": self.npass,
-                "log_radix": list(self.log_radix), "log_cols": list(self.log_cols)}
+                "log_radix": list(self.log_radix), "log_cols": list(self.log_cols), "min_blocks": self.min_blocks}
 
 
 class WhirGpuError(RuntimeError):

@@ -75,7 +75,10 @@ __device__ __forceinline__ u64 twiddle(u64 e, u32 logM, const u64* hi, const u64
     return gl_mul(hi[E >> TW_HALF], lo[E & ((1ull << TW_HALF) - 1)]);
 }
 
-__global__ void __launch_bounds__(256, 2) k_ntt_pass(NttPassArgs a) {
+// One pass over all planes (blockIdx.y = plane).  MINB = CTAs per SM the
+// register allocation is sized for (the pass plan picks the variant).
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     extern __shared__ u64 sm[];
     const u32 logR = a.logR, R = 1u << logR, W = 1u << a.logW, halfR = R >> 1;
     const u32 tileN = W << logR;
@@ -116,17 +119,21 @@ __global__ void __launch_bounds__(256, 2) k_ntt_pass(NttPassArgs a) {
     const u32 logE = a.logE, E = 1u << logE;
     const u32 mrows_log = logR - logE;
     if (!last) {
-        const u32 n = W << mrows_log;
-        for (u32 e = threadIdx.x; e < n; e += blockDim.x) {
-            const u32 w = e & (W - 1), j = e >> a.logW;
-            u64 v;
-            if (first) {
-                const u64 idx = (u64)j * S + col0 + w;
-                v = idx < a.m ? src[idx] : 0;
-            } else {
-                v = tmp[(P * R + j) * S + col0 + w];
-            }
-            sm[w * cs + pidx(bitrev(j, logR))] = v;
+        // Thread t always serves column w = t mod W; its rows advance by J.
+        const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
+        const u32 nrows = 1u << mrows_log;
+        u64* col = sm + w * cs;
+        if (first) {
+            const u64 stride = (u64)J * S;
+            u64 idx = (u64)(threadIdx.x >> a.logW) * S + col0 + w;
+#pragma unroll 4
+            for (u32 j = threadIdx.x >> a.logW; j < nrows; j += J, idx += stride)
+                col[pidx(bitrev(j, logR))] = idx < a.m ? src[idx] : 0;
+        } else {
+            const u64 stride = (u64)J * S;
+            const u64* p = tmp + (P * R + (threadIdx.x >> a.logW)) * S + col0 + w;
+#pragma unroll 4
+            for (u32 j = threadIdx.x >> a.logW; j < nrows; j += J, p += stride) col[pidx(bitrev(j, logR))] = *p;
         }
     } else {
         const u32 n = W << mrows_log;
@@ -145,9 +152,19 @@ __global__ void __launch_bounds__(256, 2) k_ntt_pass(NttPassArgs a) {
     }
     __syncthreads();
     if (logE) {
-        for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
-            const u32 w = e >> logR, p = e & (R - 1);
-            if (p & (E - 1)) sm[w * cs + pidx(p)] = sm[w * cs + pidx(p & ~(E - 1))];
+        const u32 nblk = W << mrows_log;  // blocks of E words, head at a multiple of E
+        if (E >= 8 && nblk >= blockDim.x) {
+            for (u32 b = threadIdx.x; b < nblk; b += blockDim.x) {
+                u64* col = sm + (b >> mrows_log) * cs;
+                const u32 p0 = (b & ((1u << mrows_log) - 1)) << logE;
+                const u64 v = col[pidx(p0)];
+                for (u32 k = 1; k < E; ++k) col[pidx(p0 + k)] = v;
+            }
+        } else {
+            for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
+                const u32 w = e >> logR, p = e & (R - 1);
+                if (p & (E - 1)) sm[w * cs + pidx(p)] = sm[w * cs + pidx(p & ~(E - 1))];
+            }
         }
         __syncthreads();
     }
@@ -166,22 +183,33 @@ __global__ void __launch_bounds__(256, 2) k_ntt_pass(NttPassArgs a) {
 
     // Store.
     if (!last) {
+        // Inter-pass twiddle w_{Ns}^(col i): thread t keeps col fixed and steps i
+        // by J, so the twiddle advances by the constant factor w_{Ns}^(col J).
         const u32 logNs = logR + a.logS;  // size of the sub-transform this pass belongs to
-        for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
-            const u32 w = e & (W - 1), i = e >> a.logW;
-            const u64 col = col0 + w;
-            u64 v = sm[w * cs + pidx(i)];
-            v = gl_mul(v, twiddle(col * i, logNs, a.tw_hi, a.tw_lo));
-            tmp[(P * R + i) * S + col] = v;
+        const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
+        const u64 col = col0 + w;
+        u32 i = threadIdx.x >> a.logW;
+        u64 tw = twiddle(col * i, logNs, a.tw_hi, a.tw_lo);
+        const u64 step = twiddle(col * J, logNs, a.tw_hi, a.tw_lo);
+        const u64 stride = (u64)J * S;
+        u64* dst = tmp + (P * R + i) * S + col;
+        const u64* scol = sm + w * cs;
+#pragma unroll 2
+        for (; i < R; i += J, dst += stride) {
+            *dst = gl_mul(scol[pidx(i)], tw);
+            tw = gl_mul(tw, step);
         }
     } else {
         u64* out = a.out + (u64)plane * N;
         const u64 outer = N >> logR;
         const u64 obase = a.npass == 3 ? i0base + ((u64)i1 << a.logR0) : i0base;
-        for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
-            const u32 w = e & (W - 1), i = e >> a.logW;
-            out[obase + w + outer * i] = sm[w * cs + pidx(i)];
-        }
+        const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
+        const u64* scol = sm + w * cs;
+        u32 i = threadIdx.x >> a.logW;
+        u64* dst = out + obase + w + outer * i;
+        const u64 stride = outer * J;
+#pragma unroll 4
+        for (; i < R; i += J, dst += stride) *dst = scol[pidx(i)];
     }
 }
 
@@ -234,6 +262,7 @@ static u32 pass_logW(const LdePlan& pl, u32 s, u32 logS) {
 
 bool lde_plan_valid(const LdePlan& p) {
     if (p.npass < 1 || p.npass > 3 || p.logN > TW_LOG) return false;
+    if (p.minb != 0 && (p.minb < 2 || p.minb > 4)) return false;
     u32 sum = 0;
     for (u32 s = 0; s < p.npass; ++s) {
         if (p.logR[s] < 1 || p.logR[s] > TW_STAGE_LOG) return false;
@@ -243,7 +272,7 @@ bool lde_plan_valid(const LdePlan& p) {
     u32 rest = p.logN;
     for (u32 s = 0; s < p.npass; ++s) {
         rest -= p.logR[s];
-        if (p.logW[s] != LDE_W_AUTO && p.logW[s] > 6) return false;
+        if (p.logW[s] != LDE_W_AUTO && p.logW[s] > 6) return false;  // blockDim (256) must be a multiple of W
         if (lde_smem_bytes(p.logR[s], pass_logW(p, s, rest)) > LDE_SMEM_MAX) return false;
     }
     return true;
@@ -330,7 +359,10 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
             a.logE = a.logR > lr ? a.logR - lr : 0;
         }
         size_t smem = lde_smem_bytes(a.logR, a.logW);
-        k_ntt_pass<<<grid, 256, smem, st>>>(a);
+        const u32 mb = pl.minb ? pl.minb : LDE_MINB_DEFAULT;
+        if (mb == 2) k_ntt_pass<2><<<grid, 256, smem, st>>>(a);
+        else if (mb == 4) k_ntt_pass<4><<<grid, 256, smem, st>>>(a);
+        else k_ntt_pass<3><<<grid, 256, smem, st>>>(a);
         count_launches(1);
     }
     return 0;
@@ -344,8 +376,10 @@ int launch_lde(const LdeArgs& L, cudaStream_t st) {
 }
 
 int lde_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LDE_SMEM_MAX);
-    return e == cudaSuccess ? 0 : -1;
+    for (auto f : {k_ntt_pass<2>, k_ntt_pass<3>, k_ntt_pass<4>})
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LDE_SMEM_MAX) != cudaSuccess)
+            return -1;
+    return 0;
 }
 
 }  // namespace wg

@@ -199,20 +199,22 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
         if (lde_plan_valid(p)) cand.push_back(p);
     };
     const u32 A = LDE_W_AUTO;
-    const u32 wopts[] = {A, 0, 1, 2, 3, 4, 5};
-    if (log_n <= 11) add(LdePlan{log_n, 1, {log_n, 0, 0}, {A, A, A}});
-    for (u32 r0 = 1; r0 < log_n && r0 <= 11; ++r0) {
-        const u32 r1 = log_n - r0;
-        if (r1 > 11) continue;
-        for (u32 w0 : wopts)
-            for (u32 w1 : wopts) add(LdePlan{log_n, 2, {r0, r1, 0}, {w0, w1, A}});
+    const u32 wopts[] = {A, 1, 2, 3, 4};
+    for (u32 mb = 2; mb <= 4; ++mb) {
+        if (log_n <= 11) add(LdePlan{log_n, 1, {log_n, 0, 0}, {A, A, A}, mb});
+        for (u32 r0 = 1; r0 < log_n && r0 <= 11; ++r0) {
+            const u32 r1 = log_n - r0;
+            if (r1 > 11) continue;
+            for (u32 w0 : wopts)
+                for (u32 w1 : wopts) add(LdePlan{log_n, 2, {r0, r1, 0}, {w0, w1, A}, mb});
+        }
+        if (log_n >= 12)
+            for (u32 r0 = 1; r0 <= 11; ++r0)
+                for (u32 r1 = 1; r1 <= 11 && r0 + r1 < log_n; ++r1) {
+                    const u32 r2 = log_n - r0 - r1;
+                    if (r2 >= 1 && r2 <= 11) add(LdePlan{log_n, 3, {r0, r1, r2}, {A, A, A}, mb});
+                }
     }
-    if (log_n >= 12)
-        for (u32 r0 = 1; r0 <= 11; ++r0)
-            for (u32 r1 = 1; r1 <= 11 && r0 + r1 < log_n; ++r1) {
-                const u32 r2 = log_n - r0 - r1;
-                if (r2 >= 1 && r2 <= 11) add(LdePlan{log_n, 3, {r0, r1, r2}, {A, A, A}});
-            }
     if (cand.empty()) return fail(c, WHIRGPU_E_INVALID, "no valid plan");
 
     unsigned long long want = 0;
@@ -256,6 +258,7 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
     best->log_n = log_n;
     best->log_expansion = log_expansion;
     best->npass = best_p.npass;
+    best->min_blocks = best_p.minb;
     for (int k = 0; k < 3; ++k) {
         best->log_radix[k] = best_p.logR[k];
         best->log_cols[k] = best_p.logW[k];
@@ -271,6 +274,7 @@ whirgpu_status whirgpu_ntt_set_plan(const whirgpu_ntt_plan* p) {
     LdePlan q{};
     q.logN = p->log_n;
     q.npass = p->npass;
+    q.minb = p->min_blocks;
     for (int k = 0; k < 3; ++k) {
         q.logR[k] = k < (int)p->npass ? p->log_radix[k] : 0;
         q.logW[k] = k < (int)p->npass ? p->log_cols[k] : LDE_W_AUTO;
@@ -286,6 +290,7 @@ whirgpu_status whirgpu_ntt_get_plan(uint32_t log_n, uint32_t log_expansion, whir
     out->log_n = log_n;
     out->log_expansion = log_expansion;
     out->npass = p.npass;
+    out->min_blocks = p.minb;
     for (int k = 0; k < 3; ++k) {
         out->log_radix[k] = p.logR[k];
         out->log_cols[k] = p.logW[k];
@@ -303,6 +308,7 @@ size_t whirgpu_ntt_list_plans(whirgpu_ntt_plan* out, size_t cap) {
         out[i].log_n = keys[i] >> 8;
         out[i].log_expansion = keys[i] & 0xFF;
         out[i].npass = plans[i].npass;
+        out[i].min_blocks = plans[i].minb;
         for (int k = 0; k < 3; ++k) {
             out[i].log_radix[k] = plans[i].logR[k];
             out[i].log_cols[k] = plans[i].logW[k];
@@ -312,8 +318,9 @@ size_t whirgpu_ntt_list_plans(whirgpu_ntt_plan* out, size_t cap) {
 }
 
 // Plan files: {"plans": [{"log_n": 22, "log_expansion": 2, "npass": 2,
-//   "log_radix": [11, 11, 0], "log_cols": [2, 2, 255]}, ...]} -- the objects of the
-// "plans" array are read by key; anything else in the file is ignored.
+//   "log_radix": [11, 11, 0], "log_cols": [2, 2, 255], "min_blocks": 3}, ...]} --
+// the objects of the "plans" array are read by key (min_blocks optional);
+// anything else in the file is ignored.
 static bool read_int_field(const std::string& obj, const char* key, long* out) {
     const std::string k = std::string("\"") + key + "\"";
     size_t p = obj.find(k);
@@ -362,7 +369,10 @@ whirgpu_status whirgpu_ntt_load_plans(const char* path, size_t* loaded) {
         if (!read_int_field(obj, "log_n", &ln) || !read_int_field(obj, "log_expansion", &lx) ||
             !read_int_field(obj, "npass", &np) || !read_triple(obj, "log_radix", r) || !read_triple(obj, "log_cols", w))
             continue;
+        long mb = 0;
+        read_int_field(obj, "min_blocks", &mb);  // optional
         whirgpu_ntt_plan pl{};
+        pl.min_blocks = (uint32_t)mb;
         pl.log_n = (uint32_t)ln;
         pl.log_expansion = (uint32_t)lx;
         pl.npass = (uint32_t)np;
@@ -388,9 +398,9 @@ whirgpu_status whirgpu_ntt_save_plans(const char* path) {
         const auto& p = v[i];
         std::fprintf(f,
                      "  {\"log_n\": %u, \"log_expansion\": %u, \"npass\": %u, \"log_radix\": [%u, %u, %u], "
-                     "\"log_cols\": [%u, %u, %u]}%s\n",
+                     "\"log_cols\": [%u, %u, %u], \"min_blocks\": %u}%s\n",
                      p.log_n, p.log_expansion, p.npass, p.log_radix[0], p.log_radix[1], p.log_radix[2], p.log_cols[0],
-                     p.log_cols[1], p.log_cols[2], i + 1 < v.size() ? "," : "");
+                     p.log_cols[1], p.log_cols[2], p.min_blocks, i + 1 < v.size() ? "," : "");
     }
     std::fprintf(f, "]}\n");
     std::fclose(f);

@@ -19,11 +19,13 @@ constexpr u32 TW_LOG = 26, TW_HALF = 13, TW_STAGE_LOG = 11;
 // ---- Reed-Solomon encoder -------------------------------------------------
 // A pass plan: npass passes of radix 2^logR[s] (sum = logN, each <= 2^11),
 // pass s staging 2^logW[s] columns per CTA (LDE_W_AUTO: the built-in choice).
-constexpr u32 LDE_W_AUTO = 0xFF;
+// minb: CTAs per SM the kernel's registers are sized for (2, 3 or 4; 0 = default).
+constexpr u32 LDE_W_AUTO = 0xFF, LDE_MINB_DEFAULT = 3;
 struct LdePlan {
     u32 logN, npass;
     u32 logR[3];
     u32 logW[3];
+    u32 minb;
 };
 struct NttPassArgs {
     const u64* src[3];
