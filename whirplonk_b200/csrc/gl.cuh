@@ -184,6 +184,33 @@ __device__ __forceinline__ Acc192 acc_product(u64 a, u64 b) {
     x.w2 = 0;
     return x;
 }
+// x += a * b with the full 128-bit product formed on 32-bit limbs.
+__device__ __forceinline__ void acc_mac(Acc192& x, u64 a, u64 b) {
+    unsigned r0, r1, r2, r3;
+    asm("mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "addc.u32 %3, %3, 0;"
+        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
+        : "r"((unsigned)a), "r"((unsigned)(a >> 32)), "r"((unsigned)b), "r"((unsigned)(b >> 32)));
+    asm("add.cc.u64 %0, %0, %3;\n\t"
+        "addc.cc.u64 %1, %1, %4;\n\t"
+        "addc.u64 %2, %2, 0;"
+        : "+l"(x.w0), "+l"(x.w1), "+l"(x.w2)
+        : "l"(((u64)r1 << 32) | r0), "l"(((u64)r3 << 32) | r2));
+}
+__device__ __forceinline__ void acc_add(Acc192& x, const Acc192& y) {
+    asm("add.cc.u64 %0, %0, %3;\n\t"
+        "addc.cc.u64 %1, %1, %4;\n\t"
+        "addc.u64 %2, %2, %5;"
+        : "+l"(x.w0), "+l"(x.w1), "+l"(x.w2)
+        : "l"(y.w0), "l"(y.w1), "l"(y.w2));
+}
 __device__ __forceinline__ void acc_double(Acc192& x) {
     x.w2 = (x.w2 << 1) | (x.w1 >> 63);
     x.w1 = (x.w1 << 1) | (x.w0 >> 63);
@@ -209,6 +236,36 @@ __device__ __forceinline__ E3 e3_mul(E3 a, E3 b) {
     acc_mul(s2, a.c1, b.c1);
     acc_mul(s2, a.c2, b.c0);
     return E3{acc_reduce(s0), acc_reduce(s1), acc_reduce(s2)};
+}
+// Delayed-reduction Ext3 multiply-accumulate: sum a_k b_k over many k, reduced once.
+struct E3Acc {
+    Acc192 s0, s1, s2;  // plain terms of c0, c1, c2
+    Acc192 d0, d1;      // terms of c0, c1 that carry the factor 2 of X^3 = 2
+};
+__device__ __forceinline__ E3Acc e3acc_zero() { return E3Acc{{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}; }
+__device__ __forceinline__ void e3acc_mac(E3Acc& x, const E3& a, const E3& b) {
+    acc_mac(x.s0, a.c0, b.c0);
+    acc_mac(x.d0, a.c1, b.c2);
+    acc_mac(x.d0, a.c2, b.c1);
+    acc_mac(x.s1, a.c0, b.c1);
+    acc_mac(x.s1, a.c1, b.c0);
+    acc_mac(x.d1, a.c2, b.c2);
+    acc_mac(x.s2, a.c0, b.c2);
+    acc_mac(x.s2, a.c1, b.c1);
+    acc_mac(x.s2, a.c2, b.c0);
+}
+__device__ __forceinline__ void e3acc_mac_base(E3Acc& x, const E3& a, u64 b) {
+    acc_mac(x.s0, a.c0, b);
+    acc_mac(x.s1, a.c1, b);
+    acc_mac(x.s2, a.c2, b);
+}
+// Valid while every accumulator's top word stays below 2^31 (< 2^31 products).
+__device__ __forceinline__ E3 e3acc_reduce(E3Acc x) {
+    acc_double(x.d0);
+    acc_double(x.d1);
+    acc_add(x.s0, x.d0);
+    acc_add(x.s1, x.d1);
+    return E3{acc_reduce(x.s0), acc_reduce(x.s1), acc_reduce(x.s2)};
 }
 __device__ __forceinline__ E3 e3_mul_base(E3 a, u64 b) { return E3{gl_mul(a.c0, b), gl_mul(a.c1, b), gl_mul(a.c2, b)}; }
 __device__ __forceinline__ E3 e3_pow(E3 b, u64 e) {

@@ -10,6 +10,8 @@
 // Merkle tree (merkle_tree.hpp:104-147): parent = BLAKE3(left || right),
 // node array [leaves | level 1 | ... | root].  A CTA hashes a 512-leaf subtree
 // (9 levels) in shared memory, so a 2^22-leaf tree takes three launches.
+#include <algorithm>
+
 #include "launch.h"
 #include "blake3.cuh"
 #include "state.cuh"
@@ -171,12 +173,16 @@ int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaSt
 
 // ---------------------------------------------------------------------------
 // Out-of-domain evaluation: value_j = sum_i v_i z_j^i
-// (irs_commit.hpp:472-554 -> utilities.hpp:196-246).  Thread g of T handles
-// i = g + T e with running power z^g (z^T)^e; exact field sums, so the
-// association order is free.  The last CTA (ticket) finishes the sums and sends
-// the values as prover messages.
+// (irs_commit.hpp:472-554 -> utilities.hpp:196-246).  With i = h 2^LO + l,
+//   value_j = sum_h z_j^(h 2^LO) * sum_l v_(h,l) z_j^l :
+// a warp owns whole blocks of 2^LO consecutive coefficients and accumulates
+// the inner sum as unreduced 192-bit products against the table z_j^l, reduces
+// once per block and scales by the table entry z_j^(h 2^LO).  Exact field
+// sums, so the association order is free.  The last CTA (ticket) finishes the
+// sums and sends the values as prover messages.
 // ---------------------------------------------------------------------------
 constexpr int OOD_GRID = 592, OOD_THREADS = 256;
+constexpr u32 OOD_LO = 10;
 
 __device__ __forceinline__ E3 block_sum_e3(E3 v, E3* red) {
     v = e3_warp_sum(v);
@@ -190,22 +196,42 @@ __device__ __forceinline__ E3 block_sum_e3(E3 v, E3* red) {
     return r;  // valid in thread 0
 }
 
+static u32 ood_hi_count(u64 size) { return (u32)((size + (1ull << OOD_LO) - 1) >> OOD_LO); }
+
+// tab[j]: z_j^l for l < 2^LO, then z_j^(h 2^LO) for h < hi_count.
+__global__ void k_ood_tables(const ProofScalars* sc, int commit_idx, int n_ood, u32 hi_count, E3* tab) {
+    const u32 per = (1u << OOD_LO) + hi_count;
+    const u64 total = (u64)per * n_ood;
+    for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
+        const u32 j = (u32)(e / per), k = (u32)(e % per);
+        const E3 z = sc->ood_pts[commit_idx][j];
+        tab[e] = k < (1u << OOD_LO) ? e3_pow(z, k) : e3_pow(z, (u64)(k - (1u << OOD_LO)) << OOD_LO);
+    }
+}
+
 __global__ void __launch_bounds__(OOD_THREADS) k_ood(const u64* v0, const u64* v1, const u64* v2, int ext3, u64 size,
                                                      TxState* tx, ProofScalars* sc, int commit_idx, int n_ood,
-                                                     E3* partials, unsigned* counter) {
+                                                     const E3* tab, u32 hi_count, E3* partials, unsigned* counter) {
     __shared__ E3 red[32];
     __shared__ bool is_last;
-    const u64 T = (u64)gridDim.x * blockDim.x;
-    const u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 lane = threadIdx.x & 31;
+    const u64 gw = (u64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const u64 nw = (u64)gridDim.x * (blockDim.x >> 5);
+    const u32 per = (1u << OOD_LO) + hi_count;
     for (int j = 0; j < n_ood; ++j) {
-        const E3 z = sc->ood_pts[commit_idx][j];
-        E3 p = e3_pow(z, g);
-        const E3 zT = e3_pow(z, T);
+        const E3* zlo = tab + (u64)j * per;
+        const E3* zhi = zlo + (1u << OOD_LO);
         E3 acc = e3_zero();
-        for (u64 i = g; i < size; i += T) {
-            if (ext3) acc = e3_add(acc, e3_mul(E3{v0[i], v1[i], v2[i]}, p));
-            else acc = e3_add(acc, e3_mul_base(p, v0[i]));
-            p = e3_mul(p, zT);
+        for (u64 h = gw; h < hi_count; h += nw) {
+            const u64 base = h << OOD_LO;
+            const u32 cnt = (u32)((size - base) < (1ull << OOD_LO) ? (size - base) : (1ull << OOD_LO));
+            E3Acc s = e3acc_zero();
+            if (ext3) {
+                for (u32 l = lane; l < cnt; l += 32) e3acc_mac(s, zlo[l], E3{v0[base + l], v1[base + l], v2[base + l]});
+            } else {
+                for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], v0[base + l]);
+            }
+            acc = e3_add(acc, e3_mul(e3acc_reduce(s), zhi[h]));
         }
         E3 bs = block_sum_e3(acc, red);
         if (threadIdx.x == 0) partials[blockIdx.x * MAX_OOD + j] = bs;
@@ -232,17 +258,28 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(const u64* v0, const u64* v
     if (threadIdx.x == 0) *counter = 0;
 }
 
-size_t ood_scratch_bytes() { return (size_t)OOD_GRID * MAX_OOD * sizeof(E3) + 256; }
+size_t ood_scratch_bytes(u64 max_size) {
+    return 256 + (size_t)OOD_GRID * MAX_OOD * sizeof(E3) +
+           (size_t)MAX_OOD * ((1u << OOD_LO) + ood_hi_count(max_size)) * sizeof(E3);
+}
 
 int launch_ood(const u64* v0, const u64* v1, const u64* v2, bool ext3, u64 size, TxState* tx, ProofScalars* sc,
                int commit_idx, int n_ood, void* scratch, cudaStream_t st) {
     if (n_ood <= 0) return 0;
-    if (n_ood > MAX_OOD) return -1;
-    u64 want = (size + OOD_THREADS * 8 - 1) / (OOD_THREADS * 8);
+    if (n_ood > MAX_OOD || size == 0) return -1;
+    const u32 hc = ood_hi_count(size);
+    char* base = reinterpret_cast<char*>(scratch);
+    unsigned* counter = reinterpret_cast<unsigned*>(base);
+    E3* partials = reinterpret_cast<E3*>(base + 256);
+    E3* tab = partials + (size_t)OOD_GRID * MAX_OOD;
+    const u64 entries = (u64)((1u << OOD_LO) + hc) * n_ood;
+    k_ood_tables<<<(unsigned)std::min<u64>(296, (entries + 255) / 256), 256, 0, st>>>(sc, commit_idx, n_ood, hc, tab);
+    count_launches(1);
+    const u64 warps_per_cta = OOD_THREADS / 32;
+    u64 want = (hc + warps_per_cta - 1) / warps_per_cta;
     unsigned grid = (unsigned)(want < 1 ? 1 : (want > OOD_GRID ? OOD_GRID : want));
-    E3* partials = reinterpret_cast<E3*>(scratch);
-    unsigned* counter = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(scratch) + (size_t)OOD_GRID * MAX_OOD * sizeof(E3));
-    k_ood<<<grid, OOD_THREADS, 0, st>>>(v0, v1, v2, ext3 ? 1 : 0, size, tx, sc, commit_idx, n_ood, partials, counter);
+    k_ood<<<grid, OOD_THREADS, 0, st>>>(v0, v1, v2, ext3 ? 1 : 0, size, tx, sc, commit_idx, n_ood, tab, hc, partials,
+                                        counter);
     count_launches(1);
     return 0;
 }

@@ -18,6 +18,10 @@
 namespace wg {
 
 constexpr int SC_THREADS = 256, SC_GRID = 148 * 4;
+// CTAs per SM the round kernel's registers are sized for.
+#ifndef SC_MINB
+#define SC_MINB 3
+#endif
 
 __device__ __forceinline__ E3 block_sum(E3 v, E3* red) {
     v = e3_warp_sum(v);
@@ -64,7 +68,7 @@ __device__ __forceinline__ E3 load_b(const ScKernelArgs& a, u64 i, const E3& r) 
     return e3_add(y0, e3_mul(r, e3_sub(y1, y0)));
 }
 
-__global__ void __launch_bounds__(SC_THREADS) k_sumcheck_round(ScKernelArgs a) {
+__global__ void __launch_bounds__(SC_THREADS, SC_MINB) k_sumcheck_round(ScKernelArgs a) {
     __shared__ E3 red[32];
     __shared__ bool is_last;
     const E3 r = a.fold ? a.sc->sc_r[a.fold_r] : e3_zero();
@@ -244,8 +248,9 @@ __global__ void __launch_bounds__(256) k_cov_init(CovInitArgs a, const E3* tab) 
     const u64 S = 1ull << a.logS;
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < S; i += (u64)gridDim.x * blockDim.x) {
         const u32 hi = (u32)(i >> lo_bits), lo = (u32)(i & (nlo - 1));
-        E3 acc = e3_zero();
-        for (int t = 0; t < nterms; ++t) acc = e3_add(acc, e3_mul(tab[(u64)t * per + nlo + hi], tab[(u64)t * per + lo]));
+        E3Acc s = e3acc_zero();
+        for (int t = 0; t < nterms; ++t) e3acc_mac(s, tab[(u64)t * per + nlo + hi], tab[(u64)t * per + lo]);
+        const E3 acc = e3acc_reduce(s);
         a.cov[0][i] = acc.c0;
         a.cov[1][i] = acc.c1;
         a.cov[2][i] = acc.c2;
@@ -277,11 +282,12 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // STIR covector update: cov[i] += sum_j rlc_j z_j^i for the round's OOD points
-// (Ext3) and in-domain points (base field, lifted).  Thread-contiguous chunks
-// of CA_E elements: start power from two tables (z^(hi 2^LO), z^lo), then one
-// multiplication per step.
+// (Ext3) and in-domain points (base field, lifted).  With i = h 2^LO + l the
+// tables hold T_j[h] = rlc_j z_j^(h 2^LO) (Ext3) and z_j^l; an element's sum
+// over the points is accumulated as unreduced 192-bit products (3 per base
+// point, 9 per Ext3 point) and reduced once.
 // ---------------------------------------------------------------------------
-constexpr u32 CA_E = 8, CA_LO = 10;
+constexpr u32 CA_LO = 10;
 
 __global__ void k_cov_acc_tables(const ProofScalars* sc, int n_points, u32 hi_count, E3* tab) {
     const u32 per = (1u << CA_LO) + hi_count;
@@ -289,51 +295,24 @@ __global__ void k_cov_acc_tables(const ProofScalars* sc, int n_points, u32 hi_co
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 j = (u32)(e / per), k = (u32)(e % per);
         const E3 z = sc->stir_pts[j];
-        tab[e] = k < (1u << CA_LO) ? e3_pow(z, k) : e3_pow(z, (u64)(k - (1u << CA_LO)) << CA_LO);
+        tab[e] = k < (1u << CA_LO) ? e3_pow(z, k)
+                                   : e3_mul(sc->stir_rlc[j], e3_pow(z, (u64)(k - (1u << CA_LO)) << CA_LO));
     }
 }
 
 __global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* tab, u32 hi_count) {
     const u32 per = (1u << CA_LO) + hi_count;
     const int npts = a.n_ext + a.n_base;
-    const u64 nchunks = (a.size + CA_E - 1) / CA_E;
-    for (u64 ch = (u64)blockIdx.x * blockDim.x + threadIdx.x; ch < nchunks; ch += (u64)gridDim.x * blockDim.x) {
-        const u64 i0 = ch * CA_E;
-        const u32 cnt = (u32)((a.size - i0) < CA_E ? (a.size - i0) : CA_E);
-        E3 acc[CA_E];
-#pragma unroll
-        for (u32 e = 0; e < CA_E; ++e) acc[e] = e3_zero();
-        const u32 hi = (u32)(i0 >> CA_LO), lo = (u32)(i0 & ((1u << CA_LO) - 1));
-        for (int j = 0; j < npts; ++j) {
-            const E3 s = a.sc->stir_rlc[j];
-            const E3* tj = tab + (u64)j * per;
-            if (j < a.n_ext) {
-                const E3 z = a.sc->stir_pts[j];
-                E3 p = e3_mul(s, e3_mul(tj[(1u << CA_LO) + hi], tj[lo]));
-#pragma unroll
-                for (u32 e = 0; e < CA_E; ++e) {
-                    acc[e] = e3_add(acc[e], p);
-                    p = e3_mul(p, z);
-                }
-            } else {
-                const u64 z = a.sc->stir_pts[j].c0;
-                u64 w = gl_mul(tj[(1u << CA_LO) + hi].c0, tj[lo].c0);
-#pragma unroll
-                for (u32 e = 0; e < CA_E; ++e) {
-                    acc[e] = e3_add(acc[e], e3_mul_base(s, w));
-                    w = gl_mul(w, z);
-                }
-            }
-        }
-#pragma unroll
-        for (u32 e = 0; e < CA_E; ++e) {
-            if (e < cnt) {
-                const u64 i = i0 + e;
-                a.cov[0][i] = gl_add(a.cov[0][i], acc[e].c0);
-                a.cov[1][i] = gl_add(a.cov[1][i], acc[e].c1);
-                a.cov[2][i] = gl_add(a.cov[2][i], acc[e].c2);
-            }
-        }
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.size; i += (u64)gridDim.x * blockDim.x) {
+        const u32 hi = (u32)(i >> CA_LO), lo = (u32)(i & ((1u << CA_LO) - 1));
+        E3Acc s = e3acc_zero();
+        const E3* tj = tab;
+        for (int j = 0; j < a.n_ext; ++j, tj += per) e3acc_mac(s, tj[(1u << CA_LO) + hi], tj[lo]);
+        for (int j = a.n_ext; j < npts; ++j, tj += per) e3acc_mac_base(s, tj[(1u << CA_LO) + hi], tj[lo].c0);
+        const E3 add = e3acc_reduce(s);
+        a.cov[0][i] = gl_add(a.cov[0][i], add.c0);
+        a.cov[1][i] = gl_add(a.cov[1][i], add.c1);
+        a.cov[2][i] = gl_add(a.cov[2][i], add.c2);
     }
 }
 
@@ -348,10 +327,9 @@ int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
     if (npts == 0 || a.size == 0) return 0;
     const u32 hc = ca_hi_count(a.size);
     E3* tab = reinterpret_cast<E3*>(a.scratch);
-    k_cov_acc_tables<<<148, 256, 0, st>>>(a.sc, npts, hc, tab);
+    k_cov_acc_tables<<<296, 256, 0, st>>>(a.sc, npts, hc, tab);
     count_launches(1);
-    const u64 nchunks = (a.size + CA_E - 1) / CA_E;
-    u64 want = (nchunks + 255) / 256;
+    u64 want = (a.size + 255) / 256;
     k_cov_accumulate<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab, hc);
     count_launches(1);
     return 0;

@@ -86,7 +86,7 @@ int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaSt
 // sc->ood_vals[commit_idx].
 int launch_ood(const u64* v0, const u64* v1, const u64* v2, bool ext3, u64 size, TxState* tx, ProofScalars* sc,
                int commit_idx, int n_ood, void* scratch, cudaStream_t st);
-size_t ood_scratch_bytes();
+size_t ood_scratch_bytes(u64 max_size);
 
 // ---- Transcript / protocol steps (single-thread kernels) ---------------------
 int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,

@@ -81,7 +81,7 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
     for (const auto& r : s.rounds) add_commit(r.irs, 3);
     p.off_tmp = b.take(tmp_words * 8);
     p.off_sc_scratch = b.take(sumcheck_scratch_bytes());
-    p.off_ood_scratch = b.take(ood_scratch_bytes());
+    p.off_ood_scratch = b.take(ood_scratch_bytes(1ull << n));
     size_t cov_scratch = cov_init_scratch_bytes(n, n_forms, (int)s.initial.out_domain);
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;

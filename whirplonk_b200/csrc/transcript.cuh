@@ -59,31 +59,69 @@ __constant__ const unsigned long long KECCAK_RC[24] = {
 
 __device__ __forceinline__ u64 rotl64(u64 v, int s) { return s == 0 ? v : ((v << s) | (v >> (64 - s))); }
 
+// rho-pi as one in-place cycle: lane PI_LANE[i] receives lane PI_LANE[i-1]
+// (PI_LANE[-1] = 1) rotated by RHO_CYCLE[i].  Both follow the orbit
+// (x, y) -> (y, 2x + 3y) starting at (1, 0), as keccak_rho does.
+__host__ __device__ constexpr int keccak_pi_lane(int i) {
+    int x = 1, y = 0;
+    for (int t = 0; t <= i; ++t) {
+        const int nx = y, ny = (2 * x + 3 * y) % 5;
+        x = nx;
+        y = ny;
+    }
+    return x + 5 * y;
+}
+__host__ __device__ constexpr int keccak_pi_rot(int i) {
+    int x = 1, y = 0;
+    for (int t = 0; t < i; ++t) {
+        const int nx = y, ny = (2 * x + 3 * y) % 5;
+        x = nx;
+        y = ny;
+    }
+    return keccak_rho(x, y);
+}
+
 // Keccak-f[1600] on a 25-lane state in memory: lanes are pulled into
-// registers (constant indices only), permuted, written back.
+// registers (constant indices only), permuted in place with at most five
+// temporaries (so the state stays in registers even under a tight register
+// budget of the calling kernel), written back.
 static __device__ __noinline__ void keccak_f1600(u64* st) {
     u64 a[25];
 #pragma unroll
     for (int i = 0; i < 25; ++i) a[i] = st[i];
+#pragma unroll 1
     for (int round = 0; round < 24; ++round) {
-        u64 c[5], b[25];
+        {  // theta
+            u64 c[5];
 #pragma unroll
-        for (int x = 0; x < 5; ++x) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
+            for (int x = 0; x < 5; ++x) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
 #pragma unroll
-        for (int x = 0; x < 5; ++x) {
-            u64 d = c[(x + 4) % 5] ^ rotl64(c[(x + 1) % 5], 1);
+            for (int x = 0; x < 5; ++x) {
+                const u64 d = c[(x + 4) % 5] ^ rotl64(c[(x + 1) % 5], 1);
 #pragma unroll
-            for (int y = 0; y < 5; ++y) a[x + 5 * y] ^= d;
+                for (int y = 0; y < 5; ++y) a[x + 5 * y] ^= d;
+            }
+        }
+        {  // rho and pi
+            u64 t = a[1];
+#pragma unroll
+            for (int i = 0; i < 24; ++i) {
+                const int j = keccak_pi_lane(i);
+                const u64 nxt = a[j];
+                a[j] = rotl64(t, keccak_pi_rot(i));
+                t = nxt;
+            }
         }
 #pragma unroll
-        for (int x = 0; x < 5; ++x)
-#pragma unroll
-            for (int y = 0; y < 5; ++y) b[y + 5 * ((2 * x + 3 * y) % 5)] = rotl64(a[x + 5 * y], keccak_rho(x, y));
-#pragma unroll
-        for (int y = 0; y < 5; ++y)
-#pragma unroll
-            for (int x = 0; x < 5; ++x) a[x + 5 * y] = b[x + 5 * y] ^ (~b[(x + 1) % 5 + 5 * y] & b[(x + 2) % 5 + 5 * y]);
-        a[0] ^= KECCAK_RC[round];
+        for (int y = 0; y < 5; ++y) {  // chi
+            const u64 r0 = a[5 * y], r1 = a[5 * y + 1], r2 = a[5 * y + 2], r3 = a[5 * y + 3], r4 = a[5 * y + 4];
+            a[5 * y] = r0 ^ (~r1 & r2);
+            a[5 * y + 1] = r1 ^ (~r2 & r3);
+            a[5 * y + 2] = r2 ^ (~r3 & r4);
+            a[5 * y + 3] = r3 ^ (~r4 & r0);
+            a[5 * y + 4] = r4 ^ (~r0 & r1);
+        }
+        a[0] ^= KECCAK_RC[round];  // iota
     }
 #pragma unroll
     for (int i = 0; i < 25; ++i) st[i] = a[i];
