@@ -66,25 +66,33 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
     store_node(nodes, i, cv);
 }
 
+__host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
+    // [leaves (2^logN) | 2^(logN-1) | ... ]: offset of level l = 2^(logN+1) - 2^(logN+1-l)
+    return (2ull << logN) - (2ull << (logN - l));
+}
+
+// parent = BLAKE3(left || right)
+__device__ __forceinline__ void parent_cv(const unsigned l[8], const unsigned r[8], unsigned out[8]) {
+    unsigned m[16];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { m[k] = l[k]; m[8 + k] = r[k]; }
+    b3_hash64(m, out);
+}
+
 int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
                        u64 node_stride, cudaStream_t st) {
     if (depth * ncomp * 8 > 1024) return -1;  // multi-chunk BLAKE3 rows are not on this path
     if (count == 0 || count > 65535) return -1;
+    if (ncomp != 1 && ncomp != 3) return -1;
     const dim3 grid((unsigned)((N + 255) / 256), count);
     if (ncomp == 1) k_leaves<1><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
-    else if (ncomp == 3) k_leaves<3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
-    else return -1;
+    else k_leaves<3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
     count_launches(1);
     return 0;
 }
 
 int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st) {
     return launch_leaves_batch(planes, N, depth, ncomp, nodes, 1, 0, 0, st);
-}
-
-__host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
-    // [leaves (2^logN) | 2^(logN-1) | ... ]: offset of level l = 2^(logN+1) - 2^(logN+1-l)
-    return (2ull << logN) - (2ull << (logN - l));
 }
 
 // One CTA hashes a subtree of height `levels` whose children sit at level
@@ -138,12 +146,42 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
     }
 }
 
+// Three tree levels at once: a thread reads 8 consecutive nodes of level
+// `level_in` and writes their 4 parents, 2 grandparents and 1 great-grandparent.
+__global__ void __launch_bounds__(256) k_merkle8(u32* nodes, u32 logN, u32 level_in, u64 node_stride) {
+    const u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (1ull << (logN - level_in - 3))) return;
+    nodes += blockIdx.y * node_stride;
+    const u64 in = level_offset(logN, level_in) + 8 * g;
+    const u64 o1 = level_offset(logN, level_in + 1) + 4 * g;
+    const u64 o2 = level_offset(logN, level_in + 2) + 2 * g;
+    const u64 o3 = level_offset(logN, level_in + 3) + g;
+    unsigned m[16], p0[8], p1[8], q0[8], q1[8];
+    load_node(nodes, in + 0, m); load_node(nodes, in + 1, m + 8); b3_hash64(m, p0); store_node(nodes, o1 + 0, p0);
+    load_node(nodes, in + 2, m); load_node(nodes, in + 3, m + 8); b3_hash64(m, p1); store_node(nodes, o1 + 1, p1);
+    parent_cv(p0, p1, q0);
+    store_node(nodes, o2 + 0, q0);
+    load_node(nodes, in + 4, m); load_node(nodes, in + 5, m + 8); b3_hash64(m, p0); store_node(nodes, o1 + 2, p0);
+    load_node(nodes, in + 6, m); load_node(nodes, in + 7, m + 8); b3_hash64(m, p1); store_node(nodes, o1 + 3, p1);
+    parent_cv(p0, p1, q1);
+    store_node(nodes, o2 + 1, q1);
+    parent_cv(q0, q1, p0);
+    store_node(nodes, o3, p0);
+}
+
 // `count` trees `node_stride` words apart; the transcript step (tx non-null)
 // is for a single tree only.
 static int merkle_levels(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, u32 count,
                          u64 node_stride, cudaStream_t st) {
     if (count == 0 || count > 65535 || (tx && count != 1)) return -1;
     u32 level = 0;
+    // wide levels: 3 at a time while a launch still has >= 2^12 threads
+    while (logN - level >= 3 + 12) {
+        const u64 threads = 1ull << (logN - level - 3);
+        k_merkle8<<<dim3((unsigned)((threads + 255) / 256), count), 256, 0, st>>>(nodes, logN, level, node_stride);
+        count_launches(1);
+        level += 3;
+    }
     if (logN == 0) {
         if (tx) {
             k_merkle<<<dim3(1, count), 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1, node_stride);

@@ -22,6 +22,9 @@ constexpr int SC_THREADS = 256, SC_GRID = 148 * 4;
 #ifndef SC_MINB
 #define SC_MINB 3
 #endif
+#ifndef SC_MINB_FOLD
+#define SC_MINB_FOLD 2
+#endif
 
 __device__ __forceinline__ E3 block_sum(E3 v, E3* red) {
     v = e3_warp_sum(v);
@@ -68,33 +71,47 @@ __device__ __forceinline__ E3 load_b(const ScKernelArgs& a, u64 i, const E3& r) 
     return e3_add(y0, e3_mul(r, e3_sub(y1, y0)));
 }
 
-__global__ void __launch_bounds__(SC_THREADS, SC_MINB) k_sumcheck_round(ScKernelArgs a) {
-    __shared__ E3 red[32];
-    __shared__ bool is_last;
-    const E3 r = a.fold ? a.sc->sc_r[a.fold_r] : e3_zero();
-    const u64 half = a.size >> 1;
-    E3 c0 = e3_zero(), c2 = e3_zero();
-    const u64 T = (u64)gridDim.x * blockDim.x;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += T) {
-        const E3 al = load_a(a, i, r), ah = load_a(a, i + half, r);
-        const E3 bl = load_b(a, i, r), bh = load_b(a, i + half, r);
-        if (a.fold) {
-            st3(a.a_out, i, al); st3(a.a_out, i + half, ah);
-            st3(a.b, i, bl); st3(a.b, i + half, bh);
-        }
-        c0 = e3_add(c0, e3_mul(al, bl));
-        c2 = e3_add(c2, e3_mul(e3_sub(ah, al), e3_sub(bh, bl)));
-    }
+// Unreduced sums of Ext3 products (X^3 = 2): the doubled cross terms are fed
+// with 2 a1, 2 a2, so three 192-bit accumulators suffice.  A thread adds at
+// most 3 products per accumulator per pair it visits, far below the 2^31
+// products acc_reduce allows.
+struct E3AccL {
+    Acc192 s0, s1, s2;
+};
+__device__ __forceinline__ void accl_mac(E3AccL& x, const E3& a, const E3& b) {
+    const u64 a1d = gl_add(a.c1, a.c1), a2d = gl_add(a.c2, a.c2);
+    acc_mac(x.s0, a.c0, b.c0);
+    acc_mac(x.s0, a1d, b.c2);
+    acc_mac(x.s0, a2d, b.c1);
+    acc_mac(x.s1, a.c0, b.c1);
+    acc_mac(x.s1, a.c1, b.c0);
+    acc_mac(x.s1, a2d, b.c2);
+    acc_mac(x.s2, a.c0, b.c2);
+    acc_mac(x.s2, a.c1, b.c1);
+    acc_mac(x.s2, a.c2, b.c0);
+}
+__device__ __forceinline__ void accl_mac_base(E3AccL& x, u64 a, const E3& b) {
+    acc_mac(x.s0, a, b.c0);
+    acc_mac(x.s1, a, b.c1);
+    acc_mac(x.s2, a, b.c2);
+}
+__device__ __forceinline__ E3 accl_reduce(const E3AccL& x) {
+    return E3{acc_reduce(x.s0), acc_reduce(x.s1), acc_reduce(x.s2)};
+}
+
+// CTA sums of (c0, c2), then the last CTA (ticket) sums the partials and does
+// the transcript step on one thread.
+__device__ __forceinline__ void sc_round_finish(const ScKernelArgs& a, E3 c0, E3 c2, E3* red, bool* is_last) {
     const E3 s0 = block_sum(c0, red);
     const E3 s2 = block_sum(c2, red);
     if (threadIdx.x == 0) {
         a.partials[2 * blockIdx.x] = s0;
         a.partials[2 * blockIdx.x + 1] = s2;
         __threadfence();
-        is_last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
+        *is_last = atomicAdd(a.counter, 1u) == gridDim.x - 1;
     }
     __syncthreads();
-    if (!is_last) return;
+    if (!*is_last) return;
     E3 t0 = e3_zero(), t2 = e3_zero();
     for (u32 k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
         const E3* p0 = &a.partials[2 * k];
@@ -123,6 +140,35 @@ __global__ void __launch_bounds__(SC_THREADS, SC_MINB) k_sumcheck_round(ScKernel
             sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
         }
     }
+}
+
+// One round on pairs (i, i + s/2).  FOLD: the vectors still hold the previous
+// round's size-2s arrays, folded with its challenge on load (and written back
+// folded).  BASE: a is the base-field coefficient array (first rounds only).
+template <bool FOLD, bool BASE>
+__global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_sumcheck_round(ScKernelArgs a) {
+    __shared__ E3 red[32];
+    __shared__ bool is_last;
+    const E3 r = FOLD ? a.sc->sc_r[a.fold_r] : e3_zero();
+    const u64 half = a.size >> 1;
+    E3AccL c0{}, c2{};
+    const u64 T = (u64)gridDim.x * blockDim.x;
+    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += T) {
+        if (BASE && !FOLD) {
+            const u64 al = a.a_base[i], ah = a.a_base[i + half];
+            const E3 bl = ld3(a.b, i), bh = ld3(a.b, i + half);
+            accl_mac_base(c0, al, bl);
+            accl_mac_base(c2, gl_sub(ah, al), e3_sub(bh, bl));
+        } else {
+            const E3 al = load_a(a, i, r), bl = load_b(a, i, r);
+            if (FOLD) { st3(a.a_out, i, al); st3(a.b, i, bl); }
+            accl_mac(c0, al, bl);
+            const E3 ah = load_a(a, i + half, r), bh = load_b(a, i + half, r);
+            if (FOLD) { st3(a.a_out, i + half, ah); st3(a.b, i + half, bh); }
+            accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
+        }
+    }
+    sc_round_finish(a, accl_reduce(c0), accl_reduce(c2), red, &is_last);
 }
 
 // After a round PoW: send the nonce, squeeze r, update the sum.
@@ -164,7 +210,14 @@ int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
     const u64 half = s.size >> 1;
     u64 want = (half + SC_THREADS - 1) / SC_THREADS;
     const unsigned grid = (unsigned)(want > SC_GRID ? SC_GRID : (want < 1 ? 1 : want));
-    k_sumcheck_round<<<grid, SC_THREADS, 0, st>>>(a);
+    const bool base = a.a_base != nullptr;
+    if (a.fold) {
+        if (base) k_sumcheck_round<true, true><<<grid, SC_THREADS, 0, st>>>(a);
+        else k_sumcheck_round<true, false><<<grid, SC_THREADS, 0, st>>>(a);
+    } else {
+        if (base) k_sumcheck_round<false, true><<<grid, SC_THREADS, 0, st>>>(a);
+        else k_sumcheck_round<false, false><<<grid, SC_THREADS, 0, st>>>(a);
+    }
     count_launches(1);
     if (s.pow_threshold != ~0ull) {
         launch_pow_grind_only(s.sc, s.pow_threshold, st);
