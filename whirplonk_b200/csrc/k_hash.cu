@@ -15,6 +15,7 @@
 #include "launch.h"
 #include "blake3.cuh"
 #include "state.cuh"
+#include "wtx.cuh"
 
 namespace wg {
 
@@ -136,13 +137,19 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
             cur ^= 1;
         }
     }
-    if (finish && tx && threadIdx.x == 0) {
+    if (finish && tx && threadIdx.x < 32) {  // warp 0: root message, OOD points
         __threadfence();
         const u64 root = level_offset(logN, logN);
         u64 w[4];
         for (int k = 0; k < 4; ++k) w[k] = (u64)nodes[root * 8 + 2 * k] | ((u64)nodes[root * 8 + 2 * k + 1] << 32);
-        tx_message_words(tx, w, 4);
-        for (int j = 0; j < n_ood; ++j) sc->ood_pts[commit_idx][j] = tx_challenge_e3(tx);
+        WarpTx t;
+        wtx_load(t, tx);
+        wtx_message_words(t, w, 4);
+        for (int j = 0; j < n_ood; ++j) {
+            const E3 z = wtx_challenge_e3(t);
+            if (threadIdx.x == 0) sc->ood_pts[commit_idx][j] = z;
+        }
+        wtx_store(t, tx);
     }
 }
 
@@ -281,6 +288,7 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(const u64* v0, const u64* v
     }
     __syncthreads();
     if (!is_last) return;
+    __shared__ E3 totals[MAX_OOD];
     for (int j = 0; j < n_ood; ++j) {
         E3 acc = e3_zero();
         for (u32 b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
@@ -290,8 +298,15 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(const u64* v0, const u64* v
         E3 total = block_sum_e3(acc, red);
         if (threadIdx.x == 0) {
             sc->ood_vals[commit_idx][j] = total;
-            tx_message_e3(tx, total);
+            totals[j] = total;
         }
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // warp 0 sends the values
+        WarpTx t;
+        wtx_load(t, tx);
+        for (int j = 0; j < n_ood; ++j) wtx_message_e3(t, totals[j]);
+        wtx_store(t, tx);
     }
     if (threadIdx.x == 0) *counter = 0;
 }

@@ -14,6 +14,7 @@
 // later cov[i] += sum_j stir_rlc_j z_j^i per round (utilities.hpp:261-307).
 #include "launch.h"
 #include "state.cuh"
+#include "wtx.cuh"
 
 namespace wg {
 
@@ -119,26 +120,40 @@ __device__ __forceinline__ void sc_round_finish(const ScKernelArgs& a, E3 c0, E3
         t0 = e3_add(t0, E3{__ldcg(&p0->c0), __ldcg(&p0->c1), __ldcg(&p0->c2)});
         t2 = e3_add(t2, E3{__ldcg(&p2->c0), __ldcg(&p2->c1), __ldcg(&p2->c2)});
     }
-    const E3 C0 = block_sum(t0, red);
-    const E3 C2 = block_sum(t2, red);
+    const E3 C0s = block_sum(t0, red);
+    const E3 C2s = block_sum(t2, red);
     if (threadIdx.x == 0) {
-        *a.counter = 0;
+        red[0] = C0s;  // block_sum is done with red: hand the totals to warp 0
+        red[1] = C2s;
+    }
+    __syncwarp();
+    if (threadIdx.x < 32) {  // warp 0: c0, c2 messages, [PoW challenge | r], sum
+        const E3 C0 = red[0], C2 = red[1];
         ProofScalars* sc = a.sc;
-        TxState* tx = a.tx;
-        sc->c0 = C0;
-        sc->c2 = C2;
-        tx_message_e3(tx, C0);
-        tx_message_e3(tx, C2);
+        WarpTx t;
+        wtx_load(t, a.tx);
+        wtx_message_e3(t, C0);
+        wtx_message_e3(t, C2);
         if (a.pow_threshold != ~0ull) {
             // PoW follows in-stream (ordered windows, then k_sc_after_pow).
-            tx_squeeze(tx, sc->pow_ch, 32);
-            sc->pow_best = ~0ull;
+            wtx_squeeze_bytes(t, sc->pow_ch, 32);
+            if (threadIdx.x == 0) {
+                sc->c0 = C0;
+                sc->c2 = C2;
+                sc->pow_best = ~0ull;
+            }
         } else {
-            const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
-            const E3 rn = tx_challenge_e3(tx);
-            sc->sc_r[a.r_slot] = rn;
-            sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+            const E3 rn = wtx_challenge_e3(t);
+            if (threadIdx.x == 0) {
+                const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
+                sc->c0 = C0;
+                sc->c2 = C2;
+                sc->sc_r[a.r_slot] = rn;
+                sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+            }
         }
+        wtx_store(t, a.tx);
+        if (threadIdx.x == 0) *a.counter = 0;
     }
 }
 
@@ -172,16 +187,22 @@ __global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_s
 }
 
 // After a round PoW: send the nonce, squeeze r, update the sum.
+// One warp.
 __global__ void k_sc_after_pow(TxState* tx, ProofScalars* sc, int r_slot) {
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x >= 32) return;
     const u64 n = sc->pow_best;
-    if (n == ~0ull) tx->err |= TX_ERR_POW_EXHAUSTED;
-    tx_message_u64(tx, n);
-    const E3 C0 = sc->c0, C2 = sc->c2;
-    const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
-    const E3 rn = tx_challenge_e3(tx);
-    sc->sc_r[r_slot] = rn;
-    sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+    WarpTx t;
+    wtx_load(t, tx);
+    if (n == ~0ull) t.err |= TX_ERR_POW_EXHAUSTED;
+    wtx_message_u64(t, n);
+    const E3 rn = wtx_challenge_e3(t);
+    if (threadIdx.x == 0) {
+        const E3 C0 = sc->c0, C2 = sc->c2;
+        const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
+        sc->sc_r[r_slot] = rn;
+        sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+    }
+    wtx_store(t, tx);
 }
 
 static ScKernelArgs make_sc(const SumcheckArgs& s) {

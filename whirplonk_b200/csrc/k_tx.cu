@@ -6,6 +6,7 @@
 #include "launch.h"
 #include "blake3.cuh"
 #include "state.cuh"
+#include "wtx.cuh"
 
 namespace wg {
 
@@ -13,18 +14,21 @@ namespace wg {
 // Transcript start: ProverState::from_ds (transcript.hpp:605-610) absorbs
 // protocol_id || session_id || instance bytes.
 // ---------------------------------------------------------------------------
+// One warp.
 __global__ void k_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
                           unsigned char* hints, u64 hints_cap, ProofScalars* sc) {
-    if (threadIdx.x != 0) return;
-    for (int i = 0; i < 25; ++i) { tx->hasher[i] = 0; tx->reader[i] = 0; }
-    tx->hpos = tx->rpos = tx->has_reader = tx->err = 0;
-    tx->narg_len = tx->hints_len = 0;
-    tx->narg_cap = narg_cap;
-    tx->hints_cap = hints_cap;
-    tx->narg = narg;
-    tx->hints = hints;
-    tx_absorb(tx, ds, ds_len);
-    for (int i = 0; i < 64; ++i) sc->counters[i] = 0;
+    if (threadIdx.x >= 32) return;
+    WarpTx t;
+    t.h = t.r = 0;
+    t.hpos = t.rpos = t.has_reader = t.err = 0;
+    t.narg_len = t.hints_len = 0;
+    t.narg_cap = narg_cap;
+    t.hints_cap = hints_cap;
+    t.narg = narg;
+    t.hints = hints;
+    wtx_absorb_bytes(t, ds, ds_len);
+    wtx_store(t, tx);
+    for (int i = threadIdx.x; i < 64; i += 32) sc->counters[i] = 0;
 }
 
 int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
@@ -34,25 +38,22 @@ int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned ch
     return 0;
 }
 
-// geometric_challenge (geometric_challenge.hpp:39-44): [] / [1] / squeeze x -> [1, x, x^2, ...].
-__device__ void geometric_challenge(TxState* tx, E3* out, int count) {
-    if (count <= 0) return;
-    out[0] = e3_one();
-    if (count == 1) return;
-    const E3 x = tx_challenge_e3(tx);
-    for (int i = 1; i < count; ++i) out[i] = e3_mul(out[i - 1], x);
-}
-
 // Constraint RLC and "the sum" (whir_prover.hpp:150-197) for one vector:
 // sum = sum_f crlc_f eval_f + sum_j crlc_{F+j} ood_val_j.
+// One warp (n_forms + n_ood <= 16).
 __global__ void k_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood) {
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x >= 32) return;
     const int count = n_forms + n_ood;
-    geometric_challenge(tx, sc->crlc, count);
-    E3 sum = e3_zero();
-    for (int f = 0; f < n_forms; ++f) sum = e3_add(sum, e3_mul(sc->crlc[f], sc->forms_eval[f]));
-    for (int j = 0; j < n_ood; ++j) sum = e3_add(sum, e3_mul(sc->crlc[n_forms + j], sc->ood_vals[0][j]));
-    sc->sum = sum;
+    WarpTx t;
+    wtx_load(t, tx);
+    wtx_geometric(t, sc->crlc, count);
+    wtx_store(t, tx);
+    const int l = threadIdx.x;
+    E3 v = e3_zero();
+    if (l < n_forms) v = e3_mul(sc->crlc[l], sc->forms_eval[l]);
+    else if (l < count) v = e3_mul(sc->crlc[l], sc->ood_vals[0][l - n_forms]);
+    v = wtx_sum(v);
+    if (l == 0) sc->sum = v;
 }
 
 int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood, cudaStream_t st) {
@@ -79,10 +80,14 @@ int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood,
 constexpr u64 POW_NONCE_LIMIT = 1ull << 36;
 constexpr unsigned POW_GRID = 148 * 6, POW_THREADS = 256;
 
+// One warp.
 __global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
-    if (threadIdx.x != 0) return;
-    tx_squeeze(tx, sc->pow_ch, 32);
-    sc->pow_best = ~0ull;
+    if (threadIdx.x >= 32) return;
+    WarpTx t;
+    wtx_load(t, tx);
+    wtx_squeeze_bytes(t, sc->pow_ch, 32);
+    wtx_store(t, tx);
+    if (threadIdx.x == 0) sc->pow_best = ~0ull;
 }
 
 __global__ void __launch_bounds__(POW_THREADS) k_pow_window(ProofScalars* sc, u64 threshold, u64 base, u64 count) {
@@ -136,12 +141,16 @@ int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st) {
     return 0;
 }
 
+// One warp.
 __global__ void k_pow_finish(TxState* tx, ProofScalars* sc, int slot) {
-    if (threadIdx.x != 0) return;
+    if (threadIdx.x >= 32) return;
     const u64 n = sc->pow_best;
-    if (n == ~0ull) tx->err |= TX_ERR_POW_EXHAUSTED;
-    if (slot >= 0 && slot < MAX_COMMITS + 4) sc->pow_nonces[slot] = n;
-    tx_message_u64(tx, n);
+    WarpTx t;
+    wtx_load(t, tx);
+    if (n == ~0ull) t.err |= TX_ERR_POW_EXHAUSTED;
+    if (threadIdx.x == 0 && slot >= 0 && slot < MAX_COMMITS + 4) sc->pow_nonces[slot] = n;
+    wtx_message_u64(t, n);
+    wtx_store(t, tx);
 }
 
 int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, cudaStream_t st) {
@@ -155,9 +164,13 @@ int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, cudaStrea
 }
 
 // Final vector: prover_message of every coefficient (whir_prover.hpp:360-362).
+// One warp.
 __global__ void k_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size) {
-    if (threadIdx.x != 0) return;
-    for (u64 i = 0; i < size; ++i) tx_message_e3(tx, E3{c0[i], c1[i], c2[i]});
+    if (threadIdx.x >= 32) return;
+    WarpTx t;
+    wtx_load(t, tx);
+    for (u64 i = 0; i < size; ++i) wtx_message_e3(t, E3{c0[i], c1[i], c2[i]});
+    wtx_store(t, tx);
 }
 
 int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size, cudaStream_t st) {
@@ -208,26 +221,27 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
     __shared__ u32 total;
     __shared__ E3 eqw[MAX_DEPTH];
     __shared__ u64 hint_base;
-    TxState* tx = a.tx;
+    __shared__ unsigned char idx_bytes[MAX_QUERIES * 8];
+    const TxState* tx = a.tx;  // hint pointers and capacity only; warp 0 carries the sponge
     ProofScalars* sc = a.sc;
     const u32 t = threadIdx.x;
     const u32 q = a.q;
+    const u32 nbytes = (a.logN + 7) / 8;
 
-    // 1. indices
+    // 1. indices: warp 0 squeezes q * nbytes bytes (big-endian per index)
+    WarpTx wt;
+    if (t < 32) {
+        wtx_load(wt, a.tx);
+        if (a.N != 1) wtx_squeeze_bytes(wt, idx_bytes, q * nbytes);
+    }
+    __syncthreads();
+    for (u32 i = t; i < q; i += blockDim.x) {
+        u64 acc = 0;
+        for (u32 k = 0; k < nbytes; ++k) acc = (acc << 8) | idx_bytes[i * nbytes + k];
+        idx_s[i] = a.N == 1 ? 0 : (acc & (a.N - 1));  // N is a power of two
+    }
     if (t == 0) {
-        if (a.N == 1) {
-            for (u32 i = 0; i < q; ++i) idx_s[i] = 0;
-        } else {
-            const u32 nbytes = (a.logN + 7) / 8;
-            for (u32 i = 0; i < q; ++i) {
-                unsigned char b[8];
-                tx_squeeze(tx, b, nbytes);
-                u64 acc = 0;
-                for (u32 k = 0; k < nbytes; ++k) acc = (acc << 8) | b[k];
-                idx_s[i] = acc & (a.N - 1);  // N is a power of two
-            }
-        }
-        hint_base = tx->hints_len;
+        hint_base = wt.hints_len;
         // 3a. eq weights of the last `fold` folding challenges (multilinear_point.hpp:40-62)
         if (a.stir) {
             const u32 d = 1u << a.fold;
@@ -344,9 +358,10 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
         level_off += level_len;
         level_len >>= 1;
     }
-    if (t == 0) {
-        if (!fits || node_hint_off > tx->hints_cap) tx->err |= TX_ERR_HINT_OVERFLOW;
-        else tx->hints_len = node_hint_off;
+    if (t < 32) {
+        if (!fits || node_hint_off > wt.hints_cap) wt.err |= TX_ERR_HINT_OVERFLOW;
+        else wt.hints_len = node_hint_off;
+        wtx_store(wt, a.tx);
     }
 }
 
@@ -360,17 +375,24 @@ int launch_open(const OpenArgs& a, cudaStream_t st) {
 // STIR combination: the new commitment's OOD points/values first, then the
 // in-domain ones written by k_open; RLC = geometric_challenge(O + q);
 // sum += <rlc, values>.
+// One warp.
 __global__ void k_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int q) {
-    if (threadIdx.x != 0) return;
-    for (int j = 0; j < n_ood; ++j) {
-        sc->stir_pts[j] = sc->ood_pts[commit_idx][j];
-        sc->stir_vals[j] = sc->ood_vals[commit_idx][j];
+    if (threadIdx.x >= 32) return;
+    const int l = threadIdx.x;
+    if (l < n_ood) {
+        sc->stir_pts[l] = sc->ood_pts[commit_idx][l];
+        sc->stir_vals[l] = sc->ood_vals[commit_idx][l];
     }
+    __syncwarp();
     const int count = n_ood + q;
-    geometric_challenge(tx, sc->stir_rlc, count);
-    E3 acc = sc->sum;
-    for (int j = 0; j < count; ++j) acc = e3_add(acc, e3_mul(sc->stir_rlc[j], sc->stir_vals[j]));
-    sc->sum = acc;
+    WarpTx t;
+    wtx_load(t, tx);
+    wtx_geometric(t, sc->stir_rlc, count);
+    wtx_store(t, tx);
+    E3 acc = e3_zero();
+    for (int j = l; j < count; j += 32) acc = e3_add(acc, e3_mul(sc->stir_rlc[j], sc->stir_vals[j]));
+    acc = wtx_sum(acc);
+    if (l == 0) sc->sum = e3_add(sc->sum, acc);
 }
 
 int launch_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int q, cudaStream_t st) {
