@@ -205,6 +205,111 @@ __global__ void k_sc_after_pow(TxState* tx, ProofScalars* sc, int r_slot) {
     wtx_store(t, tx);
 }
 
+// ---------------------------------------------------------------------------
+// Small sumchecks (size <= SC_SMALL_MAX, no round PoW): all rounds of one
+// sumcheck, and the fold after the last one, in ONE CTA.  Round t folds with
+// the previous challenge on load exactly as k_sumcheck_round does; warp 0
+// carries the transcript across the rounds; __syncthreads orders the rounds.
+// This replaces a chain of grid launches whose fixed cost dominates at these
+// sizes.
+// ---------------------------------------------------------------------------
+constexpr u64 SC_SMALL_MAX = 1ull << 12;
+constexpr int SC_SMALL_THREADS = 1024;
+
+struct ScSmallArgs {
+    const u64* a_base;  // base-field coefficients (first sumcheck) or null
+    u64* a[3];
+    u64* b[3];
+    u64 size;           // size of round 0
+    int rounds, r_slot, fold_after;
+    TxState* tx;
+    ProofScalars* sc;
+};
+
+__global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs a) {
+    __shared__ E3 red[32];
+    __shared__ E3 tot[2];
+    ProofScalars* sc = a.sc;
+    WarpTx wt;
+    if (threadIdx.x < 32) wtx_load(wt, a.tx);
+    for (int t = 0; t <= a.rounds; ++t) {
+        const bool last = t == a.rounds;  // only the trailing fold
+        if (last && !a.fold_after) break;
+        const u64 size = a.size >> t;
+        const bool fold = t > 0;
+        const bool base = a.a_base && t <= 1;
+        const E3 r = fold ? sc->sc_r[a.r_slot + t - 1] : e3_zero();
+        ScKernelArgs k{};
+        k.a_base = base ? a.a_base : nullptr;
+        for (int c = 0; c < 3; ++c) { k.a_in[c] = a.a[c]; k.a_out[c] = a.a[c]; k.b[c] = a.b[c]; }
+        k.size = size;
+        k.fold = fold;
+        if (last) {  // fold only
+            for (u64 i = threadIdx.x; i < size; i += blockDim.x) {
+                st3(k.a_out, i, load_a(k, i, r));
+                st3(k.b, i, load_b(k, i, r));
+            }
+            break;
+        }
+        const u64 half = size >> 1;
+        E3AccL c0{}, c2{};
+        for (u64 i = threadIdx.x; i < half; i += blockDim.x) {
+            if (base && !fold) {
+                const u64 al = a.a_base[i], ah = a.a_base[i + half];
+                const E3 bl = ld3(k.b, i), bh = ld3(k.b, i + half);
+                accl_mac_base(c0, al, bl);
+                accl_mac_base(c2, gl_sub(ah, al), e3_sub(bh, bl));
+            } else {
+                const E3 al = load_a(k, i, r), bl = load_b(k, i, r);
+                if (fold) { st3(k.a_out, i, al); st3(k.b, i, bl); }
+                accl_mac(c0, al, bl);
+                const E3 ah = load_a(k, i + half, r), bh = load_b(k, i + half, r);
+                if (fold) { st3(k.a_out, i + half, ah); st3(k.b, i + half, bh); }
+                accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
+            }
+        }
+        const E3 s0 = block_sum(accl_reduce(c0), red);
+        const E3 s2 = block_sum(accl_reduce(c2), red);
+        if (threadIdx.x == 0) {
+            tot[0] = s0;
+            tot[1] = s2;
+        }
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            const E3 C0 = tot[0], C2 = tot[1];
+            wtx_message_e3(wt, C0);
+            wtx_message_e3(wt, C2);
+            const E3 rn = wtx_challenge_e3(wt);
+            if (threadIdx.x == 0) {
+                const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
+                sc->c0 = C0;
+                sc->c2 = C2;
+                sc->sc_r[a.r_slot + t] = rn;
+                sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 32) wtx_store(wt, a.tx);
+}
+
+int launch_sumcheck_small(const SumcheckArgs& s, int rounds, int fold_after, cudaStream_t st) {
+    if (s.size > SC_SMALL_MAX || s.pow_threshold != ~0ull || rounds < 1) return 1;  // not this path
+    if ((s.size >> rounds) < 1) return -1;
+    ScSmallArgs a{};
+    a.a_base = s.a_base;
+    for (int c = 0; c < 3; ++c) { a.a[c] = s.a_in[c]; a.b[c] = s.b[c]; }
+    a.size = s.size;
+    a.rounds = rounds;
+    a.r_slot = s.r_slot;
+    a.fold_after = fold_after;
+    a.tx = s.tx;
+    a.sc = s.sc;
+    k_sumcheck_small<<<1, SC_SMALL_THREADS, 0, st>>>(a);
+    count_launches(1);
+    return 0;
+}
+
 static ScKernelArgs make_sc(const SumcheckArgs& s) {
     ScKernelArgs a{};
     a.a_base = s.a_base;

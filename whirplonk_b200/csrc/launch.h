@@ -159,6 +159,11 @@ struct SumcheckArgs {
 // One sumcheck round (sumcheck_protocol.hpp:99-135) with the previous round's
 // fold fused in.  PoW (if any) and the challenge squeeze happen in-stream.
 int launch_sumcheck_round(const SumcheckArgs& a, cudaStream_t st);
+// All `rounds` rounds of a small sumcheck (and the fold after the last one when
+// fold_after) in one single-CTA kernel: round t's challenge goes to
+// sc_r[r_slot + t].  Returns 1 (nothing launched) when the sumcheck is too
+// large or has round PoW.
+int launch_sumcheck_small(const SumcheckArgs& a, int rounds, int fold_after, cudaStream_t st);
 // Fold only: a_out[i] = a_in[i] + r (a_in[i+size] - a_in[i]), same for b.
 int launch_fold(const SumcheckArgs& a, cudaStream_t st);
 size_t sumcheck_scratch_bytes();

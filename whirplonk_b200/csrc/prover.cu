@@ -188,6 +188,22 @@ int commit_vector(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t n
 // vector is still the base-field coefficient array (first sumcheck only).
 // Leaves a, cov folded to size >> rounds when `fold_after` is set.
 int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_first, int& r_slot, bool fold_after) {
+    if (s.num_rounds > 0) {  // small sumchecks: one single-CTA kernel for every round
+        SumcheckArgs a{};
+        a.a_base = base_first ? c.w(c.p.off_coeffs) : nullptr;
+        for (int k = 0; k < 3; ++k) { a.a_in[k] = c.a(k); a.a_out[k] = c.a(k); a.b[k] = c.cov(k); }
+        a.size = size;
+        a.r_slot = r_slot;
+        a.pow_threshold = s.pow_threshold;
+        a.tx = c.tx();
+        a.sc = c.sc();
+        int rc = 1;
+        WG_TIMED(c, FAM_SUMCHECK, (rc = launch_sumcheck_small(a, (int)s.num_rounds, fold_after ? 1 : 0, c.st)) < 0 ? rc : 0);
+        if (rc == 0) {
+            r_slot += (int)s.num_rounds;
+            return 0;
+        }
+    }
     for (uint64_t t = 0; t < s.num_rounds; ++t) {
         SumcheckArgs a{};
         const bool from_base = base_first && t <= 1;
