@@ -141,6 +141,7 @@ __device__ __forceinline__ void sc_round_finish(const ScKernelArgs& a, E3 c0, E3
                 sc->c0 = C0;
                 sc->c2 = C2;
                 sc->pow_best = ~0ull;
+                sc->pow_next = 0;
             }
         } else {
             const E3 rn = wtx_challenge_e3(t);

@@ -67,81 +67,81 @@ int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood,
 // Proof of work (proof_of_work.hpp:95-193, 236-257): the smallest nonce n >= 0
 // with LE_u64(BLAKE3(challenge || n_le || 0^24)[0..8]) <= threshold.
 //
-// The nonce space is scanned in ordered windows [base, base + count), one
-// kernel launch per window.  A window is scanned completely (a thread only
-// skips nonces above an already published hit), so the smallest hit of the
-// first window that has one is the global minimum -- the reference's answer,
-// whatever the warp scheduling.  Later windows see the published result at
-// launch and return at once.  Window sizes grow geometrically from the
-// expected search length 2^64 / threshold until 64x that length has been
-// covered (miss probability e^-64), capped at POW_NONCE_LIMIT; running out
-// sets TX_ERR_POW_EXHAUSTED.
+// One launch: CTAs claim chunks of POW_CHUNK consecutive nonces in increasing
+// order from a counter (atomicAdd), scan a claimed chunk completely and claim
+// the next one while the previous hit published in pow_best (atomicMin) is not
+// below the chunk.  Every chunk that starts at or below the final minimum is
+// therefore claimed and fully scanned, so the minimum is exact -- the
+// reference's answer, whatever the scheduling -- and the work past it is at
+// most one chunk per CTA.  The search stops at 64x the expected length
+// 2^64 / threshold (miss probability e^-64), capped at POW_NONCE_LIMIT; running
+// out sets TX_ERR_POW_EXHAUSTED.
 // ---------------------------------------------------------------------------
 constexpr u64 POW_NONCE_LIMIT = 1ull << 36;
-constexpr unsigned POW_GRID = 148 * 6, POW_THREADS = 256;
+constexpr unsigned POW_THREADS = 256, POW_GRID = 148 * 2, POW_CHUNK = 2 * POW_THREADS;
 
-// One warp.
+// One warp.  Also resets the search state.
 __global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
     if (threadIdx.x >= 32) return;
     WarpTx t;
     wtx_load(t, tx);
     wtx_squeeze_bytes(t, sc->pow_ch, 32);
     wtx_store(t, tx);
-    if (threadIdx.x == 0) sc->pow_best = ~0ull;
+    if (threadIdx.x == 0) {
+        sc->pow_best = ~0ull;
+        sc->pow_next = 0;
+    }
 }
 
-__global__ void __launch_bounds__(POW_THREADS) k_pow_window(ProofScalars* sc, u64 threshold, u64 base, u64 count) {
-    const u64* best = &sc->pow_best;
-    // A hit below `base` came from an earlier window and is the minimum.  A hit
-    // of this window (>= base) must not stop a CTA that starts late: its
-    // nonces may lie below that hit, so it scans up to the published hit.
-    if (__ldcg(best) < base) return;
+__global__ void __launch_bounds__(POW_THREADS) k_pow_search(ProofScalars* sc, u64 threshold, u64 limit) {
     __shared__ unsigned ch[8];
+    __shared__ u64 claim[2];
+    __shared__ int stop;
+    unsigned long long* next = reinterpret_cast<unsigned long long*>(&sc->pow_next);
     if (threadIdx.x < 8) {
         const unsigned char* c = sc->pow_ch + 4 * threadIdx.x;
         ch[threadIdx.x] = (unsigned)c[0] | ((unsigned)c[1] << 8) | ((unsigned)c[2] << 16) | ((unsigned)c[3] << 24);
     }
+    if (threadIdx.x == 0) claim[0] = atomicAdd(next, (unsigned long long)POW_CHUNK);
     __syncthreads();
     unsigned m[16];
 #pragma unroll
     for (int k = 0; k < 8; ++k) m[k] = ch[k];
 #pragma unroll
     for (int k = 10; k < 16; ++k) m[k] = 0;
-    const u64 T = (u64)gridDim.x * blockDim.x;
-    for (u64 off = (u64)blockIdx.x * blockDim.x + threadIdx.x; off < count; off += T) {
-        const u64 n = base + off;
-        if (n > __ldcg(best)) break;  // only nonces above a published hit are skipped
-        m[8] = (unsigned)n;
-        m[9] = (unsigned)(n >> 32);
-        unsigned h[8];
-        b3_hash64(m, h);
-        const u64 v = (u64)h[0] | ((u64)h[1] << 32);
-        if (v <= threshold) {
-            atomicMin(reinterpret_cast<unsigned long long*>(&sc->pow_best), (unsigned long long)n);
-            break;
+    for (unsigned it = 0;; ++it) {
+        const u64 base = claim[it & 1];
+        if (threadIdx.x == 0) {
+            stop = base >= limit || base > __ldcg(&sc->pow_best);
+            // claim the next chunk now, so the counter's latency overlaps the hashing
+            if (!stop) claim[(it + 1) & 1] = atomicAdd(next, (unsigned long long)POW_CHUNK);
         }
+        __syncthreads();
+        if (stop) break;
+#pragma unroll
+        for (unsigned k = 0; k < POW_CHUNK / POW_THREADS; ++k) {
+            const u64 n = base + k * POW_THREADS + threadIdx.x;
+            if (n >= limit) break;
+            m[8] = (unsigned)n;
+            m[9] = (unsigned)(n >> 32);
+            unsigned h[8];
+            b3_hash64(m, h);
+            const u64 v = (u64)h[0] | ((u64)h[1] << 32);
+            if (v <= threshold) atomicMin(reinterpret_cast<unsigned long long*>(&sc->pow_best), (unsigned long long)n);
+        }
+        __syncthreads();
     }
 }
 
-// Launches the ordered windows for one PoW search (challenge already squeezed).
+// The search for one PoW (challenge already squeezed, pow_best / pow_next reset).
 int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st) {
     const double expect = threshold == 0 ? 1.8446744073709552e19 : 18446744073709551616.0 / (double)threshold;
-    u64 cover = expect * 64.0 >= (double)POW_NONCE_LIMIT ? POW_NONCE_LIMIT : (u64)(expect * 64.0) + 1;
-    u64 win = expect < (double)(1u << 18) ? (1ull << 18) : (u64)expect;
-    const u64 max_win = 1ull << 27;
-    if (win > max_win) win = max_win;
-    u64 base = 0;
-    while (base < cover) {
-        const u64 cnt = win < cover - base ? win : cover - base;
-        k_pow_window<<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, base, cnt);
-        count_launches(1);
-        base += cnt;
-        if (win < max_win) win <<= 1;
-    }
+    const u64 limit = expect * 64.0 >= (double)POW_NONCE_LIMIT ? POW_NONCE_LIMIT : (u64)(expect * 64.0) + 1;
+    k_pow_search<<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, limit);
+    count_launches(1);
     return 0;
 }
 
-// One warp.
 __global__ void k_pow_finish(TxState* tx, ProofScalars* sc, int slot) {
     if (threadIdx.x >= 32) return;
     const u64 n = sc->pow_best;

@@ -31,6 +31,7 @@ struct ProofScalars {
     E3 stir_vals[MAX_QUERIES + MAX_OOD];
     u64 indices[MAX_QUERIES];                // opened rows of the current opening
     u64 pow_best;                            // minimum valid nonce (atomicMin target)
+    u64 pow_next;                            // next unclaimed nonce chunk of the search
     u64 pow_nonces[MAX_COMMITS + 4];         // recorded nonces (diagnostics)
     unsigned char pow_ch[32];
     unsigned counters[64];                   // self-resetting last-block tickets
