@@ -60,6 +60,11 @@ WORKLOADS = {
 }
 DEFAULT_WORKLOAD = "whir_served_mixed_n12_24"
 FALLBACK_HBM_GBS = 6650.0
+# Families whose kernels saturate the integer-ALU pipe before HBM (ncu summaries
+# in profiles/): their HBM fraction is low by nature.
+ALU_BOUND = {"ntt": "integer ALU pipe (67-76 % busy in ncu; butterflies of Goldilocks arithmetic)",
+             "leaf_hash": "integer ALU pipe (80-90 % busy in ncu; BLAKE3 compressions)",
+             "merkle": "integer ALU pipe (BLAKE3 compressions)"}
 DATA = "synthetic (seeded ChaCha20 coefficients, seeded Ext3 points)"
 DTYPE = "u64 (Goldilocks; Ext3 challenges)"
 
@@ -166,14 +171,18 @@ def read_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def read_traffic(family):
+def read_traffic(family, alg_bytes_per_proof):
+    """DRAM bytes per proof of `family`: the measured traffic / algorithmic-bytes
+    ratio of profiles/dram_traffic.json (one ncu-captured proof) times this
+    workload's algorithmic bytes; None when the family was not captured."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.json")
     try:
         with open(path) as f:
             t = json.load(f)
-        return t.get(family)
-    except (OSError, ValueError):
+        ratio = t["families"][family]["ratio"]
+    except (OSError, ValueError, KeyError):
         return None
+    return alg_bytes_per_proof * ratio
 
 
 # ---------------------------------------------------------------------------
@@ -419,8 +428,10 @@ def family_roofline(ctx, inputs, shapes):
     achieved = alg[dominant] / (fam_ms[dominant] / 1000.0) / 1e9
     per = len(shapes)
     return ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-             "traffic": read_traffic(dominant), "kernel": dominant, "peak_source": peak_kind,
-             "algorithmic_bytes_per_proof": alg[dominant] / per, "ms_per_proof": fam_ms[dominant] / per},
+             "traffic": read_traffic(dominant, alg[dominant] / per), "kernel": dominant, "peak_source": peak_kind,
+             "algorithmic_bytes_per_proof": alg[dominant] / per, "ms_per_proof": fam_ms[dominant] / per,
+             "traffic_unit": "DRAM bytes per proof of the family",
+             "binding_limit": ALU_BOUND.get(dominant, "HBM")},
             {f: round(v / per, 4) for f, v in fam_ms.items()})
 
 
