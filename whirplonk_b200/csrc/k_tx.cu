@@ -323,41 +323,62 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
     if (present) cur[pos] = pv;
     __syncthreads();
 
-    u64 node_hint_off = hint_base + total_hint;
-    u32 u = tot_distinct;
-    u64 level_off = 0, level_len = a.N;
-    // (the reference leaf layer is 2^ceil(log2 N) = N for power-of-two N)
-    for (u32 lvl = 0; lvl < a.logN; ++lvl) {
-        const bool act = t < u;
-        u64 v = act ? cur[t] : 0;
-        bool sib_present = false;
-        if (act) {
-            if ((v & 1) == 0) sib_present = (t + 1 < u) && cur[t + 1] == v + 1;
-            else sib_present = (t > 0) && cur[t - 1] == v - 1;
+    // Per level L the nodes are the distinct values of cur[j] >> L (cur is sorted,
+    // so equal values are adjacent); a node x emits its sibling x ^ 1 unless the
+    // sibling is itself a node.  Warp L handles level L: it walks cur in chunks
+    // of 32 lanes and ranks its emitters with a ballot.  The per-level counts are
+    // prefix-summed, so every warp writes its siblings at the reference's
+    // position (level by level, increasing x within a level) after one barrier.
+    __shared__ u32 lvl_cnt[32];
+    const u32 u = tot_distinct;
+    const u32 warp = t >> 5, lane = t & 31;
+    auto present_at = [&](u64 y, u32 L) -> bool {  // is y a node of level L?
+        u32 lo = 0, hi = u;
+        while (lo < hi) {
+            const u32 mid = (lo + hi) >> 1;
+            if ((cur[mid] >> L) < y) lo = mid + 1;
+            else hi = mid;
         }
-        const bool emit = act && !sib_present;
-        const u32 epos = block_scan(emit, warp_tot, &total);
-        const u32 nemit = total;
-        if (emit && fits && node_hint_off + 32ull * (epos + 1) <= tx->hints_cap) {
-            const uint4* src = reinterpret_cast<const uint4*>(a.nodes + (level_off + (v ^ 1)) * 8);
-            const uint4 h0 = src[0], h1 = src[1];
-            unsigned char* dst = tx->hints + node_hint_off + 32ull * epos;
-            const unsigned w8[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
-            for (int k = 0; k < 32; ++k) dst[k] = (unsigned char)(w8[k >> 2] >> (8 * (k & 3)));
-        }
-        node_hint_off += 32ull * nemit;
-        // next level: parents, deduplicated (sorted input -> equal parents are adjacent)
-        const u64 par = v >> 1;
-        const bool keep = act && (t == 0 || (cur[t - 1] >> 1) != par);
-        __syncthreads();
-        const u32 kpos = block_scan(keep, warp_tot, &total);
-        const u32 nu = total;
-        if (keep) cur[kpos] = par;
-        __syncthreads();
-        u = nu;
-        level_off += level_len;
-        level_len >>= 1;
+        return lo < u && (cur[lo] >> L) == y;
+    };
+    auto emits = [&](u32 j, u32 L) -> bool {
+        if (j >= u) return false;
+        const u64 x = cur[j] >> L;
+        const bool first = j == 0 || (cur[j - 1] >> L) != x;
+        return first && !present_at(x ^ 1, L);
+    };
+    if (warp < a.logN) {
+        u32 cnt = 0;
+        for (u32 j0 = 0; j0 < u; j0 += 32) cnt += __popc(__ballot_sync(0xFFFFFFFFu, emits(j0 + lane, warp)));
+        if (lane == 0) lvl_cnt[warp] = cnt;
     }
+    __syncthreads();
+    u64 node_hint_off = hint_base + total_hint;
+    if (warp < a.logN) {
+        const u32 L = warp;
+        u64 base = node_hint_off;
+        for (u32 k = 0; k < L; ++k) base += 32ull * lvl_cnt[k];
+        const u64 level_off = (2ull << a.logN) - (2ull << (a.logN - L));
+        u32 rank = 0;
+        for (u32 j0 = 0; j0 < u; j0 += 32) {
+            const u32 j = j0 + lane;
+            const bool e = emits(j, L);
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, e);
+            if (e) {
+                const u64 dst_off = base + 32ull * (rank + __popc(m & ((1u << lane) - 1)));
+                if (fits && dst_off + 32 <= tx->hints_cap) {
+                    const u64 x = cur[j] >> L;
+                    const uint4* src = reinterpret_cast<const uint4*>(a.nodes + (level_off + (x ^ 1)) * 8);
+                    const uint4 h0 = src[0], h1 = src[1];
+                    unsigned char* dst = tx->hints + dst_off;
+                    const unsigned w8[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+                    for (int k = 0; k < 32; ++k) dst[k] = (unsigned char)(w8[k >> 2] >> (8 * (k & 3)));
+                }
+            }
+            rank += __popc(m);
+        }
+    }
+    for (u32 k = 0; k < a.logN; ++k) node_hint_off += 32ull * lvl_cnt[k];
     if (t < 32) {
         if (!fits || node_hint_off > wt.hints_cap) wt.err |= TX_ERR_HINT_OVERFLOW;
         else wt.hints_len = node_hint_off;
