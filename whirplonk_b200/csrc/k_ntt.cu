@@ -27,9 +27,11 @@ namespace wg {
 __device__ __forceinline__ u32 bitrev(u32 j, u32 bits) { return bits ? (__brev(j) >> (32 - bits)) : 0; }
 
 // Shared-memory word of column element e: one pad word every 32 words keeps
-// strided group accesses off a single bank.
+// strided group accesses off a single bank; the extra word per column puts the
+// W columns of a tile on different banks (the transposed store phase reads
+// one element of each column per step).
 __device__ __forceinline__ u32 pidx(u32 e) { return e + (e >> 5); }
-__host__ __device__ __forceinline__ u32 col_stride(u32 logR) { return (1u << logR) + ((1u << logR) >> 5); }
+__host__ __device__ __forceinline__ u32 col_stride(u32 logR) { return (1u << logR) + ((1u << logR) >> 5) + 1; }
 
 // Stages s0+1 .. s0+RR of a radix-2 DIT on W bit-reversed columns of 2^L
 // words, done as independent radix-2^RR groups in registers: a group is the
@@ -137,6 +139,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
         }
     } else {
         const u32 n = W << mrows_log;
+#pragma unroll 4
         for (u32 e = threadIdx.x; e < n; e += blockDim.x) {
             const u32 w = e >> mrows_log, j = e & ((1u << mrows_log) - 1);
             u64 v;
