@@ -87,6 +87,26 @@ size_t oracle_merkle_open(const u8* leaves, size_t n, const u64* idx, size_t nid
     return hints.size();
 }
 u64 oracle_find_nonce(const u8* ch, u64 threshold) { return find_nonce(ch, threshold); }
+u64 oracle_find_nonce_sha2(const u8* ch, u64 threshold) { return find_nonce(ch, threshold, Engine::Sha2); }
+void oracle_sha256(const u8* d, size_t n, u8* out) {
+    Hash h = sha256(d, n);
+    std::memcpy(out, h.data(), 32);
+}
+// Merkle root / opening hints with SHA-256 nodes.
+void oracle_merkle_root_sha2(const u8* leaves, size_t n, u8* root_out) {
+    std::vector<Hash> lv(n);
+    for (size_t i = 0; i < n; ++i) std::memcpy(lv[i].data(), leaves + 32 * i, 32);
+    auto nodes = merkle_build(lv, Engine::Sha2);
+    std::memcpy(root_out, nodes.back().data(), 32);
+}
+size_t oracle_merkle_open_sha2(const u8* leaves, size_t n, const u64* idx, size_t nidx, u8* out, size_t cap) {
+    std::vector<Hash> lv(n);
+    for (size_t i = 0; i < n; ++i) std::memcpy(lv[i].data(), leaves + 32 * i, 32);
+    auto nodes = merkle_build(lv, Engine::Sha2);
+    auto hints = merkle_open(nodes, layers_for(n), std::vector<u64>(idx, idx + nidx));
+    for (size_t i = 0; i < hints.size() && i < cap; ++i) std::memcpy(out + 32 * i, hints[i].data(), 32);
+    return hints.size();
+}
 
 // Opaque transcript for the per-primitive pins (base/Ext3 challenges).
 void* oracle_tx_new(void) { return new (std::nothrow) Transcript(); }
@@ -144,9 +164,10 @@ void oracle_mle_eval_base(const u64* v, u64 n, const u64* point, u64* out) {
 // (the buffers receive min(cap, len) bytes).
 int oracle_whir_prove(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique, const u64* coeffs,
                       const u64* points, size_t npoints, const u64* evals, u8* narg, size_t narg_cap,
-                      u8* hints, size_t hints_cap, u64* lens) {
+                      u8* hints, size_t hints_cap, u64* lens, int sha2) {
     try {
         Params p = make_params(rho, k, sec, powb, unique);
+        if (sha2) std::memcpy(p.hash_id, SHA2_ENGINE_ID, 32);
         std::vector<u64> v(coeffs, coeffs + (1ull << n));
         Statement st;
         for (size_t i = 0; i < npoints; ++i) st.mle_points.push_back(read_e3(points + 3 * n * i, n));

@@ -28,6 +28,7 @@
 #include "whir/algebra/goldilocks_ext3.hpp"
 #include "whir/algebra/linear_form.hpp"
 #include "whir/hash/blake3_engine.hpp"
+#include "whir/hash/sha2_engine.hpp"
 #include "whir/parameters.hpp"
 #include "whir/protocols/whir/whir.hpp"
 #include "whir/transcript/transcript.hpp"
@@ -129,11 +130,12 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "usage: ref_driver INPUT OUTPUT [--verify] [--reps R] [--config]\n");
         return 2;
     }
-    bool do_verify = false, print_cfg = false;
+    bool do_verify = false, print_cfg = false, use_sha2 = false;
     int reps = 1;
     for (int i = 3; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--verify")) do_verify = true;
         else if (!std::strcmp(argv[i], "--config")) print_cfg = true;
+        else if (!std::strcmp(argv[i], "--sha2")) use_sha2 = true;
         else if (!std::strcmp(argv[i], "--reps") && i + 1 < argc) reps = std::atoi(argv[++i]);
         else die("bad flag");
     }
@@ -167,7 +169,7 @@ int main(int argc, char** argv) {
     params.unique_decoding = false;
     params.starting_log_inv_rate = rho;
     params.batch_size = 1;
-    params.hash_id = ::whir::hash::ENGINE_ID_BLAKE3;
+    params.hash_id = use_sha2 ? ::whir::hash::ENGINE_ID_SHA2 : ::whir::hash::ENGINE_ID_BLAKE3;
 
     auto config = ::whir::protocols::whir::Config<M>::from_params(size, params);
     if (print_cfg) {

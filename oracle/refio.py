@@ -61,7 +61,7 @@ def ref_available() -> bool:
 
 
 def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1, threads=None,
-                  timeout=3600) -> RefProof:
+                  timeout=3600, sha2=False) -> RefProof:
     """Runs the unmodified reference prover (compiled in place by oracle/Makefile)."""
     if not ref_available():
         raise FileNotFoundError(f"{REF_DRIVER} not built (make -C oracle ref)")
@@ -73,6 +73,8 @@ def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1
         inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         write_input(inp, n, k, rho, sec, pow_bits, points, coeffs)
         cmd = [REF_DRIVER, inp, out] + (["--verify"] if verify else []) + (["--reps", str(reps)] if reps > 1 else [])
+        if sha2:
+            cmd.append("--sha2")
         subprocess.run(cmd, check=True, env=env, timeout=timeout, stdout=subprocess.DEVNULL)
         return read_output(out, npts)
 
@@ -151,13 +153,27 @@ class Oracle:
         L.oracle_whir_config.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, p, sz]
         L.oracle_whir_config.restype = sz
         L.oracle_mle_eval_base.argtypes = [p, u64, p, p]
-        L.oracle_whir_prove.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, p, p, sz, p, p, sz, p, sz, p]
+        L.oracle_whir_prove.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, p, p, sz, p, p, sz, p, sz, p,
+                                        ctypes.c_int]
+        L.oracle_sha256.argtypes = [p, sz, p]
+        L.oracle_sha256.restype = None
+        L.oracle_merkle_root_sha2.argtypes = [p, sz, p]
+        L.oracle_merkle_root_sha2.restype = None
+        L.oracle_merkle_open_sha2.argtypes = [p, sz, p, sz, p, sz]
+        L.oracle_merkle_open_sha2.restype = sz
+        L.oracle_find_nonce_sha2.argtypes = [p, u64]
+        L.oracle_find_nonce_sha2.restype = u64
         L.oracle_whir_prove.restype = ctypes.c_int
 
     # -- primitives -------------------------------------------------------
     def blake3(self, data: bytes) -> bytes:
         out = ctypes.create_string_buffer(32)
         self.lib.oracle_blake3(data, len(data), out)
+        return out.raw
+
+    def sha256(self, data: bytes) -> bytes:
+        out = ctypes.create_string_buffer(32)
+        self.lib.oracle_sha256(data, len(data), out)
         return out.raw
 
     def indices(self, entropy: bytes, N: int, count: int, dedup: bool) -> list:
@@ -192,19 +208,27 @@ class Oracle:
         self.lib.oracle_rs_encode_e3(v.ctypes.data, v.shape[0], N, depth, out.ctypes.data)
         return out
 
-    def merkle_root(self, leaves: bytes) -> bytes:
+    def merkle_root(self, leaves: bytes, sha2: bool = False) -> bytes:
         out = ctypes.create_string_buffer(32)
-        self.lib.oracle_merkle_root(leaves, len(leaves) // 32, out, None)
+        if sha2:
+            self.lib.oracle_merkle_root_sha2(leaves, len(leaves) // 32, out)
+        else:
+            self.lib.oracle_merkle_root(leaves, len(leaves) // 32, out, None)
         return out.raw
 
-    def merkle_open(self, leaves: bytes, idx) -> list:
+    def merkle_open(self, leaves: bytes, idx, sha2: bool = False) -> list:
         idx = np.ascontiguousarray(idx, dtype=np.uint64)
         cap = 64 * max(1, idx.size)
         out = ctypes.create_string_buffer(32 * cap)
+        if sha2:
+            cnt = self.lib.oracle_merkle_open_sha2(leaves, len(leaves) // 32, idx.ctypes.data, idx.size, out, cap)
+            return [out.raw[32 * i:32 * i + 32] for i in range(cnt)]
         cnt = self.lib.oracle_merkle_open(leaves, len(leaves) // 32, idx.ctypes.data, idx.size, out, cap)
         return [out.raw[32 * i:32 * i + 32] for i in range(cnt)]
 
-    def find_nonce(self, challenge: bytes, threshold: int) -> int:
+    def find_nonce(self, challenge: bytes, threshold: int, sha2: bool = False) -> int:
+        if sha2:
+            return self.lib.oracle_find_nonce_sha2(challenge, threshold)
         return self.lib.oracle_find_nonce(challenge, threshold)
 
     def domain_separator(self, rho, k, sec, pow_bits, unique=False) -> bytes:
@@ -225,7 +249,7 @@ class Oracle:
         self.lib.oracle_mle_eval_base(coeffs.ctypes.data, n, point.ctypes.data, out.ctypes.data)
         return out
 
-    def prove(self, n, k, rho, sec, pow_bits, points, coeffs, evaluations):
+    def prove(self, n, k, rho, sec, pow_bits, points, coeffs, evaluations, sha2=False):
         coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
         points = np.ascontiguousarray(points, dtype=np.uint64).reshape(-1, n, 3)
         evals = np.ascontiguousarray(evaluations, dtype=np.uint64).reshape(-1, 3)
@@ -234,7 +258,8 @@ class Oracle:
         hints = ctypes.create_string_buffer(cap)
         lens = (ctypes.c_uint64 * 2)()
         rc = self.lib.oracle_whir_prove(n, rho, k, sec, pow_bits, 0, coeffs.ctypes.data, points.ctypes.data,
-                                        points.shape[0], evals.ctypes.data, narg, cap, hints, cap, lens)
+                                        points.shape[0], evals.ctypes.data, narg, cap, hints, cap, lens,
+                                        int(sha2))
         if rc != 0:
             raise RuntimeError("oracle prove failed")
         return narg.raw[:lens[0]], hints.raw[:lens[1]]

@@ -265,6 +265,86 @@ inline Hash blake3(const u8* d, size_t n) {
 }
 
 // ---------------------------------------------------------------------------
+// SHA-256 (FIPS 180-4), the reference's second hash engine
+// (cpp/include/whir/hash/sha2_engine.hpp:47-81 over cpp/third_party/sha256).
+// The round constants and the initial hash value are derived here from their
+// definitions: the first 32 fractional bits of the cube roots of the first 64
+// primes and of the square roots of the first 8 primes.
+// ---------------------------------------------------------------------------
+constexpr u64 sha_prime(int k) {
+    u64 n = 1;
+    for (int found = -1; found < k;) {
+        ++n;
+        bool prime = true;
+        for (u64 d = 2; d * d <= n; ++d)
+            if (n % d == 0) { prime = false; break; }
+        if (prime) ++found;
+    }
+    return n;
+}
+// floor(root-th root of p, with 32 fractional bits) mod 2^32
+constexpr u32 sha_root_frac(u64 p, int root) {
+    using u128 = unsigned __int128;
+    const u128 target = (u128)p << (32 * root);
+    u64 lo = 0, hi = 1ull << 40;
+    while (lo + 1 < hi) {
+        const u64 mid = (lo + hi) / 2;
+        u128 v = 1;
+        for (int i = 0; i < root; ++i) v *= mid;
+        if (v <= target) lo = mid;
+        else hi = mid;
+    }
+    return (u32)lo;
+}
+struct Sha256Consts {
+    u32 k[64], h0[8];
+    constexpr Sha256Consts() : k(), h0() {
+        for (int i = 0; i < 64; ++i) k[i] = sha_root_frac(sha_prime(i), 3);
+        for (int i = 0; i < 8; ++i) h0[i] = sha_root_frac(sha_prime(i), 2);
+    }
+};
+inline constexpr Sha256Consts SHA256_C{};
+inline u32 ror32(u32 x, int s) { return (x >> s) | (x << (32 - s)); }
+inline void sha256_compress(u32 h[8], const u8 blk[64]) {
+    u32 w[64];
+    for (int i = 0; i < 16; ++i) w[i] = (u32)blk[4 * i] << 24 | (u32)blk[4 * i + 1] << 16 | (u32)blk[4 * i + 2] << 8 | blk[4 * i + 3];
+    for (int i = 16; i < 64; ++i) {
+        const u32 s0 = ror32(w[i - 15], 7) ^ ror32(w[i - 15], 18) ^ (w[i - 15] >> 3);
+        const u32 s1 = ror32(w[i - 2], 17) ^ ror32(w[i - 2], 19) ^ (w[i - 2] >> 10);
+        w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+    }
+    u32 a = h[0], b = h[1], c = h[2], d = h[3], e = h[4], f = h[5], g = h[6], hh = h[7];
+    for (int i = 0; i < 64; ++i) {
+        const u32 t1 = hh + (ror32(e, 6) ^ ror32(e, 11) ^ ror32(e, 25)) + ((e & f) ^ (~e & g)) + SHA256_C.k[i] + w[i];
+        const u32 t2 = (ror32(a, 2) ^ ror32(a, 13) ^ ror32(a, 22)) + ((a & b) ^ (a & c) ^ (b & c));
+        hh = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + t2;
+    }
+    h[0] += a; h[1] += b; h[2] += c; h[3] += d; h[4] += e; h[5] += f; h[6] += g; h[7] += hh;
+}
+inline Hash sha256(const u8* d, size_t n) {
+    u32 h[8];
+    for (int i = 0; i < 8; ++i) h[i] = SHA256_C.h0[i];
+    size_t full = n / 64;
+    for (size_t b = 0; b < full; ++b) sha256_compress(h, d + 64 * b);
+    u8 tail[128] = {};
+    const size_t rem = n - 64 * full;
+    if (rem) std::memcpy(tail, d + 64 * full, rem);
+    tail[rem] = 0x80;
+    const size_t tl = rem + 9 <= 64 ? 64 : 128;
+    const u64 bits = (u64)n * 8;
+    for (int i = 0; i < 8; ++i) tail[tl - 1 - i] = (u8)(bits >> (8 * i));
+    for (size_t b = 0; b < tl / 64; ++b) sha256_compress(h, tail + 64 * b);
+    Hash out;
+    for (int i = 0; i < 8; ++i) for (int j = 0; j < 4; ++j) out[4 * i + j] = (u8)(h[i] >> (24 - 8 * j));
+    return out;
+}
+
+// The engine a configuration's hash_id selects (irs_commit.hpp:62-74): SHA-256
+// for ENGINE_ID_SHA2, BLAKE3 otherwise.
+enum class Engine { Blake3, Sha2 };
+inline Hash hash_with(Engine e, const u8* d, size_t n) { return e == Engine::Sha2 ? sha256(d, n) : blake3(d, n); }
+
+// ---------------------------------------------------------------------------
 // Fiat-Shamir transcript (cpp/include/whir/transcript/transcript.hpp).
 // absorb continues the SHAKE128 hasher; the first squeeze after an absorb
 // finalises a clone of the hasher and later squeezes keep reading that XOF
@@ -312,6 +392,11 @@ struct Transcript {
 // "Example at src/bin/main.rs:133"); absorbed as protocol_id || session_id ||
 // instance bytes (transcript.hpp:533-539; instance Empty -> no bytes).
 // ---------------------------------------------------------------------------
+// Engine ids of the reference's hash engines (cpp/include/whir/hash/blake3_engine.hpp,
+// sha2_engine.hpp:38-43), copied: they are identifiers, not computed here.
+constexpr u8 SHA2_ENGINE_ID[32] = {0x01, 0x8e, 0xaa, 0x24, 0x7c, 0xb8, 0x95, 0x7a, 0xb1, 0xe9, 0xfd,
+                                   0xac, 0x88, 0x54, 0x50, 0x40, 0x3c, 0x5e, 0x7b, 0xda, 0x1a, 0xca,
+                                   0xaa, 0x50, 0x4e, 0x4c, 0xc8, 0xf2, 0xf7, 0x6b, 0xb0, 0x76};
 constexpr u8 BLAKE3_ENGINE_ID[32] = {0x03, 0xe0, 0x17, 0x49, 0xeb, 0xcc, 0x04, 0x77, 0x92, 0x42, 0x54,
                                      0xeb, 0x48, 0x20, 0x66, 0xb8, 0x64, 0xa8, 0xdd, 0x4d, 0x77, 0x25,
                                      0x24, 0x64, 0xca, 0x6f, 0x5b, 0x6f, 0x5c, 0xc0, 0x5b, 0x4c};
@@ -522,7 +607,7 @@ inline std::vector<E3> rs_encode_e3(const std::vector<E3>& v, u64 N, u64 depth) 
 // parent = BLAKE3(left || right), node array [leaves | level 1 | ... | root].
 // ---------------------------------------------------------------------------
 inline u64 layers_for(u64 n) { u64 k = 0; while ((1ull << k) < n) ++k; return n <= 1 ? 0 : k; }
-inline std::vector<Hash> merkle_build(std::vector<Hash> leaves) {
+inline std::vector<Hash> merkle_build(std::vector<Hash> leaves, Engine eng = Engine::Blake3) {
     u64 L = layers_for(leaves.size());
     u64 leaf_layer = 1ull << L;
     std::vector<Hash> nodes = std::move(leaves);
@@ -535,7 +620,7 @@ inline std::vector<Hash> merkle_build(std::vector<Hash> leaves) {
             u8 buf[64];
             std::memcpy(buf, nodes[prev_off + 2 * i].data(), 32);
             std::memcpy(buf + 32, nodes[prev_off + 2 * i + 1].data(), 32);
-            nodes[cur + i] = blake3(buf, 64);
+            nodes[cur + i] = hash_with(eng, buf, 64);
         }
         prev_off = cur;
         prev_len = cur_len;
@@ -565,20 +650,20 @@ inline std::vector<Hash> merkle_open(const std::vector<Hash>& nodes, u64 L, std:
 
 // Leaf hashes of a row-major matrix, LE canonical bytes per element
 // (matrix_commit.hpp:74-195).
-inline std::vector<Hash> leaves_base(const std::vector<u64>& mat, u64 cols) {
+inline std::vector<Hash> leaves_base(const std::vector<u64>& mat, u64 cols, Engine eng = Engine::Blake3) {
     u64 rows = mat.size() / cols;
     std::vector<Hash> out(rows);
 #pragma omp parallel for if (rows >= 1024)
     for (long long r = 0; r < (long long)rows; ++r)
-        out[r] = blake3(reinterpret_cast<const u8*>(&mat[r * cols]), cols * 8);
+        out[r] = hash_with(eng, reinterpret_cast<const u8*>(&mat[r * cols]), cols * 8);
     return out;
 }
-inline std::vector<Hash> leaves_e3(const std::vector<E3>& mat, u64 cols) {
+inline std::vector<Hash> leaves_e3(const std::vector<E3>& mat, u64 cols, Engine eng = Engine::Blake3) {
     u64 rows = mat.size() / cols;
     std::vector<Hash> out(rows);
 #pragma omp parallel for if (rows >= 1024)
     for (long long r = 0; r < (long long)rows; ++r)
-        out[r] = blake3(reinterpret_cast<const u8*>(&mat[r * cols]), cols * 24);
+        out[r] = hash_with(eng, reinterpret_cast<const u8*>(&mat[r * cols]), cols * 24);
     return out;
 }
 
@@ -586,31 +671,31 @@ inline std::vector<Hash> leaves_e3(const std::vector<E3>& mat, u64 cols) {
 // Proof of work (proof_of_work.hpp:95-193, 236-257): smallest nonce n >= 0 with
 // LE_u64(BLAKE3(challenge || n_le8 || 0^24)[0..8]) <= threshold.
 // ---------------------------------------------------------------------------
-inline u64 pow_hash_u64(const u8 ch[32], u64 nonce) {
+inline u64 pow_hash_u64(const u8 ch[32], u64 nonce, Engine eng = Engine::Blake3) {
     u8 msg[64] = {};
     std::memcpy(msg, ch, 32);
     std::memcpy(msg + 32, &nonce, 8);
-    Hash h = blake3(msg, 64);
+    Hash h = hash_with(eng, msg, 64);
     u64 v;
     std::memcpy(&v, h.data(), 8);
     return v;
 }
-inline u64 find_nonce(const u8 ch[32], u64 threshold) {
+inline u64 find_nonce(const u8 ch[32], u64 threshold, Engine eng = Engine::Blake3) {
     if (threshold == ~0ull) return 0;
     const u64 W = 1 << 14;
     for (u64 base = 0;; base += W * 64) {
         u64 best = ~0ull;
 #pragma omp parallel for reduction(min : best) schedule(static)
         for (long long i = 0; i < (long long)(W * 64); ++i)
-            if (pow_hash_u64(ch, base + (u64)i) <= threshold) best = std::min(best, base + (u64)i);
+            if (pow_hash_u64(ch, base + (u64)i, eng) <= threshold) best = std::min(best, base + (u64)i);
         if (best != ~0ull) return best;
     }
 }
-inline void pow_prove(Transcript& t, u64 threshold) {
+inline void pow_prove(Transcript& t, u64 threshold, Engine eng = Engine::Blake3) {
     if (threshold == ~0ull) return;
     u8 ch[32];
     t.squeeze(ch, 32);
-    t.message_u64(find_nonce(ch, threshold));
+    t.message_u64(find_nonce(ch, threshold, eng));
 }
 
 // ---------------------------------------------------------------------------
@@ -689,7 +774,7 @@ inline void fold(std::vector<E3>& v, const E3& r) {
     v.resize(h);
 }
 inline std::vector<E3> sumcheck_prove(Transcript& t, const SumcheckCfg& cfg, std::vector<E3>& a,
-                                      std::vector<E3>& b, E3& sum) {
+                                      std::vector<E3>& b, E3& sum, Engine eng = Engine::Blake3) {
     std::vector<E3> rs;
     for (u64 r = 0; r < cfg.num_rounds; ++r) {
         size_t h = a.size() / 2;
@@ -701,7 +786,7 @@ inline std::vector<E3> sumcheck_prove(Transcript& t, const SumcheckCfg& cfg, std
         E3 c1 = sum - (c0 + c0) - c2;
         t.message_e3(c0);
         t.message_e3(c2);
-        pow_prove(t, cfg.pow_threshold);
+        pow_prove(t, cfg.pow_threshold, eng);
         E3 rnd = t.challenge_e3();
         rs.push_back(rnd);
         fold(a, rnd);
@@ -724,11 +809,11 @@ struct Witness {
     Hash root() const { return nodes.back(); }
 };
 
-inline Witness commit_base(Transcript& t, const IrsCfg& c, const std::vector<u64>& v) {
+inline Witness commit_base(Transcript& t, const IrsCfg& c, const std::vector<u64>& v, Engine eng = Engine::Blake3) {
     Witness w;
     w.base = true; w.N = c.codeword_length; w.depth = c.depth; w.layers = layers_for(w.N);
     w.mat_base = rs_encode_base(v, w.N, w.depth);
-    w.nodes = merkle_build(leaves_base(w.mat_base, w.depth));
+    w.nodes = merkle_build(leaves_base(w.mat_base, w.depth, eng), eng);
     t.message_hash(w.root());
     for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_e3());
     for (const E3& z : w.ood_points) {
@@ -738,11 +823,11 @@ inline Witness commit_base(Transcript& t, const IrsCfg& c, const std::vector<u64
     }
     return w;
 }
-inline Witness commit_e3(Transcript& t, const IrsCfg& c, const std::vector<E3>& v) {
+inline Witness commit_e3(Transcript& t, const IrsCfg& c, const std::vector<E3>& v, Engine eng = Engine::Blake3) {
     Witness w;
     w.base = false; w.N = c.codeword_length; w.depth = c.depth; w.layers = layers_for(w.N);
     w.mat_e3 = rs_encode_e3(v, w.N, w.depth);
-    w.nodes = merkle_build(leaves_e3(w.mat_e3, w.depth));
+    w.nodes = merkle_build(leaves_e3(w.mat_e3, w.depth, eng), eng);
     t.message_hash(w.root());
     for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_e3());
     for (const E3& z : w.ood_points) {
@@ -816,12 +901,13 @@ struct ProofOut { std::vector<u8> narg, hints; std::vector<E3> evaluation_point;
 
 inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statement& st, const DomainSep& ds) {
     WhirCfg cfg = whir_from_params(v.size(), p);
+    const Engine eng = std::memcmp(p.hash_id, SHA2_ENGINE_ID, 32) == 0 ? Engine::Sha2 : Engine::Blake3;
     Transcript t;
     t.absorb(ds.protocol_id, 64);
     t.absorb(ds.session_id, 32);
     ProofOut out;
     // commit
-    Witness w0 = commit_base(t, cfg.initial, v);
+    Witness w0 = commit_base(t, cfg.initial, v, eng);
     out.initial_root = w0.root();
     const size_t nforms = st.mle_points.size() + st.covectors.size();
     // step 2: vector RLC of one vector is [1], no squeeze; lift
@@ -848,10 +934,10 @@ inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statemen
     for (size_t j = 0; j < ood_rlc.size(); ++j) sum = sum + ood_rlc[j] * w0.ood_values[j];
     // step 5: initial sumcheck
     std::vector<E3> last_r;
-    if (has_constraints) last_r = sumcheck_prove(t, cfg.initial_sumcheck, vec, cov, sum);
+    if (has_constraints) last_r = sumcheck_prove(t, cfg.initial_sumcheck, vec, cov, sum, eng);
     else {
         for (u64 r = 0; r < cfg.initial_sumcheck.num_rounds; ++r) last_r.push_back(t.challenge_e3());
-        pow_prove(t, cfg.initial_skip_pow);
+        pow_prove(t, cfg.initial_skip_pow, eng);
         for (const E3& r : last_r) fold(vec, r);
         cov.assign(cfg.initial_sumcheck.initial_size >> cfg.initial_sumcheck.num_rounds, E3());
     }
@@ -863,9 +949,9 @@ inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statemen
     stored.reserve(cfg.rounds.size());
     for (size_t rd = 0; rd < cfg.rounds.size(); ++rd) {
         const RoundCfg& rc = cfg.rounds[rd];
-        stored.push_back(commit_e3(t, rc.irs, vec));
+        stored.push_back(commit_e3(t, rc.irs, vec, eng));
         const Witness& nw = stored.back();
-        pow_prove(t, rc.pow_threshold);
+        pow_prove(t, rc.pow_threshold, eng);
         Opening o = open_witness(t, *prev_cfg, *prev);
         std::vector<E3> pts = nw.ood_points;
         pts.insert(pts.end(), o.points.begin(), o.points.end());
@@ -879,16 +965,16 @@ inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statemen
         auto srlc = geometric_challenge(t, pts.size());
         geometric_accumulate(cov, srlc, pts);
         for (size_t j = 0; j < srlc.size(); ++j) sum = sum + srlc[j] * vals[j];
-        last_r = sumcheck_prove(t, rc.sumcheck, vec, cov, sum);
+        last_r = sumcheck_prove(t, rc.sumcheck, vec, cov, sum, eng);
         out.evaluation_point.insert(out.evaluation_point.end(), last_r.begin(), last_r.end());
         prev = &nw;
         prev_cfg = &rc.irs;
     }
     // steps 7-10
     for (const E3& c : vec) t.message_e3(c);
-    pow_prove(t, cfg.final_pow);
+    pow_prove(t, cfg.final_pow, eng);
     open_witness(t, *prev_cfg, *prev);
-    auto fr = sumcheck_prove(t, cfg.final_sumcheck, vec, cov, sum);
+    auto fr = sumcheck_prove(t, cfg.final_sumcheck, vec, cov, sum, eng);
     out.evaluation_point.insert(out.evaluation_point.end(), fr.begin(), fr.end());
     out.narg = std::move(t.narg);
     out.hints = std::move(t.hints);

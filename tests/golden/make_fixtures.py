@@ -87,7 +87,7 @@ def fields():
     return out
 
 
-def hashes():
+def hashes(engine="blake3"):
     rng = Lcg(0xAAAAAAAAAAAAAAAA)
 
     def make_bytes(n):
@@ -108,7 +108,7 @@ def hashes():
     for (eng, size, cnt), c in zip(spec, got):
         data = make_bytes(size * cnt)
         assert f"{eng} size={size} count={cnt}" in c["head"], c["head"]
-        if eng != "blake3":
+        if eng != engine:
             continue
         digests = [r.split()[1] for r in c["rows"]]
         out.append({"size": size, "messages": [data[i * size:(i + 1) * size].hex() for i in range(cnt)],
@@ -116,12 +116,12 @@ def hashes():
     return out
 
 
-def merkle():
+def merkle(engine="blake3"):
     got = cases(sections(read(f"{DUMPS}/merkle_tree_output/golden_merkle_tree_cpp.txt"))["merkle_tree"])
     spec = [("blake3", 16, [3, 5, 11]), ("blake3", 32, [0, 1, 2, 31]), ("sha2", 8, [2, 6])]
     out = []
     for (eng, nl, idx), c in zip(spec, got):
-        if eng != "blake3":
+        if eng != engine:
             continue
         leaves = bytes(((i * 31 + j) & 0xFF) for i in range(nl) for j in range(32))
         rows = {r.split()[0]: r.split()[1] for r in c["rows"]}
@@ -215,10 +215,12 @@ def sumcheck():
     return out
 
 
-PROOF_CASES = [  # (n, k, rho, security, pow_bits, seed, n_points)
+PROOF_CASES = [  # (n, k, rho, security, pow_bits, seed, n_points[, hash engine])
     (4, 4, 1, 100, 20, 11, 1), (5, 4, 1, 100, 20, 12, 1), (8, 4, 1, 100, 20, 13, 1), (9, 2, 2, 80, 10, 14, 1),
     (10, 4, 1, 100, 20, 15, 2), (12, 3, 2, 100, 20, 16, 1), (13, 1, 1, 64, 16, 17, 1), (14, 4, 1, 100, 20, 18, 1),
     (16, 4, 3, 100, 0, 19, 1), (18, 4, 1, 100, 20, 20, 1), (20, 4, 2, 128, 20, 21, 1),
+    (5, 4, 1, 100, 20, 31, 1, "sha2"), (10, 4, 2, 100, 20, 32, 1, "sha2"), (14, 4, 1, 100, 20, 33, 2, "sha2"),
+    (16, 4, 3, 100, 16, 34, 1, "sha2"),
 ]
 
 
@@ -227,12 +229,15 @@ def proofs():
     from whirplonk_b200 import sample_goldilocks
 
     out = []
-    for n, k, rho, sec, pb, seed, npts in PROOF_CASES:
+    for case in PROOF_CASES:
+        n, k, rho, sec, pb, seed, npts = case[:7]
+        sha2 = len(case) > 7 and case[7] == "sha2"
         coeffs = sample_goldilocks(seed, 1 << n)
         points = sample_goldilocks(seed + 5000, npts * n * 3).reshape(npts, n, 3)
-        ref = run_reference(n, k, rho, sec, pb, points, coeffs, verify=True)
+        ref = run_reference(n, k, rho, sec, pb, points, coeffs, verify=True, sha2=sha2)
         assert ref.verify_ok == 1.0
         rec = {"n": n, "k": k, "rho": rho, "security": sec, "pow_bits": pb, "seed": seed, "n_points": npts,
+               "hash": "sha2" if sha2 else "blake3",
                "evaluations": [[int(x) for x in row] for row in ref.evaluations],
                "narg_len": len(ref.narg), "hints_len": len(ref.hints),
                "narg_sha256": hashlib.sha256(ref.narg).hexdigest(),
@@ -247,7 +252,8 @@ def proofs():
 def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
-            "indices": indices(), "pow": pow_golden(), "sumcheck": sumcheck()}
+            "indices": indices(), "pow": pow_golden(), "sumcheck": sumcheck(),
+            "sha2": hashes("sha2"), "merkle_sha2": merkle("sha2")}
     with open(os.path.join(HERE, "reference_goldens.json"), "w") as f:
         json.dump(gold, f, indent=1)
     with open(os.path.join(HERE, "reference_proofs.json"), "w") as f:

@@ -63,6 +63,24 @@ def test_merkle_known_answers(oracle):
         assert [h.hex() for h in oracle.merkle_open(leaves, case["indices"])] == case["hints"]
 
 
+def test_sha256_known_answers(oracle):
+    """The reference's SHA-256 engine dumps (hash_output, sha2 cases) and hashlib."""
+    for case in GOLD["sha2"]:
+        for msg, dig in zip(case["messages"], case["digests"]):
+            assert oracle.sha256(bytes.fromhex(msg)).hex() == dig
+            assert hashlib.sha256(bytes.fromhex(msg)).hexdigest() == dig
+    for n in (0, 55, 56, 63, 64, 119, 120, 128, 384):
+        m = bytes((7 * i + 3) & 0xFF for i in range(n))
+        assert oracle.sha256(m) == hashlib.sha256(m).digest()
+
+
+def test_merkle_sha2_known_answers(oracle):
+    for case in GOLD["merkle_sha2"]:
+        leaves = bytes.fromhex(case["leaves"])
+        assert oracle.merkle_root(leaves, sha2=True).hex() == case["root"]
+        assert [h.hex() for h in oracle.merkle_open(leaves, case["indices"], sha2=True)] == case["hints"]
+
+
 def test_matrix_commit_leaves(oracle):
     for case in GOLD["matrix_commit"]:
         for row, leaf in zip(case["rows"], case["leaves"]):
@@ -115,14 +133,15 @@ def _case_inputs(case):
     return coeffs, points
 
 
-@pytest.mark.parametrize("case", PROOFS, ids=lambda c: f"n{c['n']}k{c['k']}r{c['rho']}s{c['security']}p{c['pow_bits']}")
+@pytest.mark.parametrize("case", PROOFS,
+                         ids=lambda c: f"n{c['n']}k{c['k']}r{c['rho']}s{c['security']}p{c['pow_bits']}{c['hash']}")
 def test_oracle_proofs_match_reference_fixtures(oracle, case):
     coeffs, points = _case_inputs(case)
     evals = np.array(case["evaluations"], dtype=np.uint64)
     for i in range(case["n_points"]):
         assert [int(x) for x in oracle.mle_eval_base(coeffs, points[i])] == case["evaluations"][i]
     narg, hints = oracle.prove(case["n"], case["k"], case["rho"], case["security"], case["pow_bits"], points, coeffs,
-                               evals)
+                               evals, sha2=case["hash"] == "sha2")
     assert (len(narg), len(hints)) == (case["narg_len"], case["hints_len"])
     assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
     assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
@@ -131,11 +150,12 @@ def test_oracle_proofs_match_reference_fixtures(oracle, case):
 
 
 @pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("n,k,rho,sec,pb,seed", [(6, 2, 1, 90, 12, 901), (11, 4, 2, 100, 20, 902), (15, 3, 1, 100, 18, 903)])
-def test_oracle_matches_live_reference(oracle, n, k, rho, sec, pb, seed):
+@pytest.mark.parametrize("n,k,rho,sec,pb,seed,sha2", [(6, 2, 1, 90, 12, 901, False), (11, 4, 2, 100, 20, 902, False),
+                                                      (15, 3, 1, 100, 18, 903, False), (9, 4, 2, 100, 20, 904, True)])
+def test_oracle_matches_live_reference(oracle, n, k, rho, sec, pb, seed, sha2):
     coeffs = sample_goldilocks(seed, 1 << n)
     points = sample_goldilocks(seed + 1, n * 3).reshape(1, n, 3)
-    ref = run_reference(n, k, rho, sec, pb, points, coeffs, verify=True)
+    ref = run_reference(n, k, rho, sec, pb, points, coeffs, verify=True, sha2=sha2)
     assert ref.verify_ok == 1.0
-    narg, hints = oracle.prove(n, k, rho, sec, pb, points, coeffs, ref.evaluations)
+    narg, hints = oracle.prove(n, k, rho, sec, pb, points, coeffs, ref.evaluations, sha2=sha2)
     assert narg == ref.narg and hints == ref.hints
