@@ -5,7 +5,7 @@
  * ProtocolParameters, the same SHAKE128 Fiat-Shamir transcript and the same
  * proof byte layout ({narg_string, hints}), for
  *   M = Basefield<GoldilocksExt3> (Goldilocks vectors, Ext3 challenges),
- *   hash = BLAKE3, one committed vector, MultilinearExtension statements.
+ *   hash = BLAKE3 or SHA-2, one committed vector, MultilinearExtension statements.
  * Everything below is plain C: opaque handles, pointers, sizes and status
  * codes; no C++ types or exceptions cross this boundary.
  *
@@ -26,7 +26,7 @@ extern "C" {
 typedef enum {
     WHIRGPU_OK = 0,
     WHIRGPU_E_INVALID = 1,     /* bad argument or parameters the reference asserts on */
-    WHIRGPU_E_UNSUPPORTED = 2, /* valid for the reference but not on this path (e.g. SHA2 hash) */
+    WHIRGPU_E_UNSUPPORTED = 2, /* valid for the reference but not on this path (e.g. batch_size > 1) */
     WHIRGPU_E_OOM = 3,         /* device or pinned memory exhausted, or above the HBM budget */
     WHIRGPU_E_CUDA = 4,        /* CUDA runtime error (text in whirgpu_last_error) */
     WHIRGPU_E_DEVICE = 5,      /* a kernel reported an error word (overflow, PoW exhausted) */
@@ -44,7 +44,7 @@ typedef struct {
     uint64_t security_level;
     uint64_t pow_bits;
     uint64_t batch_size;
-    uint8_t hash_id[32]; /* EngineId; only BLAKE3 (03e01749...5b4c) is on this path */
+    uint8_t hash_id[32]; /* EngineId: BLAKE3 (03e01749...5b4c) or SHA-2 (018eaa24...b076) */
 } whirgpu_params;
 
 typedef struct whirgpu_ctx whirgpu_ctx;

@@ -57,7 +57,7 @@ bool is_pinned_host(const void* p) {
 }
 
 whirgpu_status check_request(whirgpu_ctx* c, const whirgpu_request& r) {
-    if (!is_blake3(&r.params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 engine is on this path");
+    if (!engine_supported(&r.params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 and SHA-2 engines are on this path");
     if (r.num_variables >= 40 || r.num_points > (uint64_t)MAX_FORMS) return fail(c, WHIRGPU_E_INVALID, "bad request");
     if (r.num_points && (!r.points || !r.evaluations)) return fail(c, WHIRGPU_E_INVALID, "bad statement");
     if (!r.coeffs) return fail(c, WHIRGPU_E_INVALID, "null coefficients");

@@ -171,7 +171,8 @@ whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_param
     }
     auto key = std::make_tuple(n, params->starting_log_inv_rate, params->initial_folding_factor, params->folding_factor,
                                params->security_level, params->pow_bits,
-                               (uint64_t)params->unique_decoding | ((uint64_t)std::max<size_t>(ds_len, 96) << 1));
+                               (uint64_t)params->unique_decoding | ((uint64_t)std::max<size_t>(ds_len, 96) << 1) |
+                                   ((uint64_t)is_sha2(params) << 62));  // the plan carries the hash engine
     std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
     for (Workspace* w : c->cache[key])
         if (!w->busy) {
@@ -205,6 +206,8 @@ whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_param
 }
 
 bool is_blake3(const whirgpu_params* p) { return std::memcmp(p->hash_id, BLAKE3_ENGINE_ID, 32) == 0; }
+bool is_sha2(const whirgpu_params* p) { return std::memcmp(p->hash_id, SHA2_ENGINE_ID, 32) == 0; }
+bool engine_supported(const whirgpu_params* p) { return is_blake3(p) || is_sha2(p); }
 
 void release_workspace(whirgpu_ctx* c, Workspace* w) {
     if (!w) return;
@@ -229,6 +232,7 @@ ProtocolParams to_params(const whirgpu_params* p) {
     q.security_level = p->security_level;
     q.pow_bits = p->pow_bits;
     q.batch_size = p->batch_size;
+    q.hash = is_sha2(p) ? 1 : 0;
     return q;
 }
 
@@ -349,7 +353,7 @@ whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, cons
                               uint64_t n, int where, whirgpu_transcript* tx, whirgpu_witness** out) {
     if (!c || !params || !coeffs || !tx || !out || tx->ctx != c) return fail(c, WHIRGPU_E_INVALID, "null argument");
     *out = nullptr;
-    if (!is_blake3(params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 engine is on this path");
+    if (!engine_supported(params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 and SHA-2 engines are on this path");
     if (n >= 40) return fail(c, WHIRGPU_E_INVALID, "num_variables too large");
     Workspace* ws = nullptr;
     whirgpu_status s = acquire_workspace(c, n, params, tx->ds.size(), &ws);

@@ -19,6 +19,11 @@
 
 namespace wg {
 
+// Engine ids (identifiers of the reference's hash engines, blake3_engine.hpp,
+// sha2_engine.hpp:38-43; carried in ProtocolParameters::hash_id).
+constexpr uint8_t SHA2_ENGINE_ID[32] = {0x01, 0x8e, 0xaa, 0x24, 0x7c, 0xb8, 0x95, 0x7a, 0xb1, 0xe9, 0xfd,
+                                        0xac, 0x88, 0x54, 0x50, 0x40, 0x3c, 0x5e, 0x7b, 0xda, 0x1a, 0xca,
+                                        0xaa, 0x50, 0x4e, 0x4c, 0xc8, 0xf2, 0xf7, 0x6b, 0xb0, 0x76};
 constexpr uint8_t BLAKE3_ENGINE_ID[32] = {0x03, 0xe0, 0x17, 0x49, 0xeb, 0xcc, 0x04, 0x77, 0x92, 0x42, 0x54,
                                           0xeb, 0x48, 0x20, 0x66, 0xb8, 0x64, 0xa8, 0xdd, 0x4d, 0x77, 0x25,
                                           0x24, 0x64, 0xca, 0x6f, 0x5b, 0x6f, 0x5c, 0xc0, 0x5b, 0x4c};
@@ -131,6 +136,8 @@ void release_workspace(whirgpu_ctx* c, Workspace* w);
 void set_capturing(bool on);
 uint64_t graph_kernel_nodes(cudaGraph_t g);
 bool is_blake3(const whirgpu_params* p);
+bool is_sha2(const whirgpu_params* p);
+bool engine_supported(const whirgpu_params* p);  // BLAKE3 or SHA-2
 // Plan size of one proof (bytes of device workspace), or 0 when invalid.
 size_t workspace_bytes(uint64_t n, const whirgpu_params* params);
 }  // namespace wg

@@ -14,6 +14,7 @@
 
 #include "launch.h"
 #include "blake3.cuh"
+#include "sha256.cuh"
 #include "state.cuh"
 #include "wtx.cuh"
 
@@ -31,17 +32,71 @@ __device__ __forceinline__ void load_node(const u32* nodes, u64 idx, unsigned* m
     m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
 }
 
+// The engine a configuration's hash_id selects (irs_commit.hpp:62-74).
+constexpr int HASH_BLAKE3 = 0, HASH_SHA256 = 1;
+template <int H>
+__device__ __forceinline__ void hash64(const unsigned m[16], unsigned out[8]) {
+    if (H == HASH_SHA256) sha256_hash64(m, out);
+    else b3_hash64(m, out);
+}
+
 // Row i = words w = 0 .. depth*ncomp-1 with w -> (element w / ncomp, component w % ncomp),
 // read from plane (component * depth + element).
+template <int NCOMP>
+__device__ __forceinline__ u64 row_word(const u64* __restrict__ planes, u64 N, u32 depth, u64 i, u32 w) {
+    const u32 el = w / NCOMP, c = w - el * NCOMP;
+    return planes[((u64)c * depth + el) * N + i];
+}
+
+// SHA-256 of row i's LE bytes: the 8-byte words become big-endian message
+// words; the 0x80 marker follows the data (always on a word boundary) and the
+// bit length closes the last block.
+template <int NCOMP>
+__device__ __forceinline__ void leaf_sha256(const u64* __restrict__ planes, u64 N, u32 depth, u64 i, unsigned out[8]) {
+    const u32 nwords = depth * NCOMP;
+    const u32 bytes = nwords * 8;
+    const u32 nblk = (bytes + 9 + 63) / 64;
+    unsigned h[8];
+    sha256_init(h);
+    for (u32 t = 0; t < nblk; ++t) {
+        unsigned m[16];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const u32 w = t * 8 + q;
+            if (w < nwords) {
+                const u64 v = row_word<NCOMP>(planes, N, depth, i, w);
+                m[2 * q] = bswap32((unsigned)v);
+                m[2 * q + 1] = bswap32((unsigned)(v >> 32));
+            } else {
+                m[2 * q] = w == nwords ? 0x80000000u : 0u;
+                m[2 * q + 1] = 0;
+            }
+        }
+        if (t + 1 == nblk) {
+            m[14] = 0;
+            m[15] = bytes * 8;
+        }
+        sha256_compress(h, m);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) out[k] = bswap32(h[k]);
+}
+
 // blockIdx.y selects one of several independent matrices (planes and node
 // arrays `plane_stride` / `node_stride` words apart).
-template <int NCOMP>
+template <int NCOMP, int H>
 __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes,
                                                 u64 plane_stride, u64 node_stride) {
     const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     planes += blockIdx.y * plane_stride;
     nodes += blockIdx.y * node_stride;
+    if (H == HASH_SHA256) {
+        unsigned out[8];
+        leaf_sha256<NCOMP>(planes, N, depth, i, out);
+        store_node(nodes, i, out);
+        return;
+    }
     const u32 nwords = depth * NCOMP;           // 64-bit words per row
     const u32 bytes = nwords * 8;
     const u32 nblocks = (bytes + 63) / 64;
@@ -53,10 +108,7 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
         for (int q = 0; q < 8; ++q) {
             const u32 w = t * 8 + q;
             u64 v = 0;
-            if (w < nwords) {
-                const u32 el = w / NCOMP, c = w - el * NCOMP;
-                v = planes[((u64)c * depth + el) * N + i];
-            }
+            if (w < nwords) v = row_word<NCOMP>(planes, N, depth, i, w);
             m[2 * q] = (unsigned)v;
             m[2 * q + 1] = (unsigned)(v >> 32);
         }
@@ -72,32 +124,39 @@ __host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
     return (2ull << logN) - (2ull << (logN - l));
 }
 
-// parent = BLAKE3(left || right)
+// parent = H(left || right)
+template <int H>
 __device__ __forceinline__ void parent_cv(const unsigned l[8], const unsigned r[8], unsigned out[8]) {
     unsigned m[16];
 #pragma unroll
     for (int k = 0; k < 8; ++k) { m[k] = l[k]; m[8 + k] = r[k]; }
-    b3_hash64(m, out);
+    hash64<H>(m, out);
 }
 
 int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
-                       u64 node_stride, cudaStream_t st) {
-    if (depth * ncomp * 8 > 1024) return -1;  // multi-chunk BLAKE3 rows are not on this path
+                       u64 node_stride, int hash, cudaStream_t st) {
+    if (hash != HASH_SHA256 && depth * ncomp * 8 > 1024) return -1;  // multi-chunk BLAKE3 rows are not on this path
     if (count == 0 || count > 65535) return -1;
     if (ncomp != 1 && ncomp != 3) return -1;
     const dim3 grid((unsigned)((N + 255) / 256), count);
-    if (ncomp == 1) k_leaves<1><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
-    else k_leaves<3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+    if (hash == HASH_SHA256) {
+        if (ncomp == 1) k_leaves<1, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+        else k_leaves<3, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+    } else {
+        if (ncomp == 1) k_leaves<1, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+        else k_leaves<3, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+    }
     count_launches(1);
     return 0;
 }
 
-int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st) {
-    return launch_leaves_batch(planes, N, depth, ncomp, nodes, 1, 0, 0, st);
+int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, int hash, cudaStream_t st) {
+    return launch_leaves_batch(planes, N, depth, ncomp, nodes, 1, 0, 0, hash, st);
 }
 
 // One CTA hashes a subtree of height `levels` whose children sit at level
 // `level_in`; every produced level is written to global memory.
+template <int H>
 __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_in, u32 levels, TxState* tx,
                                                 ProofScalars* sc, int commit_idx, int n_ood, int finish,
                                                 u64 node_stride) {
@@ -113,7 +172,7 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
             load_node(nodes, in_off + child, m);
             load_node(nodes, in_off + child + 1, m + 8);
             unsigned cv[8];
-            b3_hash64(m, cv);
+            hash64<H>(m, cv);
             store_node(nodes, out_off + ((u64)blockIdx.x << (levels - 1)) + t, cv);
 #pragma unroll
             for (int k = 0; k < 8; ++k) buf[0][t * 8 + k] = cv[k];
@@ -128,7 +187,7 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
 #pragma unroll
                 for (int k = 0; k < 16; ++k) m[k] = buf[cur][t * 16 + k];
                 unsigned cv[8];
-                b3_hash64(m, cv);
+                hash64<H>(m, cv);
                 store_node(nodes, off + ((u64)blockIdx.x << (levels - 1 - lv)) + t, cv);
 #pragma unroll
                 for (int k = 0; k < 8; ++k) buf[cur ^ 1][t * 8 + k] = cv[k];
@@ -155,6 +214,7 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
 
 // Three tree levels at once: a thread reads 8 consecutive nodes of level
 // `level_in` and writes their 4 parents, 2 grandparents and 1 great-grandparent.
+template <int H>
 __global__ void __launch_bounds__(256) k_merkle8(u32* nodes, u32 logN, u32 level_in, u64 node_stride) {
     const u64 g = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= (1ull << (logN - level_in - 3))) return;
@@ -164,34 +224,35 @@ __global__ void __launch_bounds__(256) k_merkle8(u32* nodes, u32 logN, u32 level
     const u64 o2 = level_offset(logN, level_in + 2) + 2 * g;
     const u64 o3 = level_offset(logN, level_in + 3) + g;
     unsigned m[16], p0[8], p1[8], q0[8], q1[8];
-    load_node(nodes, in + 0, m); load_node(nodes, in + 1, m + 8); b3_hash64(m, p0); store_node(nodes, o1 + 0, p0);
-    load_node(nodes, in + 2, m); load_node(nodes, in + 3, m + 8); b3_hash64(m, p1); store_node(nodes, o1 + 1, p1);
-    parent_cv(p0, p1, q0);
+    load_node(nodes, in + 0, m); load_node(nodes, in + 1, m + 8); hash64<H>(m, p0); store_node(nodes, o1 + 0, p0);
+    load_node(nodes, in + 2, m); load_node(nodes, in + 3, m + 8); hash64<H>(m, p1); store_node(nodes, o1 + 1, p1);
+    parent_cv<H>(p0, p1, q0);
     store_node(nodes, o2 + 0, q0);
-    load_node(nodes, in + 4, m); load_node(nodes, in + 5, m + 8); b3_hash64(m, p0); store_node(nodes, o1 + 2, p0);
-    load_node(nodes, in + 6, m); load_node(nodes, in + 7, m + 8); b3_hash64(m, p1); store_node(nodes, o1 + 3, p1);
-    parent_cv(p0, p1, q1);
+    load_node(nodes, in + 4, m); load_node(nodes, in + 5, m + 8); hash64<H>(m, p0); store_node(nodes, o1 + 2, p0);
+    load_node(nodes, in + 6, m); load_node(nodes, in + 7, m + 8); hash64<H>(m, p1); store_node(nodes, o1 + 3, p1);
+    parent_cv<H>(p0, p1, q1);
     store_node(nodes, o2 + 1, q1);
-    parent_cv(q0, q1, p0);
+    parent_cv<H>(q0, q1, p0);
     store_node(nodes, o3, p0);
 }
 
 // `count` trees `node_stride` words apart; the transcript step (tx non-null)
 // is for a single tree only.
-static int merkle_levels(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, u32 count,
-                         u64 node_stride, cudaStream_t st) {
+template <int H>
+static int merkle_levels_h(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, u32 count,
+                           u64 node_stride, cudaStream_t st) {
     if (count == 0 || count > 65535 || (tx && count != 1)) return -1;
     u32 level = 0;
     // wide levels: 3 at a time while a launch still has >= 2^12 threads
     while (logN - level >= 3 + 12) {
         const u64 threads = 1ull << (logN - level - 3);
-        k_merkle8<<<dim3((unsigned)((threads + 255) / 256), count), 256, 0, st>>>(nodes, logN, level, node_stride);
+        k_merkle8<H><<<dim3((unsigned)((threads + 255) / 256), count), 256, 0, st>>>(nodes, logN, level, node_stride);
         count_launches(1);
         level += 3;
     }
     if (logN == 0) {
         if (tx) {
-            k_merkle<<<dim3(1, count), 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1, node_stride);
+            k_merkle<H><<<dim3(1, count), 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1, node_stride);
             count_launches(1);
         }
         return 0;
@@ -200,7 +261,7 @@ static int merkle_levels(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, in
         const u32 levels = (logN - level) < 9 ? (logN - level) : 9;
         const u32 ctas = 1u << (logN - level - levels);
         const int finish = (level + levels == logN) ? 1 : 0;
-        k_merkle<<<dim3(ctas, count), 256, 0, st>>>(nodes, logN, level, levels, tx, sc, commit_idx, n_ood, finish,
+        k_merkle<H><<<dim3(ctas, count), 256, 0, st>>>(nodes, logN, level, levels, tx, sc, commit_idx, n_ood, finish,
                                                     node_stride);
         count_launches(1);
         level += levels;
@@ -208,12 +269,20 @@ static int merkle_levels(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, in
     return 0;
 }
 
-int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, cudaStream_t st) {
-    return merkle_levels(nodes, logN, tx, sc, commit_idx, n_ood, 1, 0, st);
+static int merkle_levels(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, u32 count,
+                         u64 node_stride, int hash, cudaStream_t st) {
+    if (hash == HASH_SHA256)
+        return merkle_levels_h<HASH_SHA256>(nodes, logN, tx, sc, commit_idx, n_ood, count, node_stride, st);
+    return merkle_levels_h<HASH_BLAKE3>(nodes, logN, tx, sc, commit_idx, n_ood, count, node_stride, st);
+}
+
+int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int hash,
+                  cudaStream_t st) {
+    return merkle_levels(nodes, logN, tx, sc, commit_idx, n_ood, 1, 0, hash, st);
 }
 
 int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaStream_t st) {
-    return merkle_levels(nodes, logN, nullptr, nullptr, 0, 0, count, node_stride, st);
+    return merkle_levels(nodes, logN, nullptr, nullptr, 0, 0, count, node_stride, HASH_BLAKE3, st);
 }
 
 // ---------------------------------------------------------------------------

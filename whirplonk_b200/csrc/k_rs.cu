@@ -153,7 +153,7 @@ whirgpu_status whirgpu_rs_commit_batch(whirgpu_ctx* c, const uint64_t* vectors, 
     const LdeArgs L = lde_args(c, src, 1ull << (log_len - log_depth), (u32)planes, logN, tmp, out);
     if (launch_lde(L, c->stream) != 0) return fail(c, WHIRGPU_E_INVALID, "LDE launch");
     const u32 depth = 1u << log_depth;
-    if (launch_leaves_batch(out, N, depth, 1, nodes, (u32)count, (u64)depth * N, node_words, c->stream) != 0)
+    if (launch_leaves_batch(out, N, depth, 1, nodes, (u32)count, (u64)depth * N, node_words, 0, c->stream) != 0)
         return fail(c, WHIRGPU_E_INVALID, "leaf launch");
     if (launch_merkle_batch(nodes, logN, (u32)count, node_words, c->stream) != 0)
         return fail(c, WHIRGPU_E_INVALID, "merkle launch");

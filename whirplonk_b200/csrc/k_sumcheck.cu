@@ -329,7 +329,7 @@ static ScKernelArgs make_sc(const SumcheckArgs& s) {
 
 size_t sumcheck_scratch_bytes() { return (size_t)SC_GRID * 2 * sizeof(E3) + 256; }
 
-int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st);  // k_tx.cu
+int launch_pow_grind_only(ProofScalars* sc, u64 threshold, int hash, cudaStream_t st);  // k_tx.cu
 
 int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
     if (s.size < 2) return -1;
@@ -347,7 +347,7 @@ int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
     }
     count_launches(1);
     if (s.pow_threshold != ~0ull) {
-        launch_pow_grind_only(s.sc, s.pow_threshold, st);
+        launch_pow_grind_only(s.sc, s.pow_threshold, s.hash, st);
         k_sc_after_pow<<<1, 32, 0, st>>>(s.tx, s.sc, s.r_slot);
         count_launches(1);
     }

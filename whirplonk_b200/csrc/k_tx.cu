@@ -5,6 +5,7 @@
 // cpp/include/whir/protocols/whir/whir_prover.hpp:56-407.
 #include "launch.h"
 #include "blake3.cuh"
+#include "sha256.cuh"
 #include "state.cuh"
 #include "wtx.cuh"
 
@@ -93,6 +94,8 @@ __global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
     }
 }
 
+// H: 0 = BLAKE3, 1 = SHA-256 (the PoW engine follows the hash_id, whir.hpp:134-140).
+template <int H>
 __global__ void __launch_bounds__(POW_THREADS) k_pow_search(ProofScalars* sc, u64 threshold, u64 limit) {
     __shared__ unsigned ch[8];
     __shared__ u64 claim[2];
@@ -125,8 +128,9 @@ __global__ void __launch_bounds__(POW_THREADS) k_pow_search(ProofScalars* sc, u6
             m[8] = (unsigned)n;
             m[9] = (unsigned)(n >> 32);
             unsigned h[8];
-            b3_hash64(m, h);
-            const u64 v = (u64)h[0] | ((u64)h[1] << 32);
+            if (H == 1) sha256_hash64(m, h);
+            else b3_hash64(m, h);
+            const u64 v = (u64)h[0] | ((u64)h[1] << 32);  // first 8 digest bytes, LE
             if (v <= threshold) atomicMin(reinterpret_cast<unsigned long long*>(&sc->pow_best), (unsigned long long)n);
         }
         __syncthreads();
@@ -134,10 +138,11 @@ __global__ void __launch_bounds__(POW_THREADS) k_pow_search(ProofScalars* sc, u6
 }
 
 // The search for one PoW (challenge already squeezed, pow_best / pow_next reset).
-int launch_pow_grind_only(ProofScalars* sc, u64 threshold, cudaStream_t st) {
+int launch_pow_grind_only(ProofScalars* sc, u64 threshold, int hash, cudaStream_t st) {
     const double expect = threshold == 0 ? 1.8446744073709552e19 : 18446744073709551616.0 / (double)threshold;
     const u64 limit = expect * 64.0 >= (double)POW_NONCE_LIMIT ? POW_NONCE_LIMIT : (u64)(expect * 64.0) + 1;
-    k_pow_search<<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, limit);
+    if (hash == 1) k_pow_search<1><<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, limit);
+    else k_pow_search<0><<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, limit);
     count_launches(1);
     return 0;
 }
@@ -153,11 +158,11 @@ __global__ void k_pow_finish(TxState* tx, ProofScalars* sc, int slot) {
     wtx_store(t, tx);
 }
 
-int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, cudaStream_t st) {
+int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, int hash, cudaStream_t st) {
     if (threshold == ~0ull) return 0;  // zero difficulty: nothing sent (proof_of_work.hpp:241)
     k_pow_challenge<<<1, 32, 0, st>>>(tx, sc);
     count_launches(1);
-    launch_pow_grind_only(sc, threshold, st);
+    launch_pow_grind_only(sc, threshold, hash, st);
     k_pow_finish<<<1, 32, 0, st>>>(tx, sc, slot);
     count_launches(1);
     return 0;

@@ -66,17 +66,19 @@ int lde_prepare();
 // ---- Merkle commitment ------------------------------------------------------
 // Leaf i = BLAKE3 of row i (LE bytes of `depth` elements of `ncomp` words),
 // written to nodes[i].  Rows are gathered from the codeword planes.
-int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, cudaStream_t st);
+// hash: 0 = BLAKE3, 1 = SHA-256 (the engine a configuration's hash_id selects).
+int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, int hash, cudaStream_t st);
 // `count` independent matrices: planes and node arrays `plane_stride` /
 // `node_stride` words apart.
 int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
-                        u64 node_stride, cudaStream_t st);
+                        u64 node_stride, int hash, cudaStream_t st);
 // Builds all Merkle levels above the leaves of a 2^logN-leaf tree in `nodes`
 // ([leaves | level 1 | ... | root], 8 words per node).  The CTA that computes
 // the root also performs the transcript step of irs_commit::commit
 // (irs_commit.hpp:433-478): prover_message(root), then squeezes `n_ood`
 // Ext3 out-of-domain points into sc->ood_pts[commit_idx].
-int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, cudaStream_t st);
+int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int hash,
+                  cudaStream_t st);
 // Tree levels only (no transcript) of `count` trees `node_stride` words apart.
 int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaStream_t st);
 
@@ -94,7 +96,7 @@ int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned ch
 // Constraint RLC + initial sum (whir_prover.hpp:150-197).
 int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood, cudaStream_t st);
 // PoW: squeeze the 32-byte challenge, grind the minimum nonce, send it.
-int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, cudaStream_t st);
+int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, int hash, cudaStream_t st);
 // Sends every coefficient of the final folded vector (whir_prover.hpp:360-362).
 int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size, cudaStream_t st);
 
@@ -152,6 +154,7 @@ struct SumcheckArgs {
     int fold_r;
     int r_slot;         // this round's challenge goes to sc->sc_r[r_slot]
     u64 pow_threshold;
+    int hash;           // PoW engine (0 BLAKE3, 1 SHA-256)
     TxState* tx;
     ProofScalars* sc;
     void* scratch;

@@ -21,6 +21,7 @@ struct ProtocolParams {  // whir::ProtocolParameters (cpp/include/whir/parameter
     uint64_t security_level = 100;
     uint64_t pow_bits = 20;
     uint64_t batch_size = 1;
+    int hash = 0;  // engine of hash_id: 0 BLAKE3, 1 SHA-256 (leaves, Merkle, PoW)
 };
 
 struct IrsSchedule {

@@ -42,12 +42,12 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
     p.n_forms = n_forms;
     if (n_forms < 0 || n_forms > MAX_FORMS) throw std::invalid_argument("too many statement forms");
     const WhirSchedule& s = p.sch;
-    auto check_irs = [](const IrsSchedule& c, uint32_t ncomp) {
+    auto check_irs = [&params](const IrsSchedule& c, uint32_t ncomp) {
         const uint64_t N = c.codeword_length;
         if (N == 0 || (N & (N - 1))) throw std::invalid_argument("codeword length must be a power of two");
         if (ilog2(N) > TW_LOG) throw std::invalid_argument("codeword length above 2^26");
         if (c.depth > (uint64_t)MAX_DEPTH) throw std::invalid_argument("folding factor too large");
-        if (c.depth * ncomp * 8 > 1024) throw std::invalid_argument("rows above one BLAKE3 chunk");
+        if (params.hash == 0 && c.depth * ncomp * 8 > 1024) throw std::invalid_argument("rows above one BLAKE3 chunk");
         if (c.in_domain > (uint64_t)MAX_QUERIES) throw std::invalid_argument("too many in-domain samples");
         if (c.out_domain > (uint64_t)MAX_OOD) throw std::invalid_argument("too many out-of-domain samples");
         if (N % c.message_length() != 0) throw std::invalid_argument("codeword length not a multiple of message length");
@@ -177,8 +177,8 @@ int commit_vector(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t n
     L.tw_lo = c.tw.tw_lo;
     WG_TIMED(c, FAM_NTT, launch_lde(L, c.st));
     uint32_t* nodes = reinterpret_cast<uint32_t*>(c.ws + cb.nodes);
-    WG_TIMED(c, FAM_LEAF, launch_leaves(c.w(cb.planes), cb.N, cb.depth, ncomp, nodes, c.st));
-    WG_TIMED(c, FAM_MERKLE, launch_merkle(nodes, cb.logN, c.tx(), c.sc(), ci, n_ood, c.st));
+    WG_TIMED(c, FAM_LEAF, launch_leaves(c.w(cb.planes), cb.N, cb.depth, ncomp, nodes, c.p.params.hash, c.st));
+    WG_TIMED(c, FAM_MERKLE, launch_merkle(nodes, cb.logN, c.tx(), c.sc(), ci, n_ood, c.p.params.hash, c.st));
     WG_TIMED(c, FAM_OOD, launch_ood(src[0], src[1], src[2], ncomp == 3, vsize, c.tx(), c.sc(), ci, n_ood,
                                     c.ws + c.p.off_ood_scratch, c.st));
     return 0;
@@ -195,6 +195,7 @@ int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_f
         a.size = size;
         a.r_slot = r_slot;
         a.pow_threshold = s.pow_threshold;
+        a.hash = c.p.params.hash;
         a.tx = c.tx();
         a.sc = c.sc();
         int rc = 1;
@@ -214,6 +215,7 @@ int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_f
         a.fold_r = r_slot - 1;
         a.r_slot = r_slot;
         a.pow_threshold = s.pow_threshold;
+        a.hash = c.p.params.hash;
         a.tx = c.tx();
         a.sc = c.sc();
         a.scratch = c.ws + c.p.off_sc_scratch;
@@ -275,7 +277,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         const int ci = (int)r + 1;
         const uint64_t* src[3] = {c.a(0), c.a(1), c.a(2)};
         WG_TRY(commit_vector(c, ci, src, 3, vsize, (int)rc.irs.out_domain));
-        WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), rc.pow_threshold, ci, st));
+        WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), rc.pow_threshold, ci, c.p.params.hash, st));
         // open the previous commitment
         const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;
         const CommitBuffers& pb = p.commits[ci - 1];
@@ -311,7 +313,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
 
     // final vector, PoW, opening, sumcheck
     WG_TIMED(c, FAM_TX, launch_send_vector(c.tx(), c.a(0), c.a(1), c.a(2), vsize, st));
-    WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), s.final_pow, (int)s.rounds.size() + 1, st));
+    WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), s.final_pow, (int)s.rounds.size() + 1, c.p.params.hash, st));
     {
         const IrsSchedule& last = s.rounds.empty() ? s.initial : s.rounds.back().irs;
         const CommitBuffers& lb = p.commits.back();
