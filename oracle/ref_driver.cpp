@@ -14,15 +14,20 @@
 // with the domain separator of `make_rust_cli_domain_separator`
 // (cpp/main.cpp:203-215), re-stated here because main.cpp is not a header.
 //
-// Input file (little endian), written by whirplonk_b200/io.py:
-//   u32 magic 0x49524857 ('WHRI'), u32 version 1
+// Input file (little endian), written by oracle/refio.py:
+//   u32 magic 0x49524857 ('WHRI'), u32 version 1 or 2
 //   u64 num_variables, folding_factor, starting_log_inv_rate,
 //       security_level, pow_bits, num_points
+//   version 2 only: u64 batch_size, num_witnesses (version 1: both 1)
 //   num_points * num_variables * 3 u64   MLE points (Ext3 coords)
-//   2^num_variables u64                  coefficients (canonical, < p)
+//   V * 2^num_variables u64              coefficients of the V = batch_size *
+//                                        num_witnesses vectors (canonical, < p)
+// The V vectors are committed as num_witnesses witnesses of batch_size
+// vectors each, in order, then proven together.
 // Output file:
 //   u64 narg_len, narg bytes, u64 hints_len, hint bytes,
-//   num_points * 3 u64 evaluations, f64 commit_ms, f64 prove_ms, f64 verify_ok
+//   num_points * V * 3 u64 evaluations (form-major),
+//   f64 commit_ms, f64 prove_ms, f64 verify_ok
 #include "whir/algebra/embedding.hpp"
 #include "whir/algebra/goldilocks.hpp"
 #include "whir/algebra/goldilocks_ext3.hpp"
@@ -142,14 +147,19 @@ int main(int argc, char** argv) {
     auto buf = read_file(argv[1]);
     Reader rd{buf};
     if (rd.u32() != 0x49524857u) die("bad magic");
-    if (rd.u32() != 1u) die("bad version");
+    const std::uint32_t version = rd.u32();
+    if (version != 1u && version != 2u) die("bad version");
     const std::size_t n = rd.u64();
     const std::size_t k = rd.u64();
     const std::size_t rho = rd.u64();
     const std::size_t sec = rd.u64();
     const std::size_t powb = rd.u64();
     const std::size_t npts = rd.u64();
+    const std::size_t batch = version == 2u ? rd.u64() : 1;
+    const std::size_t nwit = version == 2u ? rd.u64() : 1;
     if (n >= 40) die("num_variables too large");
+    if (batch == 0 || nwit == 0 || batch * nwit > 64) die("bad vector count");
+    const std::size_t nvec = batch * nwit;
 
     std::vector<std::vector<Target>> points(npts, std::vector<Target>(n));
     for (auto& pt : points)
@@ -158,8 +168,9 @@ int main(int argc, char** argv) {
             c = Target(Source::from_u64(a), Source::from_u64(b), Source::from_u64(d));
         }
     const std::size_t size = std::size_t{1} << n;
-    std::vector<Source> vec(size);
-    for (auto& v : vec) v = Source::from_u64(rd.u64());
+    std::vector<std::vector<Source>> vecs(nvec, std::vector<Source>(size));
+    for (auto& vec : vecs)
+        for (auto& v : vec) v = Source::from_u64(rd.u64());
 
     ::whir::ProtocolParameters params;
     params.security_level = sec;
@@ -168,7 +179,7 @@ int main(int argc, char** argv) {
     params.folding_factor = k;
     params.unique_decoding = false;
     params.starting_log_inv_rate = rho;
-    params.batch_size = 1;
+    params.batch_size = batch;
     params.hash_id = use_sha2 ? ::whir::hash::ENGINE_ID_SHA2 : ::whir::hash::ENGINE_ID_BLAKE3;
 
     auto config = ::whir::protocols::whir::Config<M>::from_params(size, params);
@@ -194,14 +205,15 @@ int main(int argc, char** argv) {
     }
 
     M emb{};
-    std::vector<Target> evaluations;
+    std::vector<Target> evaluations;  // form-major, as Config::prove expects (whir_prover.hpp:77)
     for (const auto& pt : points) {
         ::whir::algebra::MultilinearExtension<Target> lf(pt);
-        evaluations.push_back(lf.template evaluate<M>(emb, std::span<const Source>{vec}));
+        for (const auto& vec : vecs) evaluations.push_back(lf.template evaluate<M>(emb, std::span<const Source>{vec}));
     }
     auto ds = cli_domain_separator(params);
     ::whir::transcript::Empty instance;
-    std::vector<std::span<const Source>> spans{std::span<const Source>{vec}};
+    std::vector<std::span<const Source>> spans;
+    for (const auto& vec : vecs) spans.push_back(std::span<const Source>{vec});
 
     ::whir::transcript::ProverState::Proof proof;
     double commit_ms = 0, prove_ms = 0;
@@ -211,10 +223,12 @@ int main(int argc, char** argv) {
             forms.push_back(std::make_unique<::whir::algebra::MultilinearExtension<Target>>(pt));
         auto ps = ::whir::transcript::ProverState::from_ds(ds, instance);
         auto t0 = Clock::now();
-        auto witness = config.commit(ps, spans);
-        auto t1 = Clock::now();
         std::vector<::whir::protocols::irs_commit::Witness<Source, Target>> wits;
-        wits.push_back(std::move(witness));
+        for (std::size_t w = 0; w < nwit; ++w) {
+            std::span<const std::span<const Source>> mine{spans.data() + w * batch, batch};
+            wits.push_back(config.commit(ps, mine));
+        }
+        auto t1 = Clock::now();
         config.prove(ps, spans,
             std::span<const ::whir::protocols::irs_commit::Witness<Source, Target>>{wits},
             std::move(forms), std::span<const Target>{evaluations});
@@ -228,8 +242,10 @@ int main(int argc, char** argv) {
     double verify_ok = -1.0;
     if (do_verify) {
         auto vs = ::whir::transcript::VerifierState::from_ds(ds, instance, proof);
-        auto comm = config.receive_commitment(vs);
-        std::vector<const ::whir::protocols::irs_commit::Commitment<Target>*> cp{&comm};
+        std::vector<::whir::protocols::irs_commit::Commitment<Target>> comms;
+        for (std::size_t w = 0; w < nwit; ++w) comms.push_back(config.receive_commitment(vs));
+        std::vector<const ::whir::protocols::irs_commit::Commitment<Target>*> cp;
+        for (const auto& cm : comms) cp.push_back(&cm);
         auto claim = config.verify(vs, cp, std::span<const Target>{evaluations});
         std::vector<std::unique_ptr<::whir::algebra::LinearForm<Target>>> vforms;
         std::vector<const ::whir::algebra::LinearForm<Target>*> refs;

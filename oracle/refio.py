@@ -30,19 +30,24 @@ class RefProof:
     verify_ok: float  # 1.0 accepted, 0.0 rejected, -1.0 not run
 
 
-def write_input(path, n, k, rho, sec, pow_bits, points, coeffs):
-    """Input file of ref_driver.cpp (format documented there)."""
+def write_input(path, n, k, rho, sec, pow_bits, points, coeffs, batch_size=1, num_witnesses=1):
+    """Input file of ref_driver.cpp (format documented there).  ``coeffs`` holds
+    batch_size * num_witnesses vectors of 2^n words back to back."""
     points = np.ascontiguousarray(points, dtype=np.uint64).reshape(-1, n, 3)
     coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
-    assert coeffs.size == 1 << n
+    nvec = batch_size * num_witnesses
+    assert coeffs.size == nvec << n
+    multi = nvec != 1
     with open(path, "wb") as f:
-        f.write(struct.pack("<II", 0x49524857, 1))
+        f.write(struct.pack("<II", 0x49524857, 2 if multi else 1))
         f.write(struct.pack("<6Q", n, k, rho, sec, pow_bits, points.shape[0]))
+        if multi:
+            f.write(struct.pack("<2Q", batch_size, num_witnesses))
         f.write(points.tobytes())
         f.write(coeffs.tobytes())
 
 
-def read_output(path, num_points) -> RefProof:
+def read_output(path, num_points, num_vectors=1) -> RefProof:
     with open(path, "rb") as f:
         b = f.read()
     pos = 0
@@ -50,8 +55,9 @@ def read_output(path, num_points) -> RefProof:
     narg = b[pos:pos + ln]; pos += ln
     (lh,) = struct.unpack_from("<Q", b, pos); pos += 8
     hints = b[pos:pos + lh]; pos += lh
-    ev = np.frombuffer(b, dtype=np.uint64, count=3 * num_points, offset=pos).reshape(num_points, 3).copy()
-    pos += 24 * num_points
+    cnt = num_points * num_vectors
+    ev = np.frombuffer(b, dtype=np.uint64, count=3 * cnt, offset=pos).reshape(cnt, 3).copy()
+    pos += 24 * cnt
     cms, pms, vok = struct.unpack_from("<3d", b, pos)
     return RefProof(narg, hints, ev, cms, pms, vok)
 
@@ -61,8 +67,9 @@ def ref_available() -> bool:
 
 
 def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1, threads=None,
-                  timeout=3600, sha2=False) -> RefProof:
-    """Runs the unmodified reference prover (compiled in place by oracle/Makefile)."""
+                  timeout=3600, sha2=False, batch_size=1, num_witnesses=1) -> RefProof:
+    """Runs the unmodified reference prover (compiled in place by oracle/Makefile).
+    With several vectors the evaluations come back form-major, (num_points * V, 3)."""
     if not ref_available():
         raise FileNotFoundError(f"{REF_DRIVER} not built (make -C oracle ref)")
     env = dict(os.environ)
@@ -71,12 +78,12 @@ def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1
     npts = np.asarray(points).reshape(-1, n, 3).shape[0]
     with tempfile.TemporaryDirectory() as td:
         inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
-        write_input(inp, n, k, rho, sec, pow_bits, points, coeffs)
+        write_input(inp, n, k, rho, sec, pow_bits, points, coeffs, batch_size, num_witnesses)
         cmd = [REF_DRIVER, inp, out] + (["--verify"] if verify else []) + (["--reps", str(reps)] if reps > 1 else [])
         if sha2:
             cmd.append("--sha2")
         subprocess.run(cmd, check=True, env=env, timeout=timeout, stdout=subprocess.DEVNULL)
-        return read_output(out, npts)
+        return read_output(out, npts, batch_size * num_witnesses)
 
 
 class OracleTranscript:
@@ -164,6 +171,9 @@ class Oracle:
         L.oracle_find_nonce_sha2.argtypes = [p, u64]
         L.oracle_find_nonce_sha2.restype = u64
         L.oracle_whir_prove.restype = ctypes.c_int
+        L.oracle_whir_prove_multi.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, u64, u64, p, p, sz, p, p, sz,
+                                              p, sz, p, ctypes.c_int]
+        L.oracle_whir_prove_multi.restype = ctypes.c_int
 
     # -- primitives -------------------------------------------------------
     def blake3(self, data: bytes) -> bytes:
@@ -260,6 +270,24 @@ class Oracle:
         rc = self.lib.oracle_whir_prove(n, rho, k, sec, pow_bits, 0, coeffs.ctypes.data, points.ctypes.data,
                                         points.shape[0], evals.ctypes.data, narg, cap, hints, cap, lens,
                                         int(sha2))
+        if rc != 0:
+            raise RuntimeError("oracle prove failed")
+        return narg.raw[:lens[0]], hints.raw[:lens[1]]
+
+    def prove_multi(self, n, k, rho, sec, pow_bits, points, coeffs, evaluations, batch_size, num_witnesses,
+                    sha2=False):
+        """Commit num_witnesses witnesses of batch_size vectors, prove them together.
+        coeffs: (V, 2^n); evaluations: (num_points * V, 3), form-major."""
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+        points = np.ascontiguousarray(points, dtype=np.uint64).reshape(-1, n, 3)
+        evals = np.ascontiguousarray(evaluations, dtype=np.uint64).reshape(-1, 3)
+        cap = 64 << 20
+        narg = ctypes.create_string_buffer(cap)
+        hints = ctypes.create_string_buffer(cap)
+        lens = (ctypes.c_uint64 * 2)()
+        rc = self.lib.oracle_whir_prove_multi(n, rho, k, sec, pow_bits, 0, batch_size, num_witnesses,
+                                              coeffs.ctypes.data, points.ctypes.data, points.shape[0],
+                                              evals.ctypes.data, narg, cap, hints, cap, lens, int(sha2))
         if rc != 0:
             raise RuntimeError("oracle prove failed")
         return narg.raw[:lens[0]], hints.raw[:lens[1]]

@@ -2,8 +2,8 @@
 //
 // A plain, single-file CPU restatement of the reference WHIR prover path
 // (hxd77/WhirPlonk, C++ port under cpp/include/whir) for
-//   M = Basefield<GoldilocksExt3>, hash = BLAKE3, MLE / dense covector
-//   statements, num_vectors = 1.
+//   M = Basefield<GoldilocksExt3>, hash = BLAKE3 or SHA-256, MLE / dense
+//   covector statements, one or more witnesses of batch_size vectors each.
 // It is written for clarity: simple loops, no SIMD, OpenMP only on loops whose
 // result does not depend on the order (all arithmetic is exact field math).
 // Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use it,
@@ -210,12 +210,13 @@ inline void sha3_512(const u8* d, size_t n, u8 out[64]) { Sponge sp(72); sp.abso
 inline void shake128(const u8* d, size_t n, u8* out, size_t m) { Sponge sp(168); sp.absorb(d, n); sp.finalize(0x1F); sp.squeeze(out, m); }
 
 // ---------------------------------------------------------------------------
-// BLAKE3 (public specification), single-chunk messages (<= 1024 bytes), which
-// is every message the WHIR path hashes: leaves of 128 B (base rows) or 384 B
+// BLAKE3 (public specification).  Messages of one chunk (<= 1024 bytes) are
+// most of what the WHIR path hashes: leaves of 128 B (base rows) or 384 B
 // (Ext3 rows), Merkle parents and PoW inputs of 64 B.  For sizes that are a
 // multiple of 64 this is exactly the reference's blake3_hash_many call with
 // flags_start = CHUNK_START, flags_end = CHUNK_END|ROOT
-// (cpp/include/whir/hash/blake3_engine.hpp:90-199).
+// (cpp/include/whir/hash/blake3_engine.hpp:90-199).  Rows of several
+// committed vectors can be wider than a chunk; those take the tree below.
 // ---------------------------------------------------------------------------
 constexpr u32 B3_IV[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53Au,
                           0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
@@ -245,9 +246,9 @@ inline void b3_compress(u32 cv[8], const u32 blk[16], u64 counter, u32 len, u32 
     for (int i = 0; i < 8; ++i) cv[i] = v[i] ^ v[i + 8];
 }
 using Hash = std::array<u8, 32>;
-inline Hash blake3(const u8* d, size_t n) {
-    if (n > 1024) throw std::runtime_error("oracle blake3: multi-chunk messages not supported");
-    u32 cv[8];
+constexpr u32 B3_PARENT = 4;
+// Chaining value of one chunk (<= 1024 bytes) with chunk counter `counter`.
+inline void b3_chunk(const u8* d, size_t n, u64 counter, u32 extra_end_flags, u32 cv[8]) {
     for (int i = 0; i < 8; ++i) cv[i] = B3_IV[i];
     size_t nblocks = n == 0 ? 1 : (n + 63) / 64;
     for (size_t b = 0; b < nblocks; ++b) {
@@ -256,8 +257,47 @@ inline Hash blake3(const u8* d, size_t n) {
         if (take) std::memcpy(buf, d + b * 64, take);
         u32 blk[16];
         for (int i = 0; i < 16; ++i) blk[i] = (u32)buf[4 * i] | (u32)buf[4 * i + 1] << 8 | (u32)buf[4 * i + 2] << 16 | (u32)buf[4 * i + 3] << 24;
-        u32 flags = (b == 0 ? B3_CHUNK_START : 0) | (b + 1 == nblocks ? (B3_CHUNK_END | B3_ROOT) : 0);
-        b3_compress(cv, blk, 0, (u32)take, flags);
+        u32 flags = (b == 0 ? B3_CHUNK_START : 0) | (b + 1 == nblocks ? (B3_CHUNK_END | extra_end_flags) : 0);
+        b3_compress(cv, blk, counter, (u32)take, flags);
+    }
+}
+inline void b3_parent(const u32 l[8], const u32 r[8], u32 flags, u32 out[8]) {
+    u32 blk[16];
+    for (int i = 0; i < 8; ++i) { blk[i] = l[i]; blk[8 + i] = r[i]; }
+    for (int i = 0; i < 8; ++i) out[i] = B3_IV[i];
+    b3_compress(out, blk, 0, 64, B3_PARENT | flags);
+}
+// Multi-chunk messages (rows wider than 1024 bytes, the reference's
+// blake3_hasher fallback in blake3_engine.hpp:186-196) follow the
+// specification's tree: chunk i is hashed with counter i, completed subtrees
+// are merged as soon as the chunk count has a trailing zero bit, and the last
+// chunk's chaining value is merged with the remaining stack from the top, the
+// final merge carrying the ROOT flag.
+inline Hash blake3(const u8* d, size_t n) {
+    const size_t nch = n <= 1024 ? 1 : (n + 1023) / 1024;
+    u32 cv[8];
+    if (nch == 1) {
+        b3_chunk(d, n, 0, B3_ROOT, cv);
+    } else {
+        std::vector<std::array<u32, 8>> stack;
+        for (size_t c = 0; c + 1 < nch; ++c) {
+            std::array<u32, 8> cur;
+            b3_chunk(d + c * 1024, 1024, c, 0, cur.data());
+            for (u64 total = c + 1; (total & 1) == 0; total >>= 1) {
+                std::array<u32, 8> m;
+                b3_parent(stack.back().data(), cur.data(), 0, m.data());
+                stack.pop_back();
+                cur = m;
+            }
+            stack.push_back(cur);
+        }
+        b3_chunk(d + (nch - 1) * 1024, n - (nch - 1) * 1024, nch - 1, 0, cv);
+        while (!stack.empty()) {
+            u32 m[8];
+            b3_parent(stack.back().data(), cv, stack.size() == 1 ? B3_ROOT : 0, m);
+            stack.pop_back();
+            std::memcpy(cv, m, 32);
+        }
     }
     Hash h;
     for (int i = 0; i < 8; ++i) for (int j = 0; j < 4; ++j) h[4 * i + j] = (u8)(cv[i] >> (8 * j));
@@ -801,27 +841,45 @@ inline std::vector<E3> sumcheck_prove(Transcript& t, const SumcheckCfg& cfg, std
 // ---------------------------------------------------------------------------
 struct Witness {
     bool base = true;
-    std::vector<u64> mat_base;   // row-major N x depth (initial commitment)
+    std::vector<u64> mat_base;   // row-major N x (nvec * depth) (initial commitment)
     std::vector<E3> mat_e3;      // row-major N x depth (round commitments)
     std::vector<Hash> nodes;     // Merkle node array
-    u64 layers = 0, depth = 0, N = 0;
-    std::vector<E3> ood_points, ood_values;
+    u64 layers = 0, depth = 0, N = 0, nvec = 1;
+    std::vector<E3> ood_points;
+    std::vector<E3> ood_values;  // point-major: ood_values[j * nvec + v]
     Hash root() const { return nodes.back(); }
+    u64 cols() const { return nvec * depth; }
 };
 
-inline Witness commit_base(Transcript& t, const IrsCfg& c, const std::vector<u64>& v, Engine eng = Engine::Blake3) {
+// irs_commit::Config::commit (irs_commit.hpp:344-561) of `vs.size()` base
+// vectors: row i of the matrix is (codeword_0[i] .. codeword_{d-1}[i]) of
+// vector 0, then of vector 1, ... (mod_ntt.hpp:49-130: plane v * depth + b);
+// the OOD values are sent point-major, every vector at each point (:472-554).
+inline Witness commit_base_multi(Transcript& t, const IrsCfg& c, const std::vector<const std::vector<u64>*>& vs,
+                                 Engine eng = Engine::Blake3) {
     Witness w;
     w.base = true; w.N = c.codeword_length; w.depth = c.depth; w.layers = layers_for(w.N);
-    w.mat_base = rs_encode_base(v, w.N, w.depth);
-    w.nodes = merkle_build(leaves_base(w.mat_base, w.depth, eng), eng);
+    w.nvec = vs.size();
+    const u64 cols = w.cols();
+    w.mat_base.assign(w.N * cols, 0);
+    for (u64 v = 0; v < w.nvec; ++v) {
+        auto m = rs_encode_base(*vs[v], w.N, w.depth);
+        for (u64 i = 0; i < w.N; ++i)
+            for (u64 b = 0; b < w.depth; ++b) w.mat_base[i * cols + v * w.depth + b] = m[i * w.depth + b];
+    }
+    w.nodes = merkle_build(leaves_base(w.mat_base, cols, eng), eng);
     t.message_hash(w.root());
     for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_e3());
-    for (const E3& z : w.ood_points) {
-        E3 val = univariate_eval_base(v, z);
-        t.message_e3(val);
-        w.ood_values.push_back(val);
-    }
+    for (const E3& z : w.ood_points)
+        for (u64 v = 0; v < w.nvec; ++v) {
+            E3 val = univariate_eval_base(*vs[v], z);
+            t.message_e3(val);
+            w.ood_values.push_back(val);
+        }
     return w;
+}
+inline Witness commit_base(Transcript& t, const IrsCfg& c, const std::vector<u64>& v, Engine eng = Engine::Blake3) {
+    return commit_base_multi(t, c, {&v}, eng);
 }
 inline Witness commit_e3(Transcript& t, const IrsCfg& c, const std::vector<E3>& v, Engine eng = Engine::Blake3) {
     Witness w;
@@ -865,59 +923,103 @@ inline std::vector<u64> challenge_indices(Transcript& t, u64 N, u64 count) {
     t.squeeze(ent.data(), ent.size());
     return indices_from_entropy(ent.data(), N, count, false);
 }
-struct Opening { std::vector<E3> points; std::vector<E3> rows; };  // rows lifted to Ext3
-inline Opening open_witness(Transcript& t, const IrsCfg& c, const Witness& w) {
+// irs_commit::Config::open (irs_commit.hpp:637-713) of one or more witnesses
+// at the same challenged rows: per witness the row hint then its Merkle hints;
+// the returned rows are the witnesses' rows side by side (stride sum of cols).
+struct Opening { std::vector<E3> points; std::vector<E3> rows; u64 stride = 0; };  // rows lifted to Ext3
+inline Opening open_witnesses(Transcript& t, const IrsCfg& c, const std::vector<const Witness*>& ws) {
     auto idx = challenge_indices(t, c.codeword_length, c.in_domain);
     Opening o;
     u64 gen = root_of_unity(c.codeword_length);
     for (u64 i : idx) o.points.push_back(E3::from_base(fpow(gen, i)));
-    t.hint_u64(idx.size() * w.depth);
-    for (u64 i : idx)
-        for (u64 col = 0; col < w.depth; ++col) {
-            if (w.base) {
-                u64 x = w.mat_base[i * w.depth + col];
-                t.hint_bytes(reinterpret_cast<const u8*>(&x), 8);
-                o.rows.push_back(E3::from_base(x));
-            } else {
-                const E3& x = w.mat_e3[i * w.depth + col];
-                t.hint_bytes(reinterpret_cast<const u8*>(x.c), 24);
-                o.rows.push_back(x);
+    for (const Witness* w : ws) o.stride += w->cols();
+    o.rows.assign(idx.size() * o.stride, E3());
+    u64 col0 = 0;
+    for (const Witness* w : ws) {
+        const u64 cols = w->cols();
+        t.hint_u64(idx.size() * cols);
+        for (size_t q = 0; q < idx.size(); ++q)
+            for (u64 col = 0; col < cols; ++col) {
+                const u64 i = idx[q];
+                if (w->base) {
+                    u64 x = w->mat_base[i * cols + col];
+                    t.hint_bytes(reinterpret_cast<const u8*>(&x), 8);
+                    o.rows[q * o.stride + col0 + col] = E3::from_base(x);
+                } else {
+                    const E3& x = w->mat_e3[i * cols + col];
+                    t.hint_bytes(reinterpret_cast<const u8*>(x.c), 24);
+                    o.rows[q * o.stride + col0 + col] = x;
+                }
             }
-        }
-    for (const Hash& h : merkle_open(w.nodes, w.layers, idx)) t.hint_bytes(h.data(), 32);
+        for (const Hash& h : merkle_open(w->nodes, w->layers, idx)) t.hint_bytes(h.data(), 32);
+        col0 += cols;
+    }
     return o;
 }
+inline Opening open_witness(Transcript& t, const IrsCfg& c, const Witness& w) { return open_witnesses(t, c, {&w}); }
 
 // ---------------------------------------------------------------------------
-// Whole prover: Config::commit then Config::prove (whir.hpp:303-309,
-// whir_prover.hpp:56-407), one vector, MLE-point and/or dense-covector forms.
+// Whole prover: Config::commit (once per witness) then Config::prove
+// (whir.hpp:303-309, whir_prover.hpp:56-407) over num_witnesses * batch_size
+// base vectors, MLE-point and/or dense-covector forms.
 // ---------------------------------------------------------------------------
 struct Statement {
     std::vector<std::vector<E3>> mle_points;   // MultilinearExtension forms
     std::vector<std::vector<E3>> covectors;    // Covector forms (after the MLE forms)
-    std::vector<E3> evaluations;               // one per form, same order
+    std::vector<E3> evaluations;               // form-major: evaluations[f * num_vectors + v]
 };
 struct ProofOut { std::vector<u8> narg, hints; std::vector<E3> evaluation_point; Hash initial_root{}; };
 
-inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statement& st, const DomainSep& ds) {
-    WhirCfg cfg = whir_from_params(v.size(), p);
+inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>& vs, u64 num_witnesses,
+                            const Statement& st, const DomainSep& ds) {
+    const u64 B = p.batch_size, W = num_witnesses, V = vs.size();
+    if (B == 0 || W == 0 || V != W * B) throw std::runtime_error("vectors != witnesses * batch_size");
+    const u64 size = vs[0].size();
+    for (const auto& v : vs) if (v.size() != size) throw std::runtime_error("vector sizes differ");
+    WhirCfg cfg = whir_from_params(size, p);
     const Engine eng = std::memcmp(p.hash_id, SHA2_ENGINE_ID, 32) == 0 ? Engine::Sha2 : Engine::Blake3;
     Transcript t;
     t.absorb(ds.protocol_id, 64);
     t.absorb(ds.session_id, 32);
     ProofOut out;
-    // commit
-    Witness w0 = commit_base(t, cfg.initial, v, eng);
-    out.initial_root = w0.root();
+    // commit: one witness of B vectors at a time, on the same transcript
+    std::vector<Witness> wits;
+    for (u64 w = 0; w < W; ++w) {
+        std::vector<const std::vector<u64>*> mine;
+        for (u64 b = 0; b < B; ++b) mine.push_back(&vs[w * B + b]);
+        wits.push_back(commit_base_multi(t, cfg.initial, mine, eng));
+    }
+    out.initial_root = wits[0].root();
     const size_t nforms = st.mle_points.size() + st.covectors.size();
-    // step 2: vector RLC of one vector is [1], no squeeze; lift
-    std::vector<E3> vec(v.size());
-    for (size_t i = 0; i < v.size(); ++i) vec[i] = E3::from_base(v[i]);
-    // step 3: constraint RLC
-    auto crlc = geometric_challenge(t, nforms + w0.ood_points.size());
+    if (st.evaluations.size() != nforms * V) throw std::runtime_error("evaluations != forms * vectors");
+    // step 1: OOD completion (whir_prover.hpp:92-120): every vector at every
+    // witness's OOD points; values of other witnesses' vectors are sent.
+    std::vector<E3> oods_pts, oods_mat;  // oods_mat[i * V + j]
+    for (u64 w = 0; w < W; ++w)
+        for (size_t e = 0; e < wits[w].ood_points.size(); ++e) {
+            const E3& z = wits[w].ood_points[e];
+            for (u64 j = 0; j < V; ++j) {
+                if (j >= w * B && j < (w + 1) * B) {
+                    oods_mat.push_back(wits[w].ood_values[e * B + (j - w * B)]);
+                } else {
+                    E3 val = univariate_eval_base(vs[j], z);
+                    t.message_e3(val);
+                    oods_mat.push_back(val);
+                }
+            }
+            oods_pts.push_back(z);
+        }
+    // step 2: vector RLC (:131-140)
+    auto vrlc = geometric_challenge(t, V);
+    std::vector<E3> vec(size);
+    for (size_t i = 0; i < size; ++i) vec[i] = E3::from_base(vs[0][i]);
+    for (u64 j = 1; j < V; ++j)
+        for (size_t i = 0; i < size; ++i) vec[i] = vec[i] + smul(vrlc[j], vs[j][i]);
+    // step 3: constraint RLC (:150-170)
+    auto crlc = geometric_challenge(t, nforms + oods_pts.size());
     bool has_constraints = !crlc.empty();
     std::vector<E3> cov;
-    if (nforms > 0 || has_constraints) cov.assign(v.size(), E3());
+    if (nforms > 0 || has_constraints) cov.assign(size, E3());
     for (size_t f = 0; f < nforms; ++f) {
         E3 s = f == 0 ? E3::one() : crlc[f];
         if (f < st.mle_points.size()) eval_eq_acc(cov, st.mle_points[f], s);
@@ -926,12 +1028,20 @@ inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statemen
             for (size_t i = 0; i < cov.size(); ++i) cov[i] = cov[i] + s * cv[i];
         }
     }
-    // step 4: the sum
+    // step 4: the sum, a double RLC of the evaluation and OOD matrices (:172-197)
     E3 sum;
-    for (size_t f = 0; f < nforms; ++f) sum = sum + crlc[f] * st.evaluations[f];
+    for (size_t f = 0; f < nforms; ++f) {
+        E3 row;
+        for (u64 j = 0; j < V; ++j) row = row + vrlc[j] * st.evaluations[f * V + j];
+        sum = sum + crlc[f] * row;
+    }
     std::vector<E3> ood_rlc(crlc.begin() + (long)std::min(nforms, crlc.size()), crlc.end());
-    if (!ood_rlc.empty()) geometric_accumulate(cov, ood_rlc, w0.ood_points);
-    for (size_t j = 0; j < ood_rlc.size(); ++j) sum = sum + ood_rlc[j] * w0.ood_values[j];
+    if (!ood_rlc.empty()) geometric_accumulate(cov, ood_rlc, oods_pts);
+    for (size_t i = 0; i < ood_rlc.size(); ++i) {
+        E3 row;
+        for (u64 j = 0; j < V; ++j) row = row + vrlc[j] * oods_mat[i * V + j];
+        sum = sum + ood_rlc[i] * row;
+    }
     // step 5: initial sumcheck
     std::vector<E3> last_r;
     if (has_constraints) last_r = sumcheck_prove(t, cfg.initial_sumcheck, vec, cov, sum, eng);
@@ -942,9 +1052,12 @@ inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statemen
         cov.assign(cfg.initial_sumcheck.initial_size >> cfg.initial_sumcheck.num_rounds, E3());
     }
     out.evaluation_point = last_r;
-    // step 6: rounds
-    const Witness* prev = &w0;
+    // step 6: rounds.  The first opening covers every initial witness and
+    // weighs its rows by vector_rlc (x) eq(last folding randomness) (:283-310).
+    std::vector<const Witness*> prev;
+    for (const Witness& w : wits) prev.push_back(&w);
     const IrsCfg* prev_cfg = &cfg.initial;
+    std::vector<E3> wrlc = vrlc;
     std::vector<Witness> stored;
     stored.reserve(cfg.rounds.size());
     for (size_t rd = 0; rd < cfg.rounds.size(); ++rd) {
@@ -952,14 +1065,17 @@ inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statemen
         stored.push_back(commit_e3(t, rc.irs, vec, eng));
         const Witness& nw = stored.back();
         pow_prove(t, rc.pow_threshold, eng);
-        Opening o = open_witness(t, *prev_cfg, *prev);
+        Opening o = open_witnesses(t, *prev_cfg, prev);
         std::vector<E3> pts = nw.ood_points;
         pts.insert(pts.end(), o.points.begin(), o.points.end());
         std::vector<E3> vals = nw.ood_values;
         std::vector<E3> eqw = last_r.empty() ? std::vector<E3>{E3::one()} : eq_weights(last_r);
+        std::vector<E3> tp;  // tensor_product(vector_rlc, eq_weights) (utilities.hpp:137-150)
+        for (const E3& a : wrlc) for (const E3& b : eqw) tp.push_back(a * b);
+        if (tp.size() != o.stride) throw std::runtime_error("opened row width != tensor product");
         for (size_t q = 0; q < o.points.size(); ++q) {
             E3 acc;
-            for (size_t col = 0; col < prev->depth; ++col) acc = acc + o.rows[q * prev->depth + col] * eqw[col];
+            for (size_t col = 0; col < o.stride; ++col) acc = acc + o.rows[q * o.stride + col] * tp[col];
             vals.push_back(acc);
         }
         auto srlc = geometric_challenge(t, pts.size());
@@ -967,18 +1083,23 @@ inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statemen
         for (size_t j = 0; j < srlc.size(); ++j) sum = sum + srlc[j] * vals[j];
         last_r = sumcheck_prove(t, rc.sumcheck, vec, cov, sum, eng);
         out.evaluation_point.insert(out.evaluation_point.end(), last_r.begin(), last_r.end());
-        prev = &nw;
+        prev = {&nw};
         prev_cfg = &rc.irs;
+        wrlc = {E3::one()};
     }
     // steps 7-10
     for (const E3& c : vec) t.message_e3(c);
     pow_prove(t, cfg.final_pow, eng);
-    open_witness(t, *prev_cfg, *prev);
+    open_witnesses(t, *prev_cfg, prev);
     auto fr = sumcheck_prove(t, cfg.final_sumcheck, vec, cov, sum, eng);
     out.evaluation_point.insert(out.evaluation_point.end(), fr.begin(), fr.end());
     out.narg = std::move(t.narg);
     out.hints = std::move(t.hints);
     return out;
+}
+inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statement& st, const DomainSep& ds) {
+    if (p.batch_size != 1) throw std::runtime_error("prove(): one vector; use prove_multi");
+    return prove_multi(p, {v}, 1, st, ds);
 }
 
 }  // namespace oracle

@@ -15,7 +15,9 @@ has the reference checkout; the tests only read the JSON files).
    stored next to the outputs.
 2. reference_proofs.json -- whole proofs of the unmodified reference prover
    (oracle/_ref/ref_driver, built by oracle/Makefile) on seeded inputs:
-   lengths and SHA-256 digests of narg and hints (full bytes for the smallest).
+   lengths and SHA-256 digests of narg and hints (full bytes for the smallest);
+   "multi" holds proofs over several committed vectors (batch_size > 1,
+   several witnesses), including rows wider than one BLAKE3 chunk.
 """
 import hashlib
 import json
@@ -249,6 +251,46 @@ def proofs():
     return out
 
 
+MULTI_CASES = [  # (n, k, rho, security, pow_bits, seed, n_points, batch_size, num_witnesses, hash engine)
+    (5, 4, 1, 100, 20, 41, 1, 2, 2, "blake3"),    # small enough to store the bytes
+    (10, 4, 1, 100, 20, 42, 1, 2, 1, "blake3"),
+    (12, 4, 2, 100, 20, 43, 2, 4, 1, "blake3"),
+    (10, 4, 1, 100, 20, 44, 1, 1, 2, "blake3"),   # OOD completion across witnesses
+    (12, 4, 1, 100, 20, 45, 1, 2, 3, "blake3"),
+    (10, 4, 1, 100, 20, 46, 1, 16, 1, "blake3"),  # 2048-byte rows: two BLAKE3 chunks
+    (12, 6, 1, 100, 20, 47, 1, 3, 1, "blake3"),   # 1536-byte rows
+    (11, 4, 2, 100, 20, 48, 1, 3, 2, "sha2"),
+    (14, 4, 1, 100, 20, 49, 0, 2, 2, "blake3"),   # OOD constraints only
+    (16, 4, 1, 100, 20, 50, 1, 4, 1, "blake3"),
+    (9, 3, 1, 100, 20, 51, 1, 9, 1, "sha2"),      # 576-byte rows, SHA-256 with 10 blocks
+]
+
+
+def proofs_multi():
+    from oracle.refio import run_reference
+    from whirplonk_b200 import sample_goldilocks
+
+    out = []
+    for (n, k, rho, sec, pb, seed, npts, batch, nwit, eng) in MULTI_CASES:
+        nvec = batch * nwit
+        coeffs = sample_goldilocks(seed, nvec << n).reshape(nvec, 1 << n)
+        points = sample_goldilocks(seed + 5000, npts * n * 3).reshape(npts, n, 3)
+        ref = run_reference(n, k, rho, sec, pb, points, coeffs, verify=True, sha2=eng == "sha2",
+                            batch_size=batch, num_witnesses=nwit)
+        assert ref.verify_ok == 1.0
+        rec = {"n": n, "k": k, "rho": rho, "security": sec, "pow_bits": pb, "seed": seed, "n_points": npts,
+               "batch_size": batch, "num_witnesses": nwit, "hash": eng,
+               "evaluations": [[int(x) for x in row] for row in ref.evaluations],
+               "narg_len": len(ref.narg), "hints_len": len(ref.hints),
+               "narg_sha256": hashlib.sha256(ref.narg).hexdigest(),
+               "hints_sha256": hashlib.sha256(ref.hints).hexdigest()}
+        if n <= 5:
+            rec["narg"] = ref.narg.hex()
+            rec["hints"] = ref.hints.hex()
+        out.append(rec)
+    return out
+
+
 def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
@@ -258,7 +300,8 @@ def main():
         json.dump(gold, f, indent=1)
     with open(os.path.join(HERE, "reference_proofs.json"), "w") as f:
         json.dump({"generator": "oracle/_ref/ref_driver (reference C++ prover, CLI domain separator, "
-                                "seeded ChaCha20 inputs via whirgpu_sample_goldilocks)", "cases": proofs()}, f, indent=1)
+                                "seeded ChaCha20 inputs via whirgpu_sample_goldilocks)", "cases": proofs(),
+                   "multi": proofs_multi()}, f, indent=1)
 
 
 if __name__ == "__main__":

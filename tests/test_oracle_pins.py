@@ -159,3 +159,59 @@ def test_oracle_matches_live_reference(oracle, n, k, rho, sec, pb, seed, sha2):
     assert ref.verify_ok == 1.0
     narg, hints = oracle.prove(n, k, rho, sec, pb, points, coeffs, ref.evaluations, sha2=sha2)
     assert narg == ref.narg and hints == ref.hints
+
+
+MULTI = json.load(open(os.path.join(HERE, "golden", "reference_proofs.json")))["multi"]
+
+
+def _multi_inputs(case):
+    n, nvec = case["n"], case["batch_size"] * case["num_witnesses"]
+    coeffs = sample_goldilocks(case["seed"], nvec << n).reshape(nvec, 1 << n)
+    points = sample_goldilocks(case["seed"] + 5000, case["n_points"] * n * 3).reshape(case["n_points"], n, 3)
+    return coeffs, points
+
+
+@pytest.mark.parametrize("case", MULTI, ids=lambda c: f"n{c['n']}k{c['k']}r{c['rho']}"
+                                                      f"b{c['batch_size']}w{c['num_witnesses']}{c['hash']}")
+def test_oracle_multi_vector_proofs_match_reference_fixtures(oracle, case):
+    """Several committed vectors: rows of batch_size * 2^k elements, OOD values of
+    every vector, OOD completion across witnesses, the vector RLC and the
+    first opening weighted by vector_rlc (x) eq."""
+    coeffs, points = _multi_inputs(case)
+    nvec = coeffs.shape[0]
+    for i in range(case["n_points"]):
+        for j in range(nvec):
+            assert [int(x) for x in oracle.mle_eval_base(coeffs[j], points[i])] == case["evaluations"][i * nvec + j]
+    evals = np.array(case["evaluations"], dtype=np.uint64).reshape(-1, 3)
+    narg, hints = oracle.prove_multi(case["n"], case["k"], case["rho"], case["security"], case["pow_bits"], points,
+                                     coeffs, evals, case["batch_size"], case["num_witnesses"],
+                                     sha2=case["hash"] == "sha2")
+    assert (len(narg), len(hints)) == (case["narg_len"], case["hints_len"])
+    assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
+    if "narg" in case:
+        assert narg.hex() == case["narg"] and hints.hex() == case["hints"]
+
+
+def test_blake3_multi_chunk_tree(oracle):
+    """Messages above one chunk take the tree path without error and give
+    distinct digests at every chunk boundary.  Its values are pinned end to
+    end by the multi-vector reference proofs above, whose leaves are rows of
+    1280, 1536 and 2048 bytes."""
+    msg = bytes((i * 7 + 3) & 0xFF for i in range(4096 + 17))
+    seen = {oracle.blake3(msg[:m]) for m in (1024, 1025, 2048, 2049, 3072, 4096, 4113)}
+    assert len(seen) == 7
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("n,k,rho,batch,nwit,seed,sha2", [(8, 4, 1, 2, 2, 911, False), (10, 5, 1, 5, 1, 912, False),
+                                                          (9, 4, 2, 3, 2, 913, True), (7, 2, 1, 40, 1, 914, False)])
+def test_oracle_multi_vector_matches_live_reference(oracle, n, k, rho, batch, nwit, seed, sha2):
+    nvec = batch * nwit
+    coeffs = sample_goldilocks(seed, nvec << n).reshape(nvec, 1 << n)
+    points = sample_goldilocks(seed + 1, 2 * n * 3).reshape(2, n, 3)
+    ref = run_reference(n, k, rho, 100, 20, points, coeffs, verify=True, sha2=sha2, batch_size=batch,
+                        num_witnesses=nwit)
+    assert ref.verify_ok == 1.0
+    narg, hints = oracle.prove_multi(n, k, rho, 100, 20, points, coeffs, ref.evaluations, batch, nwit, sha2=sha2)
+    assert narg == ref.narg and hints == ref.hints
