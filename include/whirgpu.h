@@ -5,7 +5,8 @@
  * ProtocolParameters, the same SHAKE128 Fiat-Shamir transcript and the same
  * proof byte layout ({narg_string, hints}), for
  *   M = Basefield<GoldilocksExt3> (Goldilocks vectors, Ext3 challenges),
- *   hash = BLAKE3 or SHA-2, one committed vector, MultilinearExtension statements.
+ *   hash = BLAKE3 or SHA-2, one or more witnesses of batch_size vectors,
+ *   MultilinearExtension statements.
  * Everything below is plain C: opaque handles, pointers, sizes and status
  * codes; no C++ types or exceptions cross this boundary.
  *
@@ -26,7 +27,7 @@ extern "C" {
 typedef enum {
     WHIRGPU_OK = 0,
     WHIRGPU_E_INVALID = 1,     /* bad argument or parameters the reference asserts on */
-    WHIRGPU_E_UNSUPPORTED = 2, /* valid for the reference but not on this path (e.g. batch_size > 1) */
+    WHIRGPU_E_UNSUPPORTED = 2, /* valid for the reference but not on this path (e.g. more than 32 vectors) */
     WHIRGPU_E_OOM = 3,         /* device or pinned memory exhausted, or above the HBM budget */
     WHIRGPU_E_CUDA = 4,        /* CUDA runtime error (text in whirgpu_last_error) */
     WHIRGPU_E_DEVICE = 5,      /* a kernel reported an error word (overflow, PoW exhausted) */
@@ -90,19 +91,33 @@ whirgpu_status whirgpu_proof_get(const whirgpu_transcript* tx, const uint8_t** n
                                  const uint8_t** hints, size_t* hints_len);
 
 /* ---- commit (Config::commit, whir.hpp:303-309) ---------------------------------
- * Encodes, hashes and commits one vector of 2^num_variables canonical
- * Goldilocks words; the codeword matrix and Merkle tree stay in HBM in the
- * witness.  Work is queued on the context stream; the call returns without
+ * Encodes, hashes and commits params->batch_size vectors of 2^num_variables
+ * canonical Goldilocks words each, back to back in `coeffs`
+ * (irs_commit::Config::commit with num_vectors = batch_size,
+ * irs_commit.hpp:344-561); the codeword matrix and Merkle tree stay in HBM in
+ * the witness.  Work is queued on the context stream; the call returns without
  * waiting for it. */
 whirgpu_status whirgpu_commit(whirgpu_ctx* ctx, const whirgpu_params* params, const uint64_t* coeffs,
                               uint64_t num_variables, int coeffs_location, whirgpu_transcript* tx,
                               whirgpu_witness** out);
+/* num_witnesses commits in a row on the same transcript, the reference caller's
+ * `for (...) witnesses.push_back(config.commit(ps, vectors_w))` before one
+ * Config::prove over all of them (whir_prover.hpp:56-120): coeffs holds
+ * num_witnesses * batch_size vectors, witness w's first.  The handle stands
+ * for all of them; whirgpu_prove then proves every vector.  At most
+ * WHIRGPU_MAX_WITNESSES witnesses and WHIRGPU_MAX_VECTORS vectors in all. */
+#define WHIRGPU_MAX_WITNESSES 8
+#define WHIRGPU_MAX_VECTORS 32
+whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* ctx, const whirgpu_params* params, const uint64_t* coeffs,
+                                        uint64_t num_witnesses, uint64_t num_variables, int coeffs_location,
+                                        whirgpu_transcript* tx, whirgpu_witness** out);
 void whirgpu_witness_destroy(whirgpu_witness* w);
 
 /* ---- prove (Config::prove, whir_prover.hpp:56-407) ---------------------------
  * Statement: num_points MultilinearExtension forms; points are
  * num_points * num_variables Ext3 coordinates (3 words each, c0 c1 c2),
- * evaluations are num_points Ext3 values (the claimed MLE values).
+ * evaluations are num_points * V Ext3 values, form-major (the claimed MLE value
+ * of form f on vector v at f * V + v), V = the witness's committed vectors.
  * On return the proof is complete and readable with whirgpu_proof_get.
  * evaluation_point (optional) receives num_variables Ext3 values (the
  * FinalClaim evaluation point), rlc (optional) num_points Ext3 values. */
@@ -119,10 +134,10 @@ void whirgpu_last_io_bytes(const whirgpu_ctx* ctx, uint64_t* h2d, uint64_t* d2h)
 typedef struct {
     uint64_t num_variables;
     whirgpu_params params;
-    const uint64_t* coeffs;      /* 2^num_variables canonical words */
+    const uint64_t* coeffs;      /* params.batch_size vectors of 2^num_variables canonical words */
     int coeffs_location;         /* WHIRGPU_INPUT_HOST / WHIRGPU_INPUT_DEVICE */
     const uint64_t* points;      /* num_points * num_variables Ext3 coordinates */
-    const uint64_t* evaluations; /* num_points Ext3 values */
+    const uint64_t* evaluations; /* num_points * batch_size Ext3 values, form-major */
     uint64_t num_points;
     uint8_t protocol_id[64];
     uint8_t session_id[32];

@@ -22,13 +22,14 @@ from .whir import Context, DomainSeparator, ProtocolParameters, cli_domain_separ
 
 @dataclass
 class ProofRequest:
-    """One complete commit + prove of a vector of 2^num_variables coefficients."""
+    """One complete commit + prove of params.batch_size vectors of
+    2^num_variables coefficients."""
 
     num_variables: int
     params: ProtocolParameters
-    coeffs: object  # numpy uint64 array, or a device pointer (int) with on_device=True
+    coeffs: object  # numpy uint64 array (batch_size rows), or a device pointer (int) with on_device=True
     points: np.ndarray  # (num_points, n, 3) uint64
-    evaluations: np.ndarray  # (num_points, 3) uint64
+    evaluations: np.ndarray  # (num_points * batch_size, 3) uint64, form-major
     ds: Optional[DomainSeparator] = None
     on_device: bool = False
     _keep: list = field(default_factory=list, repr=False)
@@ -41,7 +42,7 @@ class ProofRequest:
             r.coeffs, r.coeffs_location = int(self.coeffs), 1
         else:
             c = np.ascontiguousarray(self.coeffs, dtype=np.uint64)
-            assert c.size == 1 << self.num_variables
+            assert c.size == self.params.batch_size << self.num_variables
             self._keep.append(c)
             r.coeffs, r.coeffs_location = c.ctypes.data, 0
         pts = np.ascontiguousarray(self.points, dtype=np.uint64).reshape(-1, self.num_variables, 3)

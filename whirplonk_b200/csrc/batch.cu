@@ -43,7 +43,7 @@ struct Slot {
     uint64_t graph_kernels = 0;        // kernel nodes in `graph`
 };
 
-size_t coeff_bytes(const ProofPlan& p) { return 8ull << p.n; }
+size_t coeff_bytes(const ProofPlan& p) { return (size_t)p.nvec * (8ull << p.n); }  // batch_size vectors
 size_t points_off() { return 96; }
 size_t evals_off(const ProofPlan& p) { return 96 + (size_t)MAX_FORMS * p.n * 24; }
 
@@ -71,7 +71,7 @@ whirgpu_status slot_bind(whirgpu_ctx* c, const whirgpu_request& r, Workspace* ws
     s.plan.n_forms = (int)r.num_points;
     if (r.num_points + s.plan.sch.initial.out_domain == 0)
         return fail(c, WHIRGPU_E_UNSUPPORTED, "statement-free proofs are not on this path");
-    s.hin_bytes = evals_off(s.plan) + MAX_FORMS * 24;
+    s.hin_bytes = evals_off(s.plan) + (size_t)MAX_FORMS * MAX_VECTORS * 24;
     s.hout_bytes = sizeof(TxState) + s.plan.narg_len + s.plan.hints_cap;
     if (cudaMallocHost(&s.hin, s.hin_bytes) != cudaSuccess || cudaMallocHost(&s.hout, s.hout_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -109,7 +109,7 @@ whirgpu_status slot_stage(whirgpu_ctx* c, Slot& s, const whirgpu_request& r) {
     std::memcpy(s.hin + 64, r.session_id, 32);
     if (r.num_points) {
         std::memcpy(s.hin + points_off(), r.points, r.num_points * n * 24);
-        std::memcpy(s.hin + evals_off(s.plan), r.evaluations, r.num_points * 24);
+        std::memcpy(s.hin + evals_off(s.plan), r.evaluations, r.num_points * s.plan.nvec * 24);
     }
     return WHIRGPU_OK;
 }
@@ -134,7 +134,8 @@ int slot_enqueue(whirgpu_ctx* c, Slot& s, cudaStream_t st, bool with_coeffs) {
         if (cudaMemcpyAsync(ws + p.off_points, s.hin + points_off(), p.n_forms * n * 24, cudaMemcpyHostToDevice, st) !=
             cudaSuccess)
             return -1;
-        if (cudaMemcpyAsync(&sc->forms_eval[0], s.hin + evals_off(p), p.n_forms * 24, cudaMemcpyHostToDevice, st) !=
+        if (cudaMemcpyAsync(&sc->forms_eval[0], s.hin + evals_off(p), (size_t)p.n_forms * p.nvec * 24,
+                            cudaMemcpyHostToDevice, st) !=
             cudaSuccess)
             return -1;
     }

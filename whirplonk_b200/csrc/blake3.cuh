@@ -1,12 +1,14 @@
 // blake3.cuh -- BLAKE3 compression on the device (public BLAKE3 spec).
 //
-// The WHIR path only hashes single-chunk messages whose length is a multiple
+// Most messages of the WHIR path are single chunks whose length is a multiple
 // of 64 bytes: codeword rows (128 B base, 384 B Ext3), Merkle parents and
 // proof-of-work inputs (64 B).  Each such hash is a chain of compressions with
 // counter 0, block_len 64, CHUNK_START on the first block and CHUNK_END|ROOT on
 // the last -- the reference's blake3_hash_many call
-// (cpp/include/whir/hash/blake3_engine.hpp:90-199).  ~700 integer ops per
-// compression (add, xor, funnel-shift rotates), all on the CUDA cores.
+// (cpp/include/whir/hash/blake3_engine.hpp:90-199).  Rows of several committed
+// vectors can span several chunks; those use the chunk counter and the PARENT
+// flag of the tree mode.  ~700 integer ops per compression (add, xor,
+// funnel-shift rotates), all on the CUDA cores.
 #pragma once
 #include <cstdint>
 
@@ -14,7 +16,7 @@ namespace wg {
 
 constexpr unsigned B3_IV0 = 0x6A09E667u, B3_IV1 = 0xBB67AE85u, B3_IV2 = 0x3C6EF372u, B3_IV3 = 0xA54FF53Au;
 constexpr unsigned B3_IV4 = 0x510E527Fu, B3_IV5 = 0x9B05688Cu, B3_IV6 = 0x1F83D9ABu, B3_IV7 = 0x5BE0CD19u;
-constexpr unsigned B3_CHUNK_START = 1u, B3_CHUNK_END = 2u, B3_ROOT = 8u;
+constexpr unsigned B3_CHUNK_START = 1u, B3_CHUNK_END = 2u, B3_PARENT = 4u, B3_ROOT = 8u;
 
 // Message word used by G-call slot s (0..15) in round r: the spec's message
 // permutation applied r times.  Folded to a constant after unrolling.
@@ -55,11 +57,13 @@ __device__ __forceinline__ void b3_round(unsigned& v0, unsigned& v1, unsigned& v
     WG_B3_G(v3, v4, v9, v14, m[s14], m[s15]);
 }
 
-// cv <- first half of compress(cv, m, counter = 0, block_len, flags).
-__device__ __forceinline__ void b3_compress(unsigned cv[8], const unsigned m[16], unsigned flags, unsigned block_len = 64) {
+// cv <- first half of compress(cv, m, counter, block_len, flags); counters
+// stay below 2^32 on this path (chunk index within one row).
+__device__ __forceinline__ void b3_compress(unsigned cv[8], const unsigned m[16], unsigned flags, unsigned block_len = 64,
+                                            unsigned counter = 0) {
     unsigned v0 = cv[0], v1 = cv[1], v2 = cv[2], v3 = cv[3], v4 = cv[4], v5 = cv[5], v6 = cv[6], v7 = cv[7];
     unsigned v8 = B3_IV0, v9 = B3_IV1, v10 = B3_IV2, v11 = B3_IV3;
-    unsigned v12 = 0, v13 = 0, v14 = block_len, v15 = flags;
+    unsigned v12 = counter, v13 = 0, v14 = block_len, v15 = flags;
     b3_round<0>(v0, v1, v2, v3, v4, v5, v6, v7, v8, v9, v10, v11, v12, v13, v14, v15, m);
     b3_round<1>(v0, v1, v2, v3, v4, v5, v6, v7, v8, v9, v10, v11, v12, v13, v14, v15, m);
     b3_round<2>(v0, v1, v2, v3, v4, v5, v6, v7, v8, v9, v10, v11, v12, v13, v14, v15, m);

@@ -162,17 +162,20 @@ bool evict_idle(whirgpu_ctx* c, uint64_t need, uint64_t limit) {
 }  // namespace
 
 whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out,
-                                 uint64_t cap) {
+                                 uint64_t cap, uint32_t nwit) {
     ProofPlan plan;
     try {
-        plan = make_plan((uint32_t)n, to_params(params), MAX_FORMS, std::max<size_t>(ds_len, 96));
+        plan = make_plan((uint32_t)n, to_params(params), MAX_FORMS, std::max<size_t>(ds_len, 96), nwit);
     } catch (const std::exception& e) {
         return fail(c, WHIRGPU_E_INVALID, e.what());
     }
+    // The plan carries the hash engine and the vector layout: bits 0 unique
+    // decoding, 1..31 ds length, 32..39 batch size, 40..47 witnesses, 62 SHA-2.
     auto key = std::make_tuple(n, params->starting_log_inv_rate, params->initial_folding_factor, params->folding_factor,
                                params->security_level, params->pow_bits,
                                (uint64_t)params->unique_decoding | ((uint64_t)std::max<size_t>(ds_len, 96) << 1) |
-                                   ((uint64_t)is_sha2(params) << 62));  // the plan carries the hash engine
+                                   (params->batch_size << 32) | ((uint64_t)nwit << 40) |
+                                   ((uint64_t)is_sha2(params) << 62));
     std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
     for (Workspace* w : c->cache[key])
         if (!w->busy) {
@@ -215,9 +218,9 @@ void release_workspace(whirgpu_ctx* c, Workspace* w) {
     w->busy = false;
 }
 
-size_t workspace_bytes(uint64_t n, const whirgpu_params* params) {
+size_t workspace_bytes(uint64_t n, const whirgpu_params* params, uint32_t nwit) {
     try {
-        return make_plan((uint32_t)n, to_params(params), MAX_FORMS, 96).total_bytes;
+        return make_plan((uint32_t)n, to_params(params), MAX_FORMS, 96, nwit).total_bytes;
     } catch (const std::exception&) {
         return 0;
     }
@@ -349,23 +352,28 @@ whirgpu_status whirgpu_proof_get(const whirgpu_transcript* t, const uint8_t** na
     return WHIRGPU_OK;
 }
 
-whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs,
-                              uint64_t n, int where, whirgpu_transcript* tx, whirgpu_witness** out) {
+whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs,
+                                        uint64_t num_witnesses, uint64_t n, int where, whirgpu_transcript* tx,
+                                        whirgpu_witness** out) {
     if (!c || !params || !coeffs || !tx || !out || tx->ctx != c) return fail(c, WHIRGPU_E_INVALID, "null argument");
     *out = nullptr;
     if (!engine_supported(params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 and SHA-2 engines are on this path");
     if (n >= 40) return fail(c, WHIRGPU_E_INVALID, "num_variables too large");
+    if (params->batch_size == 0 || num_witnesses == 0) return fail(c, WHIRGPU_E_INVALID, "no vectors to commit");
+    if (num_witnesses > (uint64_t)MAX_WITNESSES || params->batch_size * num_witnesses > (uint64_t)MAX_VECTORS)
+        return fail(c, WHIRGPU_E_UNSUPPORTED, "more committed vectors than this path holds");
     Workspace* ws = nullptr;
-    whirgpu_status s = acquire_workspace(c, n, params, tx->ds.size(), &ws);
+    whirgpu_status s = acquire_workspace(c, n, params, tx->ds.size(), &ws, 0, (uint32_t)num_witnesses);
     if (s != WHIRGPU_OK) return s;
     const ProofPlan& p = ws->plan;
-    cudaError_t e = cudaMemcpyAsync(ws->dev + p.off_coeffs, coeffs, (8ull << n),
+    const size_t coeff_bytes = (size_t)p.nvec * (8ull << n);
+    cudaError_t e = cudaMemcpyAsync(ws->dev + p.off_coeffs, coeffs, coeff_bytes,
                                     where == WHIRGPU_INPUT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                     c->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(ws->dev + p.off_ds, tx->ds.data(), tx->ds.size(), cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) { release_workspace(c, ws); return cuda_fail(c, e, "input copy"); }
-    c->io_h2d = (where == WHIRGPU_INPUT_DEVICE ? 0 : (8ull << n)) + tx->ds.size();
+    c->io_h2d = (where == WHIRGPU_INPUT_DEVICE ? 0 : coeff_bytes) + tx->ds.size();
     c->io_d2h = 0;
     if (enqueue_commit(p, ws->dev, (uint32_t)tx->ds.size(), c->tw, c->stream, c->timer.get()) != 0) {
         release_workspace(c, ws);
@@ -380,6 +388,11 @@ whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, cons
     tx->complete = false;
     *out = w;
     return WHIRGPU_OK;
+}
+
+whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs, uint64_t n,
+                              int where, whirgpu_transcript* tx, whirgpu_witness** out) {
+    return whirgpu_commit_witnesses(c, params, coeffs, 1, n, where, tx, out);
 }
 
 void whirgpu_witness_destroy(whirgpu_witness* w) {
@@ -407,9 +420,10 @@ whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t*
     if (num_points) {
         e = cudaMemcpyAsync(ws + p.off_points, points, num_points * p.n * 24, cudaMemcpyHostToDevice, c->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpyAsync(&sc->forms_eval[0], evaluations, num_points * 24, cudaMemcpyHostToDevice, c->stream);
+            e = cudaMemcpyAsync(&sc->forms_eval[0], evaluations, num_points * p.nvec * 24, cudaMemcpyHostToDevice,
+                                c->stream);
         if (e != cudaSuccess) return cuda_fail(c, e, "statement upload");
-        c->io_h2d += num_points * p.n * 24 + num_points * 24;
+        c->io_h2d += num_points * p.n * 24 + num_points * p.nvec * 24;
     }
     if (enqueue_prove(p, ws, c->tw, c->stream, c->timer.get()) != 0) return fail(c, WHIRGPU_E_INVALID, "prove launch failed");
     e = cudaGetLastError();

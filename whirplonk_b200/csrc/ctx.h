@@ -123,13 +123,13 @@ ProtocolParams to_params(const whirgpu_params* p);
 whirgpu_status fail(whirgpu_ctx* c, whirgpu_status s, const std::string& msg);
 whirgpu_status cuda_fail(whirgpu_ctx* c, cudaError_t e, const char* what);
 whirgpu_status ensure_pinned(whirgpu_ctx* c, size_t bytes);
-// A free workspace for (n, params, ds_len), allocated on first use and kept in
-// the context cache; marked busy until release_workspace.  Allocation keeps the
-// context's bytes within min(ctx budget, cap) (0 = no limit) by freeing idle
-// workspaces, least recently used first; a failed cudaMalloc frees every idle
-// workspace and tries once more.
+// A free workspace for (n, params, ds_len, nwit initial commitments),
+// allocated on first use and kept in the context cache; marked busy until
+// release_workspace.  Allocation keeps the context's bytes within min(ctx
+// budget, cap) (0 = no limit) by freeing idle workspaces, least recently used
+// first; a failed cudaMalloc frees every idle workspace and tries once more.
 whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out,
-                                 uint64_t cap = 0);
+                                 uint64_t cap = 0, uint32_t nwit = 1);
 void release_workspace(whirgpu_ctx* c, Workspace* w);
 // While set, kernel launches of this thread are stream-captured, not run: the
 // launch counter skips them and graph launches add their kernel-node counts.
@@ -139,5 +139,5 @@ bool is_blake3(const whirgpu_params* p);
 bool is_sha2(const whirgpu_params* p);
 bool engine_supported(const whirgpu_params* p);  // BLAKE3 or SHA-2
 // Plan size of one proof (bytes of device workspace), or 0 when invalid.
-size_t workspace_bytes(uint64_t n, const whirgpu_params* params);
+size_t workspace_bytes(uint64_t n, const whirgpu_params* params, uint32_t nwit = 1);
 }  // namespace wg

@@ -119,6 +119,73 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
     store_node(nodes, i, cv);
 }
 
+// Rows wider than one chunk (1024 bytes: several committed vectors side by
+// side) take BLAKE3's tree mode (blake3_engine.hpp:186-196, the hasher
+// fallback): chunk c is compressed with counter c; a finished chunk's value is
+// merged with the stack while the count of finished chunks has a trailing
+// zero bit; the last chunk's value is merged with the stack from the top, the
+// final merge carrying ROOT.  At most B3_MAX_CHUNKS chunks (16 KiB rows).
+constexpr u32 B3_MAX_CHUNKS = 16;
+__device__ __forceinline__ void b3_parent_cv(const unsigned l[8], const unsigned r[8], unsigned flags, unsigned out[8]) {
+    unsigned m[16];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { m[k] = l[k]; m[8 + k] = r[k]; }
+    b3_init(out);
+    b3_compress(out, m, B3_PARENT | flags);
+}
+
+template <int NCOMP>
+__global__ void __launch_bounds__(128) k_leaves_wide(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes) {
+    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const u32 nwords = depth * NCOMP;
+    const u32 nch = (nwords + 127) / 128;
+    unsigned stack[5][8];  // a tree of < 32 chunks holds at most 5 pending subtrees
+    u32 sp = 0;
+    unsigned cv[8];
+    for (u32 c = 0; c < nch; ++c) {
+        const u32 w0 = c * 128;
+        const u32 cw = min(128u, nwords - w0);
+        const u32 bytes = cw * 8;
+        const u32 nblocks = (bytes + 63) / 64;
+        b3_init(cv);
+        for (u32 t = 0; t < nblocks; ++t) {
+            unsigned m[16];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const u32 w = t * 8 + q;
+                u64 v = 0;
+                if (w < cw) v = row_word<NCOMP>(planes, N, depth, i, w0 + w);
+                m[2 * q] = (unsigned)v;
+                m[2 * q + 1] = (unsigned)(v >> 32);
+            }
+            const u32 len = (t + 1 == nblocks) ? bytes - 64 * t : 64;
+            const unsigned flags = (t == 0 ? B3_CHUNK_START : 0u) |
+                                   (t + 1 == nblocks ? (B3_CHUNK_END | (nch == 1 ? B3_ROOT : 0u)) : 0u);
+            b3_compress(cv, m, flags, len, c);
+        }
+        if (c + 1 < nch) {
+            for (u32 total = c + 1; (total & 1) == 0 && sp > 0; total >>= 1) {
+                unsigned p[8];
+                b3_parent_cv(stack[--sp], cv, 0u, p);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) cv[k] = p[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) stack[sp][k] = cv[k];
+            ++sp;
+        }
+    }
+    while (sp > 0) {
+        --sp;
+        unsigned p[8];
+        b3_parent_cv(stack[sp], cv, sp == 0 ? B3_ROOT : 0u, p);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cv[k] = p[k];
+    }
+    store_node(nodes, i, cv);
+}
+
 __host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
     // [leaves (2^logN) | 2^(logN-1) | ... ]: offset of level l = 2^(logN+1) - 2^(logN+1-l)
     return (2ull << logN) - (2ull << (logN - l));
@@ -135,9 +202,16 @@ __device__ __forceinline__ void parent_cv(const unsigned l[8], const unsigned r[
 
 int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
                        u64 node_stride, int hash, cudaStream_t st) {
-    if (hash != HASH_SHA256 && depth * ncomp * 8 > 1024) return -1;  // multi-chunk BLAKE3 rows are not on this path
     if (count == 0 || count > 65535) return -1;
     if (ncomp != 1 && ncomp != 3) return -1;
+    if (hash != HASH_SHA256 && depth * ncomp * 8 > 1024) {  // BLAKE3 tree mode, one matrix at a time
+        if (count != 1 || depth * ncomp > 128 * B3_MAX_CHUNKS) return -1;
+        const unsigned grid = (unsigned)((N + 127) / 128);
+        if (ncomp == 1) k_leaves_wide<1><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
+        else k_leaves_wide<3><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
+        count_launches(1);
+        return 0;
+    }
     const dim3 grid((unsigned)((N + 255) / 256), count);
     if (hash == HASH_SHA256) {
         if (ncomp == 1) k_leaves<1, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
@@ -286,17 +360,22 @@ int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaSt
 }
 
 // ---------------------------------------------------------------------------
-// Out-of-domain evaluation: value_j = sum_i v_i z_j^i
-// (irs_commit.hpp:472-554 -> utilities.hpp:196-246).  With i = h 2^LO + l,
-//   value_j = sum_h z_j^(h 2^LO) * sum_l v_(h,l) z_j^l :
+// Out-of-domain evaluation: value_(j,v) = sum_i v_i z_j^i for every point z_j
+// and committed vector v (irs_commit.hpp:472-554 -> utilities.hpp:196-246),
+// and the cross-witness completion of Config::prove (whir_prover.hpp:92-120),
+// which evaluates the other witnesses' vectors at a witness's points.  With
+// i = h 2^LO + l,
+//   value = sum_h z_j^(h 2^LO) * sum_l v_(h,l) z_j^l :
 // a warp owns whole blocks of 2^LO consecutive coefficients and accumulates
 // the inner sum as unreduced 192-bit products against the table z_j^l, reduces
 // once per block and scales by the table entry z_j^(h 2^LO).  Exact field
 // sums, so the association order is free.  The last CTA (ticket) finishes the
-// sums and sends the values as prover messages.
+// sums and sends the values as prover messages, point-major, every evaluated
+// vector at each point.
 // ---------------------------------------------------------------------------
 constexpr int OOD_GRID = 592, OOD_THREADS = 256;
 constexpr u32 OOD_LO = 10;
+constexpr int OOD_MAX_VALUES = MAX_OOD * MAX_VECTORS;
 
 __device__ __forceinline__ E3 block_sum_e3(E3 v, E3* red) {
     v = e3_warp_sum(v);
@@ -313,42 +392,49 @@ __device__ __forceinline__ E3 block_sum_e3(E3 v, E3* red) {
 static u32 ood_hi_count(u64 size) { return (u32)((size + (1ull << OOD_LO) - 1) >> OOD_LO); }
 
 // tab[j]: z_j^l for l < 2^LO, then z_j^(h 2^LO) for h < hi_count.
-__global__ void k_ood_tables(const ProofScalars* sc, int commit_idx, int n_ood, u32 hi_count, E3* tab) {
+__global__ void k_ood_tables(const E3* pts, int n_ood, u32 hi_count, E3* tab) {
     const u32 per = (1u << OOD_LO) + hi_count;
     const u64 total = (u64)per * n_ood;
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 j = (u32)(e / per), k = (u32)(e % per);
-        const E3 z = sc->ood_pts[commit_idx][j];
+        const E3 z = pts[j];
         tab[e] = k < (1u << OOD_LO) ? e3_pow(z, k) : e3_pow(z, (u64)(k - (1u << OOD_LO)) << OOD_LO);
     }
 }
 
-__global__ void __launch_bounds__(OOD_THREADS) k_ood(const u64* v0, const u64* v1, const u64* v2, int ext3, u64 size,
-                                                     TxState* tx, ProofScalars* sc, int commit_idx, int n_ood,
-                                                     const E3* tab, u32 hi_count, E3* partials, unsigned* counter) {
+__global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u32 hi_count, E3* partials,
+                                                     unsigned* counter) {
     __shared__ E3 red[32];
     __shared__ bool is_last;
+    __shared__ E3 totals[OOD_MAX_VALUES];
     const u32 lane = threadIdx.x & 31;
     const u64 gw = (u64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const u64 nw = (u64)gridDim.x * (blockDim.x >> 5);
     const u32 per = (1u << OOD_LO) + hi_count;
-    for (int j = 0; j < n_ood; ++j) {
+    const u64 size = a.size;
+    const u32 nvals = (u32)a.n_ood * a.nvec;
+    for (int j = 0; j < a.n_ood; ++j) {
         const E3* zlo = tab + (u64)j * per;
         const E3* zhi = zlo + (1u << OOD_LO);
-        E3 acc = e3_zero();
-        for (u64 h = gw; h < hi_count; h += nw) {
-            const u64 base = h << OOD_LO;
-            const u32 cnt = (u32)((size - base) < (1ull << OOD_LO) ? (size - base) : (1ull << OOD_LO));
-            E3Acc s = e3acc_zero();
-            if (ext3) {
-                for (u32 l = lane; l < cnt; l += 32) e3acc_mac(s, zlo[l], E3{v0[base + l], v1[base + l], v2[base + l]});
-            } else {
-                for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], v0[base + l]);
+        for (u32 v = 0; v < a.nvec; ++v) {
+            if (v >= a.skip_lo && v < a.skip_hi) continue;
+            const u64* b0 = a.v[0] + (u64)v * a.vec_stride;
+            E3 acc = e3_zero();
+            for (u64 h = gw; h < hi_count; h += nw) {
+                const u64 base = h << OOD_LO;
+                const u32 cnt = (u32)((size - base) < (1ull << OOD_LO) ? (size - base) : (1ull << OOD_LO));
+                E3Acc s = e3acc_zero();
+                if (a.ext3) {
+                    for (u32 l = lane; l < cnt; l += 32)
+                        e3acc_mac(s, zlo[l], E3{b0[base + l], a.v[1][base + l], a.v[2][base + l]});
+                } else {
+                    for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], b0[base + l]);
+                }
+                acc = e3_add(acc, e3_mul(e3acc_reduce(s), zhi[h]));
             }
-            acc = e3_add(acc, e3_mul(e3acc_reduce(s), zhi[h]));
+            E3 bs = block_sum_e3(acc, red);
+            if (threadIdx.x == 0) partials[(u64)blockIdx.x * nvals + (u32)j * a.nvec + v] = bs;
         }
-        E3 bs = block_sum_e3(acc, red);
-        if (threadIdx.x == 0) partials[blockIdx.x * MAX_OOD + j] = bs;
     }
     if (threadIdx.x == 0) {
         __threadfence();
@@ -357,51 +443,55 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(const u64* v0, const u64* v
     }
     __syncthreads();
     if (!is_last) return;
-    __shared__ E3 totals[MAX_OOD];
-    for (int j = 0; j < n_ood; ++j) {
+    for (u32 k = 0; k < nvals; ++k) {
+        const u32 v = k % a.nvec;
+        if (v >= a.skip_lo && v < a.skip_hi) continue;
         E3 acc = e3_zero();
         for (u32 b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-            const E3* pp = &partials[b * MAX_OOD + j];
+            const E3* pp = &partials[(u64)b * nvals + k];
             acc = e3_add(acc, E3{__ldcg(&pp->c0), __ldcg(&pp->c1), __ldcg(&pp->c2)});
         }
         E3 total = block_sum_e3(acc, red);
         if (threadIdx.x == 0) {
-            sc->ood_vals[commit_idx][j] = total;
-            totals[j] = total;
+            a.out[(k / a.nvec) * a.out_stride + v] = total;
+            totals[k] = total;
         }
     }
     __syncthreads();
     if (threadIdx.x < 32) {  // warp 0 sends the values
         WarpTx t;
-        wtx_load(t, tx);
-        for (int j = 0; j < n_ood; ++j) wtx_message_e3(t, totals[j]);
-        wtx_store(t, tx);
+        wtx_load(t, a.tx);
+        for (u32 k = 0; k < nvals; ++k) {
+            const u32 v = k % a.nvec;
+            if (v < a.skip_lo || v >= a.skip_hi) wtx_message_e3(t, totals[k]);
+        }
+        wtx_store(t, a.tx);
     }
     if (threadIdx.x == 0) *counter = 0;
 }
 
-size_t ood_scratch_bytes(u64 max_size) {
-    return 256 + (size_t)OOD_GRID * MAX_OOD * sizeof(E3) +
+size_t ood_scratch_bytes(u64 max_size, u32 max_values) {
+    return 256 + (size_t)OOD_GRID * max_values * sizeof(E3) +
            (size_t)MAX_OOD * ((1u << OOD_LO) + ood_hi_count(max_size)) * sizeof(E3);
 }
 
-int launch_ood(const u64* v0, const u64* v1, const u64* v2, bool ext3, u64 size, TxState* tx, ProofScalars* sc,
-               int commit_idx, int n_ood, void* scratch, cudaStream_t st) {
-    if (n_ood <= 0) return 0;
-    if (n_ood > MAX_OOD || size == 0) return -1;
-    const u32 hc = ood_hi_count(size);
-    char* base = reinterpret_cast<char*>(scratch);
+int launch_ood(const OodArgs& a, cudaStream_t st) {
+    if (a.n_ood <= 0) return 0;
+    if (a.n_ood > MAX_OOD || a.size == 0 || a.nvec == 0 || a.nvec > (u32)MAX_VECTORS) return -1;
+    if (a.ext3 && a.nvec != 1) return -1;
+    if ((u32)a.n_ood * a.nvec > a.scratch_values) return -1;
+    const u32 hc = ood_hi_count(a.size);
+    char* base = reinterpret_cast<char*>(a.scratch);
     unsigned* counter = reinterpret_cast<unsigned*>(base);
     E3* partials = reinterpret_cast<E3*>(base + 256);
-    E3* tab = partials + (size_t)OOD_GRID * MAX_OOD;
-    const u64 entries = (u64)((1u << OOD_LO) + hc) * n_ood;
-    k_ood_tables<<<(unsigned)std::min<u64>(296, (entries + 255) / 256), 256, 0, st>>>(sc, commit_idx, n_ood, hc, tab);
+    E3* tab = partials + (size_t)OOD_GRID * a.scratch_values;
+    const u64 entries = (u64)((1u << OOD_LO) + hc) * a.n_ood;
+    k_ood_tables<<<(unsigned)std::min<u64>(296, (entries + 255) / 256), 256, 0, st>>>(a.pts, a.n_ood, hc, tab);
     count_launches(1);
     const u64 warps_per_cta = OOD_THREADS / 32;
     u64 want = (hc + warps_per_cta - 1) / warps_per_cta;
     unsigned grid = (unsigned)(want < 1 ? 1 : (want > OOD_GRID ? OOD_GRID : want));
-    k_ood<<<grid, OOD_THREADS, 0, st>>>(v0, v1, v2, ext3 ? 1 : 0, size, tx, sc, commit_idx, n_ood, tab, hc, partials,
-                                        counter);
+    k_ood<<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
     count_launches(1);
     return 0;
 }

@@ -412,7 +412,7 @@ __global__ void k_cov_tables(const u64* points, u32 logS, int n_forms, int n_ood
             }
         } else {
             const int j = (int)term - n_forms;
-            const E3 z = sc->ood_pts[0][j];
+            const E3 z = sc->init_ood_pts[j];
             if (k < nlo) v = e3_pow(z, k);
             else v = e3_mul(sc->crlc[n_forms + j], e3_pow(z, (u64)(k - nlo) << lo_bits));
         }
@@ -434,6 +434,14 @@ __global__ void __launch_bounds__(256) k_cov_init(CovInitArgs a, const E3* tab) 
         a.cov[0][i] = acc.c0;
         a.cov[1][i] = acc.c1;
         a.cov[2][i] = acc.c2;
+        if (a.nvec > 1) {
+            E3Acc r = e3acc_zero();
+            for (u32 v = 0; v < a.nvec; ++v) e3acc_mac_base(r, a.sc->vrlc[v], a.vecs[(u64)v * S + i]);
+            const E3 x = e3acc_reduce(r);
+            a.vec_out[0][i] = x.c0;
+            a.vec_out[1][i] = x.c1;
+            a.vec_out[2][i] = x.c2;
+        }
     }
     (void)nhi;
 }
@@ -444,11 +452,12 @@ size_t cov_init_scratch_bytes(u32 logS, int n_forms, int n_ood) {
 }
 
 int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
-    if (a.n_forms > MAX_FORMS || a.n_ood > MAX_OOD) return -1;
+    if (a.n_forms > MAX_FORMS || a.n_ood > MAX_INIT_OOD || a.nvec < 1 || a.nvec > (u32)MAX_VECTORS) return -1;
     E3* tab = reinterpret_cast<E3*>(a.scratch);
     const int nterms = a.n_forms + a.n_ood;
     const u64 S = 1ull << a.logS;
     if (nterms == 0) {
+        if (a.nvec > 1) return -1;  // statement-free proofs are not on this path
         for (int c = 0; c < 3; ++c) cudaMemsetAsync(a.cov[c], 0, S * 8, st);
         return 0;
     }

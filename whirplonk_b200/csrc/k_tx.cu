@@ -39,27 +39,37 @@ int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned ch
     return 0;
 }
 
-// Constraint RLC and "the sum" (whir_prover.hpp:150-197) for one vector:
-// sum = sum_f crlc_f eval_f + sum_j crlc_{F+j} ood_val_j.
-// One warp (n_forms + n_ood <= 16).
-__global__ void k_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood) {
+// Vector RLC, constraint RLC and "the sum" (whir_prover.hpp:122-197):
+//   vrlc = geometric_challenge(V), crlc = geometric_challenge(F + O),
+//   sum  = sum_f crlc_f sum_v vrlc_v eval_(f,v) + sum_i crlc_(F+i) sum_v vrlc_v ood_(i,v)
+// over the O = nwit * ood initial OOD points, whose coordinates are also laid
+// out contiguously for the covector.  One warp.
+__global__ void k_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int nwit, int ood, int nvec) {
     if (threadIdx.x >= 32) return;
+    const int l = threadIdx.x;
+    const int n_ood = nwit * ood;
+    for (int i = l; i < n_ood; i += 32) sc->init_ood_pts[i] = sc->ood_pts[i / ood][i % ood];
     const int count = n_forms + n_ood;
     WarpTx t;
     wtx_load(t, tx);
+    wtx_geometric(t, sc->vrlc, nvec);
     wtx_geometric(t, sc->crlc, count);
     wtx_store(t, tx);
-    const int l = threadIdx.x;
     E3 v = e3_zero();
-    if (l < n_forms) v = e3_mul(sc->crlc[l], sc->forms_eval[l]);
-    else if (l < count) v = e3_mul(sc->crlc[l], sc->ood_vals[0][l - n_forms]);
+    for (int r = l; r < count; r += 32) {
+        const E3* vals = r < n_forms ? &sc->forms_eval[r * nvec] : &sc->init_ood_mat[(r - n_forms) * nvec];
+        E3 row = e3_zero();
+        for (int k = 0; k < nvec; ++k) row = e3_add(row, e3_mul(sc->vrlc[k], vals[k]));
+        v = e3_add(v, e3_mul(sc->crlc[r], row));
+    }
     v = wtx_sum(v);
     if (l == 0) sc->sum = v;
 }
 
-int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood, cudaStream_t st) {
-    if (n_forms > MAX_FORMS || n_ood > MAX_OOD) return -1;
-    k_constraint_rlc<<<1, 32, 0, st>>>(tx, sc, n_forms, n_ood);
+int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int nwit, int ood, int nvec, cudaStream_t st) {
+    if (n_forms > MAX_FORMS || ood > MAX_OOD || nwit < 1 || nwit > MAX_WITNESSES || nvec < 1 || nvec > MAX_VECTORS)
+        return -1;
+    k_constraint_rlc<<<1, 32, 0, st>>>(tx, sc, n_forms, nwit, ood, nvec);
     count_launches(1);
     return 0;
 }
@@ -186,12 +196,17 @@ int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2,
 
 // ---------------------------------------------------------------------------
 // Opening (irs_commit.hpp:600-713, challenge_indices.hpp:56-119,
-// merkle_tree.hpp:165-211), one CTA of 1024 threads:
+// merkle_tree.hpp:165-211) of nwit commitments at the same rows, one CTA of
+// 1024 threads:
 //   1. squeeze q * ceil(log2(N)/8) bytes, index = big-endian bytes mod N;
-//   2. hint: u64 (q * depth), then the q rows in index order (duplicates kept);
-//   3. (STIR) point gen^idx and value <row, eq_weights(last folding randomness)>;
-//   4. Merkle hints: sorted, deduplicated indices climbed level by level, a
-//      node's sibling is emitted unless the sibling is itself in the set.
+//   2. per commitment: hint u64 (q * depth), the q rows in index order
+//      (duplicates kept), then its Merkle hints -- sorted, deduplicated
+//      indices climbed level by level, a node's sibling is emitted unless the
+//      sibling is itself in the set.  Every commitment has the same tree shape
+//      and indices, so its hint block has the same length;
+//   3. (STIR) point gen^idx and value <rows, vector_rlc (x) eq_weights(last
+//      folding randomness)> over the rows of all commitments side by side
+//      (whir_prover.hpp:283-310).
 // ---------------------------------------------------------------------------
 constexpr int OPEN_THREADS = 1024;
 
@@ -227,11 +242,14 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
     __shared__ E3 eqw[MAX_DEPTH];
     __shared__ u64 hint_base;
     __shared__ unsigned char idx_bytes[MAX_QUERIES * 8];
+    __shared__ unsigned char occ[MAX_QUERIES];
+    __shared__ u32 lvl_cnt[32];
     const TxState* tx = a.tx;  // hint pointers and capacity only; warp 0 carries the sponge
     ProofScalars* sc = a.sc;
     const u32 t = threadIdx.x;
     const u32 q = a.q;
     const u32 nbytes = (a.logN + 7) / 8;
+    const u32 nwit = a.nwit;
 
     // 1. indices: warp 0 squeezes q * nbytes bytes (big-endian per index)
     WarpTx wt;
@@ -247,7 +265,7 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
     }
     if (t == 0) {
         hint_base = wt.hints_len;
-        // 3a. eq weights of the last `fold` folding challenges (multilinear_point.hpp:40-62)
+        // eq weights of the last `fold` folding challenges (multilinear_point.hpp:40-62)
         if (a.stir) {
             const u32 d = 1u << a.fold;
             for (u32 i = 0; i < d; ++i) {
@@ -261,54 +279,12 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
             }
         }
     }
+    for (u32 s2 = t; s2 < (u32)MAX_QUERIES; s2 += blockDim.x) occ[s2] = 0;
     __syncthreads();
     for (u32 i = t; i < q; i += blockDim.x) sc->indices[i] = idx_s[i];
 
-    // 2. row hint
-    const u64 esz = 8ull * a.ncomp;
-    const u64 row_bytes = esz * a.depth;
-    const u64 total_hint = 8 + row_bytes * q + 0;
-    const bool fits = hint_base + total_hint <= tx->hints_cap;
-    unsigned char* hb = tx->hints + hint_base;
-    if (fits) {
-        if (t == 0) {
-            const u64 len = (u64)q * a.depth;
-            for (int k = 0; k < 8; ++k) hb[k] = (unsigned char)(len >> (8 * k));
-        }
-        const u64 nwords = (u64)q * a.depth * a.ncomp;
-        for (u64 w = t; w < nwords; w += blockDim.x) {
-            const u64 qi = w / ((u64)a.depth * a.ncomp);
-            const u64 rem = w - qi * a.depth * a.ncomp;
-            const u32 el = (u32)(rem / a.ncomp), c = (u32)(rem % a.ncomp);
-            const u64 v = a.planes[((u64)c * a.depth + el) * a.N + idx_s[qi]];
-            unsigned char* dst = hb + 8 + qi * row_bytes + (u64)el * esz + 8ull * c;
-            for (int k = 0; k < 8; ++k) dst[k] = (unsigned char)(v >> (8 * k));
-        }
-    }
-
-    // 3b. STIR point and value of each opened row
-    if (a.stir) {
-        for (u32 i = t; i < q; i += blockDim.x) {
-            const u64 id = idx_s[i];
-            E3 val = e3_zero();
-            for (u32 el = 0; el < a.depth; ++el) {
-                E3 x;
-                if (a.ncomp == 1) x = e3_base(a.planes[(u64)el * a.N + id]);
-                else x = E3{a.planes[(u64)el * a.N + id], a.planes[((u64)a.depth + el) * a.N + id],
-                            a.planes[((u64)2 * a.depth + el) * a.N + id]};
-                val = e3_add(val, e3_mul(x, eqw[el]));
-            }
-            sc->stir_pts[a.ood_offset + i] = e3_base(gl_pow(a.gen, id));
-            sc->stir_vals[a.ood_offset + i] = val;
-        }
-    }
-
-    // 4. Merkle hints.  Sort + dedup: a first occurrence v goes to slot
-    //    #{j : idx_j < v}; distinct values get distinct, order-preserving
-    //    slots, which are then compacted with a CTA scan.
-    __shared__ unsigned char occ[MAX_QUERIES];
-    for (u32 s2 = t; s2 < (u32)MAX_QUERIES; s2 += blockDim.x) occ[s2] = 0;
-    __syncthreads();
+    // Sort + dedup: a first occurrence v goes to slot #{j : idx_j < v}; distinct
+    // values get distinct, order-preserving slots, compacted with a CTA scan.
     if (t < q) {
         const u64 v = idx_s[t];
         u32 lt = 0;
@@ -324,18 +300,17 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
     const bool present = t < q && occ[t];
     const u64 pv = present ? cur[t] : 0;
     const u32 pos = block_scan(present, warp_tot, &total);
-    const u32 tot_distinct = total;
+    const u32 u = total;
     if (present) cur[pos] = pv;
     __syncthreads();
 
-    // Per level L the nodes are the distinct values of cur[j] >> L (cur is sorted,
-    // so equal values are adjacent); a node x emits its sibling x ^ 1 unless the
-    // sibling is itself a node.  Warp L handles level L: it walks cur in chunks
-    // of 32 lanes and ranks its emitters with a ballot.  The per-level counts are
-    // prefix-summed, so every warp writes its siblings at the reference's
-    // position (level by level, increasing x within a level) after one barrier.
-    __shared__ u32 lvl_cnt[32];
-    const u32 u = tot_distinct;
+    // Merkle levels.  Per level L the nodes are the distinct values of
+    // cur[j] >> L (cur is sorted, so equal values are adjacent); a node x emits
+    // its sibling x ^ 1 unless the sibling is itself a node.  Warp L handles
+    // level L: it walks cur in chunks of 32 lanes and ranks its emitters with a
+    // ballot.  The per-level counts are prefix-summed, so every warp writes its
+    // siblings at the reference's position (level by level, increasing x within
+    // a level).
     const u32 warp = t >> 5, lane = t & 31;
     auto present_at = [&](u64 y, u32 L) -> bool {  // is y a node of level L?
         u32 lo = 0, hi = u;
@@ -358,24 +333,81 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
         if (lane == 0) lvl_cnt[warp] = cnt;
     }
     __syncthreads();
-    u64 node_hint_off = hint_base + total_hint;
+    u64 merkle_bytes = 0;
+    for (u32 k = 0; k < a.logN; ++k) merkle_bytes += 32ull * lvl_cnt[k];
+    const u64 esz = 8ull * a.ncomp;
+    const u64 row_bytes = esz * a.depth;
+    const u64 row_hint = 8 + row_bytes * q;
+    const u64 blk = row_hint + merkle_bytes;  // hint bytes of one commitment
+    const bool fits = hint_base + blk * nwit <= tx->hints_cap;
+
+    // 2a. row hints
+    if (fits) {
+        const u64 nwords = (u64)q * a.depth * a.ncomp;
+        for (u32 w = 0; w < nwit; ++w) {
+            unsigned char* hb = tx->hints + hint_base + w * blk;
+            const u64* planes = a.planes + w * a.planes_stride;
+            if (t == 0) {
+                const u64 len = (u64)q * a.depth;
+                for (int k = 0; k < 8; ++k) hb[k] = (unsigned char)(len >> (8 * k));
+            }
+            for (u64 x = t; x < nwords; x += blockDim.x) {
+                const u64 qi = x / ((u64)a.depth * a.ncomp);
+                const u64 rem = x - qi * a.depth * a.ncomp;
+                const u32 el = (u32)(rem / a.ncomp), c = (u32)(rem % a.ncomp);
+                const u64 v = planes[((u64)c * a.depth + el) * a.N + idx_s[qi]];
+                unsigned char* dst = hb + 8 + qi * row_bytes + (u64)el * esz + 8ull * c;
+                for (int k = 0; k < 8; ++k) dst[k] = (unsigned char)(v >> (8 * k));
+            }
+        }
+    }
+
+    // 3. STIR point and value of each opened row
+    if (a.stir) {
+        const u32 dmask = (1u << a.fold) - 1;
+        for (u32 i = t; i < q; i += blockDim.x) {
+            const u64 id = idx_s[i];
+            E3 val = e3_zero();
+            for (u32 w = 0; w < nwit; ++w) {
+                const u64* planes = a.planes + w * a.planes_stride;
+                for (u32 v0 = 0; v0 < a.depth; v0 += dmask + 1) {  // one committed vector's 2^fold columns
+                    E3 inner = e3_zero();
+                    for (u32 e = 0; e <= dmask; ++e) {
+                        const u32 el = v0 + e;
+                        E3 x;
+                        if (a.ncomp == 1) x = e3_base(planes[(u64)el * a.N + id]);
+                        else x = E3{planes[(u64)el * a.N + id], planes[((u64)a.depth + el) * a.N + id],
+                                    planes[((u64)2 * a.depth + el) * a.N + id]};
+                        inner = e3_add(inner, e3_mul(x, eqw[e]));
+                    }
+                    const u32 vec = w * (a.depth >> a.fold) + (v0 >> a.fold);
+                    val = e3_add(val, a.use_vrlc ? e3_mul(inner, sc->vrlc[vec]) : inner);
+                }
+            }
+            sc->stir_pts[a.ood_offset + i] = e3_base(gl_pow(a.gen, id));
+            sc->stir_vals[a.ood_offset + i] = val;
+        }
+    }
+
+    // 2b. Merkle hints of every commitment
     if (warp < a.logN) {
         const u32 L = warp;
-        u64 base = node_hint_off;
-        for (u32 k = 0; k < L; ++k) base += 32ull * lvl_cnt[k];
+        u64 lvl_base = row_hint;
+        for (u32 k = 0; k < L; ++k) lvl_base += 32ull * lvl_cnt[k];
         const u64 level_off = (2ull << a.logN) - (2ull << (a.logN - L));
         u32 rank = 0;
         for (u32 j0 = 0; j0 < u; j0 += 32) {
             const u32 j = j0 + lane;
             const bool e = emits(j, L);
             const unsigned m = __ballot_sync(0xFFFFFFFFu, e);
-            if (e) {
-                const u64 dst_off = base + 32ull * (rank + __popc(m & ((1u << lane) - 1)));
-                if (fits && dst_off + 32 <= tx->hints_cap) {
-                    const u64 x = cur[j] >> L;
-                    const uint4* src = reinterpret_cast<const uint4*>(a.nodes + (level_off + (x ^ 1)) * 8);
+            if (e && fits) {
+                const u64 x = cur[j] >> L;
+                const u64 rel = lvl_base + 32ull * (rank + __popc(m & ((1u << lane) - 1)));
+                for (u32 w = 0; w < nwit; ++w) {
+                    const u32* nodes = a.nodes + w * a.nodes_stride;
+                    const uint4* src = reinterpret_cast<const uint4*>(nodes + (level_off + (x ^ 1)) * 8);
                     const uint4 h0 = src[0], h1 = src[1];
-                    unsigned char* dst = tx->hints + dst_off;
+                    unsigned char* dst = tx->hints + hint_base + w * blk + rel;
                     const unsigned w8[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
                     for (int k = 0; k < 32; ++k) dst[k] = (unsigned char)(w8[k >> 2] >> (8 * (k & 3)));
                 }
@@ -383,16 +415,16 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
             rank += __popc(m);
         }
     }
-    for (u32 k = 0; k < a.logN; ++k) node_hint_off += 32ull * lvl_cnt[k];
     if (t < 32) {
-        if (!fits || node_hint_off > wt.hints_cap) wt.err |= TX_ERR_HINT_OVERFLOW;
-        else wt.hints_len = node_hint_off;
+        if (!fits) wt.err |= TX_ERR_HINT_OVERFLOW;
+        else wt.hints_len = hint_base + blk * nwit;
         wtx_store(wt, a.tx);
     }
 }
 
 int launch_open(const OpenArgs& a, cudaStream_t st) {
-    if (a.q > (u32)MAX_QUERIES || a.depth > (u32)MAX_DEPTH) return -1;
+    if (a.q > (u32)MAX_QUERIES || (1u << a.fold) > (u32)MAX_DEPTH || a.nwit < 1 || a.nwit > (u32)MAX_WITNESSES) return -1;
+    if (a.stir && (a.depth & ((1u << a.fold) - 1)) != 0) return -1;
     k_open<<<1, OPEN_THREADS, 0, st>>>(a);
     count_launches(1);
     return 0;

@@ -11,6 +11,7 @@ typedef uint64_t u64;
 typedef unsigned int u32;
 struct TxState;
 struct ProofScalars;
+struct E3;
 
 // Twiddle tables: w_{2^TW_LOG}^E = tw_hi[E >> TW_HALF] * tw_lo[E & (2^TW_HALF - 1)],
 // and stage twiddles tw_stage[u] = w_{2^TW_STAGE_LOG}^u, u < 2^(TW_STAGE_LOG-1).
@@ -83,18 +84,35 @@ int launch_merkle(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, int commi
 int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaStream_t st);
 
 // ---- Out-of-domain evaluation ----------------------------------------------
-// value_j = sum_i v_i z_j^i for z_j = sc->ood_pts[commit_idx][j]; the last CTA
-// sends every value as a prover message (in point order) and stores them in
-// sc->ood_vals[commit_idx].
-int launch_ood(const u64* v0, const u64* v1, const u64* v2, bool ext3, u64 size, TxState* tx, ProofScalars* sc,
-               int commit_idx, int n_ood, void* scratch, cudaStream_t st);
-size_t ood_scratch_bytes(u64 max_size);
+// value_(j,v) = sum_i x_v[i] z_j^i for the points z_j = pts[j] and the vectors
+// x_v, v < nvec (base vectors vec_stride words apart, or one Ext3 vector in
+// three planes).  Vectors in [skip_lo, skip_hi) are skipped.  The last CTA
+// stores value_(j,v) at out[j * out_stride + v] and sends the values as prover
+// messages, point-major.
+struct OodArgs {
+    const u64* v[3];
+    int ext3;
+    u64 size;                 // coefficients per vector
+    u32 nvec;
+    u64 vec_stride;
+    u32 skip_lo, skip_hi;
+    const E3* pts;
+    int n_ood;
+    E3* out;
+    u32 out_stride;
+    TxState* tx;
+    void* scratch;
+    u32 scratch_values;       // n_ood * nvec capacity of the scratch
+};
+int launch_ood(const OodArgs& a, cudaStream_t st);
+size_t ood_scratch_bytes(u64 max_size, u32 max_values);
 
 // ---- Transcript / protocol steps (single-thread kernels) ---------------------
 int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
                    unsigned char* hints, u64 hints_cap, ProofScalars* sc, cudaStream_t st);
-// Constraint RLC + initial sum (whir_prover.hpp:150-197).
-int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int n_ood, cudaStream_t st);
+// Vector RLC, constraint RLC + initial sum (whir_prover.hpp:122-197) over
+// nvec vectors and nwit initial commitments of `ood` OOD points each.
+int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int nwit, int ood, int nvec, cudaStream_t st);
 // PoW: squeeze the 32-byte challenge, grind the minimum nonce, send it.
 int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, int hash, cudaStream_t st);
 // Sends every coefficient of the final folded vector (whir_prover.hpp:360-362).
@@ -104,17 +122,21 @@ int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2,
 struct OpenArgs {
     TxState* tx;
     ProofScalars* sc;
-    const u64* planes;  // codeword planes of the opened commitment
+    const u64* planes;  // codeword planes of the first opened commitment
     const u32* nodes;   // its Merkle nodes
+    u32 nwit;           // commitments opened at the same rows (initial commitments)
+    u64 planes_stride;  // words from one commitment's planes to the next
+    u64 nodes_stride;   // u32 words from one commitment's nodes to the next
     u64 N;              // codeword length
     u32 logN;
-    u32 depth, ncomp;   // row = depth elements of ncomp words
+    u32 depth, ncomp;   // row = depth elements of ncomp words (vectors x 2^fold)
     u32 q;              // in-domain samples
     u64 gen;            // w_N (evaluation-domain generator)
     int stir;           // also fill sc->stir_pts/stir_vals[ood_offset + i]
+    int use_vrlc;       // weigh vector v's columns by sc->vrlc[v] (first round)
     int ood_offset;
     int r_offset;       // sc->sc_r[r_offset .. r_offset + fold) are the folding randomness
-    u32 fold;           // number of folding variables (depth = 2^fold)
+    u32 fold;           // number of folding variables (2^fold columns per vector)
 };
 int launch_open(const OpenArgs& a, cudaStream_t st);
 // STIR combination (whir_prover.hpp:283-336): copy the new commitment's OOD
@@ -122,7 +144,10 @@ int launch_open(const OpenArgs& a, cudaStream_t st);
 int launch_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_ood, int q, cudaStream_t st);
 
 // ---- Covector / sumcheck ---------------------------------------------------------
-// cov[i] = sum_f crlc_f eq(p_f, i) + sum_j crlc_{F+j} z_j^i over 2^logS entries.
+// cov[i] = sum_f crlc_f eq(p_f, i) + sum_j crlc_{F+j} z_j^i over 2^logS entries
+// (z_j = sc->init_ood_pts[j]).  With nvec > 1 the same pass writes the vector
+// RLC vec[i] = sum_v vrlc_v x_v[i] of the committed base vectors
+// (whir_prover.hpp:131-140).
 struct CovInitArgs {
     u64* cov[3];
     u32 logS;
@@ -130,6 +155,9 @@ struct CovInitArgs {
     int n_forms, n_ood;
     ProofScalars* sc;
     void* scratch;
+    u32 nvec;           // committed vectors (1: no vector RLC)
+    const u64* vecs;    // nvec base vectors, 2^logS words each, back to back
+    u64* vec_out[3];    // Ext3 planes of the combined vector
 };
 int launch_cov_init(const CovInitArgs& a, cudaStream_t st);
 size_t cov_init_scratch_bytes(u32 logS, int n_forms, int n_ood);

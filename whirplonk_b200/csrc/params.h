@@ -98,7 +98,7 @@ inline WhirSchedule make_schedule(uint64_t num_variables, const ProtocolParams& 
     if (p.initial_folding_factor == 0 || p.folding_factor == 0) throw std::invalid_argument("folding factor must be >= 1");
     if (num_variables < p.initial_folding_factor) throw std::invalid_argument("num_variables < initial folding factor");
     if (p.pow_bits > p.security_level) throw std::invalid_argument("pow_bits > security_level");
-    if (p.batch_size != 1) throw std::invalid_argument("batch_size != 1 is not supported");
+    if (p.batch_size == 0) throw std::invalid_argument("batch_size must be >= 1");
     const uint64_t size = 1ull << num_variables;
     WhirSchedule c;
     c.num_variables = num_variables;

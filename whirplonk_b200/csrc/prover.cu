@@ -1,11 +1,13 @@
 // prover.cu -- workspace layout and kernel schedule of commit + prove.
 //
 // The order of steps is the reference's (cpp/include/whir/protocols/whir/
-// whir.hpp:303-309 and whir_prover.hpp:56-407) specialised to one committed
-// vector over Goldilocks with Ext3 challenges:
-//   commit:  RS encode -> leaves -> Merkle root (message) -> OOD points/values
-//   prove:   constraint RLC, covector, initial sumcheck,
-//            per round: commit folded vector, PoW, open previous commitment,
+// whir.hpp:303-309 and whir_prover.hpp:56-407) over Goldilocks vectors with
+// Ext3 challenges, for nwit initial commitments of batch_size vectors each:
+//   commit:  per commitment: RS encode (batch_size * 2^k planes) -> leaves ->
+//            Merkle root (message) -> OOD points / values of its vectors
+//   prove:   OOD completion across commitments, vector + constraint RLC,
+//            covector (and the combined vector), initial sumcheck,
+//            per round: commit folded vector, PoW, open previous commitment(s),
 //                       STIR RLC + covector update, sumcheck;
 //            final vector, final PoW, final opening, final sumcheck.
 #include <algorithm>
@@ -34,55 +36,79 @@ uint32_t ilog2(uint64_t v) {
 }
 }  // namespace
 
-ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_t ds_len) {
+ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_t ds_len, uint32_t nwit) {
     ProofPlan p;
     p.sch = make_schedule(n, params);
     p.params = params;
     p.n = n;
     p.n_forms = n_forms;
     if (n_forms < 0 || n_forms > MAX_FORMS) throw std::invalid_argument("too many statement forms");
+    if (params.batch_size == 0 || nwit == 0) throw std::invalid_argument("no committed vectors");
+    if (nwit > (uint32_t)MAX_WITNESSES) throw std::invalid_argument("too many witnesses");
+    if (params.batch_size * nwit > (uint64_t)MAX_VECTORS) throw std::invalid_argument("too many committed vectors");
+    p.nwit = nwit;
+    p.nvec = (uint32_t)params.batch_size * nwit;
+    const uint32_t batch = (uint32_t)params.batch_size;
     const WhirSchedule& s = p.sch;
-    auto check_irs = [&params](const IrsSchedule& c, uint32_t ncomp) {
+    auto check_irs = [&params](const IrsSchedule& c, uint32_t row_elems, uint32_t ncomp) {
         const uint64_t N = c.codeword_length;
         if (N == 0 || (N & (N - 1))) throw std::invalid_argument("codeword length must be a power of two");
         if (ilog2(N) > TW_LOG) throw std::invalid_argument("codeword length above 2^26");
         if (c.depth > (uint64_t)MAX_DEPTH) throw std::invalid_argument("folding factor too large");
-        if (params.hash == 0 && c.depth * ncomp * 8 > 1024) throw std::invalid_argument("rows above one BLAKE3 chunk");
+        if (params.hash == 0 && (uint64_t)row_elems * ncomp * 8 > 16384)
+            throw std::invalid_argument("rows above 16 BLAKE3 chunks");
         if (c.in_domain > (uint64_t)MAX_QUERIES) throw std::invalid_argument("too many in-domain samples");
         if (c.out_domain > (uint64_t)MAX_OOD) throw std::invalid_argument("too many out-of-domain samples");
         if (N % c.message_length() != 0) throw std::invalid_argument("codeword length not a multiple of message length");
     };
-    check_irs(s.initial, 1);
-    for (const auto& r : s.rounds) check_irs(r.irs, 3);
+    check_irs(s.initial, (uint32_t)s.initial.depth * batch, 1);
+    for (const auto& r : s.rounds) check_irs(r.irs, (uint32_t)r.irs.depth, 3);
     if ((size_t)n > (size_t)MAX_SC_ROUNDS) throw std::invalid_argument("too many variables");
-    if (s.rounds.size() + 1 > (size_t)MAX_COMMITS) throw std::invalid_argument("too many rounds");
+    if (s.rounds.size() + nwit > (size_t)MAX_COMMITS) throw std::invalid_argument("too many rounds");
 
     Bump b;
     const uint64_t size = 1ull << n;
-    p.off_coeffs = b.take(size * 8);
-    p.a_plane_words = std::max<uint64_t>(size / 2, 1);
+    p.off_coeffs = b.take((size_t)p.nvec * size * 8);
+    // One vector: round 0 reads the base coefficients and the first fold
+    // writes half the size.  Several: the combined Ext3 vector is full size.
+    p.a_plane_words = p.nvec > 1 ? size : std::max<uint64_t>(size / 2, 1);
     p.off_a = b.take(3 * p.a_plane_words * 8);
     p.cov_plane_words = size;
     p.off_cov = b.take(3 * size * 8);
     size_t tmp_words = 0;
-    auto add_commit = [&](const IrsSchedule& c, uint32_t ncomp) {
+    auto commit_of = [&](const IrsSchedule& c, uint32_t row_elems, uint32_t ncomp) {
         CommitBuffers cb;
         cb.N = c.codeword_length;
         cb.logN = ilog2(cb.N);
-        cb.depth = (uint32_t)c.depth;
+        cb.depth = row_elems;
         cb.ncomp = ncomp;
-        const size_t words = (size_t)cb.N * cb.depth * ncomp;
-        cb.planes = b.take(words * 8);
-        cb.nodes = b.take((2 * cb.N - 1) * 32);
-        tmp_words = std::max(tmp_words, words);
-        p.commits.push_back(cb);
+        tmp_words = std::max(tmp_words, (size_t)cb.N * cb.depth * ncomp);
+        return cb;
     };
-    add_commit(s.initial, 1);
-    for (const auto& r : s.rounds) add_commit(r.irs, 3);
+    {  // initial commitments: planes side by side, then node arrays side by side
+        CommitBuffers cb = commit_of(s.initial, (uint32_t)s.initial.depth * batch, 1);
+        p.init_planes_stride = align_up((size_t)cb.N * cb.depth * 8, 256);
+        p.init_nodes_stride = align_up((2 * cb.N - 1) * 32, 256);
+        const size_t planes0 = b.take(p.init_planes_stride * nwit);
+        const size_t nodes0 = b.take(p.init_nodes_stride * nwit);
+        for (uint32_t w = 0; w < nwit; ++w) {
+            cb.planes = planes0 + w * p.init_planes_stride;
+            cb.nodes = nodes0 + w * p.init_nodes_stride;
+            p.commits.push_back(cb);
+        }
+    }
+    for (const auto& r : s.rounds) {
+        CommitBuffers cb = commit_of(r.irs, (uint32_t)r.irs.depth, 3);
+        cb.planes = b.take((size_t)cb.N * cb.depth * 3 * 8);
+        cb.nodes = b.take((2 * cb.N - 1) * 32);
+        p.commits.push_back(cb);
+    }
     p.off_tmp = b.take(tmp_words * 8);
     p.off_sc_scratch = b.take(sumcheck_scratch_bytes());
-    p.off_ood_scratch = b.take(ood_scratch_bytes(1ull << n));
-    size_t cov_scratch = cov_init_scratch_bytes(n, n_forms, (int)s.initial.out_domain);
+    p.ood_values = std::max<uint32_t>((uint32_t)s.initial.out_domain * p.nvec, (uint32_t)MAX_OOD);
+    p.off_ood_scratch = b.take(ood_scratch_bytes(1ull << n, p.ood_values));
+    const int init_ood = (int)(s.initial.out_domain * nwit);
+    size_t cov_scratch = cov_init_scratch_bytes(n, n_forms, init_ood);
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;
         const int npts = (int)(s.rounds[r].irs.out_domain + prev.in_domain);
@@ -94,26 +120,27 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
 
     // Proof stream sizes.
     size_t narg = 0, hints = 0;
-    auto commit_narg = [](const IrsSchedule& c) { return 32 + 24 * c.out_domain; };
+    auto commit_narg = [](const IrsSchedule& c, uint64_t vectors) { return 32 + 24 * c.out_domain * vectors; };
     auto pow_narg = [](uint64_t thr) { return thr == ~0ull ? 0 : 8; };
     auto sumcheck_narg = [&](const SumcheckSchedule& sc) { return sc.num_rounds * (48 + pow_narg(sc.pow_threshold)); };
-    auto open_hints = [](const IrsSchedule& c, uint32_t ncomp) {
+    auto open_hints = [](const IrsSchedule& c, uint64_t vectors, uint32_t ncomp, uint64_t commitments) {
         const uint64_t logN = ilog2(c.codeword_length);
         const uint64_t merkle = std::min<uint64_t>(c.in_domain * logN, c.codeword_length);
-        return 8 + c.in_domain * c.depth * 8 * ncomp + 32 * merkle;
+        return commitments * (8 + c.in_domain * c.depth * vectors * 8 * ncomp + 32 * merkle);
     };
-    narg += commit_narg(s.initial);
+    narg += nwit * commit_narg(s.initial, batch);
+    narg += 24 * s.initial.out_domain * nwit * (p.nvec - batch);  // OOD completion
     const bool has_constraints = n_forms + s.initial.out_domain > 0;
     if (has_constraints) narg += sumcheck_narg(s.initial_sumcheck);
     else narg += pow_narg(s.initial_skip_pow);
     size_t sc_rounds = s.initial_sumcheck.num_rounds;
     for (size_t r = 0; r < s.rounds.size(); ++r) {
-        narg += commit_narg(s.rounds[r].irs) + pow_narg(s.rounds[r].pow_threshold) + sumcheck_narg(s.rounds[r].sumcheck);
-        hints += r == 0 ? open_hints(s.initial, 1) : open_hints(s.rounds[r - 1].irs, 3);
+        narg += commit_narg(s.rounds[r].irs, 1) + pow_narg(s.rounds[r].pow_threshold) + sumcheck_narg(s.rounds[r].sumcheck);
+        hints += r == 0 ? open_hints(s.initial, batch, 1, nwit) : open_hints(s.rounds[r - 1].irs, 1, 3, 1);
         sc_rounds += s.rounds[r].sumcheck.num_rounds;
     }
     narg += 24 * s.final_sumcheck.initial_size + pow_narg(s.final_pow) + sumcheck_narg(s.final_sumcheck);
-    hints += s.rounds.empty() ? open_hints(s.initial, 1) : open_hints(s.rounds.back().irs, 3);
+    hints += s.rounds.empty() ? open_hints(s.initial, batch, 1, nwit) : open_hints(s.rounds.back().irs, 1, 3, 1);
     sc_rounds += s.final_sumcheck.num_rounds;
     p.narg_len = narg;
     p.hints_cap = hints;
@@ -160,13 +187,16 @@ struct Ctx {
         if (_rc != 0) return _rc;                          \
     } while (0)
 
-// RS encode + leaves + Merkle + OOD of commitment `ci` whose message is the
-// vector (src planes, vsize words each).
-int commit_vector(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t ncomp, uint64_t vsize, int n_ood) {
+// RS encode + leaves + Merkle of commitment `ci` whose message is `vectors`
+// vectors (src planes, vsize words each, consecutive), then the OOD values of
+// those vectors at the commitment's points, stored at out[j * out_stride + v].
+int commit_vectors(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t ncomp, uint64_t vsize,
+                   uint32_t vectors, int n_ood, E3* out, uint32_t out_stride) {
     const CommitBuffers& cb = c.p.commits[ci];
+    const uint32_t fold_depth = cb.depth / vectors;
     LdeArgs L{};
     for (int k = 0; k < 3; ++k) L.src[k] = src[k] ? src[k] : src[0];
-    L.m = vsize / cb.depth;
+    L.m = vsize / fold_depth;
     L.depth = cb.depth;
     L.planes = cb.depth * ncomp;
     L.logN = cb.logN;
@@ -179,8 +209,20 @@ int commit_vector(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t n
     uint32_t* nodes = reinterpret_cast<uint32_t*>(c.ws + cb.nodes);
     WG_TIMED(c, FAM_LEAF, launch_leaves(c.w(cb.planes), cb.N, cb.depth, ncomp, nodes, c.p.params.hash, c.st));
     WG_TIMED(c, FAM_MERKLE, launch_merkle(nodes, cb.logN, c.tx(), c.sc(), ci, n_ood, c.p.params.hash, c.st));
-    WG_TIMED(c, FAM_OOD, launch_ood(src[0], src[1], src[2], ncomp == 3, vsize, c.tx(), c.sc(), ci, n_ood,
-                                    c.ws + c.p.off_ood_scratch, c.st));
+    OodArgs o{};
+    for (int k = 0; k < 3; ++k) o.v[k] = src[k] ? src[k] : src[0];
+    o.ext3 = ncomp == 3;
+    o.size = vsize;
+    o.nvec = vectors;
+    o.vec_stride = vsize;
+    o.pts = &c.sc()->ood_pts[ci][0];
+    o.n_ood = n_ood;
+    o.out = out;
+    o.out_stride = out_stride;
+    o.tx = c.tx();
+    o.scratch = c.ws + c.p.off_ood_scratch;
+    o.scratch_values = c.p.ood_values;
+    WG_TIMED(c, FAM_OOD, launch_ood(o, c.st));
     return 0;
 }
 
@@ -244,29 +286,61 @@ int enqueue_commit(const ProofPlan& p, char* ws, uint32_t ds_len, const DeviceTa
     WG_TIMED(c, FAM_TX, launch_tx_init(c.tx(), reinterpret_cast<const unsigned char*>(ws + p.off_ds), ds_len,
                           reinterpret_cast<unsigned char*>(ws + p.off_narg), p.narg_len + 64,
                           reinterpret_cast<unsigned char*>(ws + p.off_hints), p.hints_cap + 64, c.sc(), st));
-    const uint64_t* src[3] = {c.w(p.off_coeffs), nullptr, nullptr};
-    return commit_vector(c, 0, src, 1, 1ull << p.n, (int)p.sch.initial.out_domain);
+    const uint64_t size = 1ull << p.n;
+    const uint32_t batch = (uint32_t)p.params.batch_size;
+    const int ood = (int)p.sch.initial.out_domain;
+    for (uint32_t w = 0; w < p.nwit; ++w) {
+        const uint64_t* src[3] = {c.w(p.off_coeffs) + (size_t)w * batch * size, nullptr, nullptr};
+        E3* out = &c.sc()->init_ood_mat[(size_t)w * ood * p.nvec + (size_t)w * batch];
+        WG_TRY(commit_vectors(c, (int)w, src, 1, size, batch, ood, out, p.nvec));
+    }
+    return 0;
 }
 
 int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStream_t st, Timer* timer) {
     Ctx c{p, ws, tw, st, timer};
     const WhirSchedule& s = p.sch;
     const int ood0 = (int)s.initial.out_domain;
-    WG_TIMED(c, FAM_TX, launch_constraint_rlc(c.tx(), c.sc(), p.n_forms, ood0, st));
+    const uint32_t W = p.nwit, V = p.nvec, batch = (uint32_t)p.params.batch_size;
+    const uint64_t size0 = 1ull << p.n;
+    // OOD completion (whir_prover.hpp:92-120): the other commitments' vectors
+    // at each commitment's points, sent in order.
+    if (W > 1 && ood0 > 0) {
+        for (uint32_t w = 0; w < W; ++w) {
+            OodArgs o{};
+            o.v[0] = o.v[1] = o.v[2] = c.w(p.off_coeffs);
+            o.ext3 = 0;
+            o.size = size0;
+            o.nvec = V;
+            o.vec_stride = size0;
+            o.skip_lo = w * batch;
+            o.skip_hi = (w + 1) * batch;
+            o.pts = &c.sc()->ood_pts[w][0];
+            o.n_ood = ood0;
+            o.out = &c.sc()->init_ood_mat[(size_t)w * ood0 * V];
+            o.out_stride = V;
+            o.tx = c.tx();
+            o.scratch = ws + p.off_ood_scratch;
+            o.scratch_values = p.ood_values;
+            WG_TIMED(c, FAM_OOD, launch_ood(o, st));
+        }
+    }
+    WG_TIMED(c, FAM_TX, launch_constraint_rlc(c.tx(), c.sc(), p.n_forms, (int)W, ood0, (int)V, st));
     const bool has_constraints = p.n_forms + ood0 > 0;
     int r_slot = 0;
-    const uint64_t size0 = 1ull << p.n;
     if (has_constraints) {
         CovInitArgs ci{};
-        for (int k = 0; k < 3; ++k) ci.cov[k] = c.cov(k);
+        for (int k = 0; k < 3; ++k) { ci.cov[k] = c.cov(k); ci.vec_out[k] = c.a(k); }
         ci.logS = p.n;
         ci.points = c.w(p.off_points);
         ci.n_forms = p.n_forms;
-        ci.n_ood = ood0;
+        ci.n_ood = ood0 * (int)W;
         ci.sc = c.sc();
         ci.scratch = ws + p.off_cov_scratch;
+        ci.nvec = V;
+        ci.vecs = c.w(p.off_coeffs);
         WG_TIMED(c, FAM_COV, launch_cov_init(ci, st));
-        WG_TRY(sumcheck(c, s.initial_sumcheck, size0, true, r_slot, true));
+        WG_TRY(sumcheck(c, s.initial_sumcheck, size0, V == 1, r_slot, true));
     } else {
         return -2;  // statement-free proofs (unique decoding, no forms) are not on this path
     }
@@ -274,18 +348,21 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
     uint64_t vsize = size0 >> s.initial_sumcheck.num_rounds;
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         const RoundSchedule& rc = s.rounds[r];
-        const int ci = (int)r + 1;
+        const int ci = (int)(W + r);
         const uint64_t* src[3] = {c.a(0), c.a(1), c.a(2)};
-        WG_TRY(commit_vector(c, ci, src, 3, vsize, (int)rc.irs.out_domain));
+        WG_TRY(commit_vectors(c, ci, src, 3, vsize, 1, (int)rc.irs.out_domain, &c.sc()->ood_vals[ci][0], 1));
         WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), rc.pow_threshold, ci, c.p.params.hash, st));
-        // open the previous commitment
+        // open the previous commitment (the first round: every initial commitment)
         const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;
-        const CommitBuffers& pb = p.commits[ci - 1];
+        const CommitBuffers& pb = p.commits[r == 0 ? 0 : ci - 1];
         OpenArgs oa{};
         oa.tx = c.tx();
         oa.sc = c.sc();
         oa.planes = c.w(pb.planes);
         oa.nodes = reinterpret_cast<const uint32_t*>(ws + pb.nodes);
+        oa.nwit = r == 0 ? W : 1;
+        oa.planes_stride = r == 0 ? p.init_planes_stride / 8 : 0;
+        oa.nodes_stride = r == 0 ? p.init_nodes_stride / 4 : 0;
         oa.N = pb.N;
         oa.logN = pb.logN;
         oa.depth = pb.depth;
@@ -293,6 +370,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         oa.q = (uint32_t)prev.in_domain;
         oa.gen = gl_pow_host(7, (GL_P - 1) / pb.N);  // w_N = 7^((p-1)/N)
         oa.stir = 1;
+        oa.use_vrlc = r == 0 && V > 1;
         oa.ood_offset = (int)rc.irs.out_domain;
         const uint32_t prev_fold = (uint32_t)(r == 0 ? s.initial_sumcheck.num_rounds : s.rounds[r - 1].sumcheck.num_rounds);
         oa.fold = prev_fold;
@@ -313,15 +391,19 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
 
     // final vector, PoW, opening, sumcheck
     WG_TIMED(c, FAM_TX, launch_send_vector(c.tx(), c.a(0), c.a(1), c.a(2), vsize, st));
-    WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), s.final_pow, (int)s.rounds.size() + 1, c.p.params.hash, st));
+    WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), s.final_pow, (int)(W + s.rounds.size()), c.p.params.hash, st));
     {
-        const IrsSchedule& last = s.rounds.empty() ? s.initial : s.rounds.back().irs;
-        const CommitBuffers& lb = p.commits.back();
+        const bool initial = s.rounds.empty();
+        const IrsSchedule& last = initial ? s.initial : s.rounds.back().irs;
+        const CommitBuffers& lb = initial ? p.commits[0] : p.commits.back();
         OpenArgs oa{};
         oa.tx = c.tx();
         oa.sc = c.sc();
         oa.planes = c.w(lb.planes);
         oa.nodes = reinterpret_cast<const uint32_t*>(ws + lb.nodes);
+        oa.nwit = initial ? W : 1;
+        oa.planes_stride = initial ? p.init_planes_stride / 8 : 0;
+        oa.nodes_stride = initial ? p.init_nodes_stride / 4 : 0;
         oa.N = lb.N;
         oa.logN = lb.logN;
         oa.depth = lb.depth;

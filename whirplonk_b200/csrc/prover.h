@@ -30,12 +30,16 @@ struct ProofPlan {
     ProtocolParams params;
     uint32_t n = 0;          // num_variables
     int n_forms = 0;
+    uint32_t nwit = 1;       // initial commitments (witnesses), each of params.batch_size vectors
+    uint32_t nvec = 1;       // committed vectors: nwit * batch_size
+    size_t init_planes_stride = 0, init_nodes_stride = 0;  // bytes between the initial commitments' buffers
     // byte offsets in the workspace
     size_t off_coeffs = 0, off_a = 0, off_cov = 0, off_tmp = 0;
     size_t off_sc_scratch = 0, off_ood_scratch = 0, off_cov_scratch = 0;
     size_t off_tx = 0, off_scalars = 0, off_narg = 0, off_hints = 0, off_ds = 0, off_points = 0;
-    std::vector<CommitBuffers> commits;  // [initial, round 0, round 1, ...]
+    std::vector<CommitBuffers> commits;  // [initial 0 .. initial nwit-1, round 0, round 1, ...]
     size_t a_plane_words = 0, cov_plane_words = 0;
+    uint32_t ood_values = 0;   // OOD scratch capacity in values (points x vectors)
     size_t narg_len = 0;       // exact narg length (every message has a fixed size)
     size_t hints_cap = 0;      // upper bound of the hint stream
     size_t ds_cap = 0;
@@ -43,8 +47,10 @@ struct ProofPlan {
     size_t total_sumcheck_rounds = 0;
 };
 
-// Throws std::invalid_argument on unsupported parameters.
-ProofPlan make_plan(uint32_t num_variables, const ProtocolParams& p, int n_forms, size_t ds_len);
+// Throws std::invalid_argument on unsupported parameters.  The plan covers
+// num_witnesses initial commitments of p.batch_size vectors each.
+ProofPlan make_plan(uint32_t num_variables, const ProtocolParams& p, int n_forms, size_t ds_len,
+                    uint32_t num_witnesses = 1);
 
 struct DeviceTables {
     uint64_t* tw_stage = nullptr;
@@ -52,13 +58,15 @@ struct DeviceTables {
     uint64_t* tw_lo = nullptr;
 };
 
-// Enqueue the whole commit (Config::commit) on `st`.  The workspace must hold
-// the coefficients at off_coeffs and the domain-separator bytes at off_ds.
+// Enqueue the whole commit (Config::commit, once per initial commitment) on
+// `st`.  The workspace must hold the nvec coefficient vectors at off_coeffs and
+// the domain-separator bytes at off_ds.
 struct Timer;
 int enqueue_commit(const ProofPlan& p, char* ws, uint32_t ds_len, const DeviceTables& tw, cudaStream_t st,
                    Timer* timer = nullptr);
 // Enqueue Config::prove for MLE-point statements (points at off_points,
-// claimed evaluations already in ProofScalars::forms_eval).
+// claimed evaluations already in ProofScalars::forms_eval, form-major over
+// the nvec vectors).
 int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStream_t st, Timer* timer = nullptr);
 
 TxState* plan_tx(const ProofPlan& p, char* ws);

@@ -15,17 +15,25 @@ constexpr int MAX_OOD = 8;          // out-of-domain samples per commitment
 constexpr int MAX_FORMS = 8;        // statement linear forms
 constexpr int MAX_QUERIES = 1024;   // in-domain samples per opening
 constexpr int MAX_SC_ROUNDS = 64;   // total sumcheck rounds (= num_variables)
-constexpr int MAX_COMMITS = 24;     // initial + round commitments
+constexpr int MAX_WITNESSES = 8;    // initial commitments proven together
+constexpr int MAX_VECTORS = 32;     // committed vectors over all initial commitments
+constexpr int MAX_COMMITS = 32;     // initial + round commitments
 constexpr int MAX_DEPTH = 64;       // interleaving depth 2^k
+constexpr int MAX_INIT_OOD = MAX_WITNESSES * MAX_OOD;
 
 struct ProofScalars {
     E3 sum;                                  // claimed <vector, covector>
     E3 c0, c2;                               // current sumcheck round polynomial
     E3 sc_r[MAX_SC_ROUNDS];                  // folding randomness, in order (= evaluation point)
-    E3 ood_pts[MAX_COMMITS][MAX_OOD];
-    E3 ood_vals[MAX_COMMITS][MAX_OOD];
-    E3 crlc[MAX_FORMS + MAX_OOD];            // constraint RLC coefficients
-    E3 forms_eval[MAX_FORMS];                // claimed evaluations (input)
+    E3 ood_pts[MAX_COMMITS][MAX_OOD];        // commitment c's OOD points (initial commitments first)
+    E3 ood_vals[MAX_COMMITS][MAX_OOD];       // round commitments' OOD values
+    // The initial commitments' OOD points in order, and the values of every
+    // committed vector at each of them: init_ood_mat[i * V + v].
+    E3 init_ood_pts[MAX_INIT_OOD];
+    E3 init_ood_mat[MAX_INIT_OOD * MAX_VECTORS];
+    E3 vrlc[MAX_VECTORS];                    // vector RLC coefficients
+    E3 crlc[MAX_FORMS + MAX_INIT_OOD];       // constraint RLC coefficients
+    E3 forms_eval[MAX_FORMS * MAX_VECTORS];  // claimed evaluations (input), form-major [f * V + v]
     E3 stir_rlc[MAX_QUERIES + MAX_OOD];      // STIR combination coefficients of the current round
     E3 stir_pts[MAX_QUERIES + MAX_OOD];      // OOD points then in-domain points (base, lifted)
     E3 stir_vals[MAX_QUERIES + MAX_OOD];

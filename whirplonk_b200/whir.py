@@ -6,8 +6,8 @@ Names and call order follow the reference C++ API so a caller of
     params = ProtocolParameters(security_level=100, pow_bits=20, ...)
     config = Config.from_params(1 << n, params)            # whir.hpp:118
     ps = ProverState.from_ds(cli_domain_separator(params))  # transcript.hpp:605
-    witness = config.commit(ps, vector)                     # whir.hpp:303
-    claim = config.prove(ps, vector, [witness],
+    witness = config.commit(ps, vectors)                    # whir.hpp:303 (batch_size vectors)
+    claim = config.prove(ps, vectors, [witness],
                          [MultilinearExtension(point)], [evaluation])  # whir_prover.hpp:56
     narg, hints = ps.proof()                                # transcript.hpp:653
 
@@ -198,10 +198,17 @@ class FinalClaim:
 
 
 class Witness:
-    def __init__(self, handle, ctx: Context, vector_ptr_keepalive=None):
+    """Committed matrix (or matrices) in HBM.  One handle may stand for several
+    consecutive commitments (``Config.commit_witnesses``); ``num_vectors`` is
+    the number of vectors they hold together."""
+
+    def __init__(self, handle, ctx: Context, vector_ptr_keepalive=None, num_vectors: int = 1,
+                 num_witnesses: int = 1):
         self.handle = handle
         self.ctx = ctx
         self._keep = vector_ptr_keepalive
+        self.num_vectors = num_vectors
+        self.num_witnesses = num_witnesses
 
     def __del__(self):
         try:
@@ -245,32 +252,47 @@ class Config:
     def n_rounds(self) -> int:
         return self.schedule[0]
 
-    def commit(self, prover_state: ProverState, vector, on_device_ptr: Optional[int] = None) -> Witness:
+    def commit(self, prover_state: ProverState, vectors, on_device_ptr: Optional[int] = None) -> Witness:
+        """irs_commit::Config::commit of params.batch_size vectors (a 1-D array
+        when batch_size is 1, else batch_size rows)."""
+        return self.commit_witnesses(prover_state, vectors, 1, on_device_ptr)
+
+    def commit_witnesses(self, prover_state: ProverState, vectors, num_witnesses: int,
+                         on_device_ptr: Optional[int] = None) -> Witness:
+        """num_witnesses commits in a row on one transcript; ``vectors`` holds
+        num_witnesses * batch_size rows, witness 0's first."""
         ctx = prover_state.ctx
         c = self.params.to_c()
         h = ctypes.c_void_p()
+        nvec = self.params.batch_size * num_witnesses
         if on_device_ptr is not None:
             ptr, where, keep = on_device_ptr, 1, None
         else:
-            keep = np.ascontiguousarray(vector, dtype=np.uint64)
-            if keep.size != self.size:
-                raise ValueError("vector length != config size")
+            keep = np.ascontiguousarray(vectors, dtype=np.uint64)
+            if keep.size != self.size * nvec:
+                raise ValueError("vectors != batch_size * num_witnesses vectors of the config size")
             ptr, where = keep.ctypes.data, 0
-        _lib.check(ctx._L.whirgpu_commit(ctx.handle, ctypes.byref(c), ptr, self.num_variables, where,
-                                         prover_state.handle, ctypes.byref(h)), ctx.handle)
-        return Witness(h.value, ctx, keep)
+        _lib.check(ctx._L.whirgpu_commit_witnesses(ctx.handle, ctypes.byref(c), ptr, num_witnesses,
+                                                   self.num_variables, where, prover_state.handle, ctypes.byref(h)),
+                   ctx.handle)
+        return Witness(h.value, ctx, keep, nvec, num_witnesses)
 
-    def prove(self, prover_state: ProverState, vector, witnesses: Sequence[Witness], linear_forms: Sequence,
+    def prove(self, prover_state: ProverState, vectors, witnesses: Sequence[Witness], linear_forms: Sequence,
               evaluations: Sequence) -> FinalClaim:
+        """Config::prove; ``evaluations`` holds len(linear_forms) * num_vectors
+        Ext3 values, form-major (whir_prover.hpp:77)."""
         ctx = prover_state.ctx
         if len(witnesses) != 1:
-            raise ValueError("one committed vector per proof on this path")
+            raise ValueError("pass the one handle of commit / commit_witnesses")
+        nvec = witnesses[0].num_vectors
         n = self.num_variables
         pts = np.zeros((max(len(linear_forms), 1), n, 3), dtype=np.uint64)
         for i, lf in enumerate(linear_forms):
             if not isinstance(lf, MultilinearExtension):
                 raise TypeError("only MultilinearExtension statements are on this path")
             pts[i] = np.asarray(lf.point, dtype=np.uint64).reshape(n, 3)
+        if len(evaluations) != len(linear_forms) * nvec:
+            raise ValueError("evaluations != linear forms * committed vectors")
         ev = np.zeros((max(len(evaluations), 1), 3), dtype=np.uint64)
         for i, e in enumerate(evaluations):
             ev[i] = np.asarray(e, dtype=np.uint64).reshape(3)
@@ -284,13 +306,15 @@ class Config:
 
 
 def prove_once(n: int, params: ProtocolParameters, coeffs, points, evaluations, ctx: Optional[Context] = None,
-               ds: Optional[DomainSeparator] = None, on_device_ptr: Optional[int] = None):
-    """commit + prove of one vector with the CLI domain separator; returns (narg, hints, claim)."""
+               ds: Optional[DomainSeparator] = None, on_device_ptr: Optional[int] = None, num_witnesses: int = 1):
+    """commit (num_witnesses witnesses of params.batch_size vectors) + prove with
+    the CLI domain separator; returns (narg, hints, claim).  ``evaluations``
+    holds num_points * num_vectors Ext3 values, form-major."""
     ctx = ctx or default_context()
     ds = ds or cli_domain_separator(params)
     config = Config.from_params(1 << n, params)
     ps = ProverState.from_ds(ds, b"", ctx)
-    w = config.commit(ps, coeffs, on_device_ptr=on_device_ptr)
+    w = config.commit_witnesses(ps, coeffs, num_witnesses, on_device_ptr=on_device_ptr)
     pts = np.asarray(points, dtype=np.uint64).reshape(-1, n, 3)
     forms = [MultilinearExtension(pts[i]) for i in range(pts.shape[0])]
     claim = config.prove(ps, coeffs, [w], forms, [tuple(e) for e in np.asarray(evaluations).reshape(-1, 3)])
