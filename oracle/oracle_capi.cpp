@@ -183,6 +183,43 @@ int oracle_whir_prove(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique, cons
     }
 }
 
+// Commit + prove with a statement of mixed forms: kinds[f] = 0 MultilinearExtension
+// (n Ext3 coordinates), 1 dense Covector (2^n Ext3 values); form_data holds the
+// forms' words back to back in form order.  evals: nforms * V values, form-major.
+int oracle_whir_prove_forms(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique, u64 batch_size, u64 num_witnesses,
+                            const u64* coeffs, const int* kinds, size_t nforms, const u64* form_data, const u64* evals,
+                            u8* narg, size_t narg_cap, u8* hints, size_t hints_cap, u64* lens, int sha2) {
+    try {
+        Params p = make_params(rho, k, sec, powb, unique);
+        p.batch_size = batch_size;
+        if (sha2) std::memcpy(p.hash_id, SHA2_ENGINE_ID, 32);
+        const u64 V = batch_size * num_witnesses, size = 1ull << n;
+        std::vector<std::vector<u64>> vs(V);
+        for (u64 j = 0; j < V; ++j) vs[j].assign(coeffs + j * size, coeffs + (j + 1) * size);
+        Statement st;
+        const u64* d = form_data;
+        for (size_t f = 0; f < nforms; ++f) {
+            if (kinds[f] == 0) {
+                st.mle_points.push_back(read_e3(d, n));
+                d += 3 * n;
+            } else {
+                st.covectors.push_back(read_e3(d, size));
+                d += 3 * size;
+            }
+            st.dense.push_back(kinds[f] != 0);
+        }
+        st.evaluations = read_e3(evals, nforms * V);
+        ProofOut o = prove_multi(p, vs, num_witnesses, st, cli_domain_separator(p));
+        lens[0] = o.narg.size();
+        lens[1] = o.hints.size();
+        std::memcpy(narg, o.narg.data(), std::min(narg_cap, o.narg.size()));
+        std::memcpy(hints, o.hints.data(), std::min(hints_cap, o.hints.size()));
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
 // Commit of num_witnesses witnesses of batch_size vectors each, then one
 // prove over all of them.  coeffs: num_witnesses * batch_size vectors of 2^n
 // words, back to back; evals: npoints * num_vectors Ext3 values, form-major.

@@ -15,11 +15,13 @@
 // (cpp/main.cpp:203-215), re-stated here because main.cpp is not a header.
 //
 // Input file (little endian), written by oracle/refio.py:
-//   u32 magic 0x49524857 ('WHRI'), u32 version 1 or 2
+//   u32 magic 0x49524857 ('WHRI'), u32 version 1, 2 or 3
 //   u64 num_variables, folding_factor, starting_log_inv_rate,
-//       security_level, pow_bits, num_points
-//   version 2 only: u64 batch_size, num_witnesses (version 1: both 1)
-//   num_points * num_variables * 3 u64   MLE points (Ext3 coords)
+//       security_level, pow_bits, num_points (= number of linear forms)
+//   versions 2, 3: u64 batch_size, num_witnesses (version 1: both 1)
+//   versions 1, 2: num_points * num_variables * 3 u64   MLE points (Ext3 coords)
+//   version 3: per form u64 kind, then kind 0: num_variables * 3 u64 (an MLE
+//              point), kind 1: 2^num_variables * 3 u64 (a dense Covector)
 //   V * 2^num_variables u64              coefficients of the V = batch_size *
 //                                        num_witnesses vectors (canonical, < p)
 // The V vectors are committed as num_witnesses witnesses of batch_size
@@ -148,26 +150,39 @@ int main(int argc, char** argv) {
     Reader rd{buf};
     if (rd.u32() != 0x49524857u) die("bad magic");
     const std::uint32_t version = rd.u32();
-    if (version != 1u && version != 2u) die("bad version");
+    if (version < 1u || version > 3u) die("bad version");
     const std::size_t n = rd.u64();
     const std::size_t k = rd.u64();
     const std::size_t rho = rd.u64();
     const std::size_t sec = rd.u64();
     const std::size_t powb = rd.u64();
     const std::size_t npts = rd.u64();
-    const std::size_t batch = version == 2u ? rd.u64() : 1;
-    const std::size_t nwit = version == 2u ? rd.u64() : 1;
+    const std::size_t batch = version >= 2u ? rd.u64() : 1;
+    const std::size_t nwit = version >= 2u ? rd.u64() : 1;
     if (n >= 40) die("num_variables too large");
     if (batch == 0 || nwit == 0 || batch * nwit > 64) die("bad vector count");
     const std::size_t nvec = batch * nwit;
 
-    std::vector<std::vector<Target>> points(npts, std::vector<Target>(n));
-    for (auto& pt : points)
-        for (auto& c : pt) {
-            auto a = rd.u64(), b = rd.u64(), d = rd.u64();
-            c = Target(Source::from_u64(a), Source::from_u64(b), Source::from_u64(d));
-        }
     const std::size_t size = std::size_t{1} << n;
+    auto read_target = [&rd]() {
+        auto a = rd.u64(), b = rd.u64(), d = rd.u64();
+        return Target(Source::from_u64(a), Source::from_u64(b), Source::from_u64(d));
+    };
+    std::vector<bool> dense(npts, false);
+    std::vector<std::vector<Target>> points(npts);  // MLE point, or the covector's values
+    for (std::size_t f = 0; f < npts; ++f) {
+        if (version == 3u) {
+            const std::uint64_t kind = rd.u64();
+            if (kind > 1) die("bad form kind");
+            dense[f] = kind == 1;
+        }
+        points[f].resize(dense[f] ? size : n);
+        for (auto& c : points[f]) c = read_target();
+    }
+    auto make_form = [&](std::size_t f) -> std::unique_ptr<::whir::algebra::LinearForm<Target>> {
+        if (dense[f]) return std::make_unique<::whir::algebra::Covector<Target>>(points[f]);
+        return std::make_unique<::whir::algebra::MultilinearExtension<Target>>(points[f]);
+    };
     std::vector<std::vector<Source>> vecs(nvec, std::vector<Source>(size));
     for (auto& vec : vecs)
         for (auto& v : vec) v = Source::from_u64(rd.u64());
@@ -206,9 +221,16 @@ int main(int argc, char** argv) {
 
     M emb{};
     std::vector<Target> evaluations;  // form-major, as Config::prove expects (whir_prover.hpp:77)
-    for (const auto& pt : points) {
-        ::whir::algebra::MultilinearExtension<Target> lf(pt);
-        for (const auto& vec : vecs) evaluations.push_back(lf.template evaluate<M>(emb, std::span<const Source>{vec}));
+    for (std::size_t f = 0; f < npts; ++f) {
+        for (const auto& vec : vecs) {
+            if (dense[f]) {
+                ::whir::algebra::Covector<Target> cv(points[f]);
+                evaluations.push_back(cv.template evaluate<M>(emb, std::span<const Source>{vec}));
+            } else {
+                ::whir::algebra::MultilinearExtension<Target> lf(points[f]);
+                evaluations.push_back(lf.template evaluate<M>(emb, std::span<const Source>{vec}));
+            }
+        }
     }
     auto ds = cli_domain_separator(params);
     ::whir::transcript::Empty instance;
@@ -219,8 +241,7 @@ int main(int argc, char** argv) {
     double commit_ms = 0, prove_ms = 0;
     for (int rep = 0; rep < reps; ++rep) {
         std::vector<std::unique_ptr<::whir::algebra::LinearForm<Target>>> forms;
-        for (const auto& pt : points)
-            forms.push_back(std::make_unique<::whir::algebra::MultilinearExtension<Target>>(pt));
+        for (std::size_t f = 0; f < npts; ++f) forms.push_back(make_form(f));
         auto ps = ::whir::transcript::ProverState::from_ds(ds, instance);
         auto t0 = Clock::now();
         std::vector<::whir::protocols::irs_commit::Witness<Source, Target>> wits;
@@ -249,8 +270,8 @@ int main(int argc, char** argv) {
         auto claim = config.verify(vs, cp, std::span<const Target>{evaluations});
         std::vector<std::unique_ptr<::whir::algebra::LinearForm<Target>>> vforms;
         std::vector<const ::whir::algebra::LinearForm<Target>*> refs;
-        for (const auto& pt : points) {
-            vforms.push_back(std::make_unique<::whir::algebra::MultilinearExtension<Target>>(pt));
+        for (std::size_t f = 0; f < npts; ++f) {
+            vforms.push_back(make_form(f));
             refs.push_back(vforms.back().get());
         }
         verify_ok = (claim.verify(refs) && vs.check_eof()) ? 1.0 : 0.0;

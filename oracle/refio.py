@@ -30,20 +30,32 @@ class RefProof:
     verify_ok: float  # 1.0 accepted, 0.0 rejected, -1.0 not run
 
 
-def write_input(path, n, k, rho, sec, pow_bits, points, coeffs, batch_size=1, num_witnesses=1):
+def write_input(path, n, k, rho, sec, pow_bits, points, coeffs, batch_size=1, num_witnesses=1, forms=None):
     """Input file of ref_driver.cpp (format documented there).  ``coeffs`` holds
-    batch_size * num_witnesses vectors of 2^n words back to back."""
-    points = np.ascontiguousarray(points, dtype=np.uint64).reshape(-1, n, 3)
+    batch_size * num_witnesses vectors of 2^n words back to back.  ``forms``
+    (optional) replaces ``points``: a list of ("mle", (n, 3) array) or
+    ("covector", (2^n, 3) array) linear forms in statement order."""
     coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
     nvec = batch_size * num_witnesses
     assert coeffs.size == nvec << n
     multi = nvec != 1
     with open(path, "wb") as f:
-        f.write(struct.pack("<II", 0x49524857, 2 if multi else 1))
-        f.write(struct.pack("<6Q", n, k, rho, sec, pow_bits, points.shape[0]))
-        if multi:
+        if forms is not None:
+            f.write(struct.pack("<II", 0x49524857, 3))
+            f.write(struct.pack("<6Q", n, k, rho, sec, pow_bits, len(forms)))
             f.write(struct.pack("<2Q", batch_size, num_witnesses))
-        f.write(points.tobytes())
+            for kind, data in forms:
+                data = np.ascontiguousarray(data, dtype=np.uint64)
+                assert data.size == 3 * (n if kind == "mle" else 1 << n)
+                f.write(struct.pack("<Q", 0 if kind == "mle" else 1))
+                f.write(data.tobytes())
+        else:
+            points = np.ascontiguousarray(points, dtype=np.uint64).reshape(-1, n, 3)
+            f.write(struct.pack("<II", 0x49524857, 2 if multi else 1))
+            f.write(struct.pack("<6Q", n, k, rho, sec, pow_bits, points.shape[0]))
+            if multi:
+                f.write(struct.pack("<2Q", batch_size, num_witnesses))
+            f.write(points.tobytes())
         f.write(coeffs.tobytes())
 
 
@@ -67,18 +79,19 @@ def ref_available() -> bool:
 
 
 def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1, threads=None,
-                  timeout=3600, sha2=False, batch_size=1, num_witnesses=1) -> RefProof:
+                  timeout=3600, sha2=False, batch_size=1, num_witnesses=1, forms=None) -> RefProof:
     """Runs the unmodified reference prover (compiled in place by oracle/Makefile).
-    With several vectors the evaluations come back form-major, (num_points * V, 3)."""
+    With several vectors the evaluations come back form-major, (num_forms * V, 3).
+    ``forms`` (see write_input) replaces ``points`` for mixed MLE / Covector statements."""
     if not ref_available():
         raise FileNotFoundError(f"{REF_DRIVER} not built (make -C oracle ref)")
     env = dict(os.environ)
     if threads is not None:
         env["OMP_NUM_THREADS"] = str(threads)
-    npts = np.asarray(points).reshape(-1, n, 3).shape[0]
+    npts = len(forms) if forms is not None else np.asarray(points).reshape(-1, n, 3).shape[0]
     with tempfile.TemporaryDirectory() as td:
         inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
-        write_input(inp, n, k, rho, sec, pow_bits, points, coeffs, batch_size, num_witnesses)
+        write_input(inp, n, k, rho, sec, pow_bits, points, coeffs, batch_size, num_witnesses, forms)
         cmd = [REF_DRIVER, inp, out] + (["--verify"] if verify else []) + (["--reps", str(reps)] if reps > 1 else [])
         if sha2:
             cmd.append("--sha2")
@@ -174,6 +187,9 @@ class Oracle:
         L.oracle_whir_prove_multi.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, u64, u64, p, p, sz, p, p, sz,
                                               p, sz, p, ctypes.c_int]
         L.oracle_whir_prove_multi.restype = ctypes.c_int
+        L.oracle_whir_prove_forms.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, u64, u64, p, p, sz, p, p, p,
+                                              sz, p, sz, p, ctypes.c_int]
+        L.oracle_whir_prove_forms.restype = ctypes.c_int
 
     # -- primitives -------------------------------------------------------
     def blake3(self, data: bytes) -> bytes:
@@ -287,6 +303,26 @@ class Oracle:
         lens = (ctypes.c_uint64 * 2)()
         rc = self.lib.oracle_whir_prove_multi(n, rho, k, sec, pow_bits, 0, batch_size, num_witnesses,
                                               coeffs.ctypes.data, points.ctypes.data, points.shape[0],
+                                              evals.ctypes.data, narg, cap, hints, cap, lens, int(sha2))
+        if rc != 0:
+            raise RuntimeError("oracle prove failed")
+        return narg.raw[:lens[0]], hints.raw[:lens[1]]
+
+    def prove_forms(self, n, k, rho, sec, pow_bits, forms, coeffs, evaluations, batch_size=1, num_witnesses=1,
+                    sha2=False):
+        """Statement of mixed linear forms: ``forms`` is a list of ("mle", (n, 3))
+        or ("covector", (2^n, 3)) arrays; evaluations: (num_forms * V, 3)."""
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+        kinds = (ctypes.c_int * max(len(forms), 1))(*[0 if kd == "mle" else 1 for kd, _ in forms])
+        data = np.concatenate([np.ascontiguousarray(d, dtype=np.uint64).reshape(-1) for _, d in forms]) \
+            if forms else np.zeros(1, dtype=np.uint64)
+        evals = np.ascontiguousarray(evaluations, dtype=np.uint64).reshape(-1, 3)
+        cap = 64 << 20
+        narg = ctypes.create_string_buffer(cap)
+        hints = ctypes.create_string_buffer(cap)
+        lens = (ctypes.c_uint64 * 2)()
+        rc = self.lib.oracle_whir_prove_forms(n, rho, k, sec, pow_bits, 0, batch_size, num_witnesses,
+                                              coeffs.ctypes.data, kinds, len(forms), data.ctypes.data,
                                               evals.ctypes.data, narg, cap, hints, cap, lens, int(sha2))
         if rc != 0:
             raise RuntimeError("oracle prove failed")

@@ -963,10 +963,17 @@ inline Opening open_witness(Transcript& t, const IrsCfg& c, const Witness& w) { 
 // (whir.hpp:303-309, whir_prover.hpp:56-407) over num_witnesses * batch_size
 // base vectors, MLE-point and/or dense-covector forms.
 // ---------------------------------------------------------------------------
+// Linear forms of the statement (linear_form.hpp:54-138): a MultilinearExtension
+// at a point (accumulate = scalar * eq(point, .)) or a dense Covector
+// (accumulate = scalar * vector).  `dense[f]` tells form f's kind; the
+// points and covectors are listed in form order within their own kind.
 struct Statement {
     std::vector<std::vector<E3>> mle_points;   // MultilinearExtension forms
-    std::vector<std::vector<E3>> covectors;    // Covector forms (after the MLE forms)
+    std::vector<std::vector<E3>> covectors;    // Covector forms
+    std::vector<bool> dense;                   // per form; empty = MLE forms, then covectors
     std::vector<E3> evaluations;               // form-major: evaluations[f * num_vectors + v]
+    size_t num_forms() const { return mle_points.size() + covectors.size(); }
+    bool is_dense(size_t f) const { return dense.empty() ? f >= mle_points.size() : (bool)dense[f]; }
 };
 struct ProofOut { std::vector<u8> narg, hints; std::vector<E3> evaluation_point; Hash initial_root{}; };
 
@@ -990,7 +997,8 @@ inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>
         wits.push_back(commit_base_multi(t, cfg.initial, mine, eng));
     }
     out.initial_root = wits[0].root();
-    const size_t nforms = st.mle_points.size() + st.covectors.size();
+    const size_t nforms = st.num_forms();
+    if (!st.dense.empty() && st.dense.size() != nforms) throw std::runtime_error("form kinds != forms");
     if (st.evaluations.size() != nforms * V) throw std::runtime_error("evaluations != forms * vectors");
     // step 1: OOD completion (whir_prover.hpp:92-120): every vector at every
     // witness's OOD points; values of other witnesses' vectors are sent.
@@ -1020,12 +1028,13 @@ inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>
     bool has_constraints = !crlc.empty();
     std::vector<E3> cov;
     if (nforms > 0 || has_constraints) cov.assign(size, E3());
-    for (size_t f = 0; f < nforms; ++f) {
-        E3 s = f == 0 ? E3::one() : crlc[f];
-        if (f < st.mle_points.size()) eval_eq_acc(cov, st.mle_points[f], s);
+    for (size_t f = 0, fm = 0, fc = 0; f < nforms; ++f) {
+        E3 s = f == 0 ? E3::one() : crlc[f];  // linear_forms[0] with ONE (whir_prover.hpp:161)
+        if (!st.is_dense(f)) eval_eq_acc(cov, st.mle_points[fm++], s);
         else {
-            const auto& cv = st.covectors[f - st.mle_points.size()];
-            for (size_t i = 0; i < cov.size(); ++i) cov[i] = cov[i] + s * cv[i];
+            const auto& cv = st.covectors[fc++];
+            if (cv.size() != cov.size()) throw std::runtime_error("covector size != vector size");
+            for (size_t i = 0; i < cov.size(); ++i) cov[i] = cov[i] + s * cv[i];  // scalar_mul_add
         }
     }
     // step 4: the sum, a double RLC of the evaluation and OOD matrices (:172-197)

@@ -17,7 +17,8 @@ has the reference checkout; the tests only read the JSON files).
    (oracle/_ref/ref_driver, built by oracle/Makefile) on seeded inputs:
    lengths and SHA-256 digests of narg and hints (full bytes for the smallest);
    "multi" holds proofs over several committed vectors (batch_size > 1,
-   several witnesses), including rows wider than one BLAKE3 chunk.
+   several witnesses), including rows wider than one BLAKE3 chunk; "forms"
+   statements that mix MultilinearExtension and dense Covector linear forms.
 """
 import hashlib
 import json
@@ -291,6 +292,39 @@ def proofs_multi():
     return out
 
 
+FORMS_CASES = [  # (n, k, rho, seed, form kinds, batch_size, num_witnesses, hash engine)
+    (5, 4, 1, 61, ("covector",), 1, 1, "blake3"),
+    (10, 4, 1, 62, ("covector",), 1, 1, "blake3"),
+    (11, 4, 2, 63, ("mle", "covector", "mle"), 1, 1, "blake3"),
+    (12, 4, 1, 64, ("covector", "mle"), 2, 2, "blake3"),
+    (9, 3, 1, 65, ("covector", "covector"), 1, 1, "sha2"),
+    (14, 4, 1, 66, ("mle", "covector"), 3, 1, "blake3"),
+]
+
+
+def proofs_forms():
+    from oracle.refio import run_reference
+    from tests.golden.forms import form_inputs
+
+    out = []
+    for (n, k, rho, seed, kinds, batch, nwit, eng) in FORMS_CASES:
+        coeffs, forms = form_inputs(n, seed, kinds, batch * nwit)
+        ref = run_reference(n, k, rho, 100, 20, None, coeffs, verify=True, sha2=eng == "sha2", batch_size=batch,
+                            num_witnesses=nwit, forms=forms)
+        assert ref.verify_ok == 1.0
+        rec = {"n": n, "k": k, "rho": rho, "security": 100, "pow_bits": 20, "seed": seed, "kinds": list(kinds),
+               "batch_size": batch, "num_witnesses": nwit, "hash": eng,
+               "evaluations": [[int(x) for x in row] for row in ref.evaluations],
+               "narg_len": len(ref.narg), "hints_len": len(ref.hints),
+               "narg_sha256": hashlib.sha256(ref.narg).hexdigest(),
+               "hints_sha256": hashlib.sha256(ref.hints).hexdigest()}
+        if n <= 5:
+            rec["narg"] = ref.narg.hex()
+            rec["hints"] = ref.hints.hex()
+        out.append(rec)
+    return out
+
+
 def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
@@ -301,7 +335,7 @@ def main():
     with open(os.path.join(HERE, "reference_proofs.json"), "w") as f:
         json.dump({"generator": "oracle/_ref/ref_driver (reference C++ prover, CLI domain separator, "
                                 "seeded ChaCha20 inputs via whirgpu_sample_goldilocks)", "cases": proofs(),
-                   "multi": proofs_multi()}, f, indent=1)
+                   "multi": proofs_multi(), "forms": proofs_forms()}, f, indent=1)
 
 
 if __name__ == "__main__":

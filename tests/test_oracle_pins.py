@@ -215,3 +215,37 @@ def test_oracle_multi_vector_matches_live_reference(oracle, n, k, rho, batch, nw
     assert ref.verify_ok == 1.0
     narg, hints = oracle.prove_multi(n, k, rho, 100, 20, points, coeffs, ref.evaluations, batch, nwit, sha2=sha2)
     assert narg == ref.narg and hints == ref.hints
+
+
+FORMS = json.load(open(os.path.join(HERE, "golden", "reference_proofs.json")))["forms"]
+
+
+@pytest.mark.parametrize("case", FORMS, ids=lambda c: f"n{c['n']}-{'-'.join(c['kinds'])}"
+                                                      f"-b{c['batch_size']}w{c['num_witnesses']}{c['hash']}")
+def test_oracle_covector_statements_match_reference_fixtures(oracle, case):
+    """Statements that mix MultilinearExtension and dense Covector forms
+    (linear_form.hpp:54-138): the covector accumulates scalar * vector."""
+    from tests.golden.forms import form_inputs
+
+    coeffs, forms = form_inputs(case["n"], case["seed"], case["kinds"], case["batch_size"] * case["num_witnesses"])
+    evals = np.array(case["evaluations"], dtype=np.uint64).reshape(-1, 3)
+    narg, hints = oracle.prove_forms(case["n"], case["k"], case["rho"], case["security"], case["pow_bits"], forms,
+                                     coeffs, evals, case["batch_size"], case["num_witnesses"],
+                                     sha2=case["hash"] == "sha2")
+    assert (len(narg), len(hints)) == (case["narg_len"], case["hints_len"])
+    assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
+    if "narg" in case:
+        assert narg.hex() == case["narg"] and hints.hex() == case["hints"]
+
+
+@pytest.mark.skipif(not ref_available(), reason="oracle/_ref not built")
+def test_oracle_covector_statement_matches_live_reference(oracle):
+    from tests.golden.forms import form_inputs
+
+    n, kinds = 12, ("covector", "mle", "covector")
+    coeffs, forms = form_inputs(n, 921, kinds, 2)
+    ref = run_reference(n, 4, 2, 100, 20, None, coeffs, verify=True, batch_size=2, forms=forms)
+    assert ref.verify_ok == 1.0
+    narg, hints = oracle.prove_forms(n, 4, 2, 100, 20, forms, coeffs, ref.evaluations, 2, 1)
+    assert narg == ref.narg and hints == ref.hints
