@@ -6,7 +6,7 @@
  * proof byte layout ({narg_string, hints}), for
  *   M = Basefield<GoldilocksExt3> (Goldilocks vectors, Ext3 challenges),
  *   hash = BLAKE3 or SHA-2, one or more witnesses of batch_size vectors,
- *   MultilinearExtension statements.
+ *   statements of MultilinearExtension and dense Covector forms.
  * Everything below is plain C: opaque handles, pointers, sizes and status
  * codes; no C++ types or exceptions cross this boundary.
  *
@@ -124,6 +124,23 @@ void whirgpu_witness_destroy(whirgpu_witness* w);
 whirgpu_status whirgpu_prove(whirgpu_ctx* ctx, whirgpu_witness* witness, const uint64_t* points, size_t num_points,
                              const uint64_t* evaluations, whirgpu_transcript* tx, uint64_t* evaluation_point,
                              uint64_t* rlc);
+
+/* The statement's linear forms as the reference builds them (linear_form.hpp:54-138):
+ * a MultilinearExtension at a point, or a dense Covector -- the two LinearForm
+ * kinds callers construct.  Forms are combined in the order given. */
+#define WHIRGPU_FORM_MLE 0      /* data: num_variables Ext3 coordinates (host memory) */
+#define WHIRGPU_FORM_COVECTOR 1 /* data: 2^num_variables Ext3 values, c0 c1 c2 each (host or device) */
+typedef struct {
+    uint32_t kind;
+    int location;           /* WHIRGPU_INPUT_HOST / WHIRGPU_INPUT_DEVICE, for covector data */
+    const uint64_t* data;
+} whirgpu_linear_form;
+/* Config::prove with num_forms (<= 8) forms of either kind; evaluations as in
+ * whirgpu_prove (num_forms * V values, form-major).  Host covectors are copied
+ * to a temporary device buffer freed before the call returns. */
+whirgpu_status whirgpu_prove_forms(whirgpu_ctx* ctx, whirgpu_witness* witness, const whirgpu_linear_form* forms,
+                                   size_t num_forms, const uint64_t* evaluations, whirgpu_transcript* tx,
+                                   uint64_t* evaluation_point, uint64_t* rlc);
 
 /* Bytes the last commit + prove pair moved host->device and device->host. */
 void whirgpu_last_io_bytes(const whirgpu_ctx* ctx, uint64_t* h2d, uint64_t* d2h);

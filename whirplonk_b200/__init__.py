@@ -1,5 +1,5 @@
 """B200-native WHIR prover (commit + prove over Goldilocks, Ext3 sumcheck,
-BLAKE3 Merkle commitments) behind the reference C++ prover API.
+BLAKE3 or SHA-256 Merkle commitments) behind the reference C++ prover API.
 
 The prover itself is libwhirgpu.so (hand-written sm_100a CUDA kernels behind
 the C ABI in include/whirgpu.h); this package is its Python mirror.
@@ -10,6 +10,7 @@ from .whir import (  # noqa: F401
     P,
     Config,
     Context,
+    Covector,
     DomainSeparator,
     FinalClaim,
     MultilinearExtension,

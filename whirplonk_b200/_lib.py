@@ -24,7 +24,7 @@ EXPORTED = [
     "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_schedule",
     "whirgpu_workspace_bytes",
     "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
-    "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
+    "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
     "whirgpu_debug_field_ops", "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
     "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
     "whirgpu_batch_create", "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_batch_destroy",
@@ -65,6 +65,14 @@ class Request(ctypes.Structure):
         ("protocol_id", ctypes.c_uint8 * 64),
         ("session_id", ctypes.c_uint8 * 32),
     ]
+
+
+FORM_MLE, FORM_COVECTOR = 0, 1
+
+
+class LinearForm(ctypes.Structure):
+    """Mirror of whirgpu_linear_form."""
+    _fields_ = [("kind", ctypes.c_uint32), ("location", ctypes.c_int), ("data", ctypes.c_void_p)]
 
 
 class Result(ctypes.Structure):
@@ -135,6 +143,7 @@ def load() -> ctypes.CDLL:
     L.whirgpu_commit_witnesses.argtypes = [p, ctypes.POINTER(WhirParams), p, u64, u64, i32, p, vp]
     L.whirgpu_witness_destroy.argtypes = [p]
     L.whirgpu_prove.argtypes = [p, p, p, sz, p, p, p, p]
+    L.whirgpu_prove_forms.argtypes = [p, p, ctypes.POINTER(LinearForm), sz, p, p, p, p]
     L.whirgpu_mle_evaluate.argtypes = [p, p, u64, i32, p, p]
     L.whirgpu_mle_evaluate_noalloc.argtypes = [p, u64, p, p, p]
     L.whirgpu_debug_field_ops.argtypes = [p, p, p, u64, i32]
@@ -185,7 +194,7 @@ def load() -> ctypes.CDLL:
                  "whirgpu_ntt_get_plan", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans"):
         getattr(L, name).restype = i32
     for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
-                 "whirgpu_proof_get", "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_prove", "whirgpu_mle_evaluate",
+                 "whirgpu_proof_get", "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate",
                  "whirgpu_mle_evaluate_noalloc", "whirgpu_debug_field_ops", "whirgpu_batch_create",
                  "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_server_create", "whirgpu_server_submit",
                  "whirgpu_server_poll",

@@ -404,27 +404,61 @@ void whirgpu_witness_destroy(whirgpu_witness* w) {
     delete w;
 }
 
-whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t* points, size_t num_points,
-                             const uint64_t* evaluations, whirgpu_transcript* tx, uint64_t* evaluation_point,
-                             uint64_t* rlc) {
+namespace {
+// Device buffer for the host covectors of one prove call, freed on every return path.
+struct TempDevice {
+    void* p = nullptr;
+    ~TempDevice() {
+        if (p) cudaFree(p);
+    }
+};
+}  // namespace
+
+whirgpu_status whirgpu_prove_forms(whirgpu_ctx* c, whirgpu_witness* w, const whirgpu_linear_form* forms,
+                                   size_t num_points, const uint64_t* evaluations, whirgpu_transcript* tx,
+                                   uint64_t* evaluation_point, uint64_t* rlc) {
     if (!c || !w || !tx || w->ctx != c || w->tx != tx) return fail(c, WHIRGPU_E_INVALID, "bad handles");
-    if (num_points > (size_t)MAX_FORMS || (num_points && (!points || !evaluations)))
+    if (num_points > (size_t)MAX_FORMS || (num_points && (!forms || !evaluations)))
         return fail(c, WHIRGPU_E_INVALID, "bad statement");
     ProofPlan p = w->ws->plan;
     p.n_forms = (int)num_points;
     if (num_points + p.sch.initial.out_domain == 0)
         return fail(c, WHIRGPU_E_UNSUPPORTED, "statement-free proofs are not on this path");
+    const size_t cov_bytes = (size_t)24 << p.n;
+    size_t host_dense = 0;
+    for (size_t f = 0; f < num_points; ++f) {
+        if (!forms[f].data || forms[f].kind > WHIRGPU_FORM_COVECTOR) return fail(c, WHIRGPU_E_INVALID, "bad linear form");
+        if (forms[f].kind == WHIRGPU_FORM_COVECTOR && forms[f].location != WHIRGPU_INPUT_DEVICE) ++host_dense;
+    }
     char* ws = w->ws->dev;
     ProofScalars* sc = plan_scalars(p, ws);
+    TempDevice tmp;
+    if (host_dense) WG_CUDA(c, cudaMalloc(&tmp.p, host_dense * cov_bytes), "cudaMalloc covectors");
     cudaError_t e = cudaSuccess;
-    if (num_points) {
-        e = cudaMemcpyAsync(ws + p.off_points, points, num_points * p.n * 24, cudaMemcpyHostToDevice, c->stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync(&sc->forms_eval[0], evaluations, num_points * p.nvec * 24, cudaMemcpyHostToDevice,
+    size_t slot = 0;
+    for (size_t f = 0; f < num_points && e == cudaSuccess; ++f) {
+        if (forms[f].kind == WHIRGPU_FORM_MLE) {
+            e = cudaMemcpyAsync(ws + p.off_points + f * p.n * 24, forms[f].data, p.n * 24, cudaMemcpyHostToDevice,
                                 c->stream);
-        if (e != cudaSuccess) return cuda_fail(c, e, "statement upload");
-        c->io_h2d += num_points * p.n * 24 + num_points * p.nvec * 24;
+            c->io_h2d += p.n * 24;
+            continue;
+        }
+        p.dense_mask |= 1u << f;
+        if (forms[f].location == WHIRGPU_INPUT_DEVICE) {
+            p.dense[f] = forms[f].data;
+        } else {
+            uint64_t* dst = reinterpret_cast<uint64_t*>(static_cast<char*>(tmp.p) + slot++ * cov_bytes);
+            e = cudaMemcpyAsync(dst, forms[f].data, cov_bytes, cudaMemcpyHostToDevice, c->stream);
+            p.dense[f] = dst;
+            c->io_h2d += cov_bytes;
+        }
     }
+    if (e == cudaSuccess && num_points) {
+        e = cudaMemcpyAsync(&sc->forms_eval[0], evaluations, num_points * p.nvec * 24, cudaMemcpyHostToDevice,
+                            c->stream);
+        c->io_h2d += num_points * p.nvec * 24;
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "statement upload");
     if (enqueue_prove(p, ws, c->tw, c->stream, c->timer.get()) != 0) return fail(c, WHIRGPU_E_INVALID, "prove launch failed");
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "prove kernels");
@@ -464,6 +498,17 @@ whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t*
     if (evaluation_point) std::memcpy(evaluation_point, hr, p.total_sumcheck_rounds * 24);
     if (rlc && num_points) std::memcpy(rlc, hrlc, num_points * 24);
     return WHIRGPU_OK;
+}
+
+whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t* points, size_t num_points,
+                             const uint64_t* evaluations, whirgpu_transcript* tx, uint64_t* evaluation_point,
+                             uint64_t* rlc) {
+    if (!c || !w) return fail(c, WHIRGPU_E_INVALID, "bad handles");
+    if (num_points > (size_t)MAX_FORMS || (num_points && !points)) return fail(c, WHIRGPU_E_INVALID, "bad statement");
+    const uint64_t n = w->ws->plan.n;
+    whirgpu_linear_form forms[MAX_FORMS];
+    for (size_t f = 0; f < num_points; ++f) forms[f] = {WHIRGPU_FORM_MLE, WHIRGPU_INPUT_HOST, points + f * n * 3};
+    return whirgpu_prove_forms(c, w, forms, num_points, evaluations, tx, evaluation_point, rlc);
 }
 
 whirgpu_status whirgpu_mle_evaluate(whirgpu_ctx* c, const uint64_t* coeffs, uint64_t n, int where,

@@ -381,7 +381,8 @@ int launch_fold(const SumcheckArgs& s, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 constexpr u32 COV_LO = 10;
 
-__global__ void k_cov_tables(const u64* points, u32 logS, int n_forms, int n_ood, ProofScalars* sc, E3* tab) {
+__global__ void k_cov_tables(const u64* points, u32 logS, int n_forms, int n_ood, u32 dense_mask, ProofScalars* sc,
+                             E3* tab) {
     const u32 lo_bits = logS < COV_LO ? logS : COV_LO, hi_bits = logS - lo_bits;
     const u32 nlo = 1u << lo_bits, nhi = 1u << hi_bits;
     const u32 per = nlo + nhi;
@@ -390,7 +391,9 @@ __global__ void k_cov_tables(const u64* points, u32 logS, int n_forms, int n_ood
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 term = (u32)(e / per), k = (u32)(e % per);
         E3 v;
-        if ((int)term < n_forms) {
+        if ((int)term < n_forms && ((dense_mask >> term) & 1)) {
+            v = e3_zero();  // dense covector: not tabulated (k_cov_init reads it)
+        } else if ((int)term < n_forms) {
             const u64* pt = points + (u64)term * logS * 3;
             // coordinate c <-> bit (logS - 1 - c) of i; hi bits are coordinates 0..hi_bits-1
             v = e3_one();
@@ -429,7 +432,15 @@ __global__ void __launch_bounds__(256) k_cov_init(CovInitArgs a, const E3* tab) 
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < S; i += (u64)gridDim.x * blockDim.x) {
         const u32 hi = (u32)(i >> lo_bits), lo = (u32)(i & (nlo - 1));
         E3Acc s = e3acc_zero();
-        for (int t = 0; t < nterms; ++t) e3acc_mac(s, tab[(u64)t * per + nlo + hi], tab[(u64)t * per + lo]);
+        for (int t = 0; t < nterms; ++t) {
+            if (t < a.n_forms && ((a.dense_mask >> t) & 1)) {
+                // Covector::accumulate: scalar * vector (linear_form.hpp:75-78)
+                const u64* d = a.dense[t] + 3 * i;
+                e3acc_mac(s, t == 0 ? e3_one() : a.sc->crlc[t], E3{d[0], d[1], d[2]});
+            } else {
+                e3acc_mac(s, tab[(u64)t * per + nlo + hi], tab[(u64)t * per + lo]);
+            }
+        }
         const E3 acc = e3acc_reduce(s);
         a.cov[0][i] = acc.c0;
         a.cov[1][i] = acc.c1;
@@ -461,7 +472,9 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
         for (int c = 0; c < 3; ++c) cudaMemsetAsync(a.cov[c], 0, S * 8, st);
         return 0;
     }
-    k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.sc, tab);
+    for (int f = 0; f < a.n_forms; ++f)
+        if (((a.dense_mask >> f) & 1) && !a.dense[f]) return -1;
+    k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.dense_mask, a.sc, tab);
     count_launches(1);
     u64 want = (S + 255) / 256;
     k_cov_init<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab);
@@ -572,7 +585,7 @@ int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch
     E3* partials = reinterpret_cast<E3*>(base + 256);
     E3* tab = reinterpret_cast<E3*>(base + 256 + 592 * sizeof(E3));
     cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
-    k_cov_tables<<<148, 256, 0, st>>>(point, logS, 1, 0, nullptr, tab);
+    k_cov_tables<<<148, 256, 0, st>>>(point, logS, 1, 0, 0u, nullptr, tab);
     count_launches(1);
     const u64 S = 1ull << logS;
     u64 want = (S + 255) / 256;

@@ -158,6 +158,8 @@ struct CovInitArgs {
     u32 nvec;           // committed vectors (1: no vector RLC)
     const u64* vecs;    // nvec base vectors, 2^logS words each, back to back
     u64* vec_out[3];    // Ext3 planes of the combined vector
+    u32 dense_mask;     // forms f with bit f set are dense covectors (their points slot is unused):
+    const u64* dense[8];  // cov[i] += crlc_f * dense[f][i] (Ext3, AoS), crlc_0 = 1
 };
 int launch_cov_init(const CovInitArgs& a, cudaStream_t st);
 size_t cov_init_scratch_bytes(u32 logS, int n_forms, int n_ood);

@@ -19,6 +19,8 @@
 
 namespace wg {
 
+static_assert(MAX_FORMS == 8, "ProofPlan::dense and CovInitArgs::dense hold MAX_FORMS pointers");
+
 namespace {
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 struct Bump {
@@ -339,6 +341,8 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         ci.scratch = ws + p.off_cov_scratch;
         ci.nvec = V;
         ci.vecs = c.w(p.off_coeffs);
+        ci.dense_mask = p.dense_mask;
+        for (int f = 0; f < 8; ++f) ci.dense[f] = p.dense[f];
         WG_TIMED(c, FAM_COV, launch_cov_init(ci, st));
         WG_TRY(sumcheck(c, s.initial_sumcheck, size0, V == 1, r_slot, true));
     } else {

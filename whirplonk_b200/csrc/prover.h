@@ -30,6 +30,8 @@ struct ProofPlan {
     ProtocolParams params;
     uint32_t n = 0;          // num_variables
     int n_forms = 0;
+    uint32_t dense_mask = 0;                 // statement forms that are dense covectors (bit f)
+    const uint64_t* dense[8] = {};           // their device data: 2^n Ext3 values each, AoS (c0 c1 c2)
     uint32_t nwit = 1;       // initial commitments (witnesses), each of params.batch_size vectors
     uint32_t nvec = 1;       // committed vectors: nwit * batch_size
     size_t init_planes_stride = 0, init_nodes_stride = 0;  // bytes between the initial commitments' buffers

@@ -188,6 +188,16 @@ class MultilinearExtension:
 
 
 @dataclass
+class Covector:
+    """Covector linear form (linear_form.hpp:54-91): a dense vector of 2^n Ext3
+    values (an (2^n, 3) uint64 array), or a device pointer to one with
+    on_device=True."""
+
+    vector: object
+    on_device: bool = False
+
+
+@dataclass
 class FinalClaim:
     """FinalClaim (whir.hpp:376-425) as the prover returns it."""
 
@@ -286,11 +296,24 @@ class Config:
             raise ValueError("pass the one handle of commit / commit_witnesses")
         nvec = witnesses[0].num_vectors
         n = self.num_variables
-        pts = np.zeros((max(len(linear_forms), 1), n, 3), dtype=np.uint64)
+        cforms = (_lib.LinearForm * max(len(linear_forms), 1))()
+        keep = []
         for i, lf in enumerate(linear_forms):
-            if not isinstance(lf, MultilinearExtension):
-                raise TypeError("only MultilinearExtension statements are on this path")
-            pts[i] = np.asarray(lf.point, dtype=np.uint64).reshape(n, 3)
+            if isinstance(lf, MultilinearExtension):
+                a = np.ascontiguousarray(np.asarray(lf.point, dtype=np.uint64).reshape(n, 3))
+                cforms[i] = _lib.LinearForm(_lib.FORM_MLE, 0, a.ctypes.data)
+            elif isinstance(lf, Covector):
+                if lf.on_device:
+                    cforms[i] = _lib.LinearForm(_lib.FORM_COVECTOR, 1, int(lf.vector))
+                    keep.append(lf)
+                    continue
+                a = np.ascontiguousarray(lf.vector, dtype=np.uint64)
+                if a.size != 3 * self.size:
+                    raise ValueError("covector length != config size")
+                cforms[i] = _lib.LinearForm(_lib.FORM_COVECTOR, 0, a.ctypes.data)
+            else:
+                raise TypeError("MultilinearExtension and Covector statements are on this path")
+            keep.append(a)
         if len(evaluations) != len(linear_forms) * nvec:
             raise ValueError("evaluations != linear forms * committed vectors")
         ev = np.zeros((max(len(evaluations), 1), 3), dtype=np.uint64)
@@ -298,25 +321,29 @@ class Config:
             ev[i] = np.asarray(e, dtype=np.uint64).reshape(3)
         eval_point = np.zeros((n, 3), dtype=np.uint64)
         rlc = np.zeros((max(len(linear_forms), 1), 3), dtype=np.uint64)
-        _lib.check(ctx._L.whirgpu_prove(ctx.handle, witnesses[0].handle, pts.ctypes.data, len(linear_forms),
-                                        ev.ctypes.data, prover_state.handle, eval_point.ctypes.data,
-                                        rlc.ctypes.data), ctx.handle)
+        _lib.check(ctx._L.whirgpu_prove_forms(ctx.handle, witnesses[0].handle, cforms, len(linear_forms),
+                                              ev.ctypes.data, prover_state.handle, eval_point.ctypes.data,
+                                              rlc.ctypes.data), ctx.handle)
         return FinalClaim([tuple(int(x) for x in r) for r in eval_point],
                           [tuple(int(x) for x in r) for r in rlc[:len(linear_forms)]])
 
 
 def prove_once(n: int, params: ProtocolParameters, coeffs, points, evaluations, ctx: Optional[Context] = None,
-               ds: Optional[DomainSeparator] = None, on_device_ptr: Optional[int] = None, num_witnesses: int = 1):
+               ds: Optional[DomainSeparator] = None, on_device_ptr: Optional[int] = None, num_witnesses: int = 1,
+               forms: Optional[Sequence] = None):
     """commit (num_witnesses witnesses of params.batch_size vectors) + prove with
-    the CLI domain separator; returns (narg, hints, claim).  ``evaluations``
-    holds num_points * num_vectors Ext3 values, form-major."""
+    the CLI domain separator; returns (narg, hints, claim).  The statement is
+    one MultilinearExtension per point, or ``forms`` (MultilinearExtension /
+    Covector objects) when given; ``evaluations`` holds num_forms * num_vectors
+    Ext3 values, form-major."""
     ctx = ctx or default_context()
     ds = ds or cli_domain_separator(params)
     config = Config.from_params(1 << n, params)
     ps = ProverState.from_ds(ds, b"", ctx)
     w = config.commit_witnesses(ps, coeffs, num_witnesses, on_device_ptr=on_device_ptr)
-    pts = np.asarray(points, dtype=np.uint64).reshape(-1, n, 3)
-    forms = [MultilinearExtension(pts[i]) for i in range(pts.shape[0])]
+    if forms is None:
+        pts = np.asarray(points, dtype=np.uint64).reshape(-1, n, 3)
+        forms = [MultilinearExtension(pts[i]) for i in range(pts.shape[0])]
     claim = config.prove(ps, coeffs, [w], forms, [tuple(e) for e in np.asarray(evaluations).reshape(-1, 3)])
     narg, hints = ps.proof()
     return narg, hints, claim
