@@ -134,15 +134,16 @@ void put_f64(FILE* f, double v) { std::fwrite(&v, 8, 1, f); }
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: ref_driver INPUT OUTPUT [--verify] [--reps R] [--config]\n");
+        std::fprintf(stderr, "usage: ref_driver INPUT OUTPUT [--verify] [--reps R] [--config] [--sha2] [--unique]\n");
         return 2;
     }
-    bool do_verify = false, print_cfg = false, use_sha2 = false;
+    bool do_verify = false, print_cfg = false, use_sha2 = false, unique = false;
     int reps = 1;
     for (int i = 3; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--verify")) do_verify = true;
         else if (!std::strcmp(argv[i], "--config")) print_cfg = true;
         else if (!std::strcmp(argv[i], "--sha2")) use_sha2 = true;
+        else if (!std::strcmp(argv[i], "--unique")) unique = true;
         else if (!std::strcmp(argv[i], "--reps") && i + 1 < argc) reps = std::atoi(argv[++i]);
         else die("bad flag");
     }
@@ -192,7 +193,7 @@ int main(int argc, char** argv) {
     params.pow_bits = powb;
     params.initial_folding_factor = k;
     params.folding_factor = k;
-    params.unique_decoding = false;
+    params.unique_decoding = unique;
     params.starting_log_inv_rate = rho;
     params.batch_size = batch;
     params.hash_id = use_sha2 ? ::whir::hash::ENGINE_ID_SHA2 : ::whir::hash::ENGINE_ID_BLAKE3;

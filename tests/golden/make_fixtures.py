@@ -18,7 +18,8 @@ has the reference checkout; the tests only read the JSON files).
    lengths and SHA-256 digests of narg and hints (full bytes for the smallest);
    "multi" holds proofs over several committed vectors (batch_size > 1,
    several witnesses), including rows wider than one BLAKE3 chunk; "forms"
-   statements that mix MultilinearExtension and dense Covector linear forms.
+   statements that mix MultilinearExtension and dense Covector linear forms;
+   "unique" proofs under unique decoding, including statement-free ones.
 """
 import hashlib
 import json
@@ -325,6 +326,39 @@ def proofs_forms():
     return out
 
 
+UNIQUE_CASES = [  # unique decoding (no OOD samples): (n, k, rho, seed, form kinds, batch_size, num_witnesses, hash)
+    (5, 4, 1, 71, (), 1, 1, "blake3"),            # no constraint at all: folds without a sumcheck
+    (10, 4, 1, 72, (), 1, 1, "blake3"),
+    (12, 4, 2, 73, ("mle",), 1, 1, "blake3"),
+    (12, 4, 1, 74, (), 2, 2, "blake3"),
+    (9, 3, 1, 75, ("covector",), 1, 1, "sha2"),
+    (16, 4, 1, 76, (), 1, 1, "blake3"),
+]
+
+
+def proofs_unique():
+    from oracle.refio import run_reference
+    from tests.golden.forms import form_inputs
+
+    out = []
+    for (n, k, rho, seed, kinds, batch, nwit, eng) in UNIQUE_CASES:
+        coeffs, forms = form_inputs(n, seed, kinds, batch * nwit)
+        ref = run_reference(n, k, rho, 100, 20, None, coeffs, verify=True, sha2=eng == "sha2", batch_size=batch,
+                            num_witnesses=nwit, forms=forms, unique=True)
+        assert ref.verify_ok == 1.0
+        rec = {"n": n, "k": k, "rho": rho, "security": 100, "pow_bits": 20, "seed": seed, "kinds": list(kinds),
+               "batch_size": batch, "num_witnesses": nwit, "hash": eng, "unique_decoding": True,
+               "evaluations": [[int(x) for x in row] for row in ref.evaluations],
+               "narg_len": len(ref.narg), "hints_len": len(ref.hints),
+               "narg_sha256": hashlib.sha256(ref.narg).hexdigest(),
+               "hints_sha256": hashlib.sha256(ref.hints).hexdigest()}
+        if n <= 5:
+            rec["narg"] = ref.narg.hex()
+            rec["hints"] = ref.hints.hex()
+        out.append(rec)
+    return out
+
+
 def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
@@ -335,7 +369,7 @@ def main():
     with open(os.path.join(HERE, "reference_proofs.json"), "w") as f:
         json.dump({"generator": "oracle/_ref/ref_driver (reference C++ prover, CLI domain separator, "
                                 "seeded ChaCha20 inputs via whirgpu_sample_goldilocks)", "cases": proofs(),
-                   "multi": proofs_multi(), "forms": proofs_forms()}, f, indent=1)
+                   "multi": proofs_multi(), "forms": proofs_forms(), "unique": proofs_unique()}, f, indent=1)
 
 
 if __name__ == "__main__":

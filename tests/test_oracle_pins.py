@@ -249,3 +249,26 @@ def test_oracle_covector_statement_matches_live_reference(oracle):
     assert ref.verify_ok == 1.0
     narg, hints = oracle.prove_forms(n, 4, 2, 100, 20, forms, coeffs, ref.evaluations, 2, 1)
     assert narg == ref.narg and hints == ref.hints
+
+
+UNIQUE = json.load(open(os.path.join(HERE, "golden", "reference_proofs.json")))["unique"]
+
+
+@pytest.mark.parametrize("case", UNIQUE, ids=lambda c: f"n{c['n']}-{'-'.join(c['kinds']) or 'none'}"
+                                                       f"-b{c['batch_size']}w{c['num_witnesses']}{c['hash']}")
+def test_oracle_unique_decoding_matches_reference_fixtures(oracle, case):
+    """Unique decoding (no OOD samples); without linear forms the proof has no
+    constraint: the folding randomness is squeezed directly, the skip-PoW runs
+    and the vector is folded without a sumcheck (whir_prover.hpp:211-218)."""
+    from tests.golden.forms import form_inputs
+
+    coeffs, forms = form_inputs(case["n"], case["seed"], case["kinds"], case["batch_size"] * case["num_witnesses"])
+    evals = np.array(case["evaluations"], dtype=np.uint64).reshape(-1, 3)
+    narg, hints = oracle.prove_forms(case["n"], case["k"], case["rho"], case["security"], case["pow_bits"], forms,
+                                     coeffs, evals, case["batch_size"], case["num_witnesses"],
+                                     sha2=case["hash"] == "sha2", unique=True)
+    assert (len(narg), len(hints)) == (case["narg_len"], case["hints_len"])
+    assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
+    if "narg" in case:
+        assert narg.hex() == case["narg"] and hints.hex() == case["hints"]

@@ -69,6 +69,7 @@ class Batch:
         h = ctypes.c_void_p()
         _lib.check(self._L.whirgpu_batch_create(ctx.handle, arr, len(requests), mode, ctypes.byref(h)), ctx.handle)
         self.handle = h.value
+        ctx.adopt(self)
 
     def run(self):
         _lib.check(self._L.whirgpu_batch_run(self.handle), self.ctx.handle)
@@ -117,6 +118,7 @@ class Server:
         h = ctypes.c_void_p()
         _lib.check(self._L.whirgpu_server_create(ctx.handle, hbm_budget, max_inflight, ctypes.byref(h)), ctx.handle)
         self.handle = h.value
+        ctx.adopt(self)
         self._live = {}
 
     def submit(self, req: ProofRequest) -> int:

@@ -68,9 +68,7 @@ whirgpu_status check_request(whirgpu_ctx* c, const whirgpu_request& r) {
 whirgpu_status slot_bind(whirgpu_ctx* c, const whirgpu_request& r, Workspace* ws, Slot& s) {
     s.ws = ws;
     s.plan = ws->plan;
-    s.plan.n_forms = (int)r.num_points;
-    if (r.num_points + s.plan.sch.initial.out_domain == 0)
-        return fail(c, WHIRGPU_E_UNSUPPORTED, "statement-free proofs are not on this path");
+    plan_set_forms(s.plan, (int)r.num_points);
     s.hin_bytes = evals_off(s.plan) + (size_t)MAX_FORMS * MAX_VECTORS * 24;
     s.hout_bytes = sizeof(TxState) + s.plan.narg_len + s.plan.hints_cap;
     if (cudaMallocHost(&s.hin, s.hin_bytes) != cudaSuccess || cudaMallocHost(&s.hout, s.hout_bytes) != cudaSuccess) {

@@ -269,6 +269,14 @@ void whirgpu_ctx_destroy(whirgpu_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    {
+        std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+        for (whirgpu_witness* w : c->live_witnesses) {  // their workspaces are freed below
+            w->ws = nullptr;
+            w->ctx = nullptr;
+        }
+        c->live_witnesses.clear();
+    }
     for (auto& kv : c->cache)
         for (Workspace* w : kv.second) free_workspace(c, w);
     cudaFree(c->tw.tw_stage);
@@ -386,6 +394,10 @@ whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* c, const whirgpu_params* pa
     w->ws = ws;
     w->tx = tx;
     tx->complete = false;
+    {
+        std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+        c->live_witnesses.insert(w);
+    }
     *out = w;
     return WHIRGPU_OK;
 }
@@ -397,9 +409,13 @@ whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, cons
 
 void whirgpu_witness_destroy(whirgpu_witness* w) {
     if (!w) return;
-    if (w->ws) {
-        cudaStreamSynchronize(w->ctx->stream);
-        release_workspace(w->ctx, w->ws);
+    if (w->ctx) {
+        if (w->ws) {
+            cudaStreamSynchronize(w->ctx->stream);
+            release_workspace(w->ctx, w->ws);
+        }
+        std::lock_guard<std::recursive_mutex> lk(w->ctx->cache_mu);
+        w->ctx->live_witnesses.erase(w);
     }
     delete w;
 }
@@ -417,13 +433,11 @@ struct TempDevice {
 whirgpu_status whirgpu_prove_forms(whirgpu_ctx* c, whirgpu_witness* w, const whirgpu_linear_form* forms,
                                    size_t num_points, const uint64_t* evaluations, whirgpu_transcript* tx,
                                    uint64_t* evaluation_point, uint64_t* rlc) {
-    if (!c || !w || !tx || w->ctx != c || w->tx != tx) return fail(c, WHIRGPU_E_INVALID, "bad handles");
+    if (!c || !w || !tx || w->ctx != c || w->tx != tx || !w->ws) return fail(c, WHIRGPU_E_INVALID, "bad handles");
     if (num_points > (size_t)MAX_FORMS || (num_points && (!forms || !evaluations)))
         return fail(c, WHIRGPU_E_INVALID, "bad statement");
     ProofPlan p = w->ws->plan;
-    p.n_forms = (int)num_points;
-    if (num_points + p.sch.initial.out_domain == 0)
-        return fail(c, WHIRGPU_E_UNSUPPORTED, "statement-free proofs are not on this path");
+    plan_set_forms(p, (int)num_points);
     const size_t cov_bytes = (size_t)24 << p.n;
     size_t host_dense = 0;
     for (size_t f = 0; f < num_points; ++f) {
@@ -503,7 +517,7 @@ whirgpu_status whirgpu_prove_forms(whirgpu_ctx* c, whirgpu_witness* w, const whi
 whirgpu_status whirgpu_prove(whirgpu_ctx* c, whirgpu_witness* w, const uint64_t* points, size_t num_points,
                              const uint64_t* evaluations, whirgpu_transcript* tx, uint64_t* evaluation_point,
                              uint64_t* rlc) {
-    if (!c || !w) return fail(c, WHIRGPU_E_INVALID, "bad handles");
+    if (!c || !w || !w->ws) return fail(c, WHIRGPU_E_INVALID, "bad handles");
     if (num_points > (size_t)MAX_FORMS || (num_points && !points)) return fail(c, WHIRGPU_E_INVALID, "bad statement");
     const uint64_t n = w->ws->plan.n;
     whirgpu_linear_form forms[MAX_FORMS];

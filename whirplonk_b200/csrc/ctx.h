@@ -7,6 +7,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <set>
 #include <mutex>
 #include <memory>
 #include <string>
@@ -103,6 +104,9 @@ struct whirgpu_ctx {
     uint64_t io_h2d = 0, io_d2h = 0;
     std::recursive_mutex cache_mu;  // workspace cache (the serving thread shares the context)
     uint64_t use_clock = 0;
+    // Witnesses not yet destroyed: destroying the context detaches them, so a
+    // witness destroyed afterwards only frees its handle.
+    std::set<whirgpu_witness*> live_witnesses;
 };
 
 struct whirgpu_transcript {

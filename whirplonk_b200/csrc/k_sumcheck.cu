@@ -467,15 +467,16 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
     E3* tab = reinterpret_cast<E3*>(a.scratch);
     const int nterms = a.n_forms + a.n_ood;
     const u64 S = 1ull << a.logS;
-    if (nterms == 0) {
-        if (a.nvec > 1) return -1;  // statement-free proofs are not on this path
+    if (nterms == 0 && a.nvec == 1) {  // no constraint and no vector RLC: a zero covector
         for (int c = 0; c < 3; ++c) cudaMemsetAsync(a.cov[c], 0, S * 8, st);
         return 0;
     }
     for (int f = 0; f < a.n_forms; ++f)
         if (((a.dense_mask >> f) & 1) && !a.dense[f]) return -1;
-    k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.dense_mask, a.sc, tab);
-    count_launches(1);
+    if (nterms > 0) {
+        k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.dense_mask, a.sc, tab);
+        count_launches(1);
+    }
     u64 want = (S + 255) / 256;
     k_cov_init<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab);
     count_launches(1);

@@ -194,6 +194,28 @@ int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2,
     return 0;
 }
 
+// `count` Ext3 challenges in a row into sc->sc_r[slot ..] -- the folding
+// randomness of a proof without constraints (whir_prover.hpp:211-218,
+// verifier_message_vec).  One warp.
+__global__ void k_squeeze_e3(TxState* tx, ProofScalars* sc, int slot, int count) {
+    if (threadIdx.x >= 32) return;
+    WarpTx t;
+    wtx_load(t, tx);
+    for (int k = 0; k < count; ++k) {
+        const E3 r = wtx_challenge_e3(t);
+        if (threadIdx.x == 0) sc->sc_r[slot + k] = r;
+    }
+    wtx_store(t, tx);
+}
+
+int launch_squeeze_challenges(TxState* tx, ProofScalars* sc, int slot, int count, cudaStream_t st) {
+    if (count <= 0) return 0;
+    if (slot < 0 || slot + count > MAX_SC_ROUNDS) return -1;
+    k_squeeze_e3<<<1, 32, 0, st>>>(tx, sc, slot, count);
+    count_launches(1);
+    return 0;
+}
+
 // ---------------------------------------------------------------------------
 // Opening (irs_commit.hpp:600-713, challenge_indices.hpp:56-119,
 // merkle_tree.hpp:165-211) of nwit commitments at the same rows, one CTA of

@@ -115,6 +115,8 @@ int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned ch
 int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int nwit, int ood, int nvec, cudaStream_t st);
 // PoW: squeeze the 32-byte challenge, grind the minimum nonce, send it.
 int launch_pow(TxState* tx, ProofScalars* sc, u64 threshold, int slot, int hash, cudaStream_t st);
+// `count` Ext3 challenges into sc->sc_r[slot ..] (verifier_message_vec).
+int launch_squeeze_challenges(TxState* tx, ProofScalars* sc, int slot, int count, cudaStream_t st);
 // Sends every coefficient of the final folded vector (whir_prover.hpp:360-362).
 int launch_send_vector(TxState* tx, const u64* c0, const u64* c1, const u64* c2, u64 size, cudaStream_t st);
 

@@ -132,9 +132,9 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
     };
     narg += nwit * commit_narg(s.initial, batch);
     narg += 24 * s.initial.out_domain * nwit * (p.nvec - batch);  // OOD completion
-    const bool has_constraints = n_forms + s.initial.out_domain > 0;
-    if (has_constraints) narg += sumcheck_narg(s.initial_sumcheck);
-    else narg += pow_narg(s.initial_skip_pow);
+    // initial sumcheck, or (no constraint) the skip-PoW: added below per variant
+    const size_t narg_initial_constrained = sumcheck_narg(s.initial_sumcheck);
+    const size_t narg_initial_free = pow_narg(s.initial_skip_pow);
     size_t sc_rounds = s.initial_sumcheck.num_rounds;
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         narg += commit_narg(s.rounds[r].irs, 1) + pow_narg(s.rounds[r].pow_threshold) + sumcheck_narg(s.rounds[r].sumcheck);
@@ -144,16 +144,23 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
     narg += 24 * s.final_sumcheck.initial_size + pow_narg(s.final_pow) + sumcheck_narg(s.final_sumcheck);
     hints += s.rounds.empty() ? open_hints(s.initial, batch, 1, nwit) : open_hints(s.rounds.back().irs, 1, 3, 1);
     sc_rounds += s.final_sumcheck.num_rounds;
-    p.narg_len = narg;
+    p.narg_len_constrained = narg + narg_initial_constrained;
+    p.narg_len_free = narg + narg_initial_free;
+    p.narg_len = std::max(p.narg_len_constrained, p.narg_len_free);  // stream capacity until the forms are known
     p.hints_cap = hints;
     p.total_sumcheck_rounds = sc_rounds;
-    p.off_narg = b.take(narg + 64);
+    p.off_narg = b.take(p.narg_len + 64);
     p.off_hints = b.take(hints + 64);
     p.ds_cap = std::max<size_t>(ds_len, 96);
     p.off_ds = b.take(p.ds_cap);
     p.off_points = b.take((size_t)std::max(n_forms, 1) * n * 24 + 64);
     p.total_bytes = b.cur;
     return p;
+}
+
+void plan_set_forms(ProofPlan& p, int n_forms) {
+    p.n_forms = n_forms;
+    p.narg_len = n_forms + p.sch.initial.out_domain > 0 ? p.narg_len_constrained : p.narg_len_free;
 }
 
 TxState* plan_tx(const ProofPlan& p, char* ws) { return reinterpret_cast<TxState*>(ws + p.off_tx); }
@@ -330,7 +337,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
     WG_TIMED(c, FAM_TX, launch_constraint_rlc(c.tx(), c.sc(), p.n_forms, (int)W, ood0, (int)V, st));
     const bool has_constraints = p.n_forms + ood0 > 0;
     int r_slot = 0;
-    if (has_constraints) {
+    {  // covector (zero without constraints) and, with several vectors, the combined vector
         CovInitArgs ci{};
         for (int k = 0; k < 3; ++k) { ci.cov[k] = c.cov(k); ci.vec_out[k] = c.a(k); }
         ci.logS = p.n;
@@ -344,9 +351,27 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         ci.dense_mask = p.dense_mask;
         for (int f = 0; f < 8; ++f) ci.dense[f] = p.dense[f];
         WG_TIMED(c, FAM_COV, launch_cov_init(ci, st));
+    }
+    if (has_constraints) {
         WG_TRY(sumcheck(c, s.initial_sumcheck, size0, V == 1, r_slot, true));
     } else {
-        return -2;  // statement-free proofs (unique decoding, no forms) are not on this path
+        // No constraint (unique decoding, no forms; whir_prover.hpp:211-218): the
+        // folding randomness is squeezed directly, the skip-PoW keeps the
+        // transcript in step, and the vector is folded once per challenge (the
+        // zero covector folds to zero).
+        const int k = (int)s.initial_sumcheck.num_rounds;
+        WG_TIMED(c, FAM_TX, launch_squeeze_challenges(c.tx(), c.sc(), 0, k, st));
+        WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), s.initial_skip_pow, MAX_COMMITS + 1, c.p.params.hash, st));
+        for (int t = 0; t < k; ++t) {
+            SumcheckArgs a{};
+            a.a_base = (V == 1 && t == 0) ? c.w(p.off_coeffs) : nullptr;
+            for (int q = 0; q < 3; ++q) { a.a_in[q] = c.a(q); a.a_out[q] = c.a(q); a.b[q] = c.cov(q); }
+            a.size = size0 >> (t + 1);
+            a.fold_r = t;
+            a.sc = c.sc();
+            WG_TIMED(c, FAM_SUMCHECK, launch_fold(a, st));
+        }
+        r_slot = k;
     }
 
     uint64_t vsize = size0 >> s.initial_sumcheck.num_rounds;

@@ -43,11 +43,16 @@ struct ProofPlan {
     size_t a_plane_words = 0, cov_plane_words = 0;
     uint32_t ood_values = 0;   // OOD scratch capacity in values (points x vectors)
     size_t narg_len = 0;       // exact narg length (every message has a fixed size)
+    size_t narg_len_constrained = 0, narg_len_free = 0;  // with / without any constraint
     size_t hints_cap = 0;      // upper bound of the hint stream
     size_t ds_cap = 0;
     size_t total_bytes = 0;
     size_t total_sumcheck_rounds = 0;
 };
+
+// Sets the statement's form count; a proof with no form and no OOD sample has
+// no constraint (no initial sumcheck), which changes the narg length.
+void plan_set_forms(ProofPlan& p, int n_forms);
 
 // Throws std::invalid_argument on unsupported parameters.  The plan covers
 // num_witnesses initial commitments of p.batch_size vectors each.

@@ -18,6 +18,7 @@ this module only marshals arguments.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -87,9 +88,16 @@ class Context:
         h = ctypes.c_void_p()
         _lib.check(self._L.whirgpu_ctx_create(device, hbm_budget, ctypes.byref(h)))
         self.handle = h.value
+        self._children = weakref.WeakSet()  # batches and servers: closed before the context
+
+    def adopt(self, child):
+        """Registers an object whose close() must run before the context goes."""
+        self._children.add(child)
 
     def close(self):
         if self.handle:
+            for ch in list(self._children):
+                ch.close()
             self._L.whirgpu_ctx_destroy(self.handle)
             self.handle = None
 
@@ -223,6 +231,7 @@ class Witness:
     def __del__(self):
         try:
             if self.handle:
+                # after Context.close() the library has detached the witness; this frees its handle only
                 self.ctx._L.whirgpu_witness_destroy(self.handle)
                 self.handle = None
         except Exception:
