@@ -220,6 +220,87 @@ int oracle_whir_prove_forms(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique
     }
 }
 
+// Commit + prove for a Config given field by field (the reference's golden
+// dumpers build it so, cpp/tests/dump_whir.cpp:121-148) and a given domain
+// separator.  cfg words:
+//   [0..4] initial committer: vector_size, codeword_length, depth, in_domain, out_domain
+//   [5..7] initial sumcheck rounds, its PoW threshold, the skip-PoW threshold
+//   [8] R, then per round 8 words: vector_size, codeword_length, depth, in_domain,
+//       out_domain, PoW threshold, sumcheck rounds, sumcheck PoW threshold
+//   then final sumcheck rounds, its PoW threshold, the final PoW threshold.
+// deg: 3 Basefield<GoldilocksExt3>, 1 Identity<Goldilocks>.  eval_point
+// receives the FinalClaim evaluation point (3 words per coordinate).
+int oracle_whir_prove_config(const u64* cfg, size_t cfg_len, int deg, int sha2, const u8* ds96, u64 batch_size,
+                             u64 num_witnesses, const u64* coeffs, const int* kinds, size_t nforms,
+                             const u64* form_data, const u64* evals, u8* narg, size_t narg_cap, u8* hints,
+                             size_t hints_cap, u64* lens, u64* eval_point, size_t eval_point_cap) {
+    try {
+        if (cfg_len < 12) return 2;
+        WhirCfg c;
+        auto irs = [&](const u64* w) {
+            IrsCfg r;
+            r.num_vectors = 1;
+            r.vector_size = w[0];
+            r.codeword_length = w[1];
+            r.depth = w[2];
+            r.in_domain = w[3];
+            r.out_domain = w[4];
+            return r;
+        };
+        c.initial = irs(cfg);
+        c.initial.num_vectors = batch_size;
+        c.initial_sumcheck = {cfg[0], cfg[5], cfg[6]};
+        c.initial_skip_pow = cfg[7];
+        const u64 R = cfg[8];
+        if (cfg_len != 12 + 8 * R) return 2;
+        u64 size = cfg[0] >> cfg[5];
+        for (u64 r = 0; r < R; ++r) {
+            const u64* w = cfg + 9 + 8 * r;
+            RoundCfg rc;
+            rc.irs = irs(w);
+            rc.pow_threshold = w[5];
+            rc.sumcheck = {w[0], w[6], w[7]};
+            c.rounds.push_back(rc);
+            size = w[0] >> w[6];
+        }
+        const u64* f = cfg + 9 + 8 * R;
+        c.final_sumcheck = {size, f[0], f[1]};
+        c.final_pow = f[2];
+        const u64 V = batch_size * num_witnesses, vsize = cfg[0];
+        std::vector<std::vector<u64>> vs(V);
+        for (u64 j = 0; j < V; ++j) vs[j].assign(coeffs + j * vsize, coeffs + (j + 1) * vsize);
+        u64 n = 0;
+        while ((1ull << n) < vsize) ++n;
+        Statement st;
+        const u64* d = form_data;
+        for (size_t k = 0; k < nforms; ++k) {
+            if (kinds[k] == 0) {
+                st.mle_points.push_back(read_e3(d, n));
+                d += 3 * n;
+            } else {
+                st.covectors.push_back(read_e3(d, vsize));
+                d += 3 * vsize;
+            }
+            st.dense.push_back(kinds[k] != 0);
+        }
+        st.evaluations = read_e3(evals, nforms * V);
+        DomainSep ds;
+        std::memcpy(ds.protocol_id, ds96, 64);
+        std::memcpy(ds.session_id, ds96 + 64, 32);
+        ProofOut o = prove_cfg(c, sha2 ? Engine::Sha2 : Engine::Blake3, deg, batch_size, vs, num_witnesses, st, ds);
+        lens[0] = o.narg.size();
+        lens[1] = o.hints.size();
+        lens[2] = o.evaluation_point.size();
+        std::memcpy(narg, o.narg.data(), std::min(narg_cap, o.narg.size()));
+        std::memcpy(hints, o.hints.data(), std::min(hints_cap, o.hints.size()));
+        for (size_t k = 0; k < o.evaluation_point.size() && k < eval_point_cap; ++k)
+            for (int j = 0; j < 3; ++j) eval_point[3 * k + j] = o.evaluation_point[k].c[j];
+        return 0;
+    } catch (const std::exception&) {
+        return 1;
+    }
+}
+
 // Commit of num_witnesses witnesses of batch_size vectors each, then one
 // prove over all of them.  coeffs: num_witnesses * batch_size vectors of 2^n
 // words, back to back; evals: npoints * num_vectors Ext3 values, form-major.

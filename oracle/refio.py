@@ -192,6 +192,9 @@ class Oracle:
         L.oracle_whir_prove_forms.argtypes = [u64, u64, u64, u64, u64, ctypes.c_int, u64, u64, p, p, sz, p, p, p,
                                               sz, p, sz, p, ctypes.c_int]
         L.oracle_whir_prove_forms.restype = ctypes.c_int
+        L.oracle_whir_prove_config.argtypes = [p, sz, ctypes.c_int, ctypes.c_int, p, u64, u64, p, p, sz, p, p, p, sz,
+                                               p, sz, p, p, sz]
+        L.oracle_whir_prove_config.restype = ctypes.c_int
 
     # -- primitives -------------------------------------------------------
     def blake3(self, data: bytes) -> bytes:
@@ -329,3 +332,26 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle prove failed")
         return narg.raw[:lens[0]], hints.raw[:lens[1]]
+
+    def prove_config(self, cfg_words, ds96, forms, coeffs, evaluations, batch_size=1, num_witnesses=1, deg=3,
+                     sha2=False):
+        """Commit + prove for an explicit Config (word layout in oracle_capi.cpp)
+        and domain separator; returns (narg, hints, evaluation_point (k, 3))."""
+        cfg = np.ascontiguousarray(cfg_words, dtype=np.uint64)
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
+        kinds = (ctypes.c_int * max(len(forms), 1))(*[0 if kd == "mle" else 1 for kd, _ in forms])
+        data = np.concatenate([np.ascontiguousarray(d, dtype=np.uint64).reshape(-1) for _, d in forms]) \
+            if forms else np.zeros(1, dtype=np.uint64)
+        evals = np.ascontiguousarray(evaluations, dtype=np.uint64).reshape(-1, 3)
+        cap = 16 << 20
+        narg = ctypes.create_string_buffer(cap)
+        hints = ctypes.create_string_buffer(cap)
+        lens = (ctypes.c_uint64 * 3)()
+        ep = np.zeros((64, 3), dtype=np.uint64)
+        rc = self.lib.oracle_whir_prove_config(cfg.ctypes.data, cfg.size, deg, int(sha2), bytes(ds96), batch_size,
+                                               num_witnesses, coeffs.ctypes.data, kinds, len(forms),
+                                               data.ctypes.data, evals.ctypes.data, narg, cap, hints, cap, lens,
+                                               ep.ctypes.data, 64)
+        if rc != 0:
+            raise RuntimeError("oracle prove failed")
+        return narg.raw[:lens[0]], hints.raw[:lens[1]], ep[:lens[2]]

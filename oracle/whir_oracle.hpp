@@ -424,6 +424,21 @@ struct Transcript {
         for (int i = 0; i < 3; ++i) r.c[i] = decode40(b + 40 * i);
         return r;
     }
+    // The protocol's target field: Ext3 (Basefield<GoldilocksExt3>, deg 3) or the
+    // base field itself (Identity<Goldilocks>, deg 1), whose elements are kept
+    // here as Ext3 values (x, 0, 0) -- the base field is a subfield, so the
+    // arithmetic is unchanged -- and cross the transcript as 8 bytes / 40-byte
+    // challenges (transcript.hpp:375-453).
+    int deg = 3;
+    E3 challenge_t() { return deg == 1 ? E3::from_base(challenge_base()) : challenge_e3(); }
+    void message_t(const E3& v) {
+        if (deg == 1) {
+            if (v.c[1] || v.c[2]) throw std::runtime_error("base-field message outside the subfield");
+            message_u64(v.c[0]);
+        } else {
+            message_e3(v);
+        }
+    }
 };
 
 // ---------------------------------------------------------------------------
@@ -538,12 +553,12 @@ struct WhirCfg {
 inline u64 pow_threshold_of(double diff) {
     return diff <= 0.0 ? ~0ull : (u64)std::ceil(std::exp2(64.0 - diff));
 }
-inline WhirCfg whir_from_params(u64 size, const Params& p) {
+// fbits = Target::field_size_bits: 192 for Ext3, 64 for Identity<Goldilocks>.
+inline WhirCfg whir_from_params(u64 size, const Params& p, double fbits = 192.0) {
     if (!size || (size & (size - 1))) throw std::runtime_error("size must be a power of two");
     WhirCfg c;
     const double sec = (double)p.security_level;
     const double psec = (double)(p.security_level - p.pow_bits);
-    const double fbits = 192.0;
     u64 lir = p.starting_log_inv_rate;
     u64 nv = 0;
     for (u64 s = size; s > 1; s >>= 1) ++nv;
@@ -750,7 +765,7 @@ inline std::vector<E3> geometric(const E3& x, size_t n) {  // utilities.hpp:85-9
 inline std::vector<E3> geometric_challenge(Transcript& t, size_t n) {  // geometric_challenge.hpp:39-44
     if (n == 0) return {};
     if (n == 1) return {E3::one()};
-    return geometric(t.challenge_e3(), n);
+    return geometric(t.challenge_t(), n);
 }
 // acc[i] += scalar * eq(point, i), point[0] <-> most significant bit of i (multilinear.hpp:121-133)
 inline void eval_eq_acc(std::vector<E3>& acc, const std::vector<E3>& pt, const E3& scalar) {
@@ -824,10 +839,10 @@ inline std::vector<E3> sumcheck_prove(Transcript& t, const SumcheckCfg& cfg, std
             c2 = c2 + (a[h + i] - a[i]) * (b[h + i] - b[i]);
         }
         E3 c1 = sum - (c0 + c0) - c2;
-        t.message_e3(c0);
-        t.message_e3(c2);
+        t.message_t(c0);
+        t.message_t(c2);
         pow_prove(t, cfg.pow_threshold, eng);
-        E3 rnd = t.challenge_e3();
+        E3 rnd = t.challenge_t();
         rs.push_back(rnd);
         fold(a, rnd);
         fold(b, rnd);
@@ -869,11 +884,11 @@ inline Witness commit_base_multi(Transcript& t, const IrsCfg& c, const std::vect
     }
     w.nodes = merkle_build(leaves_base(w.mat_base, cols, eng), eng);
     t.message_hash(w.root());
-    for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_e3());
+    for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_t());
     for (const E3& z : w.ood_points)
         for (u64 v = 0; v < w.nvec; ++v) {
             E3 val = univariate_eval_base(*vs[v], z);
-            t.message_e3(val);
+            t.message_t(val);
             w.ood_values.push_back(val);
         }
     return w;
@@ -887,10 +902,10 @@ inline Witness commit_e3(Transcript& t, const IrsCfg& c, const std::vector<E3>& 
     w.mat_e3 = rs_encode_e3(v, w.N, w.depth);
     w.nodes = merkle_build(leaves_e3(w.mat_e3, w.depth, eng), eng);
     t.message_hash(w.root());
-    for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_e3());
+    for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_t());
     for (const E3& z : w.ood_points) {
         E3 val = univariate_eval_e3(v, z);
-        t.message_e3(val);
+        t.message_t(val);
         w.ood_values.push_back(val);
     }
     return w;
@@ -977,15 +992,19 @@ struct Statement {
 };
 struct ProofOut { std::vector<u8> narg, hints; std::vector<E3> evaluation_point; Hash initial_root{}; };
 
-inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>& vs, u64 num_witnesses,
-                            const Statement& st, const DomainSep& ds) {
-    const u64 B = p.batch_size, W = num_witnesses, V = vs.size();
+// Commit + prove for an explicit configuration (a Config built field by field,
+// as the reference's golden dumper does, or from_params), target field of
+// degree `deg` (3: Basefield<GoldilocksExt3>, 1: Identity<Goldilocks>).
+inline ProofOut prove_cfg(const WhirCfg& cfg, Engine eng, int deg, u64 B, const std::vector<std::vector<u64>>& vs,
+                          u64 num_witnesses, const Statement& st, const DomainSep& ds) {
+    const u64 W = num_witnesses, V = vs.size();
     if (B == 0 || W == 0 || V != W * B) throw std::runtime_error("vectors != witnesses * batch_size");
+    if (deg != 1 && deg != 3) throw std::runtime_error("target field degree must be 1 or 3");
     const u64 size = vs[0].size();
     for (const auto& v : vs) if (v.size() != size) throw std::runtime_error("vector sizes differ");
-    WhirCfg cfg = whir_from_params(size, p);
-    const Engine eng = std::memcmp(p.hash_id, SHA2_ENGINE_ID, 32) == 0 ? Engine::Sha2 : Engine::Blake3;
+    if (cfg.initial.vector_size != size) throw std::runtime_error("config size != vector size");
     Transcript t;
+    t.deg = deg;
     t.absorb(ds.protocol_id, 64);
     t.absorb(ds.session_id, 32);
     ProofOut out;
@@ -1011,7 +1030,7 @@ inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>
                     oods_mat.push_back(wits[w].ood_values[e * B + (j - w * B)]);
                 } else {
                     E3 val = univariate_eval_base(vs[j], z);
-                    t.message_e3(val);
+                    t.message_t(val);
                     oods_mat.push_back(val);
                 }
             }
@@ -1055,7 +1074,7 @@ inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>
     std::vector<E3> last_r;
     if (has_constraints) last_r = sumcheck_prove(t, cfg.initial_sumcheck, vec, cov, sum, eng);
     else {
-        for (u64 r = 0; r < cfg.initial_sumcheck.num_rounds; ++r) last_r.push_back(t.challenge_e3());
+        for (u64 r = 0; r < cfg.initial_sumcheck.num_rounds; ++r) last_r.push_back(t.challenge_t());
         pow_prove(t, cfg.initial_skip_pow, eng);
         for (const E3& r : last_r) fold(vec, r);
         cov.assign(cfg.initial_sumcheck.initial_size >> cfg.initial_sumcheck.num_rounds, E3());
@@ -1071,7 +1090,13 @@ inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>
     stored.reserve(cfg.rounds.size());
     for (size_t rd = 0; rd < cfg.rounds.size(); ++rd) {
         const RoundCfg& rc = cfg.rounds[rd];
-        stored.push_back(commit_e3(t, rc.irs, vec, eng));
+        if (deg == 1) {  // base-field round vector: 8-byte row elements
+            std::vector<u64> b(vec.size());
+            for (size_t i = 0; i < vec.size(); ++i) b[i] = vec[i].c[0];
+            stored.push_back(commit_base(t, rc.irs, b, eng));
+        } else {
+            stored.push_back(commit_e3(t, rc.irs, vec, eng));
+        }
         const Witness& nw = stored.back();
         pow_prove(t, rc.pow_threshold, eng);
         Opening o = open_witnesses(t, *prev_cfg, prev);
@@ -1097,7 +1122,7 @@ inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>
         wrlc = {E3::one()};
     }
     // steps 7-10
-    for (const E3& c : vec) t.message_e3(c);
+    for (const E3& c : vec) t.message_t(c);
     pow_prove(t, cfg.final_pow, eng);
     open_witnesses(t, *prev_cfg, prev);
     auto fr = sumcheck_prove(t, cfg.final_sumcheck, vec, cov, sum, eng);
@@ -1105,6 +1130,13 @@ inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>
     out.narg = std::move(t.narg);
     out.hints = std::move(t.hints);
     return out;
+}
+inline ProofOut prove_multi(const Params& p, const std::vector<std::vector<u64>>& vs, u64 num_witnesses,
+                            const Statement& st, const DomainSep& ds, int deg = 3) {
+    if (vs.empty()) throw std::runtime_error("no vectors");
+    const WhirCfg cfg = whir_from_params(vs[0].size(), p, deg == 1 ? 64.0 : 192.0);
+    const Engine eng = std::memcmp(p.hash_id, SHA2_ENGINE_ID, 32) == 0 ? Engine::Sha2 : Engine::Blake3;
+    return prove_cfg(cfg, eng, deg, p.batch_size, vs, num_witnesses, st, ds);
 }
 inline ProofOut prove(const Params& p, const std::vector<u64>& v, const Statement& st, const DomainSep& ds) {
     if (p.batch_size != 1) throw std::runtime_error("prove(): one vector; use prove_multi");

@@ -5,7 +5,8 @@ has the reference checkout; the tests only read the JSON files).
 1. reference_goldens.json -- the known-answer vectors of the reference's own
    golden dumps (cpp/dump_output/*/golden_*_cpp.txt, identical to the
    *_rs.txt dumps of the Rust crate for these sections), restricted to the
-   sections on the WHIR path: field arithmetic (base, Ext3), BLAKE3 hashes,
+   sections on the WHIR path: whole WHIR proofs (whir_output, Identity<Goldilocks>,
+   identical in the Rust and C++ dumps), field arithmetic (base, Ext3), BLAKE3 hashes,
    Merkle roots and opening hints, matrix-commit leaves, challenge indices and
    proof of work; plus the base-field sumcheck transcript, taken from the
    reference's sumcheck dumper rebuilt from its current sources (its committed
@@ -359,11 +360,45 @@ def proofs_unique():
     return out
 
 
+WHIR_GOLDEN_SHAPES = [(1, 2), (1, 4), (1, 8), (3, 4), (4, 8)]  # (num_vectors, vector_size), cpp/tests/dump_whir.cpp:197-205
+
+
+def whir_golden():
+    """The reference's whole-proof golden (cpp/tests/dump_whir.cpp; the Rust
+    dump golden_whir_rs.txt is byte-identical to the C++ one): Identity<Goldilocks>,
+    a Config built field by field (depth 1, codeword 2x, 1 OOD sample,
+    min(size, 3) queries, SHA-2 Merkle, no initial sumcheck round, no STIR round,
+    final sumcheck to size 1, no PoW), one all-ones Covector form, the domain
+    separator SHA3-512(CBOR uint 0xBEEF) / SHA3-256(CBOR text "whir_<case>")."""
+    rs = read(f"{DUMPS}/whir_output/golden_whir_rs.txt")
+    cpp = read(f"{DUMPS}/whir_output/golden_whir_cpp.txt")
+    assert rs.replace("\r", "") == cpp.replace("\r", ""), "Rust and C++ WHIR goldens differ"
+    out = []
+    for i, c in enumerate(cases(sections(rs)["whir"])):
+        nvec, size = WHIR_GOLDEN_SHAPES[i]
+        rows = {}
+        for r in c["rows"]:
+            k, _, v = r.partition(" ")
+            rows[k] = v.split()
+        rec = {"case": i, "num_vectors": nvec, "vector_size": size,
+               "inputs": [[int(x) for x in rows[f"input_vector{v}"]] for v in range(nvec)],
+               "witness_matrix": [int(x) for x in rows["witness_matrix"]],
+               "ood_points": [int(x) for x in rows["ood_points"]],
+               "ood_matrix": [int(x) for x in rows["ood_matrix"]],
+               "eval_point": [int(x) for x in rows["eval_point"]],
+               "rlc_coeffs": [int(x) for x in rows["rlc_coeffs"]],
+               "narg": rows["proof_narg"][0], "hints": rows["proof_hints"][0],
+               "check_eof": int(rows["check_eof"][0])}
+        assert all(len(v) == size for v in rec["inputs"])
+        out.append(rec)
+    return out
+
+
 def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
             "indices": indices(), "pow": pow_golden(), "sumcheck": sumcheck(),
-            "sha2": hashes("sha2"), "merkle_sha2": merkle("sha2")}
+            "sha2": hashes("sha2"), "merkle_sha2": merkle("sha2"), "whir": whir_golden()}
     with open(os.path.join(HERE, "reference_goldens.json"), "w") as f:
         json.dump(gold, f, indent=1)
     with open(os.path.join(HERE, "reference_proofs.json"), "w") as f:

@@ -272,3 +272,38 @@ def test_oracle_unique_decoding_matches_reference_fixtures(oracle, case):
     assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
     if "narg" in case:
         assert narg.hex() == case["narg"] and hints.hex() == case["hints"]
+
+
+def whir_golden_config(case):
+    """The Config of cpp/tests/dump_whir.cpp:run_case as oracle/GPU config words:
+    depth 1, codeword 2x, min(size, 3) queries, 1 OOD sample, no initial
+    sumcheck round, no STIR round, final sumcheck to size 1, no PoW."""
+    size = case["vector_size"]
+    none = (1 << 64) - 1
+    log_size = size.bit_length() - 1
+    return [size, 2 * size, 1, min(size, 3), 1, 0, none, none, 0, log_size, none, none]
+
+
+def whir_golden_ds(case):
+    proto = hashlib.sha3_512(bytes([0x19, 0xBE, 0xEF])).digest()
+    label = f"whir_{case['case']}".encode()
+    sess = hashlib.sha3_256(bytes([0x60 + len(label)]) + label).digest()
+    return proto + sess
+
+
+@pytest.mark.parametrize("case", GOLD["whir"], ids=lambda c: f"case{c['case']}")
+def test_oracle_matches_reference_whir_golden(oracle, case):
+    """Whole proofs of the reference's WHIR golden dump (C++ and Rust identical):
+    Identity<Goldilocks>, SHA-2 Merkle, a hand-built Config, one all-ones
+    Covector form, several vectors in cases 3 and 4."""
+    P = 0xFFFFFFFF00000001
+    size = case["vector_size"]
+    coeffs = np.array(case["inputs"], dtype=np.uint64)
+    ones = np.zeros((size, 3), dtype=np.uint64)
+    ones[:, 0] = 1
+    evals = np.array([[sum(v) % P, 0, 0] for v in case["inputs"]], dtype=np.uint64)
+    narg, hints, ep = oracle.prove_config(whir_golden_config(case), whir_golden_ds(case), [("covector", ones)], coeffs,
+                                          evals, batch_size=case["num_vectors"], deg=1, sha2=True)
+    assert narg.hex() == case["narg"]
+    assert hints.hex() == case["hints"]
+    assert [int(x) for x in ep[:, 0]] == case["eval_point"] and not ep[:, 1:].any()
