@@ -113,6 +113,49 @@ whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* ctx, const whirgpu_params* 
                                         whirgpu_transcript* tx, whirgpu_witness** out);
 void whirgpu_witness_destroy(whirgpu_witness* w);
 
+/* ---- a Config given field by field -----------------------------------------------
+ * Config<M> (whir.hpp:104-116) as the reference's callers can also build it
+ * by hand (cpp/tests/dump_whir.cpp:121-148), and the embedding M: the CLI's
+ * --field Goldilocks3 (Basefield<GoldilocksExt3>, the default) or Goldilocks1
+ * (Identity<Goldilocks>: challenges, sums and messages in the base field).
+ * Each committer's interleaving depth is 2^(rounds of the sumcheck after it) and
+ * sizes chain from round to round (checked; WHIRGPU_E_INVALID otherwise). */
+#define WHIRGPU_FIELD_GOLDILOCKS1 1
+#define WHIRGPU_FIELD_GOLDILOCKS3 3
+#define WHIRGPU_MAX_ROUNDS 24
+typedef struct {
+    uint64_t vector_size, codeword_length, interleaving_depth, in_domain_samples, out_domain_samples;
+} whirgpu_irs_config;
+typedef struct {
+    uint64_t num_rounds;
+    uint64_t pow_threshold; /* UINT64_MAX: no PoW */
+} whirgpu_sumcheck_config;
+typedef struct {
+    whirgpu_irs_config irs_committer;
+    uint64_t pow_threshold;
+    whirgpu_sumcheck_config sumcheck;
+} whirgpu_round_config;
+typedef struct {
+    uint32_t field;         /* WHIRGPU_FIELD_GOLDILOCKS3 / _GOLDILOCKS1 */
+    uint64_t batch_size;    /* vectors per commitment (initial_committer.num_vectors) */
+    uint8_t hash_id[32];    /* engine of every Merkle layer and PoW */
+    whirgpu_irs_config initial_committer;
+    whirgpu_sumcheck_config initial_sumcheck;
+    uint64_t initial_skip_pow;
+    uint64_t num_rounds;
+    whirgpu_round_config round_configs[WHIRGPU_MAX_ROUNDS];
+    whirgpu_sumcheck_config final_sumcheck;
+    uint64_t final_pow;
+} whirgpu_config;
+/* Config::from_params (whir.hpp:118-224) for the given field. */
+whirgpu_status whirgpu_config_from_params(const whirgpu_params* params, uint64_t num_variables, uint32_t field,
+                                          whirgpu_config* out);
+/* whirgpu_commit_witnesses for a Config given field by field;
+ * num_variables = log2(initial_committer.vector_size). */
+whirgpu_status whirgpu_commit_config(whirgpu_ctx* ctx, const whirgpu_config* config, const uint64_t* coeffs,
+                                     uint64_t num_witnesses, int coeffs_location, whirgpu_transcript* tx,
+                                     whirgpu_witness** out);
+
 /* ---- prove (Config::prove, whir_prover.hpp:56-407) ---------------------------
  * Statement: num_points MultilinearExtension forms; points are
  * num_points * num_variables Ext3 coordinates (3 words each, c0 c1 c2),

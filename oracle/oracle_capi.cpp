@@ -186,13 +186,16 @@ int oracle_whir_prove(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique, cons
 // Commit + prove with a statement of mixed forms: kinds[f] = 0 MultilinearExtension
 // (n Ext3 coordinates), 1 dense Covector (2^n Ext3 values); form_data holds the
 // forms' words back to back in form order.  evals: nforms * V values, form-major.
+// flags: bit 0 SHA-2 engine, bit 1 Identity<Goldilocks> target (base-field
+// values given as (x, 0, 0)).
 int oracle_whir_prove_forms(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique, u64 batch_size, u64 num_witnesses,
                             const u64* coeffs, const int* kinds, size_t nforms, const u64* form_data, const u64* evals,
                             u8* narg, size_t narg_cap, u8* hints, size_t hints_cap, u64* lens, int sha2) {
     try {
         Params p = make_params(rho, k, sec, powb, unique);
         p.batch_size = batch_size;
-        if (sha2) std::memcpy(p.hash_id, SHA2_ENGINE_ID, 32);
+        if (sha2 & 1) std::memcpy(p.hash_id, SHA2_ENGINE_ID, 32);
+        const int deg = (sha2 & 2) ? 1 : 3;
         const u64 V = batch_size * num_witnesses, size = 1ull << n;
         std::vector<std::vector<u64>> vs(V);
         for (u64 j = 0; j < V; ++j) vs[j].assign(coeffs + j * size, coeffs + (j + 1) * size);
@@ -209,7 +212,7 @@ int oracle_whir_prove_forms(u64 n, u64 rho, u64 k, u64 sec, u64 powb, int unique
             st.dense.push_back(kinds[f] != 0);
         }
         st.evaluations = read_e3(evals, nforms * V);
-        ProofOut o = prove_multi(p, vs, num_witnesses, st, cli_domain_separator(p));
+        ProofOut o = prove_multi(p, vs, num_witnesses, st, cli_domain_separator(p), deg);
         lens[0] = o.narg.size();
         lens[1] = o.hints.size();
         std::memcpy(narg, o.narg.data(), std::min(narg_cap, o.narg.size()));

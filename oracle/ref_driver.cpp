@@ -8,7 +8,8 @@
 // as the timed reference CPU prover.
 //
 // Call chain mirrored from the reference CLI `run_pcs` (cpp/main.cpp:292-467):
-//   Config<Basefield<GoldilocksExt3>>::from_params (whir.hpp:118)
+//   Config<M>::from_params (whir.hpp:118), M = Basefield<GoldilocksExt3>, or
+//   Identity<Goldilocks> with --field1 (the CLI's --field Goldilocks1)
 //   ProverState::from_ds(ds, Empty)               (transcript.hpp:605)
 //   config.commit / config.prove                   (whir.hpp:303, whir_prover.hpp:56)
 // with the domain separator of `make_rust_cli_domain_separator`
@@ -48,14 +49,15 @@
 #include <memory>
 #include <span>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
-using M = ::whir::algebra::Basefield<::whir::algebra::GoldilocksExt3>;
-using Source = M::Source;
-using Target = M::Target;
+using Source = ::whir::algebra::Goldilocks;
+using M3 = ::whir::algebra::Basefield<::whir::algebra::GoldilocksExt3>;  // --field Goldilocks3 (default)
+using M1 = ::whir::algebra::Identity<::whir::algebra::Goldilocks>;       // --field Goldilocks1
 
 [[noreturn]] void die(const char* msg) {
     std::fprintf(stderr, "ref_driver: %s\n", msg);
@@ -130,76 +132,69 @@ void cbor_params(std::vector<std::uint8_t>& out, const ::whir::ProtocolParameter
 void put_u64(FILE* f, std::uint64_t v) { std::fwrite(&v, 8, 1, f); }
 void put_f64(FILE* f, double v) { std::fwrite(&v, 8, 1, f); }
 
-}  // namespace
-
-int main(int argc, char** argv) {
-    if (argc < 3) {
-        std::fprintf(stderr, "usage: ref_driver INPUT OUTPUT [--verify] [--reps R] [--config] [--sha2] [--unique]\n");
-        return 2;
+// Target-field element from three input words (c0 c1 c2); a base-field target
+// takes c0 and requires c1 = c2 = 0.
+template <typename T>
+T make_target(std::uint64_t a, std::uint64_t b, std::uint64_t c) {
+    if constexpr (std::is_same_v<T, ::whir::algebra::Goldilocks>) {
+        if (b || c) die("base-field target given an extension element");
+        return T::from_u64(a);
+    } else {
+        return T(Source::from_u64(a), Source::from_u64(b), Source::from_u64(c));
     }
+}
+template <typename T>
+void put_target(FILE* f, const T& e) {
+    if constexpr (std::is_same_v<T, ::whir::algebra::Goldilocks>) {
+        put_u64(f, e.as_canonical_u64());
+        put_u64(f, 0);
+        put_u64(f, 0);
+    } else {
+        put_u64(f, e.c0().as_canonical_u64());
+        put_u64(f, e.c1().as_canonical_u64());
+        put_u64(f, e.c2().as_canonical_u64());
+    }
+}
+
+// Parsed input file and flags.
+struct Job {
+    std::size_t n = 0, k = 0, rho = 0, sec = 0, powb = 0, npts = 0, batch = 1, nwit = 1;
+    std::vector<bool> dense;
+    std::vector<std::vector<std::uint64_t>> forms;  // 3 words per element
+    std::vector<std::vector<Source>> vecs;
     bool do_verify = false, print_cfg = false, use_sha2 = false, unique = false;
     int reps = 1;
-    for (int i = 3; i < argc; ++i) {
-        if (!std::strcmp(argv[i], "--verify")) do_verify = true;
-        else if (!std::strcmp(argv[i], "--config")) print_cfg = true;
-        else if (!std::strcmp(argv[i], "--sha2")) use_sha2 = true;
-        else if (!std::strcmp(argv[i], "--unique")) unique = true;
-        else if (!std::strcmp(argv[i], "--reps") && i + 1 < argc) reps = std::atoi(argv[++i]);
-        else die("bad flag");
-    }
-    auto buf = read_file(argv[1]);
-    Reader rd{buf};
-    if (rd.u32() != 0x49524857u) die("bad magic");
-    const std::uint32_t version = rd.u32();
-    if (version < 1u || version > 3u) die("bad version");
-    const std::size_t n = rd.u64();
-    const std::size_t k = rd.u64();
-    const std::size_t rho = rd.u64();
-    const std::size_t sec = rd.u64();
-    const std::size_t powb = rd.u64();
-    const std::size_t npts = rd.u64();
-    const std::size_t batch = version >= 2u ? rd.u64() : 1;
-    const std::size_t nwit = version >= 2u ? rd.u64() : 1;
-    if (n >= 40) die("num_variables too large");
-    if (batch == 0 || nwit == 0 || batch * nwit > 64) die("bad vector count");
-    const std::size_t nvec = batch * nwit;
+    const char* out_path = nullptr;
+};
 
-    const std::size_t size = std::size_t{1} << n;
-    auto read_target = [&rd]() {
-        auto a = rd.u64(), b = rd.u64(), d = rd.u64();
-        return Target(Source::from_u64(a), Source::from_u64(b), Source::from_u64(d));
-    };
-    std::vector<bool> dense(npts, false);
-    std::vector<std::vector<Target>> points(npts);  // MLE point, or the covector's values
-    for (std::size_t f = 0; f < npts; ++f) {
-        if (version == 3u) {
-            const std::uint64_t kind = rd.u64();
-            if (kind > 1) die("bad form kind");
-            dense[f] = kind == 1;
-        }
-        points[f].resize(dense[f] ? size : n);
-        for (auto& c : points[f]) c = read_target();
-    }
+}  // namespace
+
+template <typename M>
+int run(const Job& j) {
+    using Target = typename M::Target;
+    const std::size_t n = j.n, npts = j.npts, batch = j.batch, nwit = j.nwit, size = std::size_t{1} << n;
+    const auto& vecs = j.vecs;
+    const int reps = j.reps;
+    std::vector<std::vector<Target>> points(npts);
+    for (std::size_t f = 0; f < npts; ++f)
+        for (std::size_t e = 0; e < j.forms[f].size() / 3; ++e)
+            points[f].push_back(make_target<Target>(j.forms[f][3 * e], j.forms[f][3 * e + 1], j.forms[f][3 * e + 2]));
     auto make_form = [&](std::size_t f) -> std::unique_ptr<::whir::algebra::LinearForm<Target>> {
-        if (dense[f]) return std::make_unique<::whir::algebra::Covector<Target>>(points[f]);
+        if (j.dense[f]) return std::make_unique<::whir::algebra::Covector<Target>>(points[f]);
         return std::make_unique<::whir::algebra::MultilinearExtension<Target>>(points[f]);
     };
-    std::vector<std::vector<Source>> vecs(nvec, std::vector<Source>(size));
-    for (auto& vec : vecs)
-        for (auto& v : vec) v = Source::from_u64(rd.u64());
-
     ::whir::ProtocolParameters params;
-    params.security_level = sec;
-    params.pow_bits = powb;
-    params.initial_folding_factor = k;
-    params.folding_factor = k;
-    params.unique_decoding = unique;
-    params.starting_log_inv_rate = rho;
+    params.security_level = j.sec;
+    params.pow_bits = j.powb;
+    params.initial_folding_factor = j.k;
+    params.folding_factor = j.k;
+    params.unique_decoding = j.unique;
+    params.starting_log_inv_rate = j.rho;
     params.batch_size = batch;
-    params.hash_id = use_sha2 ? ::whir::hash::ENGINE_ID_SHA2 : ::whir::hash::ENGINE_ID_BLAKE3;
+    params.hash_id = j.use_sha2 ? ::whir::hash::ENGINE_ID_SHA2 : ::whir::hash::ENGINE_ID_BLAKE3;
 
     auto config = ::whir::protocols::whir::Config<M>::from_params(size, params);
-    if (print_cfg) {
+    if (j.print_cfg) {
         std::printf("initial codeword %zu q %zu ood %zu\n",
             config.initial_committer.codeword_length,
             config.initial_committer.in_domain_samples,
@@ -224,7 +219,7 @@ int main(int argc, char** argv) {
     std::vector<Target> evaluations;  // form-major, as Config::prove expects (whir_prover.hpp:77)
     for (std::size_t f = 0; f < npts; ++f) {
         for (const auto& vec : vecs) {
-            if (dense[f]) {
+            if (j.dense[f]) {
                 ::whir::algebra::Covector<Target> cv(points[f]);
                 evaluations.push_back(cv.template evaluate<M>(emb, std::span<const Source>{vec}));
             } else {
@@ -262,7 +257,7 @@ int main(int argc, char** argv) {
     }
 
     double verify_ok = -1.0;
-    if (do_verify) {
+    if (j.do_verify) {
         auto vs = ::whir::transcript::VerifierState::from_ds(ds, instance, proof);
         std::vector<::whir::protocols::irs_commit::Commitment<Target>> comms;
         for (std::size_t w = 0; w < nwit; ++w) comms.push_back(config.receive_commitment(vs));
@@ -278,20 +273,70 @@ int main(int argc, char** argv) {
         verify_ok = (claim.verify(refs) && vs.check_eof()) ? 1.0 : 0.0;
     }
 
-    FILE* f = std::fopen(argv[2], "wb");
+    FILE* f = std::fopen(j.out_path, "wb");
     if (!f) die("cannot open output");
     put_u64(f, proof.narg_string.size());
     std::fwrite(proof.narg_string.data(), 1, proof.narg_string.size(), f);
     put_u64(f, proof.hints.size());
     std::fwrite(proof.hints.data(), 1, proof.hints.size(), f);
-    for (const auto& e : evaluations) {
-        put_u64(f, e.c0().as_canonical_u64());
-        put_u64(f, e.c1().as_canonical_u64());
-        put_u64(f, e.c2().as_canonical_u64());
-    }
+    for (const auto& e : evaluations) put_target(f, e);
     put_f64(f, commit_ms);
     put_f64(f, prove_ms);
     put_f64(f, verify_ok);
     std::fclose(f);
     return 0;
 }
+
+int main(int argc, char** argv) {
+    if (argc < 3) {
+        std::fprintf(stderr, "usage: ref_driver INPUT OUTPUT [--verify] [--reps R] [--config] [--sha2] [--unique] [--field1]\n");
+        return 2;
+    }
+    Job j;
+    j.out_path = argv[2];
+    bool field1 = false;
+    for (int i = 3; i < argc; ++i) {
+        if (!std::strcmp(argv[i], "--verify")) j.do_verify = true;
+        else if (!std::strcmp(argv[i], "--config")) j.print_cfg = true;
+        else if (!std::strcmp(argv[i], "--sha2")) j.use_sha2 = true;
+        else if (!std::strcmp(argv[i], "--unique")) j.unique = true;
+        else if (!std::strcmp(argv[i], "--field1")) field1 = true;
+        else if (!std::strcmp(argv[i], "--reps") && i + 1 < argc) j.reps = std::atoi(argv[++i]);
+        else die("bad flag");
+    }
+    auto buf = read_file(argv[1]);
+    Reader rd{buf};
+    if (rd.u32() != 0x49524857u) die("bad magic");
+    const std::uint32_t version = rd.u32();
+    if (version < 1u || version > 3u) die("bad version");
+    const std::size_t n = rd.u64();
+    const std::size_t k = rd.u64();
+    const std::size_t rho = rd.u64();
+    const std::size_t sec = rd.u64();
+    const std::size_t powb = rd.u64();
+    const std::size_t npts = rd.u64();
+    const std::size_t batch = version >= 2u ? rd.u64() : 1;
+    const std::size_t nwit = version >= 2u ? rd.u64() : 1;
+    if (n >= 40) die("num_variables too large");
+    if (batch == 0 || nwit == 0 || batch * nwit > 64) die("bad vector count");
+    const std::size_t nvec = batch * nwit;
+
+    const std::size_t size = std::size_t{1} << n;
+    j.n = n; j.k = k; j.rho = rho; j.sec = sec; j.powb = powb; j.npts = npts; j.batch = batch; j.nwit = nwit;
+    j.dense.assign(npts, false);
+    j.forms.resize(npts);  // MLE point, or the covector's values
+    for (std::size_t f = 0; f < npts; ++f) {
+        if (version == 3u) {
+            const std::uint64_t kind = rd.u64();
+            if (kind > 1) die("bad form kind");
+            j.dense[f] = kind == 1;
+        }
+        j.forms[f].resize(3 * (j.dense[f] ? size : n));
+        for (auto& w : j.forms[f]) w = rd.u64();
+    }
+    j.vecs.assign(nvec, std::vector<Source>(size));
+    for (auto& vec : j.vecs)
+        for (auto& v : vec) v = Source::from_u64(rd.u64());
+    return field1 ? run<M1>(j) : run<M3>(j);
+}
+

@@ -79,7 +79,8 @@ def ref_available() -> bool:
 
 
 def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1, threads=None,
-                  timeout=3600, sha2=False, batch_size=1, num_witnesses=1, forms=None, unique=False) -> RefProof:
+                  timeout=3600, sha2=False, batch_size=1, num_witnesses=1, forms=None, unique=False,
+                  field1=False) -> RefProof:
     """Runs the unmodified reference prover (compiled in place by oracle/Makefile).
     With several vectors the evaluations come back form-major, (num_forms * V, 3).
     ``forms`` (see write_input) replaces ``points`` for mixed MLE / Covector statements."""
@@ -97,6 +98,8 @@ def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1
             cmd.append("--sha2")
         if unique:
             cmd.append("--unique")
+        if field1:
+            cmd.append("--field1")
         subprocess.run(cmd, check=True, env=env, timeout=timeout, stdout=subprocess.DEVNULL)
         return read_output(out, npts, batch_size * num_witnesses)
 
@@ -314,7 +317,7 @@ class Oracle:
         return narg.raw[:lens[0]], hints.raw[:lens[1]]
 
     def prove_forms(self, n, k, rho, sec, pow_bits, forms, coeffs, evaluations, batch_size=1, num_witnesses=1,
-                    sha2=False, unique=False):
+                    sha2=False, unique=False, field1=False):
         """Statement of mixed linear forms: ``forms`` is a list of ("mle", (n, 3))
         or ("covector", (2^n, 3)) arrays; evaluations: (num_forms * V, 3)."""
         coeffs = np.ascontiguousarray(coeffs, dtype=np.uint64)
@@ -328,7 +331,8 @@ class Oracle:
         lens = (ctypes.c_uint64 * 2)()
         rc = self.lib.oracle_whir_prove_forms(n, rho, k, sec, pow_bits, int(unique), batch_size, num_witnesses,
                                               coeffs.ctypes.data, kinds, len(forms), data.ctypes.data,
-                                              evals.ctypes.data, narg, cap, hints, cap, lens, int(sha2))
+                                              evals.ctypes.data, narg, cap, hints, cap, lens,
+                                              int(sha2) | (2 if field1 else 0))
         if rc != 0:
             raise RuntimeError("oracle prove failed")
         return narg.raw[:lens[0]], hints.raw[:lens[1]]

@@ -20,7 +20,8 @@ has the reference checkout; the tests only read the JSON files).
    "multi" holds proofs over several committed vectors (batch_size > 1,
    several witnesses), including rows wider than one BLAKE3 chunk; "forms"
    statements that mix MultilinearExtension and dense Covector linear forms;
-   "unique" proofs under unique decoding, including statement-free ones.
+   "unique" proofs under unique decoding, including statement-free ones;
+   "field1" proofs over Identity<Goldilocks> (the CLI's --field Goldilocks1).
 """
 import hashlib
 import json
@@ -394,6 +395,40 @@ def whir_golden():
     return out
 
 
+FIELD1_CASES = [  # Identity<Goldilocks> (the CLI's --field Goldilocks1), from_params with field_size_bits 64:
+    # (n, k, rho, security, pow_bits, seed, form kinds, batch_size, num_witnesses, hash, unique_decoding)
+    (5, 4, 1, 40, 10, 81, ("mle",), 1, 1, "blake3", False),
+    (10, 4, 1, 40, 10, 82, ("mle",), 1, 1, "blake3", False),
+    (12, 4, 2, 40, 10, 83, ("mle", "covector"), 2, 1, "blake3", False),
+    (14, 3, 1, 32, 8, 84, ("mle",), 1, 1, "sha2", False),
+    (11, 4, 1, 40, 10, 85, (), 1, 1, "blake3", True),
+    (12, 4, 1, 36, 10, 86, ("covector",), 2, 2, "blake3", False),
+]
+
+
+def proofs_field1():
+    from oracle.refio import run_reference
+    from tests.golden.forms import form_inputs
+
+    out = []
+    for (n, k, rho, sec, pb, seed, kinds, batch, nwit, eng, unique) in FIELD1_CASES:
+        coeffs, forms = form_inputs(n, seed, kinds, batch * nwit, base_field=True)
+        ref = run_reference(n, k, rho, sec, pb, None, coeffs, verify=True, sha2=eng == "sha2", batch_size=batch,
+                            num_witnesses=nwit, forms=forms, unique=unique, field1=True)
+        assert ref.verify_ok == 1.0
+        rec = {"n": n, "k": k, "rho": rho, "security": sec, "pow_bits": pb, "seed": seed, "kinds": list(kinds),
+               "batch_size": batch, "num_witnesses": nwit, "hash": eng, "unique_decoding": unique,
+               "evaluations": [[int(x) for x in row] for row in ref.evaluations],
+               "narg_len": len(ref.narg), "hints_len": len(ref.hints),
+               "narg_sha256": hashlib.sha256(ref.narg).hexdigest(),
+               "hints_sha256": hashlib.sha256(ref.hints).hexdigest()}
+        if n <= 5:
+            rec["narg"] = ref.narg.hex()
+            rec["hints"] = ref.hints.hex()
+        out.append(rec)
+    return out
+
+
 def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
@@ -404,7 +439,8 @@ def main():
     with open(os.path.join(HERE, "reference_proofs.json"), "w") as f:
         json.dump({"generator": "oracle/_ref/ref_driver (reference C++ prover, CLI domain separator, "
                                 "seeded ChaCha20 inputs via whirgpu_sample_goldilocks)", "cases": proofs(),
-                   "multi": proofs_multi(), "forms": proofs_forms(), "unique": proofs_unique()}, f, indent=1)
+                   "multi": proofs_multi(), "forms": proofs_forms(), "unique": proofs_unique(),
+                   "field1": proofs_field1()}, f, indent=1)
 
 
 if __name__ == "__main__":

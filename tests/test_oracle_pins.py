@@ -307,3 +307,26 @@ def test_oracle_matches_reference_whir_golden(oracle, case):
     assert narg.hex() == case["narg"]
     assert hints.hex() == case["hints"]
     assert [int(x) for x in ep[:, 0]] == case["eval_point"] and not ep[:, 1:].any()
+
+
+FIELD1 = json.load(open(os.path.join(HERE, "golden", "reference_proofs.json")))["field1"]
+
+
+@pytest.mark.parametrize("case", FIELD1, ids=lambda c: f"n{c['n']}-{'-'.join(c['kinds']) or 'none'}"
+                                                       f"-b{c['batch_size']}w{c['num_witnesses']}{c['hash']}")
+def test_oracle_goldilocks1_matches_reference_fixtures(oracle, case):
+    """Identity<Goldilocks> (the CLI's --field Goldilocks1): challenges, sums and
+    messages in the base field, field_size_bits 64 in from_params."""
+    from tests.golden.forms import form_inputs
+
+    coeffs, forms = form_inputs(case["n"], case["seed"], case["kinds"], case["batch_size"] * case["num_witnesses"],
+                                base_field=True)
+    evals = np.array(case["evaluations"], dtype=np.uint64).reshape(-1, 3)
+    narg, hints = oracle.prove_forms(case["n"], case["k"], case["rho"], case["security"], case["pow_bits"], forms,
+                                     coeffs, evals, case["batch_size"], case["num_witnesses"],
+                                     sha2=case["hash"] == "sha2", unique=case["unique_decoding"], field1=True)
+    assert (len(narg), len(hints)) == (case["narg_len"], case["hints_len"])
+    assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
+    if "narg" in case:
+        assert narg.hex() == case["narg"] and hints.hex() == case["hints"]

@@ -7,6 +7,8 @@ the C ABI in include/whirgpu.h); this package is its Python mirror.
 from .whir import (  # noqa: F401
     ENGINE_ID_BLAKE3,
     ENGINE_ID_SHA2,
+    FIELD_GOLDILOCKS1,
+    FIELD_GOLDILOCKS3,
     P,
     Config,
     Context,

@@ -24,7 +24,7 @@ EXPORTED = [
     "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_schedule",
     "whirgpu_workspace_bytes",
     "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
-    "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
+    "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_config_from_params", "whirgpu_commit_config", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
     "whirgpu_debug_field_ops", "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
     "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
     "whirgpu_batch_create", "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_batch_destroy",
@@ -68,6 +68,33 @@ class Request(ctypes.Structure):
 
 
 FORM_MLE, FORM_COVECTOR = 0, 1
+FIELD_GOLDILOCKS1, FIELD_GOLDILOCKS3 = 1, 3
+MAX_ROUNDS = 24
+NO_POW = (1 << 64) - 1
+
+
+class IrsConfig(ctypes.Structure):
+    """Mirror of whirgpu_irs_config (irs_commit::Config's shape fields)."""
+    _fields_ = [("vector_size", ctypes.c_uint64), ("codeword_length", ctypes.c_uint64),
+                ("interleaving_depth", ctypes.c_uint64), ("in_domain_samples", ctypes.c_uint64),
+                ("out_domain_samples", ctypes.c_uint64)]
+
+
+class SumcheckConfig(ctypes.Structure):
+    _fields_ = [("num_rounds", ctypes.c_uint64), ("pow_threshold", ctypes.c_uint64)]
+
+
+class RoundConfig(ctypes.Structure):
+    _fields_ = [("irs_committer", IrsConfig), ("pow_threshold", ctypes.c_uint64), ("sumcheck", SumcheckConfig)]
+
+
+class WhirConfig(ctypes.Structure):
+    """Mirror of whirgpu_config (Config<M>, whir.hpp:104-116, plus the field M)."""
+    _fields_ = [("field", ctypes.c_uint32), ("batch_size", ctypes.c_uint64), ("hash_id", ctypes.c_uint8 * 32),
+                ("initial_committer", IrsConfig), ("initial_sumcheck", SumcheckConfig),
+                ("initial_skip_pow", ctypes.c_uint64), ("num_rounds", ctypes.c_uint64),
+                ("round_configs", RoundConfig * MAX_ROUNDS), ("final_sumcheck", SumcheckConfig),
+                ("final_pow", ctypes.c_uint64)]
 
 
 class LinearForm(ctypes.Structure):
@@ -141,6 +168,8 @@ def load() -> ctypes.CDLL:
     L.whirgpu_proof_get.argtypes = [p, vp, ctypes.POINTER(sz), vp, ctypes.POINTER(sz)]
     L.whirgpu_commit.argtypes = [p, ctypes.POINTER(WhirParams), p, u64, i32, p, vp]
     L.whirgpu_commit_witnesses.argtypes = [p, ctypes.POINTER(WhirParams), p, u64, u64, i32, p, vp]
+    L.whirgpu_config_from_params.argtypes = [ctypes.POINTER(WhirParams), u64, ctypes.c_uint32, ctypes.POINTER(WhirConfig)]
+    L.whirgpu_commit_config.argtypes = [p, ctypes.POINTER(WhirConfig), p, u64, i32, p, vp]
     L.whirgpu_witness_destroy.argtypes = [p]
     L.whirgpu_prove.argtypes = [p, p, p, sz, p, p, p, p]
     L.whirgpu_prove_forms.argtypes = [p, p, ctypes.POINTER(LinearForm), sz, p, p, p, p]
@@ -194,7 +223,8 @@ def load() -> ctypes.CDLL:
                  "whirgpu_ntt_get_plan", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans"):
         getattr(L, name).restype = i32
     for name in ("whirgpu_ctx_create", "whirgpu_cli_domain_separator", "whirgpu_transcript_create",
-                 "whirgpu_proof_get", "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate",
+                 "whirgpu_proof_get", "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_config_from_params", "whirgpu_commit_config", "whirgpu_prove",
+                 "whirgpu_prove_forms", "whirgpu_mle_evaluate",
                  "whirgpu_mle_evaluate_noalloc", "whirgpu_debug_field_ops", "whirgpu_batch_create",
                  "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_server_create", "whirgpu_server_submit",
                  "whirgpu_server_poll",

@@ -161,21 +161,41 @@ bool evict_idle(whirgpu_ctx* c, uint64_t need, uint64_t limit) {
 
 }  // namespace
 
+namespace {
+// Serialised plan shape: equal keys give equal plans.
+std::string plan_key(const WhirSchedule& s, const ProtocolParams& pp, size_t ds_len, uint32_t nwit) {
+    std::vector<uint64_t> w{s.initial.vector_size, s.initial.codeword_length, s.initial.depth, s.initial.in_domain,
+                            s.initial.out_domain, s.initial_sumcheck.num_rounds, s.initial_sumcheck.pow_threshold,
+                            s.initial_skip_pow, s.rounds.size()};
+    for (const RoundSchedule& r : s.rounds)
+        w.insert(w.end(), {r.irs.vector_size, r.irs.codeword_length, r.irs.depth, r.irs.in_domain, r.irs.out_domain,
+                           r.pow_threshold, r.sumcheck.num_rounds, r.sumcheck.pow_threshold});
+    w.insert(w.end(), {s.final_sumcheck.num_rounds, s.final_sumcheck.pow_threshold, s.final_pow, pp.batch_size,
+                       (uint64_t)pp.hash, (uint64_t)pp.field_degree, (uint64_t)std::max<size_t>(ds_len, 96), nwit});
+    return std::string(reinterpret_cast<const char*>(w.data()), w.size() * sizeof(uint64_t));
+}
+}  // namespace
+
 whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out,
                                  uint64_t cap, uint32_t nwit) {
-    ProofPlan plan;
+    WhirSchedule sched;
     try {
-        plan = make_plan((uint32_t)n, to_params(params), MAX_FORMS, std::max<size_t>(ds_len, 96), nwit);
+        sched = make_schedule(n, to_params(params));
     } catch (const std::exception& e) {
         return fail(c, WHIRGPU_E_INVALID, e.what());
     }
-    // The plan carries the hash engine and the vector layout: bits 0 unique
-    // decoding, 1..31 ds length, 32..39 batch size, 40..47 witnesses, 62 SHA-2.
-    auto key = std::make_tuple(n, params->starting_log_inv_rate, params->initial_folding_factor, params->folding_factor,
-                               params->security_level, params->pow_bits,
-                               (uint64_t)params->unique_decoding | ((uint64_t)std::max<size_t>(ds_len, 96) << 1) |
-                                   (params->batch_size << 32) | ((uint64_t)nwit << 40) |
-                                   ((uint64_t)is_sha2(params) << 62));
+    return acquire_workspace_sched(c, sched, to_params(params), ds_len, out, cap, nwit);
+}
+
+whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched, const ProtocolParams& pp, size_t ds_len,
+                                       Workspace** out, uint64_t cap, uint32_t nwit) {
+    ProofPlan plan;
+    try {
+        plan = make_plan(sched, pp, MAX_FORMS, std::max<size_t>(ds_len, 96), nwit);
+    } catch (const std::exception& e) {
+        return fail(c, WHIRGPU_E_INVALID, e.what());
+    }
+    const std::string key = plan_key(sched, pp, ds_len, nwit);
     std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
     for (Workspace* w : c->cache[key])
         if (!w->busy) {
@@ -360,21 +380,19 @@ whirgpu_status whirgpu_proof_get(const whirgpu_transcript* t, const uint8_t** na
     return WHIRGPU_OK;
 }
 
-whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs,
-                                        uint64_t num_witnesses, uint64_t n, int where, whirgpu_transcript* tx,
-                                        whirgpu_witness** out) {
-    if (!c || !params || !coeffs || !tx || !out || tx->ctx != c) return fail(c, WHIRGPU_E_INVALID, "null argument");
-    *out = nullptr;
-    if (!engine_supported(params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 and SHA-2 engines are on this path");
-    if (n >= 40) return fail(c, WHIRGPU_E_INVALID, "num_variables too large");
-    if (params->batch_size == 0 || num_witnesses == 0) return fail(c, WHIRGPU_E_INVALID, "no vectors to commit");
-    if (num_witnesses > (uint64_t)MAX_WITNESSES || params->batch_size * num_witnesses > (uint64_t)MAX_VECTORS)
+namespace {
+// Commit of num_witnesses witnesses for a schedule (from params or given).
+whirgpu_status commit_schedule(whirgpu_ctx* c, const WhirSchedule& sched, const ProtocolParams& pp,
+                               const uint64_t* coeffs, uint64_t num_witnesses, int where, whirgpu_transcript* tx,
+                               whirgpu_witness** out) {
+    if (pp.batch_size == 0 || num_witnesses == 0) return fail(c, WHIRGPU_E_INVALID, "no vectors to commit");
+    if (num_witnesses > (uint64_t)MAX_WITNESSES || pp.batch_size * num_witnesses > (uint64_t)MAX_VECTORS)
         return fail(c, WHIRGPU_E_UNSUPPORTED, "more committed vectors than this path holds");
     Workspace* ws = nullptr;
-    whirgpu_status s = acquire_workspace(c, n, params, tx->ds.size(), &ws, 0, (uint32_t)num_witnesses);
+    whirgpu_status s = acquire_workspace_sched(c, sched, pp, tx->ds.size(), &ws, 0, (uint32_t)num_witnesses);
     if (s != WHIRGPU_OK) return s;
     const ProofPlan& p = ws->plan;
-    const size_t coeff_bytes = (size_t)p.nvec * (8ull << n);
+    const size_t coeff_bytes = (size_t)p.nvec * (8ull << p.n);
     cudaError_t e = cudaMemcpyAsync(ws->dev + p.off_coeffs, coeffs, coeff_bytes,
                                     where == WHIRGPU_INPUT_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                     c->stream);
@@ -400,6 +418,103 @@ whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* c, const whirgpu_params* pa
     }
     *out = w;
     return WHIRGPU_OK;
+}
+
+void to_irs(const IrsSchedule& a, whirgpu_irs_config& b) {
+    b = {a.vector_size, a.codeword_length, a.depth, a.in_domain, a.out_domain};
+}
+IrsSchedule from_irs(const whirgpu_irs_config& b) {
+    IrsSchedule a;
+    a.vector_size = b.vector_size;
+    a.codeword_length = b.codeword_length;
+    a.depth = b.interleaving_depth;
+    a.in_domain = b.in_domain_samples;
+    a.out_domain = b.out_domain_samples;
+    return a;
+}
+}  // namespace
+
+whirgpu_status whirgpu_config_from_params(const whirgpu_params* params, uint64_t n, uint32_t field, whirgpu_config* out) {
+    if (!params || !out || (field != WHIRGPU_FIELD_GOLDILOCKS1 && field != WHIRGPU_FIELD_GOLDILOCKS3))
+        return WHIRGPU_E_INVALID;
+    ProtocolParams pp = to_params(params);
+    pp.field_degree = (int)field;
+    WhirSchedule s;
+    try {
+        s = make_schedule(n, pp);
+    } catch (const std::exception&) {
+        return WHIRGPU_E_INVALID;
+    }
+    if (s.rounds.size() > WHIRGPU_MAX_ROUNDS) return WHIRGPU_E_UNSUPPORTED;
+    std::memset(out, 0, sizeof(*out));
+    out->field = field;
+    out->batch_size = params->batch_size;
+    std::memcpy(out->hash_id, params->hash_id, 32);
+    to_irs(s.initial, out->initial_committer);
+    out->initial_sumcheck = {s.initial_sumcheck.num_rounds, s.initial_sumcheck.pow_threshold};
+    out->initial_skip_pow = s.initial_skip_pow;
+    out->num_rounds = s.rounds.size();
+    for (size_t r = 0; r < s.rounds.size(); ++r) {
+        to_irs(s.rounds[r].irs, out->round_configs[r].irs_committer);
+        out->round_configs[r].pow_threshold = s.rounds[r].pow_threshold;
+        out->round_configs[r].sumcheck = {s.rounds[r].sumcheck.num_rounds, s.rounds[r].sumcheck.pow_threshold};
+    }
+    out->final_sumcheck = {s.final_sumcheck.num_rounds, s.final_sumcheck.pow_threshold};
+    out->final_pow = s.final_pow;
+    return WHIRGPU_OK;
+}
+
+whirgpu_status whirgpu_commit_config(whirgpu_ctx* c, const whirgpu_config* cfg, const uint64_t* coeffs,
+                                     uint64_t num_witnesses, int where, whirgpu_transcript* tx, whirgpu_witness** out) {
+    if (!c || !cfg || !coeffs || !tx || !out || tx->ctx != c) return fail(c, WHIRGPU_E_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->field != WHIRGPU_FIELD_GOLDILOCKS1 && cfg->field != WHIRGPU_FIELD_GOLDILOCKS3)
+        return fail(c, WHIRGPU_E_INVALID, "unknown field");
+    if (cfg->num_rounds > WHIRGPU_MAX_ROUNDS) return fail(c, WHIRGPU_E_INVALID, "too many rounds");
+    whirgpu_params hp{};
+    hp.batch_size = cfg->batch_size;
+    std::memcpy(hp.hash_id, cfg->hash_id, 32);
+    if (!engine_supported(&hp)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 and SHA-2 engines are on this path");
+    ProtocolParams pp;
+    pp.batch_size = cfg->batch_size;
+    pp.hash = is_sha2(&hp) ? 1 : 0;
+    pp.field_degree = (int)cfg->field;
+    WhirSchedule s;
+    s.initial = from_irs(cfg->initial_committer);
+    s.initial_sumcheck = {s.initial.vector_size, cfg->initial_sumcheck.num_rounds, cfg->initial_sumcheck.pow_threshold};
+    s.initial_skip_pow = cfg->initial_skip_pow;
+    uint64_t size = cfg->initial_sumcheck.num_rounds < 64 ? s.initial.vector_size >> cfg->initial_sumcheck.num_rounds : 0;
+    for (uint64_t r = 0; r < cfg->num_rounds; ++r) {
+        const whirgpu_round_config& rc = cfg->round_configs[r];
+        RoundSchedule q;
+        q.irs = from_irs(rc.irs_committer);
+        q.pow_threshold = rc.pow_threshold;
+        q.sumcheck = {size, rc.sumcheck.num_rounds, rc.sumcheck.pow_threshold};
+        size = rc.sumcheck.num_rounds < 64 ? size >> rc.sumcheck.num_rounds : 0;
+        s.rounds.push_back(q);
+    }
+    s.final_sumcheck = {size, cfg->final_sumcheck.num_rounds, cfg->final_sumcheck.pow_threshold};
+    s.final_pow = cfg->final_pow;
+    int n = 0;
+    while (n < 40 && (1ull << n) < s.initial.vector_size) ++n;
+    s.num_variables = (uint64_t)n;
+    return commit_schedule(c, s, pp, coeffs, num_witnesses, where, tx, out);
+}
+
+whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs,
+                                        uint64_t num_witnesses, uint64_t n, int where, whirgpu_transcript* tx,
+                                        whirgpu_witness** out) {
+    if (!c || !params || !coeffs || !tx || !out || tx->ctx != c) return fail(c, WHIRGPU_E_INVALID, "null argument");
+    *out = nullptr;
+    if (!engine_supported(params)) return fail(c, WHIRGPU_E_UNSUPPORTED, "only the BLAKE3 and SHA-2 engines are on this path");
+    if (n >= 40) return fail(c, WHIRGPU_E_INVALID, "num_variables too large");
+    WhirSchedule s;
+    try {
+        s = make_schedule(n, to_params(params));
+    } catch (const std::exception& e) {
+        return fail(c, WHIRGPU_E_INVALID, e.what());
+    }
+    return commit_schedule(c, s, to_params(params), coeffs, num_witnesses, where, tx, out);
 }
 
 whirgpu_status whirgpu_commit(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs, uint64_t n,

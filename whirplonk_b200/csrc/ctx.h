@@ -90,8 +90,9 @@ struct whirgpu_ctx {
     uint64_t allocated = 0;
     wg::DeviceTables tw;
     std::string err;
-    std::map<std::tuple<uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t, uint64_t>, std::vector<wg::Workspace*>>
-        cache;
+    // Workspaces by plan shape: the schedule, hash engine, vector layout, field
+    // degree and domain-separator length, serialised (plan_key).
+    std::map<std::string, std::vector<wg::Workspace*>> cache;
     uint8_t* pinned = nullptr;
     size_t pinned_bytes = 0;
     char* mle_scratch = nullptr;
@@ -134,6 +135,9 @@ whirgpu_status ensure_pinned(whirgpu_ctx* c, size_t bytes);
 // first; a failed cudaMalloc frees every idle workspace and tries once more.
 whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_params* params, size_t ds_len, Workspace** out,
                                  uint64_t cap = 0, uint32_t nwit = 1);
+// The same for a schedule given field by field.
+whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched, const ProtocolParams& pp, size_t ds_len,
+                                       Workspace** out, uint64_t cap = 0, uint32_t nwit = 1);
 void release_workspace(whirgpu_ctx* c, Workspace* w);
 // While set, kernel launches of this thread are stream-captured, not run: the
 // launch counter skips them and graph launches add their kernel-node counts.

@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
         wtx_load(t, tx);
         wtx_message_words(t, w, 4);
         for (int j = 0; j < n_ood; ++j) {
-            const E3 z = wtx_challenge_e3(t);
+            const E3 z = wtx_challenge_t(t);
             if (threadIdx.x == 0) sc->ood_pts[commit_idx][j] = z;
         }
         wtx_store(t, tx);
@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u
         wtx_load(t, a.tx);
         for (u32 k = 0; k < nvals; ++k) {
             const u32 v = k % a.nvec;
-            if (v < a.skip_lo || v >= a.skip_hi) wtx_message_e3(t, totals[k]);
+            if (v < a.skip_lo || v >= a.skip_hi) wtx_message_t(t, totals[k]);
         }
         wtx_store(t, a.tx);
     }

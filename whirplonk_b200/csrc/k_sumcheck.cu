@@ -132,8 +132,8 @@ __device__ __forceinline__ void sc_round_finish(const ScKernelArgs& a, E3 c0, E3
         ProofScalars* sc = a.sc;
         WarpTx t;
         wtx_load(t, a.tx);
-        wtx_message_e3(t, C0);
-        wtx_message_e3(t, C2);
+        wtx_message_t(t, C0);
+        wtx_message_t(t, C2);
         if (a.pow_threshold != ~0ull) {
             // PoW follows in-stream (ordered windows, then k_sc_after_pow).
             wtx_squeeze_bytes(t, sc->pow_ch, 32);
@@ -144,7 +144,7 @@ __device__ __forceinline__ void sc_round_finish(const ScKernelArgs& a, E3 c0, E3
                 sc->pow_next = 0;
             }
         } else {
-            const E3 rn = wtx_challenge_e3(t);
+            const E3 rn = wtx_challenge_t(t);
             if (threadIdx.x == 0) {
                 const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
                 sc->c0 = C0;
@@ -196,7 +196,7 @@ __global__ void k_sc_after_pow(TxState* tx, ProofScalars* sc, int r_slot) {
     wtx_load(t, tx);
     if (n == ~0ull) t.err |= TX_ERR_POW_EXHAUSTED;
     wtx_message_u64(t, n);
-    const E3 rn = wtx_challenge_e3(t);
+    const E3 rn = wtx_challenge_t(t);
     if (threadIdx.x == 0) {
         const E3 C0 = sc->c0, C2 = sc->c2;
         const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
@@ -278,9 +278,9 @@ __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs
         __syncthreads();
         if (threadIdx.x < 32) {
             const E3 C0 = tot[0], C2 = tot[1];
-            wtx_message_e3(wt, C0);
-            wtx_message_e3(wt, C2);
-            const E3 rn = wtx_challenge_e3(wt);
+            wtx_message_t(wt, C0);
+            wtx_message_t(wt, C2);
+            const E3 rn = wtx_challenge_t(wt);
             if (threadIdx.x == 0) {
                 const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
                 sc->c0 = C0;
@@ -445,7 +445,7 @@ __global__ void __launch_bounds__(256) k_cov_init(CovInitArgs a, const E3* tab) 
         a.cov[0][i] = acc.c0;
         a.cov[1][i] = acc.c1;
         a.cov[2][i] = acc.c2;
-        if (a.nvec > 1) {
+        if (a.write_vec) {
             E3Acc r = e3acc_zero();
             for (u32 v = 0; v < a.nvec; ++v) e3acc_mac_base(r, a.sc->vrlc[v], a.vecs[(u64)v * S + i]);
             const E3 x = e3acc_reduce(r);
@@ -464,10 +464,11 @@ size_t cov_init_scratch_bytes(u32 logS, int n_forms, int n_ood) {
 
 int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
     if (a.n_forms > MAX_FORMS || a.n_ood > MAX_INIT_OOD || a.nvec < 1 || a.nvec > (u32)MAX_VECTORS) return -1;
+    if (a.nvec > 1 && !a.write_vec) return -1;
     E3* tab = reinterpret_cast<E3*>(a.scratch);
     const int nterms = a.n_forms + a.n_ood;
     const u64 S = 1ull << a.logS;
-    if (nterms == 0 && a.nvec == 1) {  // no constraint and no vector RLC: a zero covector
+    if (nterms == 0 && !a.write_vec) {  // no constraint and no vector to write: a zero covector
         for (int c = 0; c < 3; ++c) cudaMemsetAsync(a.cov[c], 0, S * 8, st);
         return 0;
     }

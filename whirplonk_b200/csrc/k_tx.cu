@@ -17,11 +17,12 @@ namespace wg {
 // ---------------------------------------------------------------------------
 // One warp.
 __global__ void k_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
-                          unsigned char* hints, u64 hints_cap, ProofScalars* sc) {
+                          unsigned char* hints, u64 hints_cap, ProofScalars* sc, unsigned deg) {
     if (threadIdx.x >= 32) return;
     WarpTx t;
     t.h = t.r = 0;
     t.hpos = t.rpos = t.has_reader = t.err = 0;
+    t.deg = deg;
     t.narg_len = t.hints_len = 0;
     t.narg_cap = narg_cap;
     t.hints_cap = hints_cap;
@@ -33,8 +34,9 @@ __global__ void k_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsi
 }
 
 int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
-                   unsigned char* hints, u64 hints_cap, ProofScalars* sc, cudaStream_t st) {
-    k_tx_init<<<1, 32, 0, st>>>(tx, ds, ds_len, narg, narg_cap, hints, hints_cap, sc);
+                   unsigned char* hints, u64 hints_cap, ProofScalars* sc, unsigned deg, cudaStream_t st) {
+    if (deg != 1 && deg != 3) return -1;
+    k_tx_init<<<1, 32, 0, st>>>(tx, ds, ds_len, narg, narg_cap, hints, hints_cap, sc, deg);
     count_launches(1);
     return 0;
 }
@@ -184,7 +186,7 @@ __global__ void k_send_vector(TxState* tx, const u64* c0, const u64* c1, const u
     if (threadIdx.x >= 32) return;
     WarpTx t;
     wtx_load(t, tx);
-    for (u64 i = 0; i < size; ++i) wtx_message_e3(t, E3{c0[i], c1[i], c2[i]});
+    for (u64 i = 0; i < size; ++i) wtx_message_t(t, E3{c0[i], c1[i], c2[i]});
     wtx_store(t, tx);
 }
 
@@ -202,7 +204,7 @@ __global__ void k_squeeze_e3(TxState* tx, ProofScalars* sc, int slot, int count)
     WarpTx t;
     wtx_load(t, tx);
     for (int k = 0; k < count; ++k) {
-        const E3 r = wtx_challenge_e3(t);
+        const E3 r = wtx_challenge_t(t);
         if (threadIdx.x == 0) sc->sc_r[slot + k] = r;
     }
     wtx_store(t, tx);

@@ -108,8 +108,10 @@ int launch_ood(const OodArgs& a, cudaStream_t st);
 size_t ood_scratch_bytes(u64 max_size, u32 max_values);
 
 // ---- Transcript / protocol steps (single-thread kernels) ---------------------
+// deg: degree of the target field (3 Ext3, 1 Goldilocks): field elements cross
+// the transcript as 3 or 1 words.
 int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
-                   unsigned char* hints, u64 hints_cap, ProofScalars* sc, cudaStream_t st);
+                   unsigned char* hints, u64 hints_cap, ProofScalars* sc, unsigned deg, cudaStream_t st);
 // Vector RLC, constraint RLC + initial sum (whir_prover.hpp:122-197) over
 // nvec vectors and nwit initial commitments of `ood` OOD points each.
 int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int nwit, int ood, int nvec, cudaStream_t st);
@@ -158,6 +160,7 @@ struct CovInitArgs {
     ProofScalars* sc;
     void* scratch;
     u32 nvec;           // committed vectors (1: no vector RLC)
+    bool write_vec;     // write vec_out (several vectors, or the lifted vector when no round reads the base one)
     const u64* vecs;    // nvec base vectors, 2^logS words each, back to back
     u64* vec_out[3];    // Ext3 planes of the combined vector
     u32 dense_mask;     // forms f with bit f set are dense covectors (their points slot is unused):

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdint>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 namespace wg {
@@ -22,6 +23,10 @@ struct ProtocolParams {  // whir::ProtocolParameters (cpp/include/whir/parameter
     uint64_t pow_bits = 20;
     uint64_t batch_size = 1;
     int hash = 0;  // engine of hash_id: 0 BLAKE3, 1 SHA-256 (leaves, Merkle, PoW)
+    // Not a ProtocolParameters field but the embedding M of Config<M>: the
+    // target field's degree over Goldilocks, 3 for Basefield<GoldilocksExt3>
+    // (field_size_bits 192), 1 for Identity<Goldilocks> (64).
+    int field_degree = 3;
 };
 
 struct IrsSchedule {
@@ -104,7 +109,7 @@ inline WhirSchedule make_schedule(uint64_t num_variables, const ProtocolParams& 
     c.num_variables = num_variables;
     const double security = (double)p.security_level;
     const double psec = (double)(p.security_level - p.pow_bits);
-    const double fbits = 192.0;
+    const double fbits = p.field_degree == 1 ? 64.0 : 192.0;  // Target::field_size_bits
     uint64_t lir = p.starting_log_inv_rate;
     uint64_t nv = num_variables;
     const double irate = std::pow(0.5, (double)p.starting_log_inv_rate);
@@ -144,6 +149,36 @@ inline WhirSchedule make_schedule(uint64_t num_variables, const ProtocolParams& 
     c.final_sumcheck = {1ull << nv, nv, pow_threshold(ffpb)};
     c.final_pow = pow_threshold(fpb2);
     return c;
+}
+
+// Structural checks of a schedule given field by field (a Config built by the
+// caller, as the reference's golden dumpers do): the shapes the prove order
+// relies on.  Each commitment's depth is 2^(rounds of the sumcheck that
+// follows it), so the STIR rows match the eq weights of the folding randomness
+// (whir_prover.hpp:283-310); sizes chain from round to round.  Throws
+// std::invalid_argument.
+inline void validate_schedule(const WhirSchedule& s) {
+    auto pow2 = [](uint64_t v) { return v && !(v & (v - 1)); };
+    auto irs_ok = [&](const IrsSchedule& c, uint64_t vsize, uint64_t rounds, const char* what) {
+        if (c.vector_size != vsize) throw std::invalid_argument(std::string(what) + ": vector size does not chain");
+        if (rounds >= 64 || c.depth != (1ull << rounds))
+            throw std::invalid_argument(std::string(what) + ": depth != 2^(sumcheck rounds)");
+        if (!pow2(c.codeword_length) || c.depth > vsize || c.codeword_length % (vsize / c.depth) != 0)
+            throw std::invalid_argument(std::string(what) + ": codeword length");
+    };
+    if (!pow2(s.initial.vector_size)) throw std::invalid_argument("vector size must be a power of two");
+    irs_ok(s.initial, s.initial.vector_size, s.initial_sumcheck.num_rounds, "initial committer");
+    if (s.initial_sumcheck.initial_size != s.initial.vector_size)
+        throw std::invalid_argument("initial sumcheck size != vector size");
+    uint64_t size = s.initial.vector_size >> s.initial_sumcheck.num_rounds;
+    for (const RoundSchedule& r : s.rounds) {
+        irs_ok(r.irs, size, r.sumcheck.num_rounds, "round committer");
+        if (r.sumcheck.initial_size != size) throw std::invalid_argument("round sumcheck size does not chain");
+        size >>= r.sumcheck.num_rounds;
+    }
+    if (s.final_sumcheck.initial_size != size || (s.final_sumcheck.num_rounds < 64 && (size >> s.final_sumcheck.num_rounds) == 0) ||
+        s.final_sumcheck.num_rounds >= 64)
+        throw std::invalid_argument("final sumcheck does not fit the folded vector");
 }
 
 }  // namespace wg

@@ -39,11 +39,19 @@ uint32_t ilog2(uint64_t v) {
 }  // namespace
 
 ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_t ds_len, uint32_t nwit) {
+    return make_plan(make_schedule(n, params), params, n_forms, ds_len, nwit);
+}
+
+ProofPlan make_plan(const WhirSchedule& sched, const ProtocolParams& params, int n_forms, size_t ds_len, uint32_t nwit) {
+    validate_schedule(sched);
+    if (params.field_degree != 1 && params.field_degree != 3) throw std::invalid_argument("field degree must be 1 or 3");
+    const uint32_t n = ilog2(sched.initial.vector_size);
     ProofPlan p;
-    p.sch = make_schedule(n, params);
+    p.sch = sched;
     p.params = params;
     p.n = n;
     p.n_forms = n_forms;
+    const uint32_t deg = (uint32_t)params.field_degree;  // words per target-field element
     if (n_forms < 0 || n_forms > MAX_FORMS) throw std::invalid_argument("too many statement forms");
     if (params.batch_size == 0 || nwit == 0) throw std::invalid_argument("no committed vectors");
     if (nwit > (uint32_t)MAX_WITNESSES) throw std::invalid_argument("too many witnesses");
@@ -64,7 +72,7 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
         if (N % c.message_length() != 0) throw std::invalid_argument("codeword length not a multiple of message length");
     };
     check_irs(s.initial, (uint32_t)s.initial.depth * batch, 1);
-    for (const auto& r : s.rounds) check_irs(r.irs, (uint32_t)r.irs.depth, 3);
+    for (const auto& r : s.rounds) check_irs(r.irs, (uint32_t)r.irs.depth, deg);
     if ((size_t)n > (size_t)MAX_SC_ROUNDS) throw std::invalid_argument("too many variables");
     if (s.rounds.size() + nwit > (size_t)MAX_COMMITS) throw std::invalid_argument("too many rounds");
 
@@ -72,8 +80,10 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
     const uint64_t size = 1ull << n;
     p.off_coeffs = b.take((size_t)p.nvec * size * 8);
     // One vector: round 0 reads the base coefficients and the first fold
-    // writes half the size.  Several: the combined Ext3 vector is full size.
-    p.a_plane_words = p.nvec > 1 ? size : std::max<uint64_t>(size / 2, 1);
+    // writes half the size.  Several vectors, or no initial round: the
+    // covector pass writes the (combined, lifted) vector at full size.
+    p.full_vector = p.nvec > 1 || s.initial_sumcheck.num_rounds == 0;
+    p.a_plane_words = p.full_vector ? size : std::max<uint64_t>(size / 2, 1);
     p.off_a = b.take(3 * p.a_plane_words * 8);
     p.cov_plane_words = size;
     p.off_cov = b.take(3 * size * 8);
@@ -100,8 +110,8 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
         }
     }
     for (const auto& r : s.rounds) {
-        CommitBuffers cb = commit_of(r.irs, (uint32_t)r.irs.depth, 3);
-        cb.planes = b.take((size_t)cb.N * cb.depth * 3 * 8);
+        CommitBuffers cb = commit_of(r.irs, (uint32_t)r.irs.depth, deg);
+        cb.planes = b.take((size_t)cb.N * cb.depth * deg * 8);
         cb.nodes = b.take((2 * cb.N - 1) * 32);
         p.commits.push_back(cb);
     }
@@ -122,27 +132,28 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
 
     // Proof stream sizes.
     size_t narg = 0, hints = 0;
-    auto commit_narg = [](const IrsSchedule& c, uint64_t vectors) { return 32 + 24 * c.out_domain * vectors; };
+    const uint64_t esz = 8ull * deg;  // bytes of a target-field element message
+    auto commit_narg = [esz](const IrsSchedule& c, uint64_t vectors) { return 32 + esz * c.out_domain * vectors; };
     auto pow_narg = [](uint64_t thr) { return thr == ~0ull ? 0 : 8; };
-    auto sumcheck_narg = [&](const SumcheckSchedule& sc) { return sc.num_rounds * (48 + pow_narg(sc.pow_threshold)); };
+    auto sumcheck_narg = [&](const SumcheckSchedule& sc) { return sc.num_rounds * (2 * esz + pow_narg(sc.pow_threshold)); };
     auto open_hints = [](const IrsSchedule& c, uint64_t vectors, uint32_t ncomp, uint64_t commitments) {
         const uint64_t logN = ilog2(c.codeword_length);
         const uint64_t merkle = std::min<uint64_t>(c.in_domain * logN, c.codeword_length);
         return commitments * (8 + c.in_domain * c.depth * vectors * 8 * ncomp + 32 * merkle);
     };
     narg += nwit * commit_narg(s.initial, batch);
-    narg += 24 * s.initial.out_domain * nwit * (p.nvec - batch);  // OOD completion
+    narg += esz * s.initial.out_domain * nwit * (p.nvec - batch);  // OOD completion
     // initial sumcheck, or (no constraint) the skip-PoW: added below per variant
     const size_t narg_initial_constrained = sumcheck_narg(s.initial_sumcheck);
     const size_t narg_initial_free = pow_narg(s.initial_skip_pow);
     size_t sc_rounds = s.initial_sumcheck.num_rounds;
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         narg += commit_narg(s.rounds[r].irs, 1) + pow_narg(s.rounds[r].pow_threshold) + sumcheck_narg(s.rounds[r].sumcheck);
-        hints += r == 0 ? open_hints(s.initial, batch, 1, nwit) : open_hints(s.rounds[r - 1].irs, 1, 3, 1);
+        hints += r == 0 ? open_hints(s.initial, batch, 1, nwit) : open_hints(s.rounds[r - 1].irs, 1, deg, 1);
         sc_rounds += s.rounds[r].sumcheck.num_rounds;
     }
-    narg += 24 * s.final_sumcheck.initial_size + pow_narg(s.final_pow) + sumcheck_narg(s.final_sumcheck);
-    hints += s.rounds.empty() ? open_hints(s.initial, batch, 1, nwit) : open_hints(s.rounds.back().irs, 1, 3, 1);
+    narg += esz * s.final_sumcheck.initial_size + pow_narg(s.final_pow) + sumcheck_narg(s.final_sumcheck);
+    hints += s.rounds.empty() ? open_hints(s.initial, batch, 1, nwit) : open_hints(s.rounds.back().irs, 1, deg, 1);
     sc_rounds += s.final_sumcheck.num_rounds;
     p.narg_len_constrained = narg + narg_initial_constrained;
     p.narg_len_free = narg + narg_initial_free;
@@ -294,7 +305,8 @@ int enqueue_commit(const ProofPlan& p, char* ws, uint32_t ds_len, const DeviceTa
     Ctx c{p, ws, tw, st, timer};
     WG_TIMED(c, FAM_TX, launch_tx_init(c.tx(), reinterpret_cast<const unsigned char*>(ws + p.off_ds), ds_len,
                           reinterpret_cast<unsigned char*>(ws + p.off_narg), p.narg_len + 64,
-                          reinterpret_cast<unsigned char*>(ws + p.off_hints), p.hints_cap + 64, c.sc(), st));
+                          reinterpret_cast<unsigned char*>(ws + p.off_hints), p.hints_cap + 64, c.sc(),
+                          (unsigned)p.params.field_degree, st));
     const uint64_t size = 1ull << p.n;
     const uint32_t batch = (uint32_t)p.params.batch_size;
     const int ood = (int)p.sch.initial.out_domain;
@@ -347,13 +359,14 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         ci.sc = c.sc();
         ci.scratch = ws + p.off_cov_scratch;
         ci.nvec = V;
+        ci.write_vec = p.full_vector;
         ci.vecs = c.w(p.off_coeffs);
         ci.dense_mask = p.dense_mask;
         for (int f = 0; f < 8; ++f) ci.dense[f] = p.dense[f];
         WG_TIMED(c, FAM_COV, launch_cov_init(ci, st));
     }
     if (has_constraints) {
-        WG_TRY(sumcheck(c, s.initial_sumcheck, size0, V == 1, r_slot, true));
+        WG_TRY(sumcheck(c, s.initial_sumcheck, size0, !p.full_vector, r_slot, true));
     } else {
         // No constraint (unique decoding, no forms; whir_prover.hpp:211-218): the
         // folding randomness is squeezed directly, the skip-PoW keeps the
@@ -364,7 +377,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), s.initial_skip_pow, MAX_COMMITS + 1, c.p.params.hash, st));
         for (int t = 0; t < k; ++t) {
             SumcheckArgs a{};
-            a.a_base = (V == 1 && t == 0) ? c.w(p.off_coeffs) : nullptr;
+            a.a_base = (!p.full_vector && t == 0) ? c.w(p.off_coeffs) : nullptr;
             for (int q = 0; q < 3; ++q) { a.a_in[q] = c.a(q); a.a_out[q] = c.a(q); a.b[q] = c.cov(q); }
             a.size = size0 >> (t + 1);
             a.fold_r = t;
@@ -378,8 +391,9 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         const RoundSchedule& rc = s.rounds[r];
         const int ci = (int)(W + r);
-        const uint64_t* src[3] = {c.a(0), c.a(1), c.a(2)};
-        WG_TRY(commit_vectors(c, ci, src, 3, vsize, 1, (int)rc.irs.out_domain, &c.sc()->ood_vals[ci][0], 1));
+        const uint32_t deg = (uint32_t)p.params.field_degree;  // base-field rounds commit the c0 plane only
+        const uint64_t* src[3] = {c.a(0), deg == 3 ? c.a(1) : nullptr, deg == 3 ? c.a(2) : nullptr};
+        WG_TRY(commit_vectors(c, ci, src, deg, vsize, 1, (int)rc.irs.out_domain, &c.sc()->ood_vals[ci][0], 1));
         WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), rc.pow_threshold, ci, c.p.params.hash, st));
         // open the previous commitment (the first round: every initial commitment)
         const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;

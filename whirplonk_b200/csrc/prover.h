@@ -41,6 +41,7 @@ struct ProofPlan {
     size_t off_tx = 0, off_scalars = 0, off_narg = 0, off_hints = 0, off_ds = 0, off_points = 0;
     std::vector<CommitBuffers> commits;  // [initial 0 .. initial nwit-1, round 0, round 1, ...]
     size_t a_plane_words = 0, cov_plane_words = 0;
+    bool full_vector = false;  // the covector pass writes the lifted / combined vector (no base-field first round)
     uint32_t ood_values = 0;   // OOD scratch capacity in values (points x vectors)
     size_t narg_len = 0;       // exact narg length (every message has a fixed size)
     size_t narg_len_constrained = 0, narg_len_free = 0;  // with / without any constraint
@@ -57,6 +58,10 @@ void plan_set_forms(ProofPlan& p, int n_forms);
 // Throws std::invalid_argument on unsupported parameters.  The plan covers
 // num_witnesses initial commitments of p.batch_size vectors each.
 ProofPlan make_plan(uint32_t num_variables, const ProtocolParams& p, int n_forms, size_t ds_len,
+                    uint32_t num_witnesses = 1);
+// The same for a schedule given field by field (checked by validate_schedule);
+// p supplies the hash engine, batch_size and field degree.
+ProofPlan make_plan(const WhirSchedule& sched, const ProtocolParams& p, int n_forms, size_t ds_len,
                     uint32_t num_witnesses = 1);
 
 struct DeviceTables {

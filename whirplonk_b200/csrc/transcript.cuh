@@ -61,12 +61,13 @@ constexpr unsigned TX_RATE = 168;
 
 // Error bits recorded in TxState::err (never a trap: the host reads them).
 constexpr unsigned TX_ERR_NARG_OVERFLOW = 1u, TX_ERR_HINT_OVERFLOW = 2u, TX_ERR_POW_EXHAUSTED = 4u,
-                   TX_ERR_BAD_INDEX = 8u;
+                   TX_ERR_BAD_INDEX = 8u, TX_ERR_FIELD = 16u;
 
 struct TxState {
     u64 hasher[25];
     u64 reader[25];
     unsigned hpos, rpos, has_reader, err;
+    unsigned deg;  // degree of the target field over Goldilocks: 3 (Ext3) or 1 (the base field)
     u64 narg_len, hints_len;
     u64 narg_cap, hints_cap;
     u8* narg;

@@ -19,7 +19,7 @@ namespace wg {
 
 struct WarpTx {
     u64 h, r;  // this lane's hasher / reader word (lanes 0..24)
-    unsigned hpos, rpos, has_reader, err;
+    unsigned hpos, rpos, has_reader, err, deg;
     u64 narg_len, hints_len, narg_cap, hints_cap;
     u8* narg;
     u8* hints;
@@ -71,6 +71,7 @@ __device__ __forceinline__ void wtx_load(WarpTx& t, const TxState* g) {
     t.rpos = g->rpos;
     t.has_reader = g->has_reader;
     t.err = g->err;
+    t.deg = g->deg;
     t.narg_len = g->narg_len;
     t.hints_len = g->hints_len;
     t.narg_cap = g->narg_cap;
@@ -89,6 +90,7 @@ __device__ __forceinline__ void wtx_store(const WarpTx& t, TxState* g) {
         g->rpos = t.rpos;
         g->has_reader = t.has_reader;
         g->err = t.err;
+        g->deg = t.deg;
         g->narg_len = t.narg_len;
         g->hints_len = t.hints_len;
         g->narg_cap = t.narg_cap;
@@ -223,6 +225,23 @@ __device__ __forceinline__ E3 wtx_challenge_e3(WarpTx& t) {
     return E3{c0, c1, c2};
 }
 
+// Elements of the protocol's target field.  With the base field as target
+// (Identity<Goldilocks>) its elements are carried as Ext3 values (x, 0, 0) --
+// a subfield, so every kernel's arithmetic is unchanged -- and cross the
+// transcript as one 8-byte word / one 40-byte challenge (transcript.hpp:375-453).
+__device__ __forceinline__ E3 wtx_challenge_t(WarpTx& t) {
+    if (t.deg == 1) return E3{wtx_challenge_base(t), 0, 0};
+    return wtx_challenge_e3(t);
+}
+__device__ __forceinline__ void wtx_message_t(WarpTx& t, E3 v) {
+    if (t.deg == 1) {
+        if (v.c1 | v.c2) t.err |= TX_ERR_FIELD;  // outside the base field: caller input was not base-field
+        wtx_message_u64(t, v.c0);
+    } else {
+        wtx_message_e3(t, v);
+    }
+}
+
 // geometric_challenge (geometric_challenge.hpp:39-44): [] / [1] / squeeze x ->
 // [1, x, x^2, ...]; the powers are formed 32 at a time (lane k: x^(32 j + k)).
 __device__ __forceinline__ void wtx_geometric(WarpTx& t, E3* out, int count) {
@@ -233,7 +252,7 @@ __device__ __forceinline__ void wtx_geometric(WarpTx& t, E3* out, int count) {
         __syncwarp();
         return;
     }
-    const E3 x = wtx_challenge_e3(t);
+    const E3 x = wtx_challenge_t(t);
     // lane k: x^k by an in-warp prefix product (Hillis-Steele on multipliers)
     E3 p = l == 0 ? e3_one() : x;
 #pragma unroll

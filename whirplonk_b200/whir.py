@@ -238,16 +238,24 @@ class Witness:
             pass
 
 
+FIELD_GOLDILOCKS1, FIELD_GOLDILOCKS3 = _lib.FIELD_GOLDILOCKS1, _lib.FIELD_GOLDILOCKS3
+
+
 @dataclass
 class Config:
-    """Config<Basefield<GoldilocksExt3>> (whir.hpp:104-343)."""
+    """Config<M> (whir.hpp:104-343) with M = Basefield<GoldilocksExt3> (field 3,
+    the CLI's Goldilocks3) or Identity<Goldilocks> (field 1, Goldilocks1).
+    ``from_params`` derives it as the reference does; ``custom`` takes one built
+    field by field (``_lib.WhirConfig``), as the reference's golden dumpers do."""
 
     size: int
     params: ProtocolParameters
     schedule: list = field(default_factory=list)
+    target_field: int = FIELD_GOLDILOCKS3
+    cconfig: Optional[object] = None  # whirgpu_config when committing through whirgpu_commit_config
 
     @classmethod
-    def from_params(cls, size: int, params: ProtocolParameters) -> "Config":
+    def from_params(cls, size: int, params: ProtocolParameters, target_field: int = FIELD_GOLDILOCKS3) -> "Config":
         if size <= 0 or size & (size - 1):
             raise ValueError("size must be a power of two")
         n = size.bit_length() - 1
@@ -257,7 +265,18 @@ class Config:
         cnt = L.whirgpu_schedule(ctypes.byref(c), n, out, 1024)
         if cnt == 0:
             raise ValueError("invalid protocol parameters")
-        return cls(size, params, list(out[:cnt]))
+        cconfig = None
+        if target_field != FIELD_GOLDILOCKS3:
+            cconfig = _lib.WhirConfig()
+            _lib.check(L.whirgpu_config_from_params(ctypes.byref(c), n, target_field, ctypes.byref(cconfig)))
+        return cls(size, params, list(out[:cnt]), target_field, cconfig)
+
+    @classmethod
+    def custom(cls, cconfig) -> "Config":
+        """A Config given field by field as a ``_lib.WhirConfig``."""
+        size = int(cconfig.initial_committer.vector_size)
+        params = ProtocolParameters(batch_size=int(cconfig.batch_size), hash_id=bytes(cconfig.hash_id))
+        return cls(size, params, [], int(cconfig.field), cconfig)
 
     def workspace_bytes(self) -> int:
         """Device memory one proof of this shape occupies (HBM-budget unit)."""
@@ -291,9 +310,13 @@ class Config:
             if keep.size != self.size * nvec:
                 raise ValueError("vectors != batch_size * num_witnesses vectors of the config size")
             ptr, where = keep.ctypes.data, 0
-        _lib.check(ctx._L.whirgpu_commit_witnesses(ctx.handle, ctypes.byref(c), ptr, num_witnesses,
-                                                   self.num_variables, where, prover_state.handle, ctypes.byref(h)),
-                   ctx.handle)
+        if self.cconfig is not None:
+            _lib.check(ctx._L.whirgpu_commit_config(ctx.handle, ctypes.byref(self.cconfig), ptr, num_witnesses, where,
+                                                    prover_state.handle, ctypes.byref(h)), ctx.handle)
+        else:
+            _lib.check(ctx._L.whirgpu_commit_witnesses(ctx.handle, ctypes.byref(c), ptr, num_witnesses,
+                                                       self.num_variables, where, prover_state.handle,
+                                                       ctypes.byref(h)), ctx.handle)
         return Witness(h.value, ctx, keep, nvec, num_witnesses)
 
     def prove(self, prover_state: ProverState, vectors, witnesses: Sequence[Witness], linear_forms: Sequence,
@@ -339,15 +362,17 @@ class Config:
 
 def prove_once(n: int, params: ProtocolParameters, coeffs, points, evaluations, ctx: Optional[Context] = None,
                ds: Optional[DomainSeparator] = None, on_device_ptr: Optional[int] = None, num_witnesses: int = 1,
-               forms: Optional[Sequence] = None):
+               forms: Optional[Sequence] = None, target_field: int = FIELD_GOLDILOCKS3,
+               config: Optional[Config] = None):
     """commit (num_witnesses witnesses of params.batch_size vectors) + prove with
     the CLI domain separator; returns (narg, hints, claim).  The statement is
     one MultilinearExtension per point, or ``forms`` (MultilinearExtension /
     Covector objects) when given; ``evaluations`` holds num_forms * num_vectors
-    Ext3 values, form-major."""
+    Ext3 values, form-major.  ``config`` (a Config, e.g. Config.custom) replaces
+    the one from_params derives; ``target_field`` selects the embedding."""
     ctx = ctx or default_context()
     ds = ds or cli_domain_separator(params)
-    config = Config.from_params(1 << n, params)
+    config = config or Config.from_params(1 << n, params, target_field)
     ps = ProverState.from_ds(ds, b"", ctx)
     w = config.commit_witnesses(ps, coeffs, num_witnesses, on_device_ptr=on_device_ptr)
     if forms is None:
