@@ -38,7 +38,10 @@ __host__ __device__ __forceinline__ u32 col_stride(u32 logR) { return (1u << log
 // 2^RR elements base + j 2^s0 (j < 2^RR) of one column, and the butterflies of
 // stage s pair j with j + 2^(t-1) (t = s - s0) under the twiddle
 // w_{2^s}^(lo + (j mod 2^(t-1)) 2^s0), lo = base mod 2^s0.
-template <int RR>
+// S0ZERO: the group starts at stage 1 (s0 = 0), so lo = 0 and the butterflies
+// with j mod 2^(t-1) = 0 have the twiddle w^0 = 1: their multiply is skipped
+// (all of stage 1, half of stage 2, ...).
+template <int RR, bool S0ZERO>
 __device__ __forceinline__ void dit_group_pass(u64* sm, u32 W, u32 L, u32 s0, const u64* tws) {
     constexpr int G = 1 << RR;
     const u32 gpc_log = L - RR;  // groups per column (log2)
@@ -47,8 +50,8 @@ __device__ __forceinline__ void dit_group_pass(u64* sm, u32 W, u32 L, u32 s0, co
     for (u32 g = threadIdx.x; g < total; g += blockDim.x) {
         const u32 w = g >> gpc_log;
         const u32 gb = g & ((1u << gpc_log) - 1);
-        const u32 lo = gb & ((1u << s0) - 1);
-        const u32 base = lo + ((gb >> s0) << (s0 + RR));
+        const u32 lo = S0ZERO ? 0u : (gb & ((1u << s0) - 1));
+        const u32 base = S0ZERO ? (gb << RR) : lo + ((gb >> s0) << (s0 + RR));
         u64* col = sm + w * cs;
         u64 x[G];
 #pragma unroll
@@ -60,8 +63,14 @@ __device__ __forceinline__ void dit_group_pass(u64* sm, u32 W, u32 L, u32 s0, co
 #pragma unroll
             for (int j = 0; j < G; ++j) {
                 if (j & half) continue;
-                const u64 tw = tws[(lo + ((u32)(j & (half - 1)) << s0)) << sh];
-                const u64 u = x[j], v = gl_mul(x[j + half], tw);
+                const u64 u = x[j];
+                u64 v;
+                if (S0ZERO && (j & (half - 1)) == 0) {
+                    v = x[j + half];
+                } else {
+                    const u64 tw = tws[(lo + ((u32)(j & (half - 1)) << s0)) << sh];
+                    v = gl_mul(x[j + half], tw);
+                }
                 x[j] = gl_add(u, v);
                 x[j + half] = gl_sub(u, v);
             }
@@ -176,10 +185,17 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     for (u32 s0 = logE; s0 < logR;) {
         const u32 left = logR - s0;
         const u32 rr = left >= 8 ? 4 : (left > 4 ? (left + 1) / 2 : left);
-        if (rr == 4) dit_group_pass<4>(sm, W, logR, s0, tws);
-        else if (rr == 3) dit_group_pass<3>(sm, W, logR, s0, tws);
-        else if (rr == 2) dit_group_pass<2>(sm, W, logR, s0, tws);
-        else dit_group_pass<1>(sm, W, logR, s0, tws);
+        if (s0 == 0) {
+            if (rr == 4) dit_group_pass<4, true>(sm, W, logR, s0, tws);
+            else if (rr == 3) dit_group_pass<3, true>(sm, W, logR, s0, tws);
+            else if (rr == 2) dit_group_pass<2, true>(sm, W, logR, s0, tws);
+            else dit_group_pass<1, true>(sm, W, logR, s0, tws);
+        } else {
+            if (rr == 4) dit_group_pass<4, false>(sm, W, logR, s0, tws);
+            else if (rr == 3) dit_group_pass<3, false>(sm, W, logR, s0, tws);
+            else if (rr == 2) dit_group_pass<2, false>(sm, W, logR, s0, tws);
+            else dit_group_pass<1, false>(sm, W, logR, s0, tws);
+        }
         s0 += rr;
         __syncthreads();
     }
