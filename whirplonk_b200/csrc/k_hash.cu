@@ -427,6 +427,15 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u
                 if (a.ext3) {
                     for (u32 l = lane; l < cnt; l += 32)
                         e3acc_mac(s, zlo[l], E3{b0[base + l], a.v[1][base + l], a.v[2][base + l]});
+                } else if (cnt == (1u << OOD_LO)) {
+                    // a full block: eight coalesced loads in flight per lane before the products
+                    for (u32 l0 = lane; l0 < cnt; l0 += 256) {
+                        u64 x[8];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) x[k] = b0[base + l0 + 32 * k];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) e3acc_mac_base(s, zlo[l0 + 32 * k], x[k]);
+                    }
                 } else {
                     for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], b0[base + l]);
                 }

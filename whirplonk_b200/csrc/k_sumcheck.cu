@@ -493,18 +493,27 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 constexpr u32 CA_LO = 10;
 
-__global__ void k_cov_acc_tables(const ProofScalars* sc, int n_points, u32 hi_count, E3* tab) {
+// Point j's table: z_j^l (l < 2^LO) then rlc_j z_j^(h 2^LO).  For the base-field
+// (in-domain) points z_j^l is a base element and goes to the compact array
+// lo_base[j - n_ext][l] instead, so a warp reads 8 contiguous bytes per lane.
+__global__ void k_cov_acc_tables(const ProofScalars* sc, int n_ext, int n_points, u32 hi_count, E3* tab, u64* lo_base) {
     const u32 per = (1u << CA_LO) + hi_count;
     const u64 total = (u64)per * n_points;
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 j = (u32)(e / per), k = (u32)(e % per);
         const E3 z = sc->stir_pts[j];
-        tab[e] = k < (1u << CA_LO) ? e3_pow(z, k)
-                                   : e3_mul(sc->stir_rlc[j], e3_pow(z, (u64)(k - (1u << CA_LO)) << CA_LO));
+        if ((int)j < n_ext) {
+            tab[e] = k < (1u << CA_LO) ? e3_pow(z, k)
+                                       : e3_mul(sc->stir_rlc[j], e3_pow(z, (u64)(k - (1u << CA_LO)) << CA_LO));
+        } else if (k < (1u << CA_LO)) {
+            lo_base[(u64)(j - n_ext) * (1u << CA_LO) + k] = gl_pow(z.c0, k);
+        } else {
+            tab[e] = e3_mul_base(sc->stir_rlc[j], gl_pow(z.c0, (u64)(k - (1u << CA_LO)) << CA_LO));
+        }
     }
 }
 
-__global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* tab, u32 hi_count) {
+__global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* tab, const u64* lo_base, u32 hi_count) {
     const u32 per = (1u << CA_LO) + hi_count;
     const int npts = a.n_ext + a.n_base;
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.size; i += (u64)gridDim.x * blockDim.x) {
@@ -512,7 +521,9 @@ __global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* 
         E3Acc s = e3acc_zero();
         const E3* tj = tab;
         for (int j = 0; j < a.n_ext; ++j, tj += per) e3acc_mac(s, tj[(1u << CA_LO) + hi], tj[lo]);
-        for (int j = a.n_ext; j < npts; ++j, tj += per) e3acc_mac_base(s, tj[(1u << CA_LO) + hi], tj[lo].c0);
+        const u64* lb = lo_base + lo;
+        for (int j = a.n_ext; j < npts; ++j, tj += per, lb += (1u << CA_LO))
+            e3acc_mac_base(s, tj[(1u << CA_LO) + hi], *lb);
         const E3 add = e3acc_reduce(s);
         a.cov[0][i] = gl_add(a.cov[0][i], add.c0);
         a.cov[1][i] = gl_add(a.cov[1][i], add.c1);
@@ -523,7 +534,8 @@ __global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* 
 static u32 ca_hi_count(u64 size) { return (u32)((size + (1ull << CA_LO) - 1) >> CA_LO) + 1; }
 
 size_t cov_acc_scratch_bytes(u64 size, int n_points) {
-    return ((size_t)(1u << CA_LO) + ca_hi_count(size)) * (size_t)n_points * sizeof(E3) + 256;
+    return ((size_t)(1u << CA_LO) + ca_hi_count(size)) * (size_t)n_points * sizeof(E3) + 256 +
+           (size_t)n_points * (1u << CA_LO) * sizeof(u64);
 }
 
 int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
@@ -531,10 +543,12 @@ int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
     if (npts == 0 || a.size == 0) return 0;
     const u32 hc = ca_hi_count(a.size);
     E3* tab = reinterpret_cast<E3*>(a.scratch);
-    k_cov_acc_tables<<<296, 256, 0, st>>>(a.sc, npts, hc, tab);
+    const size_t tab_bytes = ((size_t)(1u << CA_LO) + hc) * (size_t)npts * sizeof(E3);
+    u64* lo_base = reinterpret_cast<u64*>(reinterpret_cast<char*>(a.scratch) + (tab_bytes + 255) / 256 * 256);
+    k_cov_acc_tables<<<296, 256, 0, st>>>(a.sc, a.n_ext, npts, hc, tab, lo_base);
     count_launches(1);
     u64 want = (a.size + 255) / 256;
-    k_cov_accumulate<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab, hc);
+    k_cov_accumulate<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab, lo_base, hc);
     count_launches(1);
     return 0;
 }

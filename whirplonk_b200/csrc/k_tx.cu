@@ -287,21 +287,18 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
         for (u32 k = 0; k < nbytes; ++k) acc = (acc << 8) | idx_bytes[i * nbytes + k];
         idx_s[i] = a.N == 1 ? 0 : (acc & (a.N - 1));  // N is a power of two
     }
-    if (t == 0) {
-        hint_base = wt.hints_len;
-        // eq weights of the last `fold` folding challenges (multilinear_point.hpp:40-62)
-        if (a.stir) {
-            const u32 d = 1u << a.fold;
-            for (u32 i = 0; i < d; ++i) {
-                E3 acc = e3_one();
-                for (u32 k = 0; k < a.fold; ++k) {
-                    const E3 r = sc->sc_r[a.r_offset + k];
-                    const bool bit = (i >> (a.fold - 1 - k)) & 1;
-                    acc = e3_mul(acc, bit ? r : e3_sub(e3_one(), r));
-                }
-                eqw[i] = acc;
-            }
+    if (t == 0) hint_base = wt.hints_len;
+    // eq weights of the last `fold` folding challenges (multilinear_point.hpp:40-62),
+    // one entry per thread of warps 1.. (they do not wait for warp 0's squeeze)
+    if (a.stir && t >= 32 && t - 32 < (1u << a.fold)) {
+        const u32 i = t - 32;
+        E3 acc = e3_one();
+        for (u32 k = 0; k < a.fold; ++k) {
+            const E3 r = sc->sc_r[a.r_offset + k];
+            const bool bit = (i >> (a.fold - 1 - k)) & 1;
+            acc = e3_mul(acc, bit ? r : e3_sub(e3_one(), r));
         }
+        eqw[i] = acc;
     }
     for (u32 s2 = t; s2 < (u32)MAX_QUERIES; s2 += blockDim.x) occ[s2] = 0;
     __syncthreads();
@@ -386,30 +383,34 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
         }
     }
 
-    // 3. STIR point and value of each opened row
+    // 3. STIR point and value of each opened row: a warp per row, its lanes over
+    //    the row's elements (all commitments side by side), a warp sum at the end.
     if (a.stir) {
         const u32 dmask = (1u << a.fold) - 1;
-        for (u32 i = t; i < q; i += blockDim.x) {
+        const u32 total = nwit * a.depth;
+        const u32 nwarps = blockDim.x >> 5;
+        for (u32 i = warp; i < q; i += nwarps) {
             const u64 id = idx_s[i];
             E3 val = e3_zero();
-            for (u32 w = 0; w < nwit; ++w) {
+            for (u32 k = lane; k < total; k += 32) {
+                const u32 w = k / a.depth, el = k - w * a.depth;
                 const u64* planes = a.planes + w * a.planes_stride;
-                for (u32 v0 = 0; v0 < a.depth; v0 += dmask + 1) {  // one committed vector's 2^fold columns
-                    E3 inner = e3_zero();
-                    for (u32 e = 0; e <= dmask; ++e) {
-                        const u32 el = v0 + e;
-                        E3 x;
-                        if (a.ncomp == 1) x = e3_base(planes[(u64)el * a.N + id]);
-                        else x = E3{planes[(u64)el * a.N + id], planes[((u64)a.depth + el) * a.N + id],
-                                    planes[((u64)2 * a.depth + el) * a.N + id]};
-                        inner = e3_add(inner, e3_mul(x, eqw[e]));
-                    }
-                    const u32 vec = w * (a.depth >> a.fold) + (v0 >> a.fold);
-                    val = e3_add(val, a.use_vrlc ? e3_mul(inner, sc->vrlc[vec]) : inner);
+                E3 term;
+                if (a.ncomp == 1) {
+                    term = e3_mul_base(eqw[el & dmask], planes[(u64)el * a.N + id]);
+                } else {
+                    term = e3_mul(E3{planes[(u64)el * a.N + id], planes[((u64)a.depth + el) * a.N + id],
+                                     planes[((u64)2 * a.depth + el) * a.N + id]},
+                                  eqw[el & dmask]);
                 }
+                if (a.use_vrlc) term = e3_mul(term, sc->vrlc[w * (a.depth >> a.fold) + (el >> a.fold)]);
+                val = e3_add(val, term);
             }
-            sc->stir_pts[a.ood_offset + i] = e3_base(gl_pow(a.gen, id));
-            sc->stir_vals[a.ood_offset + i] = val;
+            val = e3_warp_sum(val);
+            if (lane == 0) {
+                sc->stir_pts[a.ood_offset + i] = e3_base(gl_pow(a.gen, id));
+                sc->stir_vals[a.ood_offset + i] = val;
+            }
         }
     }
 
