@@ -104,6 +104,54 @@ def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1
         return read_output(out, npts, batch_size * num_witnesses)
 
 
+REF_ZK_DRIVER = os.path.join(HERE, "_ref", "ref_zk_driver")
+
+
+@dataclass
+class RefZkProof:
+    narg: bytes
+    hints: bytes
+    evaluations: np.ndarray  # (num_forms * num_polys,) uint64, form-major
+    verify_ok: float
+    num_blinding_variables: int
+    blinded_queries: int
+    blinding_batch: int
+
+
+def run_reference_zk(n, k, rho, sec, pow_bits, forms, polys, seed, sha2=False, no_pow=True, policy=(0, 0, 0, 0),
+                     verify=True, timeout=3600) -> RefZkProof:
+    """Runs the reference zero-knowledge WHIR prover (oracle/_ref/ref_zk_driver).
+    ``forms``: [("mle", (n,) words) | ("covector", (2^n,) words)] over the base
+    field; ``polys``: (num_polys, 2^n).  ``policy`` (q_delta_1, q_delta_2, t1, t2),
+    all 0 to derive it from the parameters."""
+    polys = np.ascontiguousarray(polys, dtype=np.uint64).reshape(-1, 1 << n)
+    with tempfile.TemporaryDirectory() as td:
+        inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(inp, "wb") as f:
+            f.write(struct.pack("<II", 0x4B5A4857, 1))
+            f.write(struct.pack("<14Q", n, k, rho, sec, pow_bits, len(forms), polys.shape[0], int(sha2),
+                                int(no_pow), *policy, seed))
+            for kind, data in forms:
+                data = np.ascontiguousarray(data, dtype=np.uint64).reshape(-1)
+                assert data.size == (n if kind == "mle" else 1 << n)
+                f.write(struct.pack("<Q", 0 if kind == "mle" else 1))
+                f.write(data.tobytes())
+            f.write(polys.tobytes())
+        cmd = [REF_ZK_DRIVER, inp, out] + (["--verify"] if verify else [])
+        subprocess.run(cmd, check=True, timeout=timeout, stdout=subprocess.DEVNULL)
+        b = open(out, "rb").read()
+    pos = 0
+    (ln,) = struct.unpack_from("<Q", b, pos); pos += 8
+    narg = b[pos:pos + ln]; pos += ln
+    (lh,) = struct.unpack_from("<Q", b, pos); pos += 8
+    hints = b[pos:pos + lh]; pos += lh
+    cnt = len(forms) * polys.shape[0]
+    ev = np.frombuffer(b, dtype=np.uint64, count=cnt, offset=pos).copy(); pos += 8 * cnt
+    (vok,) = struct.unpack_from("<d", b, pos); pos += 8
+    nbv, q, nb = struct.unpack_from("<3Q", b, pos)
+    return RefZkProof(narg, hints, ev, vok, nbv, q, nb)
+
+
 class OracleTranscript:
     """The oracle's SHAKE128 prover transcript (absorb / message / squeeze)."""
 

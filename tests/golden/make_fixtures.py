@@ -21,7 +21,9 @@ has the reference checkout; the tests only read the JSON files).
    several witnesses), including rows wider than one BLAKE3 chunk; "forms"
    statements that mix MultilinearExtension and dense Covector linear forms;
    "unique" proofs under unique decoding, including statement-free ones;
-   "field1" proofs over Identity<Goldilocks> (the CLI's --field Goldilocks1).
+   "field1" proofs over Identity<Goldilocks> (the CLI's --field Goldilocks1);
+   "zk" zero-knowledge WHIR proofs (oracle/_ref/ref_zk_driver, masks from the
+   reference's DeterministicRng with the case's seed).
 """
 import hashlib
 import json
@@ -429,6 +431,38 @@ def proofs_field1():
     return out
 
 
+ZK_CASES = [  # zero-knowledge WHIR (ZkConfig<Goldilocks>), every PoW disabled as the reference's dumper does:
+    # (n, k, rho, security, seed, form kinds, num_polynomials, hash, policy (q_delta_1, q_delta_2, t1, t2) or None)
+    (8, 2, 1, 16, 101, ("covector",), 1, "sha2", (4, 4, 4, 4)),   # the shape of cpp/tests/dump_whir_zk.cpp
+    (10, 2, 1, 16, 102, ("mle",), 1, "blake3", (4, 4, 4, 4)),
+    (12, 3, 2, 20, 103, ("mle", "covector"), 2, "blake3", (6, 6, 6, 6)),
+    (16, 4, 1, 32, 104, ("mle",), 1, "blake3", None),
+    (18, 4, 1, 40, 105, ("mle", "covector"), 1, "sha2", None),
+]
+
+
+def proofs_zk():
+    from oracle.refio import run_reference_zk
+    from tests.golden.forms import form_inputs
+
+    out = []
+    for (n, k, rho, sec, seed, kinds, npolys, eng, policy) in ZK_CASES:
+        polys, forms = form_inputs(n, seed, kinds, npolys, base_field=True)
+        ref = run_reference_zk(n, k, rho, sec, 0, [(kind, d[:, 0]) for kind, d in forms], polys, seed,
+                               sha2=eng == "sha2", no_pow=True, policy=policy or (0, 0, 0, 0))
+        assert ref.verify_ok == 1.0
+        rec = {"n": n, "k": k, "rho": rho, "security": sec, "seed": seed, "kinds": list(kinds),
+               "num_polynomials": npolys, "hash": eng, "policy": list(policy) if policy else None,
+               "evaluations": [int(x) for x in ref.evaluations],
+               "num_blinding_variables": ref.num_blinding_variables, "blinded_queries": ref.blinded_queries,
+               "blinding_batch": ref.blinding_batch,
+               "narg_len": len(ref.narg), "hints_len": len(ref.hints),
+               "narg_sha256": hashlib.sha256(ref.narg).hexdigest(),
+               "hints_sha256": hashlib.sha256(ref.hints).hexdigest()}
+        out.append(rec)
+    return out
+
+
 def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
@@ -440,7 +474,7 @@ def main():
         json.dump({"generator": "oracle/_ref/ref_driver (reference C++ prover, CLI domain separator, "
                                 "seeded ChaCha20 inputs via whirgpu_sample_goldilocks)", "cases": proofs(),
                    "multi": proofs_multi(), "forms": proofs_forms(), "unique": proofs_unique(),
-                   "field1": proofs_field1()}, f, indent=1)
+                   "field1": proofs_field1(), "zk": proofs_zk()}, f, indent=1)
 
 
 if __name__ == "__main__":
