@@ -107,7 +107,7 @@ whirgpu_status whirgpu_commit(whirgpu_ctx* ctx, const whirgpu_params* params, co
  * for all of them; whirgpu_prove then proves every vector.  At most
  * WHIRGPU_MAX_WITNESSES witnesses and WHIRGPU_MAX_VECTORS vectors in all. */
 #define WHIRGPU_MAX_WITNESSES 8
-#define WHIRGPU_MAX_VECTORS 32
+#define WHIRGPU_MAX_VECTORS 64
 whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* ctx, const whirgpu_params* params, const uint64_t* coeffs,
                                         uint64_t num_witnesses, uint64_t num_variables, int coeffs_location,
                                         whirgpu_transcript* tx, whirgpu_witness** out);
@@ -187,6 +187,47 @@ whirgpu_status whirgpu_prove_forms(whirgpu_ctx* ctx, whirgpu_witness* witness, c
 
 /* Bytes the last commit + prove pair moved host->device and device->host. */
 void whirgpu_last_io_bytes(const whirgpu_ctx* ctx, uint64_t* h2d, uint64_t* d2h);
+
+/* ---- zero-knowledge WHIR (ZkConfig<Goldilocks>, protocols/whir_zk) ------------------
+ * ZkConfig::from_params / from_params_with_policy (whir_zk.hpp:95-105, 270-289):
+ * `blinded` is the Config<Identity<Goldilocks>> of each f_hat = f + mask (one
+ * vector per commitment), `blinding` the Config of the num_polynomials *
+ * (num_variables + 1) blinding vectors of 2^(num_blinding_variables + 1)
+ * entries.  policy NULL: BlindingSizePolicy::from_whir_params
+ * (whir_zk.hpp:48-62).  WHIRGPU_E_INVALID where the reference asserts
+ * (num_blinding_variables + 1 >= num_variables). */
+typedef struct {
+    uint64_t q_delta_1, q_delta_2, t1, t2, sumcheck_round_degree;
+} whirgpu_zk_policy;
+typedef struct {
+    whirgpu_config blinded, blinding;
+    uint64_t num_polynomials, num_witness_variables, num_blinding_variables;
+} whirgpu_zk_config;
+whirgpu_status whirgpu_zk_config_from_params(const whirgpu_params* params, uint64_t num_variables,
+                                             uint64_t num_polynomials, const whirgpu_zk_policy* policy,
+                                             whirgpu_zk_config* out);
+typedef struct whirgpu_zk_witness whirgpu_zk_witness;
+/* ZkConfig::commit (whir_zk_impl.hpp:42-95) with the masks drawn from
+ * DeterministicRng(seed, rng_domain) (deterministic_rng.hpp) starting at
+ * counter 0: coeffs holds num_polynomials * 2^num_variables base-field
+ * coefficients, polynomial i's first.  The num_polynomials blinded
+ * commitments and the blinding commitment go to tx in that order.  Up to
+ * WHIRGPU_MAX_WITNESSES polynomials and WHIRGPU_MAX_VECTORS blinding vectors;
+ * rng_domain up to 128 bytes. */
+whirgpu_status whirgpu_zk_commit(whirgpu_ctx* ctx, const whirgpu_zk_config* config, const uint64_t* coeffs,
+                                 int coeffs_location, const uint8_t seed[32], const char* rng_domain,
+                                 size_t rng_domain_len, whirgpu_transcript* tx, whirgpu_zk_witness** out);
+/* ZkConfig::prove (whir_zk_impl.hpp:150-330): up to 7 linear forms as in
+ * whirgpu_prove_forms, over the base field (every Ext3 value (x, 0, 0)), and
+ * num_forms * num_polynomials claimed evaluations (Ext3 layout, form-major).
+ * On return the proof is complete and readable with whirgpu_proof_get. */
+whirgpu_status whirgpu_zk_prove(whirgpu_ctx* ctx, whirgpu_zk_witness* witness, const whirgpu_linear_form* forms,
+                                size_t num_forms, const uint64_t* evaluations, whirgpu_transcript* tx);
+void whirgpu_zk_witness_destroy(whirgpu_zk_witness* witness);
+/* The DeterministicRng byte stream (deterministic_rng.hpp:16-98) as 64-bit LE
+ * words first_word .. first_word + count - 1, computed on the device. */
+whirgpu_status whirgpu_deterministic_rng(whirgpu_ctx* ctx, const uint8_t seed[32], const char* domain,
+                                         size_t domain_len, uint64_t first_word, uint64_t* out, size_t count);
 
 /* ---- many proofs at once --------------------------------------------------------
  * A request is one complete commit + prove (with its own domain separator).

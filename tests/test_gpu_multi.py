@@ -144,11 +144,11 @@ def test_multi_vector_batch_and_server_identity():
 
 def test_multi_vector_limits(gpu_ctx):
     n = 8
-    coeffs = sample_goldilocks(6180, 33 << n).reshape(33, 1 << n)
+    coeffs = sample_goldilocks(6180, 65 << n).reshape(65, 1 << n)
     points = sample_goldilocks(6181, n * 3).reshape(1, n, 3)
-    evals = np.zeros((33, 3), dtype=np.uint64)
-    with pytest.raises(WhirGpuError):  # more than 32 vectors
-        prove_once(n, params(batch=33), coeffs, points, evals, ctx=gpu_ctx)
+    evals = np.zeros((65, 3), dtype=np.uint64)
+    with pytest.raises(WhirGpuError):  # more than 64 vectors
+        prove_once(n, params(batch=65), coeffs, points, evals, ctx=gpu_ctx)
     with pytest.raises(WhirGpuError):  # more than 8 witnesses
         prove_once(n, params(batch=1), coeffs[:9], points, evals[:9], ctx=gpu_ctx, num_witnesses=9)
     # the context stays usable

@@ -1,0 +1,82 @@
+"""Zero-knowledge WHIR (ZkConfig<Goldilocks>) on the GPU: every proof must equal,
+byte for byte, the reference prover's proof for the same polynomials, forms and
+DeterministicRng seed (the "zk" fixtures of reference_proofs.json, made by
+oracle/_ref/ref_zk_driver, which the reference's verifier accepted)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from tests.zk_cases import case_config, case_params, case_seed, case_statement
+from whirplonk_b200 import ProverState, cli_domain_separator
+from whirplonk_b200._lib import WhirGpuError
+from whirplonk_b200.zk import DeterministicRng, prove_zk_once
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+ZK = json.load(open(os.path.join(HERE, "golden", "reference_proofs.json")))["zk"]
+
+
+def rng_words_oracle(oracle, seed, domain, first, count):
+    """DeterministicRng (deterministic_rng.hpp:16-98) over the oracle's BLAKE3."""
+    d = domain.encode()
+    pre = b"WHIR_DETERMINISTIC_RNG_V1" + len(d).to_bytes(4, "little") + d + seed
+    stream = b""
+    c = first // 4
+    while len(stream) < 8 * (first - 4 * (first // 4) + count):
+        stream += oracle.blake3(pre + c.to_bytes(8, "little"))
+        c += 1
+    skip = 8 * (first % 4)
+    return np.frombuffer(stream[skip:skip + 8 * count], dtype=np.uint64)
+
+
+def test_deterministic_rng_matches_construction(gpu_ctx, oracle):
+    seed = bytes(range(32))
+    for domain, first, count in (("WHIR_ZK:mask", 0, 37), ("x" * 100, 5, 50), ("", 3, 1)):
+        got = DeterministicRng(seed, domain).words(first, count, gpu_ctx)
+        assert np.array_equal(got, rng_words_oracle(oracle, seed, domain, first, count))
+
+
+@pytest.mark.parametrize("case", ZK, ids=lambda c: f"n{c['n']}_s{c['seed']}")
+def test_zk_proof_equals_reference(gpu_ctx, case):
+    cfg = case_config(case)
+    polys, forms, evals = case_statement(case)
+    narg, hints = prove_zk_once(case["n"], case_params(case), polys, forms, evals, case_seed(case), ctx=gpu_ctx,
+                                config=cfg)
+    assert (len(narg), len(hints)) == (case["narg_len"], case["hints_len"])
+    assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    assert hashlib.sha256(hints).hexdigest() == case["hints_sha256"]
+
+
+def test_zk_proof_from_device_input_and_reuse(gpu_ctx):
+    """Coefficients already in HBM give the same proof; a witness proves once."""
+    import torch
+
+    case = ZK[1]
+    cfg = case_config(case)
+    polys, forms, evals = case_statement(case)
+    dev = torch.from_numpy(polys.view(np.int64).copy()).cuda()
+    torch.cuda.synchronize()
+    ps = ProverState.from_ds(cli_domain_separator(case_params(case)), b"", gpu_ctx)
+    rng = DeterministicRng(case_seed(case))
+    w = cfg.commit(ps, None, rng, on_device_ptr=dev.data_ptr())
+    cfg.prove(ps, polys, w, forms, evals, rng)
+    narg, _ = ps.proof()
+    assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    with pytest.raises(WhirGpuError):
+        cfg.prove(ps, polys, w, forms, evals, rng)
+
+
+def test_zk_masks_follow_the_seed(gpu_ctx):
+    """Another RNG seed gives other masks, hence other commitments and another
+    proof of the same statement."""
+    case = ZK[0]
+    cfg = case_config(case)
+    polys, forms, evals = case_statement(case)
+    seed = bytearray(case_seed(case))
+    seed[31] ^= 1
+    narg, _ = prove_zk_once(case["n"], case_params(case), polys, forms, evals, bytes(seed), ctx=gpu_ctx, config=cfg)
+    assert len(narg) == case["narg_len"]
+    assert hashlib.sha256(narg).hexdigest() != case["narg_sha256"]

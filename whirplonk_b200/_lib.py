@@ -33,6 +33,8 @@ EXPORTED = [
     "whirgpu_rs_encode", "whirgpu_rs_commit_batch",
     "whirgpu_ntt_autotune", "whirgpu_ntt_set_plan", "whirgpu_ntt_get_plan", "whirgpu_ntt_clear_plans",
     "whirgpu_ntt_list_plans", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans", "whirgpu_ntt_load_default_plans",
+    "whirgpu_zk_config_from_params", "whirgpu_zk_commit", "whirgpu_zk_prove", "whirgpu_zk_witness_destroy",
+    "whirgpu_deterministic_rng",
 ]
 
 
@@ -95,6 +97,18 @@ class WhirConfig(ctypes.Structure):
                 ("initial_skip_pow", ctypes.c_uint64), ("num_rounds", ctypes.c_uint64),
                 ("round_configs", RoundConfig * MAX_ROUNDS), ("final_sumcheck", SumcheckConfig),
                 ("final_pow", ctypes.c_uint64)]
+
+
+class ZkPolicy(ctypes.Structure):
+    """Mirror of whirgpu_zk_policy (BlindingSizePolicy, whir_zk.hpp:45-63)."""
+    _fields_ = [("q_delta_1", ctypes.c_uint64), ("q_delta_2", ctypes.c_uint64), ("t1", ctypes.c_uint64),
+                ("t2", ctypes.c_uint64), ("sumcheck_round_degree", ctypes.c_uint64)]
+
+
+class ZkConfig(ctypes.Structure):
+    """Mirror of whirgpu_zk_config (ZkConfig<Goldilocks>, whir_zk.hpp:83-93)."""
+    _fields_ = [("blinded", WhirConfig), ("blinding", WhirConfig), ("num_polynomials", ctypes.c_uint64),
+                ("num_witness_variables", ctypes.c_uint64), ("num_blinding_variables", ctypes.c_uint64)]
 
 
 class LinearForm(ctypes.Structure):
@@ -219,6 +233,15 @@ def load() -> ctypes.CDLL:
     L.whirgpu_ntt_save_plans.argtypes = [ctypes.c_char_p]
     L.whirgpu_ntt_load_default_plans.argtypes = []
     L.whirgpu_ntt_load_default_plans.restype = None
+    L.whirgpu_zk_config_from_params.argtypes = [ctypes.POINTER(WhirParams), u64, u64, ctypes.POINTER(ZkPolicy),
+                                                ctypes.POINTER(ZkConfig)]
+    L.whirgpu_zk_commit.argtypes = [p, ctypes.POINTER(ZkConfig), p, i32, p, ctypes.c_char_p, sz, p, vp]
+    L.whirgpu_zk_prove.argtypes = [p, p, ctypes.POINTER(LinearForm), sz, p, p]
+    L.whirgpu_zk_witness_destroy.argtypes = [p]
+    L.whirgpu_zk_witness_destroy.restype = None
+    L.whirgpu_deterministic_rng.argtypes = [p, p, ctypes.c_char_p, sz, u64, p, sz]
+    for name in ("whirgpu_zk_config_from_params", "whirgpu_zk_commit", "whirgpu_zk_prove", "whirgpu_deterministic_rng"):
+        getattr(L, name).restype = i32
     for name in ("whirgpu_rs_encode", "whirgpu_rs_commit_batch", "whirgpu_ntt_autotune", "whirgpu_ntt_set_plan",
                  "whirgpu_ntt_get_plan", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans"):
         getattr(L, name).restype = i32

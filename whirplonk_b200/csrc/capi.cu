@@ -297,6 +297,7 @@ void whirgpu_ctx_destroy(whirgpu_ctx* c) {
         }
         c->live_witnesses.clear();
     }
+    zk_detach_all(c);
     for (auto& kv : c->cache)
         for (Workspace* w : kv.second) free_workspace(c, w);
     cudaFree(c->tw.tw_stage);
@@ -479,6 +480,14 @@ whirgpu_status whirgpu_commit_config(whirgpu_ctx* c, const whirgpu_config* cfg, 
     pp.batch_size = cfg->batch_size;
     pp.hash = is_sha2(&hp) ? 1 : 0;
     pp.field_degree = (int)cfg->field;
+    const WhirSchedule s = schedule_from_config(cfg);
+    return commit_schedule(c, s, pp, coeffs, num_witnesses, where, tx, out);
+}
+
+}  // extern "C"
+
+namespace wg {
+WhirSchedule schedule_from_config(const whirgpu_config* cfg) {
     WhirSchedule s;
     s.initial = from_irs(cfg->initial_committer);
     s.initial_sumcheck = {s.initial.vector_size, cfg->initial_sumcheck.num_rounds, cfg->initial_sumcheck.pow_threshold};
@@ -498,8 +507,11 @@ whirgpu_status whirgpu_commit_config(whirgpu_ctx* c, const whirgpu_config* cfg, 
     int n = 0;
     while (n < 40 && (1ull << n) < s.initial.vector_size) ++n;
     s.num_variables = (uint64_t)n;
-    return commit_schedule(c, s, pp, coeffs, num_witnesses, where, tx, out);
+    return s;
 }
+}  // namespace wg
+
+extern "C" {
 
 whirgpu_status whirgpu_commit_witnesses(whirgpu_ctx* c, const whirgpu_params* params, const uint64_t* coeffs,
                                         uint64_t num_witnesses, uint64_t n, int where, whirgpu_transcript* tx,

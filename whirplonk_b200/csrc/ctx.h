@@ -108,6 +108,7 @@ struct whirgpu_ctx {
     // Witnesses not yet destroyed: destroying the context detaches them, so a
     // witness destroyed afterwards only frees its handle.
     std::set<whirgpu_witness*> live_witnesses;
+    std::set<whirgpu_zk_witness*> live_zk;  // the same for zero-knowledge witnesses
 };
 
 struct whirgpu_transcript {
@@ -148,4 +149,9 @@ bool is_sha2(const whirgpu_params* p);
 bool engine_supported(const whirgpu_params* p);  // BLAKE3 or SHA-2
 // Plan size of one proof (bytes of device workspace), or 0 when invalid.
 size_t workspace_bytes(uint64_t n, const whirgpu_params* params, uint32_t nwit = 1);
+// The schedule of a Config given field by field (shape checks: validate_schedule).
+WhirSchedule schedule_from_config(const whirgpu_config* cfg);
+// Frees the device memory of every live zero-knowledge witness of the context
+// and detaches them (their later destroy only frees the handle).
+void zk_detach_all(whirgpu_ctx* c);
 }  // namespace wg

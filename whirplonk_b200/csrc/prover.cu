@@ -174,7 +174,7 @@ void plan_set_forms(ProofPlan& p, int n_forms) {
     p.narg_len = n_forms + p.sch.initial.out_domain > 0 ? p.narg_len_constrained : p.narg_len_free;
 }
 
-TxState* plan_tx(const ProofPlan& p, char* ws) { return reinterpret_cast<TxState*>(ws + p.off_tx); }
+TxState* plan_tx(const ProofPlan& p, char* ws) { return p.tx_ext ? p.tx_ext : reinterpret_cast<TxState*>(ws + p.off_tx); }
 ProofScalars* plan_scalars(const ProofPlan& p, char* ws) { return reinterpret_cast<ProofScalars*>(ws + p.off_scalars); }
 
 namespace {
@@ -301,9 +301,10 @@ int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_f
 }  // namespace
 
 int enqueue_commit(const ProofPlan& p, char* ws, uint32_t ds_len, const DeviceTables& tw, cudaStream_t st,
-                   Timer* timer) {
+                   Timer* timer, bool init_tx) {
     Ctx c{p, ws, tw, st, timer};
-    WG_TIMED(c, FAM_TX, launch_tx_init(c.tx(), reinterpret_cast<const unsigned char*>(ws + p.off_ds), ds_len,
+    if (init_tx)
+        WG_TIMED(c, FAM_TX, launch_tx_init(c.tx(), reinterpret_cast<const unsigned char*>(ws + p.off_ds), ds_len,
                           reinterpret_cast<unsigned char*>(ws + p.off_narg), p.narg_len + 64,
                           reinterpret_cast<unsigned char*>(ws + p.off_hints), p.hints_cap + 64, c.sc(),
                           (unsigned)p.params.field_degree, st));

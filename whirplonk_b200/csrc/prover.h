@@ -49,6 +49,10 @@ struct ProofPlan {
     size_t ds_cap = 0;
     size_t total_bytes = 0;
     size_t total_sumcheck_rounds = 0;
+    // When set, the transcript state lives here instead of in the workspace:
+    // several plans then share one sponge and one proof stream (the two inner
+    // proofs of the zero-knowledge prover).
+    TxState* tx_ext = nullptr;
 };
 
 // Sets the statement's form count; a proof with no form and no OOD sample has
@@ -72,10 +76,11 @@ struct DeviceTables {
 
 // Enqueue the whole commit (Config::commit, once per initial commitment) on
 // `st`.  The workspace must hold the nvec coefficient vectors at off_coeffs and
-// the domain-separator bytes at off_ds.
+// the domain-separator bytes at off_ds.  Without init_tx the commit continues
+// the transcript already in plan_tx(p, ws).
 struct Timer;
 int enqueue_commit(const ProofPlan& p, char* ws, uint32_t ds_len, const DeviceTables& tw, cudaStream_t st,
-                   Timer* timer = nullptr);
+                   Timer* timer = nullptr, bool init_tx = true);
 // Enqueue Config::prove for MLE-point statements (points at off_points,
 // claimed evaluations already in ProofScalars::forms_eval, form-major over
 // the nvec vectors).

@@ -16,7 +16,7 @@ constexpr int MAX_FORMS = 8;        // statement linear forms
 constexpr int MAX_QUERIES = 1024;   // in-domain samples per opening
 constexpr int MAX_SC_ROUNDS = 64;   // total sumcheck rounds (= num_variables)
 constexpr int MAX_WITNESSES = 8;    // initial commitments proven together
-constexpr int MAX_VECTORS = 32;     // committed vectors over all initial commitments
+constexpr int MAX_VECTORS = 64;     // committed vectors over all initial commitments
 constexpr int MAX_COMMITS = 32;     // initial + round commitments
 constexpr int MAX_DEPTH = 64;       // interleaving depth 2^k
 constexpr int MAX_INIT_OOD = MAX_WITNESSES * MAX_OOD;
