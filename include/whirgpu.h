@@ -6,7 +6,9 @@
  * proof byte layout ({narg_string, hints}), for
  *   M = Basefield<GoldilocksExt3> (Goldilocks vectors, Ext3 challenges),
  *   hash = BLAKE3 or SHA-2, one or more witnesses of batch_size vectors,
- *   statements of MultilinearExtension and dense Covector forms.
+ *   statements of MultilinearExtension and dense Covector forms;
+ * also M = Identity<Goldilocks>, Configs given field by field, and the
+ * zero-knowledge prover ZkConfig<Goldilocks> (protocols/whir_zk).
  * Everything below is plain C: opaque handles, pointers, sizes and status
  * codes; no C++ types or exceptions cross this boundary.
  *
@@ -27,7 +29,7 @@ extern "C" {
 typedef enum {
     WHIRGPU_OK = 0,
     WHIRGPU_E_INVALID = 1,     /* bad argument or parameters the reference asserts on */
-    WHIRGPU_E_UNSUPPORTED = 2, /* valid for the reference but not on this path (e.g. more than 32 vectors) */
+    WHIRGPU_E_UNSUPPORTED = 2, /* valid for the reference but not on this path (e.g. more than 64 vectors) */
     WHIRGPU_E_OOM = 3,         /* device or pinned memory exhausted, or above the HBM budget */
     WHIRGPU_E_CUDA = 4,        /* CUDA runtime error (text in whirgpu_last_error) */
     WHIRGPU_E_DEVICE = 5,      /* a kernel reported an error word (overflow, PoW exhausted) */
@@ -206,6 +208,15 @@ typedef struct {
 whirgpu_status whirgpu_zk_config_from_params(const whirgpu_params* params, uint64_t num_variables,
                                              uint64_t num_polynomials, const whirgpu_zk_policy* policy,
                                              whirgpu_zk_config* out);
+/* The canonical ZK configuration bytes and domain separator
+ * (canonical_config.hpp:38-87, whir_zk_domain_separator): config_bytes
+ * (optional, WHIRGPU_ZK_CONFIG_BYTES bytes) = "WHIR_ZK_CONFIG_V1" || sizes,
+ * parameters and policy as LE u64 words; out = SHA3-512(config_bytes) ||
+ * SHA3-256(CBOR text session).  policy NULL: the derived policy.  Host only. */
+#define WHIRGPU_ZK_CONFIG_BYTES 154
+whirgpu_status whirgpu_zk_domain_separator(const whirgpu_params* params, uint64_t vector_size, uint64_t num_polynomials,
+                                          const whirgpu_zk_policy* policy, const char* session, size_t session_len,
+                                          uint8_t* config_bytes, uint8_t out[96]);
 typedef struct whirgpu_zk_witness whirgpu_zk_witness;
 /* ZkConfig::commit (whir_zk_impl.hpp:42-95) with the masks drawn from
  * DeterministicRng(seed, rng_domain) (deterministic_rng.hpp) starting at

@@ -366,6 +366,30 @@ def proofs_unique():
 WHIR_GOLDEN_SHAPES = [(1, 2), (1, 4), (1, 8), (3, 4), (4, 8)]  # (num_vectors, vector_size), cpp/tests/dump_whir.cpp:197-205
 
 
+def whir_zk_golden():
+    """The reference's zero-knowledge dumper (cpp/tests/dump_whir_zk.cpp, built
+    unmodified into oracle/_ref/dump_whir_zk; no dump of it is committed in the
+    reference): n = 8, SHA-2, policy (4, 4, 4, 4), polynomial 17 i + 3, an
+    all-ones Covector, the canonical ZK domain separator with session
+    "whir_zk_0", DeterministicRng(0..31, "WHIR_ZK:mask"), PoW off."""
+    import subprocess
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "dump_whir_zk")
+    text = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    rows = {}
+    for line in text.splitlines():
+        if line.startswith("    "):
+            k, _, v = line.strip().partition(" ")
+            rows[k] = v.split()
+    assert rows["verify"] == ["1"] and rows["check_eof"] == ["1"]
+    return {"canonical_config": rows["canonical_config"][0], "ds_protocol_id": rows["ds_protocol_id"][0],
+            "ds_session_id": rows["ds_session_id"][0],
+            "input_vector0": [int(x) for x in rows["input_vector0"]],
+            "f_hat_vector0": [int(x) for x in rows["f_hat_vector0"]],
+            "blinding_m_poly0": [int(x) for x in rows["blinding_m_poly0"]],
+            "narg": rows["proof_narg"][0], "hints": rows["proof_hints"][0]}
+
+
 def whir_golden():
     """The reference's whole-proof golden (cpp/tests/dump_whir.cpp; the Rust
     dump golden_whir_rs.txt is byte-identical to the C++ one): Identity<Goldilocks>,
@@ -467,7 +491,7 @@ def main():
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True, stdout=subprocess.DEVNULL)
     gold = {"fields": fields(), "blake3": hashes(), "merkle": merkle(), "matrix_commit": matrix_commit(),
             "indices": indices(), "pow": pow_golden(), "sumcheck": sumcheck(),
-            "sha2": hashes("sha2"), "merkle_sha2": merkle("sha2"), "whir": whir_golden()}
+            "sha2": hashes("sha2"), "merkle_sha2": merkle("sha2"), "whir": whir_golden(), "whir_zk": whir_zk_golden()}
     with open(os.path.join(HERE, "reference_goldens.json"), "w") as f:
         json.dump(gold, f, indent=1)
     with open(os.path.join(HERE, "reference_proofs.json"), "w") as f:

@@ -80,3 +80,32 @@ def test_zk_masks_follow_the_seed(gpu_ctx):
     narg, _ = prove_zk_once(case["n"], case_params(case), polys, forms, evals, bytes(seed), ctx=gpu_ctx, config=cfg)
     assert len(narg) == case["narg_len"]
     assert hashlib.sha256(narg).hexdigest() != case["narg_sha256"]
+
+
+GOLD_ZK = json.load(open(os.path.join(HERE, "golden", "reference_goldens.json")))["whir_zk"]
+
+
+def test_reference_zk_dump(gpu_ctx):
+    """The reference's own ZK dumper (cpp/tests/dump_whir_zk.cpp): canonical
+    domain separator, SHA-2, explicit policy, Covector of ones, seed 0..31."""
+    from whirplonk_b200 import Covector, ProtocolParameters
+    from whirplonk_b200.whir import ENGINE_ID_SHA2
+    from whirplonk_b200.zk import BlindingSizePolicy, ZkConfig, whir_zk_domain_separator
+    from tests.zk_cases import disable_pow
+
+    n = 8
+    p = ProtocolParameters(False, 1, 2, 2, 16, 0, 1, ENGINE_ID_SHA2)
+    pol = BlindingSizePolicy(4, 4, 4, 4, 3)
+    cfg = ZkConfig.from_params(1 << n, p, 1, pol)
+    disable_pow(cfg.raw.blinded)
+    disable_pow(cfg.raw.blinding)
+    poly = np.array(GOLD_ZK["input_vector0"], dtype=np.uint64)
+    assert np.array_equal(poly, (np.arange(1 << n, dtype=np.uint64) * 17 + 3))
+    ones = np.zeros((1 << n, 3), dtype=np.uint64)
+    ones[:, 0] = 1
+    ev = int(sum(int(x) for x in poly) % 0xFFFFFFFF00000001)
+    _, ds = whir_zk_domain_separator(1 << n, 1, p, pol, "whir_zk_0")
+    narg, hints = prove_zk_once(n, p, poly.reshape(1, -1), [Covector(ones)], [(ev, 0, 0)], bytes(range(32)),
+                                ctx=gpu_ctx, config=cfg, ds=ds)
+    assert narg.hex() == GOLD_ZK["narg"]
+    assert hints.hex() == GOLD_ZK["hints"]

@@ -35,3 +35,26 @@ def test_zk_config_rejects_what_the_reference_asserts():
         ZkConfig.from_params(1 << 12, ProtocolParameters(False, 1, 2, 2, 16, 0, 2), 1, BlindingSizePolicy(4, 4, 4, 4))
     small = ZkConfig.from_params(1 << 10, ProtocolParameters(False, 1, 2, 2, 16, 0, 1), 1, BlindingSizePolicy(4, 4, 4, 4))
     assert small.num_blinding_variables < 9
+
+
+GOLD_ZK = json.load(open(os.path.join(HERE, "golden", "reference_goldens.json")))["whir_zk"]
+
+
+def dumper_params():
+    """cpp/tests/dump_whir_zk.cpp's parameters and policy."""
+    from whirplonk_b200.whir import ENGINE_ID_SHA2
+
+    return ProtocolParameters(False, 1, 2, 2, 16, 0, 1, ENGINE_ID_SHA2), BlindingSizePolicy(4, 4, 4, 4, 3)
+
+
+def test_canonical_zk_domain_separator_matches_reference_dump():
+    from whirplonk_b200.zk import whir_zk_domain_separator
+
+    p, pol = dumper_params()
+    cb, ds = whir_zk_domain_separator(1 << 8, 1, p, pol, "whir_zk_0")
+    assert cb.hex() == GOLD_ZK["canonical_config"]
+    assert ds.protocol_id.hex() == GOLD_ZK["ds_protocol_id"]
+    assert ds.session_id.hex() == GOLD_ZK["ds_session_id"]
+    # without a policy the derived one (q_delta from the parameters) fills the tail
+    cb2, _ = whir_zk_domain_separator(1 << 8, 1, p, None, "s")
+    assert len(cb2) == len(cb) and cb2[:-40] == cb[:-40] and cb2[-40:] != cb[-40:]

@@ -34,7 +34,7 @@ EXPORTED = [
     "whirgpu_ntt_autotune", "whirgpu_ntt_set_plan", "whirgpu_ntt_get_plan", "whirgpu_ntt_clear_plans",
     "whirgpu_ntt_list_plans", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans", "whirgpu_ntt_load_default_plans",
     "whirgpu_zk_config_from_params", "whirgpu_zk_commit", "whirgpu_zk_prove", "whirgpu_zk_witness_destroy",
-    "whirgpu_deterministic_rng",
+    "whirgpu_deterministic_rng", "whirgpu_zk_domain_separator",
 ]
 
 
@@ -73,6 +73,7 @@ FORM_MLE, FORM_COVECTOR = 0, 1
 FIELD_GOLDILOCKS1, FIELD_GOLDILOCKS3 = 1, 3
 MAX_ROUNDS = 24
 NO_POW = (1 << 64) - 1
+ZK_CONFIG_BYTES = 154
 
 
 class IrsConfig(ctypes.Structure):
@@ -240,7 +241,10 @@ def load() -> ctypes.CDLL:
     L.whirgpu_zk_witness_destroy.argtypes = [p]
     L.whirgpu_zk_witness_destroy.restype = None
     L.whirgpu_deterministic_rng.argtypes = [p, p, ctypes.c_char_p, sz, u64, p, sz]
-    for name in ("whirgpu_zk_config_from_params", "whirgpu_zk_commit", "whirgpu_zk_prove", "whirgpu_deterministic_rng"):
+    L.whirgpu_zk_domain_separator.argtypes = [ctypes.POINTER(WhirParams), u64, u64, ctypes.POINTER(ZkPolicy),
+                                              ctypes.c_char_p, sz, p, p]
+    for name in ("whirgpu_zk_config_from_params", "whirgpu_zk_commit", "whirgpu_zk_prove", "whirgpu_deterministic_rng",
+                 "whirgpu_zk_domain_separator"):
         getattr(L, name).restype = i32
     for name in ("whirgpu_rs_encode", "whirgpu_rs_commit_batch", "whirgpu_ntt_autotune", "whirgpu_ntt_set_plan",
                  "whirgpu_ntt_get_plan", "whirgpu_ntt_load_plans", "whirgpu_ntt_save_plans"):

@@ -357,6 +357,34 @@ whirgpu_status whirgpu_cli_domain_separator(const whirgpu_params* p, uint8_t out
     return WHIRGPU_OK;
 }
 
+whirgpu_status whirgpu_zk_domain_separator(const whirgpu_params* p, uint64_t vector_size, uint64_t num_polynomials,
+                                          const whirgpu_zk_policy* policy, const char* session, size_t session_len,
+                                          uint8_t* config_bytes, uint8_t out[96]) {
+    if (!p || !out || (session_len && !session)) return WHIRGPU_E_INVALID;
+    const whirgpu_zk_policy pol = policy ? *policy : zk_default_policy(p);
+    std::vector<uint8_t> c;
+    auto u64le = [&c](uint64_t v) {
+        for (int i = 0; i < 8; ++i) c.push_back((uint8_t)(v >> (8 * i)));
+    };
+    static const char kMagic[] = "WHIR_ZK_CONFIG_V1";
+    c.insert(c.end(), kMagic, kMagic + sizeof(kMagic) - 1);
+    u64le(vector_size);
+    u64le(num_polynomials);
+    c.push_back(p->unique_decoding ? 1 : 0);
+    for (uint64_t v : {p->starting_log_inv_rate, p->initial_folding_factor, p->folding_factor, p->security_level,
+                       p->pow_bits, p->batch_size})
+        u64le(v);
+    c.insert(c.end(), p->hash_id, p->hash_id + 32);
+    for (uint64_t v : {pol.q_delta_1, pol.q_delta_2, pol.t1, pol.t2, pol.sumcheck_round_degree}) u64le(v);
+    if (config_bytes) std::memcpy(config_bytes, c.data(), c.size());
+    sha3_host(c.data(), c.size(), 72, out, 64);
+    std::vector<uint8_t> s;
+    cbor_head(s, 3, session_len);
+    s.insert(s.end(), session, session + session_len);
+    sha3_host(s.data(), s.size(), 136, out + 64, 32);
+    return WHIRGPU_OK;
+}
+
 whirgpu_status whirgpu_transcript_create(whirgpu_ctx* ctx, const uint8_t protocol_id[64], const uint8_t session_id[32],
                                          const uint8_t* instance, size_t instance_len, whirgpu_transcript** out) {
     if (!ctx || !protocol_id || !session_id || !out || (instance_len && !instance)) return WHIRGPU_E_INVALID;

@@ -154,4 +154,6 @@ WhirSchedule schedule_from_config(const whirgpu_config* cfg);
 // Frees the device memory of every live zero-knowledge witness of the context
 // and detaches them (their later destroy only frees the handle).
 void zk_detach_all(whirgpu_ctx* c);
+// BlindingSizePolicy::from_whir_params (whir_zk.hpp:48-62).
+whirgpu_zk_policy zk_default_policy(const whirgpu_params* p);
 }  // namespace wg

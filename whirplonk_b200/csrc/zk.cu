@@ -416,6 +416,14 @@ struct whirgpu_zk_witness {
 };
 
 namespace wg {
+whirgpu_zk_policy zk_default_policy(const whirgpu_params* p) {
+    const double rate = std::pow(0.5, (double)p->starting_log_inv_rate);
+    const bool ud = p->unique_decoding != 0;
+    const uint64_t q1 = (uint64_t)in_domain_queries(ud, (double)(p->security_level - p->pow_bits), rate);
+    const uint64_t q2 = (uint64_t)in_domain_queries(ud, (double)p->security_level, rate);
+    return {q1, q2, q1, q2, 3};
+}
+
 void zk_detach_all(whirgpu_ctx* c) {
     std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
     for (whirgpu_zk_witness* w : c->live_zk) {
@@ -444,16 +452,7 @@ whirgpu_status whirgpu_zk_config_from_params(const whirgpu_params* params, uint6
     std::memset(out, 0, sizeof(*out));
     whirgpu_status s = whirgpu_config_from_params(params, n, WHIRGPU_FIELD_GOLDILOCKS1, &out->blinded);
     if (s != WHIRGPU_OK) return s;
-    whirgpu_zk_policy pol;
-    if (policy) {
-        pol = *policy;
-    } else {  // BlindingSizePolicy::from_whir_params (whir_zk.hpp:48-62)
-        const double rate = std::pow(0.5, (double)params->starting_log_inv_rate);
-        const bool ud = params->unique_decoding != 0;
-        const uint64_t q1 = (uint64_t)in_domain_queries(ud, (double)(params->security_level - params->pow_bits), rate);
-        const uint64_t q2 = (uint64_t)in_domain_queries(ud, (double)params->security_level, rate);
-        pol = {q1, q2, q1, q2, 3};
-    }
+    const whirgpu_zk_policy pol = policy ? *policy : zk_default_policy(params);
     // from_params_with_policy (whir_zk.hpp:270-289)
     if (out->blinded.initial_sumcheck.num_rounds >= 40 || params->initial_folding_factor >= 40) return WHIRGPU_E_INVALID;
     const uint64_t k1 = 1ull << out->blinded.initial_sumcheck.num_rounds;

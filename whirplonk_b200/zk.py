@@ -23,8 +23,8 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from .whir import Context, Covector, MultilinearExtension, ProtocolParameters, ProverState, cli_domain_separator, \
-    default_context
+from .whir import Context, Covector, DomainSeparator, MultilinearExtension, ProtocolParameters, ProverState, \
+    cli_domain_separator, default_context
 
 
 @dataclass
@@ -39,6 +39,20 @@ class BlindingSizePolicy:
 
     def to_c(self) -> _lib.ZkPolicy:
         return _lib.ZkPolicy(self.q_delta_1, self.q_delta_2, self.t1, self.t2, self.sumcheck_round_degree)
+
+
+def whir_zk_domain_separator(vector_size: int, num_polynomials: int, params: ProtocolParameters,
+                             policy: Optional[BlindingSizePolicy], session: str):
+    """canonical_config::whir_zk_domain_separator (canonical_config.hpp:76-87):
+    (config bytes, DomainSeparator); policy None: the derived one."""
+    cb = ctypes.create_string_buffer(_lib.ZK_CONFIG_BYTES)
+    out = ctypes.create_string_buffer(96)
+    c = params.to_c()
+    pol = ctypes.byref(policy.to_c()) if policy is not None else None
+    s = session.encode()
+    _lib.check(_lib.load().whirgpu_zk_domain_separator(ctypes.byref(c), vector_size, num_polynomials, pol, s, len(s),
+                                                       cb, out))
+    return cb.raw, DomainSeparator(out.raw[:64], out.raw[64:])
 
 
 @dataclass
@@ -176,12 +190,14 @@ class ZkConfig:
 
 def prove_zk_once(n: int, params: ProtocolParameters, polynomials, forms: Sequence, evaluations: Sequence,
                   seed: bytes, ctx: Optional[Context] = None, policy: Optional[BlindingSizePolicy] = None,
-                  rng_domain: str = "WHIR_ZK:mask", config: Optional[ZkConfig] = None):
-    """commit + prove with the CLI domain separator; returns (narg, hints)."""
+                  rng_domain: str = "WHIR_ZK:mask", config: Optional[ZkConfig] = None,
+                  ds: Optional[DomainSeparator] = None):
+    """commit + prove; the domain separator defaults to the CLI one of params.
+    Returns (narg, hints)."""
     ctx = ctx or default_context()
     polys = np.ascontiguousarray(polynomials, dtype=np.uint64).reshape(-1, 1 << n)
     config = config or ZkConfig.from_params(1 << n, params, polys.shape[0], policy)
-    ps = ProverState.from_ds(cli_domain_separator(params), b"", ctx)
+    ps = ProverState.from_ds(ds or cli_domain_separator(params), b"", ctx)
     rng = DeterministicRng(seed, rng_domain)
     w = config.commit(ps, polys, rng)
     config.prove(ps, polys, w, forms, evaluations, rng)
