@@ -21,6 +21,12 @@ ChaCha20 keystream):
       log_inv_rate on {1, 2, 3}, in one captured CUDA graph.  A step = one run
       of the batch.
   whir_prove_n24_rate4 / _n22_rate4 / _n18_rate2: one plain proof per step.
+  whir_zk_prove_n22_rate4: one zero-knowledge proof (ZkConfig<Goldilocks>:
+      commit with DeterministicRng masks + prove) per step, n = 22, rate 1/4,
+      one polynomial, one MLE statement at a seeded base-field point; every
+      PoW off in both inner configs (over the 64-bit field the derived PoW
+      bits are 37-58, far above what any prover grinds; the reference's own ZK
+      dumper disables them the same way).
 
 Every batched or served proof is checked byte-for-byte against the plain
 path's proof of the same request.  Multi-GPU: independent replicas (each rank
@@ -57,7 +63,9 @@ WORKLOADS = {
     "whir_prove_n24_rate4": {"kind": "single", "n": 24, "rho": 2},
     "whir_prove_n22_rate4": {"kind": "single", "n": 22, "rho": 2},
     "whir_prove_n18_rate2": {"kind": "single", "n": 18, "rho": 1},
+    "whir_zk_prove_n22_rate4": {"kind": "zk", "n": 22, "rho": 2},
 }
+ZK_SEED = bytes(range(1, 9)) + bytes(24)  # the reference driver takes 8 seed bytes (the rest zero)
 DEFAULT_WORKLOAD = "whir_served_mixed_n12_24"
 FALLBACK_HBM_GBS = 6650.0
 # Families whose kernels saturate the integer-ALU pipe before HBM (ncu summaries
@@ -275,7 +283,7 @@ def reference_proof_seconds(n, rho, coeffs, point, threads):
 
 
 def workload_shapes(w, count_steps):
-    if w["kind"] == "single":
+    if w["kind"] in ("single", "zk"):
         return [(w["n"], w["rho"])] * count_steps
     if w["kind"] == "batch":
         return draw_requests(w, w["count"], w["seed"])
@@ -285,7 +293,12 @@ def workload_shapes(w, count_steps):
 def config_of(name, w, world):
     cfg = {"workload": name, "folding_factor": FOLD, "security_level": SEC, "pow_bits": POW, "hash": "BLAKE3",
            "field": "Goldilocks3", "statement": "1 MLE evaluation at a seeded Ext3 point"}
-    if w["kind"] == "single":
+    if w["kind"] == "zk":
+        cfg.update(num_variables=w["n"], log_inv_rate=w["rho"], field="Identity<Goldilocks> (ZkConfig<Goldilocks>)",
+                   statement="1 MLE evaluation at a seeded base-field point", num_polynomials=1,
+                   pow_bits="disabled in both inner configs (as the reference's ZK dumper)",
+                   masks="DeterministicRng(seed 01..08 then zeros, \"WHIR_ZK:mask\")")
+    elif w["kind"] == "single":
         cfg.update(num_variables=w["n"], log_inv_rate=w["rho"])
     else:
         cfg.update(num_variables=f"{w['dist']} on [{w['n'][0]}, {w['n'][1]}]", log_inv_rate=list(w["rho"]),
@@ -296,12 +309,31 @@ def config_of(name, w, world):
     return cfg
 
 
+def zk_inputs(n):
+    """Coefficients and a base-field MLE point (Ext3 layout, zero high parts)."""
+    from whirplonk_b200 import sample_goldilocks
+
+    coeffs = sample_goldilocks(1000 + n, 1 << n)
+    point = np.zeros((n, 3), dtype=np.uint64)
+    point[:, 0] = sample_goldilocks(9000 + n, n)
+    return coeffs, point
+
+
+def zk_reference(n, rho, coeffs, point, threads):
+    from oracle.refio import run_reference_zk
+
+    return run_reference_zk(n, FOLD, rho, SEC, POW, [("mle", point[:, 0])], coeffs.reshape(1, -1),
+                            int.from_bytes(ZK_SEED[:8], "little"), no_pow=True, verify=False, threads=threads)
+
+
 def run_reference_arm(args, rank, world):
     from oracle.refio import ref_available
 
     if rank != 0:
         return 0
     w = WORKLOADS[args.workload]
+    if w["kind"] == "zk":
+        return run_reference_zk_arm(args, w, world)
     if not ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built"}))
         return 0
@@ -332,6 +364,33 @@ def run_reference_arm(args, rank, world):
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+    return 0
+
+
+def run_reference_zk_arm(args, w, world):
+    from oracle.refio import REF_ZK_DRIVER
+
+    if not os.path.exists(REF_ZK_DRIVER):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_zk_driver not built"}))
+        return 0
+    threads = os.cpu_count() or 1
+    n, rho = w["n"], w["rho"]
+    coeffs, point = zk_inputs(n)
+    warm = min(args.warmup, 1)
+    times = [zk_reference(n, rho, coeffs, point, threads).prove_ms / 1000.0 for _ in range(warm + args.steps)]
+    timed = times[warm:]
+    total = sum(timed)
+    value = len(timed) / total
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": warm, "ms_per_step": 1000.0 * total / len(timed), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": DATA,
+        "config": config_of(args.workload, w, world) | {"parallelism": "host OpenMP (reference C++ ZK prover)"},
+        "p50_ms": 1000.0 * statistics.median(timed), "p99_ms": 1000.0 * max(timed),
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "reference",
+                         "sample": f"{len(timed)} zero-knowledge proofs (commit+prove, driver clock)"},
+        "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
     return 0
 
 
@@ -512,6 +571,140 @@ def run_single(args, H, ctx, w):
     if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample([(n, rho)], inputs, budget_s=0.0)
     inputs.close()
+    return line
+
+
+def zk_algorithmic_bytes(cfg):
+    """Per-family algorithmic bytes of one ZK proof: the two inner
+    Config<Identity<Goldilocks>> proofs with 8-byte elements (the formulas of
+    algorithmic_bytes, base field throughout)."""
+    out = {"ntt": 0, "leaf_hash": 0, "merkle": 0, "sumcheck": 0}
+    for inner, nvec in ((cfg.raw.blinded, cfg.num_polynomials), (cfg.raw.blinding, int(cfg.raw.blinding.batch_size))):
+        ic = inner.initial_committer
+        commits = [(int(ic.vector_size) * nvec, int(ic.codeword_length), int(ic.interleaving_depth) * nvec)]
+        for r in range(inner.num_rounds):
+            rc = inner.round_configs[r].irs_committer
+            commits.append((int(rc.vector_size), int(rc.codeword_length), int(rc.interleaving_depth)))
+        out["ntt"] += sum(8 * (v + N * d) for v, N, d in commits)
+        out["leaf_hash"] += sum(8 * d * N + 32 * N for v, N, d in commits)
+        out["merkle"] += sum(3 * 32 * N for v, N, d in commits)
+        size = int(ic.vector_size)
+        rounds = [int(inner.initial_sumcheck.num_rounds)] + \
+                 [int(inner.round_configs[r].sumcheck.num_rounds) for r in range(inner.num_rounds)] + \
+                 [int(inner.final_sumcheck.num_rounds)]
+        for k in rounds:  # read a and b, write both folded halves (a: the combined vector)
+            for _ in range(k):
+                out["sumcheck"] += 8 * size + 8 * size + 2 * 8 * (size // 2)
+                size //= 2
+    return out
+
+
+def run_zk(args, H, ctx, w):
+    import hashlib
+
+    from whirplonk_b200 import MultilinearExtension, ProverState, cli_domain_separator
+    from whirplonk_b200.zk import DeterministicRng, ZkConfig
+
+    torch = H.torch
+    n, rho = w["n"], w["rho"]
+    params = params_for(rho)
+    cfg = ZkConfig.from_params(1 << n, params, 1).disable_pow()
+    coeffs, point = zk_inputs(n)
+    ev = ctx.mle_evaluate(coeffs, point)
+    dev = torch.from_numpy(coeffs.view(np.int64)).to(H.device)
+    ptr = ctx._L.whirgpu_host_alloc(coeffs.nbytes)
+    pinned = np.ctypeslib.as_array((ctypes.c_uint64 * coeffs.size).from_address(ptr))
+    pinned[:] = coeffs
+    ds = cli_domain_separator(params)
+    forms = [MultilinearExtension(point)]
+    stream = torch.cuda.ExternalStream(ctx.stream, device=H.device)
+
+    def one(where):
+        ps = ProverState.from_ds(ds, b"", ctx)
+        rng = DeterministicRng(ZK_SEED)
+        if where == "device":
+            wit = cfg.commit(ps, None, rng, on_device_ptr=dev.data_ptr())
+        else:
+            wit = cfg.commit(ps, pinned, rng)
+        cfg.prove(ps, None, wit, forms, [ev], rng)
+        out = ps.proof()
+        del wit
+        return out
+
+    ref_proof = one("device")
+    for _ in range(max(args.warmup, 3) - 1):
+        one("device")
+    assert one("host") == ref_proof, "host and device inputs differ"
+    clocks = ClockSampler(H.local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = ctx.launch_count()
+    lat = []
+
+    def device_steps():
+        out = None
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = one("device")
+            b.record(stream)
+            lat.append((a, b))
+        return out
+
+    elapsed, out = H.timed(stream, device_steps)
+    launches = ctx.launch_count() - launches0
+    assert out == ref_proof
+    lat = sorted(a.elapsed_time(b) for a, b in lat)
+
+    def host_steps():
+        o = None
+        for _ in range(args.steps):
+            o = one("host")
+        return o
+
+    e2e_ms, out = H.timed(stream, host_steps)
+    h2d, d2h = ctx.last_io_bytes()
+    clk = clocks.stop()
+    assert out == ref_proof
+    # per-family device time over steps proofs against the inner proofs' algorithmic bytes
+    ctx.set_timing(True)
+    ctx.kernel_stats(reset=True)
+    for _ in range(args.steps):
+        one("device")
+    fam = {f: v[1] / args.steps for f, v in ctx.kernel_stats(reset=True).items()}
+    ctx.set_timing(False)
+    alg = zk_algorithmic_bytes(cfg)
+    dominant = max(alg.keys(), key=lambda f: fam.get(f, 0.0))
+    peak, peak_kind = read_peaks()
+    achieved = alg[dominant] / (fam[dominant] / 1000.0) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": read_traffic(dominant, alg[dominant]), "kernel": dominant, "peak_source": peak_kind,
+            "algorithmic_bytes_per_proof": alg[dominant], "ms_per_proof": fam[dominant],
+            "traffic_unit": "DRAM bytes per proof of the family (ratio of the plain-proof capture)",
+            "binding_limit": ALU_BOUND.get(dominant, "HBM")}
+    total = args.steps * H.world
+    line = {
+        "value": total / (elapsed / 1000.0), "ms_per_step": elapsed / args.steps, "prove_ms": elapsed / args.steps,
+        "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99),
+        "e2e": {"value": total / (e2e_ms / 1000.0), "unit": "proofs/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches, "roofline": roof, "families_ms_per_proof": {f: round(v, 4) for f, v in fam.items()},
+        "clocks": clk, "proof_bytes": len(ref_proof[0]) + len(ref_proof[1]),
+    }
+    if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
+        from oracle.refio import REF_ZK_DRIVER
+
+        if os.path.exists(REF_ZK_DRIVER):
+            threads = os.cpu_count() or 1
+            r = zk_reference(n, rho, coeffs, point, threads)
+            same = (r.narg, r.hints) == ref_proof
+            assert same, "GPU zero-knowledge proof differs from the reference's"
+            line["cpu_baseline"] = {"value": 1000.0 / r.prove_ms, "unit": "proofs/s", "cores": threads,
+                                    "kind": "reference",
+                                    "sample": f"one zero-knowledge proof of the same input by the reference C++ "
+                                              f"prover (oracle/_ref/ref_zk_driver), {r.prove_ms / 1000.0:.2f} s; "
+                                              f"its proof bytes equal the GPU's: {same}"}
+    ctx._L.whirgpu_host_free(ptr)
     return line
 
 
@@ -710,7 +903,7 @@ def run_gpu_arm(args, rank, world, local_rank):
     H = Harness(rank, world, local_rank)
     w = WORKLOADS[args.workload]
     ctx = Context(local_rank)
-    body = {"single": run_single, "batch": run_batch, "served": run_served}[w["kind"]](args, H, ctx, w)
+    body = {"single": run_single, "batch": run_batch, "served": run_served, "zk": run_zk}[w["kind"]](args, H, ctx, w)
     line = {"metric": METRIC, "value": body.pop("value"), "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": body.pop("ms_per_step"), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": DATA,

@@ -116,10 +116,11 @@ class RefZkProof:
     num_blinding_variables: int
     blinded_queries: int
     blinding_batch: int
+    prove_ms: float = 0.0  # commit + prove inside the driver
 
 
 def run_reference_zk(n, k, rho, sec, pow_bits, forms, polys, seed, sha2=False, no_pow=True, policy=(0, 0, 0, 0),
-                     verify=True, timeout=3600) -> RefZkProof:
+                     verify=True, timeout=3600, threads=None) -> RefZkProof:
     """Runs the reference zero-knowledge WHIR prover (oracle/_ref/ref_zk_driver).
     ``forms``: [("mle", (n,) words) | ("covector", (2^n,) words)] over the base
     field; ``polys``: (num_polys, 2^n).  ``policy`` (q_delta_1, q_delta_2, t1, t2),
@@ -138,7 +139,8 @@ def run_reference_zk(n, k, rho, sec, pow_bits, forms, polys, seed, sha2=False, n
                 f.write(data.tobytes())
             f.write(polys.tobytes())
         cmd = [REF_ZK_DRIVER, inp, out] + (["--verify"] if verify else [])
-        subprocess.run(cmd, check=True, timeout=timeout, stdout=subprocess.DEVNULL)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads)) if threads else None
+        subprocess.run(cmd, check=True, timeout=timeout, stdout=subprocess.DEVNULL, env=env)
         b = open(out, "rb").read()
     pos = 0
     (ln,) = struct.unpack_from("<Q", b, pos); pos += 8
@@ -149,7 +151,9 @@ def run_reference_zk(n, k, rho, sec, pow_bits, forms, polys, seed, sha2=False, n
     ev = np.frombuffer(b, dtype=np.uint64, count=cnt, offset=pos).copy(); pos += 8 * cnt
     (vok,) = struct.unpack_from("<d", b, pos); pos += 8
     nbv, q, nb = struct.unpack_from("<3Q", b, pos)
-    return RefZkProof(narg, hints, ev, vok, nbv, q, nb)
+    pos += 24
+    (ms,) = struct.unpack_from("<d", b, pos)
+    return RefZkProof(narg, hints, ev, vok, nbv, q, nb, ms)
 
 
 class OracleTranscript:

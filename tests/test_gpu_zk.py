@@ -91,14 +91,10 @@ def test_reference_zk_dump(gpu_ctx):
     from whirplonk_b200 import Covector, ProtocolParameters
     from whirplonk_b200.whir import ENGINE_ID_SHA2
     from whirplonk_b200.zk import BlindingSizePolicy, ZkConfig, whir_zk_domain_separator
-    from tests.zk_cases import disable_pow
-
     n = 8
     p = ProtocolParameters(False, 1, 2, 2, 16, 0, 1, ENGINE_ID_SHA2)
     pol = BlindingSizePolicy(4, 4, 4, 4, 3)
-    cfg = ZkConfig.from_params(1 << n, p, 1, pol)
-    disable_pow(cfg.raw.blinded)
-    disable_pow(cfg.raw.blinding)
+    cfg = ZkConfig.from_params(1 << n, p, 1, pol).disable_pow()
     poly = np.array(GOLD_ZK["input_vector0"], dtype=np.uint64)
     assert np.array_equal(poly, (np.arange(1 << n, dtype=np.uint64) * 17 + 3))
     ones = np.zeros((1 << n, 3), dtype=np.uint64)

@@ -1,11 +1,8 @@
 """Shared setup of the zero-knowledge fixtures ("zk" in reference_proofs.json,
 made by oracle/_ref/ref_zk_driver): parameters, policy and the base-field
 statement of each case, as tests/golden/make_fixtures.py built them."""
-import numpy as np
-
 from tests.golden.forms import form_inputs
 from whirplonk_b200 import Covector, MultilinearExtension, ProtocolParameters
-from whirplonk_b200 import _lib
 from whirplonk_b200.whir import ENGINE_ID_BLAKE3, ENGINE_ID_SHA2
 from whirplonk_b200.zk import BlindingSizePolicy, ZkConfig
 
@@ -20,23 +17,9 @@ def case_policy(case):
     return BlindingSizePolicy(*case["policy"], 3) if case["policy"] else None
 
 
-def disable_pow(cfg):
-    """Every PoW threshold of an inner Config off, as the reference's dumper does
-    (cpp/tests/dump_whir_zk.cpp)."""
-    cfg.initial_sumcheck.pow_threshold = _lib.NO_POW
-    cfg.initial_skip_pow = _lib.NO_POW
-    for r in range(cfg.num_rounds):
-        cfg.round_configs[r].pow_threshold = _lib.NO_POW
-        cfg.round_configs[r].sumcheck.pow_threshold = _lib.NO_POW
-    cfg.final_sumcheck.pow_threshold = _lib.NO_POW
-    cfg.final_pow = _lib.NO_POW
-
-
 def case_config(case):
-    cfg = ZkConfig.from_params(1 << case["n"], case_params(case), case["num_polynomials"], case_policy(case))
-    disable_pow(cfg.raw.blinded)
-    disable_pow(cfg.raw.blinding)
-    return cfg
+    return ZkConfig.from_params(1 << case["n"], case_params(case), case["num_polynomials"],
+                                case_policy(case)).disable_pow()
 
 
 def case_statement(case):

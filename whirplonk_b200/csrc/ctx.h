@@ -109,6 +109,8 @@ struct whirgpu_ctx {
     // witness destroyed afterwards only frees its handle.
     std::set<whirgpu_witness*> live_witnesses;
     std::set<whirgpu_zk_witness*> live_zk;  // the same for zero-knowledge witnesses
+    // Device allocations of destroyed zero-knowledge witnesses, by size, for reuse.
+    std::map<size_t, std::vector<char*>> zk_pool;
 };
 
 struct whirgpu_transcript {

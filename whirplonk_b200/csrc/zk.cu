@@ -16,8 +16,10 @@
 //           [beq covector, folded forms].
 // Both inner proofs run on the device schedule of prover.cu, in two workspaces
 // of one allocation that share ONE transcript state and ONE proof stream
-// (ProofPlan::tx_ext), so commit + prove is one stream of kernels without a
-// host round trip; the steps between the inner proofs are the kernels below.
+// (ProofPlan::tx_ext); the steps between the inner proofs are the kernels
+// below, except the absorption of the per-gamma messages (tens of thousands
+// of words), which the host CPU runs on a copy of the sponge between two
+// device phases: a sequential Keccak is faster on one CPU core than on one warp.
 // All arithmetic is in the base field (rho, beta, tau1, tau2 and every message
 // are Goldilocks elements).
 #include <cuda_runtime.h>
@@ -32,6 +34,7 @@
 #include "../../include/whirgpu.h"
 #include "blake3.cuh"
 #include "ctx.h"
+#include "host_keccak.h"
 #include "launch.h"
 #include "prover.h"
 #include "state.cuh"
@@ -345,41 +348,43 @@ __global__ void k_zk_beq_final(const u64* part, u32 parts, u32 ell, const ZkScal
     out[2 * jj + 1] = e3_base(gl_mul(gl_neg(rho), acc));
 }
 
-// Step 8 claims: claims[i * (mu + 2) + s] = sum_g tau2^g res[g][i][s].
+// Step 8 claims: claims[i * (mu + 2) + s] = sum_g tau2^g res[g][i][s], one
+// CTA per claim (exact field sums: any order).
 __global__ void k_zk_claims(const u64* res, const u64* tpow, u32 G, u32 ndots, u64* claims) {
-    const u32 d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= ndots) return;
+    __shared__ u64 red[32];
+    const u32 d = blockIdx.x;
     u64 acc = 0;
-    for (u32 g = 0; g < G; ++g) acc = gl_add(acc, gl_mul(tpow[g], res[(u64)g * ndots + d]));
-    claims[d] = acc;
+    for (u32 g = threadIdx.x; g < G; g += blockDim.x) acc = gl_add(acc, gl_mul(tpow[g], res[(u64)g * ndots + d]));
+    acc = warp_sum_gl(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        u64 r = 0;
+        for (u32 k = 0; k < (blockDim.x >> 5); ++k) r = gl_add(r, red[k]);
+        claims[d] = r;
+    }
 }
 
-// Steps 8-9 messages (whir_zk_impl.hpp:262-300): per gamma and polynomial
-// m_eval and the g_hat values; the combined claims
-// m + 2 tau1 sum_t tau1^t g_t (combine_claim_from_components) and the
-// batched h claims.  The blinding proof's claims for its beq form (form 0) are
-// [m, g_hat_0 .. g_hat_{mu-1}] per polynomial, one per blinding vector.
-__global__ void k_zk_tx_c(TxState* tx, const ZkScalars* zs, const u64* res, const u64* claims, u32 G, u32 npolys,
-                          u32 mu, ProofScalars* scg) {
+// Step 9 (combine_claim_from_components, build_combined_and_subproof_claims,
+// whir_zk_utils.hpp:455-520): tail = [m + 2 tau1 sum_t tau1^t g_t per
+// polynomial, then the batched h claims]; the blinding proof's claims for its
+// beq form (form 0) are [m, g_hat_0 .. g_hat_{mu-1}] per polynomial, one per
+// blinding vector.  One warp.
+__global__ void k_zk_combine(const ZkScalars* zs, const u64* claims, u32 npolys, u32 mu, ProofScalars* scg,
+                             u64* tail) {
     if (threadIdx.x >= 32) return;
-    const u32 l = threadIdx.x;
-    const u32 stride = mu + 2;
-    WarpTx t;
-    wtx_load(t, tx);
-    for (u32 g = 0; g < G; ++g)
-        for (u32 pi = 0; pi < npolys; ++pi) wtx_message_words(t, res + ((u64)g * npolys + pi) * stride, mu + 1);
+    const u32 l = threadIdx.x, stride = mu + 2;
     const u64 tau1 = zs->tau1;
-    for (u32 pi = 0; pi < npolys; ++pi) {
+    for (u32 pi = l; pi < npolys; pi += 32) {
         const u64* c = claims + pi * stride;
         u64 gs = 0, tp = 1;
         for (u32 s = 0; s < mu; ++s) {
             gs = gl_add(gs, gl_mul(tp, c[1 + s]));
             tp = gl_mul(tp, tau1);
         }
-        wtx_message_u64(t, gl_add(c[0], gl_mul(gl_add(tau1, tau1), gs)));
+        tail[pi] = gl_add(c[0], gl_mul(gl_add(tau1, tau1), gs));
+        tail[npolys + pi] = c[mu + 1];
     }
-    for (u32 pi = 0; pi < npolys; ++pi) wtx_message_u64(t, claims[pi * stride + mu + 1]);
-    wtx_store(t, tx);
     for (u32 i = l; i < npolys * (mu + 1); i += 32) {
         const u32 pi = i / (mu + 1), s = i % (mu + 1);
         scg->forms_eval[i] = e3_base(claims[pi * stride + s]);
@@ -432,6 +437,9 @@ void zk_detach_all(whirgpu_ctx* c) {
         w->ctx = nullptr;
     }
     c->live_zk.clear();
+    for (auto& kv : c->zk_pool)
+        for (char* p : kv.second) cudaFree(p);
+    c->zk_pool.clear();
 }
 }  // namespace wg
 
@@ -571,24 +579,49 @@ whirgpu_status whirgpu_zk_commit(whirgpu_ctx* c, const whirgpu_zk_config* cfg, c
     w->off_res = take((size_t)w->G * npolys * (mu + 2) * 8);
     w->off_gx = take((size_t)w->G * ell * 8 + 8);
     w->off_tpow = take((size_t)w->G * 8);
-    w->off_claims = take((size_t)ZK_MAX_DOTS * 8);
+    w->off_claims = take((size_t)(ZK_MAX_DOTS + 2 * MAX_WITNESSES) * 8);  // claims, then the combined / h tail
     w->off_part = take((size_t)w->parts * half * 8);
     const size_t total = cur;
     w->total = total;
-    {
+    bool fresh = false;
+    {  // a pooled allocation of this size, else a new one within the budget
         std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
-        if (c->budget && c->allocated + total > c->budget)
-            return zk_fail(c, WHIRGPU_E_OOM, "zero-knowledge witness above the HBM budget");
+        auto it = c->zk_pool.find(total);
+        if (it != c->zk_pool.end() && !it->second.empty()) {
+            w->dev = it->second.back();
+            it->second.pop_back();
+        } else {
+            if (c->budget && c->allocated + total > c->budget) {
+                for (auto& kv : c->zk_pool)
+                    for (char* p : kv.second) {
+                        cudaFree(p);
+                        c->allocated -= std::min<uint64_t>(c->allocated, kv.first);
+                    }
+                c->zk_pool.clear();
+            }
+            if (c->budget && c->allocated + total > c->budget)
+                return zk_fail(c, WHIRGPU_E_OOM, "zero-knowledge witness above the HBM budget");
+            fresh = true;
+        }
     }
-    ZK_CUDA(c, cudaMalloc(&w->dev, total), "cudaMalloc zero-knowledge witness");
+    if (fresh) {
+        ZK_CUDA(c, cudaMalloc(&w->dev, total), "cudaMalloc zero-knowledge witness");
+        std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+        c->allocated += total;
+    }
     char* dev = w->dev;
     auto fail_free = [&](whirgpu_status s, const std::string& m) {
-        cudaFree(w->dev);
+        std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+        c->zk_pool[total].push_back(w->dev);
         w->dev = nullptr;
         return zk_fail(c, s, m);
     };
-    // Counters and tickets of both workspaces start at zero.
-    cudaError_t e = cudaMemsetAsync(dev, 0, total, c->stream);
+    // Counters and tickets of both workspaces start at zero (they reset
+    // themselves after use, as in the workspace cache).
+    cudaError_t e = cudaMemsetAsync(dev + w->off_b + w->pb.off_sc_scratch, 0, w->pb.off_tx - w->pb.off_sc_scratch,
+                                    c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemsetAsync(dev + w->off_g + w->pg.off_sc_scratch, 0, w->pg.off_tx - w->pg.off_sc_scratch, c->stream);
     TxState* txs = reinterpret_cast<TxState*>(dev + w->off_tx);
     w->pb.tx_ext = txs;
     w->pg.tx_ext = txs;
@@ -627,7 +660,6 @@ whirgpu_status whirgpu_zk_commit(whirgpu_ctx* c, const whirgpu_zk_config* cfg, c
     }
     {
         std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
-        c->allocated += total;
         c->live_zk.insert(w.get());
     }
     tx->complete = false;
@@ -673,8 +705,7 @@ whirgpu_status whirgpu_zk_prove(whirgpu_ctx* c, whirgpu_zk_witness* w, const whi
     fa.logP = ell + 1;
     fa.out = W + P;  // form slot 0 holds the beq covector
     cudaError_t e = cudaSuccess;
-    c->io_h2d = 0;
-    size_t slot = 0;
+    size_t slot = 0;  // io_h2d continues the commit's count
     for (size_t f = 0; f < num_forms && e == cudaSuccess; ++f) {
         if (forms[f].kind == WHIRGPU_FORM_MLE) {
             char* dst = wsb + pb.off_points + f * n * 24;
@@ -759,11 +790,55 @@ whirgpu_status whirgpu_zk_prove(whirgpu_ctx* c, whirgpu_zk_witness* w, const whi
         k_zk_beq_final<<<bx, 256, 0, st>>>(part, w->parts, ell, zs, W);
         const u32 ndots = npolys * (mu + 2);
         u64* claims = reinterpret_cast<u64*>(dev + w->off_claims);
-        k_zk_claims<<<(ndots + 127) / 128, 128, 0, st>>>(ga.res, ga.tpow, w->G, ndots, claims);
-        k_zk_tx_c<<<1, 32, 0, st>>>(txs, zs, ga.res, claims, w->G, npolys, mu, scg);
+        u64* tail = claims + ZK_MAX_DOTS;
+        k_zk_claims<<<ndots, 256, 0, st>>>(ga.res, ga.tpow, w->G, ndots, claims);
+        k_zk_combine<<<1, 32, 0, st>>>(zs, claims, npolys, mu, scg, tail);
         launched += 5;
+        count_launches(launched);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            cudaStreamSynchronize(st);
+            return wg::cuda_fail(c, e, "zero-knowledge kernels");
+        }
+        // Steps 8-9 messages (whir_zk_impl.hpp:262-300): per gamma and
+        // polynomial m_eval and the g_hat values, then the tail -- G * npolys *
+        // (mu + 1) + 2 npolys words.  The sponge is sequential; the host CPU
+        // absorbs this run several times faster than one GPU warp.
+        const size_t rows = (size_t)w->G * npolys, stride = mu + 2;
+        const size_t add = 8 * (rows * (mu + 1) + 2 * npolys);
+        const size_t need = sizeof(TxState) + rows * stride * 8 + 2 * npolys * 8 + add + 64;
+        whirgpu_status ps = ensure_pinned(c, need);
+        if (ps != WHIRGPU_OK) {
+            cudaStreamSynchronize(st);
+            return ps;
+        }
+        uint8_t* h = c->pinned;
+        TxState* ht = reinterpret_cast<TxState*>(h);
+        u64* hres = reinterpret_cast<u64*>(h + sizeof(TxState));
+        u64* htail = hres + rows * stride;
+        uint8_t* hbytes = reinterpret_cast<uint8_t*>(htail + 2 * npolys);
+        ZK_CUDA(c, cudaMemcpyAsync(ht, txs, sizeof(TxState), cudaMemcpyDeviceToHost, st), "read-back");
+        ZK_CUDA(c, cudaMemcpyAsync(hres, ga.res, rows * stride * 8, cudaMemcpyDeviceToHost, st), "read-back");
+        ZK_CUDA(c, cudaMemcpyAsync(htail, tail, 2 * npolys * 8, cudaMemcpyDeviceToHost, st), "read-back");
+        ZK_CUDA(c, cudaStreamSynchronize(st), "zero-knowledge steps");
+        if (ht->err) {
+            char buf[96];
+            std::snprintf(buf, sizeof buf, "device error word 0x%x", ht->err);
+            return zk_fail(c, WHIRGPU_E_DEVICE, buf);
+        }
+        if (ht->narg_len + add > ht->narg_cap) return zk_fail(c, WHIRGPU_E_DEVICE, "proof stream overflow");
+        size_t pos = 0;
+        ht->has_reader = 0;  // an absorb drops the pending squeeze reader
+        for (size_t r = 0; r < rows; ++r)
+            host_absorb_message_words(ht->hasher, ht->hpos, hres + r * stride, mu + 1, hbytes, pos);
+        host_absorb_message_words(ht->hasher, ht->hpos, htail, 2 * npolys, hbytes, pos);
+        ZK_CUDA(c, cudaMemcpyAsync(dev + w->off_narg + ht->narg_len, hbytes, add, cudaMemcpyHostToDevice, st),
+                "transcript upload");
+        ht->narg_len += add;
+        ZK_CUDA(c, cudaMemcpyAsync(txs, ht, sizeof(TxState), cudaMemcpyHostToDevice, st), "transcript upload");
+        c->io_d2h += sizeof(TxState) + rows * stride * 8 + 2 * npolys * 8;
+        c->io_h2d += sizeof(TxState) + add;
     }
-    count_launches(launched);
     if (enqueue_prove(pb, wsb, c->tw, st, c->timer.get()) != 0 || enqueue_prove(pg, wsg, c->tw, st, c->timer.get()) != 0) {
         cudaStreamSynchronize(st);
         return zk_fail(c, WHIRGPU_E_INVALID, "prove launch failed");
@@ -793,7 +868,7 @@ whirgpu_status whirgpu_zk_prove(whirgpu_ctx* c, whirgpu_zk_witness* w, const whi
         ZK_CUDA(c, cudaMemcpyAsync(tx->hints.data(), dev + w->off_hints, htx.hints_len, cudaMemcpyDeviceToHost, st),
                 "read-back");
     ZK_CUDA(c, cudaStreamSynchronize(st), "read-back");
-    c->io_d2h = sizeof(TxState) + htx.narg_len + htx.hints_len;
+    c->io_d2h += sizeof(TxState) + htx.narg_len + htx.hints_len;
     tx->complete = true;
     return WHIRGPU_OK;
 }
@@ -804,10 +879,7 @@ void whirgpu_zk_witness_destroy(whirgpu_zk_witness* w) {
         whirgpu_ctx* c = w->ctx;
         cudaStreamSynchronize(c->stream);
         std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
-        if (w->dev) {
-            cudaFree(w->dev);
-            c->allocated -= std::min<uint64_t>(c->allocated, w->total);
-        }
+        if (w->dev) c->zk_pool[w->total].push_back(w->dev);  // kept for the next witness of this shape
         c->live_zk.erase(w);
     }
     delete w;

@@ -114,6 +114,20 @@ class ZkConfig:
                                                              pol, ctypes.byref(raw)))
         return cls(raw)
 
+    def disable_pow(self) -> "ZkConfig":
+        """Every PoW threshold of both inner configs off, as the reference's ZK
+        dumper does (cpp/tests/dump_whir_zk.cpp): over the 64-bit field the
+        derived PoW bits are far above what a prover can grind."""
+        for cfg in (self.raw.blinded, self.raw.blinding):
+            cfg.initial_sumcheck.pow_threshold = _lib.NO_POW
+            cfg.initial_skip_pow = _lib.NO_POW
+            for r in range(cfg.num_rounds):
+                cfg.round_configs[r].pow_threshold = _lib.NO_POW
+                cfg.round_configs[r].sumcheck.pow_threshold = _lib.NO_POW
+            cfg.final_sumcheck.pow_threshold = _lib.NO_POW
+            cfg.final_pow = _lib.NO_POW
+        return self
+
     @property
     def num_polynomials(self) -> int:
         return int(self.raw.num_polynomials)
