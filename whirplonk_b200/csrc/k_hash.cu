@@ -402,47 +402,63 @@ __global__ void k_ood_tables(const E3* pts, int n_ood, u32 hi_count, E3* tab) {
     }
 }
 
+// Sum over chunk h (2^LO coefficients) of vector v against point table j, one
+// value per lane (unreduced products, reduced once, scaled by z_j^(h 2^LO)).
+__device__ __forceinline__ E3 ood_chunk(const OodArgs& a, const E3* zlo, const E3* zhi, u32 v, u64 h, u32 lane) {
+    const u64* b0 = a.v[0] + (u64)v * a.vec_stride;
+    const u64 base = h << OOD_LO;
+    const u32 cnt = (u32)((a.size - base) < (1ull << OOD_LO) ? (a.size - base) : (1ull << OOD_LO));
+    E3Acc s = e3acc_zero();
+    if (a.ext3) {
+        for (u32 l = lane; l < cnt; l += 32) e3acc_mac(s, zlo[l], E3{b0[base + l], a.v[1][base + l], a.v[2][base + l]});
+    } else if (cnt == (1u << OOD_LO)) {
+        // a full block: eight coalesced loads in flight per lane before the products
+        for (u32 l0 = lane; l0 < cnt; l0 += 256) {
+            u64 x[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) x[k] = b0[base + l0 + 32 * k];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) e3acc_mac_base(s, zlo[l0 + 32 * k], x[k]);
+        }
+    } else {
+        for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], b0[base + l]);
+    }
+    return e3_mul(e3acc_reduce(s), zhi[h]);
+}
+
+// ITEMS: one warp per (value, chunk) item, partials[k * hi_count + h] (few
+// chunks per value: small vectors, many vectors); otherwise each warp strides
+// over the chunks of every value and a CTA sum goes to partials[cta * nvals + k].
+template <bool ITEMS>
 __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u32 hi_count, E3* partials,
                                                      unsigned* counter) {
     __shared__ E3 red[32];
     __shared__ bool is_last;
     __shared__ E3 totals[OOD_MAX_VALUES];
-    const u32 lane = threadIdx.x & 31;
-    const u64 gw = (u64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const u64 nw = (u64)gridDim.x * (blockDim.x >> 5);
+    const u32 lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const u64 gw = (u64)blockIdx.x * nwarps + warp;
+    const u64 nw = (u64)gridDim.x * nwarps;
     const u32 per = (1u << OOD_LO) + hi_count;
-    const u64 size = a.size;
     const u32 nvals = (u32)a.n_ood * a.nvec;
-    for (int j = 0; j < a.n_ood; ++j) {
-        const E3* zlo = tab + (u64)j * per;
-        const E3* zhi = zlo + (1u << OOD_LO);
-        for (u32 v = 0; v < a.nvec; ++v) {
+    if (ITEMS) {
+        const u64 items = (u64)nvals * hi_count;
+        for (u64 it = gw; it < items; it += nw) {
+            const u32 k = (u32)(it / hi_count), v = k % a.nvec, j = k / a.nvec;
             if (v >= a.skip_lo && v < a.skip_hi) continue;
-            const u64* b0 = a.v[0] + (u64)v * a.vec_stride;
-            E3 acc = e3_zero();
-            for (u64 h = gw; h < hi_count; h += nw) {
-                const u64 base = h << OOD_LO;
-                const u32 cnt = (u32)((size - base) < (1ull << OOD_LO) ? (size - base) : (1ull << OOD_LO));
-                E3Acc s = e3acc_zero();
-                if (a.ext3) {
-                    for (u32 l = lane; l < cnt; l += 32)
-                        e3acc_mac(s, zlo[l], E3{b0[base + l], a.v[1][base + l], a.v[2][base + l]});
-                } else if (cnt == (1u << OOD_LO)) {
-                    // a full block: eight coalesced loads in flight per lane before the products
-                    for (u32 l0 = lane; l0 < cnt; l0 += 256) {
-                        u64 x[8];
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) x[k] = b0[base + l0 + 32 * k];
-#pragma unroll
-                        for (int k = 0; k < 8; ++k) e3acc_mac_base(s, zlo[l0 + 32 * k], x[k]);
-                    }
-                } else {
-                    for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], b0[base + l]);
-                }
-                acc = e3_add(acc, e3_mul(e3acc_reduce(s), zhi[h]));
+            const E3* zlo = tab + (u64)j * per;
+            const E3 val = e3_warp_sum(ood_chunk(a, zlo, zlo + (1u << OOD_LO), v, it % hi_count, lane));
+            if (lane == 0) partials[it] = val;
+        }
+    } else {
+        for (int j = 0; j < a.n_ood; ++j) {
+            const E3* zlo = tab + (u64)j * per;
+            for (u32 v = 0; v < a.nvec; ++v) {
+                if (v >= a.skip_lo && v < a.skip_hi) continue;
+                E3 acc = e3_zero();
+                for (u64 h = gw; h < hi_count; h += nw) acc = e3_add(acc, ood_chunk(a, zlo, zlo + (1u << OOD_LO), v, h, lane));
+                E3 bs = block_sum_e3(acc, red);
+                if (threadIdx.x == 0) partials[(u64)blockIdx.x * nvals + (u32)j * a.nvec + v] = bs;
             }
-            E3 bs = block_sum_e3(acc, red);
-            if (threadIdx.x == 0) partials[(u64)blockIdx.x * nvals + (u32)j * a.nvec + v] = bs;
         }
     }
     if (threadIdx.x == 0) {
@@ -452,16 +468,18 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u
     }
     __syncthreads();
     if (!is_last) return;
-    for (u32 k = 0; k < nvals; ++k) {
+    // one warp per value: the sum of its partials
+    const u32 nparts = ITEMS ? hi_count : gridDim.x;
+    for (u32 k = warp; k < nvals; k += nwarps) {
         const u32 v = k % a.nvec;
         if (v >= a.skip_lo && v < a.skip_hi) continue;
         E3 acc = e3_zero();
-        for (u32 b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-            const E3* pp = &partials[(u64)b * nvals + k];
+        for (u32 b = lane; b < nparts; b += 32) {
+            const E3* pp = ITEMS ? &partials[(u64)k * hi_count + b] : &partials[(u64)b * nvals + k];
             acc = e3_add(acc, E3{__ldcg(&pp->c0), __ldcg(&pp->c1), __ldcg(&pp->c2)});
         }
-        E3 total = block_sum_e3(acc, red);
-        if (threadIdx.x == 0) {
+        const E3 total = e3_warp_sum(acc);
+        if (lane == 0) {
             a.out[(k / a.nvec) * a.out_stride + v] = total;
             totals[k] = total;
         }
@@ -498,9 +516,14 @@ int launch_ood(const OodArgs& a, cudaStream_t st) {
     k_ood_tables<<<(unsigned)std::min<u64>(296, (entries + 255) / 256), 256, 0, st>>>(a.pts, a.n_ood, hc, tab);
     count_launches(1);
     const u64 warps_per_cta = OOD_THREADS / 32;
-    u64 want = (hc + warps_per_cta - 1) / warps_per_cta;
+    const u64 items = (u64)a.n_ood * a.nvec * hc;
+    // Few chunks per value: spread (value, chunk) items over the warps (the
+    // partials fit: items <= OOD_GRID * scratch_values when hc <= OOD_GRID).
+    const bool by_items = hc <= OOD_GRID && items > hc;
+    u64 want = ((by_items ? items : hc) + warps_per_cta - 1) / warps_per_cta;
     unsigned grid = (unsigned)(want < 1 ? 1 : (want > OOD_GRID ? OOD_GRID : want));
-    k_ood<<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
+    if (by_items) k_ood<true><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
+    else k_ood<false><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
     count_launches(1);
     return 0;
 }
