@@ -271,7 +271,7 @@ whirgpu_status whirgpu_ctx_create(int device, uint64_t hbm_budget, whirgpu_ctx**
     c->budget = hbm_budget;
     WG_CUDA(nullptr, cudaSetDevice(device), "cudaSetDevice");
     WG_CUDA(nullptr, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    if (lde_prepare() != 0) return WHIRGPU_E_CUDA;
+    if (lde_prepare() != 0 || sumcheck_prepare() != 0) return WHIRGPU_E_CUDA;
     whirgpu_ntt_load_default_plans();
     std::vector<uint64_t> st(1u << (TW_STAGE_LOG - 1)), hi(1u << TW_HALF), lo(1u << TW_HALF);
     host_twiddles(st.data(), hi.data(), lo.data());

@@ -175,12 +175,35 @@ __global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_s
             const E3 bl = ld3(a.b, i), bh = ld3(a.b, i + half);
             accl_mac_base(c0, al, bl);
             accl_mac_base(c2, gl_sub(ah, al), e3_sub(bh, bl));
-        } else {
-            const E3 al = load_a(a, i, r), bl = load_b(a, i, r);
-            if (FOLD) { st3(a.a_out, i, al); st3(a.b, i, bl); }
+        } else if (FOLD) {
+            // Every load of the pair before any store: the stores (i, i + half)
+            // alias no load of another pair, and the compiler cannot see that.
+            const u64 s = a.size;
+            E3 x0, x1, x2, x3;
+            if (BASE) {
+                const u64 p0 = a.a_base[i], p1 = a.a_base[i + s], p2 = a.a_base[i + half], p3 = a.a_base[i + half + s];
+                x0 = e3_base(p0); x1 = e3_base(p1); x2 = e3_base(p2); x3 = e3_base(p3);
+            } else {
+                x0 = ld3(a.a_in, i); x1 = ld3(a.a_in, i + s); x2 = ld3(a.a_in, i + half); x3 = ld3(a.a_in, i + half + s);
+            }
+            const E3 y0 = ld3(a.b, i), y1 = ld3(a.b, i + s), y2 = ld3(a.b, i + half), y3 = ld3(a.b, i + half + s);
+            E3 al, ah;
+            if (BASE) {
+                al = e3_add(x0, e3_mul_base(r, gl_sub(x1.c0, x0.c0)));
+                ah = e3_add(x2, e3_mul_base(r, gl_sub(x3.c0, x2.c0)));
+            } else {
+                al = e3_add(x0, e3_mul(r, e3_sub(x1, x0)));
+                ah = e3_add(x2, e3_mul(r, e3_sub(x3, x2)));
+            }
+            const E3 bl = e3_add(y0, e3_mul(r, e3_sub(y1, y0)));
+            const E3 bh = e3_add(y2, e3_mul(r, e3_sub(y3, y2)));
+            st3(a.a_out, i, al); st3(a.b, i, bl);
+            st3(a.a_out, i + half, ah); st3(a.b, i + half, bh);
             accl_mac(c0, al, bl);
-            const E3 ah = load_a(a, i + half, r), bh = load_b(a, i + half, r);
-            if (FOLD) { st3(a.a_out, i + half, ah); st3(a.b, i + half, bh); }
+            accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
+        } else {
+            const E3 al = ld3(a.a_in, i), bl = ld3(a.b, i), ah = ld3(a.a_in, i + half), bh = ld3(a.b, i + half);
+            accl_mac(c0, al, bl);
             accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
         }
     }
@@ -331,13 +354,33 @@ size_t sumcheck_scratch_bytes() { return (size_t)SC_GRID * 2 * sizeof(E3) + 256;
 
 int launch_pow_grind_only(ProofScalars* sc, u64 threshold, int hash, cudaStream_t st);  // k_tx.cu
 
+// Resident CTAs of k_sumcheck_round<fold, base> (index 2 fold + base); a grid
+// of at most this many runs in one wave (the grid-stride loop does the rest).
+static unsigned g_sc_resident[4] = {SC_GRID, SC_GRID, SC_GRID, SC_GRID};
+
+int sumcheck_prepare() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return -1;
+    const void* fns[4] = {(const void*)k_sumcheck_round<false, false>, (const void*)k_sumcheck_round<false, true>,
+                          (const void*)k_sumcheck_round<true, false>, (const void*)k_sumcheck_round<true, true>};
+    for (int k = 0; k < 4; ++k) {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[k], SC_THREADS, 0) != cudaSuccess) return -1;
+        const long r = (long)sms * (occ < 1 ? 1 : occ);
+        g_sc_resident[k] = (unsigned)(r > SC_GRID ? SC_GRID : r);
+    }
+    return 0;
+}
+
 int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
     if (s.size < 2) return -1;
     ScKernelArgs a = make_sc(s);
     const u64 half = s.size >> 1;
-    u64 want = (half + SC_THREADS - 1) / SC_THREADS;
-    const unsigned grid = (unsigned)(want > SC_GRID ? SC_GRID : (want < 1 ? 1 : want));
     const bool base = a.a_base != nullptr;
+    const u64 cap = g_sc_resident[(a.fold ? 2 : 0) + (base ? 1 : 0)];
+    u64 want = (half + SC_THREADS - 1) / SC_THREADS;
+    const unsigned grid = (unsigned)(want > cap ? cap : (want < 1 ? 1 : want));
     if (a.fold) {
         if (base) k_sumcheck_round<true, true><<<grid, SC_THREADS, 0, st>>>(a);
         else k_sumcheck_round<true, false><<<grid, SC_THREADS, 0, st>>>(a);

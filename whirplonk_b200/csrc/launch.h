@@ -63,6 +63,9 @@ size_t lde_installed_plans(u32* keys, LdePlan* plans, size_t cap);  // keys: log
 int launch_lde_plan(const LdeArgs& a, const LdePlan& pl, cudaStream_t st);
 int launch_lde(const LdeArgs& a, cudaStream_t st);
 int lde_prepare();
+// Resident-CTA counts of the sumcheck round kernels on the current device
+// (their grids never leave a partial wave); called once per context.
+int sumcheck_prepare();
 
 // ---- Merkle commitment ------------------------------------------------------
 // Leaf i = BLAKE3 of row i (LE bytes of `depth` elements of `ncomp` words),
