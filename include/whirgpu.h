@@ -118,11 +118,15 @@ void whirgpu_witness_destroy(whirgpu_witness* w);
 /* ---- a Config given field by field -----------------------------------------------
  * Config<M> (whir.hpp:104-116) as the reference's callers can also build it
  * by hand (cpp/tests/dump_whir.cpp:121-148), and the embedding M: the CLI's
- * --field Goldilocks3 (Basefield<GoldilocksExt3>, the default) or Goldilocks1
+ * --field Goldilocks3 (Basefield<GoldilocksExt3>, the default), Goldilocks2
+ * (Basefield<GoldilocksExt2>, Fp[X]/(X^2 - 7)) or Goldilocks1
  * (Identity<Goldilocks>: challenges, sums and messages in the base field).
+ * Target-field values cross this ABI as three words c0 c1 c2 (c2 = 0 for
+ * Ext2, c1 = c2 = 0 for the base field).
  * Each committer's interleaving depth is 2^(rounds of the sumcheck after it) and
  * sizes chain from round to round (checked; WHIRGPU_E_INVALID otherwise). */
 #define WHIRGPU_FIELD_GOLDILOCKS1 1
+#define WHIRGPU_FIELD_GOLDILOCKS2 2
 #define WHIRGPU_FIELD_GOLDILOCKS3 3
 #define WHIRGPU_MAX_ROUNDS 24
 typedef struct {
@@ -138,7 +142,7 @@ typedef struct {
     whirgpu_sumcheck_config sumcheck;
 } whirgpu_round_config;
 typedef struct {
-    uint32_t field;         /* WHIRGPU_FIELD_GOLDILOCKS3 / _GOLDILOCKS1 */
+    uint32_t field;         /* WHIRGPU_FIELD_GOLDILOCKS3 / _GOLDILOCKS2 / _GOLDILOCKS1 */
     uint64_t batch_size;    /* vectors per commitment (initial_committer.num_vectors) */
     uint8_t hash_id[32];    /* engine of every Merkle layer and PoW */
     whirgpu_irs_config initial_committer;

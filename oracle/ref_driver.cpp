@@ -9,7 +9,8 @@
 //
 // Call chain mirrored from the reference CLI `run_pcs` (cpp/main.cpp:292-467):
 //   Config<M>::from_params (whir.hpp:118), M = Basefield<GoldilocksExt3>, or
-//   Identity<Goldilocks> with --field1 (the CLI's --field Goldilocks1)
+//   Identity<Goldilocks> with --field1 (the CLI's --field Goldilocks1), or
+//   Basefield<GoldilocksExt2> with --field2 (--field Goldilocks2)
 //   ProverState::from_ds(ds, Empty)               (transcript.hpp:605)
 //   config.commit / config.prove                   (whir.hpp:303, whir_prover.hpp:56)
 // with the domain separator of `make_rust_cli_domain_separator`
@@ -33,6 +34,7 @@
 //   f64 commit_ms, f64 prove_ms, f64 verify_ok
 #include "whir/algebra/embedding.hpp"
 #include "whir/algebra/goldilocks.hpp"
+#include "whir/algebra/goldilocks_ext2.hpp"
 #include "whir/algebra/goldilocks_ext3.hpp"
 #include "whir/algebra/linear_form.hpp"
 #include "whir/hash/blake3_engine.hpp"
@@ -58,6 +60,7 @@ using Clock = std::chrono::steady_clock;
 using Source = ::whir::algebra::Goldilocks;
 using M3 = ::whir::algebra::Basefield<::whir::algebra::GoldilocksExt3>;  // --field Goldilocks3 (default)
 using M1 = ::whir::algebra::Identity<::whir::algebra::Goldilocks>;       // --field Goldilocks1
+using M2 = ::whir::algebra::Basefield<::whir::algebra::GoldilocksExt2>;  // --field Goldilocks2
 
 [[noreturn]] void die(const char* msg) {
     std::fprintf(stderr, "ref_driver: %s\n", msg);
@@ -139,6 +142,9 @@ T make_target(std::uint64_t a, std::uint64_t b, std::uint64_t c) {
     if constexpr (std::is_same_v<T, ::whir::algebra::Goldilocks>) {
         if (b || c) die("base-field target given an extension element");
         return T::from_u64(a);
+    } else if constexpr (std::is_same_v<T, ::whir::algebra::GoldilocksExt2>) {
+        if (c) die("quadratic-extension target given a cubic element");
+        return T(Source::from_u64(a), Source::from_u64(b));
     } else {
         return T(Source::from_u64(a), Source::from_u64(b), Source::from_u64(c));
     }
@@ -148,6 +154,10 @@ void put_target(FILE* f, const T& e) {
     if constexpr (std::is_same_v<T, ::whir::algebra::Goldilocks>) {
         put_u64(f, e.as_canonical_u64());
         put_u64(f, 0);
+        put_u64(f, 0);
+    } else if constexpr (std::is_same_v<T, ::whir::algebra::GoldilocksExt2>) {
+        put_u64(f, e.c0().as_canonical_u64());
+        put_u64(f, e.c1().as_canonical_u64());
         put_u64(f, 0);
     } else {
         put_u64(f, e.c0().as_canonical_u64());
@@ -289,18 +299,19 @@ int run(const Job& j) {
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: ref_driver INPUT OUTPUT [--verify] [--reps R] [--config] [--sha2] [--unique] [--field1]\n");
+        std::fprintf(stderr, "usage: ref_driver INPUT OUTPUT [--verify] [--reps R] [--config] [--sha2] [--unique] [--field1 | --field2]\n");
         return 2;
     }
     Job j;
     j.out_path = argv[2];
-    bool field1 = false;
+    bool field1 = false, field2 = false;
     for (int i = 3; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--verify")) j.do_verify = true;
         else if (!std::strcmp(argv[i], "--config")) j.print_cfg = true;
         else if (!std::strcmp(argv[i], "--sha2")) j.use_sha2 = true;
         else if (!std::strcmp(argv[i], "--unique")) j.unique = true;
         else if (!std::strcmp(argv[i], "--field1")) field1 = true;
+        else if (!std::strcmp(argv[i], "--field2")) field2 = true;
         else if (!std::strcmp(argv[i], "--reps") && i + 1 < argc) j.reps = std::atoi(argv[++i]);
         else die("bad flag");
     }
@@ -337,6 +348,6 @@ int main(int argc, char** argv) {
     j.vecs.assign(nvec, std::vector<Source>(size));
     for (auto& vec : j.vecs)
         for (auto& v : vec) v = Source::from_u64(rd.u64());
-    return field1 ? run<M1>(j) : run<M3>(j);
+    return field1 ? run<M1>(j) : field2 ? run<M2>(j) : run<M3>(j);
 }
 

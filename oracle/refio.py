@@ -80,7 +80,7 @@ def ref_available() -> bool:
 
 def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1, threads=None,
                   timeout=3600, sha2=False, batch_size=1, num_witnesses=1, forms=None, unique=False,
-                  field1=False) -> RefProof:
+                  field1=False, field2=False) -> RefProof:
     """Runs the unmodified reference prover (compiled in place by oracle/Makefile).
     With several vectors the evaluations come back form-major, (num_forms * V, 3).
     ``forms`` (see write_input) replaces ``points`` for mixed MLE / Covector statements."""
@@ -100,6 +100,8 @@ def run_reference(n, k, rho, sec, pow_bits, points, coeffs, verify=False, reps=1
             cmd.append("--unique")
         if field1:
             cmd.append("--field1")
+        if field2:
+            cmd.append("--field2")
         subprocess.run(cmd, check=True, env=env, timeout=timeout, stdout=subprocess.DEVNULL)
         return read_output(out, npts, batch_size * num_witnesses)
 

@@ -22,6 +22,7 @@ has the reference checkout; the tests only read the JSON files).
    statements that mix MultilinearExtension and dense Covector linear forms;
    "unique" proofs under unique decoding, including statement-free ones;
    "field1" proofs over Identity<Goldilocks> (the CLI's --field Goldilocks1);
+   "field2" proofs over Basefield<GoldilocksExt2> (--field Goldilocks2);
    "zk" zero-knowledge WHIR proofs (oracle/_ref/ref_zk_driver, masks from the
    reference's DeterministicRng with the case's seed).
 """
@@ -455,6 +456,41 @@ def proofs_field1():
     return out
 
 
+FIELD2_CASES = [  # Basefield<GoldilocksExt2> (the CLI's --field Goldilocks2):
+    # (n, k, rho, security, pow_bits, seed, form kinds, batch_size, num_witnesses, hash, unique_decoding)
+    (5, 4, 1, 40, 10, 91, ("mle",), 1, 1, "blake3", False),
+    (10, 4, 1, 40, 10, 92, ("mle",), 1, 1, "blake3", False),
+    (12, 4, 2, 40, 10, 93, ("mle", "covector"), 2, 1, "blake3", False),
+    (14, 3, 1, 32, 8, 94, ("mle",), 1, 1, "sha2", False),
+    (11, 4, 1, 40, 10, 95, (), 1, 1, "blake3", True),
+    (12, 4, 1, 36, 10, 96, ("covector",), 2, 2, "blake3", False),
+    (18, 4, 1, 60, 16, 97, ("mle",), 1, 1, "blake3", False),
+]
+
+
+def proofs_field2():
+    from oracle.refio import run_reference
+    from tests.golden.forms import form_inputs
+
+    out = []
+    for (n, k, rho, sec, pb, seed, kinds, batch, nwit, eng, unique) in FIELD2_CASES:
+        coeffs, forms = form_inputs(n, seed, kinds, batch * nwit, ext2=True)
+        ref = run_reference(n, k, rho, sec, pb, None, coeffs, verify=True, sha2=eng == "sha2", batch_size=batch,
+                            num_witnesses=nwit, forms=forms, unique=unique, field2=True)
+        assert ref.verify_ok == 1.0
+        rec = {"n": n, "k": k, "rho": rho, "security": sec, "pow_bits": pb, "seed": seed, "kinds": list(kinds),
+               "batch_size": batch, "num_witnesses": nwit, "hash": eng, "unique_decoding": unique,
+               "evaluations": [[int(x) for x in row] for row in ref.evaluations],
+               "narg_len": len(ref.narg), "hints_len": len(ref.hints),
+               "narg_sha256": hashlib.sha256(ref.narg).hexdigest(),
+               "hints_sha256": hashlib.sha256(ref.hints).hexdigest()}
+        if n <= 5:
+            rec["narg"] = ref.narg.hex()
+            rec["hints"] = ref.hints.hex()
+        out.append(rec)
+    return out
+
+
 ZK_CASES = [  # zero-knowledge WHIR (ZkConfig<Goldilocks>), every PoW disabled as the reference's dumper does:
     # (n, k, rho, security, seed, form kinds, num_polynomials, hash, policy (q_delta_1, q_delta_2, t1, t2) or None)
     (8, 2, 1, 16, 101, ("covector",), 1, "sha2", (4, 4, 4, 4)),   # the shape of cpp/tests/dump_whir_zk.cpp
@@ -498,7 +534,7 @@ def main():
         json.dump({"generator": "oracle/_ref/ref_driver (reference C++ prover, CLI domain separator, "
                                 "seeded ChaCha20 inputs via whirgpu_sample_goldilocks)", "cases": proofs(),
                    "multi": proofs_multi(), "forms": proofs_forms(), "unique": proofs_unique(),
-                   "field1": proofs_field1(), "zk": proofs_zk()}, f, indent=1)
+                   "field1": proofs_field1(), "field2": proofs_field2(), "zk": proofs_zk()}, f, indent=1)
 
 
 if __name__ == "__main__":

@@ -8,6 +8,7 @@ from .whir import (  # noqa: F401
     ENGINE_ID_BLAKE3,
     ENGINE_ID_SHA2,
     FIELD_GOLDILOCKS1,
+    FIELD_GOLDILOCKS2,
     FIELD_GOLDILOCKS3,
     P,
     Config,

@@ -70,7 +70,7 @@ class Request(ctypes.Structure):
 
 
 FORM_MLE, FORM_COVECTOR = 0, 1
-FIELD_GOLDILOCKS1, FIELD_GOLDILOCKS3 = 1, 3
+FIELD_GOLDILOCKS1, FIELD_GOLDILOCKS2, FIELD_GOLDILOCKS3 = 1, 2, 3
 MAX_ROUNDS = 24
 NO_POW = (1 << 64) - 1
 ZK_CONFIG_BYTES = 154

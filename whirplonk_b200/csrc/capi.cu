@@ -464,7 +464,8 @@ IrsSchedule from_irs(const whirgpu_irs_config& b) {
 }  // namespace
 
 whirgpu_status whirgpu_config_from_params(const whirgpu_params* params, uint64_t n, uint32_t field, whirgpu_config* out) {
-    if (!params || !out || (field != WHIRGPU_FIELD_GOLDILOCKS1 && field != WHIRGPU_FIELD_GOLDILOCKS3))
+    if (!params || !out || (field != WHIRGPU_FIELD_GOLDILOCKS1 && field != WHIRGPU_FIELD_GOLDILOCKS2 &&
+                            field != WHIRGPU_FIELD_GOLDILOCKS3))
         return WHIRGPU_E_INVALID;
     ProtocolParams pp = to_params(params);
     pp.field_degree = (int)field;
@@ -497,7 +498,8 @@ whirgpu_status whirgpu_commit_config(whirgpu_ctx* c, const whirgpu_config* cfg, 
                                      uint64_t num_witnesses, int where, whirgpu_transcript* tx, whirgpu_witness** out) {
     if (!c || !cfg || !coeffs || !tx || !out || tx->ctx != c) return fail(c, WHIRGPU_E_INVALID, "null argument");
     *out = nullptr;
-    if (cfg->field != WHIRGPU_FIELD_GOLDILOCKS1 && cfg->field != WHIRGPU_FIELD_GOLDILOCKS3)
+    if (cfg->field != WHIRGPU_FIELD_GOLDILOCKS1 && cfg->field != WHIRGPU_FIELD_GOLDILOCKS2 &&
+        cfg->field != WHIRGPU_FIELD_GOLDILOCKS3)
         return fail(c, WHIRGPU_E_INVALID, "unknown field");
     if (cfg->num_rounds > WHIRGPU_MAX_ROUNDS) return fail(c, WHIRGPU_E_INVALID, "too many rounds");
     whirgpu_params hp{};

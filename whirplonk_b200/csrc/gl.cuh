@@ -278,6 +278,30 @@ __device__ __forceinline__ E3 e3_pow(E3 b, u64 e) {
     return r;
 }
 
+// Basefield<GoldilocksExt2> (goldilocks_ext2.hpp: Fp[X]/(X^2 - 7)) rides on
+// the same representation: an Ext2 value is (c0, c1, 0).  For two such values
+// the X^3 = 2 rule of e3_mul / E3Acc leaves the plain polynomial product
+// (a0 b0, a0 b1 + a1 b0, a1 b1) -- no term of degree 3 or 4 arises -- and
+// X^2 = 7 folds the X^2 coefficient back: e2_fold.  It is the identity on
+// values whose c2 is zero, so an Ext2 proof applies it after every product.
+constexpr u64 GL_EXT2_NR = 7;
+__device__ __forceinline__ E3 e2_fold(E3 v) { return E3{gl_add(v.c0, gl_mul(v.c2, GL_EXT2_NR)), v.c1, 0}; }
+// Product in the target field: Ext3, or Ext2 when ext2 is set.
+__device__ __forceinline__ E3 ef_mul(E3 a, E3 b, bool ext2) {
+    const E3 r = e3_mul(a, b);
+    return ext2 ? e2_fold(r) : r;
+}
+__device__ __forceinline__ E3 ef_fix(E3 v, bool ext2) { return ext2 ? e2_fold(v) : v; }
+__device__ __forceinline__ E3 ef_pow(E3 b, u64 e, bool ext2) {
+    E3 r = e3_one();
+    while (e) {
+        if (e & 1) r = ef_mul(r, b, ext2);
+        b = ef_mul(b, b, ext2);
+        e >>= 1;
+    }
+    return r;
+}
+
 // Ext3 vectors live in HBM as three component planes (structure of arrays):
 // every component access is a coalesced 8-byte stream.
 struct E3Planes {

@@ -203,11 +203,12 @@ __device__ __forceinline__ void parent_cv(const unsigned l[8], const unsigned r[
 int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
                        u64 node_stride, int hash, cudaStream_t st) {
     if (count == 0 || count > 65535) return -1;
-    if (ncomp != 1 && ncomp != 3) return -1;
+    if (ncomp < 1 || ncomp > 3) return -1;  // base field, Ext2 (c0 c1 per element), Ext3
     if (hash != HASH_SHA256 && depth * ncomp * 8 > 1024) {  // BLAKE3 tree mode, one matrix at a time
         if (count != 1 || depth * ncomp > 128 * B3_MAX_CHUNKS) return -1;
         const unsigned grid = (unsigned)((N + 127) / 128);
         if (ncomp == 1) k_leaves_wide<1><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
+        else if (ncomp == 2) k_leaves_wide<2><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
         else k_leaves_wide<3><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
         count_launches(1);
         return 0;
@@ -215,9 +216,11 @@ int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nod
     const dim3 grid((unsigned)((N + 255) / 256), count);
     if (hash == HASH_SHA256) {
         if (ncomp == 1) k_leaves<1, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+        else if (ncomp == 2) k_leaves<2, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
         else k_leaves<3, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
     } else {
         if (ncomp == 1) k_leaves<1, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+        else if (ncomp == 2) k_leaves<2, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
         else k_leaves<3, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
     }
     count_launches(1);
@@ -392,13 +395,13 @@ __device__ __forceinline__ E3 block_sum_e3(E3 v, E3* red) {
 static u32 ood_hi_count(u64 size) { return (u32)((size + (1ull << OOD_LO) - 1) >> OOD_LO); }
 
 // tab[j]: z_j^l for l < 2^LO, then z_j^(h 2^LO) for h < hi_count.
-__global__ void k_ood_tables(const E3* pts, int n_ood, u32 hi_count, E3* tab) {
+__global__ void k_ood_tables(const E3* pts, int n_ood, u32 hi_count, E3* tab, bool ext2) {
     const u32 per = (1u << OOD_LO) + hi_count;
     const u64 total = (u64)per * n_ood;
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 j = (u32)(e / per), k = (u32)(e % per);
         const E3 z = pts[j];
-        tab[e] = k < (1u << OOD_LO) ? e3_pow(z, k) : e3_pow(z, (u64)(k - (1u << OOD_LO)) << OOD_LO);
+        tab[e] = k < (1u << OOD_LO) ? ef_pow(z, k, ext2) : ef_pow(z, (u64)(k - (1u << OOD_LO)) << OOD_LO, ext2);
     }
 }
 
@@ -423,7 +426,7 @@ __device__ __forceinline__ E3 ood_chunk(const OodArgs& a, const E3* zlo, const E
     } else {
         for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], b0[base + l]);
     }
-    return e3_mul(e3acc_reduce(s), zhi[h]);
+    return ef_mul(ef_fix(e3acc_reduce(s), a.ext2), zhi[h], a.ext2);
 }
 
 // ITEMS: one warp per (value, chunk) item, partials[k * hi_count + h] (few
@@ -449,6 +452,9 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u
             const E3 val = e3_warp_sum(ood_chunk(a, zlo, zlo + (1u << OOD_LO), v, it % hi_count, lane));
             if (lane == 0) partials[it] = val;
         }
+        // every warp's partials visible device-wide before this CTA takes its ticket
+        __threadfence();
+        __syncthreads();
     } else {
         for (int j = 0; j < a.n_ood; ++j) {
             const E3* zlo = tab + (u64)j * per;
@@ -513,7 +519,7 @@ int launch_ood(const OodArgs& a, cudaStream_t st) {
     E3* partials = reinterpret_cast<E3*>(base + 256);
     E3* tab = partials + (size_t)OOD_GRID * a.scratch_values;
     const u64 entries = (u64)((1u << OOD_LO) + hc) * a.n_ood;
-    k_ood_tables<<<(unsigned)std::min<u64>(296, (entries + 255) / 256), 256, 0, st>>>(a.pts, a.n_ood, hc, tab);
+    k_ood_tables<<<(unsigned)std::min<u64>(296, (entries + 255) / 256), 256, 0, st>>>(a.pts, a.n_ood, hc, tab, a.ext2 != 0);
     count_launches(1);
     const u64 warps_per_cta = OOD_THREADS / 32;
     const u64 items = (u64)a.n_ood * a.nvec * hc;

@@ -54,6 +54,7 @@ struct ScKernelArgs {
     ProofScalars* sc;
     E3* partials;
     unsigned* counter;
+    int ext2;
 };
 
 // Loads a_i of the round vector, folding on the fly when requested.
@@ -64,12 +65,12 @@ __device__ __forceinline__ E3 load_a(const ScKernelArgs& a, u64 i, const E3& r) 
         return e3_add(e3_base(x0), e3_mul_base(r, gl_sub(x1, x0)));
     }
     const E3 x0 = ld3(a.a_in, i), x1 = ld3(a.a_in, i + a.size);
-    return e3_add(x0, e3_mul(r, e3_sub(x1, x0)));
+    return e3_add(x0, ef_mul(r, e3_sub(x1, x0), a.ext2));
 }
 __device__ __forceinline__ E3 load_b(const ScKernelArgs& a, u64 i, const E3& r) {
     if (!a.fold) return ld3(a.b, i);
     const E3 y0 = ld3(a.b, i), y1 = ld3(a.b, i + a.size);
-    return e3_add(y0, e3_mul(r, e3_sub(y1, y0)));
+    return e3_add(y0, ef_mul(r, e3_sub(y1, y0), a.ext2));
 }
 
 // Unreduced sums of Ext3 products (X^3 = 2): the doubled cross terms are fed
@@ -150,7 +151,8 @@ __device__ __forceinline__ void sc_round_finish(const ScKernelArgs& a, E3 c0, E3
                 sc->c0 = C0;
                 sc->c2 = C2;
                 sc->sc_r[a.r_slot] = rn;
-                sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+                const bool x2 = t.deg == 2;
+                sc->sum = e3_add(ef_mul(e3_add(ef_mul(C2, rn, x2), c1), rn, x2), C0);
             }
         }
         wtx_store(t, a.tx);
@@ -192,11 +194,11 @@ __global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_s
                 al = e3_add(x0, e3_mul_base(r, gl_sub(x1.c0, x0.c0)));
                 ah = e3_add(x2, e3_mul_base(r, gl_sub(x3.c0, x2.c0)));
             } else {
-                al = e3_add(x0, e3_mul(r, e3_sub(x1, x0)));
-                ah = e3_add(x2, e3_mul(r, e3_sub(x3, x2)));
+                al = e3_add(x0, ef_mul(r, e3_sub(x1, x0), a.ext2));
+                ah = e3_add(x2, ef_mul(r, e3_sub(x3, x2), a.ext2));
             }
-            const E3 bl = e3_add(y0, e3_mul(r, e3_sub(y1, y0)));
-            const E3 bh = e3_add(y2, e3_mul(r, e3_sub(y3, y2)));
+            const E3 bl = e3_add(y0, ef_mul(r, e3_sub(y1, y0), a.ext2));
+            const E3 bh = e3_add(y2, ef_mul(r, e3_sub(y3, y2), a.ext2));
             st3(a.a_out, i, al); st3(a.b, i, bl);
             st3(a.a_out, i + half, ah); st3(a.b, i + half, bh);
             accl_mac(c0, al, bl);
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_s
             accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
         }
     }
-    sc_round_finish(a, accl_reduce(c0), accl_reduce(c2), red, &is_last);
+    sc_round_finish(a, ef_fix(accl_reduce(c0), a.ext2), ef_fix(accl_reduce(c2), a.ext2), red, &is_last);
 }
 
 // After a round PoW: send the nonce, squeeze r, update the sum.
@@ -224,7 +226,8 @@ __global__ void k_sc_after_pow(TxState* tx, ProofScalars* sc, int r_slot) {
         const E3 C0 = sc->c0, C2 = sc->c2;
         const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
         sc->sc_r[r_slot] = rn;
-        sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+        const bool x2 = t.deg == 2;
+        sc->sum = e3_add(ef_mul(e3_add(ef_mul(C2, rn, x2), c1), rn, x2), C0);
     }
     wtx_store(t, tx);
 }
@@ -248,6 +251,7 @@ struct ScSmallArgs {
     int rounds, r_slot, fold_after;
     TxState* tx;
     ProofScalars* sc;
+    int ext2;
 };
 
 __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs a) {
@@ -268,6 +272,7 @@ __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs
         for (int c = 0; c < 3; ++c) { k.a_in[c] = a.a[c]; k.a_out[c] = a.a[c]; k.b[c] = a.b[c]; }
         k.size = size;
         k.fold = fold;
+        k.ext2 = a.ext2;
         if (last) {  // fold only
             for (u64 i = threadIdx.x; i < size; i += blockDim.x) {
                 st3(k.a_out, i, load_a(k, i, r));
@@ -292,8 +297,8 @@ __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs
                 accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
             }
         }
-        const E3 s0 = block_sum(accl_reduce(c0), red);
-        const E3 s2 = block_sum(accl_reduce(c2), red);
+        const E3 s0 = block_sum(ef_fix(accl_reduce(c0), a.ext2), red);
+        const E3 s2 = block_sum(ef_fix(accl_reduce(c2), a.ext2), red);
         if (threadIdx.x == 0) {
             tot[0] = s0;
             tot[1] = s2;
@@ -309,7 +314,8 @@ __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs
                 sc->c0 = C0;
                 sc->c2 = C2;
                 sc->sc_r[a.r_slot + t] = rn;
-                sc->sum = e3_add(e3_mul(e3_add(e3_mul(C2, rn), c1), rn), C0);
+                const bool x2 = wt.deg == 2;
+                sc->sum = e3_add(ef_mul(e3_add(ef_mul(C2, rn, x2), c1), rn, x2), C0);
             }
         }
         __syncthreads();
@@ -329,6 +335,7 @@ int launch_sumcheck_small(const SumcheckArgs& s, int rounds, int fold_after, cud
     a.fold_after = fold_after;
     a.tx = s.tx;
     a.sc = s.sc;
+    a.ext2 = s.ext2;
     k_sumcheck_small<<<1, SC_SMALL_THREADS, 0, st>>>(a);
     count_launches(1);
     return 0;
@@ -345,6 +352,7 @@ static ScKernelArgs make_sc(const SumcheckArgs& s) {
     a.pow_threshold = s.pow_threshold;
     a.tx = s.tx;
     a.sc = s.sc;
+    a.ext2 = s.ext2;
     a.partials = reinterpret_cast<E3*>(s.scratch);
     a.counter = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(s.scratch) + (size_t)SC_GRID * 2 * sizeof(E3));
     return a;
@@ -425,7 +433,7 @@ int launch_fold(const SumcheckArgs& s, cudaStream_t st) {
 constexpr u32 COV_LO = 10;
 
 __global__ void k_cov_tables(const u64* points, u32 logS, int n_forms, int n_ood, u32 dense_mask, ProofScalars* sc,
-                             E3* tab) {
+                             E3* tab, bool ext2, TxState* tx) {
     const u32 lo_bits = logS < COV_LO ? logS : COV_LO, hi_bits = logS - lo_bits;
     const u32 nlo = 1u << lo_bits, nhi = 1u << hi_bits;
     const u32 per = nlo + nhi;
@@ -440,27 +448,30 @@ __global__ void k_cov_tables(const u64* points, u32 logS, int n_forms, int n_ood
             const u64* pt = points + (u64)term * logS * 3;
             // coordinate c <-> bit (logS - 1 - c) of i; hi bits are coordinates 0..hi_bits-1
             v = e3_one();
+            if (ext2 && k == 0)  // a GoldilocksExt2 point has no X^2 coordinate
+                for (u32 c = 0; c < logS; ++c)
+                    if (pt[3 * c + 2]) atomicOr(&tx->err, TX_ERR_FIELD);
             if (k < nlo) {
                 for (u32 c = hi_bits; c < logS; ++c) {
                     const E3 x{pt[3 * c], pt[3 * c + 1], pt[3 * c + 2]};
                     const bool bit = (k >> (logS - 1 - c)) & 1;
-                    v = e3_mul(v, bit ? x : e3_sub(e3_one(), x));
+                    v = ef_mul(v, bit ? x : e3_sub(e3_one(), x), ext2);
                 }
             } else {
                 const u32 h = k - nlo;
                 for (u32 c = 0; c < hi_bits; ++c) {
                     const E3 x{pt[3 * c], pt[3 * c + 1], pt[3 * c + 2]};
                     const bool bit = (h >> (hi_bits - 1 - c)) & 1;
-                    v = e3_mul(v, bit ? x : e3_sub(e3_one(), x));
+                    v = ef_mul(v, bit ? x : e3_sub(e3_one(), x), ext2);
                 }
                 // linear_forms[0] is accumulated with scalar ONE (whir_prover.hpp:161)
-                v = e3_mul(v, term == 0 ? e3_one() : sc->crlc[term]);
+                v = ef_mul(v, term == 0 ? e3_one() : sc->crlc[term], ext2);
             }
         } else {
             const int j = (int)term - n_forms;
             const E3 z = sc->init_ood_pts[j];
-            if (k < nlo) v = e3_pow(z, k);
-            else v = e3_mul(sc->crlc[n_forms + j], e3_pow(z, (u64)(k - nlo) << lo_bits));
+            if (k < nlo) v = ef_pow(z, k, ext2);
+            else v = ef_mul(sc->crlc[n_forms + j], ef_pow(z, (u64)(k - nlo) << lo_bits, ext2), ext2);
         }
         tab[e] = v;
     }
@@ -479,12 +490,13 @@ __global__ void __launch_bounds__(256) k_cov_init(CovInitArgs a, const E3* tab) 
             if (t < a.n_forms && ((a.dense_mask >> t) & 1)) {
                 // Covector::accumulate: scalar * vector (linear_form.hpp:75-78)
                 const u64* d = a.dense[t] + 3 * i;
+                if (a.ext2 && d[2]) atomicOr(&a.tx->err, TX_ERR_FIELD);  // not a GoldilocksExt2 value
                 e3acc_mac(s, t == 0 ? e3_one() : a.sc->crlc[t], E3{d[0], d[1], d[2]});
             } else {
                 e3acc_mac(s, tab[(u64)t * per + nlo + hi], tab[(u64)t * per + lo]);
             }
         }
-        const E3 acc = e3acc_reduce(s);
+        const E3 acc = ef_fix(e3acc_reduce(s), a.ext2);
         a.cov[0][i] = acc.c0;
         a.cov[1][i] = acc.c1;
         a.cov[2][i] = acc.c2;
@@ -518,7 +530,7 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
     for (int f = 0; f < a.n_forms; ++f)
         if (((a.dense_mask >> f) & 1) && !a.dense[f]) return -1;
     if (nterms > 0) {
-        k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.dense_mask, a.sc, tab);
+        k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.dense_mask, a.sc, tab, a.ext2 != 0, a.tx);
         count_launches(1);
     }
     u64 want = (S + 255) / 256;
@@ -539,15 +551,16 @@ constexpr u32 CA_LO = 10;
 // Point j's table: z_j^l (l < 2^LO) then rlc_j z_j^(h 2^LO).  For the base-field
 // (in-domain) points z_j^l is a base element and goes to the compact array
 // lo_base[j - n_ext][l] instead, so a warp reads 8 contiguous bytes per lane.
-__global__ void k_cov_acc_tables(const ProofScalars* sc, int n_ext, int n_points, u32 hi_count, E3* tab, u64* lo_base) {
+__global__ void k_cov_acc_tables(const ProofScalars* sc, int n_ext, int n_points, u32 hi_count, E3* tab, u64* lo_base,
+                                 bool ext2) {
     const u32 per = (1u << CA_LO) + hi_count;
     const u64 total = (u64)per * n_points;
     for (u64 e = (u64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (u64)gridDim.x * blockDim.x) {
         const u32 j = (u32)(e / per), k = (u32)(e % per);
         const E3 z = sc->stir_pts[j];
         if ((int)j < n_ext) {
-            tab[e] = k < (1u << CA_LO) ? e3_pow(z, k)
-                                       : e3_mul(sc->stir_rlc[j], e3_pow(z, (u64)(k - (1u << CA_LO)) << CA_LO));
+            tab[e] = k < (1u << CA_LO) ? ef_pow(z, k, ext2)
+                                       : ef_mul(sc->stir_rlc[j], ef_pow(z, (u64)(k - (1u << CA_LO)) << CA_LO, ext2), ext2);
         } else if (k < (1u << CA_LO)) {
             lo_base[(u64)(j - n_ext) * (1u << CA_LO) + k] = gl_pow(z.c0, k);
         } else {
@@ -567,7 +580,7 @@ __global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* 
         const u64* lb = lo_base + lo;
         for (int j = a.n_ext; j < npts; ++j, tj += per, lb += (1u << CA_LO))
             e3acc_mac_base(s, tj[(1u << CA_LO) + hi], *lb);
-        const E3 add = e3acc_reduce(s);
+        const E3 add = ef_fix(e3acc_reduce(s), a.ext2);
         a.cov[0][i] = gl_add(a.cov[0][i], add.c0);
         a.cov[1][i] = gl_add(a.cov[1][i], add.c1);
         a.cov[2][i] = gl_add(a.cov[2][i], add.c2);
@@ -588,7 +601,7 @@ int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
     E3* tab = reinterpret_cast<E3*>(a.scratch);
     const size_t tab_bytes = ((size_t)(1u << CA_LO) + hc) * (size_t)npts * sizeof(E3);
     u64* lo_base = reinterpret_cast<u64*>(reinterpret_cast<char*>(a.scratch) + (tab_bytes + 255) / 256 * 256);
-    k_cov_acc_tables<<<296, 256, 0, st>>>(a.sc, a.n_ext, npts, hc, tab, lo_base);
+    k_cov_acc_tables<<<296, 256, 0, st>>>(a.sc, a.n_ext, npts, hc, tab, lo_base, a.ext2 != 0);
     count_launches(1);
     u64 want = (a.size + 255) / 256;
     k_cov_accumulate<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab, lo_base, hc);
@@ -644,7 +657,7 @@ int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch
     E3* partials = reinterpret_cast<E3*>(base + 256);
     E3* tab = reinterpret_cast<E3*>(base + 256 + 592 * sizeof(E3));
     cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
-    k_cov_tables<<<148, 256, 0, st>>>(point, logS, 1, 0, 0u, nullptr, tab);
+    k_cov_tables<<<148, 256, 0, st>>>(point, logS, 1, 0, 0u, nullptr, tab, false, nullptr);
     count_launches(1);
     const u64 S = 1ull << logS;
     u64 want = (S + 255) / 256;

@@ -35,7 +35,7 @@ __global__ void k_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsi
 
 int launch_tx_init(TxState* tx, const unsigned char* ds, u32 ds_len, unsigned char* narg, u64 narg_cap,
                    unsigned char* hints, u64 hints_cap, ProofScalars* sc, unsigned deg, cudaStream_t st) {
-    if (deg != 1 && deg != 3) return -1;
+    if (deg < 1 || deg > 3) return -1;
     k_tx_init<<<1, 32, 0, st>>>(tx, ds, ds_len, narg, narg_cap, hints, hints_cap, sc, deg);
     count_launches(1);
     return 0;
@@ -61,8 +61,8 @@ __global__ void k_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int
     for (int r = l; r < count; r += 32) {
         const E3* vals = r < n_forms ? &sc->forms_eval[r * nvec] : &sc->init_ood_mat[(r - n_forms) * nvec];
         E3 row = e3_zero();
-        for (int k = 0; k < nvec; ++k) row = e3_add(row, e3_mul(sc->vrlc[k], vals[k]));
-        v = e3_add(v, e3_mul(sc->crlc[r], row));
+        for (int k = 0; k < nvec; ++k) row = e3_add(row, ef_mul(sc->vrlc[k], vals[k], t.deg == 2));
+        v = e3_add(v, ef_mul(sc->crlc[r], row, t.deg == 2));
     }
     v = wtx_sum(v);
     if (l == 0) sc->sum = v;
@@ -274,6 +274,7 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
     const u32 q = a.q;
     const u32 nbytes = (a.logN + 7) / 8;
     const u32 nwit = a.nwit;
+    const bool x2 = tx->deg == 2;  // GoldilocksExt2 target field
 
     // 1. indices: warp 0 squeezes q * nbytes bytes (big-endian per index)
     WarpTx wt;
@@ -296,7 +297,7 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
         for (u32 k = 0; k < a.fold; ++k) {
             const E3 r = sc->sc_r[a.r_offset + k];
             const bool bit = (i >> (a.fold - 1 - k)) & 1;
-            acc = e3_mul(acc, bit ? r : e3_sub(e3_one(), r));
+            acc = ef_mul(acc, bit ? r : e3_sub(e3_one(), r), x2);
         }
         eqw[i] = acc;
     }
@@ -398,12 +399,15 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
                 E3 term;
                 if (a.ncomp == 1) {
                     term = e3_mul_base(eqw[el & dmask], planes[(u64)el * a.N + id]);
+                } else if (a.ncomp == 2) {  // Ext2 rows: planes c0, c1
+                    term = ef_mul(E3{planes[(u64)el * a.N + id], planes[((u64)a.depth + el) * a.N + id], 0},
+                                  eqw[el & dmask], true);
                 } else {
                     term = e3_mul(E3{planes[(u64)el * a.N + id], planes[((u64)a.depth + el) * a.N + id],
                                      planes[((u64)2 * a.depth + el) * a.N + id]},
                                   eqw[el & dmask]);
                 }
-                if (a.use_vrlc) term = e3_mul(term, sc->vrlc[w * (a.depth >> a.fold) + (el >> a.fold)]);
+                if (a.use_vrlc) term = ef_mul(term, sc->vrlc[w * (a.depth >> a.fold) + (el >> a.fold)], x2);
                 val = e3_add(val, term);
             }
             val = e3_warp_sum(val);
@@ -473,7 +477,7 @@ __global__ void k_stir_rlc(TxState* tx, ProofScalars* sc, int commit_idx, int n_
     wtx_geometric(t, sc->stir_rlc, count);
     wtx_store(t, tx);
     E3 acc = e3_zero();
-    for (int j = l; j < count; j += 32) acc = e3_add(acc, e3_mul(sc->stir_rlc[j], sc->stir_vals[j]));
+    for (int j = l; j < count; j += 32) acc = e3_add(acc, ef_mul(sc->stir_rlc[j], sc->stir_vals[j], t.deg == 2));
     acc = wtx_sum(acc);
     if (l == 0) sc->sum = e3_add(sc->sum, acc);
 }

@@ -106,6 +106,7 @@ struct OodArgs {
     TxState* tx;
     void* scratch;
     u32 scratch_values;       // n_ood * nvec capacity of the scratch
+    int ext2;                 // target field GoldilocksExt2 (vectors and points (c0, c1, 0))
 };
 int launch_ood(const OodArgs& a, cudaStream_t st);
 size_t ood_scratch_bytes(u64 max_size, u32 max_values);
@@ -168,6 +169,8 @@ struct CovInitArgs {
     u64* vec_out[3];    // Ext3 planes of the combined vector
     u32 dense_mask;     // forms f with bit f set are dense covectors (their points slot is unused):
     const u64* dense[8];  // cov[i] += crlc_f * dense[f][i] (Ext3, AoS), crlc_0 = 1
+    int ext2;           // target field GoldilocksExt2 (values (c0, c1, 0), X^2 = 7)
+    TxState* tx;        // with ext2: a form value outside (c0, c1) sets TX_ERR_FIELD in tx->err
 };
 int launch_cov_init(const CovInitArgs& a, cudaStream_t st);
 size_t cov_init_scratch_bytes(u32 logS, int n_forms, int n_ood);
@@ -178,6 +181,7 @@ struct CovAccArgs {
     int n_ext, n_base;
     ProofScalars* sc;
     void* scratch;
+    int ext2;
 };
 int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st);
 size_t cov_acc_scratch_bytes(u64 size, int n_points);
@@ -196,6 +200,7 @@ struct SumcheckArgs {
     TxState* tx;
     ProofScalars* sc;
     void* scratch;
+    int ext2;           // target field GoldilocksExt2
 };
 // One sumcheck round (sumcheck_protocol.hpp:99-135) with the previous round's
 // fold fused in.  PoW (if any) and the challenge squeeze happen in-stream.

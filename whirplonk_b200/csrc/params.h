@@ -25,7 +25,8 @@ struct ProtocolParams {  // whir::ProtocolParameters (cpp/include/whir/parameter
     int hash = 0;  // engine of hash_id: 0 BLAKE3, 1 SHA-256 (leaves, Merkle, PoW)
     // Not a ProtocolParameters field but the embedding M of Config<M>: the
     // target field's degree over Goldilocks, 3 for Basefield<GoldilocksExt3>
-    // (field_size_bits 192), 1 for Identity<Goldilocks> (64).
+    // (field_size_bits 192), 2 for Basefield<GoldilocksExt2> (128), 1 for
+    // Identity<Goldilocks> (64).
     int field_degree = 3;
 };
 
@@ -109,7 +110,7 @@ inline WhirSchedule make_schedule(uint64_t num_variables, const ProtocolParams& 
     c.num_variables = num_variables;
     const double security = (double)p.security_level;
     const double psec = (double)(p.security_level - p.pow_bits);
-    const double fbits = p.field_degree == 1 ? 64.0 : 192.0;  // Target::field_size_bits
+    const double fbits = 64.0 * p.field_degree;  // Target::field_size_bits: 64, 128 (Ext2), 192 (Ext3)
     uint64_t lir = p.starting_log_inv_rate;
     uint64_t nv = num_variables;
     const double irate = std::pow(0.5, (double)p.starting_log_inv_rate);

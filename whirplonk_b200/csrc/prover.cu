@@ -44,7 +44,7 @@ ProofPlan make_plan(uint32_t n, const ProtocolParams& params, int n_forms, size_
 
 ProofPlan make_plan(const WhirSchedule& sched, const ProtocolParams& params, int n_forms, size_t ds_len, uint32_t nwit) {
     validate_schedule(sched);
-    if (params.field_degree != 1 && params.field_degree != 3) throw std::invalid_argument("field degree must be 1 or 3");
+    if (params.field_degree < 1 || params.field_degree > 3) throw std::invalid_argument("field degree must be 1, 2 or 3");
     const uint32_t n = ilog2(sched.initial.vector_size);
     ProofPlan p;
     p.sch = sched;
@@ -231,7 +231,8 @@ int commit_vectors(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t 
     WG_TIMED(c, FAM_MERKLE, launch_merkle(nodes, cb.logN, c.tx(), c.sc(), ci, n_ood, c.p.params.hash, c.st));
     OodArgs o{};
     for (int k = 0; k < 3; ++k) o.v[k] = src[k] ? src[k] : src[0];
-    o.ext3 = ncomp == 3;
+    o.ext3 = ncomp != 1;  // Ext2 vectors are read as (c0, c1, c2 = 0) planes
+    o.ext2 = c.p.params.field_degree == 2;
     o.size = vsize;
     o.nvec = vectors;
     o.vec_stride = vsize;
@@ -260,6 +261,7 @@ int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_f
         a.hash = c.p.params.hash;
         a.tx = c.tx();
         a.sc = c.sc();
+        a.ext2 = c.p.params.field_degree == 2;
         int rc = 1;
         WG_TIMED(c, FAM_SUMCHECK, (rc = launch_sumcheck_small(a, (int)s.num_rounds, fold_after ? 1 : 0, c.st)) < 0 ? rc : 0);
         if (rc == 0) {
@@ -280,6 +282,7 @@ int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_f
         a.hash = c.p.params.hash;
         a.tx = c.tx();
         a.sc = c.sc();
+        a.ext2 = c.p.params.field_degree == 2;
         a.scratch = c.ws + c.p.off_sc_scratch;
         if (base_first && t == 0) a.a_base = c.w(c.p.off_coeffs);
         WG_TIMED(c, FAM_SUMCHECK, launch_sumcheck_round(a, c.st));
@@ -293,6 +296,7 @@ int sumcheck(const Ctx& c, const SumcheckSchedule& s, uint64_t size, bool base_f
         a.size = size >> s.num_rounds;
         a.fold_r = r_slot - 1;
         a.sc = c.sc();
+        a.ext2 = c.p.params.field_degree == 2;
         WG_TIMED(c, FAM_SUMCHECK, launch_fold(a, c.st));
     }
     return 0;
@@ -344,6 +348,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
             o.tx = c.tx();
             o.scratch = ws + p.off_ood_scratch;
             o.scratch_values = p.ood_values;
+            o.ext2 = p.params.field_degree == 2;
             WG_TIMED(c, FAM_OOD, launch_ood(o, st));
         }
     }
@@ -364,6 +369,8 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         ci.vecs = c.w(p.off_coeffs);
         ci.dense_mask = p.dense_mask;
         for (int f = 0; f < 8; ++f) ci.dense[f] = p.dense[f];
+        ci.ext2 = p.params.field_degree == 2;
+        ci.tx = c.tx();
         WG_TIMED(c, FAM_COV, launch_cov_init(ci, st));
     }
     if (has_constraints) {
@@ -383,6 +390,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
             a.size = size0 >> (t + 1);
             a.fold_r = t;
             a.sc = c.sc();
+            a.ext2 = p.params.field_degree == 2;
             WG_TIMED(c, FAM_SUMCHECK, launch_fold(a, st));
         }
         r_slot = k;
@@ -392,8 +400,9 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         const RoundSchedule& rc = s.rounds[r];
         const int ci = (int)(W + r);
-        const uint32_t deg = (uint32_t)p.params.field_degree;  // base-field rounds commit the c0 plane only
-        const uint64_t* src[3] = {c.a(0), deg == 3 ? c.a(1) : nullptr, deg == 3 ? c.a(2) : nullptr};
+        // base-field rounds commit the c0 plane only, Ext2 rounds c0 and c1 (c2 is zero)
+        const uint32_t deg = (uint32_t)p.params.field_degree;
+        const uint64_t* src[3] = {c.a(0), deg >= 2 ? c.a(1) : nullptr, deg >= 2 ? c.a(2) : nullptr};
         WG_TRY(commit_vectors(c, ci, src, deg, vsize, 1, (int)rc.irs.out_domain, &c.sc()->ood_vals[ci][0], 1));
         WG_TIMED(c, FAM_POW, launch_pow(c.tx(), c.sc(), rc.pow_threshold, ci, c.p.params.hash, st));
         // open the previous commitment (the first round: every initial commitment)
@@ -428,6 +437,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         ca.n_base = (int)prev.in_domain;
         ca.sc = c.sc();
         ca.scratch = ws + p.off_cov_scratch;
+        ca.ext2 = p.params.field_degree == 2;
         WG_TIMED(c, FAM_COV, launch_cov_accumulate(ca, st));
         WG_TRY(sumcheck(c, rc.sumcheck, vsize, false, r_slot, true));
         vsize >>= rc.sumcheck.num_rounds;

@@ -67,7 +67,7 @@ struct TxState {
     u64 hasher[25];
     u64 reader[25];
     unsigned hpos, rpos, has_reader, err;
-    unsigned deg;  // degree of the target field over Goldilocks: 3 (Ext3) or 1 (the base field)
+    unsigned deg;  // degree of the target field over Goldilocks: 3 (Ext3), 2 (Ext2) or 1 (the base field)
     u64 narg_len, hints_len;
     u64 narg_cap, hints_cap;
     u8* narg;

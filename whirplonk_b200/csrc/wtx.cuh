@@ -228,15 +228,26 @@ __device__ __forceinline__ E3 wtx_challenge_e3(WarpTx& t) {
 // Elements of the protocol's target field.  With the base field as target
 // (Identity<Goldilocks>) its elements are carried as Ext3 values (x, 0, 0) --
 // a subfield, so every kernel's arithmetic is unchanged -- and cross the
-// transcript as one 8-byte word / one 40-byte challenge (transcript.hpp:375-453).
+// transcript as one 8-byte word / one 40-byte challenge; GoldilocksExt2
+// elements are carried as (c0, c1, 0) (products folded by e2_fold) and cross
+// it as two words / two 40-byte chunks (transcript.hpp:375-453).
 __device__ __forceinline__ E3 wtx_challenge_t(WarpTx& t) {
     if (t.deg == 1) return E3{wtx_challenge_base(t), 0, 0};
+    if (t.deg == 2) {
+        const u64 c0 = wtx_challenge_base(t);
+        const u64 c1 = wtx_challenge_base(t);
+        return E3{c0, c1, 0};
+    }
     return wtx_challenge_e3(t);
 }
 __device__ __forceinline__ void wtx_message_t(WarpTx& t, E3 v) {
     if (t.deg == 1) {
         if (v.c1 | v.c2) t.err |= TX_ERR_FIELD;  // outside the base field: caller input was not base-field
         wtx_message_u64(t, v.c0);
+    } else if (t.deg == 2) {
+        if (v.c2) t.err |= TX_ERR_FIELD;  // outside GoldilocksExt2's (c0, c1)
+        u64 w[2] = {v.c0, v.c1};
+        wtx_message_words(t, w, 2);
     } else {
         wtx_message_e3(t, v);
     }
@@ -259,14 +270,14 @@ __device__ __forceinline__ void wtx_geometric(WarpTx& t, E3* out, int count) {
     for (int o = 1; o < 32; o <<= 1) {
         const E3 q{__shfl_up_sync(0xFFFFFFFFu, p.c0, o), __shfl_up_sync(0xFFFFFFFFu, p.c1, o),
                    __shfl_up_sync(0xFFFFFFFFu, p.c2, o)};
-        if (l >= (unsigned)o) p = e3_mul(p, q);
+        if (l >= (unsigned)o) p = ef_mul(p, q, t.deg == 2);
     }
     // x^32 = (x^31) * x
     E3 x31{__shfl_sync(0xFFFFFFFFu, p.c0, 31), __shfl_sync(0xFFFFFFFFu, p.c1, 31), __shfl_sync(0xFFFFFFFFu, p.c2, 31)};
-    const E3 x32 = e3_mul(x31, x);
+    const E3 x32 = ef_mul(x31, x, t.deg == 2);
     for (int base = 0; base < count; base += 32) {
         if (base + (int)l < count) out[base + l] = p;
-        p = e3_mul(p, x32);
+        p = ef_mul(p, x32, t.deg == 2);
     }
     __syncwarp();
 }

@@ -238,13 +238,15 @@ class Witness:
             pass
 
 
-FIELD_GOLDILOCKS1, FIELD_GOLDILOCKS3 = _lib.FIELD_GOLDILOCKS1, _lib.FIELD_GOLDILOCKS3
+FIELD_GOLDILOCKS1, FIELD_GOLDILOCKS2, FIELD_GOLDILOCKS3 = (_lib.FIELD_GOLDILOCKS1, _lib.FIELD_GOLDILOCKS2,
+                                                            _lib.FIELD_GOLDILOCKS3)
 
 
 @dataclass
 class Config:
     """Config<M> (whir.hpp:104-343) with M = Basefield<GoldilocksExt3> (field 3,
-    the CLI's Goldilocks3) or Identity<Goldilocks> (field 1, Goldilocks1).
+    the CLI's Goldilocks3), Basefield<GoldilocksExt2> (field 2, Goldilocks2) or
+    Identity<Goldilocks> (field 1, Goldilocks1).
     ``from_params`` derives it as the reference does; ``custom`` takes one built
     field by field (``_lib.WhirConfig``), as the reference's golden dumpers do."""
 
