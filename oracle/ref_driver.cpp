@@ -172,7 +172,7 @@ struct Job {
     std::vector<bool> dense;
     std::vector<std::vector<std::uint64_t>> forms;  // 3 words per element
     std::vector<std::vector<Source>> vecs;
-    bool do_verify = false, print_cfg = false, use_sha2 = false, unique = false;
+    bool do_verify = false, print_cfg = false, config_only = false, use_sha2 = false, unique = false;
     int reps = 1;
     const char* out_path = nullptr;
 };
@@ -223,6 +223,7 @@ int run(const Job& j) {
             config.final_sumcheck.initial_size, config.final_sumcheck.num_rounds,
             (unsigned long long)config.final_pow.threshold_val,
             (unsigned long long)config.final_sumcheck.round_pow.threshold_val);
+        if (j.config_only) return 0;
     }
 
     M emb{};
@@ -308,6 +309,7 @@ int main(int argc, char** argv) {
     for (int i = 3; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--verify")) j.do_verify = true;
         else if (!std::strcmp(argv[i], "--config")) j.print_cfg = true;
+        else if (!std::strcmp(argv[i], "--config-only")) j.print_cfg = j.config_only = true;
         else if (!std::strcmp(argv[i], "--sha2")) j.use_sha2 = true;
         else if (!std::strcmp(argv[i], "--unique")) j.unique = true;
         else if (!std::strcmp(argv[i], "--field1")) field1 = true;
