@@ -113,21 +113,13 @@ __device__ __forceinline__ u64 gl_reduce_dev(u64 lo, u64 hi) {
         : "l"(lo), "l"(hi));
     return ((u64)r1 << 32) | r0;
 }
-// (a * b) mod p, canonical output for any 64-bit a, b.
+// (a * b) mod p, canonical output for any 64-bit a, b.  The 128-bit product
+// is left to the compiler's 64-bit multiply (measured ~2 % faster on B200 than
+// a hand-written 32-bit limb chain in a butterfly-like mix).
 __device__ __forceinline__ u64 gl_mul(u64 a, u64 b) {
-    unsigned r0, r1, r2, r3;
-    asm("mul.lo.u32 %0, %4, %6;\n\t"
-        "mul.hi.u32 %1, %4, %6;\n\t"
-        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
-        "madc.hi.u32 %2, %4, %7, 0;\n\t"
-        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
-        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
-        "madc.hi.u32 %3, %5, %7, 0;\n\t"
-        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
-        "addc.u32 %3, %3, 0;"
-        : "=&r"(r0), "=&r"(r1), "=&r"(r2), "=&r"(r3)
-        : "r"((unsigned)a), "r"((unsigned)(a >> 32)), "r"((unsigned)b), "r"((unsigned)(b >> 32)));
-    return gl_reduce_dev(((u64)r1 << 32) | r0, ((u64)r3 << 32) | r2);
+    u64 lo, hi;
+    asm("mul.lo.u64 %0, %2, %3;\n\tmul.hi.u64 %1, %2, %3;" : "=l"(lo), "=l"(hi) : "l"(a), "l"(b));
+    return gl_reduce_dev(lo, hi);
 }
 __host__ __forceinline__ u64 gl_mul_host(u64 a, u64 b) {
     unsigned __int128 x = (unsigned __int128)a * b;
