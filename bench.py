@@ -398,27 +398,34 @@ def run_reference_zk_arm(args, w, world):
 # GPU arm
 # ---------------------------------------------------------------------------
 class Harness:
-    def __init__(self, rank, world, local_rank):
+    """One rank: process group (NCCL on GPUs; gloo on the host, for the
+    multi-process tests without a GPU), barriers, max / sum over ranks."""
+
+    def __init__(self, rank, world, local_rank, backend=None):
         import torch
 
         self.torch = torch
         self.dist = None
+        self.cuda = backend != "gloo"
         if world > 1:
             import datetime
 
             import torch.distributed as dist
 
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group(backend or "nccl", timeout=datetime.timedelta(seconds=120))
             self.dist = dist
-        torch.cuda.set_device(local_rank)
-        self.device = f"cuda:{local_rank}"
+        if self.cuda:
+            torch.cuda.set_device(local_rank)
+        self.device = f"cuda:{local_rank}" if self.cuda else "cpu"
         self.rank, self.world, self.local_rank = rank, world, local_rank
 
     def barrier(self):
-        self.torch.cuda.synchronize()
+        if self.cuda:
+            self.torch.cuda.synchronize()
         if self.dist is not None:
             self.dist.barrier()
-        self.torch.cuda.synchronize()
+        if self.cuda:
+            self.torch.cuda.synchronize()
 
     def max_over_ranks(self, x):
         if self.dist is None:
