@@ -29,9 +29,17 @@ __device__ __forceinline__ unsigned wtx_lane() { return threadIdx.x & 31; }
 
 __device__ __forceinline__ u64 rotl64_var(u64 v, unsigned s) { return s ? ((v << s) | (v >> (64 - s))) : v; }
 
+// Source lane of pi for lane (X, Y): pi moves A[x][y] to (y, 2x + 3y), so lane
+// (X, Y) receives from (3 (Y - 3X) mod 5, X).
+__device__ __forceinline__ unsigned keccak_pi_src(unsigned x, unsigned y) {
+    return ((5 + 3 * ((y + 15 - 3 * x) % 5)) % 5) + 5 * x;
+}
+
 // Keccak-f[1600] with state word l in lane l (lanes 25..31 carry a dummy).
-// Lane (x, y) = x + 5 y.  pi moves A[x][y] to (y, 2x + 3y), so lane (X, Y)
-// receives from (3 (Y - 3X) mod 5, X).
+// Lane (x, y) = x + 5 y.  Each lane rotates its own word (rho), then fetches
+// the three pi-permuted words chi needs -- B[X][Y], B[X+1][Y], B[X+2][Y] --
+// straight from their source lanes: three shuffle stages per round (theta's
+// column sums, theta's D, pi + chi).
 static __device__ __noinline__ u64 keccak_f1600_warp(u64 a) {
     const unsigned l = wtx_lane();
     const bool live = l < 25;
@@ -40,8 +48,9 @@ static __device__ __noinline__ u64 keccak_f1600_warp(u64 a) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) th[k] = live ? x + 5 * ((y + 1 + k) % 5) : l;
     const unsigned cl = live ? (x + 4) % 5 + 5 * y : l, cr = live ? (x + 1) % 5 + 5 * y : l;
-    const unsigned c2 = live ? (x + 2) % 5 + 5 * y : l;
-    const unsigned pi = live ? ((5 + 3 * ((y + 15 - 3 * x) % 5)) % 5) + 5 * x : l;
+    const unsigned p0 = live ? keccak_pi_src(x, y) : l;
+    const unsigned p1 = live ? keccak_pi_src((x + 1) % 5, y) : l;
+    const unsigned p2 = live ? keccak_pi_src((x + 2) % 5, y) : l;
     unsigned rot = 0;
 #pragma unroll
     for (int yy = 0; yy < 5; ++yy)
@@ -55,9 +64,10 @@ static __device__ __noinline__ u64 keccak_f1600_warp(u64 a) {
         for (int k = 0; k < 4; ++k) c ^= __shfl_sync(0xFFFFFFFFu, a, th[k]);
         const u64 d = __shfl_sync(0xFFFFFFFFu, c, cl) ^ rotl64_var(__shfl_sync(0xFFFFFFFFu, c, cr), 1);
         a ^= d;
-        a = __shfl_sync(0xFFFFFFFFu, rotl64_var(a, rot), pi);
-        const u64 b1 = __shfl_sync(0xFFFFFFFFu, a, cr), b2 = __shfl_sync(0xFFFFFFFFu, a, c2);
-        a ^= ~b1 & b2;
+        const u64 r = rotl64_var(a, rot);
+        const u64 b0 = __shfl_sync(0xFFFFFFFFu, r, p0), b1 = __shfl_sync(0xFFFFFFFFu, r, p1),
+                  b2 = __shfl_sync(0xFFFFFFFFu, r, p2);
+        a = b0 ^ (~b1 & b2);
         if (l == 0) a ^= KECCAK_RC[round];
     }
     return a;
