@@ -235,9 +235,13 @@ whirgpu_status whirgpu_zk_commit(whirgpu_ctx* ctx, const whirgpu_zk_config* conf
 /* ZkConfig::prove (whir_zk_impl.hpp:150-330): up to 7 linear forms as in
  * whirgpu_prove_forms, over the base field (every Ext3 value (x, 0, 0)), and
  * num_forms * num_polynomials claimed evaluations (Ext3 layout, form-major).
- * On return the proof is complete and readable with whirgpu_proof_get. */
+ * On return the proof is complete and readable with whirgpu_proof_get.  The
+ * FinalClaim it returns is the blinded inner proof's (whir_zk_impl.hpp:305-310):
+ * evaluation_point (optional) receives num_variables Ext3 values, rlc
+ * (optional) num_forms Ext3 values, as in whirgpu_prove_forms. */
 whirgpu_status whirgpu_zk_prove(whirgpu_ctx* ctx, whirgpu_zk_witness* witness, const whirgpu_linear_form* forms,
-                                size_t num_forms, const uint64_t* evaluations, whirgpu_transcript* tx);
+                                size_t num_forms, const uint64_t* evaluations, whirgpu_transcript* tx,
+                                uint64_t* evaluation_point, uint64_t* rlc);
 void whirgpu_zk_witness_destroy(whirgpu_zk_witness* witness);
 /* The DeterministicRng byte stream (deterministic_rng.hpp:16-98) as 64-bit LE
  * words first_word .. first_word + count - 1, computed on the device. */

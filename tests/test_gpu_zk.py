@@ -62,9 +62,13 @@ def test_zk_proof_from_device_input_and_reuse(gpu_ctx):
     ps = ProverState.from_ds(cli_domain_separator(case_params(case)), b"", gpu_ctx)
     rng = DeterministicRng(case_seed(case))
     w = cfg.commit(ps, None, rng, on_device_ptr=dev.data_ptr())
-    cfg.prove(ps, polys, w, forms, evals, rng)
+    claim = cfg.prove(ps, polys, w, forms, evals, rng)
     narg, _ = ps.proof()
     assert hashlib.sha256(narg).hexdigest() == case["narg_sha256"]
+    # the blinded proof's FinalClaim: one base-field coordinate per variable, one
+    # RLC coefficient per form, the first being 1 (geometric_challenge)
+    assert len(claim.evaluation_point) == case["n"] and all(c[1] == c[2] == 0 for c in claim.evaluation_point)
+    assert len(claim.rlc_coefficients) == len(forms) and claim.rlc_coefficients[0] == (1, 0, 0)
     with pytest.raises(WhirGpuError):
         cfg.prove(ps, polys, w, forms, evals, rng)
 

@@ -237,7 +237,7 @@ def load() -> ctypes.CDLL:
     L.whirgpu_zk_config_from_params.argtypes = [ctypes.POINTER(WhirParams), u64, u64, ctypes.POINTER(ZkPolicy),
                                                 ctypes.POINTER(ZkConfig)]
     L.whirgpu_zk_commit.argtypes = [p, ctypes.POINTER(ZkConfig), p, i32, p, ctypes.c_char_p, sz, p, vp]
-    L.whirgpu_zk_prove.argtypes = [p, p, ctypes.POINTER(LinearForm), sz, p, p]
+    L.whirgpu_zk_prove.argtypes = [p, p, ctypes.POINTER(LinearForm), sz, p, p, p, p]
     L.whirgpu_zk_witness_destroy.argtypes = [p]
     L.whirgpu_zk_witness_destroy.restype = None
     L.whirgpu_deterministic_rng.argtypes = [p, p, ctypes.c_char_p, sz, u64, p, sz]

@@ -668,7 +668,8 @@ whirgpu_status whirgpu_zk_commit(whirgpu_ctx* c, const whirgpu_zk_config* cfg, c
 }
 
 whirgpu_status whirgpu_zk_prove(whirgpu_ctx* c, whirgpu_zk_witness* w, const whirgpu_linear_form* forms,
-                                size_t num_forms, const uint64_t* evaluations, whirgpu_transcript* tx) {
+                                size_t num_forms, const uint64_t* evaluations, whirgpu_transcript* tx,
+                                uint64_t* evaluation_point, uint64_t* rlc) {
     if (!c || !w || !tx || w->ctx != c || w->tx != tx || !w->dev) return zk_fail(c, WHIRGPU_E_INVALID, "bad handles");
     if (w->proved) return zk_fail(c, WHIRGPU_E_INVALID, "a zero-knowledge witness proves once");
     if (num_forms > (size_t)MAX_FORMS - 1 || (num_forms && (!forms || !evaluations)))
@@ -867,6 +868,12 @@ whirgpu_status whirgpu_zk_prove(whirgpu_ctx* c, whirgpu_zk_witness* w, const whi
     if (htx.hints_len)
         ZK_CUDA(c, cudaMemcpyAsync(tx->hints.data(), dev + w->off_hints, htx.hints_len, cudaMemcpyDeviceToHost, st),
                 "read-back");
+    // FinalClaim of the blinded proof: its folding randomness and constraint RLC
+    if (evaluation_point)
+        ZK_CUDA(c, cudaMemcpyAsync(evaluation_point, &scb->sc_r[0], pb.total_sumcheck_rounds * 24,
+                                   cudaMemcpyDeviceToHost, st), "read-back");
+    if (rlc && num_forms)
+        ZK_CUDA(c, cudaMemcpyAsync(rlc, &scb->crlc[0], num_forms * 24, cudaMemcpyDeviceToHost, st), "read-back");
     ZK_CUDA(c, cudaStreamSynchronize(st), "read-back");
     c->io_d2h += sizeof(TxState) + htx.narg_len + htx.hints_len;
     tx->complete = true;

@@ -23,8 +23,8 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from .whir import Context, Covector, DomainSeparator, MultilinearExtension, ProtocolParameters, ProverState, \
-    cli_domain_separator, default_context
+from .whir import Context, Covector, DomainSeparator, FinalClaim, MultilinearExtension, ProtocolParameters, \
+    ProverState, cli_domain_separator, default_context
 
 
 @dataclass
@@ -173,7 +173,8 @@ class ZkConfig:
     def prove(self, prover_state: ProverState, polynomials, witness: ZkWitness, linear_forms: Sequence,
               evaluations: Sequence, rng: Optional[DeterministicRng] = None):
         """ZkConfig::prove; ``evaluations`` holds len(linear_forms) * num_polynomials
-        values (ints or Ext3 triples with zero high parts), form-major."""
+        values (ints or Ext3 triples with zero high parts), form-major.  Returns
+        the blinded inner proof's FinalClaim, as the reference does."""
         ctx = prover_state.ctx
         n = self.num_witness_variables
         cforms = (_lib.LinearForm * max(len(linear_forms), 1))()
@@ -198,8 +199,12 @@ class ZkConfig:
         ev = np.zeros((max(len(evaluations), 1), 3), dtype=np.uint64)
         for i, e in enumerate(evaluations):
             ev[i] = np.asarray(e, dtype=np.uint64).reshape(-1)[:3] if np.ndim(e) else (int(e), 0, 0)
+        point = np.zeros((n, 3), dtype=np.uint64)
+        rlc = np.zeros((max(len(linear_forms), 1), 3), dtype=np.uint64)
         _lib.check(ctx._L.whirgpu_zk_prove(ctx.handle, witness.handle, cforms, len(linear_forms), ev.ctypes.data,
-                                           prover_state.handle), ctx.handle)
+                                           prover_state.handle, point.ctypes.data, rlc.ctypes.data), ctx.handle)
+        return FinalClaim([tuple(int(x) for x in r) for r in point],
+                          [tuple(int(x) for x in r) for r in rlc[:len(linear_forms)]])
 
 
 def prove_zk_once(n: int, params: ProtocolParameters, polynomials, forms: Sequence, evaluations: Sequence,
