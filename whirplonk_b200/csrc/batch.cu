@@ -361,6 +361,10 @@ struct whirgpu_server {
     std::map<uint64_t, std::unique_ptr<Ticket>> tickets;
     std::deque<uint64_t> queue;                 // waiting for admission, arrival order
     std::vector<uint64_t> inflight;
+    // Streams in SERVER_LEVELS priority pools of max_inflight each: stream k
+    // serves level k / max_inflight (server_level: small proofs on the
+    // highest-priority streams, so their blocks are scheduled ahead of a large
+    // proof's when both are pending; the large proofs are throughput-bound).
     std::vector<cudaStream_t> streams;
     std::vector<int> stream_busy;
     // Captured single-proof programs, one per (workspace, statement count):
@@ -434,17 +438,24 @@ whirgpu_status program_for(whirgpu_server* s, const whirgpu_request& r, cudaStre
     return WHIRGPU_OK;
 }
 
-// Admits queued requests that fit the HBM budget and a free stream, in arrival
-// order; a later request may pass an earlier one that does not fit yet.
+// Priority level of a request: 0 (high) for proofs of up to 2^18
+// coefficients -- latency-bound chains of small kernels -- 1 above.
+constexpr int SERVER_LEVELS = 2;
+int server_level(const whirgpu_request& r) { return r.num_variables <= 18 ? 0 : 1; }
+
+// Admits queued requests that fit the HBM budget and a free stream of their
+// priority level, in arrival order; a later request may pass an earlier one
+// that does not fit yet.
 void admit(whirgpu_server* s) {
     for (auto it = s->queue.begin(); it != s->queue.end();) {
         if (s->inflight.size() >= s->max_inflight) break;
         Ticket& t = *s->tickets[*it];
         if (s->budget && s->in_use + t.bytes > s->budget) { ++it; continue; }
         int k = -1;
-        for (size_t j = 0; j < s->streams.size(); ++j)
+        const size_t base = (size_t)server_level(t.req) * s->max_inflight;
+        for (size_t j = base; j < base + s->max_inflight; ++j)
             if (!s->stream_busy[j]) { k = (int)j; break; }
-        if (k < 0) break;
+        if (k < 0) { ++it; continue; }
         Slot* slot = nullptr;
         whirgpu_status st = program_for(s, t.req, s->streams[k], &slot);
         if (st == WHIRGPU_OK) {
@@ -521,9 +532,15 @@ whirgpu_status whirgpu_server_create(whirgpu_ctx* c, uint64_t hbm_budget, uint32
     s->ctx = c;
     s->budget = hbm_budget;
     s->max_inflight = max_inflight;
-    s->streams.resize(max_inflight);
-    s->stream_busy.assign(max_inflight, 0);
-    for (auto& st : s->streams) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int least = 0, greatest = 0;  // numerically: greatest <= least
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    s->streams.resize((size_t)SERVER_LEVELS * max_inflight);
+    s->stream_busy.assign(s->streams.size(), 0);
+    for (size_t k = 0; k < s->streams.size(); ++k) {
+        const int level = (int)(k / max_inflight);  // 0: greatest priority
+        const int prio = greatest + (least - greatest) * level / (SERVER_LEVELS - 1);
+        cudaStreamCreateWithPriority(&s->streams[k], cudaStreamNonBlocking, prio);
+    }
     whirgpu_server* raw = s.release();
     raw->worker = std::thread(server_loop, raw);
     *out = raw;
