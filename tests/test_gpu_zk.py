@@ -109,3 +109,25 @@ def test_reference_zk_dump(gpu_ctx):
                                 ctx=gpu_ctx, config=cfg, ds=ds)
     assert narg.hex() == GOLD_ZK["narg"]
     assert hints.hex() == GOLD_ZK["hints"]
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(HERE), "oracle", "_ref", "ref_zk_driver")),
+                    reason="oracle/_ref not built")
+def test_zk_n24_matches_live_reference(gpu_ctx):
+    """The largest size of the WHIR workloads (2^24 coefficients, rate 1/4,
+    100-bit parameters, derived policy, PoW off): the GPU's ZK proof equals the
+    reference ZK prover's."""
+    from oracle.refio import run_reference_zk
+    from whirplonk_b200 import MultilinearExtension, ProtocolParameters, sample_goldilocks
+    from whirplonk_b200.zk import ZkConfig
+
+    n, seed = 24, 4242
+    p = ProtocolParameters(False, 2, 4, 4, 100, 20, 1)
+    poly = sample_goldilocks(seed, 1 << n).reshape(1, -1)
+    point = np.zeros((n, 3), dtype=np.uint64)
+    point[:, 0] = sample_goldilocks(seed + 1, n)
+    ref = run_reference_zk(n, 4, 2, 100, 20, [("mle", point[:, 0])], poly, seed, no_pow=True, verify=False)
+    cfg = ZkConfig.from_params(1 << n, p, 1).disable_pow()
+    narg, hints = prove_zk_once(n, p, poly, [MultilinearExtension(point)], [(int(ref.evaluations[0]), 0, 0)],
+                                int(seed).to_bytes(8, "little") + bytes(24), ctx=gpu_ctx, config=cfg)
+    assert narg == ref.narg and hints == ref.hints
