@@ -1,5 +1,7 @@
-"""B200-native WHIR prover (commit + prove over Goldilocks, Ext3 sumcheck,
-BLAKE3 or SHA-256 Merkle commitments) behind the reference C++ prover API.
+"""B200-native WHIR prover (commit + prove over Goldilocks with an Ext3, Ext2
+or base-field target, BLAKE3 or SHA-256 Merkle commitments, and the
+zero-knowledge ZkConfig<Goldilocks> in ``whirplonk_b200.zk``) behind the
+reference C++ prover API.
 
 The prover itself is libwhirgpu.so (hand-written sm_100a CUDA kernels behind
 the C ABI in include/whirgpu.h); this package is its Python mirror.
