@@ -57,20 +57,41 @@ struct ScKernelArgs {
     int ext2;
 };
 
+// The fold x0 + r (x1 - x0) by the round challenge r, a constant of the
+// kernel: the X and X^2 parts of r are doubled once (X^3 = 2), x0 seeds the
+// 192-bit accumulators and each component is reduced once -- no separate
+// doubling or addition per fold.  ext2: fold X^2 = 7 afterwards (e2_fold).
+struct FoldR {
+    u64 r0, r1, r2, r1d, r2d;
+};
+__device__ __forceinline__ FoldR fold_r(const E3& r) { return FoldR{r.c0, r.c1, r.c2, gl_add(r.c1, r.c1), gl_add(r.c2, r.c2)}; }
+__device__ __forceinline__ E3 fold_e3(const E3& x0, const E3& x1, const FoldR& R, bool ext2) {
+    const E3 d = e3_sub(x1, x0);
+    Acc192 s0{x0.c0, 0, 0}, s1{x0.c1, 0, 0}, s2{x0.c2, 0, 0};
+    acc_mac(s0, R.r0, d.c0);
+    acc_mac(s0, R.r2d, d.c1);
+    acc_mac(s0, R.r1d, d.c2);
+    acc_mac(s1, R.r1, d.c0);
+    acc_mac(s1, R.r0, d.c1);
+    acc_mac(s1, R.r2d, d.c2);
+    acc_mac(s2, R.r2, d.c0);
+    acc_mac(s2, R.r1, d.c1);
+    acc_mac(s2, R.r0, d.c2);
+    return ef_fix(E3{acc_reduce(s0), acc_reduce(s1), acc_reduce(s2)}, ext2);
+}
+
 // Loads a_i of the round vector, folding on the fly when requested.
-__device__ __forceinline__ E3 load_a(const ScKernelArgs& a, u64 i, const E3& r) {
+__device__ __forceinline__ E3 load_a(const ScKernelArgs& a, u64 i, const FoldR& r) {
     if (!a.fold) return a.a_base ? e3_base(a.a_base[i]) : ld3(a.a_in, i);
     if (a.a_base) {
         const u64 x0 = a.a_base[i], x1 = a.a_base[i + a.size];
-        return e3_add(e3_base(x0), e3_mul_base(r, gl_sub(x1, x0)));
+        return e3_add(e3_base(x0), e3_mul_base(E3{r.r0, r.r1, r.r2}, gl_sub(x1, x0)));
     }
-    const E3 x0 = ld3(a.a_in, i), x1 = ld3(a.a_in, i + a.size);
-    return e3_add(x0, ef_mul(r, e3_sub(x1, x0), a.ext2));
+    return fold_e3(ld3(a.a_in, i), ld3(a.a_in, i + a.size), r, a.ext2);
 }
-__device__ __forceinline__ E3 load_b(const ScKernelArgs& a, u64 i, const E3& r) {
+__device__ __forceinline__ E3 load_b(const ScKernelArgs& a, u64 i, const FoldR& r) {
     if (!a.fold) return ld3(a.b, i);
-    const E3 y0 = ld3(a.b, i), y1 = ld3(a.b, i + a.size);
-    return e3_add(y0, ef_mul(r, e3_sub(y1, y0), a.ext2));
+    return fold_e3(ld3(a.b, i), ld3(a.b, i + a.size), r, a.ext2);
 }
 
 // Unreduced sums of Ext3 products (X^3 = 2): the doubled cross terms are fed
@@ -168,6 +189,7 @@ __global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_s
     __shared__ E3 red[32];
     __shared__ bool is_last;
     const E3 r = FOLD ? a.sc->sc_r[a.fold_r] : e3_zero();
+    const FoldR R = fold_r(r);
     const u64 half = a.size >> 1;
     E3AccL c0{}, c2{};
     const u64 T = (u64)gridDim.x * blockDim.x;
@@ -194,11 +216,11 @@ __global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_s
                 al = e3_add(x0, e3_mul_base(r, gl_sub(x1.c0, x0.c0)));
                 ah = e3_add(x2, e3_mul_base(r, gl_sub(x3.c0, x2.c0)));
             } else {
-                al = e3_add(x0, ef_mul(r, e3_sub(x1, x0), a.ext2));
-                ah = e3_add(x2, ef_mul(r, e3_sub(x3, x2), a.ext2));
+                al = fold_e3(x0, x1, R, a.ext2);
+                ah = fold_e3(x2, x3, R, a.ext2);
             }
-            const E3 bl = e3_add(y0, ef_mul(r, e3_sub(y1, y0), a.ext2));
-            const E3 bh = e3_add(y2, ef_mul(r, e3_sub(y3, y2), a.ext2));
+            const E3 bl = fold_e3(y0, y1, R, a.ext2);
+            const E3 bh = fold_e3(y2, y3, R, a.ext2);
             st3(a.a_out, i, al); st3(a.b, i, bl);
             st3(a.a_out, i + half, ah); st3(a.b, i + half, bh);
             accl_mac(c0, al, bl);
@@ -266,7 +288,7 @@ __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs
         const u64 size = a.size >> t;
         const bool fold = t > 0;
         const bool base = a.a_base && t <= 1;
-        const E3 r = fold ? sc->sc_r[a.r_slot + t - 1] : e3_zero();
+        const FoldR r = fold_r(fold ? sc->sc_r[a.r_slot + t - 1] : e3_zero());
         ScKernelArgs k{};
         k.a_base = base ? a.a_base : nullptr;
         for (int c = 0; c < 3; ++c) { k.a_in[c] = a.a[c]; k.a_out[c] = a.a[c]; k.b[c] = a.b[c]; }
@@ -406,7 +428,7 @@ int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
 }
 
 __global__ void __launch_bounds__(SC_THREADS) k_fold(ScKernelArgs a) {
-    const E3 r = a.sc->sc_r[a.fold_r];
+    const FoldR r = fold_r(a.sc->sc_r[a.fold_r]);
     const u64 T = (u64)gridDim.x * blockDim.x;
     for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.size; i += T) {
         st3(a.a_out, i, load_a(a, i, r));
