@@ -193,7 +193,30 @@ __global__ void __launch_bounds__(SC_THREADS, FOLD ? SC_MINB_FOLD : SC_MINB) k_s
     const u64 half = a.size >> 1;
     E3AccL c0{}, c2{};
     const u64 T = (u64)gridDim.x * blockDim.x;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < half; i += T) {
+    u64 i0 = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (!FOLD) {
+        // Round 0 is memory-latency bound: two pairs per iteration, every load of
+        // both issued before their products.
+        for (; i0 + T < half; i0 += 2 * T) {
+            const u64 j = i0 + T;
+            if (BASE) {
+                const u64 al = a.a_base[i0], ah = a.a_base[i0 + half], al2 = a.a_base[j], ah2 = a.a_base[j + half];
+                const E3 bl = ld3(a.b, i0), bh = ld3(a.b, i0 + half), bl2 = ld3(a.b, j), bh2 = ld3(a.b, j + half);
+                accl_mac_base(c0, al, bl);
+                accl_mac_base(c2, gl_sub(ah, al), e3_sub(bh, bl));
+                accl_mac_base(c0, al2, bl2);
+                accl_mac_base(c2, gl_sub(ah2, al2), e3_sub(bh2, bl2));
+            } else {
+                const E3 al = ld3(a.a_in, i0), bl = ld3(a.b, i0), ah = ld3(a.a_in, i0 + half), bh = ld3(a.b, i0 + half);
+                const E3 al2 = ld3(a.a_in, j), bl2 = ld3(a.b, j), ah2 = ld3(a.a_in, j + half), bh2 = ld3(a.b, j + half);
+                accl_mac(c0, al, bl);
+                accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
+                accl_mac(c0, al2, bl2);
+                accl_mac(c2, e3_sub(ah2, al2), e3_sub(bh2, bl2));
+            }
+        }
+    }
+    for (u64 i = i0; i < half; i += T) {
         if (BASE && !FOLD) {
             const u64 al = a.a_base[i], ah = a.a_base[i + half];
             const E3 bl = ld3(a.b, i), bh = ld3(a.b, i + half);
