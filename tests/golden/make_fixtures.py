@@ -498,6 +498,8 @@ ZK_CASES = [  # zero-knowledge WHIR (ZkConfig<Goldilocks>), every PoW disabled a
     (12, 3, 2, 20, 103, ("mle", "covector"), 2, "blake3", (6, 6, 6, 6)),
     (16, 4, 1, 32, 104, ("mle",), 1, "blake3", None),
     (18, 4, 1, 40, 105, ("mle", "covector"), 1, "sha2", None),
+    # the limits: 8 polynomials (64 blinding vectors), 7 forms (8 in the blinding proof)
+    (7, 1, 1, 8, 106, ("mle", "covector", "mle", "covector", "mle", "mle", "covector"), 8, "blake3", (1, 1, 1, 1)),
 ]
 
 
