@@ -59,6 +59,8 @@ def test_multi_vector_prove_matches_reference_fixtures(gpu_ctx, case):
     (11, 6, 1, 4, 2, 1, False),    # 2048-byte rows from the folding factor
     (10, 3, 2, 4, 8, 1, True),     # eight witnesses, SHA-256
     (17, 4, 1, 2, 2, 3, False), (4, 4, 1, 5, 1, 1, False),  # no round: the final opening covers the batch
+    (9, 4, 1, 64, 1, 2, False),    # the 64-vector limit: 8192-byte rows, eight BLAKE3 chunks
+    (9, 4, 1, 8, 8, 1, True),      # 8 witnesses x 8 vectors, SHA-256
 ])
 def test_multi_vector_prove_matches_oracle(gpu_ctx, oracle, n, k, rho, batch, nwit, npts, sha2):
     nvec = batch * nwit
