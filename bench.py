@@ -196,11 +196,11 @@ def read_traffic(family, alg_bytes_per_proof):
 # ---------------------------------------------------------------------------
 # workload: requests and their inputs
 # ---------------------------------------------------------------------------
-def draw_requests(w, count, seed):
-    """(num_variables, log_inv_rate) pairs drawn from the seeded ChaCha20 stream."""
-    from whirplonk_b200 import sample_goldilocks
-
-    words = sample_goldilocks(seed, 2 * count)
+def draw_requests(w, count, seed, sampler):
+    """(num_variables, log_inv_rate) pairs drawn from the seeded ChaCha20 stream
+    (`sampler`: the library's whirgpu_sample_goldilocks on the GPU arm, its
+    numpy restatement on the reference arm; both give the same words)."""
+    words = sampler(seed, 2 * count)
     lo, hi = w["n"]
     out = []
     for i in range(count):
@@ -213,12 +213,24 @@ def draw_requests(w, count, seed):
     return out
 
 
-def make_inputs(n, seed):
+def make_inputs(n, seed, sampler):
+    coeffs = sampler(seed, 1 << n)
+    point = sampler(seed + 7919, 3 * n).reshape(1, n, 3)
+    return coeffs, point
+
+
+def coeff_seed(rank, n):
+    return 1000 * (rank + 1) + n
+
+
+def point_seed(rank, n, rho):
+    return 5000 * (rank + 1) + 31 * n + rho
+
+
+def gpu_sampler(seed, count):
     from whirplonk_b200 import sample_goldilocks
 
-    coeffs = sample_goldilocks(seed, 1 << n)
-    point = sample_goldilocks(seed + 7919, 3 * n).reshape(1, n, 3)
-    return coeffs, point
+    return sample_goldilocks(seed, count)
 
 
 def params_for(rho):
@@ -234,11 +246,11 @@ class Inputs:
     def __init__(self, ctx, shapes, rank, device):
         import torch
 
-        self.ctx = ctx
+        self.ctx, self.rank, self.device = ctx, rank, device
         self.host, self.pinned, self.dev, self.pts, self.evs = {}, {}, {}, {}, {}
         self._pinned_ptrs = []
         for n in sorted({n for n, _ in shapes}):
-            coeffs, _ = make_inputs(n, 1000 * (rank + 1) + n)
+            coeffs, _ = make_inputs(n, coeff_seed(rank, n), gpu_sampler)
             self.host[n] = coeffs
             self.dev[n] = torch.from_numpy(coeffs.view(np.int64)).to(device)
             ptr = ctx._L.whirgpu_host_alloc(coeffs.nbytes)
@@ -249,7 +261,29 @@ class Inputs:
             view[:] = coeffs
             self.pinned[n] = view
         for n, rho in sorted(set(shapes)):
-            _, point = make_inputs(n, 5000 * (rank + 1) + 31 * n + rho)
+            _, point = make_inputs(n, point_seed(rank, n, rho), gpu_sampler)
+            self.pts[(n, rho)] = point
+            self.evs[(n, rho)] = np.array(ctx.mle_evaluate(self.host[n], point), dtype=np.uint64).reshape(1, 3)
+        torch.cuda.synchronize()
+
+    def extend(self, shapes):
+        """Adds the inputs of shapes not seen yet (same seeds as the constructor)."""
+        import torch
+
+        ctx, rank = self.ctx, self.rank
+        for n in sorted({n for n, _ in shapes} - set(self.host)):
+            coeffs, _ = make_inputs(n, coeff_seed(rank, n), gpu_sampler)
+            self.host[n] = coeffs
+            self.dev[n] = torch.from_numpy(coeffs.view(np.int64)).to(self.device)
+            ptr = ctx._L.whirgpu_host_alloc(coeffs.nbytes)
+            if not ptr:
+                raise MemoryError("pinned allocation failed")
+            self._pinned_ptrs.append(ptr)
+            view = np.ctypeslib.as_array((ctypes.c_uint64 * coeffs.size).from_address(ptr))
+            view[:] = coeffs
+            self.pinned[n] = view
+        for n, rho in sorted(set(shapes) - set(self.pts)):
+            _, point = make_inputs(n, point_seed(rank, n, rho), gpu_sampler)
             self.pts[(n, rho)] = point
             self.evs[(n, rho)] = np.array(ctx.mle_evaluate(self.host[n], point), dtype=np.uint64).reshape(1, 3)
         torch.cuda.synchronize()
@@ -276,21 +310,53 @@ class Inputs:
 # reference CPU prover
 # ---------------------------------------------------------------------------
 def reference_proof_seconds(n, rho, coeffs, point, threads):
+    """Commit + prove of one request by the reference C++ prover, on its own clock."""
     from oracle.refio import run_reference
 
     r = run_reference(n, FOLD, rho, SEC, POW, point, coeffs, threads=threads)
     return (r.commit_ms + r.prove_ms) / 1000.0
 
 
-def workload_shapes(w, count_steps):
+def workload_shapes(w, count_steps, sampler):
     if w["kind"] in ("single", "zk"):
         return [(w["n"], w["rho"])] * count_steps
     if w["kind"] == "batch":
-        return draw_requests(w, w["count"], w["seed"])
-    return draw_requests(w, w["per_step"] * count_steps, w["seed"])
+        return draw_requests(w, w["count"], w["seed"], sampler)
+    return draw_requests(w, w["per_step"] * count_steps, w["seed"], sampler)
 
 
-def config_of(name, w, world):
+def reference_multiset(shapes, steps, threads, inputs_of):
+    """The reference prover's rate on the multiset `shapes`: every distinct
+    (num_variables, rate) shape is proved once (the distinct shapes are spread
+    over `steps` steps, largest first), and the rate is
+    len(shapes) / sum over shapes of count(shape) * time(shape).
+    inputs_of(n, rho) -> (coefficients, point) of the same request."""
+    from collections import Counter
+
+    counts = Counter(shapes)
+    distinct = sorted(counts, key=lambda s: (-s[0], -s[1]))
+    per_shape, step_s = {}, []
+    for i in range(steps):
+        t = 0.0
+        for n, rho in distinct[i::steps]:
+            coeffs, point = inputs_of(n, rho)
+            per_shape[(n, rho)] = reference_proof_seconds(n, rho, coeffs, point, threads)
+            t += per_shape[(n, rho)]
+        step_s.append(t)
+    weighted = sum(counts[s] * per_shape[s] for s in counts)
+    return {"value": len(shapes) / weighted, "distinct": len(distinct), "count": len(shapes),
+            "measured_s": sum(step_s), "step_s": step_s, "weighted_s": weighted,
+            "per_shape_s": {f"{n},{rho}": round(t, 4) for (n, rho), t in sorted(per_shape.items())}}
+
+
+def multiset_sample_text(m):
+    return (f"same multiset as the GPU arm: the {m['count']} requests of the timed steps, {m['distinct']} distinct "
+            f"(num_variables, rate) shapes, each proved once by the reference C++ prover (oracle/_ref, commit+prove "
+            f"on its own clock, {m['measured_s']:.1f} s); value = {m['count']} / sum of count(shape) x time(shape) "
+            f"= {m['count']} / {m['weighted_s']:.1f} s")
+
+
+def config_of(name, w):
     cfg = {"workload": name, "folding_factor": FOLD, "security_level": SEC, "pow_bits": POW, "hash": "BLAKE3",
            "field": "Goldilocks3", "statement": "1 MLE evaluation at a seeded Ext3 point"}
     if w["kind"] == "zk":
@@ -304,18 +370,15 @@ def config_of(name, w, world):
         cfg.update(num_variables=f"{w['dist']} on [{w['n'][0]}, {w['n'][1]}]", log_inv_rate=list(w["rho"]),
                    seed=w["seed"])
         cfg.update(requests_per_step=w["per_step"] if w["kind"] == "served" else w["count"])
-    cfg["parallelism"] = f"replicas x{world}" if world > 1 else "1 GPU"
     cfg["l2"] = "working set of a step (GBs of codewords and trees) far above the 126 MB L2; no flush"
     return cfg
 
 
-def zk_inputs(n):
+def zk_inputs(n, sampler):
     """Coefficients and a base-field MLE point (Ext3 layout, zero high parts)."""
-    from whirplonk_b200 import sample_goldilocks
-
-    coeffs = sample_goldilocks(1000 + n, 1 << n)
+    coeffs = sampler(1000 + n, 1 << n)
     point = np.zeros((n, 3), dtype=np.uint64)
-    point[:, 0] = sample_goldilocks(9000 + n, n)
+    point[:, 0] = sampler(9000 + n, n)
     return coeffs, point
 
 
@@ -326,7 +389,15 @@ def zk_reference(n, rho, coeffs, point, threads):
                             int.from_bytes(ZK_SEED[:8], "little"), no_pow=True, verify=False, threads=threads)
 
 
+WARMUP_SHAPE = (12, 1)  # the reference arm's warm-up proof: never a request of the timed stream
+WARMUP_SEED = 424242
+
+
 def run_reference_arm(args, rank, world):
+    """The reference C++ CPU prover on the GPU arm's workload.  Loads nothing
+    from whirplonk_b200: inputs come from the numpy restatement of the sampler
+    (oracle/chacha.py), which draws the same words."""
+    from oracle.chacha import sample_goldilocks as np_sampler
     from oracle.refio import ref_available
 
     if rank != 0:
@@ -338,29 +409,32 @@ def run_reference_arm(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built"}))
         return 0
     threads = os.cpu_count() or 1
-    warm = min(args.warmup, 1)
-    # one reference proof per step: the step-th request of the workload's stream
-    shapes = workload_shapes(w, warm + args.steps)
-    inputs = {}
-    times = []
-    for i in range(warm + args.steps):
-        n, rho = shapes[i % len(shapes)]
-        if n not in inputs:
-            inputs[n] = make_inputs(n, 1000 + n)[0]
-        _, point = make_inputs(n, 5000 + 31 * n + rho)
-        times.append(reference_proof_seconds(n, rho, inputs[n], point, threads))
-    timed = times[warm:]
-    total = sum(timed)
-    value = len(timed) / total
+    warm = max(args.warmup, 3)
+    wn, wr = WARMUP_SHAPE
+    wc, wp = make_inputs(wn, WARMUP_SEED, np_sampler)
+    for _ in range(warm):
+        reference_proof_seconds(wn, wr, wc, wp, threads)
+    shapes = workload_shapes(w, args.steps, np_sampler)
+    cache = {}
+
+    def inputs_of(n, rho):
+        if n not in cache:
+            cache.clear()  # shapes arrive largest n first: keep one coefficient vector
+            cache[n] = make_inputs(n, coeff_seed(0, n), np_sampler)[0]
+        return cache[n], make_inputs(n, point_seed(0, n, rho), np_sampler)[1]
+
+    m = reference_multiset(shapes, args.steps, threads, inputs_of)
+    value = m["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world,
-        "steps": args.steps, "warmup": warm, "ms_per_step": 1000.0 * total / len(timed), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": DATA,
-        "config": config_of(args.workload, w, world) | {"parallelism": "host OpenMP (reference C++ prover)"},
-        "p50_ms": 1000.0 * statistics.median(timed), "p99_ms": 1000.0 * max(timed),
+        "steps": args.steps, "warmup": warm, "ms_per_step": 1000.0 * m["measured_s"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": DATA,
+        "config": config_of(args.workload, w), "parallelism": f"host OpenMP, {threads} threads (reference C++ prover)",
+        "ms_per_step_note": "measured reference CPU time per step (the distinct shapes spread over the steps); "
+                            "value is the rate over the whole multiset, see cpu_baseline.sample",
+        "reference_seconds_per_shape": m["per_shape_s"],
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "reference",
-                         "sample": f"{len(timed)} proofs, one per step: the first requests of the workload's "
-                                   "seeded stream (commit+prove, prover clock)"},
+                         "sample": multiset_sample_text(m)},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -373,10 +447,12 @@ def run_reference_zk_arm(args, w, world):
     if not os.path.exists(REF_ZK_DRIVER):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_zk_driver not built"}))
         return 0
+    from oracle.chacha import sample_goldilocks as np_sampler
+
     threads = os.cpu_count() or 1
     n, rho = w["n"], w["rho"]
-    coeffs, point = zk_inputs(n)
-    warm = min(args.warmup, 1)
+    coeffs, point = zk_inputs(n, np_sampler)
+    warm = max(args.warmup, 3)
     times = [zk_reference(n, rho, coeffs, point, threads).prove_ms / 1000.0 for _ in range(warm + args.steps)]
     timed = times[warm:]
     total = sum(timed)
@@ -385,7 +461,7 @@ def run_reference_zk_arm(args, w, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "proofs/s", "n_gpus": world,
         "steps": args.steps, "warmup": warm, "ms_per_step": 1000.0 * total / len(timed), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": DATA,
-        "config": config_of(args.workload, w, world) | {"parallelism": "host OpenMP (reference C++ ZK prover)"},
+        "config": config_of(args.workload, w), "parallelism": f"host OpenMP, {threads} threads (reference C++ ZK prover)",
         "p50_ms": 1000.0 * statistics.median(timed), "p99_ms": 1000.0 * max(timed),
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": threads, "kind": "reference",
                          "sample": f"{len(timed)} zero-knowledge proofs (commit+prove, driver clock)"},
@@ -501,22 +577,17 @@ def family_roofline(ctx, inputs, shapes):
             {f: round(v / per, 4) for f, v in fam_ms.items()})
 
 
-def cpu_sample(shapes, inputs, budget_s=12.0):
-    """The reference prover on the first requests of the stream until ~budget_s of CPU time."""
+def cpu_sample(shapes, steps, inputs):
+    """The reference prover on the multiset of requests the GPU arm timed
+    (every distinct shape proved once; reference_multiset), on the same inputs."""
     from oracle.refio import ref_available
 
     if not ref_available():
         return None
     threads = os.cpu_count() or 1
-    total, count = 0.0, 0
-    for n, rho in shapes:
-        total += reference_proof_seconds(n, rho, inputs.host[n], inputs.pts[(n, rho)], threads)
-        count += 1
-        if total >= budget_s:
-            break
-    return {"value": count / total, "unit": "proofs/s", "cores": threads, "kind": "reference",
-            "sample": f"the first {count} requests of the workload's stream, proved by the reference C++ prover "
-                      f"(oracle/_ref) one after another, {total:.1f} s"}
+    m = reference_multiset(shapes, steps, threads, lambda n, rho: (inputs.host[n], inputs.pts[(n, rho)]))
+    return {"value": m["value"], "unit": "proofs/s", "cores": threads, "kind": "reference",
+            "sample": multiset_sample_text(m)}
 
 
 def pct(xs, q):
@@ -576,7 +647,7 @@ def run_single(args, H, ctx, w):
         "gpu_launches": launches, "roofline": roof, "families_ms_per_proof": fams, "clocks": clk,
     }
     if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample([(n, rho)], inputs, budget_s=0.0)
+        line["cpu_baseline"] = cpu_sample([(n, rho)] * args.steps, 1, inputs)
     inputs.close()
     return line
 
@@ -616,7 +687,7 @@ def run_zk(args, H, ctx, w):
     n, rho = w["n"], w["rho"]
     params = params_for(rho)
     cfg = ZkConfig.from_params(1 << n, params, 1).disable_pow()
-    coeffs, point = zk_inputs(n)
+    coeffs, point = zk_inputs(n, gpu_sampler)
     ev = ctx.mle_evaluate(coeffs, point)
     dev = torch.from_numpy(coeffs.view(np.int64)).to(H.device)
     ptr = ctx._L.whirgpu_host_alloc(coeffs.nbytes)
@@ -715,11 +786,33 @@ def run_zk(args, H, ctx, w):
     return line
 
 
+def batch_vs_plain(H, ctx, inputs, shapes, reps):
+    """The batch of `shapes` in one captured graph (device-resident inputs)
+    against the plain path on the same proofs, both with CUDA events around
+    the whole pass; every batched proof is checked against its plain twin."""
+    from whirplonk_b200.batch import Batch
+
+    stream = H.torch.cuda.ExternalStream(ctx.stream, device=H.device)
+    expected = [plain_prove(ctx, inputs, n, rho) for n, rho in shapes]
+    plain_ms, _ = H.timed(stream, lambda: [plain_prove(ctx, inputs, n, rho) for n, rho in shapes])
+    b = Batch(ctx, [inputs.request(n, rho, "device") for n, rho in shapes], Batch.GRAPH)
+    for _ in range(2):
+        b.run()
+    batch_ms, _ = H.timed(stream, lambda: [b.run() for _ in range(reps)])
+    same = all(b.proof(i) == expected[i] for i in range(len(shapes)))
+    b.close()
+    assert same, "a batched proof differs from the plain path's"
+    plain_rate = len(shapes) / (plain_ms / 1000.0)
+    batch_rate = reps * len(shapes) / (batch_ms / 1000.0)
+    return {"batched_proofs_per_s": batch_rate, "plain_proofs_per_s": plain_rate, "ratio": batch_rate / plain_rate,
+            "identical_to_plain": same, "proofs": len(shapes), "runs": reps}
+
+
 def run_batch(args, H, ctx, w):
     from whirplonk_b200.batch import Batch
 
     torch = H.torch
-    shapes = workload_shapes(w, 1)
+    shapes = workload_shapes(w, 1, gpu_sampler)
     inputs = Inputs(ctx, shapes, H.rank, H.device)
     stream = torch.cuda.ExternalStream(ctx.stream, device=H.device)
     # plain path: one proof at a time, device-resident inputs
@@ -777,7 +870,7 @@ def run_batch(args, H, ctx, w):
         "gpu_launches": launches, "roofline": roof, "families_ms_per_proof_plain": fams, "clocks": clk,
     }
     if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(shapes, inputs)
+        line["cpu_baseline"] = cpu_sample(shapes, args.steps, inputs)
     inputs.close()
     return line
 
@@ -800,7 +893,7 @@ def run_served(args, H, ctx, w):
     from whirplonk_b200.batch import Server
 
     torch = H.torch
-    shapes = workload_shapes(w, args.steps)
+    shapes = workload_shapes(w, args.steps, gpu_sampler)
     inputs = Inputs(ctx, shapes, H.rank, H.device)
     stream = torch.cuda.ExternalStream(ctx.stream, device=H.device)
     free, _ = torch.cuda.mem_get_info()
@@ -872,14 +965,36 @@ def run_served(args, H, ctx, w):
 
     # the plain path's 2^24 prove time (config 3 shape: n=24, rate 1/4)
     if (24, 2) not in inputs.pts:
-        _, point = make_inputs(24, 5000 * (H.rank + 1) + 31 * 24 + 2)
+        _, point = make_inputs(24, point_seed(H.rank, 24, 2), gpu_sampler)
         if 24 not in inputs.host:
-            inputs.host[24], _ = make_inputs(24, 1000 * (H.rank + 1) + 24)
+            inputs.host[24], _ = make_inputs(24, coeff_seed(H.rank, 24), gpu_sampler)
             inputs.dev[24] = torch.from_numpy(inputs.host[24].view(np.int64)).to(H.device)
         inputs.pts[(24, 2)] = point
         inputs.evs[(24, 2)] = np.array(ctx.mle_evaluate(inputs.host[24], point), dtype=np.uint64).reshape(1, 3)
     plain_prove(ctx, inputs, 24, 2)
     n24_ms, _ = H.timed(stream, lambda: [plain_prove(ctx, inputs, 24, 2) for _ in range(5)])
+
+    # served / plain by size class on the same stream: each class's requests
+    # served alone, against the plain path's time on those requests.
+    classes = {}
+    srv = Server(ctx, hbm_budget=budget, max_inflight=max_inflight)
+    for name, lo, hi in (("n12_18", 12, 18), ("n19_21", 19, 21), ("n22_24", 22, 24)):
+        idx = [i for i, (n, _) in enumerate(shapes) if lo <= n <= hi]
+        if not idx:
+            continue
+        sub = [dev_reqs[i] for i in idx]
+        serve(srv, sub)  # programs of this class captured, state as in the timed pass
+        ms, res = H.timed(stream, lambda: serve(srv, sub))
+        assert all(r.status == 0 and (r.narg, r.hints) == expected[i] for i, r in zip(idx, res))
+        p_ms = sum(plain_lat[i] for i in idx)
+        classes[name] = {"requests": len(idx), "served_proofs_per_s": len(idx) / (ms / 1000.0),
+                         "plain_proofs_per_s": len(idx) / (p_ms / 1000.0), "served_vs_plain": p_ms / ms,
+                         "plain_share_of_time": p_ms / sum(plain_lat)}
+    srv.close()
+    # the 64-proof batch (n uniform on {14..22}) in one graph launch, against the plain path
+    bshapes = workload_shapes(WORKLOADS["whir_batch64_n14_22"], 1, gpu_sampler)
+    inputs.extend(bshapes)
+    b64 = batch_vs_plain(H, ctx, inputs, bshapes, reps=3)
 
     roof, fams = family_roofline(ctx, inputs, shapes[: w["per_step"]])
     h2d = sum(inputs.coeff_bytes(n) + 96 + n * 24 + 24 for n, _ in shapes) / args.steps
@@ -892,6 +1007,8 @@ def run_served(args, H, ctx, w):
         "plain_proofs_per_s": H.sum_over_ranks(plain_rate), "served_vs_plain": served_rate / plain_rate,
         "plain_p50_ms_same_arrivals": pct(plain_tot, 0.5), "plain_p99_ms_same_arrivals": pct(plain_tot, 0.99),
         "plain_p50_ms_alone": pct(plain_lat, 0.5), "plain_p99_ms_alone": pct(plain_lat, 0.99),
+        "served_vs_plain_by_size": classes,
+        "batch64_vs_plain": b64["ratio"], "batch64": b64,
         "latency_sweep": sweep, "identical_to_plain": True, "prove_ms_n24_rate4": n24_ms / 5,
         "server": {"hbm_budget_bytes": budget, "max_inflight": max_inflight, "peak_inflight": st["peak_inflight"],
                    "peak_bytes": st["peak_bytes"]},
@@ -900,7 +1017,7 @@ def run_served(args, H, ctx, w):
         "gpu_launches": launches, "roofline": roof, "families_ms_per_proof_plain": fams, "clocks": clk,
     }
     if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(shapes, inputs)
+        line["cpu_baseline"] = cpu_sample(shapes, args.steps, inputs)
     inputs.close()
     return line
 
@@ -915,7 +1032,8 @@ def run_gpu_arm(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": body.pop("value"), "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": body.pop("ms_per_step"), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": DATA,
-            "config": config_of(args.workload, w, world)}
+            "config": config_of(args.workload, w),
+            "parallelism": f"replicas x{world} (one independent request stream per GPU)" if world > 1 else "1 GPU"}
     line.update(body)
     ctx.close()
     if rank == 0:

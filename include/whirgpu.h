@@ -374,10 +374,14 @@ whirgpu_status whirgpu_mle_evaluate(whirgpu_ctx* ctx, const uint64_t* coeffs, ui
  * returns without waiting.  Working memory is a fixed file-scope device array
  * of under 0.5 MiB, held on every GPU that loads the library until the process
  * exits; num_variables above WHIRGPU_NOALLOC_MLE_MAX_VARS is rejected with
- * WHIRGPU_E_TOO_LARGE.  The first call on each device looks the array up
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All
- * calls on a device share the array: calls whose kernels overlap on the GPU
- * race and give wrong results, so order them on one stream. */
+ * WHIRGPU_E_TOO_LARGE.  Every call looks the array's device address up
+ * (cudaGetSymbolAddress, which allocates nothing); the first lookup on a device
+ * may load the library's module there, so make the first call on each device
+ * before any stream capture.  A CUDA error already pending on the calling
+ * thread is left for its owner: the call then returns WHIRGPU_E_CUDA and
+ * queues nothing.  All calls on a device share the array: calls whose kernels
+ * overlap on the GPU race and give wrong results, so order them on one
+ * stream. */
 #define WHIRGPU_NOALLOC_MLE_MAX_VARS 24
 whirgpu_status whirgpu_mle_evaluate_noalloc(const uint64_t* d_coeffs, uint64_t num_variables, const uint64_t* d_point,
                                             uint64_t* d_out, void* stream);

@@ -36,7 +36,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-DUMPS = "/root/reference/cpp/dump_output"
+DUMPS = os.path.join(os.environ.get("WHIR_REFERENCE_CPP", "/root/reference/cpp"), "dump_output")
 
 MASK = (1 << 64) - 1
 

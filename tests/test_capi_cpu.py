@@ -72,6 +72,25 @@ def test_chacha20_block_rfc8439():
         assert out.raw == enc.update(bytes(64))
 
 
+def test_numpy_sampler_matches_library():
+    """oracle/chacha.py (the benchmark's reference-arm sampler, no GPU library)
+    draws the same words as whirgpu_sample_goldilocks, and its block function
+    gives the RFC 8439 section 2.3.2 test vector."""
+    import struct
+
+    from oracle.chacha import chacha20_blocks
+    from oracle.chacha import sample_goldilocks as np_sample
+
+    for seed, count in [(1, 1), (11, 100), (1024, 1 << 16), (12345678901234567, 3000), (2**64 - 1, 77)]:
+        assert (np_sample(seed, count) == sample_goldilocks(seed, count)).all(), (seed, count)
+    key = struct.unpack("<8I", bytes(range(32)))
+    nonce = struct.unpack("<3I", bytes.fromhex("000000090000004a00000000"))
+    blk = chacha20_blocks(key, 1, 1, nonce)[0].tobytes()
+    assert blk.hex() == (
+        "10f1e7e4d13b5915500fdd1fa32071c4c7d1f4c733c068030422aa9ac3d46c4e"
+        "d2826446079faa0914c2d705d98b02a2b5129cd1de164eb9cbd083e8a2503c4e")
+
+
 def test_sampler_is_seeded_uniform_and_canonical():
     a = sample_goldilocks(123, 1 << 14)
     b = sample_goldilocks(123, 1 << 14)

@@ -25,8 +25,8 @@ def _rank(rank, world, port, q):
     H = bench.Harness(rank, world, rank, backend="gloo")
     elapsed = H.max_over_ranks(10.0 * (rank + 1))   # the slowest rank's time
     rate = H.sum_over_ranks(100.0 + rank)          # whole-job throughput
-    coeffs, point = bench.make_inputs(10, 1000 * (rank + 1) + 10)
-    shapes = bench.workload_shapes(bench.WORKLOADS["whir_served_mixed_n12_24"], 2)
+    coeffs, point = bench.make_inputs(10, bench.coeff_seed(rank, 10), bench.gpu_sampler)
+    shapes = bench.workload_shapes(bench.WORKLOADS["whir_served_mixed_n12_24"], 2, bench.gpu_sampler)
     H.barrier()
     H.close()
     q.put((rank, elapsed, rate, int(coeffs[0]), int(point[0, 0, 0]), shapes[:4]))

@@ -376,7 +376,8 @@ int launch_merkle_batch(u32* nodes, u32 logN, u32 count, u64 node_stride, cudaSt
 // sums and sends the values as prover messages, point-major, every evaluated
 // vector at each point.
 // ---------------------------------------------------------------------------
-constexpr int OOD_GRID = 592, OOD_THREADS = 256;
+// OOD_GRID: capacity of the per-CTA partials (the grid is 4 CTAs per SM, at most this).
+constexpr int OOD_GRID = 1024, OOD_THREADS = 256;
 constexpr u32 OOD_LO = 10;
 constexpr int OOD_MAX_VALUES = MAX_OOD * MAX_VECTORS;
 
@@ -519,7 +520,7 @@ int launch_ood(const OodArgs& a, cudaStream_t st) {
     E3* partials = reinterpret_cast<E3*>(base + 256);
     E3* tab = partials + (size_t)OOD_GRID * a.scratch_values;
     const u64 entries = (u64)((1u << OOD_LO) + hc) * a.n_ood;
-    k_ood_tables<<<(unsigned)std::min<u64>(296, (entries + 255) / 256), 256, 0, st>>>(a.pts, a.n_ood, hc, tab, a.ext2 != 0);
+    k_ood_tables<<<(unsigned)std::min<u64>(2ull * device_sms(), (entries + 255) / 256), 256, 0, st>>>(a.pts, a.n_ood, hc, tab, a.ext2 != 0);
     count_launches(1);
     const u64 warps_per_cta = OOD_THREADS / 32;
     const u64 items = (u64)a.n_ood * a.nvec * hc;
@@ -527,7 +528,8 @@ int launch_ood(const OodArgs& a, cudaStream_t st) {
     // partials fit: items <= OOD_GRID * scratch_values when hc <= OOD_GRID).
     const bool by_items = hc <= OOD_GRID && items > hc;
     u64 want = ((by_items ? items : hc) + warps_per_cta - 1) / warps_per_cta;
-    unsigned grid = (unsigned)(want < 1 ? 1 : (want > OOD_GRID ? OOD_GRID : want));
+    const u64 cap = std::min<u64>(4ull * device_sms(), (u64)OOD_GRID);
+    unsigned grid = (unsigned)(want < 1 ? 1 : (want > cap ? cap : want));
     if (by_items) k_ood<true><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
     else k_ood<false><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
     count_launches(1);

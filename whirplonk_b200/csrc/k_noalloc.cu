@@ -17,8 +17,6 @@
 // ordering between them) race on the array and give wrong results.
 #include <cuda_runtime.h>
 
-#include <mutex>
-
 #include "../../include/whirgpu.h"
 #include "launch.h"
 
@@ -30,25 +28,17 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = 448u * 1024u;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 namespace {
-constexpr int MAX_DEVICES = 64;
-std::mutex g_mu;
-void* g_scratch_addr[MAX_DEVICES] = {};
-
-// Device address of g_noalloc_scratch on the current device, resolved once per
-// device (the host-side symbol is only a stand-in and must not reach a kernel).
+// Device address of g_noalloc_scratch on the current device.  The host-side
+// symbol is only a stand-in and must never reach a kernel.  The address is
+// looked up on every call (the lookup allocates nothing), so it stays right
+// after a cudaDeviceReset reloads the module.  The first lookup on a device
+// may load the library's module there, which is why the first call on a device
+// must come before any stream capture.
 cudaError_t scratch_for_current_device(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= MAX_DEVICES) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = p;
-    }
-    *out = g_scratch_addr[dev];
+    *out = p;
     return cudaSuccess;
 }
 }  // namespace
@@ -61,9 +51,19 @@ extern "C" whirgpu_status whirgpu_mle_evaluate_noalloc(const uint64_t* d_coeffs,
     if (!d_coeffs || !d_point || !d_out) return WHIRGPU_E_INVALID;
     if (num_variables > WHIRGPU_NOALLOC_MLE_MAX_VARS) return WHIRGPU_E_TOO_LARGE;
     if (mle_eval_scratch_bytes((u32)num_variables) > NOALLOC_SCRATCH_BYTES) return WHIRGPU_E_TOO_LARGE;
+    // A launch error still pending on this thread belongs to the caller's
+    // earlier work: leave it for its owner (cudaGetLastError would clear it)
+    // and queue nothing.  With none pending, any error seen below is ours.
+    if (cudaPeekAtLastError() != cudaSuccess) return WHIRGPU_E_CUDA;
     void* scratch = nullptr;
-    if (scratch_for_current_device(&scratch) != cudaSuccess) return WHIRGPU_E_CUDA;
+    if (scratch_for_current_device(&scratch) != cudaSuccess) {
+        cudaGetLastError();  // clear this call's own lookup error
+        return WHIRGPU_E_CUDA;
+    }
     const cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    launch_mle_eval(d_coeffs, (u32)num_variables, d_point, scratch, d_out, st);
-    return cudaGetLastError() == cudaSuccess ? WHIRGPU_OK : WHIRGPU_E_CUDA;
+    if (launch_mle_eval(d_coeffs, (u32)num_variables, d_point, scratch, d_out, st) != 0) {
+        cudaGetLastError();  // clear this call's own memset or launch error
+        return WHIRGPU_E_CUDA;
+    }
+    return WHIRGPU_OK;
 }

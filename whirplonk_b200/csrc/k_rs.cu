@@ -182,12 +182,12 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
     u64* out = tmp + planes * N;
     u64* src = out + planes * N;
     unsigned long long* dig = reinterpret_cast<unsigned long long*>(src + planes * m);
-    k_fill_canonical<<<592, 256, 0, c->stream>>>(src, planes * m, 0x5EED0000ull + log_n);
+    k_fill_canonical<<<4 * device_sms(), 256, 0, c->stream>>>(src, planes * m, 0x5EED0000ull + log_n);
     const LdeArgs L = lde_args(c, src, m, planes, log_n, tmp, out);
 
     auto digest = [&](unsigned long long* h) -> bool {
         cudaMemsetAsync(dig, 0, 8, c->stream);
-        k_digest<<<592, 256, 0, c->stream>>>(out, planes * N, dig);
+        k_digest<<<4 * device_sms(), 256, 0, c->stream>>>(out, planes * N, dig);
         return cudaMemcpyAsync(h, dig, 8, cudaMemcpyDeviceToHost, c->stream) == cudaSuccess &&
                cudaStreamSynchronize(c->stream) == cudaSuccess;
     };

@@ -12,13 +12,17 @@
 // Covector (whir_prover.hpp:150-197, linear_form.hpp:186-206,
 // multilinear.hpp:121-133): cov[i] = sum_f crlc_f eq(p_f, i) + sum_j crlc_j z_j^i,
 // later cov[i] += sum_j stir_rlc_j z_j^i per round (utilities.hpp:261-307).
+#include <algorithm>
+#include <mutex>
+
 #include "launch.h"
 #include "state.cuh"
 #include "wtx.cuh"
 
 namespace wg {
 
-constexpr int SC_THREADS = 256, SC_GRID = 148 * 4;
+// SC_GRID: capacity of the per-CTA partials array (the grid never exceeds it).
+constexpr int SC_THREADS = 256, SC_GRID = 1024;
 // CTAs per SM the round kernel's registers are sized for.
 #ifndef SC_MINB
 #define SC_MINB 3
@@ -407,23 +411,36 @@ size_t sumcheck_scratch_bytes() { return (size_t)SC_GRID * 2 * sizeof(E3) + 256;
 
 int launch_pow_grind_only(ProofScalars* sc, u64 threshold, int hash, cudaStream_t st);  // k_tx.cu
 
-// Resident CTAs of k_sumcheck_round<fold, base> (index 2 fold + base); a grid
-// of at most this many runs in one wave (the grid-stride loop does the rest).
-static unsigned g_sc_resident[4] = {SC_GRID, SC_GRID, SC_GRID, SC_GRID};
+constexpr int MAX_DEVICES = 64;
+static u32 g_sms[MAX_DEVICES];  // 0 = not looked up yet
+static std::mutex g_sms_mu;
+
+u32 device_sms() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 148;
+    std::lock_guard<std::mutex> lk(g_sms_mu);
+    if (!g_sms[dev]) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) return 148;
+        g_sms[dev] = (u32)sms;
+    }
+    return g_sms[dev];
+}
+
+// Resident CTAs per SM of k_sumcheck_round<fold, base> (index 2 fold + base);
+// a grid of at most SMs x this many runs in one wave (the grid-stride loop
+// does the rest).  Occupancy depends on the kernel and the architecture only.
+static int g_sc_occ[4] = {1, 1, 1, 1};
 
 int sumcheck_prepare() {
-    int dev = 0, sms = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-        return -1;
     const void* fns[4] = {(const void*)k_sumcheck_round<false, false>, (const void*)k_sumcheck_round<false, true>,
                           (const void*)k_sumcheck_round<true, false>, (const void*)k_sumcheck_round<true, true>};
     for (int k = 0; k < 4; ++k) {
         int occ = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fns[k], SC_THREADS, 0) != cudaSuccess) return -1;
-        const long r = (long)sms * (occ < 1 ? 1 : occ);
-        g_sc_resident[k] = (unsigned)(r > SC_GRID ? SC_GRID : r);
+        g_sc_occ[k] = occ < 1 ? 1 : occ;
     }
-    return 0;
+    return device_sms() ? 0 : -1;
 }
 
 int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
@@ -431,7 +448,8 @@ int launch_sumcheck_round(const SumcheckArgs& s, cudaStream_t st) {
     ScKernelArgs a = make_sc(s);
     const u64 half = s.size >> 1;
     const bool base = a.a_base != nullptr;
-    const u64 cap = g_sc_resident[(a.fold ? 2 : 0) + (base ? 1 : 0)];
+    const u64 resident = (u64)device_sms() * (u64)g_sc_occ[(a.fold ? 2 : 0) + (base ? 1 : 0)];
+    const u64 cap = resident > (u64)SC_GRID ? (u64)SC_GRID : resident;
     u64 want = (half + SC_THREADS - 1) / SC_THREADS;
     const unsigned grid = (unsigned)(want > cap ? cap : (want < 1 ? 1 : want));
     if (a.fold) {
@@ -463,7 +481,8 @@ int launch_fold(const SumcheckArgs& s, cudaStream_t st) {
     ScKernelArgs a = make_sc(s);
     a.fold = 1;
     u64 want = (s.size + SC_THREADS - 1) / SC_THREADS;
-    const unsigned grid = (unsigned)(want > SC_GRID ? SC_GRID : (want < 1 ? 1 : want));
+    const u64 cap = std::min<u64>((u64)device_sms() * 4, (u64)SC_GRID);
+    const unsigned grid = (unsigned)(want > cap ? cap : (want < 1 ? 1 : want));
     k_fold<<<grid, SC_THREADS, 0, st>>>(a);
     count_launches(1);
     return 0;
@@ -575,11 +594,12 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
     for (int f = 0; f < a.n_forms; ++f)
         if (((a.dense_mask >> f) & 1) && !a.dense[f]) return -1;
     if (nterms > 0) {
-        k_cov_tables<<<148, 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.dense_mask, a.sc, tab, a.ext2 != 0, a.tx);
+        k_cov_tables<<<device_sms(), 256, 0, st>>>(a.points, a.logS, a.n_forms, a.n_ood, a.dense_mask, a.sc, tab, a.ext2 != 0, a.tx);
         count_launches(1);
     }
     u64 want = (S + 255) / 256;
-    k_cov_init<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab);
+    const u64 cap = (u64)device_sms() * 16;
+    k_cov_init<<<(unsigned)(want > cap ? cap : want), 256, 0, st>>>(a, tab);
     count_launches(1);
     return 0;
 }
@@ -646,10 +666,11 @@ int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
     E3* tab = reinterpret_cast<E3*>(a.scratch);
     const size_t tab_bytes = ((size_t)(1u << CA_LO) + hc) * (size_t)npts * sizeof(E3);
     u64* lo_base = reinterpret_cast<u64*>(reinterpret_cast<char*>(a.scratch) + (tab_bytes + 255) / 256 * 256);
-    k_cov_acc_tables<<<296, 256, 0, st>>>(a.sc, a.n_ext, npts, hc, tab, lo_base, a.ext2 != 0);
+    k_cov_acc_tables<<<2 * device_sms(), 256, 0, st>>>(a.sc, a.n_ext, npts, hc, tab, lo_base, a.ext2 != 0);
     count_launches(1);
     u64 want = (a.size + 255) / 256;
-    k_cov_accumulate<<<(unsigned)(want > 148 * 16 ? 148 * 16 : want), 256, 0, st>>>(a, tab, lo_base, hc);
+    const u64 cap = (u64)device_sms() * 16;
+    k_cov_accumulate<<<(unsigned)(want > cap ? cap : want), 256, 0, st>>>(a, tab, lo_base, hc);
     count_launches(1);
     return 0;
 }
@@ -692,24 +713,32 @@ __global__ void __launch_bounds__(256) k_mle_dot(const u64* v, u32 logS, const E
     }
 }
 
-size_t mle_eval_scratch_bytes(u32 logS) { return 256 + 592 * sizeof(E3) + cov_init_scratch_bytes(logS, 1, 0); }
+// Capacity of the per-CTA partials of k_mle_dot in the scratch layout below.
+constexpr u32 MLE_MAX_CTAS = 592;
+
+size_t mle_eval_scratch_bytes(u32 logS) { return 256 + MLE_MAX_CTAS * sizeof(E3) + cov_init_scratch_bytes(logS, 1, 0); }
 
 int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch, u64* out, cudaStream_t st) {
     // [ticket counter | per-CTA partials | eq tables]: the counter keeps a
     // fixed offset whatever logS, and is cleared before every launch.
+    // Returns 0, or the CUDA error of the memset or of a launch (the caller
+    // makes sure no error was pending before, so a launch error is this call's).
     char* base = reinterpret_cast<char*>(scratch);
     unsigned* counter = reinterpret_cast<unsigned*>(base);
     E3* partials = reinterpret_cast<E3*>(base + 256);
-    E3* tab = reinterpret_cast<E3*>(base + 256 + 592 * sizeof(E3));
-    cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
-    k_cov_tables<<<148, 256, 0, st>>>(point, logS, 1, 0, 0u, nullptr, tab, false, nullptr);
+    E3* tab = reinterpret_cast<E3*>(base + 256 + MLE_MAX_CTAS * sizeof(E3));
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
+    if (e != cudaSuccess) return (int)e;
+    k_cov_tables<<<device_sms(), 256, 0, st>>>(point, logS, 1, 0, 0u, nullptr, tab, false, nullptr);
     count_launches(1);
+    if ((e = cudaPeekAtLastError()) != cudaSuccess) return (int)e;
     const u64 S = 1ull << logS;
     u64 want = (S + 255) / 256;
-    const unsigned grid = (unsigned)(want > 592 ? 592 : want);
+    const u64 cap = std::min<u64>((u64)device_sms() * 4, MLE_MAX_CTAS);
+    const unsigned grid = (unsigned)(want > cap ? cap : want);
     k_mle_dot<<<grid, 256, 0, st>>>(coeffs, logS, tab, partials, counter, out);
     count_launches(1);
-    return 0;
+    return (int)cudaPeekAtLastError();
 }
 
 }  // namespace wg

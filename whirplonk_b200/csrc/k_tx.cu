@@ -91,7 +91,7 @@ int launch_constraint_rlc(TxState* tx, ProofScalars* sc, int n_forms, int nwit, 
 // out sets TX_ERR_POW_EXHAUSTED.
 // ---------------------------------------------------------------------------
 constexpr u64 POW_NONCE_LIMIT = 1ull << 36;
-constexpr unsigned POW_THREADS = 256, POW_GRID = 148 * 2, POW_CHUNK = 2 * POW_THREADS;
+constexpr unsigned POW_THREADS = 256, POW_CTAS_PER_SM = 2, POW_CHUNK = 2 * POW_THREADS;
 
 // One warp.  Also resets the search state.
 __global__ void k_pow_challenge(TxState* tx, ProofScalars* sc) {
@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(POW_THREADS) k_pow_search(ProofScalars* sc, u6
 int launch_pow_grind_only(ProofScalars* sc, u64 threshold, int hash, cudaStream_t st) {
     const double expect = threshold == 0 ? 1.8446744073709552e19 : 18446744073709551616.0 / (double)threshold;
     const u64 limit = expect * 64.0 >= (double)POW_NONCE_LIMIT ? POW_NONCE_LIMIT : (u64)(expect * 64.0) + 1;
-    if (hash == 1) k_pow_search<1><<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, limit);
-    else k_pow_search<0><<<POW_GRID, POW_THREADS, 0, st>>>(sc, threshold, limit);
+    if (hash == 1) k_pow_search<1><<<POW_CTAS_PER_SM * device_sms(), POW_THREADS, 0, st>>>(sc, threshold, limit);
+    else k_pow_search<0><<<POW_CTAS_PER_SM * device_sms(), POW_THREADS, 0, st>>>(sc, threshold, limit);
     count_launches(1);
     return 0;
 }

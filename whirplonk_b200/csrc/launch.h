@@ -225,6 +225,10 @@ namespace wg {
 int launch_mle_eval(const u64* coeffs, u32 logS, const u64* point, void* scratch, u64* out, cudaStream_t st);
 size_t mle_eval_scratch_bytes(u32 logS);
 
+// Streaming multiprocessors of the current device (cudaDevAttrMultiProcessorCount,
+// looked up once per device); grid-stride kernels size their grids from it.
+u32 device_sms();
+
 // Process-wide count of kernel launches issued by the launchers.
 void count_launches(u64 k);
 u64 launch_count();

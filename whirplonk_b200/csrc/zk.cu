@@ -392,7 +392,7 @@ __global__ void k_zk_combine(const ZkScalars* zs, const u64* claims, u32 npolys,
 }
 
 u32 grid_for(u64 work, u32 threads) {
-    return (u32)std::max<u64>(1, std::min<u64>((work + threads - 1) / threads, 148ull * 16));
+    return (u32)std::max<u64>(1, std::min<u64>((work + threads - 1) / threads, (u64)device_sms() * 16));
 }
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -554,7 +554,7 @@ whirgpu_status whirgpu_zk_commit(whirgpu_ctx* c, const whirgpu_zk_config* cfg, c
     w->G = (u32)(init.in_domain * init.depth);
     const u64 half = 1ull << ell, P = half << 1, mu = n;
     const u32 bx = (u32)((half + 255) / 256);
-    w->parts = std::max<u32>(1, std::min<u32>(w->G, 592 / bx));
+    w->parts = std::max<u32>(1, std::min<u32>(w->G, 4 * device_sms() / bx));
     w->chunk = (w->G + w->parts - 1) / w->parts;
     w->parts = (w->G + w->chunk - 1) / w->chunk;
     const u64 V = npolys * (mu + 1);
