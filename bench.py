@@ -169,6 +169,38 @@ def algorithmic_bytes(schedule, n, k):
     return {"ntt": lde, "leaf_hash": leaf, "merkle": merkle, "sumcheck": sumcheck}
 
 
+def algorithmic_units(schedule, n, k):
+    """Per-proof operation counts of the integer-bound families: radix-2
+    butterflies of the LDEs ((N/2) log2(m) per plane, the zero padding skipped),
+    BLAKE3 compressions of the leaves (N ceil(row bytes / 64)) and of the Merkle
+    trees (N - 1)."""
+    nr = schedule[0]
+    d = 1 << k
+    commits = [(1 << n, schedule[1], 1)]
+    for r in range(nr):
+        commits.append((schedule[6 + 6 * r], schedule[7 + 6 * r], 3))
+    bfly = leaf = merkle = 0
+    for v, N, c in commits:
+        m = max(v // d, 1)
+        bfly += c * d * (N // 2) * int(math.log2(m))
+        leaf += N * -(-(8 * c * d) // 64)
+        merkle += N - 1
+    return {"ntt": bfly, "leaf_hash": leaf, "merkle": merkle}
+
+
+def measure_int_peaks(device):
+    """whirgpu_measure_int_peaks: register-only rates of this GPU's integer pipes."""
+    from whirplonk_b200 import _lib
+
+    L = _lib.load()
+    out = (ctypes.c_double * 8)()
+    if L.whirgpu_measure_int_peaks(device, out) != 0:
+        return None
+    names = ["butterflies_per_s", "blake3_compressions_per_s", "mac64_per_s", "mad_lo_u32_per_s",
+             "mad_wide_u32_per_s", "add3_u32_per_s", "lop3_per_s", "shf_per_s"]
+    return dict(zip(names, list(out)))
+
+
 def read_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -565,16 +597,40 @@ def family_roofline(ctx, inputs, shapes):
     fam = ctx.kernel_stats(reset=True)
     ctx.set_timing(False)
     fam_ms = {f: v[1] for f, v in fam.items()}
+    units = {}
+    for n, rho in shapes:
+        sched = Config.from_params(1 << n, params_for(rho)).schedule
+        for f, v in algorithmic_units(sched, n, FOLD).items():
+            units[f] = units.get(f, 0) + v
     dominant = max(alg.keys(), key=lambda f: fam_ms.get(f, 0.0))
     peak, peak_kind = read_peaks()
     achieved = alg[dominant] / (fam_ms[dominant] / 1000.0) / 1e9
     per = len(shapes)
-    return ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-             "traffic": read_traffic(dominant, alg[dominant] / per), "kernel": dominant, "peak_source": peak_kind,
-             "algorithmic_bytes_per_proof": alg[dominant] / per, "ms_per_proof": fam_ms[dominant] / per,
-             "traffic_unit": "DRAM bytes per proof of the family",
-             "binding_limit": ALU_BOUND.get(dominant, "HBM")},
-            {f: round(v / per, 4) for f, v in fam_ms.items()})
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": read_traffic(dominant, alg[dominant] / per), "kernel": dominant, "peak_source": peak_kind,
+            "algorithmic_bytes_per_proof": alg[dominant] / per, "ms_per_proof": fam_ms[dominant] / per,
+            "traffic_unit": "DRAM bytes per proof of the family",
+            "binding_limit": ALU_BOUND.get(dominant, "HBM")}
+    sc_ms = fam_ms.get("sumcheck", 0.0) + fam_ms.get("covector", 0.0)
+    sc_ach = alg["sumcheck"] / (sc_ms / 1000.0) / 1e9 if sc_ms > 0 else None
+    roof_sc = {"bound": "hbm", "kernel": "sumcheck + covector", "achieved": sc_ach, "peak": peak, "unit": "GB/s",
+               "frac": sc_ach / peak if sc_ach else None, "peak_source": peak_kind,
+               "algorithmic_bytes_per_proof": alg["sumcheck"] / per, "ms_per_proof": sc_ms / per,
+               "bytes_note": "per round on size s: (8 or 24) s + 24 s read, 2 x 24 s/2 written (a and the covector)"}
+    extra = {"roofline_sumcheck": roof_sc}
+    pk = measure_int_peaks(ctx.device)
+    if pk:
+        ri = {}
+        for f, unit, pkey in (("ntt", "butterflies/s", "butterflies_per_s"),
+                              ("leaf_hash", "BLAKE3 compressions/s", "blake3_compressions_per_s"),
+                              ("merkle", "BLAKE3 compressions/s", "blake3_compressions_per_s")):
+            if fam_ms.get(f, 0.0) > 0:
+                a = units[f] / (fam_ms[f] / 1000.0)
+                ri[f] = {"achieved": a, "peak": pk[pkey], "unit": unit, "frac": a / pk[pkey],
+                         "units_per_proof": units[f] / per, "ms_per_proof": fam_ms[f] / per}
+        extra["roofline_int"] = ri
+        extra["int_peaks_measured"] = pk
+    return roof, {f: round(v / per, 4) for f, v in fam_ms.items()}, extra
 
 
 def cpu_sample(shapes, steps, inputs):
@@ -637,7 +693,7 @@ def run_single(args, H, ctx, w):
     h2d, d2h = ctx.last_io_bytes()
     clk = clocks.stop()
     assert out == ref_proof
-    roof, fams = family_roofline(ctx, inputs, [(n, rho)] * args.steps)
+    roof, fams, extra = family_roofline(ctx, inputs, [(n, rho)] * args.steps)
     total = args.steps * H.world
     line = {
         "value": total / (elapsed / 1000.0), "ms_per_step": elapsed / args.steps,
@@ -646,6 +702,7 @@ def run_single(args, H, ctx, w):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches, "roofline": roof, "families_ms_per_proof": fams, "clocks": clk,
     }
+    line.update(extra)
     if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample([(n, rho)] * args.steps, 1, inputs)
     inputs.close()
@@ -856,7 +913,7 @@ def run_batch(args, H, ctx, w):
     d2h = sum(len(a) + len(b) for a, b in expected)
     dev_batch.close()
     host_batch.close()
-    roof, fams = family_roofline(ctx, inputs, shapes)
+    roof, fams, extra = family_roofline(ctx, inputs, shapes)
     count = len(shapes)
     total = count * args.steps * H.world
     plain_rate = H.sum_over_ranks(count / (plain_ms / 1000.0))
@@ -869,6 +926,7 @@ def run_batch(args, H, ctx, w):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches, "roofline": roof, "families_ms_per_proof_plain": fams, "clocks": clk,
     }
+    line.update(extra)
     if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(shapes, args.steps, inputs)
     inputs.close()
@@ -996,7 +1054,7 @@ def run_served(args, H, ctx, w):
     inputs.extend(bshapes)
     b64 = batch_vs_plain(H, ctx, inputs, bshapes, reps=3)
 
-    roof, fams = family_roofline(ctx, inputs, shapes[: w["per_step"]])
+    roof, fams, extra = family_roofline(ctx, inputs, shapes[: w["per_step"]])
     h2d = sum(inputs.coeff_bytes(n) + 96 + n * 24 + 24 for n, _ in shapes) / args.steps
     d2h = sum(len(a) + len(b) for a, b in expected) / args.steps
     total_value = H.sum_over_ranks(served_rate)
@@ -1016,6 +1074,7 @@ def run_served(args, H, ctx, w):
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches, "roofline": roof, "families_ms_per_proof_plain": fams, "clocks": clk,
     }
+    line.update(extra)
     if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_sample(shapes, args.steps, inputs)
     inputs.close()

@@ -399,6 +399,17 @@ void whirgpu_chacha20_block(const uint8_t key[32], uint32_t counter, const uint8
 void* whirgpu_host_alloc(size_t bytes);
 void whirgpu_host_free(void* p);
 
+/* Integer-pipe peaks of `device`, measured (no reference counterpart): the
+ * roofline denominators of the families bound by integer arithmetic.  Each
+ * rate is operations per second of a register-only kernel over a full grid:
+ * out[0] Goldilocks radix-2 butterflies (one multiply, add, subtract),
+ * out[1] BLAKE3 compressions, out[2] 64x64-bit products accumulated into
+ * 192 bits, then PTX instruction rates: out[3] mad.lo.u32, out[4]
+ * mad.wide.u32, out[5] add.u32 (counted once per two-add pair a + b + c),
+ * out[6] lop3.b32, out[7] shf.l.wrap.b32.  Takes well under a second. */
+#define WHIRGPU_NUM_INT_PEAKS 8
+whirgpu_status whirgpu_measure_int_peaks(int device, double out[WHIRGPU_NUM_INT_PEAKS]);
+
 /* ---- timing of the hot kernels (for roofline reporting) --------------------------
  * When enabled, every kernel family is bracketed by CUDA events on the context
  * stream; whirgpu_kernel_stats returns, per family, launches and total ms

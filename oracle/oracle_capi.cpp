@@ -69,6 +69,15 @@ void oracle_rs_encode_e3(const u64* v, size_t len, u64 N, u64 depth, u64* out) {
     auto m = rs_encode_e3(read_e3(v, len), N, depth);
     std::memcpy(out, m.data(), m.size() * 24);
 }
+// Matrix-commitment root of one base vector (irs_commit.hpp:402-470 with one
+// vector): RS encode into N x depth rows, BLAKE3 leaves, Merkle root.
+void oracle_rs_commit_root(const u64* v, size_t len, u64 N, u64 depth, u8* root_out) {
+    std::vector<u64> in(v, v + len);
+    auto m = rs_encode_base(in, N, depth);
+    auto lv = leaves_base(m, depth);
+    auto nodes = merkle_build(lv);
+    std::memcpy(root_out, nodes.back().data(), 32);
+}
 // Merkle root (and optionally the node array) of `n` 32-byte leaves.
 void oracle_merkle_root(const u8* leaves, size_t n, u8* root_out, u8* nodes_out) {
     std::vector<Hash> lv(n);

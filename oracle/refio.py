@@ -216,6 +216,7 @@ class Oracle:
         L.oracle_e3_mul.argtypes = [p, p, p]
         L.oracle_ntt.argtypes = [p, sz]
         L.oracle_rs_encode_base.argtypes = [p, sz, u64, u64, p]
+        L.oracle_rs_commit_root.argtypes = [p, sz, u64, u64, p]
         L.oracle_rs_encode_e3.argtypes = [p, sz, u64, u64, p]
         L.oracle_merkle_root.argtypes = [p, sz, p, p]
         L.oracle_merkle_open.argtypes = [p, sz, p, sz, p, sz]; L.oracle_merkle_open.restype = sz
@@ -295,6 +296,14 @@ class Oracle:
         out = np.empty((N, depth, 3), dtype=np.uint64)
         self.lib.oracle_rs_encode_e3(v.ctypes.data, v.shape[0], N, depth, out.ctypes.data)
         return out
+
+    def rs_commit_root(self, v, N, depth) -> bytes:
+        """Matrix-commitment root of one base vector: RS encode (N rows of
+        `depth` elements), BLAKE3 leaves, Merkle root, in one C call."""
+        v = np.ascontiguousarray(v, dtype=np.uint64)
+        out = ctypes.create_string_buffer(32)
+        self.lib.oracle_rs_commit_root(v.ctypes.data, v.size, N, depth, out)
+        return out.raw
 
     def merkle_root(self, leaves: bytes, sha2: bool = False) -> bytes:
         out = ctypes.create_string_buffer(32)

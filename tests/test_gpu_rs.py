@@ -31,6 +31,19 @@ def test_rs_commit_roots_match_oracle(gpu_ctx, oracle, log_len, log_exp, count):
         assert roots[k] == oracle_root(oracle, v[k], log_exp), f"vector {k}"
 
 
+@pytest.mark.parametrize("log_len,count", [(16, 64), (20, 4), (24, 1)])
+@pytest.mark.parametrize("log_exp", [1, 2, 3, 4])
+def test_rs_commit_roots_at_kernel_level_sizes(gpu_ctx, oracle, log_len, log_exp, count):
+    """The kernel-level workload's sizes: 2^16 words x 64 vectors, 2^20 x 4 and
+    2^24 x 1, expansions 2, 4, 8 and 16, rows of 16 elements; every root equals
+    the oracle's matrix commitment of the same vector."""
+    v = sample_goldilocks(7000 + 17 * log_len + log_exp, count << log_len).reshape(count, -1)
+    roots = rs_commit_batch(gpu_ctx, v, log_exp)
+    N = ((1 << log_len) // 16) << log_exp
+    for k in range(count):
+        assert roots[k] == oracle.rs_commit_root(v[k], N, 16), f"vector {k}"
+
+
 def test_rs_encode_planes_match_oracle(gpu_ctx, oracle):
     import torch
 

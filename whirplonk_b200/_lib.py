@@ -27,6 +27,7 @@ EXPORTED = [
     "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_config_from_params", "whirgpu_commit_config", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
     "whirgpu_debug_field_ops", "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
     "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
+    "whirgpu_measure_int_peaks",
     "whirgpu_batch_create", "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_batch_destroy",
     "whirgpu_server_create", "whirgpu_server_submit", "whirgpu_server_poll", "whirgpu_server_release",
     "whirgpu_server_stats", "whirgpu_server_destroy",
@@ -200,6 +201,8 @@ def load() -> ctypes.CDLL:
     L.whirgpu_host_free.argtypes = [p]
     L.whirgpu_set_timing.argtypes = [p, i32]
     L.whirgpu_kernel_stats.argtypes = [p, p, p, i32]
+    L.whirgpu_measure_int_peaks.argtypes = [ctypes.c_int, p]
+    L.whirgpu_measure_int_peaks.restype = ctypes.c_int
     L.whirgpu_launch_count.argtypes = []
     L.whirgpu_launch_count.restype = u64
     L.whirgpu_last_io_bytes.argtypes = [p, ctypes.POINTER(u64), ctypes.POINTER(u64)]

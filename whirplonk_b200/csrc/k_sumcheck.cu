@@ -609,9 +609,10 @@ int launch_cov_init(const CovInitArgs& a, cudaStream_t st) {
 // (Ext3) and in-domain points (base field, lifted).  With i = h 2^LO + l the
 // tables hold T_j[h] = rlc_j z_j^(h 2^LO) (Ext3) and z_j^l; an element's sum
 // over the points is accumulated as unreduced 192-bit products (3 per base
-// point, 9 per Ext3 point) and reduced once.
+// point, 9 per Ext3 point) and reduced once.  LO = 8 keeps every point's
+// z_j^l table (2 KiB for a base point) resident in L1 next to the others.
 // ---------------------------------------------------------------------------
-constexpr u32 CA_LO = 10;
+constexpr u32 CA_LO = 8;
 
 // Point j's table: z_j^l (l < 2^LO) then rlc_j z_j^(h 2^LO).  For the base-field
 // (in-domain) points z_j^l is a base element and goes to the compact array
@@ -634,21 +635,61 @@ __global__ void k_cov_acc_tables(const ProofScalars* sc, int n_ext, int n_points
     }
 }
 
+// Two consecutive elements (same row h) per thread: each T_j[h] load serves
+// both, and the base points go four at a time with their loads first.
 __global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* tab, const u64* lo_base, u32 hi_count) {
-    const u32 per = (1u << CA_LO) + hi_count;
+    constexpr u32 NL = 1u << CA_LO;
+    const u32 per = NL + hi_count;
     const int npts = a.n_ext + a.n_base;
-    for (u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x; i < a.size; i += (u64)gridDim.x * blockDim.x) {
-        const u32 hi = (u32)(i >> CA_LO), lo = (u32)(i & ((1u << CA_LO) - 1));
-        E3Acc s = e3acc_zero();
-        const E3* tj = tab;
-        for (int j = 0; j < a.n_ext; ++j, tj += per) e3acc_mac(s, tj[(1u << CA_LO) + hi], tj[lo]);
-        const u64* lb = lo_base + lo;
-        for (int j = a.n_ext; j < npts; ++j, tj += per, lb += (1u << CA_LO))
-            e3acc_mac_base(s, tj[(1u << CA_LO) + hi], *lb);
-        const E3 add = ef_fix(e3acc_reduce(s), a.ext2);
-        a.cov[0][i] = gl_add(a.cov[0][i], add.c0);
-        a.cov[1][i] = gl_add(a.cov[1][i], add.c1);
-        a.cov[2][i] = gl_add(a.cov[2][i], add.c2);
+    const u64 npair = (a.size + 1) >> 1;
+    for (u64 pi = (u64)blockIdx.x * blockDim.x + threadIdx.x; pi < npair; pi += (u64)gridDim.x * blockDim.x) {
+        const u64 i = 2 * pi;
+        const bool two = i + 1 < a.size;
+        const u32 hi = (u32)(i >> CA_LO), lo = (u32)(i & (NL - 1));  // lo even: lo + 1 < NL
+        E3Acc s0 = e3acc_zero(), s1 = e3acc_zero();
+        for (int j = 0; j < a.n_ext; ++j) {
+            const E3* tj = tab + (u64)j * per;
+            const E3 w = tj[NL + hi];
+            e3acc_mac(s0, w, tj[lo]);
+            e3acc_mac(s1, w, tj[lo + 1]);
+        }
+        int j = a.n_ext;
+        for (; j + 4 <= npts; j += 4) {
+            E3 w[4];
+            u64 x0[4], x1[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                w[q] = tab[(u64)(j + q) * per + NL + hi];
+                const u64* lb = lo_base + (u64)(j + q - a.n_ext) * NL + lo;
+                x0[q] = lb[0];
+                x1[q] = lb[1];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                e3acc_mac_base(s0, w[q], x0[q]);
+                e3acc_mac_base(s1, w[q], x1[q]);
+            }
+        }
+        for (; j < npts; ++j) {
+            const E3 w = tab[(u64)j * per + NL + hi];
+            const u64* lb = lo_base + (u64)(j - a.n_ext) * NL + lo;
+            e3acc_mac_base(s0, w, lb[0]);
+            e3acc_mac_base(s1, w, lb[1]);
+        }
+        const E3 add0 = ef_fix(e3acc_reduce(s0), a.ext2), add1 = ef_fix(e3acc_reduce(s1), a.ext2);
+        if (two) {
+            const u64 d0[3] = {add0.c0, add0.c1, add0.c2}, d1[3] = {add1.c0, add1.c1, add1.c2};
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                ulonglong2* p = reinterpret_cast<ulonglong2*>(a.cov[c] + i);
+                const ulonglong2 v = *p;
+                *p = make_ulonglong2(gl_add(v.x, d0[c]), gl_add(v.y, d1[c]));
+            }
+        } else {
+            a.cov[0][i] = gl_add(a.cov[0][i], add0.c0);
+            a.cov[1][i] = gl_add(a.cov[1][i], add0.c1);
+            a.cov[2][i] = gl_add(a.cov[2][i], add0.c2);
+        }
     }
 }
 
@@ -668,7 +709,9 @@ int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
     u64* lo_base = reinterpret_cast<u64*>(reinterpret_cast<char*>(a.scratch) + (tab_bytes + 255) / 256 * 256);
     k_cov_acc_tables<<<2 * device_sms(), 256, 0, st>>>(a.sc, a.n_ext, npts, hc, tab, lo_base, a.ext2 != 0);
     count_launches(1);
-    u64 want = (a.size + 255) / 256;
+    for (int c = 0; c < 3; ++c)
+        if (reinterpret_cast<uintptr_t>(a.cov[c]) & 15) return -1;  // 16-byte pairs
+    u64 want = ((a.size + 1) / 2 + 255) / 256;
     const u64 cap = (u64)device_sms() * 16;
     k_cov_accumulate<<<(unsigned)(want > cap ? cap : want), 256, 0, st>>>(a, tab, lo_base, hc);
     count_launches(1);

@@ -213,6 +213,27 @@ int launch_sumcheck_small(const SumcheckArgs& a, int rounds, int fold_after, cud
 // Fold only: a_out[i] = a_in[i] + r (a_in[i+size] - a_in[i]), same for b.
 int launch_fold(const SumcheckArgs& a, cudaStream_t st);
 size_t sumcheck_scratch_bytes();
+// The initial sumcheck of one base-field vector against a covector of MLE
+// forms and OOD points, by block evaluation (k_sc_tensor.cu): the k rounds'
+// messages and challenges (sc_r[r_slot ..]), and the vector and covector folded
+// to size 2^(n - k) in a_out / cov_out -- the state the round kernels reach,
+// without writing the 2^n covector.  Target field Ext3 or the base field.
+struct TscArgs {
+    const u64* coeffs;  // 2^n base coefficients
+    u32 n, k;           // variables, initial-sumcheck rounds (no round PoW)
+    const u64* points;  // n_forms MLE points, n Ext3 coordinates each
+    int n_forms, n_ood; // terms: the forms, then sc->init_ood_pts[0 .. n_ood)
+    ProofScalars* sc;
+    TxState* tx;
+    int r_slot;
+    u64* a_out[3];
+    u64* cov_out[3];
+    void* scratch;      // tsc_scratch_bytes
+    size_t scratch_bytes;
+};
+bool tsc_applicable(u32 n, u32 k, int n_terms);
+size_t tsc_scratch_bytes(u32 n, u32 k, int n_terms);
+int launch_tsc(const TscArgs& a, cudaStream_t st);
 
 // ---- Twiddle tables ----------------------------------------------------------------
 void host_twiddles(u64* stage /*1024*/, u64* hi /*8192*/, u64* lo /*8192*/);

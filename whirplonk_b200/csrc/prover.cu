@@ -121,6 +121,7 @@ ProofPlan make_plan(const WhirSchedule& sched, const ProtocolParams& params, int
     p.off_ood_scratch = b.take(ood_scratch_bytes(1ull << n, p.ood_values));
     const int init_ood = (int)(s.initial.out_domain * nwit);
     size_t cov_scratch = cov_init_scratch_bytes(n, n_forms, init_ood);
+    cov_scratch = std::max(cov_scratch, tsc_scratch_bytes(n, (uint32_t)s.initial_sumcheck.num_rounds, n_forms + init_ood));
     for (size_t r = 0; r < s.rounds.size(); ++r) {
         const IrsSchedule& prev = r == 0 ? s.initial : s.rounds[r - 1].irs;
         const int npts = (int)(s.rounds[r].irs.out_domain + prev.in_domain);
@@ -355,7 +356,30 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
     WG_TIMED(c, FAM_TX, launch_constraint_rlc(c.tx(), c.sc(), p.n_forms, (int)W, ood0, (int)V, st));
     const bool has_constraints = p.n_forms + ood0 > 0;
     int r_slot = 0;
-    {  // covector (zero without constraints) and, with several vectors, the combined vector
+    // One base-field vector whose covector is MLE forms and OOD points only:
+    // the initial sumcheck by block evaluation (k_sc_tensor.cu) never writes
+    // the 2^n covector and leaves a, cov folded exactly as the rounds below do.
+    const uint32_t k0 = (uint32_t)s.initial_sumcheck.num_rounds;
+    const bool tensor = has_constraints && V == 1 && !p.full_vector && p.dense_mask == 0 &&
+                        p.params.field_degree != 2 && s.initial_sumcheck.pow_threshold == ~0ull &&
+                        tsc_applicable(p.n, k0, p.n_forms + ood0 * (int)W);
+    if (tensor) {
+        TscArgs ta{};
+        ta.coeffs = c.w(p.off_coeffs);
+        ta.n = p.n;
+        ta.k = k0;
+        ta.points = c.w(p.off_points);
+        ta.n_forms = p.n_forms;
+        ta.n_ood = ood0 * (int)W;
+        ta.sc = c.sc();
+        ta.tx = c.tx();
+        ta.r_slot = r_slot;
+        for (int k = 0; k < 3; ++k) { ta.a_out[k] = c.a(k); ta.cov_out[k] = c.cov(k); }
+        ta.scratch = ws + p.off_cov_scratch;
+        ta.scratch_bytes = p.off_tx - p.off_cov_scratch;  // the covector scratch region
+        WG_TIMED(c, FAM_SUMCHECK, launch_tsc(ta, st));
+        r_slot += (int)k0;
+    } else {  // covector (zero without constraints) and, with several vectors, the combined vector
         CovInitArgs ci{};
         for (int k = 0; k < 3; ++k) { ci.cov[k] = c.cov(k); ci.vec_out[k] = c.a(k); }
         ci.logS = p.n;
@@ -373,7 +397,9 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         ci.tx = c.tx();
         WG_TIMED(c, FAM_COV, launch_cov_init(ci, st));
     }
-    if (has_constraints) {
+    if (tensor) {
+        // done above
+    } else if (has_constraints) {
         WG_TRY(sumcheck(c, s.initial_sumcheck, size0, !p.full_vector, r_slot, true));
     } else {
         // No constraint (unique decoding, no forms; whir_prover.hpp:211-218): the

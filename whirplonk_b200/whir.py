@@ -85,6 +85,7 @@ class Context:
 
     def __init__(self, device: int = 0, hbm_budget: int = 0):
         self._L = _lib.load()
+        self.device = device
         h = ctypes.c_void_p()
         _lib.check(self._L.whirgpu_ctx_create(device, hbm_budget, ctypes.byref(h)))
         self.handle = h.value
