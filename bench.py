@@ -28,12 +28,23 @@ ChaCha20 keystream):
       bits are 37-58, far above what any prover grinds; the reference's own ZK
       dumper disables them the same way).
 
+  rs_commit_n22x4_exp4: the kernel-level commitment -- 4 vectors of 2^22 words,
+      expansion 4, rows of 16 elements (RS encode + BLAKE3 leaves + Merkle
+      root per vector, no transcript); beside it the reference's own CUDA
+      side-car on the same vectors (roots compared, vs_reference_gpu).
+
 Every batched or served proof is checked byte-for-byte against the plain
 path's proof of the same request.  Multi-GPU: independent replicas (each rank
 its own stream of requests, no collective on the data path), weak scaling.
 
 --impl reference times the reference C++ CPU prover (oracle/_ref/ref_driver,
-built from the reference sources) on the same workload with all host threads.
+built from the reference sources) with all host threads on the same request
+multiset as the GPU arm: every distinct (num_variables, rate) shape of the
+timed stream is proved once and the rate is the multiset's count over the sum
+of count x time.  It loads nothing from whirplonk_b200 (inputs come from the
+numpy restatement of the sampler, oracle/chacha.py) and warms up on a proof
+that is not in the stream.  For the kernel-level workload it times the
+reference's CUDA side-car instead (oracle/_ref/ref_gpu_driver).
 """
 from __future__ import annotations
 
@@ -64,6 +75,8 @@ WORKLOADS = {
     "whir_prove_n22_rate4": {"kind": "single", "n": 22, "rho": 2},
     "whir_prove_n18_rate2": {"kind": "single", "n": 18, "rho": 1},
     "whir_zk_prove_n22_rate4": {"kind": "zk", "n": 22, "rho": 2},
+    "rs_commit_n22x4_exp4": {"kind": "kernel", "log_len": 22, "count": 4, "log_exp": 2, "log_depth": 4,
+                             "seed": 2222},
 }
 ZK_SEED = bytes(range(1, 9)) + bytes(24)  # the reference driver takes 8 seed bytes (the rest zero)
 DEFAULT_WORKLOAD = "whir_served_mixed_n12_24"
@@ -425,6 +438,58 @@ WARMUP_SHAPE = (12, 1)  # the reference arm's warm-up proof: never a request of 
 WARMUP_SEED = 424242
 
 
+def kernel_vectors(w, sampler):
+    return sampler(w["seed"], w["count"] << w["log_len"]).reshape(w["count"], -1)
+
+
+def reference_gpu_commit(w, vectors, reps=3):
+    """The reference's CUDA side-car (oracle/_ref/ref_gpu_driver: its NTT engine's
+    GPU RS encode + BLAKE3 leaves, then its GPU Merkle tree, host buffers in and
+    out) on the same vectors: (roots, ms per pass over the vectors), or None."""
+    import struct
+    import tempfile
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_driver")
+    if not os.access(exe, os.X_OK):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        inp, out = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        with open(inp, "wb") as f:
+            f.write(struct.pack("<II5Q", 0x47505552, 1, w["count"], w["log_len"], w["log_exp"], w["log_depth"], reps))
+            f.write(np.ascontiguousarray(vectors, dtype=np.uint64).tobytes())
+        subprocess.run([exe, inp, out], check=True, timeout=600, stdout=subprocess.DEVNULL)
+        with open(out, "rb") as f:
+            b = f.read()
+    roots = [b[32 * k:32 * k + 32] for k in range(w["count"])]
+    (ms,) = struct.unpack_from("<d", b, 32 * w["count"])
+    return roots, ms
+
+
+def run_reference_kernel_arm(args, w, world):
+    """Kernel-level commitment: the reference's own GPU path (its CUDA
+    side-car, host buffers in and out), the same vectors as the GPU arm."""
+    from oracle.chacha import sample_goldilocks as np_sampler
+
+    vectors = kernel_vectors(w, np_sampler)
+    r = reference_gpu_commit(w, vectors, reps=max(3, args.steps))
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_gpu_driver not built"}))
+        return 0
+    _, ms = r
+    value = w["count"] / (ms / 1000.0)
+    print(json.dumps({
+        "impl": "reference", "metric": KERNEL_METRIC, "value": value, "unit": "commitments/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64 (Goldilocks)", "data": DATA,
+        "config": kernel_config(args.workload, w), "parallelism": "the reference's CUDA side-car on 1 GPU",
+        "e2e": {"value": value, "unit": "commitments/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_gpu_note": "NttEngine::try_gpu_interleaved_rs_encode_blake3_matrix_leaves + gpu_blake3_merkle_tree "
+                              "per vector, host in / host out (its API returns the codeword matrix to the host); "
+                              "median of the timed passes after a warm-up pass",
+    }))
+    return 0
+
+
 def run_reference_arm(args, rank, world):
     """The reference C++ CPU prover on the GPU arm's workload.  Loads nothing
     from whirplonk_b200: inputs come from the numpy restatement of the sampler
@@ -437,6 +502,8 @@ def run_reference_arm(args, rank, world):
     w = WORKLOADS[args.workload]
     if w["kind"] == "zk":
         return run_reference_zk_arm(args, w, world)
+    if w["kind"] == "kernel":
+        return run_reference_kernel_arm(args, w, world)
     if not ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_driver not built"}))
         return 0
@@ -1081,17 +1148,115 @@ def run_served(args, H, ctx, w):
     return line
 
 
+KERNEL_METRIC = "kernel-level RS commitment (NTT/LDE + BLAKE3 leaves + Merkle root) per vector"
+
+
+def kernel_config(name, w):
+    return {"workload": name, "vectors": w["count"], "log_len": w["log_len"], "expansion": 1 << w["log_exp"],
+            "row_elements": 1 << w["log_depth"], "hash": "BLAKE3", "seed": w["seed"],
+            "l2": "codewords of 4 x 2^24 words (512 MiB) far above the 126 MB L2; no flush"}
+
+
+def run_kernel(args, H, ctx, w):
+    """Kernel-level commitment of `count` vectors per step (rs_commit_batch):
+    device-resident inputs for `value`, pinned host inputs for `e2e`; the
+    reference's CUDA side-car on the same vectors beside it, roots compared."""
+    from whirplonk_b200.rs import rs_commit_batch
+
+    torch = H.torch
+    vectors = kernel_vectors(w, gpu_sampler)
+    count, log_len, log_exp, log_depth = w["count"], w["log_len"], w["log_exp"], w["log_depth"]
+    dev = torch.from_numpy(vectors.reshape(-1).view(np.int64)).to(H.device)
+    ptr = ctx._L.whirgpu_host_alloc(vectors.nbytes)
+    pinned = np.ctypeslib.as_array((ctypes.c_uint64 * vectors.size).from_address(ptr)).reshape(count, -1)
+    pinned[:] = vectors
+    stream = torch.cuda.ExternalStream(ctx.stream, device=H.device)
+
+    def dev_step():
+        return rs_commit_batch(ctx, None, log_exp, log_depth, on_device_ptr=dev.data_ptr(), count=count,
+                               log_len=log_len)
+
+    roots = dev_step()
+    assert rs_commit_batch(ctx, pinned, log_exp, log_depth) == roots
+    for _ in range(max(args.warmup, 3)):
+        dev_step()
+    clocks = ClockSampler(H.local_rank)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = ctx.launch_count()
+    elapsed, out = H.timed(stream, lambda: [dev_step() for _ in range(args.steps)][-1])
+    launches = ctx.launch_count() - launches0
+    assert out == roots
+    e2e_ms, out = H.timed(stream, lambda: [rs_commit_batch(ctx, pinned, log_exp, log_depth)
+                                           for _ in range(args.steps)][-1])
+    clk = clocks.stop()
+    assert out == roots
+    N = ((1 << log_len) >> log_depth) << log_exp
+    d = 1 << log_depth
+    alg = count * (8 * ((1 << log_len) + N * d) + (8 * d * N + 32 * N) + 3 * 32 * N)
+    bfly = count * d * (N // 2) * (log_len - log_depth)
+    comps = count * (N * -(-(8 * d) // 64) + N - 1)
+    step_s = elapsed / 1000.0 / args.steps
+    peak, peak_kind = read_peaks()
+    line = {
+        "value": count * args.steps * H.world / (elapsed / 1000.0), "ms_per_step": elapsed / args.steps,
+        "e2e": {"value": count * args.steps * H.world / (e2e_ms / 1000.0), "unit": "commitments/s",
+                "h2d_bytes_per_step": int(vectors.nbytes), "d2h_bytes_per_step": 32 * count},
+        "gpu_launches": launches, "clocks": clk,
+        "roofline": {"bound": "hbm", "kernel": "rs_commit (LDE + leaves + Merkle, one call)",
+                     "achieved": alg / step_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / step_s / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_step": alg},
+    }
+    pk = measure_int_peaks(ctx.device)
+    if pk:
+        line["roofline_int"] = {"whole_call": {"butterflies_per_s": bfly / step_s, "compressions_per_s": comps / step_s,
+                                               "butterfly_peak": pk["butterflies_per_s"],
+                                               "compression_peak": pk["blake3_compressions_per_s"],
+                                               "note": "the whole call's time against each unit count: lower bounds "
+                                                       "on each family's own rate"}}
+        line["int_peaks_measured"] = pk
+    if H.world == 1 and H.rank == 0 and not args.no_cpu_baseline:
+        from oracle.refio import Oracle
+
+        O = Oracle()
+        t0 = time.perf_counter()
+        oroots = [O.rs_commit_root(vectors[k], N, d) for k in range(count)]
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": count / cpu_s, "unit": "commitments/s", "cores": os.cpu_count() or 1,
+                                "kind": "port", "sample": f"the same {count} vectors through the oracle's matrix "
+                                                          f"commitment (OpenMP), {cpu_s:.1f} s; roots equal the GPU's: "
+                                                          f"{oroots == roots}"}
+        assert oroots == roots, "kernel-level roots differ from the oracle's"
+        r = reference_gpu_commit(w, vectors)
+        if r is not None:
+            rroots, rms = r
+            ours = count / (e2e_ms / 1000.0 / args.steps)
+            theirs = count / (rms / 1000.0)
+            line["reference_gpu"] = {"value": theirs, "unit": "commitments/s", "ms_per_step": rms,
+                                     "roots_equal": rroots == roots,
+                                     "sample": "the reference's CUDA side-car (oracle/_ref/ref_gpu_driver, built "
+                                               "unmodified for sm_100a) on the same vectors, host in / host out, "
+                                               "median of 3 passes after a warm-up"}
+            line["vs_reference_gpu"] = ours / theirs
+    ctx._L.whirgpu_host_free(ptr)
+    return line
+
+
 def run_gpu_arm(args, rank, world, local_rank):
     from whirplonk_b200 import Context
 
     H = Harness(rank, world, local_rank)
     w = WORKLOADS[args.workload]
     ctx = Context(local_rank)
-    body = {"single": run_single, "batch": run_batch, "served": run_served, "zk": run_zk}[w["kind"]](args, H, ctx, w)
-    line = {"metric": METRIC, "value": body.pop("value"), "unit": "proofs/s", "n_gpus": world, "steps": args.steps,
+    body = {"single": run_single, "batch": run_batch, "served": run_served, "zk": run_zk,
+            "kernel": run_kernel}[w["kind"]](args, H, ctx, w)
+    kernel = w["kind"] == "kernel"
+    line = {"metric": KERNEL_METRIC if kernel else METRIC, "value": body.pop("value"),
+            "unit": "commitments/s" if kernel else "proofs/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": body.pop("ms_per_step"), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": DATA,
-            "config": config_of(args.workload, w),
+            "config": kernel_config(args.workload, w) if kernel else config_of(args.workload, w),
             "parallelism": f"replicas x{world} (one independent request stream per GPU)" if world > 1 else "1 GPU"}
     line.update(body)
     ctx.close()
