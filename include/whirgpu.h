@@ -67,6 +67,19 @@ void whirgpu_ctx_destroy(whirgpu_ctx* ctx);
 const char* whirgpu_last_error(const whirgpu_ctx* ctx);
 /* cudaStream_t of the context, for callers that time or order work around it. */
 void* whirgpu_stream(whirgpu_ctx* ctx);
+/* Codeword row order of the commitments this context makes from now on.
+ * WHIRGPU_ORDER_NATURAL (the default): row i is the evaluation at w_N^i, as
+ * the C++ reference commits (cpp/include/whir/algebra/ntt/mod_ntt.hpp:49-130).
+ * WHIRGPU_ORDER_COSET_MAJOR: the Rust crate's order without its rs_in_order
+ * feature (rust/src/algebra/ntt/cooley_tukey.rs:375-480): with message length
+ * m and e = N / m cosets, committed row k is the evaluation at
+ * w_N^(k / m + (k mod m) e) (transpose_permute, rust/src/algebra/ntt/
+ * transpose.rs:10-15); the opened rows and their evaluation points follow.
+ * Zero-knowledge commitments accept the natural order only (the Rust ZK
+ * prover requires rs_in_order). */
+#define WHIRGPU_ORDER_NATURAL 0
+#define WHIRGPU_ORDER_COSET_MAJOR 1
+whirgpu_status whirgpu_set_codeword_order(whirgpu_ctx* ctx, int order);
 
 /* ---- parameters ------------------------------------------------------------
  * Round schedule of Config::from_params (whir.hpp:118-224) as a flat array:

@@ -30,6 +30,10 @@ std::vector<E3> read_e3(const u64* w, size_t n) {
 
 extern "C" {
 
+// Codeword order of every later commitment and opening: 0 natural (the C++
+// reference), 1 coset-major (the Rust crate without rs_in_order).
+void oracle_set_coset_major(int on) { coset_major_order() = on != 0; }
+u64 oracle_transpose_permute(u64 k, u64 rows, u64 cols) { return transpose_permute(k, rows, cols); }
 void oracle_blake3(const u8* d, size_t n, u8* out) { Hash h = blake3(d, n); std::memcpy(out, h.data(), 32); }
 void oracle_sha3_256(const u8* d, size_t n, u8* out) { sha3_256(d, n, out); }
 void oracle_sha3_512(const u8* d, size_t n, u8* out) { sha3_512(d, n, out); }

@@ -215,6 +215,8 @@ class Oracle:
         L.oracle_root_of_unity.argtypes = [u64]; L.oracle_root_of_unity.restype = u64
         L.oracle_e3_mul.argtypes = [p, p, p]
         L.oracle_ntt.argtypes = [p, sz]
+        L.oracle_set_coset_major.argtypes = [ctypes.c_int]
+        L.oracle_transpose_permute.argtypes = [u64, u64, u64]; L.oracle_transpose_permute.restype = u64
         L.oracle_rs_encode_base.argtypes = [p, sz, u64, u64, p]
         L.oracle_rs_commit_root.argtypes = [p, sz, u64, u64, p]
         L.oracle_rs_encode_e3.argtypes = [p, sz, u64, u64, p]
@@ -296,6 +298,14 @@ class Oracle:
         out = np.empty((N, depth, 3), dtype=np.uint64)
         self.lib.oracle_rs_encode_e3(v.ctypes.data, v.shape[0], N, depth, out.ctypes.data)
         return out
+
+    def set_coset_major(self, on: bool) -> None:
+        """Codeword order of later commitments and openings: natural (the C++
+        reference) or coset-major (the Rust crate without rs_in_order)."""
+        self.lib.oracle_set_coset_major(int(bool(on)))
+
+    def transpose_permute(self, k, rows, cols) -> int:
+        return int(self.lib.oracle_transpose_permute(k, rows, cols))
 
     def rs_commit_root(self, v, N, depth) -> bytes:
         """Matrix-commitment root of one base vector: RS encode (N rows of

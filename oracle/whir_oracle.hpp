@@ -854,6 +854,27 @@ inline std::vector<E3> sumcheck_prove(Transcript& t, const SumcheckCfg& cfg, std
 // ---------------------------------------------------------------------------
 // IRS commit / open (irs_commit.hpp:344-713), witness kept in the oracle.
 // ---------------------------------------------------------------------------
+// Codeword order.  The C++ reference stores codeword rows in natural order
+// (row i = evaluation at w_N^i, mod_ntt.hpp:49-130).  The Rust crate without
+// its `rs_in_order` feature stores them coset-major
+// (rust/src/algebra/ntt/cooley_tukey.rs:375-480): with coset size m (the
+// message length) and e = N / m cosets, row k holds the evaluation at
+// w_N^transpose_permute(k, e, m), transpose_permute(k, rows, cols) =
+// k / cols + (k % cols) * rows (rust/src/algebra/ntt/transpose.rs:10-15).
+// Opened rows are addressed by k and their evaluation points follow the same
+// permutation (evaluation_points, cooley_tukey.rs:375-402).  Process-wide
+// switch of the oracle (test infrastructure): false = natural order.
+inline bool& coset_major_order() {
+    static bool on = false;
+    return on;
+}
+inline u64 transpose_permute(u64 k, u64 rows, u64 cols) { return k / cols + (k % cols) * rows; }
+// Natural row index of committed row k of an N-row codeword of message length m.
+inline u64 codeword_row(u64 k, u64 N, u64 m) {
+    if (!coset_major_order() || m == 0 || N % m != 0) return k;
+    return transpose_permute(k, N / m, m);
+}
+
 struct Witness {
     bool base = true;
     std::vector<u64> mat_base;   // row-major N x (nvec * depth) (initial commitment)
@@ -879,8 +900,10 @@ inline Witness commit_base_multi(Transcript& t, const IrsCfg& c, const std::vect
     w.mat_base.assign(w.N * cols, 0);
     for (u64 v = 0; v < w.nvec; ++v) {
         auto m = rs_encode_base(*vs[v], w.N, w.depth);
-        for (u64 i = 0; i < w.N; ++i)
-            for (u64 b = 0; b < w.depth; ++b) w.mat_base[i * cols + v * w.depth + b] = m[i * w.depth + b];
+        for (u64 i = 0; i < w.N; ++i) {
+            const u64 nat = codeword_row(i, w.N, c.msg_len());
+            for (u64 b = 0; b < w.depth; ++b) w.mat_base[i * cols + v * w.depth + b] = m[nat * w.depth + b];
+        }
     }
     w.nodes = merkle_build(leaves_base(w.mat_base, cols, eng), eng);
     t.message_hash(w.root());
@@ -900,6 +923,12 @@ inline Witness commit_e3(Transcript& t, const IrsCfg& c, const std::vector<E3>& 
     Witness w;
     w.base = false; w.N = c.codeword_length; w.depth = c.depth; w.layers = layers_for(w.N);
     w.mat_e3 = rs_encode_e3(v, w.N, w.depth);
+    if (coset_major_order()) {
+        std::vector<E3> nat = w.mat_e3;
+        for (u64 i = 0; i < w.N; ++i)
+            for (u64 b = 0; b < w.depth; ++b)
+                w.mat_e3[i * w.depth + b] = nat[codeword_row(i, w.N, c.msg_len()) * w.depth + b];
+    }
     w.nodes = merkle_build(leaves_e3(w.mat_e3, w.depth, eng), eng);
     t.message_hash(w.root());
     for (u64 s = 0; s < c.out_domain; ++s) w.ood_points.push_back(t.challenge_t());
@@ -946,7 +975,7 @@ inline Opening open_witnesses(Transcript& t, const IrsCfg& c, const std::vector<
     auto idx = challenge_indices(t, c.codeword_length, c.in_domain);
     Opening o;
     u64 gen = root_of_unity(c.codeword_length);
-    for (u64 i : idx) o.points.push_back(E3::from_base(fpow(gen, i)));
+    for (u64 i : idx) o.points.push_back(E3::from_base(fpow(gen, codeword_row(i, c.codeword_length, c.msg_len()))));
     for (const Witness* w : ws) o.stride += w->cols();
     o.rows.assign(idx.size() * o.stride, E3());
     u64 col0 = 0;

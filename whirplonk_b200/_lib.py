@@ -21,7 +21,8 @@ FAMILY_NAMES = ["ntt", "leaf_hash", "merkle", "ood", "sumcheck", "covector", "po
 
 # Every symbol include/whirgpu.h declares.
 EXPORTED = [
-    "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_schedule",
+    "whirgpu_ctx_create", "whirgpu_ctx_destroy", "whirgpu_last_error", "whirgpu_stream", "whirgpu_set_codeword_order",
+    "whirgpu_schedule",
     "whirgpu_workspace_bytes",
     "whirgpu_cli_domain_separator", "whirgpu_transcript_create", "whirgpu_transcript_destroy", "whirgpu_proof_get",
     "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_config_from_params", "whirgpu_commit_config", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
@@ -201,6 +202,8 @@ def load() -> ctypes.CDLL:
     L.whirgpu_host_free.argtypes = [p]
     L.whirgpu_set_timing.argtypes = [p, i32]
     L.whirgpu_kernel_stats.argtypes = [p, p, p, i32]
+    L.whirgpu_set_codeword_order.argtypes = [p, ctypes.c_int]
+    L.whirgpu_set_codeword_order.restype = ctypes.c_int
     L.whirgpu_measure_int_peaks.argtypes = [ctypes.c_int, p]
     L.whirgpu_measure_int_peaks.restype = ctypes.c_int
     L.whirgpu_launch_count.argtypes = []

@@ -171,7 +171,8 @@ std::string plan_key(const WhirSchedule& s, const ProtocolParams& pp, size_t ds_
         w.insert(w.end(), {r.irs.vector_size, r.irs.codeword_length, r.irs.depth, r.irs.in_domain, r.irs.out_domain,
                            r.pow_threshold, r.sumcheck.num_rounds, r.sumcheck.pow_threshold});
     w.insert(w.end(), {s.final_sumcheck.num_rounds, s.final_sumcheck.pow_threshold, s.final_pow, pp.batch_size,
-                       (uint64_t)pp.hash, (uint64_t)pp.field_degree, (uint64_t)std::max<size_t>(ds_len, 96), nwit});
+                       (uint64_t)pp.hash, (uint64_t)pp.field_degree, (uint64_t)std::max<size_t>(ds_len, 96), nwit,
+                       (uint64_t)pp.coset_major});
     return std::string(reinterpret_cast<const char*>(w.data()), w.size() * sizeof(uint64_t));
 }
 }  // namespace
@@ -187,8 +188,10 @@ whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_param
     return acquire_workspace_sched(c, sched, to_params(params), ds_len, out, cap, nwit);
 }
 
-whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched, const ProtocolParams& pp, size_t ds_len,
-                                       Workspace** out, uint64_t cap, uint32_t nwit) {
+whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched, const ProtocolParams& pp_in,
+                                       size_t ds_len, Workspace** out, uint64_t cap, uint32_t nwit) {
+    ProtocolParams pp = pp_in;
+    pp.coset_major = c->codeword_order == WHIRGPU_ORDER_COSET_MAJOR ? 1 : 0;
     ProofPlan plan;
     try {
         plan = make_plan(sched, pp, MAX_FORMS, std::max<size_t>(ds_len, 96), nwit);
@@ -313,6 +316,14 @@ void whirgpu_ctx_destroy(whirgpu_ctx* c) {
 
 const char* whirgpu_last_error(const whirgpu_ctx* c) { return c ? c->err.c_str() : "no context"; }
 void* whirgpu_stream(whirgpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+whirgpu_status whirgpu_set_codeword_order(whirgpu_ctx* c, int order) {
+    if (!c) return WHIRGPU_E_INVALID;
+    if (order != WHIRGPU_ORDER_NATURAL && order != WHIRGPU_ORDER_COSET_MAJOR)
+        return fail(c, WHIRGPU_E_INVALID, "unknown codeword order");
+    c->codeword_order = order;
+    return WHIRGPU_OK;
+}
 
 size_t whirgpu_schedule(const whirgpu_params* params, uint64_t n, uint64_t* out, size_t cap) {
     if (!params) return 0;

@@ -85,6 +85,7 @@ struct Workspace {
 
 struct whirgpu_ctx {
     int device = 0;
+    int codeword_order = 0;  // WHIRGPU_ORDER_* of the commitments made from now on
     cudaStream_t stream = nullptr;
     uint64_t budget = 0;
     uint64_t allocated = 0;

@@ -86,15 +86,16 @@ __device__ __forceinline__ void leaf_sha256(const u64* __restrict__ planes, u64 
 // arrays `plane_stride` / `node_stride` words apart).
 template <int NCOMP, int H>
 __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes,
-                                                u64 plane_stride, u64 node_stride) {
-    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
+                                                u64 plane_stride, u64 node_stride, u32 logN, u32 perm_log_e) {
+    const u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    const u64 i = codeword_row(k, logN, perm_log_e);  // the row leaf k hashes
     planes += blockIdx.y * plane_stride;
     nodes += blockIdx.y * node_stride;
     if (H == HASH_SHA256) {
         unsigned out[8];
         leaf_sha256<NCOMP>(planes, N, depth, i, out);
-        store_node(nodes, i, out);
+        store_node(nodes, k, out);
         return;
     }
     const u32 nwords = depth * NCOMP;           // 64-bit words per row
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
         const unsigned flags = (t == 0 ? B3_CHUNK_START : 0u) | (t + 1 == nblocks ? (B3_CHUNK_END | B3_ROOT) : 0u);
         b3_compress(cv, m, flags, len);
     }
-    store_node(nodes, i, cv);
+    store_node(nodes, k, cv);
 }
 
 // Rows wider than one chunk (1024 bytes: several committed vectors side by
@@ -135,9 +136,11 @@ __device__ __forceinline__ void b3_parent_cv(const unsigned l[8], const unsigned
 }
 
 template <int NCOMP>
-__global__ void __launch_bounds__(128) k_leaves_wide(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes) {
-    const u64 i = (u64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
+__global__ void __launch_bounds__(128) k_leaves_wide(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes,
+                                                     u32 logN, u32 perm_log_e) {
+    const u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    const u64 i = codeword_row(k, logN, perm_log_e);  // the row leaf k hashes
     const u32 nwords = depth * NCOMP;
     const u32 nch = (nwords + 127) / 128;
     unsigned stack[5][8];  // a tree of < 32 chunks holds at most 5 pending subtrees
@@ -181,9 +184,9 @@ __global__ void __launch_bounds__(128) k_leaves_wide(const u64* __restrict__ pla
         unsigned p[8];
         b3_parent_cv(stack[sp], cv, sp == 0 ? B3_ROOT : 0u, p);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) cv[k] = p[k];
+        for (int q = 0; q < 8; ++q) cv[q] = p[q];
     }
-    store_node(nodes, i, cv);
+    store_node(nodes, k, cv);
 }
 
 __host__ __device__ __forceinline__ u64 level_offset(u32 logN, u32 l) {
@@ -201,34 +204,39 @@ __device__ __forceinline__ void parent_cv(const unsigned l[8], const unsigned r[
 }
 
 int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
-                       u64 node_stride, int hash, cudaStream_t st) {
+                       u64 node_stride, int hash, cudaStream_t st, u32 perm_log_e) {
     if (count == 0 || count > 65535) return -1;
     if (ncomp < 1 || ncomp > 3) return -1;  // base field, Ext2 (c0 c1 per element), Ext3
+    if (N == 0 || (N & (N - 1))) return -1;
+    u32 logN = 0;
+    while ((1ull << logN) < N) ++logN;
+    if (perm_log_e > logN) return -1;
     if (hash != HASH_SHA256 && depth * ncomp * 8 > 1024) {  // BLAKE3 tree mode, one matrix at a time
         if (count != 1 || depth * ncomp > 128 * B3_MAX_CHUNKS) return -1;
         const unsigned grid = (unsigned)((N + 127) / 128);
-        if (ncomp == 1) k_leaves_wide<1><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
-        else if (ncomp == 2) k_leaves_wide<2><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
-        else k_leaves_wide<3><<<grid, 128, 0, st>>>(planes, N, depth, nodes);
+        if (ncomp == 1) k_leaves_wide<1><<<grid, 128, 0, st>>>(planes, N, depth, nodes, logN, perm_log_e);
+        else if (ncomp == 2) k_leaves_wide<2><<<grid, 128, 0, st>>>(planes, N, depth, nodes, logN, perm_log_e);
+        else k_leaves_wide<3><<<grid, 128, 0, st>>>(planes, N, depth, nodes, logN, perm_log_e);
         count_launches(1);
         return 0;
     }
     const dim3 grid((unsigned)((N + 255) / 256), count);
     if (hash == HASH_SHA256) {
-        if (ncomp == 1) k_leaves<1, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
-        else if (ncomp == 2) k_leaves<2, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
-        else k_leaves<3, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+        if (ncomp == 1) k_leaves<1, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride, logN, perm_log_e);
+        else if (ncomp == 2) k_leaves<2, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride, logN, perm_log_e);
+        else k_leaves<3, HASH_SHA256><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride, logN, perm_log_e);
     } else {
-        if (ncomp == 1) k_leaves<1, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
-        else if (ncomp == 2) k_leaves<2, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
-        else k_leaves<3, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride);
+        if (ncomp == 1) k_leaves<1, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride, logN, perm_log_e);
+        else if (ncomp == 2) k_leaves<2, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride, logN, perm_log_e);
+        else k_leaves<3, HASH_BLAKE3><<<grid, 256, 0, st>>>(planes, N, depth, nodes, plane_stride, node_stride, logN, perm_log_e);
     }
     count_launches(1);
     return 0;
 }
 
-int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, int hash, cudaStream_t st) {
-    return launch_leaves_batch(planes, N, depth, ncomp, nodes, 1, 0, 0, hash, st);
+int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, int hash, cudaStream_t st,
+                  u32 perm_log_e) {
+    return launch_leaves_batch(planes, N, depth, ncomp, nodes, 1, 0, 0, hash, st, perm_log_e);
 }
 
 // One CTA hashes a subtree of height `levels` whose children sit at level

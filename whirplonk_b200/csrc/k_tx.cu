@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
                 const u64 qi = x / ((u64)a.depth * a.ncomp);
                 const u64 rem = x - qi * a.depth * a.ncomp;
                 const u32 el = (u32)(rem / a.ncomp), c = (u32)(rem % a.ncomp);
-                const u64 v = planes[((u64)c * a.depth + el) * a.N + idx_s[qi]];
+                const u64 v = planes[((u64)c * a.depth + el) * a.N + codeword_row(idx_s[qi], a.logN, a.perm_log_e)];
                 unsigned char* dst = hb + 8 + qi * row_bytes + (u64)el * esz + 8ull * c;
                 for (int k = 0; k < 8; ++k) dst[k] = (unsigned char)(v >> (8 * k));
             }
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
         const u32 total = nwit * a.depth;
         const u32 nwarps = blockDim.x >> 5;
         for (u32 i = warp; i < q; i += nwarps) {
-            const u64 id = idx_s[i];
+            const u64 id = codeword_row(idx_s[i], a.logN, a.perm_log_e);  // natural row = exponent of its point
             E3 val = e3_zero();
             for (u32 k = lane; k < total; k += 32) {
                 const u32 w = k / a.depth, el = k - w * a.depth;

@@ -71,11 +71,14 @@ int sumcheck_prepare();
 // Leaf i = BLAKE3 of row i (LE bytes of `depth` elements of `ncomp` words),
 // written to nodes[i].  Rows are gathered from the codeword planes.
 // hash: 0 = BLAKE3, 1 = SHA-256 (the engine a configuration's hash_id selects).
-int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, int hash, cudaStream_t st);
+// perm_log_e > 0: coset-major rows -- leaf k hashes natural row
+// (k >> (logN - perm_log_e)) + ((k mod 2^(logN - perm_log_e)) << perm_log_e).
+int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, int hash, cudaStream_t st,
+                  u32 perm_log_e = 0);
 // `count` independent matrices: planes and node arrays `plane_stride` /
 // `node_stride` words apart.
 int launch_leaves_batch(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, u32 count, u64 plane_stride,
-                        u64 node_stride, int hash, cudaStream_t st);
+                        u64 node_stride, int hash, cudaStream_t st, u32 perm_log_e = 0);
 // Builds all Merkle levels above the leaves of a 2^logN-leaf tree in `nodes`
 // ([leaves | level 1 | ... | root], 8 words per node).  The CTA that computes
 // the root also performs the transcript step of irs_commit::commit
@@ -145,6 +148,7 @@ struct OpenArgs {
     int ood_offset;
     int r_offset;       // sc->sc_r[r_offset .. r_offset + fold) are the folding randomness
     u32 fold;           // number of folding variables (2^fold columns per vector)
+    u32 perm_log_e;     // coset-major rows (see launch_leaves); 0 = natural order
 };
 int launch_open(const OpenArgs& a, cudaStream_t st);
 // STIR combination (whir_prover.hpp:283-336): copy the new commitment's OOD

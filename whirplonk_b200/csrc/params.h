@@ -28,6 +28,12 @@ struct ProtocolParams {  // whir::ProtocolParameters (cpp/include/whir/parameter
     // (field_size_bits 192), 2 for Basefield<GoldilocksExt2> (128), 1 for
     // Identity<Goldilocks> (64).
     int field_degree = 3;
+    // Codeword row order (not a ProtocolParameters field either): 0 natural, as
+    // the C++ reference commits (mod_ntt.hpp:49-130); 1 coset-major, as the
+    // Rust crate commits without its rs_in_order feature
+    // (rust/src/algebra/ntt/cooley_tukey.rs:375-480): committed row k is the
+    // natural row k / m + (k mod m) N / m for message length m.
+    int coset_major = 0;
 };
 
 struct IrsSchedule {

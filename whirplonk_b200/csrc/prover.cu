@@ -92,6 +92,7 @@ ProofPlan make_plan(const WhirSchedule& sched, const ProtocolParams& params, int
         CommitBuffers cb;
         cb.N = c.codeword_length;
         cb.logN = ilog2(cb.N);
+        if (params.coset_major) cb.perm_log_e = cb.logN - ilog2(c.message_length());
         cb.depth = row_elems;
         cb.ncomp = ncomp;
         tmp_words = std::max(tmp_words, (size_t)cb.N * cb.depth * ncomp);
@@ -228,7 +229,8 @@ int commit_vectors(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t 
     L.tw_lo = c.tw.tw_lo;
     WG_TIMED(c, FAM_NTT, launch_lde(L, c.st));
     uint32_t* nodes = reinterpret_cast<uint32_t*>(c.ws + cb.nodes);
-    WG_TIMED(c, FAM_LEAF, launch_leaves(c.w(cb.planes), cb.N, cb.depth, ncomp, nodes, c.p.params.hash, c.st));
+    WG_TIMED(c, FAM_LEAF, launch_leaves(c.w(cb.planes), cb.N, cb.depth, ncomp, nodes, c.p.params.hash, c.st,
+                                        cb.perm_log_e));
     WG_TIMED(c, FAM_MERKLE, launch_merkle(nodes, cb.logN, c.tx(), c.sc(), ci, n_ood, c.p.params.hash, c.st));
     OodArgs o{};
     for (int k = 0; k < 3; ++k) o.v[k] = src[k] ? src[k] : src[0];
@@ -448,6 +450,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         oa.ncomp = pb.ncomp;
         oa.q = (uint32_t)prev.in_domain;
         oa.gen = gl_pow_host(7, (GL_P - 1) / pb.N);  // w_N = 7^((p-1)/N)
+        oa.perm_log_e = pb.perm_log_e;
         oa.stir = 1;
         oa.use_vrlc = r == 0 && V > 1;
         oa.ood_offset = (int)rc.irs.out_domain;
@@ -491,6 +494,7 @@ int enqueue_prove(const ProofPlan& p, char* ws, const DeviceTables& tw, cudaStre
         oa.q = (uint32_t)last.in_domain;
         oa.gen = 1;
         oa.stir = 0;
+        oa.perm_log_e = lb.perm_log_e;
         WG_TIMED(c, FAM_OPEN, launch_open(oa, st));
     }
     if (s.final_sumcheck.num_rounds > 0) WG_TRY(sumcheck(c, s.final_sumcheck, vsize, false, r_slot, false));

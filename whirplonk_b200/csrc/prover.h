@@ -22,6 +22,7 @@ struct ProofScalars;
 struct CommitBuffers {
     uint64_t N = 0;
     uint32_t logN = 0, depth = 0, ncomp = 0;
+    uint32_t perm_log_e = 0;  // coset-major rows: log2(N / message length); 0 = natural order
     size_t planes = 0, nodes = 0;  // byte offsets in the workspace
 };
 

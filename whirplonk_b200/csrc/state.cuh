@@ -21,6 +21,15 @@ constexpr int MAX_COMMITS = 32;     // initial + round commitments
 constexpr int MAX_DEPTH = 64;       // interleaving depth 2^k
 constexpr int MAX_INIT_OOD = MAX_WITNESSES * MAX_OOD;
 
+// Natural row of committed row k: k itself, or with coset-major rows of
+// message length 2^log_m and 2^log_e cosets, k / 2^log_m + (k mod 2^log_m) 2^log_e
+// (transpose_permute, rust/src/algebra/ntt/transpose.rs:10-15).
+__host__ __device__ __forceinline__ u64 codeword_row(u64 k, u32 logN, u32 log_e) {
+    if (!log_e) return k;
+    const u32 log_m = logN - log_e;
+    return (k >> log_m) + ((k & ((1ull << log_m) - 1)) << log_e);
+}
+
 struct ProofScalars {
     E3 sum;                                  // claimed <vector, covector>
     E3 c0, c2;                               // current sumcheck round polynomial

@@ -506,6 +506,8 @@ whirgpu_status whirgpu_zk_commit(whirgpu_ctx* c, const whirgpu_zk_config* cfg, c
         return zk_fail(c, WHIRGPU_E_INVALID, "null argument");
     *out = nullptr;
     if (rng_domain_len > ZK_RNG_MAX_DOMAIN) return zk_fail(c, WHIRGPU_E_INVALID, "rng domain above 128 bytes");
+    if (c->codeword_order != WHIRGPU_ORDER_NATURAL)
+        return zk_fail(c, WHIRGPU_E_UNSUPPORTED, "zero-knowledge commitments use the natural codeword order");
     const uint64_t npolys = cfg->num_polynomials, n = cfg->num_witness_variables, ell = cfg->num_blinding_variables;
     if (cfg->blinded.field != WHIRGPU_FIELD_GOLDILOCKS1 || cfg->blinding.field != WHIRGPU_FIELD_GOLDILOCKS1)
         return zk_fail(c, WHIRGPU_E_INVALID, "zero-knowledge configs are over Identity<Goldilocks>");

@@ -108,6 +108,13 @@ class Context:
         except Exception:
             pass
 
+    ORDER_NATURAL, ORDER_COSET_MAJOR = 0, 1
+
+    def set_codeword_order(self, order: int):
+        """Codeword row order of later commitments: ORDER_NATURAL (the C++
+        reference) or ORDER_COSET_MAJOR (the Rust crate without rs_in_order)."""
+        _lib.check(self._L.whirgpu_set_codeword_order(self.handle, int(order)), self.handle)
+
     @property
     def stream(self) -> int:
         return self._L.whirgpu_stream(self.handle) or 0
