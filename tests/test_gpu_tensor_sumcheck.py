@@ -56,11 +56,13 @@ def test_tensor_initial_sumcheck_unique_decoding(gpu_ctx, oracle):
 
 
 def test_tensor_initial_sumcheck_base_field_target(gpu_ctx, oracle):
-    """Identity<Goldilocks>: every term and challenge in the base field."""
-    n, k, rho = 13, 4, 1
-    p = ProtocolParameters.cli(security_level=100, pow_bits=20, folding_factor=k, log_inv_rate=rho)
-    coeffs, points, evals = _case(gpu_ctx, n, 1, 4400, base_points=True)
+    """Identity<Goldilocks>: every term and challenge in the base field.  Over the
+    64-bit field the derived PoW bits grow with the security level, so the level is
+    kept low enough for the grinds to stay short (as in test_gpu_field1)."""
+    n, k, rho, sec, pb = 13, 4, 1, 36, 12
+    p = ProtocolParameters.cli(security_level=sec, pow_bits=pb, folding_factor=k, log_inv_rate=rho)
+    coeffs, points, evals = _case(gpu_ctx, n, 2, 4400, base_points=True)
     narg, hints, _ = prove_once(n, p, coeffs, points, evals, ctx=gpu_ctx, target_field=FIELD_GOLDILOCKS1)
-    forms = [("mle", points[0])]
-    onarg, ohints = oracle.prove_forms(n, k, rho, 100, 20, forms, coeffs, evals, field1=True)
+    forms = [("mle", points[i]) for i in range(2)]
+    onarg, ohints = oracle.prove_forms(n, k, rho, sec, pb, forms, coeffs, evals, field1=True)
     assert narg == onarg and hints == ohints

@@ -103,15 +103,24 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
     const u32 nblocks = (bytes + 63) / 64;
     unsigned cv[8];
     b3_init(cv);
+    // The next block's 8 words are loaded before this block is compressed, so
+    // their plane reads overlap the compression.
+    u64 nxt[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) nxt[q] = (u32)q < nwords ? row_word<NCOMP>(planes, N, depth, i, q) : 0;
     for (u32 t = 0; t < nblocks; ++t) {
         unsigned m[16];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const u32 w = t * 8 + q;
-            u64 v = 0;
-            if (w < nwords) v = row_word<NCOMP>(planes, N, depth, i, w);
-            m[2 * q] = (unsigned)v;
-            m[2 * q + 1] = (unsigned)(v >> 32);
+            m[2 * q] = (unsigned)nxt[q];
+            m[2 * q + 1] = (unsigned)(nxt[q] >> 32);
+        }
+        if (t + 1 < nblocks) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const u32 w = (t + 1) * 8 + q;
+                nxt[q] = w < nwords ? row_word<NCOMP>(planes, N, depth, i, w) : 0;
+            }
         }
         const u32 len = (t + 1 == nblocks) ? bytes - 64 * t : 64;
         const unsigned flags = (t == 0 ? B3_CHUNK_START : 0u) | (t + 1 == nblocks ? (B3_CHUNK_END | B3_ROOT) : 0u);
@@ -308,13 +317,19 @@ __global__ void __launch_bounds__(256) k_merkle8(u32* nodes, u32 logN, u32 level
     const u64 o1 = level_offset(logN, level_in + 1) + 4 * g;
     const u64 o2 = level_offset(logN, level_in + 2) + 2 * g;
     const u64 o3 = level_offset(logN, level_in + 3) + g;
-    unsigned m[16], p0[8], p1[8], q0[8], q1[8];
-    load_node(nodes, in + 0, m); load_node(nodes, in + 1, m + 8); hash64<H>(m, p0); store_node(nodes, o1 + 0, p0);
-    load_node(nodes, in + 2, m); load_node(nodes, in + 3, m + 8); hash64<H>(m, p1); store_node(nodes, o1 + 1, p1);
+    // Each pair of children is loaded one hash ahead (ma / mb alternate), so the
+    // node reads overlap the compressions.
+    unsigned ma[16], mb[16], p0[8], p1[8], q0[8], q1[8];
+    load_node(nodes, in + 0, ma); load_node(nodes, in + 1, ma + 8);
+    load_node(nodes, in + 2, mb); load_node(nodes, in + 3, mb + 8);
+    hash64<H>(ma, p0); store_node(nodes, o1 + 0, p0);
+    load_node(nodes, in + 4, ma); load_node(nodes, in + 5, ma + 8);
+    hash64<H>(mb, p1); store_node(nodes, o1 + 1, p1);
+    load_node(nodes, in + 6, mb); load_node(nodes, in + 7, mb + 8);
     parent_cv<H>(p0, p1, q0);
     store_node(nodes, o2 + 0, q0);
-    load_node(nodes, in + 4, m); load_node(nodes, in + 5, m + 8); hash64<H>(m, p0); store_node(nodes, o1 + 2, p0);
-    load_node(nodes, in + 6, m); load_node(nodes, in + 7, m + 8); hash64<H>(m, p1); store_node(nodes, o1 + 3, p1);
+    hash64<H>(ma, p0); store_node(nodes, o1 + 2, p0);
+    hash64<H>(mb, p1); store_node(nodes, o1 + 3, p1);
     parent_cv<H>(p0, p1, q1);
     store_node(nodes, o2 + 1, q1);
     parent_cv<H>(q0, q1, p0);

@@ -154,12 +154,13 @@ int launch_pow_grind_only(ProofScalars* sc, u64 threshold, int hash, cudaStream_
     const double expect = threshold == 0 ? 1.8446744073709552e19 : 18446744073709551616.0 / (double)threshold;
     const u64 limit = expect * 64.0 >= (double)POW_NONCE_LIMIT ? POW_NONCE_LIMIT : (u64)(expect * 64.0) + 1;
     // Every CTA finishes the chunk it holds when the minimum turns up, so the
-    // work past the answer is about one chunk per CTA: the grid is sized to
-    // keep that below a quarter of the expected search (at least 16 CTAs,
-    // at most POW_CTAS_PER_SM per SM).  The answer does not depend on it.
+    // work past the answer is about one chunk per CTA: a search expected to be
+    // short gets one CTA per SM (the latency of a proof alone stays that of a
+    // full grid), a long one up to POW_CTAS_PER_SM per SM.  The answer does not
+    // depend on the grid.
     const double want = expect / (4.0 * POW_CHUNK);
-    const unsigned cap = POW_CTAS_PER_SM * device_sms();
-    const unsigned grid = want >= (double)cap ? cap : (want <= 16.0 ? 16u : (unsigned)want);
+    const unsigned sms = device_sms(), cap = POW_CTAS_PER_SM * sms;
+    const unsigned grid = want >= (double)cap ? cap : (want <= (double)sms ? sms : (unsigned)want);
     if (hash == 1) k_pow_search<1><<<grid, POW_THREADS, 0, st>>>(sc, threshold, limit);
     else k_pow_search<0><<<grid, POW_THREADS, 0, st>>>(sc, threshold, limit);
     count_launches(1);
