@@ -683,6 +683,7 @@ def family_roofline(ctx, inputs, shapes):
     roof_sc = {"bound": "hbm", "kernel": "sumcheck + covector", "achieved": sc_ach, "peak": peak, "unit": "GB/s",
                "frac": sc_ach / peak if sc_ach else None, "peak_source": peak_kind,
                "algorithmic_bytes_per_proof": alg["sumcheck"] / per, "ms_per_proof": sc_ms / per,
+               "traffic": read_traffic("sumcheck", alg["sumcheck"] / per),
                "bytes_note": "per round on size s: (8 or 24) s + 24 s read, 2 x 24 s/2 written (a and the covector)"}
     extra = {"roofline_sumcheck": roof_sc}
     pk = measure_int_peaks(ctx.device)
