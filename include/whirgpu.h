@@ -60,8 +60,11 @@ typedef struct whirgpu_witness whirgpu_witness;
 
 /* ---- context ---------------------------------------------------------------
  * One CUDA device, one stream, a workspace cache bounded by hbm_budget bytes
- * (0 = no bound).  Replaces the reference's GpuPool singleton
- * (cpp/cuda/cuda_integration.hpp:142-282). */
+ * (0 = no bound).  Twiddle tables sit outside the bound: a few KiB of root
+ * powers, plus one table of the inter-pass NTT factors per LDE split in use
+ * (2^logN words, at most 128 MiB each, built on the first proof of a shape
+ * and only while it fits under a nonzero bound).  Replaces the reference's
+ * GpuPool singleton (cpp/cuda/cuda_integration.hpp:142-282). */
 whirgpu_status whirgpu_ctx_create(int device, uint64_t hbm_budget, whirgpu_ctx** out);
 void whirgpu_ctx_destroy(whirgpu_ctx* ctx);
 const char* whirgpu_last_error(const whirgpu_ctx* ctx);

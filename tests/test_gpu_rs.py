@@ -44,6 +44,18 @@ def test_rs_commit_roots_at_kernel_level_sizes(gpu_ctx, oracle, log_len, log_exp
         assert roots[k] == oracle.rs_commit_root(v[k], N, 16), f"vector {k}"
 
 
+@pytest.mark.parametrize("log_len,log_exp,count", [(8, 12, 2), (10, 14, 1), (12, 8, 3), (9, 10, 2), (6, 16, 1)])
+def test_rs_commit_roots_high_expansion(gpu_ctx, oracle, log_len, log_exp, count):
+    """Expansions 2^8 .. 2^16: the message fits one row of the second pass, so
+    the first pass is skipped and the last one applies the inter-pass factors
+    to the message itself; roots equal the oracle's."""
+    v = sample_goldilocks(7700 + 31 * log_len + log_exp, count << log_len).reshape(count, -1)
+    roots = rs_commit_batch(gpu_ctx, v, log_exp)
+    N = ((1 << log_len) // 16) << log_exp
+    for k in range(count):
+        assert roots[k] == oracle.rs_commit_root(v[k], N, 16), f"vector {k}"
+
+
 def test_rs_encode_planes_match_oracle(gpu_ctx, oracle):
     import torch
 

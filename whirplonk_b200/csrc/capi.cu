@@ -188,6 +188,18 @@ whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_param
     return acquire_workspace_sched(c, sched, to_params(params), ds_len, out, cap, nwit);
 }
 
+// The inter-pass twiddle tables of every LDE split `plan` launches (built once
+// per context and split, before any proof of the plan is enqueued or captured).
+// Like the other twiddle tables they sit outside the workspace budget; under a
+// budget a table is only built while it fits beside the workspaces, else the
+// passes generate their factors.
+void prepare_lde_tables(whirgpu_ctx* c, const ProofPlan& plan) {
+    for (const CommitBuffers& cb : plan.commits) {
+        const uint64_t room = c->budget ? (c->budget > c->allocated ? c->budget - c->allocated : 0) : ~0ull;
+        lde_tables_prepare(c->lde_tables, cb.logN, cb.logX, c->tw.tw_hi, c->tw.tw_lo, c->stream, room);
+    }
+}
+
 whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched, const ProtocolParams& pp_in,
                                        size_t ds_len, Workspace** out, uint64_t cap, uint32_t nwit) {
     ProtocolParams pp = pp_in;
@@ -200,6 +212,7 @@ whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched
     }
     const std::string key = plan_key(sched, pp, ds_len, nwit);
     std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+    prepare_lde_tables(c, plan);
     for (Workspace* w : c->cache[key])
         if (!w->busy) {
             w->busy = true;
@@ -284,6 +297,7 @@ whirgpu_status whirgpu_ctx_create(int device, uint64_t hbm_budget, whirgpu_ctx**
     WG_CUDA(nullptr, cudaMemcpy(c->tw.tw_stage, st.data(), st.size() * 8, cudaMemcpyHostToDevice), "upload");
     WG_CUDA(nullptr, cudaMemcpy(c->tw.tw_hi, hi.data(), hi.size() * 8, cudaMemcpyHostToDevice), "upload");
     WG_CUDA(nullptr, cudaMemcpy(c->tw.tw_lo, lo.data(), lo.size() * 8, cudaMemcpyHostToDevice), "upload");
+    c->tw.lde = &c->lde_tables;
     *out = c.release();
     return WHIRGPU_OK;
 }
@@ -306,6 +320,7 @@ void whirgpu_ctx_destroy(whirgpu_ctx* c) {
     cudaFree(c->tw.tw_stage);
     cudaFree(c->tw.tw_hi);
     cudaFree(c->tw.tw_lo);
+    lde_tables_free(c->lde_tables);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->mle_scratch) cudaFree(c->mle_scratch);
     if (c->kscratch) cudaFree(c->kscratch);

@@ -90,6 +90,7 @@ struct whirgpu_ctx {
     uint64_t budget = 0;
     uint64_t allocated = 0;
     wg::DeviceTables tw;
+    wg::LdeTables lde_tables;  // inter-pass twiddle factors of the LDE splits in use (tw.lde)
     std::string err;
     // Workspaces by plan shape: the schedule, hash engine, vector layout, field
     // degree and domain-separator length, serialised (plan_key).
@@ -143,6 +144,9 @@ whirgpu_status acquire_workspace(whirgpu_ctx* c, uint64_t n, const whirgpu_param
 whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched, const ProtocolParams& pp, size_t ds_len,
                                        Workspace** out, uint64_t cap = 0, uint32_t nwit = 1);
 void release_workspace(whirgpu_ctx* c, Workspace* w);
+// Builds the context's inter-pass twiddle tables for the LDEs of `plan` (once
+// per split; within the HBM budget).  Call outside any graph capture.
+void prepare_lde_tables(whirgpu_ctx* c, const ProofPlan& plan);
 // While set, kernel launches of this thread are stream-captured, not run: the
 // launch counter skips them and graph launches add their kernel-node counts.
 void set_capturing(bool on);

@@ -121,6 +121,41 @@ __device__ __forceinline__ u64 gl_mul(u64 a, u64 b) {
     asm("mul.lo.u64 %0, %2, %3;\n\tmul.hi.u64 %1, %2, %3;" : "=l"(lo), "=l"(hi) : "l"(a), "l"(b));
     return gl_reduce_dev(lo, hi);
 }
+// The same reduction with its add-carry corrections moved to the FMA pipe: the
+// carry c of an add becomes `mad.wide.u32 s, c, EPS, s` (s + c EPS cannot wrap
+// there), and hl * EPS one wide multiply.  Bit-identical to gl_reduce_dev; it
+// trades ~4 ALU-pipe instructions for ~3 FMA-pipe ones, which pays in kernels
+// whose ALU pipe is the bottleneck while the FMA pipe idles (the NTT passes).
+__device__ __forceinline__ u64 gl_reduce_fma(u64 lo, u64 hi) {
+    u64 s;
+    asm("{\n\t.reg .u32 l0, l1, h0, h1, t0, t1, m, c;\n\t.reg .u64 t, u;\n\t"
+        "mov.b64 {l0, l1}, %1;\n\t"
+        "mov.b64 {h0, h1}, %2;\n\t"
+        // t = lo - hh ; on borrow subtract EPS
+        "sub.cc.u32 t0, l0, h1;\n\t"
+        "subc.cc.u32 t1, l1, 0;\n\t"
+        "subc.u32 m, 0, 0;\n\t"
+        "sub.cc.u32 t0, t0, m;\n\t"
+        "subc.u32 t1, t1, 0;\n\t"
+        "mov.b64 t, {t0, t1};\n\t"
+        // s = t + hl * EPS ; on carry add EPS
+        "mul.wide.u32 u, h0, 0xFFFFFFFF;\n\t"
+        "add.cc.u64 %0, t, u;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "mad.wide.u32 %0, c, 0xFFFFFFFF, %0;\n\t"
+        // canonical: s >= p  <=>  s + EPS carries; then s + EPS (mod 2^64) = s - p
+        "add.cc.u64 t, %0, 0xFFFFFFFF;\n\t"
+        "addc.u32 c, 0, 0;\n\t"
+        "mad.wide.u32 %0, c, 0xFFFFFFFF, %0;\n\t}"
+        : "=l"(s)
+        : "l"(lo), "l"(hi));
+    return s;
+}
+__device__ __forceinline__ u64 gl_mul_fma(u64 a, u64 b) {
+    u64 lo, hi;
+    asm("mul.lo.u64 %0, %2, %3;\n\tmul.hi.u64 %1, %2, %3;" : "=l"(lo), "=l"(hi) : "l"(a), "l"(b));
+    return gl_reduce_fma(lo, hi);
+}
 __host__ __forceinline__ u64 gl_mul_host(u64 a, u64 b) {
     unsigned __int128 x = (unsigned __int128)a * b;
     return gl_reduce((u64)x, (u64)(x >> 64));

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <utility>
 
 #include "launch.h"
 #include "gl.cuh"
@@ -26,57 +27,116 @@ namespace wg {
 
 __device__ __forceinline__ u32 bitrev(u32 j, u32 bits) { return bits ? (__brev(j) >> (32 - bits)) : 0; }
 
+// Global words a pass only reads (the message, the previous pass's scratch,
+// the inter-pass tables) go through the read-only path, so the compiler may
+// issue a batch of them ahead of the stores that follow.
+__device__ __forceinline__ u64 ldg64(const u64* p) { return __ldg(reinterpret_cast<const unsigned long long*>(p)); }
+// Loads and stores of the load and store phases go in batches of NTT_BATCH
+// per thread: all loads of a batch are in flight before the first store.
+constexpr int NTT_BATCH = 8;
+
 // Shared-memory word of column element e: one pad word every 32 words keeps
 // strided group accesses off a single bank; the extra word per column puts the
 // W columns of a tile on different banks (the transposed store phase reads
 // one element of each column per step).
 __device__ __forceinline__ u32 pidx(u32 e) { return e + (e >> 5); }
-__host__ __device__ __forceinline__ u32 col_stride(u32 logR) { return (1u << logR) + ((1u << logR) >> 5) + 1; }
+__host__ __device__ constexpr u32 col_stride(u32 logR) { return (1u << logR) + ((1u << logR) >> 5) + 1; }
 
-// Stages s0+1 .. s0+RR of a radix-2 DIT on W bit-reversed columns of 2^L
-// words, done as independent radix-2^RR groups in registers: a group is the
-// 2^RR elements base + j 2^s0 (j < 2^RR) of one column, and the butterflies of
-// stage s pair j with j + 2^(t-1) (t = s - s0) under the twiddle
-// w_{2^s}^(lo + (j mod 2^(t-1)) 2^s0), lo = base mod 2^s0.
+// Stages s0+1 .. s0+RR of a radix-2 DIT on the 2^logW bit-reversed columns of
+// 2^L words, done as independent radix-2^RR groups in registers: a group is
+// the 2^RR elements base + j 2^s0 (j < 2^RR) of one column, and the
+// butterflies of stage s pair j with j + 2^(t-1) (t = s - s0) under the twiddle
+// w_{2^s}^(lo + c 2^s0), c = j mod 2^(t-1), lo = base mod 2^s0.
+//
+// L is a compile-time constant, so the twiddle of (t, c) is read at
+// tws[(lo << (L - s0)) >> t] plus the constant offset c << (L - t).  Word j of
+// the group sits at pidx(base) + j 2^s0 + floor(j 2^s0 / 32): the group's
+// 2^(s0 + RR)-word span never straddles a pad word except at the multiples
+// of 32 its own steps cross.  That offset is a compile-time constant when s0
+// is (S0C >= 0: the first group of a column, s0 = 0, and the second, s0 = 4),
+// a uniform stride for s0 >= 5, and computed per word only for 1 <= s0 <= 3.
 // S0ZERO: the group starts at stage 1 (s0 = 0), so lo = 0 and the butterflies
-// with j mod 2^(t-1) = 0 have the twiddle w^0 = 1: their multiply is skipped
-// (all of stage 1, half of stage 2, ...).
-template <int RR, bool S0ZERO>
-__device__ __forceinline__ void dit_group_pass(u64* sm, u32 W, u32 L, u32 s0, const u64* tws) {
+// with c = 0 have the twiddle w^0 = 1: their multiply is skipped (all of stage
+// 1, half of stage 2, ...).
+template <int RR, bool S0ZERO, int L, int S0C = -1>
+__device__ __forceinline__ void dit_group(u64* sm, u32 logW, u32 s0_rt, const u64* tws) {
     constexpr int G = 1 << RR;
-    const u32 gpc_log = L - RR;  // groups per column (log2)
-    const u32 total = W << gpc_log;
-    const u32 cs = col_stride(L);
+    constexpr u32 gpc_log = L - RR;  // groups per column (log2)
+    constexpr u32 cs = col_stride(L);
+    const u32 s0 = S0ZERO ? 0u : (S0C >= 0 ? (u32)S0C : s0_rt);
+    const u32 total = 1u << (logW + gpc_log);
+    const bool wide = !S0ZERO && S0C < 0 && s0 >= 5;
+    constexpr u32 SC = S0C < 0 ? 0 : (u32)S0C;
+    const u32 D = wide ? (1u << s0) + (1u << (s0 - 5)) : 0u;
     for (u32 g = threadIdx.x; g < total; g += blockDim.x) {
         const u32 w = g >> gpc_log;
         const u32 gb = g & ((1u << gpc_log) - 1);
         const u32 lo = S0ZERO ? 0u : (gb & ((1u << s0) - 1));
         const u32 base = S0ZERO ? (gb << RR) : lo + ((gb >> s0) << (s0 + RR));
         u64* col = sm + w * cs;
+        u64* p0 = col + pidx(base);
         u64 x[G];
 #pragma unroll
-        for (int j = 0; j < G; ++j) x[j] = col[pidx(base + ((u32)j << s0))];
+        for (int j = 0; j < G; ++j) {
+            if (S0ZERO) x[j] = p0[j];
+            else if (S0C >= 0) x[j] = p0[(j << SC) + ((j << SC) >> 5)];
+            else if (wide) x[j] = p0[j * D];
+            else x[j] = col[pidx(base + ((u32)j << s0))];
+        }
+        const u32 X = S0ZERO ? 0u : (lo << (L - s0));
 #pragma unroll
         for (int t = 1; t <= RR; ++t) {
             const int half = 1 << (t - 1);
-            const u32 sh = L - (s0 + t);
+            const u64* twt = tws + (X >> t);
 #pragma unroll
             for (int j = 0; j < G; ++j) {
                 if (j & half) continue;
+                const int c = j & (half - 1);
                 const u64 u = x[j];
                 u64 v;
-                if (S0ZERO && (j & (half - 1)) == 0) {
+                if (S0ZERO && c == 0) {
                     v = x[j + half];
                 } else {
-                    const u64 tw = tws[(lo + ((u32)(j & (half - 1)) << s0)) << sh];
-                    v = gl_mul(x[j + half], tw);
+                    v = gl_mul_fma(x[j + half], twt[(u32)c << (L - t)]);
                 }
                 x[j] = gl_add(u, v);
                 x[j + half] = gl_sub(u, v);
             }
         }
 #pragma unroll
-        for (int j = 0; j < G; ++j) col[pidx(base + ((u32)j << s0))] = x[j];
+        for (int j = 0; j < G; ++j) {
+            if (S0ZERO) p0[j] = x[j];
+            else if (S0C >= 0) p0[(j << SC) + ((j << SC) >> 5)] = x[j];
+            else if (wide) p0[j * D] = x[j];
+            else col[pidx(base + ((u32)j << s0))] = x[j];
+        }
+    }
+}
+
+// Stages s0+1 .. L in register groups of up to 16, natural-order output.
+template <int L>
+__device__ __forceinline__ void dit_stages(u64* sm, u32 logW, u32 s0, const u64* tws) {
+    while (s0 < (u32)L) {
+        const u32 left = L - s0;
+        const u32 rr = left >= 8 ? 4 : (left > 4 ? (left + 1) / 2 : left);
+        if (s0 == 0) {
+            if constexpr (L >= 4) { if (rr == 4) dit_group<4, true, L>(sm, logW, s0, tws); }
+            if constexpr (L >= 3) { if (rr == 3) dit_group<3, true, L>(sm, logW, s0, tws); }
+            if constexpr (L >= 2) { if (rr == 2) dit_group<2, true, L>(sm, logW, s0, tws); }
+            if (rr == 1) dit_group<1, true, L>(sm, logW, s0, tws);
+        } else if (s0 == 4) {
+            if constexpr (L >= 8) { if (rr == 4) dit_group<4, false, L, 4>(sm, logW, s0, tws); }
+            if constexpr (L >= 7) { if (rr == 3) dit_group<3, false, L, 4>(sm, logW, s0, tws); }
+            if constexpr (L >= 6) { if (rr == 2) dit_group<2, false, L, 4>(sm, logW, s0, tws); }
+            if constexpr (L >= 5) { if (rr == 1) dit_group<1, false, L, 4>(sm, logW, s0, tws); }
+        } else {
+            if constexpr (L >= 4) { if (rr == 4) dit_group<4, false, L>(sm, logW, s0, tws); }
+            if constexpr (L >= 3) { if (rr == 3) dit_group<3, false, L>(sm, logW, s0, tws); }
+            if constexpr (L >= 2) { if (rr == 2) dit_group<2, false, L>(sm, logW, s0, tws); }
+            if (rr == 1) dit_group<1, false, L>(sm, logW, s0, tws);
+        }
+        s0 += rr;
+        __syncthreads();
     }
 }
 
@@ -88,22 +148,23 @@ __device__ __forceinline__ u64 twiddle(u64 e, u32 logM, const u64* hi, const u64
 
 // One pass over all planes (blockIdx.y = plane).  MINB = CTAs per SM the
 // register allocation is sized for (the pass plan picks the variant).
-template <int MINB>
+template <int MINB, int L>
 __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     extern __shared__ u64 sm[];
-    const u32 logR = a.logR, R = 1u << logR, W = 1u << a.logW, halfR = R >> 1;
+    constexpr u32 logR = L, R = 1u << L;
+    constexpr u32 cs = col_stride(L);
+    const u32 W = 1u << a.logW;
     const u32 tileN = W << logR;
-    const u32 cs = col_stride(logR);
     u64* tws = sm + W * cs;
     const u32 plane = blockIdx.y;
     const u64 N = 1ull << a.logN;
     const bool first = a.pass == 0, last = a.pass + 1 == a.npass;
     const u32 comp = plane / a.depth, blk = plane % a.depth;
     const u64* src0 = comp == 0 ? a.src[0] : (comp == 1 ? a.src[1] : a.src[2]);  // no dynamic param indexing
-    const u64* src = first ? src0 + (u64)blk * a.m : nullptr;
+    const u64* src = first || a.twist ? src0 + (u64)blk * a.m : nullptr;
     u64* tmp = a.tmp + (u64)plane * N;
 
-    for (u32 u = threadIdx.x; u < halfR; u += blockDim.x) tws[u] = a.tw_stage[u << (TW_STAGE_LOG - logR)];
+    for (u32 u = threadIdx.x; u < R / 2; u += blockDim.x) tws[u] = a.tw_stage[u << (TW_STAGE_LOG - logR)];
 
     // Tile geometry.
     u64 S = 0, P = 0, col0 = 0;
@@ -132,34 +193,93 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     if (!last) {
         // Thread t always serves column w = t mod W; its rows advance by J.
         const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
-        const u32 nrows = 1u << mrows_log;
+        const u32 nrows = 1u << mrows_log, j0 = threadIdx.x >> a.logW;
         u64* col = sm + w * cs;
-        if (first) {
-            const u64 stride = (u64)J * S;
-            u64 idx = (u64)(threadIdx.x >> a.logW) * S + col0 + w;
-#pragma unroll 4
-            for (u32 j = threadIdx.x >> a.logW; j < nrows; j += J, idx += stride)
-                col[pidx(bitrev(j, logR))] = idx < a.m ? src[idx] : 0;
+        // Row 0 of this column.  The scratch of a middle pass is rewritten in
+        // place by this kernel, so it is read with plain loads.
+        const u64* p = first ? src + col0 + w : tmp + P * R * S + col0 + w;
+        const bool full = nrows % (NTT_BATCH * J) == 0 && (!first || ((u64)nrows << a.logS) <= a.m);
+        if (full && first) {
+            for (u32 jb = j0; jb < nrows; jb += NTT_BATCH * J) {
+                u64 v[NTT_BATCH];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) v[b] = ldg64(p + (u64)(jb + b * J) * S);
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) col[pidx(bitrev(jb + b * J, logR))] = v[b];
+            }
+        } else if (full) {
+            for (u32 jb = j0; jb < nrows; jb += NTT_BATCH * J) {
+                u64 v[NTT_BATCH];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) v[b] = p[(u64)(jb + b * J) * S];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) col[pidx(bitrev(jb + b * J, logR))] = v[b];
+            }
         } else {
-            const u64 stride = (u64)J * S;
-            const u64* p = tmp + (P * R + (threadIdx.x >> a.logW)) * S + col0 + w;
-#pragma unroll 4
-            for (u32 j = threadIdx.x >> a.logW; j < nrows; j += J, p += stride) col[pidx(bitrev(j, logR))] = *p;
+            for (u32 jb = j0; jb < nrows; jb += NTT_BATCH * J) {
+                u64 v[NTT_BATCH];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) {
+                    const u32 j = jb + b * J;
+                    const u64 idx = (u64)j * S;
+                    v[b] = j >= nrows || (first && idx + col0 + w >= a.m) ? 0 : first ? ldg64(p + idx) : p[idx];
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) {
+                    const u32 j = jb + b * J;
+                    if (j < nrows) col[pidx(bitrev(j, logR))] = v[b];
+                }
+            }
         }
     } else {
-        const u32 n = W << mrows_log;
-#pragma unroll 4
-        for (u32 e = threadIdx.x; e < n; e += blockDim.x) {
-            const u32 w = e >> mrows_log, j = e & ((1u << mrows_log) - 1);
-            u64 v;
-            if (first) {
-                v = j < a.m ? src[j] : 0;
-            } else {
-                const u64 i0 = i0base + w;
-                const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + i1;
-                v = tmp[(row << logR) + j];
+        const u32 n = W << mrows_log, jmask = (1u << mrows_log) - 1;
+        if (!first && !a.twist && n % (NTT_BATCH * blockDim.x) == 0) {
+            // The previous pass's rows, whole batches.
+            for (u32 eb = threadIdx.x; eb < n; eb += NTT_BATCH * blockDim.x) {
+                u64 v[NTT_BATCH];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) {
+                    const u32 e = eb + b * blockDim.x;
+                    const u64 i0 = i0base + (e >> mrows_log);
+                    const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + i1;
+                    v[b] = ldg64(tmp + (row << logR) + (e & jmask));
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) {
+                    const u32 e = eb + b * blockDim.x;
+                    sm[(e >> mrows_log) * cs + pidx(bitrev(e & jmask, logR))] = v[b];
+                }
             }
-            sm[w * cs + pidx(bitrev(j, logR))] = v;
+        } else {
+            for (u32 eb = threadIdx.x; eb < n; eb += NTT_BATCH * blockDim.x) {
+                u64 v[NTT_BATCH];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) {
+                    const u32 e = eb + b * blockDim.x;
+                    const u32 w = e >> mrows_log, j = e & jmask;
+                    v[b] = 0;
+                    if (e >= n) continue;
+                    if (first) {
+                        if (j < a.m) v[b] = ldg64(src + j);
+                    } else if (a.twist) {
+                        // Pass 0 would have broadcast message word j over its
+                        // column and scaled row `row` by w_N^(row j): done here.
+                        const u64 row = i0base + w;
+                        const u64 x = j < a.m ? ldg64(src + j) : 0;
+                        v[b] = gl_mul_fma(x, a.tw_pass ? ldg64(a.tw_pass + (row << logR) + j)
+                                                       : twiddle(row * j, a.logN, a.tw_hi, a.tw_lo));
+                    } else {
+                        const u64 i0 = i0base + w;
+                        const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + i1;
+                        v[b] = ldg64(tmp + (row << logR) + j);
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) {
+                    const u32 e = eb + b * blockDim.x;
+                    if (e < n) sm[(e >> mrows_log) * cs + pidx(bitrev(e & jmask, logR))] = v[b];
+                }
+            }
         }
     }
     __syncthreads();
@@ -182,41 +302,44 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     }
 
     // Decimation-in-time stages in register groups of up to 16, natural-order output.
-    for (u32 s0 = logE; s0 < logR;) {
-        const u32 left = logR - s0;
-        const u32 rr = left >= 8 ? 4 : (left > 4 ? (left + 1) / 2 : left);
-        if (s0 == 0) {
-            if (rr == 4) dit_group_pass<4, true>(sm, W, logR, s0, tws);
-            else if (rr == 3) dit_group_pass<3, true>(sm, W, logR, s0, tws);
-            else if (rr == 2) dit_group_pass<2, true>(sm, W, logR, s0, tws);
-            else dit_group_pass<1, true>(sm, W, logR, s0, tws);
-        } else {
-            if (rr == 4) dit_group_pass<4, false>(sm, W, logR, s0, tws);
-            else if (rr == 3) dit_group_pass<3, false>(sm, W, logR, s0, tws);
-            else if (rr == 2) dit_group_pass<2, false>(sm, W, logR, s0, tws);
-            else dit_group_pass<1, false>(sm, W, logR, s0, tws);
-        }
-        s0 += rr;
-        __syncthreads();
-    }
+    dit_stages<L>(sm, a.logW, logE, tws);
 
     // Store.
     if (!last) {
-        // Inter-pass twiddle w_{Ns}^(col i): thread t keeps col fixed and steps i
-        // by J, so the twiddle advances by the constant factor w_{Ns}^(col J).
-        const u32 logNs = logR + a.logS;  // size of the sub-transform this pass belongs to
+        // Inter-pass twiddle w_{Ns}^(col i) (Ns: the sub-transform this pass
+        // belongs to): read from the context's table, laid out like the tile
+        // rows, or else generated -- thread t keeps col fixed and steps i by J,
+        // so the factor advances by the constant w_{Ns}^(col J).
         const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
         const u64 col = col0 + w;
         u32 i = threadIdx.x >> a.logW;
-        u64 tw = twiddle(col * i, logNs, a.tw_hi, a.tw_lo);
-        const u64 step = twiddle(col * J, logNs, a.tw_hi, a.tw_lo);
         const u64 stride = (u64)J * S;
         u64* dst = tmp + (P * R + i) * S + col;
         const u64* scol = sm + w * cs;
+        if (a.tw_pass && R % (NTT_BATCH * J) == 0) {
+            const u64* tcol = a.tw_pass + (u64)i * S + col;
+            for (; i < R; i += NTT_BATCH * J, dst += NTT_BATCH * stride, tcol += NTT_BATCH * stride) {
+                u64 x[NTT_BATCH], f[NTT_BATCH];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) {
+                    x[b] = scol[pidx(i + b * J)];
+                    f[b] = ldg64(tcol + b * stride);
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) dst[b * stride] = gl_mul_fma(x[b], f[b]);
+            }
+        } else if (a.tw_pass) {
+            const u64* tcol = a.tw_pass + (u64)i * S + col;
+            for (; i < R; i += J, dst += stride, tcol += stride) *dst = gl_mul_fma(scol[pidx(i)], ldg64(tcol));
+        } else {
+            const u32 logNs = logR + a.logS;
+            u64 tw = twiddle(col * i, logNs, a.tw_hi, a.tw_lo);
+            const u64 step = twiddle(col * J, logNs, a.tw_hi, a.tw_lo);
 #pragma unroll 2
-        for (; i < R; i += J, dst += stride) {
-            *dst = gl_mul(scol[pidx(i)], tw);
-            tw = gl_mul(tw, step);
+            for (; i < R; i += J, dst += stride) {
+                *dst = gl_mul(scol[pidx(i)], tw);
+                tw = gl_mul(tw, step);
+            }
         }
     } else {
         u64* out = a.out + (u64)plane * N;
@@ -227,8 +350,17 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
         u32 i = threadIdx.x >> a.logW;
         u64* dst = out + obase + w + outer * i;
         const u64 stride = outer * J;
-#pragma unroll 4
-        for (; i < R; i += J, dst += stride) *dst = scol[pidx(i)];
+        if (R % (NTT_BATCH * J) == 0) {
+            for (; i < R; i += NTT_BATCH * J, dst += NTT_BATCH * stride) {
+                u64 x[NTT_BATCH];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) x[b] = scol[pidx(i + b * J)];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH; ++b) dst[b * stride] = x[b];
+            }
+        } else {
+            for (; i < R; i += J, dst += stride) *dst = scol[pidx(i)];
+        }
     }
 }
 
@@ -332,6 +464,23 @@ LdePlan plan_lde(u32 logN, u32 logX) {
     return default_plan_lde(logN);
 }
 
+// The pass kernel for (CTAs per SM, log2 radix): one instantiation per radix
+// 2^1 .. 2^TW_STAGE_LOG, so every index and stride of the stage groups is a
+// compile-time constant.
+typedef void (*NttPassKernel)(NttPassArgs);
+template <int MINB, int... Ls>
+static NttPassKernel pass_kernel_of(u32 l, std::integer_sequence<int, Ls...>) {
+    static const NttPassKernel table[] = {k_ntt_pass<MINB, Ls + 1>...};
+    return table[l - 1];
+}
+static NttPassKernel pass_kernel(u32 minb, u32 logR) {
+    static_assert(TW_STAGE_LOG == 11, "one pass kernel per radix up to 2^TW_STAGE_LOG");
+    const auto seq = std::make_integer_sequence<int, TW_STAGE_LOG>{};
+    if (minb == 2) return pass_kernel_of<2>(logR, seq);
+    if (minb == 4) return pass_kernel_of<4>(logR, seq);
+    return pass_kernel_of<3>(logR, seq);
+}
+
 int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
     if (L.logN > TW_LOG || L.planes == 0 || pl.logN != L.logN || !lde_plan_valid(pl)) return -1;
     NttPassArgs a{};
@@ -347,12 +496,20 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
     a.tw_stage = L.tw_stage;
     a.tw_hi = L.tw_hi;
     a.tw_lo = L.tw_lo;
+    // Two passes where the message fits one row of the first (m <= 2^logR1):
+    // every column of pass 0 holds at most one nonzero word, so pass 0 would
+    // only broadcast it and apply the inter-pass factors.  The last pass then
+    // reads the message and applies the factors itself (the coset form of the
+    // LDE), and pass 0 is not launched.
+    const bool twist = pl.npass == 2 && L.m <= (1ull << pl.logR[1]);
     u32 logrest = L.logN;
     for (u32 s = 0; s < pl.npass; ++s) {
         a.pass = s;
         a.logR = pl.logR[s];
         logrest -= a.logR;
         a.logS = logrest;
+        if (twist && s == 0) continue;
+        a.twist = twist ? 1u : 0u;
         a.logW = pass_logW(pl, s, a.logS);
         dim3 grid;
         if (s + 1 < pl.npass) {
@@ -377,11 +534,12 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
             while ((1ull << lr) < rows) ++lr;
             a.logE = a.logR > lr ? a.logR - lr : 0;
         }
+        a.tw_pass = !L.tables ? nullptr
+                    : s + 1 < pl.npass ? L.tables->get(a.logR + a.logS, a.logR)
+                    : twist ? L.tables->get(L.logN, pl.logR[0]) : nullptr;
         size_t smem = lde_smem_bytes(a.logR, a.logW);
         const u32 mb = pl.minb ? pl.minb : LDE_MINB_DEFAULT;
-        if (mb == 2) k_ntt_pass<2><<<grid, 256, smem, st>>>(a);
-        else if (mb == 4) k_ntt_pass<4><<<grid, 256, smem, st>>>(a);
-        else k_ntt_pass<3><<<grid, 256, smem, st>>>(a);
+        pass_kernel(mb, a.logR)<<<grid, 256, smem, st>>>(a);
         count_launches(1);
     }
     return 0;
@@ -394,10 +552,76 @@ int launch_lde(const LdeArgs& L, cudaStream_t st) {
     return launch_lde_plan(L, plan_lde(L.logN, logX), st);
 }
 
+// ---- inter-pass twiddle tables ---------------------------------------------
+// tab[i 2^logS + col] = w_{2^logNs}^(i col) for i < 2^(logNs - logS).
+__global__ void k_pass_table(u64* tab, u32 logNs, u32 logS, const u64* hi, const u64* lo) {
+    const u64 total = 1ull << logNs, mask = (1ull << logS) - 1;
+    for (u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (u64)gridDim.x * blockDim.x)
+        tab[k] = twiddle((k >> logS) * (k & mask), logNs, hi, lo);
+}
+
+long long lde_tables_prepare_plan(LdeTables& t, const LdePlan& pl, const u64* tw_hi, const u64* tw_lo,
+                                  cudaStream_t st, u64 room) {
+    if (!lde_plan_valid(pl)) return 0;
+    u64* made[3] = {};
+    u32 keys[3] = {};
+    int nmade = 0;
+    long long bytes = 0;
+    u32 logNs = pl.logN;
+    for (u32 s = 0; s + 1 < pl.npass; ++s) {
+        const u32 logR = pl.logR[s];
+        const u32 key = logNs * (TW_STAGE_LOG + 1) + logR;
+        const size_t sz = (size_t)8 << logNs;
+        if (t.tab[key].load() == nullptr && logNs <= LdeTables::MAX_LOG && (u64)bytes + sz <= room) {
+            u64* p = nullptr;
+            if (cudaMalloc(&p, sz) != cudaSuccess) {
+                cudaGetLastError();
+                break;
+            }
+            const u64 total = 1ull << logNs;
+            const unsigned grid = (unsigned)std::min<u64>((total + 255) / 256, 4096);
+            k_pass_table<<<grid, 256, 0, st>>>(p, logNs, logNs - logR, tw_hi, tw_lo);
+            count_launches(1);
+            made[nmade] = p;
+            keys[nmade++] = key;
+            bytes += (long long)sz;
+        }
+        logNs -= logR;
+    }
+    if (nmade == 0) return 0;
+    if (cudaPeekAtLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) {
+        for (int k = 0; k < nmade; ++k) cudaFree(made[k]);
+        return -1;
+    }
+    for (int k = 0; k < nmade; ++k) {
+        u64* expect = nullptr;
+        if (!t.tab[keys[k]].compare_exchange_strong(expect, made[k])) {  // built meanwhile by another thread
+            cudaFree(made[k]);
+            bytes -= (long long)((size_t)8 << (keys[k] / (TW_STAGE_LOG + 1)));
+        }
+    }
+    return bytes;
+}
+
+long long lde_tables_prepare(LdeTables& t, u32 logN, u32 logX, const u64* tw_hi, const u64* tw_lo, cudaStream_t st,
+                             u64 room) {
+    if (logN > TW_LOG) return 0;
+    return lde_tables_prepare_plan(t, plan_lde(logN, logX), tw_hi, tw_lo, st, room);
+}
+
+void lde_tables_free(LdeTables& t) {
+    for (auto& p : t.tab) {
+        u64* q = p.exchange(nullptr);
+        if (q) cudaFree(q);
+    }
+}
+
 int lde_prepare() {
-    for (auto f : {k_ntt_pass<2>, k_ntt_pass<3>, k_ntt_pass<4>})
-        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LDE_SMEM_MAX) != cudaSuccess)
-            return -1;
+    for (u32 mb = 2; mb <= 4; ++mb)
+        for (u32 l = 1; l <= TW_STAGE_LOG; ++l)
+            if (cudaFuncSetAttribute(pass_kernel(mb, l), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)LDE_SMEM_MAX) != cudaSuccess)
+                return -1;
     return 0;
 }
 

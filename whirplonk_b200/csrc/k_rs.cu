@@ -97,7 +97,15 @@ LdeArgs lde_args(whirgpu_ctx* c, const u64* src, u64 m, u32 planes, u32 logN, u6
     L.tw_stage = c->tw.tw_stage;
     L.tw_hi = c->tw.tw_hi;
     L.tw_lo = c->tw.tw_lo;
+    L.tables = &c->lde_tables;
     return L;
+}
+
+// The inter-pass tables of `pl` (kernel-level calls run outside graph capture).
+void prepare_plan_tables(whirgpu_ctx* c, const LdePlan& pl) {
+    std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+    const uint64_t room = c->budget ? (c->budget > c->allocated ? c->budget - c->allocated : 0) : ~0ull;
+    lde_tables_prepare_plan(c->lde_tables, pl, c->tw.tw_hi, c->tw.tw_lo, c->stream, room);
 }
 
 bool shape_ok(uint32_t log_len, uint32_t log_expansion, uint32_t log_depth) {
@@ -119,6 +127,7 @@ whirgpu_status whirgpu_rs_encode(whirgpu_ctx* c, const uint64_t* d_vectors, size
     const u64 planes = (u64)count << log_depth;
     if (planes > 65535) return fail(c, WHIRGPU_E_INVALID, "too many planes");
     const u32 logN = log_len - log_depth + log_expansion;
+    prepare_plan_tables(c, plan_lde(logN, log_expansion));
     const LdeArgs L = lde_args(c, d_vectors, 1ull << (log_len - log_depth), (u32)planes, logN, d_tmp, d_planes);
     if (launch_lde(L, c->stream) != 0) return fail(c, WHIRGPU_E_INVALID, "LDE launch");
     const cudaError_t e = cudaGetLastError();
@@ -134,6 +143,7 @@ whirgpu_status whirgpu_rs_commit_batch(whirgpu_ctx* c, const uint64_t* vectors, 
     const u32 logN = log_len - log_depth + log_expansion;
     const u64 N = 1ull << logN;
     const u64 in_words = count << log_len;
+    prepare_plan_tables(c, plan_lde(logN, log_expansion));
     const u64 node_words = (2 * N) * 8;  // 32-bit words of one tree's node array
     const size_t bytes = (location == WHIRGPU_INPUT_DEVICE ? 0 : in_words * 8) + 2 * planes * N * 8 +
                          count * node_words * 4 + 256;
@@ -218,6 +228,7 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
     if (cand.empty()) return fail(c, WHIRGPU_E_INVALID, "no valid plan");
 
     unsigned long long want = 0;
+    prepare_plan_tables(c, default_plan_lde(log_n));
     if (launch_lde_plan(L, default_plan_lde(log_n), c->stream) != 0 || !digest(&want))
         return fail(c, WHIRGPU_E_CUDA, "reference LDE");
     cudaEvent_t e0, e1;
@@ -228,6 +239,7 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
     uint32_t rejected = 0;
     whirgpu_status result = WHIRGPU_OK;
     for (const LdePlan& p : cand) {
+        prepare_plan_tables(c, p);  // the plans are timed as proofs run them
         cudaMemsetAsync(out, 0, planes * N * 8, c->stream);
         unsigned long long got = 0;
         if (launch_lde_plan(L, p, c->stream) != 0 || !digest(&got)) { result = fail(c, WHIRGPU_E_CUDA, "candidate"); break; }

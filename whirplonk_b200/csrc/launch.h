@@ -1,6 +1,7 @@
 // launch.h -- host-side declarations of the kernel launchers (implemented in
 // the k_*.cu files) used by the prover schedule in prover.cu.
 #pragma once
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <cuda_runtime_api.h>
@@ -34,9 +35,11 @@ struct NttPassArgs {
     u64* tmp;
     u64* out;
     u32 depth, logN, logR, logS, logW, npass, pass, logR0, logR1, logE;
+    u32 twist;  // last pass of two whose first is a pure broadcast (m <= columns): reads the message itself
     const u64* tw_stage;
     const u64* tw_hi;
     const u64* tw_lo;
+    const u64* tw_pass;  // this pass boundary's LdeTables entry, or null
 };
 struct LdeArgs {
     const u64* src[3];  // component planes of the message vector (block b at src[c] + b*m)
@@ -49,6 +52,26 @@ struct LdeArgs {
     const u64* tw_stage;
     const u64* tw_hi;
     const u64* tw_lo;
+    const struct LdeTables* tables;  // inter-pass factors of the context, or null
+};
+// Inter-pass twiddle tables of one context.  The pass boundary of a
+// 2^logNs-point (sub-)transform split as 2^logR rows x 2^logS columns
+// (logS = logNs - logR) multiplies element (row i, column col) by
+// w_{2^logNs}^(i col); its table holds those factors row by row,
+// tab[i 2^logS + col], so the storing threads read them coalesced and the pass
+// pays one multiply per element instead of two (the factor and its advance).
+// Tables are built before a proof that uses the split is enqueued
+// (lde_tables_prepare, outside any graph capture) and live as long as the
+// context; a pass whose table is missing computes its factors by multiplying.
+struct LdeTables {
+    static constexpr u32 MAX_LOG = 24;  // largest table: 2^24 words (128 MiB)
+    std::atomic<u64*> tab[(TW_LOG + 1) * (TW_STAGE_LOG + 1)];
+    LdeTables() {
+        for (auto& t : tab) t.store(nullptr);
+    }
+    const u64* get(u32 logNs, u32 logR) const {
+        return logNs <= TW_LOG && logR <= TW_STAGE_LOG ? tab[logNs * (TW_STAGE_LOG + 1) + logR].load() : nullptr;
+    }
 };
 // The plan launch_lde uses for a 2^logN codeword of a 2^logN / 2^logX message:
 // an installed (autotuned) plan for (logN, logX) if there is one, else the
@@ -63,6 +86,15 @@ size_t lde_installed_plans(u32* keys, LdePlan* plans, size_t cap);  // keys: log
 int launch_lde_plan(const LdeArgs& a, const LdePlan& pl, cudaStream_t st);
 int launch_lde(const LdeArgs& a, cudaStream_t st);
 int lde_prepare();
+// Builds the missing inter-pass tables of `pl` (or of plan_lde(logN, logX))
+// whose size fits `room` bytes, on `st`, and waits for them before publishing
+// them.  Returns the bytes allocated, or -1 after a CUDA error (the tables
+// stay missing; the LDE still runs).
+long long lde_tables_prepare_plan(LdeTables& t, const LdePlan& pl, const u64* tw_hi, const u64* tw_lo,
+                                  cudaStream_t st, u64 room);
+long long lde_tables_prepare(LdeTables& t, u32 logN, u32 logX, const u64* tw_hi, const u64* tw_lo, cudaStream_t st,
+                             u64 room);
+void lde_tables_free(LdeTables& t);
 // Resident-CTA counts of the sumcheck round kernels on the current device
 // (their grids never leave a partial wave); called once per context.
 int sumcheck_prepare();

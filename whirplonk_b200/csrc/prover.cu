@@ -92,6 +92,7 @@ ProofPlan make_plan(const WhirSchedule& sched, const ProtocolParams& params, int
         CommitBuffers cb;
         cb.N = c.codeword_length;
         cb.logN = ilog2(cb.N);
+        cb.logX = cb.logN - ilog2(c.message_length());
         if (params.coset_major) cb.perm_log_e = cb.logN - ilog2(c.message_length());
         cb.depth = row_elems;
         cb.ncomp = ncomp;
@@ -227,6 +228,7 @@ int commit_vectors(const Ctx& c, int ci, const uint64_t* const src[3], uint32_t 
     L.tw_stage = c.tw.tw_stage;
     L.tw_hi = c.tw.tw_hi;
     L.tw_lo = c.tw.tw_lo;
+    L.tables = c.tw.lde;
     WG_TIMED(c, FAM_NTT, launch_lde(L, c.st));
     uint32_t* nodes = reinterpret_cast<uint32_t*>(c.ws + cb.nodes);
     WG_TIMED(c, FAM_LEAF, launch_leaves(c.w(cb.planes), cb.N, cb.depth, ncomp, nodes, c.p.params.hash, c.st,

@@ -22,6 +22,7 @@ struct ProofScalars;
 struct CommitBuffers {
     uint64_t N = 0;
     uint32_t logN = 0, depth = 0, ncomp = 0;
+    uint32_t logX = 0;        // log2(N / message length per plane): the LDE's expansion
     uint32_t perm_log_e = 0;  // coset-major rows: log2(N / message length); 0 = natural order
     size_t planes = 0, nodes = 0;  // byte offsets in the workspace
 };
@@ -69,10 +70,12 @@ ProofPlan make_plan(uint32_t num_variables, const ProtocolParams& p, int n_forms
 ProofPlan make_plan(const WhirSchedule& sched, const ProtocolParams& p, int n_forms, size_t ds_len,
                     uint32_t num_witnesses = 1);
 
+struct LdeTables;
 struct DeviceTables {
     uint64_t* tw_stage = nullptr;
     uint64_t* tw_hi = nullptr;
     uint64_t* tw_lo = nullptr;
+    const LdeTables* lde = nullptr;  // the context's inter-pass twiddle tables
 };
 
 // Enqueue the whole commit (Config::commit, once per initial commitment) on

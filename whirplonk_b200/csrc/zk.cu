@@ -588,6 +588,8 @@ whirgpu_status whirgpu_zk_commit(whirgpu_ctx* c, const whirgpu_zk_config* cfg, c
     bool fresh = false;
     {  // a pooled allocation of this size, else a new one within the budget
         std::lock_guard<std::recursive_mutex> lk(c->cache_mu);
+        prepare_lde_tables(c, w->pb);
+        prepare_lde_tables(c, w->pg);
         auto it = c->zk_pool.find(total);
         if (it != c->zk_pool.end() && !it->second.empty()) {
             w->dev = it->second.back();
