@@ -36,11 +36,17 @@ __device__ __forceinline__ u64 ldg64(const u64* p) { return __ldg(reinterpret_ca
 constexpr int NTT_BATCH = 8;
 
 // Shared-memory word of column element e: one pad word every 32 words keeps
-// strided group accesses off a single bank; the extra word per column puts the
-// W columns of a tile on different banks (the transposed store phase reads
-// one element of each column per step).
+// strided group accesses off a single bank.
 __device__ __forceinline__ u32 pidx(u32 e) { return e + (e >> 5); }
-__host__ __device__ constexpr u32 col_stride(u32 logR) { return (1u << logR) + ((1u << logR) >> 5) + 1; }
+// Words per column of a tile of 2^logW columns: the padded column, rounded up
+// to 16 / W (mod 16) words, so that in the phases where a half-warp reads or
+// writes W columns x 16 / W rows its 16 words fall on 16 distinct 8-byte bank
+// pairs.  (In the butterfly groups a warp stays within one column.)
+__host__ __device__ constexpr u32 col_stride(u32 logR, u32 logW) {
+    const u32 base = (1u << logR) + ((1u << logR) >> 5);
+    const u32 c = logW >= 1 && logW <= 3 ? 16u >> logW : 1u;
+    return base + (c + 16 - base % 16) % 16;
+}
 
 // Stages s0+1 .. s0+RR of a radix-2 DIT on the 2^logW bit-reversed columns of
 // 2^L words, done as independent radix-2^RR groups in registers: a group is
@@ -59,10 +65,9 @@ __host__ __device__ constexpr u32 col_stride(u32 logR) { return (1u << logR) + (
 // with c = 0 have the twiddle w^0 = 1: their multiply is skipped (all of stage
 // 1, half of stage 2, ...).
 template <int RR, bool S0ZERO, int L, int S0C = -1>
-__device__ __forceinline__ void dit_group(u64* sm, u32 logW, u32 s0_rt, const u64* tws) {
+__device__ __forceinline__ void dit_group(u64* sm, u32 logW, u32 cs, u32 s0_rt, const u64* tws) {
     constexpr int G = 1 << RR;
     constexpr u32 gpc_log = L - RR;  // groups per column (log2)
-    constexpr u32 cs = col_stride(L);
     const u32 s0 = S0ZERO ? 0u : (S0C >= 0 ? (u32)S0C : s0_rt);
     const u32 total = 1u << (logW + gpc_log);
     const bool wide = !S0ZERO && S0C < 0 && s0 >= 5;
@@ -115,25 +120,25 @@ __device__ __forceinline__ void dit_group(u64* sm, u32 logW, u32 s0_rt, const u6
 
 // Stages s0+1 .. L in register groups of up to 16, natural-order output.
 template <int L>
-__device__ __forceinline__ void dit_stages(u64* sm, u32 logW, u32 s0, const u64* tws) {
+__device__ __forceinline__ void dit_stages(u64* sm, u32 logW, u32 cs, u32 s0, const u64* tws) {
     while (s0 < (u32)L) {
         const u32 left = L - s0;
         const u32 rr = left >= 8 ? 4 : (left > 4 ? (left + 1) / 2 : left);
         if (s0 == 0) {
-            if constexpr (L >= 4) { if (rr == 4) dit_group<4, true, L>(sm, logW, s0, tws); }
-            if constexpr (L >= 3) { if (rr == 3) dit_group<3, true, L>(sm, logW, s0, tws); }
-            if constexpr (L >= 2) { if (rr == 2) dit_group<2, true, L>(sm, logW, s0, tws); }
-            if (rr == 1) dit_group<1, true, L>(sm, logW, s0, tws);
+            if constexpr (L >= 4) { if (rr == 4) dit_group<4, true, L>(sm, logW, cs, s0, tws); }
+            if constexpr (L >= 3) { if (rr == 3) dit_group<3, true, L>(sm, logW, cs, s0, tws); }
+            if constexpr (L >= 2) { if (rr == 2) dit_group<2, true, L>(sm, logW, cs, s0, tws); }
+            if (rr == 1) dit_group<1, true, L>(sm, logW, cs, s0, tws);
         } else if (s0 == 4) {
-            if constexpr (L >= 8) { if (rr == 4) dit_group<4, false, L, 4>(sm, logW, s0, tws); }
-            if constexpr (L >= 7) { if (rr == 3) dit_group<3, false, L, 4>(sm, logW, s0, tws); }
-            if constexpr (L >= 6) { if (rr == 2) dit_group<2, false, L, 4>(sm, logW, s0, tws); }
-            if constexpr (L >= 5) { if (rr == 1) dit_group<1, false, L, 4>(sm, logW, s0, tws); }
+            if constexpr (L >= 8) { if (rr == 4) dit_group<4, false, L, 4>(sm, logW, cs, s0, tws); }
+            if constexpr (L >= 7) { if (rr == 3) dit_group<3, false, L, 4>(sm, logW, cs, s0, tws); }
+            if constexpr (L >= 6) { if (rr == 2) dit_group<2, false, L, 4>(sm, logW, cs, s0, tws); }
+            if constexpr (L >= 5) { if (rr == 1) dit_group<1, false, L, 4>(sm, logW, cs, s0, tws); }
         } else {
-            if constexpr (L >= 4) { if (rr == 4) dit_group<4, false, L>(sm, logW, s0, tws); }
-            if constexpr (L >= 3) { if (rr == 3) dit_group<3, false, L>(sm, logW, s0, tws); }
-            if constexpr (L >= 2) { if (rr == 2) dit_group<2, false, L>(sm, logW, s0, tws); }
-            if (rr == 1) dit_group<1, false, L>(sm, logW, s0, tws);
+            if constexpr (L >= 4) { if (rr == 4) dit_group<4, false, L>(sm, logW, cs, s0, tws); }
+            if constexpr (L >= 3) { if (rr == 3) dit_group<3, false, L>(sm, logW, cs, s0, tws); }
+            if constexpr (L >= 2) { if (rr == 2) dit_group<2, false, L>(sm, logW, cs, s0, tws); }
+            if (rr == 1) dit_group<1, false, L>(sm, logW, cs, s0, tws);
         }
         s0 += rr;
         __syncthreads();
@@ -152,8 +157,8 @@ template <int MINB, int L>
 __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     extern __shared__ u64 sm[];
     constexpr u32 logR = L, R = 1u << L;
-    constexpr u32 cs = col_stride(L);
     const u32 W = 1u << a.logW;
+    const u32 cs = a.cs;
     const u32 tileN = W << logR;
     u64* tws = sm + W * cs;
     const u32 plane = blockIdx.y;
@@ -302,7 +307,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     }
 
     // Decimation-in-time stages in register groups of up to 16, natural-order output.
-    dit_stages<L>(sm, a.logW, logE, tws);
+    dit_stages<L>(sm, a.logW, cs, logE, tws);
 
     // Store.
     if (!last) {
@@ -398,7 +403,7 @@ LdePlan default_plan_lde(u32 logN) {
 }
 
 size_t lde_smem_bytes(u32 logR, u32 logW) {
-    return ((size_t)(1u << logW) * col_stride(logR)) * 8 + ((size_t)1 << logR) / 2 * 8 + 16;
+    return ((size_t)(1u << logW) * col_stride(logR, logW)) * 8 + ((size_t)1 << logR) / 2 * 8 + 16;
 }
 constexpr size_t LDE_SMEM_MAX = 100 * 1024;
 
@@ -511,6 +516,7 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
         if (twist && s == 0) continue;
         a.twist = twist ? 1u : 0u;
         a.logW = pass_logW(pl, s, a.logS);
+        a.cs = col_stride(a.logR, a.logW);
         dim3 grid;
         if (s + 1 < pl.npass) {
             u64 prefixes = s == 0 ? 1 : (1ull << pl.logR[0]);

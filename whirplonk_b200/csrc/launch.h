@@ -36,6 +36,7 @@ struct NttPassArgs {
     u64* out;
     u32 depth, logN, logR, logS, logW, npass, pass, logR0, logR1, logE;
     u32 twist;  // last pass of two whose first is a pure broadcast (m <= columns): reads the message itself
+    u32 cs;     // shared-memory words per tile column
     const u64* tw_stage;
     const u64* tw_hi;
     const u64* tw_lo;
