@@ -38,6 +38,13 @@ constexpr int NTT_BATCH = 8;
 // Shared-memory word of column element e: one pad word every 32 words keeps
 // strided group accesses off a single bank.
 __device__ __forceinline__ u32 pidx(u32 e) { return e + (e >> 5); }
+// Word of twiddle u in the shared table: bits 0-3 of u are XORed with bits
+// 4-7 and 8-11.  A butterfly group's lanes read twiddles lo 2^d + K (16
+// consecutive lo, one d per stage, K shared); for every d <= 8 the swizzle
+// puts those 16 words on 16 distinct 8-byte bank pairs, where the plain
+// layout put them on one (d >= 4).  The map is XOR-linear, so the
+// swizzle of lo 2^d + K is the lanes' part XOR a compile-time constant.
+__host__ __device__ constexpr u32 twz(u32 u) { return u ^ (((u >> 4) ^ (u >> 8)) & 15u); }
 // Words per column of a tile of 2^logW columns: the padded column, rounded up
 // to 16 / W (mod 16) words, so that in the phases where a half-warp reads or
 // writes W columns x 16 / W rows its 16 words fall on 16 distinct 8-byte bank
@@ -54,8 +61,9 @@ __host__ __device__ constexpr u32 col_stride(u32 logR, u32 logW) {
 // butterflies of stage s pair j with j + 2^(t-1) (t = s - s0) under the twiddle
 // w_{2^s}^(lo + c 2^s0), c = j mod 2^(t-1), lo = base mod 2^s0.
 //
-// L is a compile-time constant, so the twiddle of (t, c) is read at
-// tws[(lo << (L - s0)) >> t] plus the constant offset c << (L - t).  Word j of
+// L is a compile-time constant, so the twiddle of (t, c), table entry
+// (lo << (L - s0 - t)) + (c << (L - t)), is read at tws[P_t ^ twz(c << (L - t))]
+// with P_t = twz(lo << (L - s0 - t)) computed once per stage.  Word j of
 // the group sits at pidx(base) + j 2^s0 + floor(j 2^s0 / 32): the group's
 // 2^(s0 + RR)-word span never straddles a pad word except at the multiples
 // of 32 its own steps cross.  That offset is a compile-time constant when s0
@@ -88,11 +96,11 @@ __device__ __forceinline__ void dit_group(u64* sm, u32 logW, u32 cs, u32 s0_rt, 
             else if (wide) x[j] = p0[j * D];
             else x[j] = col[pidx(base + ((u32)j << s0))];
         }
-        const u32 X = S0ZERO ? 0u : (lo << (L - s0));
+        const u32 X = S0ZERO ? 0u : (lo << (L - s0));  // entry of (t, c) = (X >> t) | (c << (L - t))
 #pragma unroll
         for (int t = 1; t <= RR; ++t) {
             const int half = 1 << (t - 1);
-            const u64* twt = tws + (X >> t);
+            const u32 Pt = twz(X >> t);
 #pragma unroll
             for (int j = 0; j < G; ++j) {
                 if (j & half) continue;
@@ -102,7 +110,7 @@ __device__ __forceinline__ void dit_group(u64* sm, u32 logW, u32 cs, u32 s0_rt, 
                 if (S0ZERO && c == 0) {
                     v = x[j + half];
                 } else {
-                    v = gl_mul_fma(x[j + half], twt[(u32)c << (L - t)]);
+                    v = gl_mul_fma(x[j + half], tws[Pt ^ twz((u32)c << (L - t))]);
                 }
                 x[j] = gl_add(u, v);
                 x[j + half] = gl_sub(u, v);
@@ -169,7 +177,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
     const u64* src = first || a.twist ? src0 + (u64)blk * a.m : nullptr;
     u64* tmp = a.tmp + (u64)plane * N;
 
-    for (u32 u = threadIdx.x; u < R / 2; u += blockDim.x) tws[u] = a.tw_stage[u << (TW_STAGE_LOG - logR)];
+    for (u32 u = threadIdx.x; u < R / 2; u += blockDim.x) tws[twz(u)] = a.tw_stage[u << (TW_STAGE_LOG - logR)];
 
     // Tile geometry.
     u64 S = 0, P = 0, col0 = 0;
