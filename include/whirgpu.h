@@ -344,14 +344,16 @@ whirgpu_status whirgpu_rs_commit_batch(whirgpu_ctx* ctx, const uint64_t* vectors
 /* The LDE of a 2^log_n codeword from a 2^(log_n - log_expansion) message runs in
  * npass passes of radix 2^log_radix[s] (sum = log_n, each <= 11); pass s stages
  * 2^log_cols[s] columns per CTA (255 = built-in choice); the kernel variant's
- * registers are sized for min_blocks CTAs per SM (2..4, 0 = built-in).  No
- * counterpart in the reference (its NTT engine picks fixed radices,
- * cooley_tukey.hpp:200-259). */
+ * registers are sized for min_blocks CTAs per SM (2..4, 0 = built-in);
+ * pipelined = 1 runs the passes as persistent CTAs that copy the next tile in
+ * while transforming the current one.  No counterpart in the reference (its
+ * NTT engine picks fixed radices, cooley_tukey.hpp:200-259). */
 typedef struct {
     uint32_t log_n, log_expansion, npass;
     uint32_t log_radix[3];
     uint32_t log_cols[3];
     uint32_t min_blocks;
+    uint32_t pipelined;
 } whirgpu_ntt_plan;
 /* Times every valid plan for the shape on `planes` synthetic planes (median of
  * `reps` runs each), checks each plan's codeword against the built-in plan's,
@@ -367,7 +369,8 @@ void whirgpu_ntt_clear_plans(void);
 /* Installed plans (returns the count; writes at most cap). */
 size_t whirgpu_ntt_list_plans(whirgpu_ntt_plan* out, size_t cap);
 /* JSON plan files: {"plans": [{"log_n": .., "log_expansion": .., "npass": ..,
- * "log_radix": [..], "log_cols": [..]}, ..]}. */
+ * "log_radix": [..], "log_cols": [..], "min_blocks": .., "pipelined": ..}, ..]}
+ * (min_blocks and pipelined optional). */
 whirgpu_status whirgpu_ntt_load_plans(const char* path, size_t* loaded);
 whirgpu_status whirgpu_ntt_save_plans(const char* path);
 /* Installs, once per process, the plans in $WHIRGPU_NTT_PLANS or else in

@@ -113,11 +113,14 @@ def test_ntt_plan_table_roundtrip(tmp_path):
     L = _lib.load()
     L.whirgpu_ntt_clear_plans()
     good = _lib.NttPlan(20, 3, 2, (9, 11, 0), (4, 2, 255))
+    piped = _lib.NttPlan(21, 2, 2, (11, 10, 0), (1, 2, 255), 3, 1)
     assert L.whirgpu_ntt_set_plan(ctypes.byref(good)) == _lib.OK
+    assert L.whirgpu_ntt_set_plan(ctypes.byref(piped)) == _lib.OK
     for bad in [_lib.NttPlan(20, 3, 2, (8, 11, 0), (255, 255, 255)),   # radices do not sum to log_n
                 _lib.NttPlan(24, 1, 2, (12, 12, 0), (255, 255, 255)),  # radix above 2^11
                 _lib.NttPlan(22, 1, 1, (22, 0, 0), (255, 255, 255)),   # one pass above 2^11
-                _lib.NttPlan(20, 3, 2, (9, 11, 0), (7, 0, 255))]:      # too many columns
+                _lib.NttPlan(20, 3, 2, (9, 11, 0), (7, 0, 255)),       # too many columns
+                _lib.NttPlan(20, 3, 2, (9, 11, 0), (4, 2, 255), 3, 2)]:  # pipelined is 0 or 1
         assert L.whirgpu_ntt_set_plan(ctypes.byref(bad)) == _lib.E_INVALID
     out = _lib.NttPlan()
     assert L.whirgpu_ntt_get_plan(20, 3, ctypes.byref(out)) == _lib.OK
@@ -129,9 +132,12 @@ def test_ntt_plan_table_roundtrip(tmp_path):
     L.whirgpu_ntt_clear_plans()
     assert L.whirgpu_ntt_list_plans(None, 0) == 0
     n = ctypes.c_size_t()
-    assert L.whirgpu_ntt_load_plans(path.encode(), ctypes.byref(n)) == _lib.OK and n.value == 1
+    assert L.whirgpu_ntt_load_plans(path.encode(), ctypes.byref(n)) == _lib.OK and n.value == 2
     assert L.whirgpu_ntt_get_plan(20, 3, ctypes.byref(out)) == _lib.OK and out.as_dict() == good.as_dict()
+    assert L.whirgpu_ntt_get_plan(21, 2, ctypes.byref(out)) == _lib.OK and out.as_dict() == piped.as_dict()
     import json
 
-    assert json.load(open(path))["plans"][0]["log_radix"] == [9, 11, 0]
+    plans = {(p["log_n"], p["log_expansion"]): p for p in json.load(open(path))["plans"]}
+    assert plans[(20, 3)]["log_radix"] == [9, 11, 0] and plans[(20, 3)]["pipelined"] == 0
+    assert plans[(21, 2)]["pipelined"] == 1
     L.whirgpu_ntt_clear_plans()

@@ -8,6 +8,7 @@ import pytest
 
 from whirplonk_b200 import Context, ProtocolParameters, _lib, prove_once, sample_goldilocks
 from whirplonk_b200.autotune import current_plan, tune
+from whirplonk_b200.autotune import load as load_plans
 from whirplonk_b200.rs import rs_commit_batch, rs_encode
 
 pytestmark = pytest.mark.gpu
@@ -136,3 +137,53 @@ def test_autotune_plans_agree_and_proofs_unchanged(gpu_ctx, oracle):
     assert before == after
     onarg, ohints = oracle.prove(n, 4, rho, 100, 20, pts, coeffs, ev)
     assert before == (onarg, ohints)
+
+
+def _pipelined(ln, lx, minb):
+    """The shape's current plan with persistent pipelined passes."""
+    plan = _lib.NttPlan()
+    _lib.check(_lib.load().whirgpu_ntt_get_plan(ln, lx, ctypes.byref(plan)))
+    plan.min_blocks = minb
+    plan.pipelined = 1
+    return plan
+
+
+@pytest.mark.parametrize("log_len,log_exp,minb", [(20, 2, 3), (18, 3, 4), (16, 5, 2), (24, 1, 3), (12, 4, 4)])
+def test_pipelined_passes_match_oracle(gpu_ctx, oracle, log_len, log_exp, minb):
+    """Persistent pipelined passes (the next tile's copies in flight while the
+    current one is transformed) give the oracle's roots."""
+    L = _lib.load()
+    ln = log_len - 4 + log_exp
+    plan = _pipelined(ln, log_exp, minb)
+    assert L.whirgpu_ntt_set_plan(ctypes.byref(plan)) == _lib.OK
+    try:
+        count = 2 if log_len <= 20 else 1
+        v = sample_goldilocks(9100 + log_len + log_exp, count << log_len).reshape(count, -1)
+        roots = rs_commit_batch(gpu_ctx, v, log_exp)
+        N = ((1 << log_len) // 16) << log_exp
+        for k in range(count):
+            assert roots[k] == oracle.rs_commit_root(v[k], N, 16), f"vector {k}"
+    finally:
+        L.whirgpu_ntt_clear_plans()
+        load_plans()
+
+
+def test_pipelined_plans_proof_matches_oracle(gpu_ctx, oracle):
+    """A whole proof with every LDE of its schedule on pipelined passes."""
+    from whirplonk_b200.autotune import lde_shapes
+
+    L = _lib.load()
+    n, rho = 18, 2
+    params = ProtocolParameters.cli(log_inv_rate=rho)
+    try:
+        for ln, lx, _ in lde_shapes(n, params):
+            plan = _pipelined(ln, lx, 3)
+            assert L.whirgpu_ntt_set_plan(ctypes.byref(plan)) == _lib.OK
+        coeffs = sample_goldilocks(91, 1 << n)
+        pts = sample_goldilocks(92, 3 * n).reshape(1, n, 3)
+        ev = np.array(gpu_ctx.mle_evaluate(coeffs, pts), dtype=np.uint64).reshape(1, 3)
+        got = prove_once(n, params, coeffs, pts, ev, ctx=gpu_ctx)[:2]
+        assert got == oracle.prove(n, 4, rho, 100, 20, pts, coeffs, ev)
+    finally:
+        L.whirgpu_ntt_clear_plans()
+        load_plans()

@@ -143,11 +143,13 @@ class NttPlan(ctypes.Structure):
         ("log_radix", ctypes.c_uint32 * 3),
         ("log_cols", ctypes.c_uint32 * 3),
         ("min_blocks", ctypes.c_uint32),
+        ("pipelined", ctypes.c_uint32),
     ]
 
     def as_dict(self):
         return {"log_n": self.log_n, "log_expansion": self.log_expansion, "npass": self.npass,
-                "log_radix": list(self.log_radix), "log_cols": list(self.log_cols), "min_blocks": self.min_blocks}
+                "log_radix": list(self.log_radix), "log_cols": list(self.log_cols), "min_blocks": self.min_blocks,
+                "pipelined": self.pipelined}
 
 
 class WhirGpuError(RuntimeError):

@@ -72,7 +72,7 @@ def tune(ctx: Context, shapes, reps: int = 5, log=print) -> list:
             d["rejected"] = note
         out.append(d)
         log(f"log_n={ln:2d} log_exp={lx:2d} planes={planes:3d}: {d['npass']} passes {d['log_radix'][:d['npass']]} "
-            f"cols {d['log_cols'][:d['npass']]} minb {d['min_blocks']}  {us.value:9.1f} us  ({tried.value} plans, "
+            f"cols {d['log_cols'][:d['npass']]} minb {d['min_blocks']} pipe {d['pipelined']}  {us.value:9.1f} us  ({tried.value} plans, "
             f"{time.perf_counter() - t0:.1f} s) {note}")
     return out
 

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <utility>
 
 #include "launch.h"
@@ -159,50 +160,54 @@ __device__ __forceinline__ u64 twiddle(u64 e, u32 logM, const u64* hi, const u64
     return gl_mul(hi[E >> TW_HALF], lo[E & ((1ull << TW_HALF) - 1)]);
 }
 
-// One pass over all planes (blockIdx.y = plane).  MINB = CTAs per SM the
-// register allocation is sized for (the pass plan picks the variant).
-template <int MINB, int L>
-__global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
-    extern __shared__ u64 sm[];
-    constexpr u32 logR = L, R = 1u << L;
-    const u32 W = 1u << a.logW;
-    const u32 cs = a.cs;
-    const u32 tileN = W << logR;
-    u64* tws = sm + W * cs;
-    const u32 plane = blockIdx.y;
+// ---- one tile of one pass --------------------------------------------------
+// A tile is 2^logW columns x 2^L rows of one plane: for a middle (or first)
+// pass the columns col0 .. col0 + W - 1 of prefix P, for the last pass W
+// consecutive rows of its sub-transforms.
+struct TileGeom {
+    u64 S, P, col0, i0base;
+    u32 i1, plane;
+    const u64* src;  // the plane's message block (first pass, coset form), else null
+    u64* tmp;        // the plane's scratch
+};
+
+template <int L>
+__device__ __forceinline__ TileGeom tile_geom(const NttPassArgs& a, u32 bx, u32 plane) {
+    TileGeom g{};
     const u64 N = 1ull << a.logN;
     const bool first = a.pass == 0, last = a.pass + 1 == a.npass;
     const u32 comp = plane / a.depth, blk = plane % a.depth;
     const u64* src0 = comp == 0 ? a.src[0] : (comp == 1 ? a.src[1] : a.src[2]);  // no dynamic param indexing
-    const u64* src = first || a.twist ? src0 + (u64)blk * a.m : nullptr;
-    u64* tmp = a.tmp + (u64)plane * N;
-
-    for (u32 u = threadIdx.x; u < R / 2; u += blockDim.x) tws[twz(u)] = a.tw_stage[u << (TW_STAGE_LOG - logR)];
-
-    // Tile geometry.
-    u64 S = 0, P = 0, col0 = 0;
-    u64 i0base = 0;  // last pass: output index of (w = 0, i = 0)
-    u32 i1 = 0;
+    g.plane = plane;
+    g.src = first || a.twist ? src0 + (u64)blk * a.m : nullptr;
+    g.tmp = a.tmp + (u64)plane * N;
     if (!last) {
-        S = 1ull << a.logS;
-        const u64 ngroups = S >> a.logW;
-        P = blockIdx.x / ngroups;
-        col0 = (blockIdx.x % ngroups) << a.logW;
+        g.S = 1ull << a.logS;
+        const u64 ngroups = g.S >> a.logW;
+        g.P = bx / ngroups;
+        g.col0 = (bx % ngroups) << a.logW;
     } else if (a.npass == 2) {
-        i0base = (u64)blockIdx.x << a.logW;
+        g.i0base = (u64)bx << a.logW;
     } else if (a.npass == 3) {
         const u32 groups = (1u << a.logR0) >> a.logW;
-        i1 = blockIdx.x / groups;
-        i0base = (u64)(blockIdx.x % groups) << a.logW;
+        g.i1 = bx / groups;
+        g.i0base = (u64)(bx % groups) << a.logW;
     }
+    return g;
+}
 
-    // Load (bit-reversed within each column).  Only the first R >> logE rows of
-    // a column can be nonzero (zero padding of the message); in bit-reversed
-    // order they land on multiples of E, and the first logE DIT stages would
-    // merely copy each of them over its block of E words -- done here as a
-    // broadcast, the butterflies then start at stage logE.
-    const u32 logE = a.logE, E = 1u << logE;
-    const u32 mrows_log = logR - logE;
+// Load (bit-reversed within each column).  Only the first R >> logE rows of
+// a column can be nonzero (zero padding of the message); in bit-reversed
+// order they land on multiples of E, and the first logE DIT stages would
+// merely copy each of them over its block of E words -- done by
+// tile_broadcast, the butterflies then start at stage logE.
+template <int L>
+__device__ __forceinline__ void tile_load(const NttPassArgs& a, const TileGeom& g, u64* sm) {
+    constexpr u32 logR = L;
+    const u32 W = 1u << a.logW, cs = a.cs;
+    const bool first = a.pass == 0, last = a.pass + 1 == a.npass;
+    const u32 mrows_log = logR - a.logE;
+    const u64 S = g.S, col0 = g.col0;
     if (!last) {
         // Thread t always serves column w = t mod W; its rows advance by J.
         const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
         u64* col = sm + w * cs;
         // Row 0 of this column.  The scratch of a middle pass is rewritten in
         // place by this kernel, so it is read with plain loads.
-        const u64* p = first ? src + col0 + w : tmp + P * R * S + col0 + w;
+        const u64* p = first ? g.src + col0 + w : g.tmp + g.P * (1ull << logR) * S + col0 + w;
         const bool full = nrows % (NTT_BATCH * J) == 0 && (!first || ((u64)nrows << a.logS) <= a.m);
         if (full && first) {
             for (u32 jb = j0; jb < nrows; jb += NTT_BATCH * J) {
@@ -253,9 +258,9 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
 #pragma unroll
                 for (int b = 0; b < NTT_BATCH; ++b) {
                     const u32 e = eb + b * blockDim.x;
-                    const u64 i0 = i0base + (e >> mrows_log);
-                    const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + i1;
-                    v[b] = ldg64(tmp + (row << logR) + (e & jmask));
+                    const u64 i0 = g.i0base + (e >> mrows_log);
+                    const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + g.i1;
+                    v[b] = ldg64(g.tmp + (row << logR) + (e & jmask));
                 }
 #pragma unroll
                 for (int b = 0; b < NTT_BATCH; ++b) {
@@ -273,18 +278,18 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
                     v[b] = 0;
                     if (e >= n) continue;
                     if (first) {
-                        if (j < a.m) v[b] = ldg64(src + j);
+                        if (j < a.m) v[b] = ldg64(g.src + j);
                     } else if (a.twist) {
                         // Pass 0 would have broadcast message word j over its
                         // column and scaled row `row` by w_N^(row j): done here.
-                        const u64 row = i0base + w;
-                        const u64 x = j < a.m ? ldg64(src + j) : 0;
+                        const u64 row = g.i0base + w;
+                        const u64 x = j < a.m ? ldg64(g.src + j) : 0;
                         v[b] = gl_mul_fma(x, a.tw_pass ? ldg64(a.tw_pass + (row << logR) + j)
                                                        : twiddle(row * j, a.logN, a.tw_hi, a.tw_lo));
                     } else {
-                        const u64 i0 = i0base + w;
-                        const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + i1;
-                        v[b] = ldg64(tmp + (row << logR) + j);
+                        const u64 i0 = g.i0base + w;
+                        const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + g.i1;
+                        v[b] = ldg64(g.tmp + (row << logR) + j);
                     }
                 }
 #pragma unroll
@@ -295,39 +300,98 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
             }
         }
     }
-    __syncthreads();
-    if (logE) {
-        const u32 nblk = W << mrows_log;  // blocks of E words, head at a multiple of E
-        if (E >= 8 && nblk >= blockDim.x) {
-            for (u32 b = threadIdx.x; b < nblk; b += blockDim.x) {
-                u64* col = sm + (b >> mrows_log) * cs;
-                const u32 p0 = (b & ((1u << mrows_log) - 1)) << logE;
-                const u64 v = col[pidx(p0)];
-                for (u32 k = 1; k < E; ++k) col[pidx(p0 + k)] = v;
-            }
-        } else {
-            for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
-                const u32 w = e >> logR, p = e & (R - 1);
-                if (p & (E - 1)) sm[w * cs + pidx(p)] = sm[w * cs + pidx(p & ~(E - 1))];
+}
+
+// The same loads as asynchronous global -> shared copies (cp.async, 8 bytes
+// each; a word past the message is zero-filled with no read).  Used by the
+// pipelined kernel, which issues a tile's copies while the previous tile is
+// transformed.  Not for the coset-form last pass (its words are products).
+__device__ __forceinline__ void cp_async8(u64* sdst, const u64* gsrc, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gsrc), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int L>
+__device__ __forceinline__ void tile_load_async(const NttPassArgs& a, const TileGeom& g, u64* sm) {
+    constexpr u32 logR = L;
+    const u32 W = 1u << a.logW, cs = a.cs;
+    const bool first = a.pass == 0, last = a.pass + 1 == a.npass;
+    const u32 mrows_log = logR - a.logE;
+    if (!last) {
+        const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
+        const u32 nrows = 1u << mrows_log;
+        u64* col = sm + w * cs;
+        const u64* p = first ? g.src + g.col0 + w : g.tmp + g.P * (1ull << logR) * g.S + g.col0 + w;
+        for (u32 j = threadIdx.x >> a.logW; j < nrows; j += J) {
+            const u64 idx = (u64)j * g.S;
+            const bool valid = !first || idx + g.col0 + w < a.m;
+            // A zero-filled word reads nothing; its source operand is still the
+            // plane's first word (column col0 + w itself may lie past the message).
+            cp_async8(col + pidx(bitrev(j, logR)), valid ? p + idx : (first ? g.src : p), valid);
+        }
+    } else {
+        const u32 n = W << mrows_log, jmask = (1u << mrows_log) - 1;
+        for (u32 e = threadIdx.x; e < n; e += blockDim.x) {
+            const u32 w = e >> mrows_log, j = e & jmask;
+            u64* d = sm + w * cs + pidx(bitrev(j, logR));
+            if (first) {
+                cp_async8(d, j < a.m ? g.src + j : g.src, j < a.m);
+            } else {
+                const u64 i0 = g.i0base + w;
+                const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + g.i1;
+                cp_async8(d, g.tmp + (row << logR) + j, true);
             }
         }
-        __syncthreads();
     }
+}
 
-    // Decimation-in-time stages in register groups of up to 16, natural-order output.
-    dit_stages<L>(sm, a.logW, cs, logE, tws);
+// Copies each loaded head over its block of E = 2^logE words (the first logE
+// stages of the zero-padded transform), then synchronises.
+template <int L>
+__device__ __forceinline__ void tile_broadcast(const NttPassArgs& a, u64* sm) {
+    constexpr u32 logR = L, R = 1u << L;
+    const u32 logE = a.logE, E = 1u << logE, cs = a.cs;
+    if (!logE) return;
+    const u32 W = 1u << a.logW, tileN = W << logR;
+    const u32 mrows_log = logR - logE;
+    const u32 nblk = W << mrows_log;  // blocks of E words, head at a multiple of E
+    if (E >= 8 && nblk >= blockDim.x) {
+        for (u32 b = threadIdx.x; b < nblk; b += blockDim.x) {
+            u64* col = sm + (b >> mrows_log) * cs;
+            const u32 p0 = (b & ((1u << mrows_log) - 1)) << logE;
+            const u64 v = col[pidx(p0)];
+            for (u32 k = 1; k < E; ++k) col[pidx(p0 + k)] = v;
+        }
+    } else {
+        for (u32 e = threadIdx.x; e < tileN; e += blockDim.x) {
+            const u32 w = e >> logR, p = e & (R - 1);
+            if (p & (E - 1)) sm[w * cs + pidx(p)] = sm[w * cs + pidx(p & ~(E - 1))];
+        }
+    }
+    __syncthreads();
+}
 
-    // Store.
+// Store: middle passes scale by the inter-pass factor and write the scratch
+// in place; the last pass writes the codeword plane transposed.
+template <int L>
+__device__ __forceinline__ void tile_store(const NttPassArgs& a, const TileGeom& g, const u64* sm) {
+    constexpr u32 logR = L, R = 1u << L;
+    const u32 W = 1u << a.logW, cs = a.cs;
+    const bool last = a.pass + 1 == a.npass;
+    const u64 N = 1ull << a.logN;
     if (!last) {
         // Inter-pass twiddle w_{Ns}^(col i) (Ns: the sub-transform this pass
         // belongs to): read from the context's table, laid out like the tile
         // rows, or else generated -- thread t keeps col fixed and steps i by J,
         // so the factor advances by the constant w_{Ns}^(col J).
+        const u64 S = g.S;
         const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
-        const u64 col = col0 + w;
+        const u64 col = g.col0 + w;
         u32 i = threadIdx.x >> a.logW;
         const u64 stride = (u64)J * S;
-        u64* dst = tmp + (P * R + i) * S + col;
+        u64* dst = g.tmp + (g.P * R + i) * S + col;
         const u64* scol = sm + w * cs;
         if (a.tw_pass && R % (NTT_BATCH * J) == 0) {
             const u64* tcol = a.tw_pass + (u64)i * S + col;
@@ -355,9 +419,9 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
             }
         }
     } else {
-        u64* out = a.out + (u64)plane * N;
+        u64* out = a.out + (u64)g.plane * N;
         const u64 outer = N >> logR;
-        const u64 obase = a.npass == 3 ? i0base + ((u64)i1 << a.logR0) : i0base;
+        const u64 obase = a.npass == 3 ? g.i0base + ((u64)g.i1 << a.logR0) : g.i0base;
         const u32 w = threadIdx.x & (W - 1), J = blockDim.x >> a.logW;
         const u64* scol = sm + w * cs;
         u32 i = threadIdx.x >> a.logW;
@@ -374,6 +438,60 @@ __global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
         } else {
             for (; i < R; i += J, dst += stride) *dst = scol[pidx(i)];
         }
+    }
+}
+
+template <int L>
+__device__ __forceinline__ void fill_twiddles(const NttPassArgs& a, u64* tws) {
+    for (u32 u = threadIdx.x; u < (1u << L) / 2; u += blockDim.x) tws[twz(u)] = a.tw_stage[u << (TW_STAGE_LOG - L)];
+}
+
+// One pass over all planes, one tile per CTA (blockIdx.x = tile of the
+// plane, blockIdx.y = plane).  MINB = CTAs per SM the register allocation is
+// sized for (the pass plan picks the variant).
+template <int MINB, int L>
+__global__ void __launch_bounds__(256, MINB) k_ntt_pass(NttPassArgs a) {
+    extern __shared__ u64 sm[];
+    u64* tws = sm + (1u << a.logW) * a.cs;
+    fill_twiddles<L>(a, tws);
+    const TileGeom g = tile_geom<L>(a, blockIdx.x, blockIdx.y);
+    tile_load<L>(a, g, sm);
+    __syncthreads();
+    tile_broadcast<L>(a, sm);
+    // Decimation-in-time stages in register groups of up to 16, natural-order output.
+    dit_stages<L>(sm, a.logW, a.cs, a.logE, tws);
+    tile_store<L>(a, g, sm);
+}
+
+// The same pass as a persistent pipeline: each CTA walks tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ... (tile = plane * tiles_per_plane +
+// tile of the plane) with two tile buffers: the copies of the next tile are
+// in flight (cp.async) while the current one is transformed and stored.  The
+// stage twiddles are filled once per CTA.
+template <int MINB, int L>
+__global__ void __launch_bounds__(256, MINB) k_ntt_pipe(NttPassArgs a) {
+    extern __shared__ u64 sm[];
+    const u32 tile_words = (1u << a.logW) * a.cs;
+    u64* tws = sm + 2 * tile_words;
+    fill_twiddles<L>(a, tws);
+    const u32 total = a.tiles_per_plane * a.planes;
+    u32 tile = blockIdx.x;
+    if (tile < total)
+        tile_load_async<L>(a, tile_geom<L>(a, tile % a.tiles_per_plane, tile / a.tiles_per_plane), sm);
+    cp_async_commit();
+    for (u32 it = 0; tile < total; tile += gridDim.x, ++it) {
+        u64* cur = (it & 1) ? sm + tile_words : sm;
+        u64* nxt = (it & 1) ? sm : sm + tile_words;
+        const u32 next = tile + gridDim.x;
+        if (next < total)
+            tile_load_async<L>(a, tile_geom<L>(a, next % a.tiles_per_plane, next / a.tiles_per_plane), nxt);
+        cp_async_commit();
+        cp_async_wait_prev();  // this tile's copies (all groups but the newest) have landed
+        __syncthreads();
+        tile_broadcast<L>(a, cur);
+        dit_stages<L>(cur, a.logW, a.cs, a.logE, tws);
+        tile_store<L>(a, tile_geom<L>(a, tile % a.tiles_per_plane, tile / a.tiles_per_plane), cur);
+        __syncthreads();  // the buffer is refilled by the next iteration's copies
     }
 }
 
@@ -410,10 +528,11 @@ LdePlan default_plan_lde(u32 logN) {
     return p;
 }
 
-size_t lde_smem_bytes(u32 logR, u32 logW) {
-    return ((size_t)(1u << logW) * col_stride(logR, logW)) * 8 + ((size_t)1 << logR) / 2 * 8 + 16;
+// Shared memory of a pass: the tile (two tiles when pipelined) and the twiddles.
+size_t lde_smem_bytes(u32 logR, u32 logW, bool pipe = false) {
+    return ((size_t)(1u << logW) * col_stride(logR, logW)) * 8 * (pipe ? 2 : 1) + ((size_t)1 << logR) / 2 * 8 + 16;
 }
-constexpr size_t LDE_SMEM_MAX = 100 * 1024;
+constexpr size_t LDE_SMEM_MAX = 100 * 1024, LDE_SMEM_PIPE_MAX = 200 * 1024;
 
 // Columns per CTA of pass s: the plan's choice, or tile <= 8192 words with at
 // most 16 columns; never more than the dimension being grouped.
@@ -427,6 +546,7 @@ static u32 pass_logW(const LdePlan& pl, u32 s, u32 logS) {
 bool lde_plan_valid(const LdePlan& p) {
     if (p.npass < 1 || p.npass > 3 || p.logN > TW_LOG) return false;
     if (p.minb != 0 && (p.minb < 2 || p.minb > 4)) return false;
+    if (p.pipe > 1) return false;
     u32 sum = 0;
     for (u32 s = 0; s < p.npass; ++s) {
         if (p.logR[s] < 1 || p.logR[s] > TW_STAGE_LOG) return false;
@@ -438,6 +558,7 @@ bool lde_plan_valid(const LdePlan& p) {
         rest -= p.logR[s];
         if (p.logW[s] != LDE_W_AUTO && p.logW[s] > 6) return false;  // blockDim (256) must be a multiple of W
         if (lde_smem_bytes(p.logR[s], pass_logW(p, s, rest)) > LDE_SMEM_MAX) return false;
+        if (p.pipe && lde_smem_bytes(p.logR[s], pass_logW(p, s, rest), true) > LDE_SMEM_PIPE_MAX) return false;
     }
     return true;
 }
@@ -482,16 +603,39 @@ LdePlan plan_lde(u32 logN, u32 logX) {
 // compile-time constant.
 typedef void (*NttPassKernel)(NttPassArgs);
 template <int MINB, int... Ls>
-static NttPassKernel pass_kernel_of(u32 l, std::integer_sequence<int, Ls...>) {
+static NttPassKernel pass_kernel_of(u32 l, bool pipe, std::integer_sequence<int, Ls...>) {
     static const NttPassKernel table[] = {k_ntt_pass<MINB, Ls + 1>...};
-    return table[l - 1];
+    static const NttPassKernel ptable[] = {k_ntt_pipe<MINB, Ls + 1>...};
+    return pipe ? ptable[l - 1] : table[l - 1];
 }
-static NttPassKernel pass_kernel(u32 minb, u32 logR) {
+static NttPassKernel pass_kernel(u32 minb, u32 logR, bool pipe = false) {
     static_assert(TW_STAGE_LOG == 11, "one pass kernel per radix up to 2^TW_STAGE_LOG");
     const auto seq = std::make_integer_sequence<int, TW_STAGE_LOG>{};
-    if (minb == 2) return pass_kernel_of<2>(logR, seq);
-    if (minb == 4) return pass_kernel_of<4>(logR, seq);
-    return pass_kernel_of<3>(logR, seq);
+    if (minb == 2) return pass_kernel_of<2>(logR, pipe, seq);
+    if (minb == 4) return pass_kernel_of<4>(logR, pipe, seq);
+    return pass_kernel_of<3>(logR, pipe, seq);
+}
+
+// Resident CTAs per SM of each pipelined kernel and tile width on this
+// device (measured once by lde_prepare; sizes the persistent grids).
+static std::mutex g_occ_mu;
+static std::map<std::tuple<int, u32, u32, u32>, int> g_pipe_occ;  // (device, minb, logR, logW)
+static int pipe_occupancy(u32 minb, u32 logR, u32 logW) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, minb, logR, logW);
+    std::lock_guard<std::mutex> lk(g_occ_mu);
+    auto it = g_pipe_occ.find(key);
+    if (it != g_pipe_occ.end()) return it->second;
+    int n = 0;
+    const size_t smem = lde_smem_bytes(logR, logW, true);
+    if (smem > LDE_SMEM_PIPE_MAX ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, pass_kernel(minb, logR, true), 256, smem) != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    g_pipe_occ[key] = n;
+    return n;
 }
 
 int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
@@ -515,6 +659,7 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
     // reads the message and applies the factors itself (the coset form of the
     // LDE), and pass 0 is not launched.
     const bool twist = pl.npass == 2 && L.m <= (1ull << pl.logR[1]);
+    a.planes = L.planes;
     u32 logrest = L.logN;
     for (u32 s = 0; s < pl.npass; ++s) {
         a.pass = s;
@@ -551,9 +696,18 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
         a.tw_pass = !L.tables ? nullptr
                     : s + 1 < pl.npass ? L.tables->get(a.logR + a.logS, a.logR)
                     : twist ? L.tables->get(L.logN, pl.logR[0]) : nullptr;
-        size_t smem = lde_smem_bytes(a.logR, a.logW);
         const u32 mb = pl.minb ? pl.minb : LDE_MINB_DEFAULT;
-        pass_kernel(mb, a.logR)<<<grid, 256, smem, st>>>(a);
+        const int occ = pl.pipe && !twist ? pipe_occupancy(mb, a.logR, a.logW) : 0;
+        if (occ > 0) {
+            // Persistent CTAs: at most the resident count, each walking tiles.
+            a.tiles_per_plane = grid.x;
+            const u64 tiles = (u64)grid.x * L.planes;
+            const u64 cap = (u64)occ * device_sms();
+            const unsigned g1 = (unsigned)std::min<u64>(tiles, cap);
+            pass_kernel(mb, a.logR, true)<<<g1, 256, lde_smem_bytes(a.logR, a.logW, true), st>>>(a);
+        } else {
+            pass_kernel(mb, a.logR)<<<grid, 256, lde_smem_bytes(a.logR, a.logW), st>>>(a);
+        }
         count_launches(1);
     }
     return 0;
@@ -632,10 +786,14 @@ void lde_tables_free(LdeTables& t) {
 
 int lde_prepare() {
     for (u32 mb = 2; mb <= 4; ++mb)
-        for (u32 l = 1; l <= TW_STAGE_LOG; ++l)
+        for (u32 l = 1; l <= TW_STAGE_LOG; ++l) {
             if (cudaFuncSetAttribute(pass_kernel(mb, l), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)LDE_SMEM_MAX) != cudaSuccess)
+                                     (int)LDE_SMEM_MAX) != cudaSuccess ||
+                cudaFuncSetAttribute(pass_kernel(mb, l, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)LDE_SMEM_PIPE_MAX) != cudaSuccess)
                 return -1;
+            for (u32 lw = 0; lw <= 6 && lw <= l; ++lw) pipe_occupancy(mb, l, lw);
+        }
     return 0;
 }
 

@@ -201,8 +201,9 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
         return cudaMemcpyAsync(h, dig, 8, cudaMemcpyDeviceToHost, c->stream) == cudaSuccess &&
                cudaStreamSynchronize(c->stream) == cudaSuccess;
     };
-    // Candidates: every radix split, and columns per CTA in {auto, 0..5} per pass
-    // (three-pass plans with the automatic columns only).
+    // Candidates: every radix split, and columns per CTA in {auto, 1..4} per pass
+    // (three-pass plans with the automatic columns only), each with one tile per
+    // CTA and pipelined.
     std::vector<LdePlan> cand;
     auto add = [&](LdePlan p) {
         p.logN = log_n;
@@ -210,21 +211,22 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
     };
     const u32 A = LDE_W_AUTO;
     const u32 wopts[] = {A, 1, 2, 3, 4};
-    for (u32 mb = 2; mb <= 4; ++mb) {
-        if (log_n <= 11) add(LdePlan{log_n, 1, {log_n, 0, 0}, {A, A, A}, mb});
-        for (u32 r0 = 1; r0 < log_n && r0 <= 11; ++r0) {
-            const u32 r1 = log_n - r0;
-            if (r1 > 11) continue;
-            for (u32 w0 : wopts)
-                for (u32 w1 : wopts) add(LdePlan{log_n, 2, {r0, r1, 0}, {w0, w1, A}, mb});
+    for (u32 pp = 0; pp <= 1; ++pp)
+        for (u32 mb = 2; mb <= 4; ++mb) {
+            if (log_n <= 11) add(LdePlan{log_n, 1, {log_n, 0, 0}, {A, A, A}, mb, pp});
+            for (u32 r0 = 1; r0 < log_n && r0 <= 11; ++r0) {
+                const u32 r1 = log_n - r0;
+                if (r1 > 11) continue;
+                for (u32 w0 : wopts)
+                    for (u32 w1 : wopts) add(LdePlan{log_n, 2, {r0, r1, 0}, {w0, w1, A}, mb, pp});
+            }
+            if (log_n >= 12)
+                for (u32 r0 = 1; r0 <= 11; ++r0)
+                    for (u32 r1 = 1; r1 <= 11 && r0 + r1 < log_n; ++r1) {
+                        const u32 r2 = log_n - r0 - r1;
+                        if (r2 >= 1 && r2 <= 11) add(LdePlan{log_n, 3, {r0, r1, r2}, {A, A, A}, mb, pp});
+                    }
         }
-        if (log_n >= 12)
-            for (u32 r0 = 1; r0 <= 11; ++r0)
-                for (u32 r1 = 1; r1 <= 11 && r0 + r1 < log_n; ++r1) {
-                    const u32 r2 = log_n - r0 - r1;
-                    if (r2 >= 1 && r2 <= 11) add(LdePlan{log_n, 3, {r0, r1, r2}, {A, A, A}, mb});
-                }
-    }
     if (cand.empty()) return fail(c, WHIRGPU_E_INVALID, "no valid plan");
 
     unsigned long long want = 0;
@@ -271,6 +273,7 @@ whirgpu_status whirgpu_ntt_autotune(whirgpu_ctx* c, uint32_t log_n, uint32_t log
     best->log_expansion = log_expansion;
     best->npass = best_p.npass;
     best->min_blocks = best_p.minb;
+    best->pipelined = best_p.pipe;
     for (int k = 0; k < 3; ++k) {
         best->log_radix[k] = best_p.logR[k];
         best->log_cols[k] = best_p.logW[k];
@@ -287,6 +290,7 @@ whirgpu_status whirgpu_ntt_set_plan(const whirgpu_ntt_plan* p) {
     q.logN = p->log_n;
     q.npass = p->npass;
     q.minb = p->min_blocks;
+    q.pipe = p->pipelined;
     for (int k = 0; k < 3; ++k) {
         q.logR[k] = k < (int)p->npass ? p->log_radix[k] : 0;
         q.logW[k] = k < (int)p->npass ? p->log_cols[k] : LDE_W_AUTO;
@@ -303,6 +307,7 @@ whirgpu_status whirgpu_ntt_get_plan(uint32_t log_n, uint32_t log_expansion, whir
     out->log_expansion = log_expansion;
     out->npass = p.npass;
     out->min_blocks = p.minb;
+    out->pipelined = p.pipe;
     for (int k = 0; k < 3; ++k) {
         out->log_radix[k] = p.logR[k];
         out->log_cols[k] = p.logW[k];
@@ -321,6 +326,7 @@ size_t whirgpu_ntt_list_plans(whirgpu_ntt_plan* out, size_t cap) {
         out[i].log_expansion = keys[i] & 0xFF;
         out[i].npass = plans[i].npass;
         out[i].min_blocks = plans[i].minb;
+        out[i].pipelined = plans[i].pipe;
         for (int k = 0; k < 3; ++k) {
             out[i].log_radix[k] = plans[i].logR[k];
             out[i].log_cols[k] = plans[i].logW[k];
@@ -381,10 +387,12 @@ whirgpu_status whirgpu_ntt_load_plans(const char* path, size_t* loaded) {
         if (!read_int_field(obj, "log_n", &ln) || !read_int_field(obj, "log_expansion", &lx) ||
             !read_int_field(obj, "npass", &np) || !read_triple(obj, "log_radix", r) || !read_triple(obj, "log_cols", w))
             continue;
-        long mb = 0;
+        long mb = 0, pp = 0;
         read_int_field(obj, "min_blocks", &mb);  // optional
+        read_int_field(obj, "pipelined", &pp);   // optional
         whirgpu_ntt_plan pl{};
         pl.min_blocks = (uint32_t)mb;
+        pl.pipelined = (uint32_t)pp;
         pl.log_n = (uint32_t)ln;
         pl.log_expansion = (uint32_t)lx;
         pl.npass = (uint32_t)np;
@@ -410,9 +418,9 @@ whirgpu_status whirgpu_ntt_save_plans(const char* path) {
         const auto& p = v[i];
         std::fprintf(f,
                      "  {\"log_n\": %u, \"log_expansion\": %u, \"npass\": %u, \"log_radix\": [%u, %u, %u], "
-                     "\"log_cols\": [%u, %u, %u], \"min_blocks\": %u}%s\n",
+                     "\"log_cols\": [%u, %u, %u], \"min_blocks\": %u, \"pipelined\": %u}%s\n",
                      p.log_n, p.log_expansion, p.npass, p.log_radix[0], p.log_radix[1], p.log_radix[2], p.log_cols[0],
-                     p.log_cols[1], p.log_cols[2], p.min_blocks, i + 1 < v.size() ? "," : "");
+                     p.log_cols[1], p.log_cols[2], p.min_blocks, p.pipelined, i + 1 < v.size() ? "," : "");
     }
     std::fprintf(f, "]}\n");
     std::fclose(f);

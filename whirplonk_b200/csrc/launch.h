@@ -22,12 +22,16 @@ constexpr u32 TW_LOG = 26, TW_HALF = 13, TW_STAGE_LOG = 11;
 // A pass plan: npass passes of radix 2^logR[s] (sum = logN, each <= 2^11),
 // pass s staging 2^logW[s] columns per CTA (LDE_W_AUTO: the built-in choice).
 // minb: CTAs per SM the kernel's registers are sized for (2, 3 or 4; 0 = default).
+// pipe: run the passes as persistent CTAs that copy the next tile in while
+// transforming the current one (two tile buffers); the coset-form last pass
+// always runs one tile per CTA.
 constexpr u32 LDE_W_AUTO = 0xFF, LDE_MINB_DEFAULT = 3;
 struct LdePlan {
     u32 logN, npass;
     u32 logR[3];
     u32 logW[3];
     u32 minb;
+    u32 pipe;
 };
 struct NttPassArgs {
     const u64* src[3];
@@ -37,6 +41,7 @@ struct NttPassArgs {
     u32 depth, logN, logR, logS, logW, npass, pass, logR0, logR1, logE;
     u32 twist;  // last pass of two whose first is a pure broadcast (m <= columns): reads the message itself
     u32 cs;     // shared-memory words per tile column
+    u32 tiles_per_plane, planes;  // pipelined kernel: tiles of one plane, planes
     const u64* tw_stage;
     const u64* tw_hi;
     const u64* tw_lo;
