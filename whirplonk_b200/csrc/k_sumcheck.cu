@@ -636,8 +636,12 @@ __global__ void k_cov_acc_tables(const ProofScalars* sc, int n_ext, int n_points
 }
 
 // Two consecutive elements (same row h) per thread: each T_j[h] load serves
-// both, and the base points go four at a time with their loads first.
-__global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* tab, const u64* lo_base, u32 hi_count) {
+// both.  The Ext3 points (the OOD samples, few) take full Ext3 products and are
+// reduced first; the base points then accumulate into three 192-bit sums per
+// element, two points at a time with their loads first -- small enough
+// accumulators for three CTAs per SM.
+__global__ void __launch_bounds__(256, 3) k_cov_accumulate(CovAccArgs a, const E3* tab, const u64* lo_base,
+                                                           u32 hi_count) {
     constexpr u32 NL = 1u << CA_LO;
     const u32 per = NL + hi_count;
     const int npts = a.n_ext + a.n_base;
@@ -646,37 +650,48 @@ __global__ void __launch_bounds__(256) k_cov_accumulate(CovAccArgs a, const E3* 
         const u64 i = 2 * pi;
         const bool two = i + 1 < a.size;
         const u32 hi = (u32)(i >> CA_LO), lo = (u32)(i & (NL - 1));  // lo even: lo + 1 < NL
-        E3Acc s0 = e3acc_zero(), s1 = e3acc_zero();
-        for (int j = 0; j < a.n_ext; ++j) {
-            const E3* tj = tab + (u64)j * per;
-            const E3 w = tj[NL + hi];
-            e3acc_mac(s0, w, tj[lo]);
-            e3acc_mac(s1, w, tj[lo + 1]);
+        E3 e0 = e3_zero(), e1 = e3_zero();
+        for (u32 k = 0; k < 2 && a.n_ext > 0; ++k) {  // one element at a time: one E3Acc live
+            E3Acc s = e3acc_zero();
+            for (int j = 0; j < a.n_ext; ++j) e3acc_mac(s, tab[(u64)j * per + NL + hi], tab[(u64)j * per + lo + k]);
+            const E3 r = e3acc_reduce(s);
+            if (k == 0) e0 = r;
+            else e1 = r;
         }
+        Acc192 b0[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, b1[3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         int j = a.n_ext;
-        for (; j + 4 <= npts; j += 4) {
-            E3 w[4];
-            u64 x0[4], x1[4];
+        for (; j + 2 <= npts; j += 2) {
+            E3 w[2];
+            u64 x0[2], x1[2];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < 2; ++q) {
                 w[q] = tab[(u64)(j + q) * per + NL + hi];
-                const u64* lb = lo_base + (u64)(j + q - a.n_ext) * NL + lo;
-                x0[q] = lb[0];
-                x1[q] = lb[1];
+                const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(lo_base + (u64)(j + q - a.n_ext) * NL + lo);
+                x0[q] = x.x;
+                x1[q] = x.y;
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                e3acc_mac_base(s0, w[q], x0[q]);
-                e3acc_mac_base(s1, w[q], x1[q]);
+            for (int q = 0; q < 2; ++q) {
+                acc_mac(b0[0], w[q].c0, x0[q]);
+                acc_mac(b0[1], w[q].c1, x0[q]);
+                acc_mac(b0[2], w[q].c2, x0[q]);
+                acc_mac(b1[0], w[q].c0, x1[q]);
+                acc_mac(b1[1], w[q].c1, x1[q]);
+                acc_mac(b1[2], w[q].c2, x1[q]);
             }
         }
         for (; j < npts; ++j) {
-            const E3 w = tab[(u64)j * per + NL + hi];
+            const E3 wj = tab[(u64)j * per + NL + hi];
             const u64* lb = lo_base + (u64)(j - a.n_ext) * NL + lo;
-            e3acc_mac_base(s0, w, lb[0]);
-            e3acc_mac_base(s1, w, lb[1]);
+            acc_mac(b0[0], wj.c0, lb[0]);
+            acc_mac(b0[1], wj.c1, lb[0]);
+            acc_mac(b0[2], wj.c2, lb[0]);
+            acc_mac(b1[0], wj.c0, lb[1]);
+            acc_mac(b1[1], wj.c1, lb[1]);
+            acc_mac(b1[2], wj.c2, lb[1]);
         }
-        const E3 add0 = ef_fix(e3acc_reduce(s0), a.ext2), add1 = ef_fix(e3acc_reduce(s1), a.ext2);
+        const E3 add0 = ef_fix(e3_add(e0, E3{acc_reduce(b0[0]), acc_reduce(b0[1]), acc_reduce(b0[2])}), a.ext2);
+        const E3 add1 = ef_fix(e3_add(e1, E3{acc_reduce(b1[0]), acc_reduce(b1[1]), acc_reduce(b1[2])}), a.ext2);
         if (two) {
             const u64 d0[3] = {add0.c0, add0.c1, add0.c2}, d1[3] = {add1.c0, add1.c1, add1.c2};
 #pragma unroll
