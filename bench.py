@@ -1110,8 +1110,12 @@ def run_served(args, H, ctx, w):
             continue
         sub = [dev_reqs[i] for i in idx]
         serve(srv, sub)  # programs of this class captured, state as in the timed pass
-        ms, res = H.timed(stream, lambda: serve(srv, sub))
-        assert all(r.status == 0 and (r.narg, r.hints) == expected[i] for i, r in zip(idx, res))
+        passes = []
+        for _ in range(3):  # a class is a fraction of a second of work: median of three passes
+            ms, res = H.timed(stream, lambda: serve(srv, sub))
+            assert all(r.status == 0 and (r.narg, r.hints) == expected[i] for i, r in zip(idx, res))
+            passes.append(ms)
+        ms = statistics.median(passes)
         p_ms = sum(plain_lat[i] for i in idx)
         classes[name] = {"requests": len(idx), "served_proofs_per_s": len(idx) / (ms / 1000.0),
                          "plain_proofs_per_s": len(idx) / (p_ms / 1000.0), "served_vs_plain": p_ms / ms,
