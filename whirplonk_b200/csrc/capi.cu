@@ -138,9 +138,51 @@ namespace {
 
 void free_workspace(whirgpu_ctx* c, Workspace* w) {
     for (auto& kv : w->on_free) kv.second();
+    for (auto& kv : w->plain_graphs) cudaGraphExecDestroy(kv.second.exec);
     cudaFree(w->dev);
     c->allocated -= w->plan.total_bytes;
     delete w;
+}
+
+// Runs `enqueue(stream, timer)` on the context stream.  Without the family
+// timer the kernels are captured into a graph on the first call with `key`
+// for this workspace (and NTT plan epoch) and replayed from then on: one graph
+// launch instead of ~100 kernel launches per proof.  Returns 0 on success.
+template <class F>
+int run_captured(whirgpu_ctx* c, Workspace* ws, uint64_t key, F enqueue) {
+    if (c->timer) return enqueue(c->stream, c->timer.get());
+    const uint32_t epoch = lde_plan_epoch();
+    key = key << 32 | epoch;
+    auto it = ws->plain_graphs.find(key);
+    if (it == ws->plain_graphs.end()) {
+        for (auto jt = ws->plain_graphs.begin(); jt != ws->plain_graphs.end();) {  // captured under older plans
+            if ((uint32_t)jt->first != epoch) {
+                cudaGraphExecDestroy(jt->second.exec);
+                jt = ws->plain_graphs.erase(jt);
+            } else {
+                ++jt;
+            }
+        }
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1;
+        set_capturing(true);
+        const int rc = enqueue(c->stream, nullptr);
+        set_capturing(false);
+        const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+        Workspace::Captured cap;
+        if (rc == 0 && ce == cudaSuccess) {
+            cap.kernels = graph_kernel_nodes(g);
+            if (cudaGraphInstantiate(&cap.exec, g, 0) != cudaSuccess) cap.exec = nullptr;
+        }
+        if (g) cudaGraphDestroy(g);
+        if (!cap.exec) {  // not capturable: launch directly
+            cudaGetLastError();
+            return rc ? rc : enqueue(c->stream, nullptr);
+        }
+        it = ws->plain_graphs.emplace(key, cap).first;
+    }
+    count_launches(it->second.kernels);
+    return cudaGraphLaunch(it->second.exec, c->stream) == cudaSuccess ? 0 : -1;
 }
 
 // Frees idle workspaces, least recently used first, until `need` more bytes
@@ -456,7 +498,9 @@ whirgpu_status commit_schedule(whirgpu_ctx* c, const WhirSchedule& sched, const 
     if (e != cudaSuccess) { release_workspace(c, ws); return cuda_fail(c, e, "input copy"); }
     c->io_h2d = (where == WHIRGPU_INPUT_DEVICE ? 0 : coeff_bytes) + tx->ds.size();
     c->io_d2h = 0;
-    if (enqueue_commit(p, ws->dev, (uint32_t)tx->ds.size(), c->tw, c->stream, c->timer.get()) != 0) {
+    const uint32_t ds_len = (uint32_t)tx->ds.size();
+    if (run_captured(c, ws, (uint64_t)ds_len << 8 | 0x1,
+                     [&](cudaStream_t st, Timer* tm) { return enqueue_commit(p, ws->dev, ds_len, c->tw, st, tm); }) != 0) {
         release_workspace(c, ws);
         return fail(c, WHIRGPU_E_INVALID, "commit launch failed");
     }
@@ -656,7 +700,12 @@ whirgpu_status whirgpu_prove_forms(whirgpu_ctx* c, whirgpu_witness* w, const whi
         c->io_h2d += num_points * p.nvec * 24;
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "statement upload");
-    if (enqueue_prove(p, ws, c->tw, c->stream, c->timer.get()) != 0) return fail(c, WHIRGPU_E_INVALID, "prove launch failed");
+    // Statements with dense covectors name caller memory: launched directly.
+    const int rc = p.dense_mask ? enqueue_prove(p, ws, c->tw, c->stream, c->timer.get())
+                                : run_captured(c, w->ws, (uint64_t)num_points << 8 | 0x2, [&](cudaStream_t st, Timer* tm) {
+                                      return enqueue_prove(p, ws, c->tw, st, tm);
+                                  });
+    if (rc != 0) return fail(c, WHIRGPU_E_INVALID, "prove launch failed");
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "prove kernels");
     // Read-back: transcript state, narg (exact size), hints (bounded), challenges.

@@ -79,6 +79,13 @@ struct Workspace {
     bool busy = false;
     uint64_t last_used = 0;                    // LRU stamp for eviction of idle workspaces
     std::map<const void*, std::function<void()>> on_free;  // per owner: drops state tied to `dev` (captured graphs)
+    // The single-proof calls' kernels as captured graphs (commit; prove per
+    // statement count), keyed with the NTT plan epoch they were captured under.
+    struct Captured {
+        cudaGraphExec_t exec = nullptr;
+        uint64_t kernels = 0;
+    };
+    std::map<uint64_t, Captured> plain_graphs;
 };
 
 }  // namespace wg

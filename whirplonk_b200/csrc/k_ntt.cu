@@ -16,6 +16,7 @@
 // LDE reads m = N/e words per plane), the last pass writes the codeword planes
 // M[plane][i] that the leaf hasher and the opener read.
 #include <algorithm>
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -565,17 +566,21 @@ bool lde_plan_valid(const LdePlan& p) {
 
 static std::mutex g_plan_mu;
 static std::map<u32, LdePlan> g_plans;  // key logN << 8 | logX
+static std::atomic<u32> g_plan_epoch{0};
 
 void lde_install_plan(u32 logX, const LdePlan& p) {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     const u32 key = p.logN << 8 | logX;
     if (p.npass == 0) g_plans.erase(key);
     else g_plans[key] = p;
+    ++g_plan_epoch;
 }
 void lde_clear_plans() {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     g_plans.clear();
+    ++g_plan_epoch;
 }
+u32 lde_plan_epoch() { return g_plan_epoch.load(); }
 size_t lde_installed_plans(u32* keys, LdePlan* plans, size_t cap) {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     size_t i = 0;

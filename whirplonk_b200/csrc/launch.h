@@ -87,6 +87,9 @@ LdePlan default_plan_lde(u32 logN);
 bool lde_plan_valid(const LdePlan& p);
 void lde_install_plan(u32 logX, const LdePlan& p);  // p.npass == 0 removes
 void lde_clear_plans();
+// Incremented by every plan install or clear (captured graphs hold the plans
+// of their capture and are re-captured after a change).
+u32 lde_plan_epoch();
 size_t lde_installed_plans(u32* keys, LdePlan* plans, size_t cap);  // keys: logN << 8 | logX
 // Launches one LDE with an explicit plan (autotuner).
 int launch_lde_plan(const LdeArgs& a, const LdePlan& pl, cudaStream_t st);
