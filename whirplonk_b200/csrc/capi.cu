@@ -19,6 +19,7 @@
 
 #include "../../include/whirgpu.h"
 #include "ctx.h"
+#include "host_keccak.h"
 #include "launch.h"
 #include "prover.h"
 #include "state.cuh"
@@ -28,40 +29,20 @@ using namespace wg;
 namespace {
 
 // ---------------------------------------------------------------------------
-// Host Keccak / SHA3 (FIPS 202) for the domain-separator helper; constants
-// from the compile-time derivations shared with the device transcript.
+// Host SHA3 (FIPS 202) for the domain-separator helpers, on the table-driven
+// host permutation of host_keccak.cpp.
 // ---------------------------------------------------------------------------
-void keccak_f1600_host(uint64_t a[25]) {
-    for (int round = 0; round < 24; ++round) {
-        uint64_t c[5], b[25];
-        for (int x = 0; x < 5; ++x) c[x] = a[x] ^ a[x + 5] ^ a[x + 10] ^ a[x + 15] ^ a[x + 20];
-        for (int x = 0; x < 5; ++x) {
-            const uint64_t r = c[(x + 1) % 5];
-            const uint64_t d = c[(x + 4) % 5] ^ ((r << 1) | (r >> 63));
-            for (int y = 0; y < 5; ++y) a[x + 5 * y] ^= d;
-        }
-        for (int x = 0; x < 5; ++x)
-            for (int y = 0; y < 5; ++y) {
-                const int s = keccak_rho(x, y);
-                const uint64_t v = a[x + 5 * y];
-                b[y + 5 * ((2 * x + 3 * y) % 5)] = s ? ((v << s) | (v >> (64 - s))) : v;
-            }
-        for (int y = 0; y < 5; ++y)
-            for (int x = 0; x < 5; ++x) a[x + 5 * y] = b[x + 5 * y] ^ (~b[(x + 1) % 5 + 5 * y] & b[(x + 2) % 5 + 5 * y]);
-        a[0] ^= keccak_rc(round);
-    }
-}
 void sha3_host(const uint8_t* d, size_t n, size_t rate, uint8_t* out, size_t outlen) {
     uint64_t s[25] = {};
     size_t pos = 0;
     auto xb = [&](size_t p, uint8_t v) { s[p / 8] ^= (uint64_t)v << (8 * (p % 8)); };
     for (size_t i = 0; i < n; ++i) {
         xb(pos++, d[i]);
-        if (pos == rate) { keccak_f1600_host(s); pos = 0; }
+        if (pos == rate) { keccak_f1600_cpu(s); pos = 0; }
     }
     xb(pos, 0x06);
     xb(rate - 1, 0x80);
-    keccak_f1600_host(s);
+    keccak_f1600_cpu(s);
     for (size_t i = 0; i < outlen; ++i) out[i] = (uint8_t)(s[i / 8] >> (8 * (i % 8)));
 }
 
