@@ -114,7 +114,10 @@ whirgpu_status whirgpu_proof_get(const whirgpu_transcript* tx, const uint8_t** n
  * (irs_commit::Config::commit with num_vectors = batch_size,
  * irs_commit.hpp:344-561); the codeword matrix and Merkle tree stay in HBM in
  * the witness.  Work is queued on the context stream; the call returns without
- * waiting for it. */
+ * waiting for it.  The commit's kernels are captured into a CUDA graph on the
+ * first call of a workspace (a proof shape) and replayed by later calls; an
+ * NTT plan install or clear, or the family timer (whirgpu_set_timing), makes
+ * the next call capture anew or launch directly. */
 whirgpu_status whirgpu_commit(whirgpu_ctx* ctx, const whirgpu_params* params, const uint64_t* coeffs,
                               uint64_t num_variables, int coeffs_location, whirgpu_transcript* tx,
                               whirgpu_witness** out);
@@ -183,7 +186,9 @@ whirgpu_status whirgpu_commit_config(whirgpu_ctx* ctx, const whirgpu_config* con
  * num_points * num_variables Ext3 coordinates (3 words each, c0 c1 c2),
  * evaluations are num_points * V Ext3 values, form-major (the claimed MLE value
  * of form f on vector v at f * V + v), V = the witness's committed vectors.
- * On return the proof is complete and readable with whirgpu_proof_get.
+ * On return the proof is complete and readable with whirgpu_proof_get.  Like
+ * the commit, the prove replays a graph captured on the workspace's first call
+ * with the same statement count (dense covector statements launch directly).
  * evaluation_point (optional) receives num_variables Ext3 values (the
  * FinalClaim evaluation point), rlc (optional) num_points Ext3 values. */
 whirgpu_status whirgpu_prove(whirgpu_ctx* ctx, whirgpu_witness* witness, const uint64_t* points, size_t num_points,

@@ -100,3 +100,30 @@ def test_prove_matches_reference_large(gpu_ctx, n, rho):
     narg, hints, _ = prove_once(n, params, coeffs, points, ev, ctx=gpu_ctx)
     assert narg == ref.narg, f"narg differs at byte {first_diff(narg, ref.narg)}"
     assert hints == ref.hints, f"hints differ at byte {first_diff(hints, ref.hints)}"
+
+
+def test_replayed_graphs_follow_inputs_statements_and_plans(gpu_ctx, oracle):
+    """Commit and prove replay graphs captured on a workspace's first call: later
+    calls of the same shape with other coefficients and points, with another
+    statement count (its own graph) and after an NTT plan change (re-captured)
+    must all still equal the oracle's proofs."""
+    import ctypes
+
+    from whirplonk_b200 import _lib
+    from whirplonk_b200.autotune import load as load_plans
+
+    n, k, rho = 12, 4, 2
+    for seed, npts in [(501, 1), (502, 1), (503, 2), (504, 1), (505, 2)]:
+        check_against_oracle(gpu_ctx, oracle, n, k, rho, 100, 20, seed=seed, npts=npts)
+    L = _lib.load()
+    plan = _lib.NttPlan()
+    ln = n - k + rho
+    _lib.check(L.whirgpu_ntt_get_plan(ln, rho, ctypes.byref(plan)))
+    forced = _lib.NttPlan(ln, rho, 2, (1, ln - 1, 0), (255, 255, 255), 3, 0)
+    try:
+        assert L.whirgpu_ntt_set_plan(ctypes.byref(forced)) == _lib.OK
+        check_against_oracle(gpu_ctx, oracle, n, k, rho, 100, 20, seed=506)
+    finally:
+        L.whirgpu_ntt_clear_plans()
+        load_plans()
+    check_against_oracle(gpu_ctx, oracle, n, k, rho, 100, 20, seed=507)
