@@ -290,7 +290,10 @@ __global__ void k_sc_after_pow(TxState* tx, ProofScalars* sc, int r_slot) {
 // sizes.
 // ---------------------------------------------------------------------------
 constexpr u64 SC_SMALL_MAX = 1ull << 12;
-constexpr int SC_SMALL_THREADS = 1024;
+// 512 threads leave the kernel 128 registers a thread: at 1024 its 192-bit
+// accumulators and the transcript state spilled to local memory.
+constexpr int SC_SMALL_THREADS = 512;
+constexpr int SC_SMALL_WARPS = SC_SMALL_THREADS / 32;
 
 struct ScSmallArgs {
     const u64* a_base;  // base-field coefficients (first sumcheck) or null
@@ -304,18 +307,23 @@ struct ScSmallArgs {
 };
 
 __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs a) {
-    __shared__ E3 red[32];
-    __shared__ E3 tot[2];
+    __shared__ E3 red[2][SC_SMALL_WARPS];
+    __shared__ E3 rsh;  // the round's challenge, handed from warp 0 to the CTA
     ProofScalars* sc = a.sc;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     WarpTx wt;
-    if (threadIdx.x < 32) wtx_load(wt, a.tx);
+    E3 sum{};
+    if (warp == 0) {
+        wtx_load(wt, a.tx);
+        sum = sc->sum;
+    }
     for (int t = 0; t <= a.rounds; ++t) {
         const bool last = t == a.rounds;  // only the trailing fold
         if (last && !a.fold_after) break;
         const u64 size = a.size >> t;
         const bool fold = t > 0;
         const bool base = a.a_base && t <= 1;
-        const FoldR r = fold_r(fold ? sc->sc_r[a.r_slot + t - 1] : e3_zero());
+        const FoldR r = fold_r(fold ? rsh : e3_zero());
         ScKernelArgs k{};
         k.a_base = base ? a.a_base : nullptr;
         for (int c = 0; c < 3; ++c) { k.a_in[c] = a.a[c]; k.a_out[c] = a.a[c]; k.b[c] = a.b[c]; }
@@ -346,30 +354,37 @@ __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs
                 accl_mac(c2, e3_sub(ah, al), e3_sub(bh, bl));
             }
         }
-        const E3 s0 = block_sum(ef_fix(accl_reduce(c0), a.ext2), red);
-        const E3 s2 = block_sum(ef_fix(accl_reduce(c2), a.ext2), red);
-        if (threadIdx.x == 0) {
-            tot[0] = s0;
-            tot[1] = s2;
+        // Both sums in one barrier: warp partials to shared memory, then warp 0
+        // adds them lane-parallel (field sums are exact, so order is free).
+        const E3 w0 = e3_warp_sum(ef_fix(accl_reduce(c0), a.ext2));
+        const E3 w2 = e3_warp_sum(ef_fix(accl_reduce(c2), a.ext2));
+        if (lane == 0) {
+            red[0][warp] = w0;
+            red[1][warp] = w2;
         }
         __syncthreads();
-        if (threadIdx.x < 32) {
-            const E3 C0 = tot[0], C2 = tot[1];
+        if (warp == 0) {
+            const E3 C0 = e3_warp_sum(lane < SC_SMALL_WARPS ? red[0][lane] : e3_zero());
+            const E3 C2 = e3_warp_sum(lane < SC_SMALL_WARPS ? red[1][lane] : e3_zero());
             wtx_message_t(wt, C0);
             wtx_message_t(wt, C2);
             const E3 rn = wtx_challenge_t(wt);
-            if (threadIdx.x == 0) {
-                const E3 c1 = e3_sub(e3_sub(sc->sum, e3_add(C0, C0)), C2);
+            const bool x2 = wt.deg == 2;
+            const E3 c1 = e3_sub(e3_sub(sum, e3_add(C0, C0)), C2);
+            sum = e3_add(ef_mul(e3_add(ef_mul(C2, rn, x2), c1), rn, x2), C0);
+            if (lane == 0) {
                 sc->c0 = C0;
                 sc->c2 = C2;
                 sc->sc_r[a.r_slot + t] = rn;
-                const bool x2 = wt.deg == 2;
-                sc->sum = e3_add(ef_mul(e3_add(ef_mul(C2, rn, x2), c1), rn, x2), C0);
+                rsh = rn;
             }
         }
         __syncthreads();
     }
-    if (threadIdx.x < 32) wtx_store(wt, a.tx);
+    if (warp == 0) {
+        if (lane == 0) sc->sum = sum;
+        wtx_store(wt, a.tx);
+    }
 }
 
 int launch_sumcheck_small(const SumcheckArgs& s, int rounds, int fold_after, cudaStream_t st) {
