@@ -340,11 +340,21 @@ __device__ __forceinline__ E3 e3_load(const E3Planes& p, u64 i) { return E3{p.c0
 __device__ __forceinline__ void e3_store(const E3Planes& p, u64 i, E3 v) { p.c0[i] = v.c0; p.c1[i] = v.c1; p.c2[i] = v.c2; }
 
 // Warp-wide field sum (exact; any association order gives the same value).
+// The loops stay rolled: these sums run once per warp per launch, mostly in
+// single-warp kernels whose time goes to fetching straight-line code.
 __device__ __forceinline__ u64 gl_warp_sum(u64 v) {
-#pragma unroll
+#pragma unroll 1
     for (int o = 16; o > 0; o >>= 1) v = gl_add(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
     return v;
 }
-__device__ __forceinline__ E3 e3_warp_sum(E3 v) { return E3{gl_warp_sum(v.c0), gl_warp_sum(v.c1), gl_warp_sum(v.c2)}; }
+__device__ __forceinline__ E3 e3_warp_sum(E3 v) {
+#pragma unroll 1
+    for (int o = 16; o > 0; o >>= 1) {
+        v.c0 = gl_add(v.c0, __shfl_xor_sync(0xFFFFFFFFu, v.c0, o));
+        v.c1 = gl_add(v.c1, __shfl_xor_sync(0xFFFFFFFFu, v.c1, o));
+        v.c2 = gl_add(v.c2, __shfl_xor_sync(0xFFFFFFFFu, v.c2, o));
+    }
+    return v;
+}
 
 }  // namespace wg

@@ -429,36 +429,60 @@ __global__ void k_ood_tables(const E3* pts, int n_ood, u32 hi_count, E3* tab, bo
     }
 }
 
-// Sum over chunk h (2^LO coefficients) of vector v against point table j, one
-// value per lane (unreduced products, reduced once, scaled by z_j^(h 2^LO)).
-__device__ __forceinline__ E3 ood_chunk(const OodArgs& a, const E3* zlo, const E3* zhi, u32 v, u64 h, u32 lane) {
+// Sum over coefficients off .. off + len - 1 of chunk h (2^LO coefficients)
+// of vector v against point table j, one value per lane (unreduced products,
+// reduced once, scaled by z_j^(h 2^LO)).  Every load of a batch -- the
+// coefficients and their table powers, 4 Ext3 or 8 base elements per lane --
+// is issued before its products, so a warp waits for memory once per batch.
+__device__ __forceinline__ E3 ood_part(const OodArgs& a, const E3* zlo, const E3* zhi, u32 v, u64 h, u32 off,
+                                       u32 len, u32 lane) {
     const u64* b0 = a.v[0] + (u64)v * a.vec_stride;
-    const u64 base = h << OOD_LO;
-    const u32 cnt = (u32)((a.size - base) < (1ull << OOD_LO) ? (a.size - base) : (1ull << OOD_LO));
+    const u64 base = (h << OOD_LO) + off;
+    const u64 rest = a.size > base ? a.size - base : 0;
+    const u32 cnt = (u32)(rest < len ? rest : len);
+    const E3* zl = zlo + off;
     E3Acc s = e3acc_zero();
-    if (a.ext3) {
-        for (u32 l = lane; l < cnt; l += 32) e3acc_mac(s, zlo[l], E3{b0[base + l], a.v[1][base + l], a.v[2][base + l]});
-    } else if (cnt == (1u << OOD_LO)) {
-        // a full block: eight coalesced loads in flight per lane before the products
-        for (u32 l0 = lane; l0 < cnt; l0 += 256) {
-            u64 x[8];
+    u32 l = lane;
+    if (a.ext3) {  // one vector (nvec == 1): components in v[0..2]
+        const u64* b1 = a.v[1];
+        const u64* b2 = a.v[2];
+        for (; l + 96 < cnt; l += 128) {
+            E3 x[4], z[4];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) x[k] = b0[base + l0 + 32 * k];
+            for (int k = 0; k < 4; ++k) {
+                const u64 i = base + l + 32 * k;
+                x[k] = E3{b0[i], b1[i], b2[i]};
+                z[k] = zl[l + 32 * k];
+            }
 #pragma unroll
-            for (int k = 0; k < 8; ++k) e3acc_mac_base(s, zlo[l0 + 32 * k], x[k]);
+            for (int k = 0; k < 4; ++k) e3acc_mac(s, z[k], x[k]);
         }
+        for (; l < cnt; l += 32) e3acc_mac(s, zl[l], E3{b0[base + l], b1[base + l], b2[base + l]});
     } else {
-        for (u32 l = lane; l < cnt; l += 32) e3acc_mac_base(s, zlo[l], b0[base + l]);
+        for (; l + 224 < cnt; l += 256) {
+            u64 x[8];
+            E3 z[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                x[k] = b0[base + l + 32 * k];
+                z[k] = zl[l + 32 * k];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) e3acc_mac_base(s, z[k], x[k]);
+        }
+        for (; l < cnt; l += 32) e3acc_mac_base(s, zl[l], b0[base + l]);
     }
     return ef_mul(ef_fix(e3acc_reduce(s), a.ext2), zhi[h], a.ext2);
 }
 
 // ITEMS: one warp per (value, chunk) item, partials[k * hi_count + h] (few
 // chunks per value: small vectors, many vectors); otherwise each warp strides
-// over the chunks of every value and a CTA sum goes to partials[cta * nvals + k].
+// over the parts of every value -- chunks cut into 2^sub_log parts, so that a
+// vector of few chunks still spreads over many warps -- and a CTA sum goes to
+// partials[cta * nvals + k].
 template <bool ITEMS>
 __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u32 hi_count, E3* partials,
-                                                     unsigned* counter) {
+                                                     unsigned* counter, u32 sub_log) {
     __shared__ E3 red[32];
     __shared__ bool is_last;
     __shared__ E3 totals[OOD_MAX_VALUES];
@@ -473,7 +497,7 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u
             const u32 k = (u32)(it / hi_count), v = k % a.nvec, j = k / a.nvec;
             if (v >= a.skip_lo && v < a.skip_hi) continue;
             const E3* zlo = tab + (u64)j * per;
-            const E3 val = e3_warp_sum(ood_chunk(a, zlo, zlo + (1u << OOD_LO), v, it % hi_count, lane));
+            const E3 val = e3_warp_sum(ood_part(a, zlo, zlo + (1u << OOD_LO), v, it % hi_count, 0, 1u << OOD_LO, lane));
             if (lane == 0) partials[it] = val;
         }
         // every warp's partials visible device-wide before this CTA takes its ticket
@@ -485,7 +509,9 @@ __global__ void __launch_bounds__(OOD_THREADS) k_ood(OodArgs a, const E3* tab, u
             for (u32 v = 0; v < a.nvec; ++v) {
                 if (v >= a.skip_lo && v < a.skip_hi) continue;
                 E3 acc = e3_zero();
-                for (u64 h = gw; h < hi_count; h += nw) acc = e3_add(acc, ood_chunk(a, zlo, zlo + (1u << OOD_LO), v, h, lane));
+                const u32 len = 1u << (OOD_LO - sub_log), pmask = (1u << sub_log) - 1;
+                for (u64 it = gw; it < ((u64)hi_count << sub_log); it += nw)
+                    acc = e3_add(acc, ood_part(a, zlo, zlo + (1u << OOD_LO), v, it >> sub_log, ((u32)it & pmask) * len, len, lane));
                 E3 bs = block_sum_e3(acc, red);
                 if (threadIdx.x == 0) partials[(u64)blockIdx.x * nvals + (u32)j * a.nvec + v] = bs;
             }
@@ -550,11 +576,15 @@ int launch_ood(const OodArgs& a, cudaStream_t st) {
     // Few chunks per value: spread (value, chunk) items over the warps (the
     // partials fit: items <= OOD_GRID * scratch_values when hc <= OOD_GRID).
     const bool by_items = hc <= OOD_GRID && items > hc;
-    u64 want = ((by_items ? items : hc) + warps_per_cta - 1) / warps_per_cta;
     const u64 cap = std::min<u64>(4ull * device_sms(), (u64)OOD_GRID);
+    // Chunks of one value cut into up to 8 parts while the parts still fit
+    // the grid's warps once (a part is one product by the chunk's power more).
+    u32 sub_log = 0;
+    while (!by_items && sub_log < 3 && ((u64)hc << (sub_log + 1)) <= cap * warps_per_cta) ++sub_log;
+    u64 want = ((by_items ? items : ((u64)hc << sub_log)) + warps_per_cta - 1) / warps_per_cta;
     unsigned grid = (unsigned)(want < 1 ? 1 : (want > cap ? cap : want));
-    if (by_items) k_ood<true><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
-    else k_ood<false><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter);
+    if (by_items) k_ood<true><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter, 0);
+    else k_ood<false><<<grid, OOD_THREADS, 0, st>>>(a, tab, hc, partials, counter, sub_log);
     count_launches(1);
     return 0;
 }

@@ -238,14 +238,34 @@ __global__ void __launch_bounds__(256) k_tsc_rounds(TscRoundArgs a) {
     __shared__ E3 Z[TSC_MAX_TERMS << TSC_MAX_K];
     __shared__ E3 G[TSC_MAX_TERMS << TSC_MAX_K];
     __shared__ E3 rs[TSC_MAX_K];
+    __shared__ E3 scr[256];
     const u32 nb = 1u << a.k;
     const u32 nv = (u32)a.T * nb;
-    for (u32 v = threadIdx.x; v < nv; v += blockDim.x) {
+    if (nv <= blockDim.x && blockDim.x <= 256) {
+        // blockDim / nv threads per value, each over a strided share of its
+        // partials (independent loads in flight), then one sum per value.
+        const u32 per = blockDim.x / nv, v = threadIdx.x % nv, s = threadIdx.x / nv;
         E3 z = e3_zero();
-        const E3* p = a.part + (u64)v * a.parts;
-        for (u32 q = 0; q < a.parts; ++q) z = e3_add(z, p[q]);
-        Z[v] = z;
-        G[v] = a.top[v];
+        if (s < per) {
+            const E3* p = a.part + (u64)v * a.parts;
+            for (u32 q = s; q < a.parts; q += per) z = e3_add(z, p[q]);
+        }
+        scr[threadIdx.x] = z;
+        __syncthreads();
+        if (threadIdx.x < nv) {
+            E3 t = scr[threadIdx.x];
+            for (u32 k = 1; k < per; ++k) t = e3_add(t, scr[threadIdx.x + k * nv]);
+            Z[threadIdx.x] = t;
+            G[threadIdx.x] = a.top[threadIdx.x];
+        }
+    } else {
+        for (u32 v = threadIdx.x; v < nv; v += blockDim.x) {
+            E3 z = e3_zero();
+            const E3* p = a.part + (u64)v * a.parts;
+            for (u32 q = 0; q < a.parts; ++q) z = e3_add(z, p[q]);
+            Z[v] = z;
+            G[v] = a.top[v];
+        }
     }
     __syncthreads();
     if (threadIdx.x < 32) {

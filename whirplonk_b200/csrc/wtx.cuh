@@ -131,6 +131,7 @@ __device__ __forceinline__ void wtx_absorb_words(WarpTx& t, const u64* w, unsign
                 t.hpos = 0;
             }
         } else {
+#pragma unroll 1
             for (int b = 0; b < 8; ++b) wtx_absorb_byte(t, (u8)(v >> (8 * b)));
         }
     }
@@ -164,6 +165,7 @@ __device__ __forceinline__ u64 wtx_squeeze_word(WarpTx& t) {
         return v;
     }
     u64 v = 0;
+#pragma unroll 1
     for (int b = 0; b < 8; ++b) {
         if (t.rpos == TX_RATE) {
             t.r = keccak_f1600_warp(t.r);
@@ -228,12 +230,40 @@ __device__ __forceinline__ u64 wtx_challenge_base(WarpTx& t) {
     for (int i = 3; i >= 0; --i) acc = gl_reduce(w[i], acc);
     return acc;
 }
-__device__ __forceinline__ E3 wtx_challenge_e3(WarpTx& t) {
-    const u64 c0 = wtx_challenge_base(t);
-    const u64 c1 = wtx_challenge_base(t);
-    const u64 c2 = wtx_challenge_base(t);
-    return E3{c0, c1, c2};
+
+// ncomp (<= 3) consecutive base-field challenges, lane-parallel when their
+// 40 ncomp bytes start word-aligned inside the current reader block: lane k <
+// 5 ncomp takes squeezed word k and scales it by 2^(64 (k mod 5)) mod p (the
+// powers are 1, 2^32 - 1, p - 2^32, 1, 2^32 - 1), and lane c sums the five
+// terms of challenge c -- the integer sum_i w_i 2^(64 i) mod p that the
+// word-by-word fold above computes.  Otherwise the challenges are squeezed
+// word by word.  Returns challenge c in component c.
+__device__ __forceinline__ E3 wtx_challenges(WarpTx& t, u32 ncomp) {
+    wtx_reader(t);
+    const unsigned l = wtx_lane();
+    if ((t.rpos & 7) == 0 && t.rpos + 40 * ncomp <= TX_RATE) {
+        const u32 k = l < 5 * ncomp ? l : 0;
+        const u64 w = __shfl_sync(0xFFFFFFFFu, t.r, (t.rpos >> 3) + k);
+        const u32 i = k % 5;
+        const u64 scale = (i == 0 || i == 3) ? 1ull : (i == 2 ? GL_P - (1ull << 32) : GL_EPS);
+        const u64 term = gl_mul(w, scale);
+        const u32 src = l < ncomp ? 5 * l : 0;
+        u64 s = __shfl_sync(0xFFFFFFFFu, term, src);
+#pragma unroll 1
+        for (u32 q = 1; q < 5; ++q) s = gl_add(s, __shfl_sync(0xFFFFFFFFu, term, src + q));
+        t.rpos += 40 * ncomp;
+        const u64 c0 = __shfl_sync(0xFFFFFFFFu, s, 0);
+        const u64 c1 = __shfl_sync(0xFFFFFFFFu, s, 1);
+        const u64 c2 = __shfl_sync(0xFFFFFFFFu, s, 2);
+        return E3{c0, ncomp > 1 ? c1 : 0, ncomp > 2 ? c2 : 0};
+    }
+    E3 r{0, 0, 0};
+    r.c0 = wtx_challenge_base(t);
+    if (ncomp > 1) r.c1 = wtx_challenge_base(t);
+    if (ncomp > 2) r.c2 = wtx_challenge_base(t);
+    return r;
 }
+__device__ __forceinline__ E3 wtx_challenge_e3(WarpTx& t) { return wtx_challenges(t, 3); }
 
 // Elements of the protocol's target field.  With the base field as target
 // (Identity<Goldilocks>) its elements are carried as Ext3 values (x, 0, 0) --
@@ -242,13 +272,7 @@ __device__ __forceinline__ E3 wtx_challenge_e3(WarpTx& t) {
 // elements are carried as (c0, c1, 0) (products folded by e2_fold) and cross
 // it as two words / two 40-byte chunks (transcript.hpp:375-453).
 __device__ __forceinline__ E3 wtx_challenge_t(WarpTx& t) {
-    if (t.deg == 1) return E3{wtx_challenge_base(t), 0, 0};
-    if (t.deg == 2) {
-        const u64 c0 = wtx_challenge_base(t);
-        const u64 c1 = wtx_challenge_base(t);
-        return E3{c0, c1, 0};
-    }
-    return wtx_challenge_e3(t);
+    return wtx_challenges(t, t.deg == 1 ? 1u : (t.deg == 2 ? 2u : 3u));
 }
 __device__ __forceinline__ void wtx_message_t(WarpTx& t, E3 v) {
     if (t.deg == 1) {
@@ -274,9 +298,10 @@ __device__ __forceinline__ void wtx_geometric(WarpTx& t, E3* out, int count) {
         return;
     }
     const E3 x = wtx_challenge_t(t);
-    // lane k: x^k by an in-warp prefix product (Hillis-Steele on multipliers)
+    // lane k: x^k by an in-warp prefix product (Hillis-Steele on multipliers;
+    // rolled: one copy of the product's code to fetch)
     E3 p = l == 0 ? e3_one() : x;
-#pragma unroll
+#pragma unroll 1
     for (int o = 1; o < 32; o <<= 1) {
         const E3 q{__shfl_up_sync(0xFFFFFFFFu, p.c0, o), __shfl_up_sync(0xFFFFFFFFu, p.c1, o),
                    __shfl_up_sync(0xFFFFFFFFu, p.c2, o)};
