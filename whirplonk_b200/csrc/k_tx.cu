@@ -371,9 +371,13 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
     const u64 blk = row_hint + merkle_bytes;  // hint bytes of one commitment
     const bool fits = hint_base + blk * nwit <= tx->hints_cap;
 
-    // 2a. row hints
+    // 2a. row hints.  Every hint word sits at a multiple of 8 bytes from the
+    // commitment's hint block, so when the block starts 8-byte aligned (the
+    // hints stream holds whole words) a word is one 8-byte store.
+    const bool hints_al8 = (reinterpret_cast<uintptr_t>(tx->hints + hint_base) & 7) == 0;
     if (fits) {
-        const u64 nwords = (u64)q * a.depth * a.ncomp;
+        const u32 rw = a.depth * a.ncomp;  // words per row (<= MAX_DEPTH * 3)
+        const u32 nwords = q * rw;
         for (u32 w = 0; w < nwit; ++w) {
             unsigned char* hb = tx->hints + hint_base + w * blk;
             const u64* planes = a.planes + w * a.planes_stride;
@@ -381,13 +385,17 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
                 const u64 len = (u64)q * a.depth;
                 for (int k = 0; k < 8; ++k) hb[k] = (unsigned char)(len >> (8 * k));
             }
-            for (u64 x = t; x < nwords; x += blockDim.x) {
-                const u64 qi = x / ((u64)a.depth * a.ncomp);
-                const u64 rem = x - qi * a.depth * a.ncomp;
-                const u32 el = (u32)(rem / a.ncomp), c = (u32)(rem % a.ncomp);
+            for (u32 x = t; x < nwords; x += blockDim.x) {
+                const u32 qi = x / rw, rem = x - qi * rw;
+                const u32 el = rem / a.ncomp, c = rem - el * a.ncomp;
                 const u64 v = planes[((u64)c * a.depth + el) * a.N + codeword_row(idx_s[qi], a.logN, a.perm_log_e)];
                 unsigned char* dst = hb + 8 + qi * row_bytes + (u64)el * esz + 8ull * c;
-                for (int k = 0; k < 8; ++k) dst[k] = (unsigned char)(v >> (8 * k));
+                if (hints_al8) {
+                    *reinterpret_cast<u64*>(dst) = v;
+                } else {
+#pragma unroll 1
+                    for (int k = 0; k < 8; ++k) dst[k] = (unsigned char)(v >> (8 * k));
+                }
             }
         }
     }
@@ -445,8 +453,17 @@ __global__ void __launch_bounds__(OPEN_THREADS) k_open(OpenArgs a) {
                     const uint4* src = reinterpret_cast<const uint4*>(nodes + (level_off + (x ^ 1)) * 8);
                     const uint4 h0 = src[0], h1 = src[1];
                     unsigned char* dst = tx->hints + hint_base + w * blk + rel;
-                    const unsigned w8[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
-                    for (int k = 0; k < 32; ++k) dst[k] = (unsigned char)(w8[k >> 2] >> (8 * (k & 3)));
+                    if (hints_al8) {
+                        u64* d8 = reinterpret_cast<u64*>(dst);
+                        d8[0] = (u64)h0.x | ((u64)h0.y << 32);
+                        d8[1] = (u64)h0.z | ((u64)h0.w << 32);
+                        d8[2] = (u64)h1.x | ((u64)h1.y << 32);
+                        d8[3] = (u64)h1.z | ((u64)h1.w << 32);
+                    } else {
+                        const unsigned w8[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+#pragma unroll 1
+                        for (int k = 0; k < 32; ++k) dst[k] = (unsigned char)(w8[k >> 2] >> (8 * (k & 3)));
+                    }
                 }
             }
             rank += __popc(m);
