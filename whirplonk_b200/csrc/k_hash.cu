@@ -9,7 +9,8 @@
 //
 // Merkle tree (merkle_tree.hpp:104-147): parent = BLAKE3(left || right),
 // node array [leaves | level 1 | ... | root].  A CTA hashes a 512-leaf subtree
-// (9 levels) in shared memory, so a 2^22-leaf tree takes three launches.
+// (9 levels) in shared memory; a proof's tree ends with one launch for its
+// top 10-18 levels (k_merkle_tail).
 #include <algorithm>
 
 #include "launch.h"
@@ -248,6 +249,77 @@ int launch_leaves(const u64* planes, u64 N, u32 depth, u32 ncomp, u32* nodes, in
     return launch_leaves_batch(planes, N, depth, ncomp, nodes, 1, 0, 0, hash, st, perm_log_e);
 }
 
+// Levels level_in + 1 .. level_in + levels (1 <= levels <= 9) of subtree
+// `blk`, whose 2^levels children sit at level level_in from node blk 2^levels
+// on; every produced level is written to global memory and the working level
+// kept in shared memory.  CG: the children were written by other CTAs of the
+// same launch, so they are read through L2.  Ends with a CTA barrier.
+__device__ __forceinline__ void load_node_cg(const u32* nodes, u64 idx, unsigned* m) {
+    const uint4* p = reinterpret_cast<const uint4*>(nodes + idx * 8);
+    const uint4 a = __ldcg(p), b = __ldcg(p + 1);
+    m[0] = a.x; m[1] = a.y; m[2] = a.z; m[3] = a.w;
+    m[4] = b.x; m[5] = b.y; m[6] = b.z; m[7] = b.w;
+}
+template <int H, bool CG>
+__device__ __forceinline__ void merkle_subtree(u32* nodes, u32 logN, u32 level_in, u32 levels, u64 blk,
+                                               unsigned (*buf)[256 * 8]) {
+    const u32 nparents = 1u << (levels - 1);
+    const u64 in_off = level_offset(logN, level_in);
+    const u64 out_off = level_offset(logN, level_in + 1);
+    for (u32 t = threadIdx.x; t < nparents; t += blockDim.x) {
+        unsigned m[16];
+        const u64 child = (blk << levels) + 2 * t;
+        if (CG) {
+            load_node_cg(nodes, in_off + child, m);
+            load_node_cg(nodes, in_off + child + 1, m + 8);
+        } else {
+            load_node(nodes, in_off + child, m);
+            load_node(nodes, in_off + child + 1, m + 8);
+        }
+        unsigned cv[8];
+        hash64<H>(m, cv);
+        store_node(nodes, out_off + (blk << (levels - 1)) + t, cv);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) buf[0][t * 8 + k] = cv[k];
+    }
+    __syncthreads();
+    int cur = 0;
+    for (u32 lv = 1; lv < levels; ++lv) {
+        const u32 np = nparents >> lv;
+        const u64 off = level_offset(logN, level_in + 1 + lv);
+        for (u32 t = threadIdx.x; t < np; t += blockDim.x) {
+            unsigned m[16];
+#pragma unroll
+            for (int k = 0; k < 16; ++k) m[k] = buf[cur][t * 16 + k];
+            unsigned cv[8];
+            hash64<H>(m, cv);
+            store_node(nodes, off + (blk << (levels - 1 - lv)) + t, cv);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) buf[cur ^ 1][t * 8 + k] = cv[k];
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+}
+
+// Warp 0, after the root is written: root message, then the commitment's OOD
+// points (irs_commit.hpp:472-554).
+__device__ __forceinline__ void merkle_send_root(const u32* nodes, u32 logN, TxState* tx, ProofScalars* sc,
+                                                 int commit_idx, int n_ood) {
+    __threadfence();
+    const u64 root = level_offset(logN, logN);
+    u64 w[4];
+    for (int k = 0; k < 4; ++k) w[k] = (u64)nodes[root * 8 + 2 * k] | ((u64)nodes[root * 8 + 2 * k + 1] << 32);
+    WarpTx t;
+    wtx_load(t, tx);
+    wtx_message_words(t, w, 4);
+    for (int j = 0; j < n_ood; ++j) {
+        const E3 z = wtx_challenge_t(t);
+        if (threadIdx.x == 0) sc->ood_pts[commit_idx][j] = z;
+    }
+    wtx_store(t, tx);
+}
+
 // One CTA hashes a subtree of height `levels` whose children sit at level
 // `level_in`; every produced level is written to global memory.
 template <int H>
@@ -256,54 +328,31 @@ __global__ void __launch_bounds__(256) k_merkle(u32* nodes, u32 logN, u32 level_
                                                 u64 node_stride) {
     __shared__ unsigned buf[2][256 * 8];
     nodes += blockIdx.y * node_stride;
-    if (levels > 0) {
-        const u32 nparents = 1u << (levels - 1);
-        const u64 in_off = level_offset(logN, level_in);
-        const u64 out_off = level_offset(logN, level_in + 1);
-        for (u32 t = threadIdx.x; t < nparents; t += blockDim.x) {
-            unsigned m[16];
-            const u64 child = ((u64)blockIdx.x << levels) + 2 * t;
-            load_node(nodes, in_off + child, m);
-            load_node(nodes, in_off + child + 1, m + 8);
-            unsigned cv[8];
-            hash64<H>(m, cv);
-            store_node(nodes, out_off + ((u64)blockIdx.x << (levels - 1)) + t, cv);
-#pragma unroll
-            for (int k = 0; k < 8; ++k) buf[0][t * 8 + k] = cv[k];
-        }
-        __syncthreads();
-        int cur = 0;
-        for (u32 lv = 1; lv < levels; ++lv) {
-            const u32 np = nparents >> lv;
-            const u64 off = level_offset(logN, level_in + 1 + lv);
-            for (u32 t = threadIdx.x; t < np; t += blockDim.x) {
-                unsigned m[16];
-#pragma unroll
-                for (int k = 0; k < 16; ++k) m[k] = buf[cur][t * 16 + k];
-                unsigned cv[8];
-                hash64<H>(m, cv);
-                store_node(nodes, off + ((u64)blockIdx.x << (levels - 1 - lv)) + t, cv);
-#pragma unroll
-                for (int k = 0; k < 8; ++k) buf[cur ^ 1][t * 8 + k] = cv[k];
-            }
-            __syncthreads();
-            cur ^= 1;
-        }
+    if (levels > 0) merkle_subtree<H, false>(nodes, logN, level_in, levels, blockIdx.x, buf);
+    if (finish && tx && threadIdx.x < 32) merkle_send_root(nodes, logN, tx, sc, commit_idx, n_ood);
+}
+
+// The top 10 .. 18 levels of a proof's tree in one launch: CTA b hashes the
+// 512-node subtree b of level level_in (9 levels); the last CTA to finish (a
+// ticket in ProofScalars) hashes the 2^(logN - level_in - 9) subtree roots up
+// to the root and sends the root message -- what a subtree launch and a
+// one-CTA top launch did, less one launch and its wait.
+template <int H>
+__global__ void __launch_bounds__(256) k_merkle_tail(u32* nodes, u32 logN, u32 level_in, TxState* tx,
+                                                     ProofScalars* sc, int commit_idx, int n_ood) {
+    __shared__ unsigned buf[2][256 * 8];
+    __shared__ bool last;
+    merkle_subtree<H, false>(nodes, logN, level_in, 9, blockIdx.x, buf);
+    if (threadIdx.x == 0) {
+        __threadfence();  // this CTA's subtree root (written by thread 0) before its ticket
+        last = atomicAdd(&sc->counters[CTR_MERKLE_TAIL], 1u) == gridDim.x - 1;
     }
-    if (finish && tx && threadIdx.x < 32) {  // warp 0: root message, OOD points
-        __threadfence();
-        const u64 root = level_offset(logN, logN);
-        u64 w[4];
-        for (int k = 0; k < 4; ++k) w[k] = (u64)nodes[root * 8 + 2 * k] | ((u64)nodes[root * 8 + 2 * k + 1] << 32);
-        WarpTx t;
-        wtx_load(t, tx);
-        wtx_message_words(t, w, 4);
-        for (int j = 0; j < n_ood; ++j) {
-            const E3 z = wtx_challenge_t(t);
-            if (threadIdx.x == 0) sc->ood_pts[commit_idx][j] = z;
-        }
-        wtx_store(t, tx);
-    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    merkle_subtree<H, true>(nodes, logN, level_in + 9, logN - level_in - 9, 0, buf);
+    if (threadIdx.x < 32) merkle_send_root(nodes, logN, tx, sc, commit_idx, n_ood);
+    if (threadIdx.x == 0) sc->counters[CTR_MERKLE_TAIL] = 0;
 }
 
 // Three tree levels at once: a thread reads 8 consecutive nodes of level
@@ -343,8 +392,9 @@ static int merkle_levels_h(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, 
                            u64 node_stride, cudaStream_t st) {
     if (count == 0 || count > 65535 || (tx && count != 1)) return -1;
     u32 level = 0;
-    // wide levels: 3 at a time while a launch still has >= 2^12 threads
-    while (logN - level >= 3 + 12) {
+    // wide levels: 3 at a time while a launch still has >= 2^12 threads (and,
+    // for a proof's tree, until at most 18 levels are left for k_merkle_tail)
+    while (logN - level >= 3 + 12 && (!tx || logN - level > 18)) {
         const u64 threads = 1ull << (logN - level - 3);
         k_merkle8<H><<<dim3((unsigned)((threads + 255) / 256), count), 256, 0, st>>>(nodes, logN, level, node_stride);
         count_launches(1);
@@ -355,6 +405,11 @@ static int merkle_levels_h(u32* nodes, u32 logN, TxState* tx, ProofScalars* sc, 
             k_merkle<H><<<dim3(1, count), 32, 0, st>>>(nodes, logN, 0, 0, tx, sc, commit_idx, n_ood, 1, node_stride);
             count_launches(1);
         }
+        return 0;
+    }
+    if (tx && logN - level > 9 && logN - level <= 18) {
+        k_merkle_tail<H><<<1u << (logN - level - 9), 256, 0, st>>>(nodes, logN, level, tx, sc, commit_idx, n_ood);
+        count_launches(1);
         return 0;
     }
     while (level < logN) {

@@ -36,6 +36,13 @@ __device__ __forceinline__ u64 ldg64(const u64* p) { return __ldg(reinterpret_ca
 // Loads and stores of the load and store phases go in batches of NTT_BATCH
 // per thread: all loads of a batch are in flight before the first store.
 constexpr int NTT_BATCH = 8;
+// 16-byte accesses to two adjacent words (tile columns w, w + 1 of one row, or
+// words j, j + 1 of one scratch row): half the memory instructions for the
+// same bytes.  Used when the pass's bases are 16-byte aligned (NttPassArgs::vec2).
+constexpr int NTT_BATCH2 = NTT_BATCH / 2;
+__device__ __forceinline__ ulonglong2 ldg128(const u64* p) { return __ldg(reinterpret_cast<const ulonglong2*>(p)); }
+__device__ __forceinline__ ulonglong2 ld128(const u64* p) { return *reinterpret_cast<const ulonglong2*>(p); }
+__device__ __forceinline__ void st128(u64* p, u64 x, u64 y) { *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(x, y); }
 
 // Shared-memory word of column element e: one pad word every 32 words keeps
 // strided group accesses off a single bank.
@@ -218,7 +225,29 @@ __device__ __forceinline__ void tile_load(const NttPassArgs& a, const TileGeom& 
         // place by this kernel, so it is read with plain loads.
         const u64* p = first ? g.src + col0 + w : g.tmp + g.P * (1ull << logR) * S + col0 + w;
         const bool full = nrows % (NTT_BATCH * J) == 0 && (!first || ((u64)nrows << a.logS) <= a.m);
-        if (full && first) {
+        if (full && a.vec2 && a.logW >= 1) {
+            // Column pairs (2 wp, 2 wp + 1): one 16-byte load per row; rows
+            // advance by 2 J, so a batch of NTT_BATCH2 pairs covers the rows a
+            // batch of NTT_BATCH words does.
+            const u32 wp = threadIdx.x & ((W >> 1) - 1), J2 = blockDim.x >> (a.logW - 1);
+            const u32 jp0 = threadIdx.x >> (a.logW - 1);
+            u64* c0 = sm + 2 * wp * cs;
+            const u64* p2 = first ? g.src + col0 + 2 * wp : g.tmp + g.P * (1ull << logR) * S + col0 + 2 * wp;
+            for (u32 jb = jp0; jb < nrows; jb += NTT_BATCH2 * J2) {
+                ulonglong2 v[NTT_BATCH2];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b) {
+                    const u64* q = p2 + (u64)(jb + b * J2) * S;
+                    v[b] = first ? ldg128(q) : ld128(q);
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b) {
+                    const u32 r = pidx(bitrev(jb + b * J2, logR));
+                    c0[r] = v[b].x;
+                    c0[cs + r] = v[b].y;
+                }
+            }
+        } else if (full && first) {
             for (u32 jb = j0; jb < nrows; jb += NTT_BATCH * J) {
                 u64 v[NTT_BATCH];
 #pragma unroll
@@ -252,7 +281,28 @@ __device__ __forceinline__ void tile_load(const NttPassArgs& a, const TileGeom& 
         }
     } else {
         const u32 n = W << mrows_log, jmask = (1u << mrows_log) - 1;
-        if (!first && !a.twist && n % (NTT_BATCH * blockDim.x) == 0) {
+        if (!first && !a.twist && a.vec2 && mrows_log >= 1 && n % (NTT_BATCH * blockDim.x) == 0) {
+            // The previous pass's rows by word pairs (j, j + 1), j even: one
+            // 16-byte load; in bit-reversed order j + 1 lands R / 2 after j.
+            for (u32 eb = threadIdx.x; 2 * eb < n; eb += NTT_BATCH2 * blockDim.x) {
+                ulonglong2 v[NTT_BATCH2];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b) {
+                    const u32 e = 2 * (eb + b * blockDim.x);
+                    const u64 i0 = g.i0base + (e >> mrows_log);
+                    const u64 row = a.npass == 2 ? i0 : (i0 << a.logR1) + g.i1;
+                    v[b] = ldg128(g.tmp + (row << logR) + (e & jmask));
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b) {
+                    const u32 e = 2 * (eb + b * blockDim.x);
+                    u64* c = sm + (e >> mrows_log) * cs;
+                    const u32 r = bitrev(e & jmask, logR);
+                    c[pidx(r)] = v[b].x;
+                    c[pidx(r + (1u << (logR - 1)))] = v[b].y;
+                }
+            }
+        } else if (!first && !a.twist && n % (NTT_BATCH * blockDim.x) == 0) {
             // The previous pass's rows, whole batches.
             for (u32 eb = threadIdx.x; eb < n; eb += NTT_BATCH * blockDim.x) {
                 u64 v[NTT_BATCH];
@@ -394,7 +444,30 @@ __device__ __forceinline__ void tile_store(const NttPassArgs& a, const TileGeom&
         const u64 stride = (u64)J * S;
         u64* dst = g.tmp + (g.P * R + i) * S + col;
         const u64* scol = sm + w * cs;
-        if (a.tw_pass && R % (NTT_BATCH * J) == 0) {
+        if (a.tw_pass && a.vec2 && a.logW >= 1 && R % (NTT_BATCH * J) == 0) {
+            // Column pairs: the factors and the scratch words of (2 wp, 2 wp + 1)
+            // are adjacent, one 16-byte load and one 16-byte store per row.
+            const u32 wp = threadIdx.x & ((W >> 1) - 1), J2 = blockDim.x >> (a.logW - 1);
+            const u64 c2 = g.col0 + 2 * wp, stride2 = (u64)J2 * S;
+            u32 i2 = threadIdx.x >> (a.logW - 1);
+            u64* d2 = g.tmp + (g.P * R + i2) * S + c2;
+            const u64* t2 = a.tw_pass + (u64)i2 * S + c2;
+            const u64* s2 = sm + 2 * wp * cs;
+            for (; i2 < R; i2 += NTT_BATCH2 * J2, d2 += NTT_BATCH2 * stride2, t2 += NTT_BATCH2 * stride2) {
+                u64 x0[NTT_BATCH2], x1[NTT_BATCH2];
+                ulonglong2 f[NTT_BATCH2];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b) {
+                    const u32 r = pidx(i2 + b * J2);
+                    x0[b] = s2[r];
+                    x1[b] = s2[cs + r];
+                    f[b] = ldg128(t2 + b * stride2);
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b)
+                    st128(d2 + b * stride2, gl_mul_fma(x0[b], f[b].x), gl_mul_fma(x1[b], f[b].y));
+            }
+        } else if (a.tw_pass && R % (NTT_BATCH * J) == 0) {
             const u64* tcol = a.tw_pass + (u64)i * S + col;
             for (; i < R; i += NTT_BATCH * J, dst += NTT_BATCH * stride, tcol += NTT_BATCH * stride) {
                 u64 x[NTT_BATCH], f[NTT_BATCH];
@@ -428,7 +501,26 @@ __device__ __forceinline__ void tile_store(const NttPassArgs& a, const TileGeom&
         u32 i = threadIdx.x >> a.logW;
         u64* dst = out + obase + w + outer * i;
         const u64 stride = outer * J;
-        if (R % (NTT_BATCH * J) == 0) {
+        if (a.vec2 && a.logW >= 1 && (outer & 1) == 0 && R % (NTT_BATCH * J) == 0) {
+            // Column pairs: codeword words obase + 2 wp + outer i and the next
+            // one, a 16-byte store (obase is a multiple of W, outer even).
+            const u32 wp = threadIdx.x & ((W >> 1) - 1), J2 = blockDim.x >> (a.logW - 1);
+            u32 i2 = threadIdx.x >> (a.logW - 1);
+            const u64 stride2 = outer * J2;
+            u64* d2 = out + obase + 2 * wp + outer * i2;
+            const u64* s2 = sm + 2 * wp * cs;
+            for (; i2 < R; i2 += NTT_BATCH2 * J2, d2 += NTT_BATCH2 * stride2) {
+                u64 x0[NTT_BATCH2], x1[NTT_BATCH2];
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b) {
+                    const u32 r = pidx(i2 + b * J2);
+                    x0[b] = s2[r];
+                    x1[b] = s2[cs + r];
+                }
+#pragma unroll
+                for (int b = 0; b < NTT_BATCH2; ++b) st128(d2 + b * stride2, x0[b], x1[b]);
+            }
+        } else if (R % (NTT_BATCH * J) == 0) {
             for (; i < R; i += NTT_BATCH * J, dst += NTT_BATCH * stride) {
                 u64 x[NTT_BATCH];
 #pragma unroll
@@ -665,6 +757,11 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
     // LDE), and pass 0 is not launched.
     const bool twist = pl.npass == 2 && L.m <= (1ull << pl.logR[1]);
     a.planes = L.planes;
+    // 16-byte word pairs need 16-byte aligned plane bases: the scratch and the
+    // codeword (N >= 2 words a plane), and the message blocks (m even).
+    auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    bool vec2 = al16(L.tmp) && al16(L.out) && L.m % 2 == 0 && L.logN >= 1 && L.depth > 0;
+    for (u32 c = 0; L.depth > 0 && c < L.planes / L.depth && c < 3; ++c) vec2 = vec2 && al16(L.src[c]);
     u32 logrest = L.logN;
     for (u32 s = 0; s < pl.npass; ++s) {
         a.pass = s;
@@ -701,6 +798,7 @@ int launch_lde_plan(const LdeArgs& L, const LdePlan& pl, cudaStream_t st) {
         a.tw_pass = !L.tables ? nullptr
                     : s + 1 < pl.npass ? L.tables->get(a.logR + a.logS, a.logR)
                     : twist ? L.tables->get(L.logN, pl.logR[0]) : nullptr;
+        a.vec2 = vec2 && (!a.tw_pass || al16(a.tw_pass)) ? 1u : 0u;
         const u32 mb = pl.minb ? pl.minb : LDE_MINB_DEFAULT;
         const int occ = pl.pipe && !twist ? pipe_occupancy(mb, a.logR, a.logW) : 0;
         if (occ > 0) {

@@ -46,6 +46,7 @@ struct NttPassArgs {
     const u64* tw_hi;
     const u64* tw_lo;
     const u64* tw_pass;  // this pass boundary's LdeTables entry, or null
+    u32 vec2;            // every plane base and the message length allow 16-byte word pairs
 };
 struct LdeArgs {
     const u64* src[3];  // component planes of the message vector (block b at src[c] + b*m)

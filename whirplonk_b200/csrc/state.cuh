@@ -53,5 +53,7 @@ struct ProofScalars {
     unsigned char pow_ch[32];
     unsigned counters[64];                   // self-resetting last-block tickets
 };
+// ProofScalars::counters slots.
+constexpr int CTR_MERKLE_TAIL = 0;  // k_merkle_tail: subtree CTAs finished
 
 }  // namespace wg
