@@ -443,6 +443,11 @@ whirgpu_status whirgpu_measure_int_peaks(int device, double out[WHIRGPU_NUM_INT_
 whirgpu_status whirgpu_set_timing(whirgpu_ctx* ctx, int enabled);
 /* Number of kernels this library has launched in the process so far. */
 uint64_t whirgpu_launch_count(void);
+/* Workspace cache of the context: bytes of device memory its workspaces hold
+ * now, workspaces allocated so far, and idle workspaces freed to make room
+ * under an HBM budget (each such free synchronises the device). */
+whirgpu_status whirgpu_workspace_stats(whirgpu_ctx* ctx, uint64_t* cached_bytes, uint64_t* allocations,
+                                       uint64_t* evictions);
 whirgpu_status whirgpu_kernel_stats(whirgpu_ctx* ctx, uint64_t launches[WHIRGPU_NUM_FAMILIES],
                                     double ms[WHIRGPU_NUM_FAMILIES], int reset);
 

@@ -28,6 +28,7 @@ EXPORTED = [
     "whirgpu_commit", "whirgpu_commit_witnesses", "whirgpu_config_from_params", "whirgpu_commit_config", "whirgpu_witness_destroy", "whirgpu_prove", "whirgpu_prove_forms", "whirgpu_mle_evaluate", "whirgpu_mle_evaluate_noalloc",
     "whirgpu_debug_field_ops", "whirgpu_sample_goldilocks", "whirgpu_chacha20_block", "whirgpu_host_alloc", "whirgpu_host_free",
     "whirgpu_set_timing", "whirgpu_kernel_stats", "whirgpu_launch_count", "whirgpu_last_io_bytes",
+    "whirgpu_workspace_stats",
     "whirgpu_measure_int_peaks",
     "whirgpu_batch_create", "whirgpu_batch_run", "whirgpu_batch_proof", "whirgpu_batch_destroy",
     "whirgpu_server_create", "whirgpu_server_submit", "whirgpu_server_poll", "whirgpu_server_release",
@@ -208,6 +209,8 @@ def load() -> ctypes.CDLL:
     L.whirgpu_set_codeword_order.restype = ctypes.c_int
     L.whirgpu_measure_int_peaks.argtypes = [ctypes.c_int, p]
     L.whirgpu_measure_int_peaks.restype = ctypes.c_int
+    L.whirgpu_workspace_stats.argtypes = [p, ctypes.POINTER(u64), ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.whirgpu_workspace_stats.restype = ctypes.c_int
     L.whirgpu_launch_count.argtypes = []
     L.whirgpu_launch_count.restype = u64
     L.whirgpu_last_io_bytes.argtypes = [p, ctypes.POINTER(u64), ctypes.POINTER(u64)]

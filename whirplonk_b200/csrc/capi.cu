@@ -179,6 +179,7 @@ bool evict_idle(whirgpu_ctx* c, uint64_t need, uint64_t limit) {
         if (!victim) return limit == 0;
         owner->erase(std::find(owner->begin(), owner->end(), victim));
         free_workspace(c, victim);
+        ++c->ws_evictions;
     }
 }
 
@@ -260,6 +261,7 @@ whirgpu_status acquire_workspace_sched(whirgpu_ctx* c, const WhirSchedule& sched
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { cudaFree(w->dev); delete w; return cuda_fail(c, e, "cudaMemset"); }
     c->allocated += plan.total_bytes;
+    ++c->ws_allocations;
     w->busy = true;
     w->last_used = ++c->use_clock;
     c->cache[key].push_back(w);
@@ -834,6 +836,16 @@ whirgpu_status whirgpu_kernel_stats(whirgpu_ctx* c, uint64_t launches[WHIRGPU_NU
 }
 
 uint64_t whirgpu_launch_count(void) { return launch_count(); }
+
+whirgpu_status whirgpu_workspace_stats(whirgpu_ctx* ctx, uint64_t* cached_bytes, uint64_t* allocations,
+                                       uint64_t* evictions) {
+    if (!ctx) return WHIRGPU_E_INVALID;
+    std::lock_guard<std::recursive_mutex> lk(ctx->cache_mu);
+    if (cached_bytes) *cached_bytes = ctx->allocated;
+    if (allocations) *allocations = ctx->ws_allocations;
+    if (evictions) *evictions = ctx->ws_evictions;
+    return WHIRGPU_OK;
+}
 
 void whirgpu_last_io_bytes(const whirgpu_ctx* c, uint64_t* h2d, uint64_t* d2h) {
     if (h2d) *h2d = c ? c->io_h2d : 0;

@@ -96,6 +96,7 @@ struct whirgpu_ctx {
     cudaStream_t stream = nullptr;
     uint64_t budget = 0;
     uint64_t allocated = 0;
+    uint64_t ws_allocations = 0, ws_evictions = 0;  // workspaces allocated / freed to make room
     wg::DeviceTables tw;
     wg::LdeTables lde_tables;  // inter-pass twiddle factors of the LDE splits in use (tw.lde)
     std::string err;

@@ -137,6 +137,12 @@ class Context:
     def launch_count() -> int:
         return int(_lib.load().whirgpu_launch_count())
 
+    def workspace_stats(self) -> dict:
+        """Workspace cache: bytes held, workspaces allocated, idle ones evicted."""
+        vals = [ctypes.c_uint64() for _ in range(3)]
+        _lib.check(self._L.whirgpu_workspace_stats(self.handle, *[ctypes.byref(v) for v in vals]), self.handle)
+        return {"cached_bytes": vals[0].value, "allocations": vals[1].value, "evictions": vals[2].value}
+
     def mle_evaluate(self, coeffs, point, on_device_ptr: Optional[int] = None):
         """MultilinearExtension::evaluate of base coefficients at an Ext3 point."""
         point = np.ascontiguousarray(point, dtype=np.uint64).reshape(-1)
