@@ -86,7 +86,7 @@ __device__ __forceinline__ void leaf_sha256(const u64* __restrict__ planes, u64 
 // blockIdx.y selects one of several independent matrices (planes and node
 // arrays `plane_stride` / `node_stride` words apart).
 template <int NCOMP, int H>
-__global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes,
+__global__ void __launch_bounds__(256, NCOMP == 3 ? 3 : 1) k_leaves(const u64* __restrict__ planes, u64 N, u32 depth, u32* nodes,
                                                 u64 plane_stride, u64 node_stride, u32 logN, u32 perm_log_e) {
     const u64 k = (u64)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= N) return;
@@ -104,11 +104,16 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
     const u32 nblocks = (bytes + 63) / 64;
     unsigned cv[8];
     b3_init(cv);
-    // The next block's 8 words are loaded before this block is compressed, so
-    // their plane reads overlap the compression.
-    u64 nxt[8];
+    // Loads run ahead of the compressions: the next block's 8 words (base and
+    // Ext2 rows) or the next two blocks' (Ext3 rows, 6 blocks of 8 planes each),
+    // so their plane reads overlap the compressions.
+    constexpr int AHEAD = NCOMP == 3 ? 2 : 1;
+    u64 nxt[8], nxt2[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) nxt[q] = (u32)q < nwords ? row_word<NCOMP>(planes, N, depth, i, q) : 0;
+    for (int q = 0; q < 8; ++q) {
+        nxt[q] = (u32)q < nwords ? row_word<NCOMP>(planes, N, depth, i, q) : 0;
+        nxt2[q] = AHEAD == 2 && (u32)(8 + q) < nwords ? row_word<NCOMP>(planes, N, depth, i, 8 + q) : 0;
+    }
     for (u32 t = 0; t < nblocks; ++t) {
         unsigned m[16];
 #pragma unroll
@@ -116,7 +121,17 @@ __global__ void __launch_bounds__(256) k_leaves(const u64* __restrict__ planes, 
             m[2 * q] = (unsigned)nxt[q];
             m[2 * q + 1] = (unsigned)(nxt[q] >> 32);
         }
-        if (t + 1 < nblocks) {
+        if (AHEAD == 2) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) nxt[q] = nxt2[q];
+            if (t + 2 < nblocks) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const u32 w = (t + 2) * 8 + q;
+                    nxt2[q] = w < nwords ? row_word<NCOMP>(planes, N, depth, i, w) : 0;
+                }
+            }
+        } else if (t + 1 < nblocks) {
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
                 const u32 w = (t + 1) * 8 + q;
