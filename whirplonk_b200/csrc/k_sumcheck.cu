@@ -364,8 +364,9 @@ __global__ void __launch_bounds__(SC_SMALL_THREADS) k_sumcheck_small(ScSmallArgs
         }
         __syncthreads();
         if (warp == 0) {
-            const E3 C0 = e3_warp_sum(lane < SC_SMALL_WARPS ? red[0][lane] : e3_zero());
-            const E3 C2 = e3_warp_sum(lane < SC_SMALL_WARPS ? red[1][lane] : e3_zero());
+            const int nwarps = (int)(blockDim.x >> 5);
+            const E3 C0 = e3_warp_sum(lane < nwarps ? red[0][lane] : e3_zero());
+            const E3 C2 = e3_warp_sum(lane < nwarps ? red[1][lane] : e3_zero());
             wtx_message_t(wt, C0);
             wtx_message_t(wt, C2);
             const E3 rn = wtx_challenge_t(wt);
@@ -400,7 +401,12 @@ int launch_sumcheck_small(const SumcheckArgs& s, int rounds, int fold_after, cud
     a.tx = s.tx;
     a.sc = s.sc;
     a.ext2 = s.ext2;
-    k_sumcheck_small<<<1, SC_SMALL_THREADS, 0, st>>>(a);
+    // As many warps as round 0 has pairs for (one warp up to 32 pairs): the
+    // rounds are chains of transcript steps, and barriers and cross-warp sums
+    // over idle warps only lengthen them.
+    u32 threads = 32;
+    while (threads < (u32)SC_SMALL_THREADS && threads < (s.size >> 1)) threads <<= 1;
+    k_sumcheck_small<<<1, threads, 0, st>>>(a);
     count_launches(1);
     return 0;
 }
@@ -723,6 +729,60 @@ __global__ void __launch_bounds__(256, 3) k_cov_accumulate(CovAccArgs a, const E
     }
 }
 
+// Small vectors (few pairs, tens of points): a CTA of CA_SPLIT warps over 32
+// pairs, warp w taking the points j = w, w + CA_SPLIT, ...; the partial sums
+// meet in shared memory and warp 0 adds them to the covector.  The same field
+// sums as k_cov_accumulate (exact, so the grouping is free), with the point
+// loop spread over 8x the threads: at these sizes the loop's latency, not its
+// multiply-accumulates, is the cost.
+constexpr int CA_SPLIT = 8;
+constexpr u64 CA_SPLIT_MAX_PAIRS = 2048;
+__global__ void __launch_bounds__(32 * CA_SPLIT) k_cov_accumulate_split(CovAccArgs a, const E3* tab, const u64* lo_base,
+                                                                         u32 hi_count) {
+    constexpr u32 NL = 1u << CA_LO;
+    __shared__ E3 part[CA_SPLIT][2][32];
+    const u32 per = NL + hi_count;
+    const int npts = a.n_ext + a.n_base;
+    const u32 lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const u64 npair = (a.size + 1) >> 1;
+    const u64 pi = (u64)blockIdx.x * 32 + lane;
+    const u64 i = 2 * pi;
+    E3 s0 = e3_zero(), s1 = e3_zero();
+    if (pi < npair) {
+        const u32 hi = (u32)(i >> CA_LO), lo = (u32)(i & (NL - 1));  // lo even: lo + 1 < NL
+        for (int j = (int)w; j < npts; j += CA_SPLIT) {
+            const E3 h = tab[(u64)j * per + NL + hi];
+            if (j < a.n_ext) {
+                s0 = e3_add(s0, e3_mul(h, tab[(u64)j * per + lo]));
+                s1 = e3_add(s1, e3_mul(h, tab[(u64)j * per + lo + 1]));
+            } else {
+                const u64* lb = lo_base + (u64)(j - a.n_ext) * NL + lo;
+                s0 = e3_add(s0, e3_mul_base(h, lb[0]));
+                s1 = e3_add(s1, e3_mul_base(h, lb[1]));
+            }
+        }
+    }
+    part[w][0][lane] = s0;
+    part[w][1][lane] = s1;
+    __syncthreads();
+    if (w != 0 || pi >= npair) return;
+#pragma unroll 1
+    for (int k = 1; k < CA_SPLIT; ++k) {
+        s0 = e3_add(s0, part[k][0][lane]);
+        s1 = e3_add(s1, part[k][1][lane]);
+    }
+    s0 = ef_fix(s0, a.ext2);
+    s1 = ef_fix(s1, a.ext2);
+    a.cov[0][i] = gl_add(a.cov[0][i], s0.c0);
+    a.cov[1][i] = gl_add(a.cov[1][i], s0.c1);
+    a.cov[2][i] = gl_add(a.cov[2][i], s0.c2);
+    if (i + 1 < a.size) {
+        a.cov[0][i + 1] = gl_add(a.cov[0][i + 1], s1.c0);
+        a.cov[1][i + 1] = gl_add(a.cov[1][i + 1], s1.c1);
+        a.cov[2][i + 1] = gl_add(a.cov[2][i + 1], s1.c2);
+    }
+}
+
 static u32 ca_hi_count(u64 size) { return (u32)((size + (1ull << CA_LO) - 1) >> CA_LO) + 1; }
 
 size_t cov_acc_scratch_bytes(u64 size, int n_points) {
@@ -741,7 +801,13 @@ int launch_cov_accumulate(const CovAccArgs& a, cudaStream_t st) {
     count_launches(1);
     for (int c = 0; c < 3; ++c)
         if (reinterpret_cast<uintptr_t>(a.cov[c]) & 15) return -1;  // 16-byte pairs
-    u64 want = ((a.size + 1) / 2 + 255) / 256;
+    const u64 npair = (a.size + 1) / 2;
+    if (npair <= CA_SPLIT_MAX_PAIRS) {
+        k_cov_accumulate_split<<<(unsigned)((npair + 31) / 32), 32 * CA_SPLIT, 0, st>>>(a, tab, lo_base, hc);
+        count_launches(1);
+        return 0;
+    }
+    u64 want = (npair + 255) / 256;
     const u64 cap = (u64)device_sms() * 16;
     k_cov_accumulate<<<(unsigned)(want > cap ? cap : want), 256, 0, st>>>(a, tab, lo_base, hc);
     count_launches(1);
