@@ -137,6 +137,11 @@ def test_server_device_inputs_and_eviction():
                 assert res.status == 0 and (res.narg, res.hints) == expected[i], f"request {i} round {rounds}"
         st = srv.stats()
         assert st["peak_bytes"] <= budget
+        # four shapes through a cache that holds two: workspaces were allocated
+        # for each and idle ones evicted; what stays cached fits the budget
+        ws = ctx2.workspace_stats()
+        assert ws["allocations"] >= 4 and ws["evictions"] >= 1, ws
+        assert 0 < ws["cached_bytes"] <= budget, ws
         srv.close()
         ctx2.close()
     finally:
